@@ -1,0 +1,161 @@
+/*
+ * rkr.h -- C ABI of the B200 reverse k-ranks engine (librkr_b200.so).
+ *
+ * The engine answers reverse k-ranks queries over user and item embeddings with the index
+ * structures of DBGroup-SUSTech/reverse-k-ranks (QSRP): per-user sampled score thresholds
+ * ("SampleSearch"), per-user regression rank-bound models ("NormalLinearRegressionLP") and the SVD
+ * transform ("SVD").  Results are the reference's results, bit for bit: the same users in the same
+ * order with the same ranks and query scores as the reference's CPU path on the same inputs.
+ *
+ * Conventions.  Every function returns RKR_OK (0) or a negative status; rkr_last_error() describes
+ * the last failure of the calling thread.  Nothing calls exit().  Host pointers are plain C arrays,
+ * row-major; device pointers are marked d_.  One rkr_index owns one CUDA stream on one device;
+ * different handles may be used from different threads, one handle from one thread at a time.
+ * Reference citations are paths inside the reference project.
+ */
+#ifndef RKR_H
+#define RKR_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RKR_OK 0
+#define RKR_ERR_INVALID (-1)   /* bad argument or size */
+#define RKR_ERR_CUDA (-2)      /* CUDA runtime error */
+#define RKR_ERR_NOMEM (-3)     /* device or host allocation failed */
+#define RKR_ERR_STATE (-4)     /* the index lacks a structure the call needs */
+#define RKR_ERR_IO (-5)        /* file read/write failed */
+
+/* Query methods (the reference's --method_name values, src/app/ReverseRankIndex.cpp:107-172). */
+#define RKR_METHOD_QS 0              /* src/impl/QS.hpp */
+#define RKR_METHOD_QSRP_NORMAL_LP 1  /* src/impl/QSRPNormalLP.hpp */
+#define RKR_METHOD_US 2              /* src/impl/US.hpp */
+
+/* One result entry: the reference's UserRankElement (src/include/struct/UserRankElement.hpp:12-17). */
+typedef struct {
+    int32_t user_id;
+    int32_t rank;
+    float query_ip;
+} rkr_user_rank;
+
+/* Per-query counters: the reference's SingleQueryPerformance fields (src/include/util/FileIO.hpp:255-277)
+ * plus the candidate count and the number of items examined during refinement. */
+typedef struct {
+    int32_t n_prune;
+    int32_t n_result;
+    int32_t n_refine;
+    int32_t n_candidate;
+    int64_t n_compute_item;
+} rkr_query_stats;
+
+typedef struct rkr_index rkr_index;
+
+const char *rkr_last_error(void);
+int rkr_version(void);
+
+/* ---- index lifecycle -------------------------------------------------------------------------- */
+
+/* Replaces the in-memory parts of QS::BuildIndex / QSRPNormalLP::BuildIndex / US::BuildIndex
+ * (src/impl/QS.hpp:259-288, src/impl/QSRPNormalLP.hpp:289-323, src/impl/US.hpp:226-242): uploads
+ * the users (already L2-normalised, as readData leaves them, src/include/util/VectorIO.hpp:39-68)
+ * and the data items to `device`, and prepares the norm-ordered item copy that refinement scans
+ * (RefineCPUIPBound ctor, src/include/alg/DiskIndex/RefineByComputation/RefineCPUIPBound.hpp:417-467). */
+int rkr_index_create(int32_t device, const float *user, int64_t n_user, const float *item, int64_t n_item,
+                     int32_t dim, rkr_index **out);
+int rkr_index_destroy(rkr_index *index);
+
+/* The split dimension of the refinement bound (SVD::check_dim_, src/include/alg/SVD.hpp:126-128),
+ * used by QS as well as QSRPNormalLP (src/impl/QS.hpp:267-282). */
+int rkr_index_set_check_dim(rkr_index *index, int32_t check_dim);
+
+/* SampleSearch::LoadIndex payload (src/include/alg/RankBoundRefinement/SampleSearch.hpp:199-244):
+ * ranks [n_sample], ascending; thresholds [n_user][n_sample], each row descending. */
+int rkr_index_load_sample_search(rkr_index *index, const int32_t *sample_rank, int32_t n_sample,
+                                 const float *thresholds);
+
+/* NormalLinearRegressionLP::LoadIndex payload (src/include/alg/RegressionPruning/
+ * NormalLinearRegressionLP.hpp:448-487), one record per user: a, b, mu, sigma, error, score_max,
+ * score_min (records [n_user][7]). */
+int rkr_index_load_regression(rkr_index *index, const int32_t *sample_rank, int32_t n_sample,
+                              const float *records);
+
+/* SVD::LoadIndex payload (src/include/alg/SVD.hpp:258-292): transfer_item [dim][dim] and the
+ * transformed users [n_user][dim]; also sets check_dim. */
+int rkr_index_load_svd(rkr_index *index, int32_t check_dim, const float *transfer_item, const float *svd_user);
+
+/* Zeroes the per-user query-score vector that QSRPNormalLP carries from one query to the next
+ * (Index::queryIP_l_, src/impl/QSRPNormalLP.hpp:73,109); a fresh index starts zeroed. */
+int rkr_index_reset_state(rkr_index *index);
+
+/* Device bytes held by the index (BaseIndex::IndexSizeByte counterpart, src/include/struct/MethodBase.hpp:23). */
+int rkr_index_size_bytes(const rkr_index *index, uint64_t *bytes);
+
+/* Builds the thresholds for `sample_rank` on the device from the resident users and items and
+ * keeps them as the index's SampleSearch table (what bsibc computes,
+ * src/app/build-index/BuildSampleIndexByComputation.cpp:66-154).  thresholds_out (host,
+ * [n_user][n_sample]) may be NULL. */
+int rkr_index_build_sample_search(rkr_index *index, const int32_t *sample_rank, int32_t n_sample,
+                                  float *thresholds_out);
+
+/* ---- query -------------------------------------------------------------------------------------- */
+
+/* BaseIndex::Retrieval (src/include/struct/MethodBase.hpp:16-18) for `method` over host query
+ * vectors [n_query][dim].  out: host [n_answered][topk]; stats: host [n_answered] or NULL.
+ * US answers only the first 100 queries when n_sample <= 1000, as the reference does
+ * (src/impl/US.hpp:113); *n_answered says how many rows were written.  topk > n_user is
+ * RKR_ERR_INVALID (the reference exits, src/impl/QS.hpp:116-119); so is topk > 4096, the largest
+ * top-k the device assembly holds. */
+int rkr_retrieval(rkr_index *index, int32_t method, const float *query, int32_t n_query, int32_t topk,
+                  rkr_user_rank *out, rkr_query_stats *stats, int32_t *n_answered);
+
+/* Same, with the queries and outputs already in device memory of the index's device; runs on
+ * `stream` (a cudaStream_t, or NULL for the index's own stream) and returns after the work is
+ * enqueued and the result is complete on that stream. */
+int rkr_retrieval_device(rkr_index *index, int32_t method, const float *d_query, int32_t n_query, int32_t topk,
+                         rkr_user_rank *d_out, rkr_query_stats *d_stats, int32_t *n_answered, void *stream);
+
+/* ---- index build --------------------------------------------------------------------------------- */
+
+/* ComputeScoreTableBatch::ComputeSortItemsBatch (src/include/score_computation/ComputeScoreTableBatch.hpp:79-92):
+ * rows_out (host, [n_rows][n_item]) = scores of users [start, start + n_rows) against all items,
+ * each row sorted descending. */
+int rkr_score_sort_batch(rkr_index *index, int64_t start_user, int64_t n_rows, float *rows_out);
+
+/* ComputeQueryRankByComputation (src/app/build-index/QueryRankByComputation.hpp:122-242):
+ * accu_out (host, [n_sample_item][n_item + 1]) is, for each sampled item, the cumulative count of
+ * users by the item's rank (number of items scoring strictly above it). */
+int rkr_index_query_rank_distribution(rkr_index *index, const int32_t *sample_item, int32_t n_sample_item,
+                                      int32_t *accu_out);
+
+/* Host-side build steps (CPU; no device needed). */
+
+/* VectorMatrix::vectorNormalize (src/include/struct/VectorMatrix.hpp:51-66), in place. */
+int rkr_normalize(float *vectors, int64_t n, int32_t dim);
+/* SampleItem (src/app/build-index/QueryRankBySample.hpp:20-37): mt19937(0) shuffle of item ids. */
+int rkr_sample_item(int32_t n_item, int32_t n_sample_item, int32_t *out);
+/* ComputeSortKthRank (src/app/build-index/QueryRankBySample.hpp:103-134). */
+int rkr_sort_kth_rank(const int32_t *accu, int64_t n_item, int32_t n_sample_item, int32_t sample_topk,
+                      int32_t *sort_kth_out, int32_t *sort_sample_id_out);
+/* FindOptimalSampleFast with the OptimalPart candidates
+ * (src/include/alg/RankBoundRefinement/FindSampleRank/OptimalSampleRankFast.hpp:269-472);
+ * sort_kth ascending, accu_sorted rows in that order. */
+int rkr_find_optimal_sample_rank(int64_t n_user, int64_t n_item, int32_t n_sample, int32_t n_sample_query,
+                                 const int32_t *sort_kth, const int32_t *accu_sorted, int32_t *out,
+                                 int64_t *train_cost);
+/* FindUniformSample (src/include/alg/RankBoundRefinement/FindSampleRank/UniformSample.hpp:17-56). */
+int rkr_uniform_sample_rank(int32_t n_item, int32_t n_sample, int32_t *out);
+/* NormalLinearRegressionLP fit (StartPreprocess / BatchLoopPreprocess,
+ * NormalLinearRegressionLP.hpp:72-310): records_out [n_user][7] as rkr_index_load_regression takes. */
+int rkr_fit_regression(const float *thresholds, int64_t n_user, int32_t n_sample, float *records_out);
+/* SVD::PerformSVD (src/include/alg/SVD.hpp:62-124): thin SVD of the users, the transfer matrix,
+ * the transformed users and check_dim for the given sigma ratio. */
+int rkr_svd_build(const float *user, int64_t n_user, int32_t dim, float sigma, float *transfer_item_out,
+                  float *svd_user_out, int32_t *check_dim_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RKR_H */

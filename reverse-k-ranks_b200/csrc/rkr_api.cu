@@ -1,0 +1,342 @@
+// rkr_api.cu -- the C ABI of librkr_b200.so (declared in include/rkr.h).
+#include <algorithm>
+#include <cstdarg>
+#include <cstring>
+#include <numeric>
+#include <vector>
+
+#include "rkr_internal.cuh"
+
+namespace rkr {
+
+static thread_local char g_err[1024] = "";
+
+void set_error(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof g_err, fmt, ap);
+    va_end(ap);
+}
+
+int ensure_device(const rkr_index *ix) {
+    RKR_CUDA(cudaSetDevice(ix->device));
+    return RKR_OK;
+}
+
+// ||v|| = sqrt(InnerProduct(v + off, v + off, len)) per row (RefineCPUIPBound.hpp:433-437,
+// RefineCPUPartDimPartNorm.hpp:39-54, PartDimPartNorm.hpp:41-50).
+__global__ void row_norm_kernel(const float *__restrict__ v, int64_t n, int dim, int off, float *__restrict__ out) {
+    const int64_t r = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    const float *p = v + r * dim + off;
+    out[r] = __fsqrt_rn(exact_dot(p, p, dim - off));
+}
+
+__global__ void gather_rows_kernel(const float *__restrict__ src, const int32_t *__restrict__ idx, int64_t n, int dim,
+                                   float *__restrict__ dst) {
+    const int64_t r = blockIdx.x;
+    if (r >= n) return;
+    const float *s = src + (int64_t) idx[r] * dim;
+    for (int j = threadIdx.x; j < dim; j += blockDim.x) dst[r * dim + j] = s[j];
+}
+
+// Norms the refinement bound needs for the current check_dim (recomputed when it changes).
+int refine_prepare_norms(rkr_index *ix) {
+    const int c = ix->check_dim;
+    RKR_TRY(ix->item_rnorm.ensure(sizeof(float) * ix->n_item));
+    RKR_TRY(ix->user_rnorm.ensure(sizeof(float) * ix->n_user));
+    row_norm_kernel<<<(unsigned) ((ix->n_item + 255) / 256), 256, 0, ix->stream>>>(ix->item_sorted.as<float>(), ix->n_item,
+                                                                                  ix->dim, c, ix->item_rnorm.as<float>());
+    RKR_CUDA(cudaGetLastError());
+    row_norm_kernel<<<(unsigned) ((ix->n_user + 255) / 256), 256, 0, ix->stream>>>(ix->user.as<float>(), ix->n_user,
+                                                                                  ix->dim, c, ix->user_rnorm.as<float>());
+    RKR_CUDA(cudaGetLastError());
+    if (ix->has_svd) {
+        RKR_TRY(ix->svd_unorm.ensure(sizeof(float) * ix->n_user));
+        row_norm_kernel<<<(unsigned) ((ix->n_user + 255) / 256), 256, 0, ix->stream>>>(
+            ix->svd_user.as<float>(), ix->n_user, ix->dim, c, ix->svd_unorm.as<float>());
+        RKR_CUDA(cudaGetLastError());
+    }
+    RKR_CUDA(cudaStreamSynchronize(ix->stream));
+    return RKR_OK;
+}
+
+}  // namespace rkr
+
+using namespace rkr;
+
+extern "C" {
+
+const char *rkr_last_error(void) { return g_err; }
+
+int rkr_version(void) { return 1; }
+
+int rkr_index_create(int32_t device, const float *user, int64_t n_user, const float *item, int64_t n_item, int32_t dim,
+                     rkr_index **out) {
+    RKR_REQUIRE(out && user && item, "rkr_index_create: null argument");
+    RKR_REQUIRE(n_user > 0 && n_item > 0 && dim > 0, "rkr_index_create: empty user/item set or dim");
+    RKR_REQUIRE(n_user < (int64_t(1) << 31) && n_item < (int64_t(1) << 31) && dim <= 4096,
+                "rkr_index_create: sizes out of range");
+    *out = nullptr;
+    int n_dev = 0;
+    RKR_CUDA(cudaGetDeviceCount(&n_dev));
+    RKR_REQUIRE(device >= 0 && device < n_dev, "rkr_index_create: device %d of %d", device, n_dev);
+    rkr_index *ix = new rkr_index();
+    ix->device = device;
+    ix->n_user = n_user;
+    ix->n_item = n_item;
+    ix->dim = dim;
+    auto fail = [&](int s) {
+        rkr_index_destroy(ix);
+        return s;
+    };
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ix->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        set_error("rkr_index_create: %s", cudaGetErrorString(e));
+        return fail(RKR_ERR_CUDA);
+    }
+    int s;
+    if ((s = ix->user.ensure(sizeof(float) * n_user * dim)) || (s = ix->item.ensure(sizeof(float) * n_item * dim)) ||
+        (s = ix->item_sorted.ensure(sizeof(float) * n_item * dim)) || (s = ix->item_norm.ensure(sizeof(float) * n_item)) ||
+        (s = ix->qip_state.ensure(sizeof(float) * n_user)))
+        return fail(s);
+    e = cudaMemcpyAsync(ix->user.p, user, sizeof(float) * n_user * dim, cudaMemcpyHostToDevice, ix->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ix->item.p, item, sizeof(float) * n_item * dim, cudaMemcpyHostToDevice, ix->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ix->qip_state.p, 0, sizeof(float) * n_user, ix->stream);
+    if (e != cudaSuccess) {
+        set_error("rkr_index_create: upload: %s", cudaGetErrorString(e));
+        return fail(RKR_ERR_CUDA);
+    }
+    // Items by norm, descending (RefineCPUIPBound.hpp:430-452).
+    row_norm_kernel<<<(unsigned) ((n_item + 255) / 256), 256, 0, ix->stream>>>(ix->item.as<float>(), n_item, dim, 0,
+                                                                              ix->item_norm.as<float>());
+    std::vector<float> norm(n_item);
+    e = cudaMemcpyAsync(norm.data(), ix->item_norm.p, sizeof(float) * n_item, cudaMemcpyDeviceToHost, ix->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ix->stream);
+    if (e != cudaSuccess) {
+        set_error("rkr_index_create: norms: %s", cudaGetErrorString(e));
+        return fail(RKR_ERR_CUDA);
+    }
+    std::vector<int32_t> order(n_item);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return norm[a] > norm[b]; });
+    ix->h_item_order = order;
+    ix->h_item_norm_sorted.resize(n_item);
+    for (int64_t i = 0; i < n_item; i++) ix->h_item_norm_sorted[i] = norm[order[i]];
+    if ((s = ix->ws_misc.ensure(sizeof(int32_t) * n_item))) return fail(s);
+    e = cudaMemcpyAsync(ix->ws_misc.p, order.data(), sizeof(int32_t) * n_item, cudaMemcpyHostToDevice, ix->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ix->item_norm.p, ix->h_item_norm_sorted.data(), sizeof(float) * n_item, cudaMemcpyHostToDevice,
+                            ix->stream);
+    if (e != cudaSuccess) {
+        set_error("rkr_index_create: %s", cudaGetErrorString(e));
+        return fail(RKR_ERR_CUDA);
+    }
+    gather_rows_kernel<<<(unsigned) n_item, 64, 0, ix->stream>>>(ix->item.as<float>(), ix->ws_misc.as<int32_t>(), n_item,
+                                                                dim, ix->item_sorted.as<float>());
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ix->stream);
+    if (e != cudaSuccess) {
+        set_error("rkr_index_create: %s", cudaGetErrorString(e));
+        return fail(RKR_ERR_CUDA);
+    }
+    *out = ix;
+    return RKR_OK;
+}
+
+int rkr_index_destroy(rkr_index *ix) {
+    if (!ix) return RKR_OK;
+    cudaSetDevice(ix->device);
+    if (ix->stream) cudaStreamSynchronize(ix->stream);
+    for (DevBuf *b : {&ix->user, &ix->item, &ix->item_sorted, &ix->item_norm, &ix->item_rnorm, &ix->user_rnorm,
+                      &ix->sample_rank, &ix->thr, &ix->reg_rank, &ix->reg, &ix->transfer_item, &ix->svd_user,
+                      &ix->svd_unorm, &ix->qip_state, &ix->ws_query, &ix->ws_qtr, &ix->ws_qnorm, &ix->ws_bucket,
+                      &ix->ws_bucket2, &ix->ws_levels, &ix->ws_cls, &ix->ws_counts, &ix->ws_hist, &ix->ws_res,
+                      &ix->ws_cand, &ix->ws_cand_off, &ix->ws_refine, &ix->ws_rank, &ix->ws_out, &ix->ws_stats,
+                      &ix->ws_misc})
+        b->release();
+    if (ix->stream) cudaStreamDestroy(ix->stream);
+    delete ix;
+    return RKR_OK;
+}
+
+int rkr_index_set_check_dim(rkr_index *ix, int32_t check_dim) {
+    RKR_REQUIRE(ix, "null index");
+    RKR_REQUIRE(check_dim >= 0 && check_dim <= ix->dim, "check_dim %d outside [0, %d]", check_dim, ix->dim);
+    RKR_TRY(ensure_device(ix));
+    ix->check_dim = check_dim;
+    return refine_prepare_norms(ix);
+}
+
+int rkr_index_load_sample_search(rkr_index *ix, const int32_t *sample_rank, int32_t n_sample, const float *thresholds) {
+    RKR_REQUIRE(ix && sample_rank && thresholds, "null argument");
+    // SampleSearch ctor: 0 < n_sample < n_data_item (SampleSearch.hpp:35-38)
+    RKR_REQUIRE(n_sample > 0 && n_sample < ix->n_item, "n_sample %d must be in (0, n_item)", n_sample);
+    RKR_REQUIRE(n_sample <= 0xfffe, "n_sample %d too large", n_sample);
+    for (int j = 0; j < n_sample; j++) {
+        RKR_REQUIRE(sample_rank[j] >= 0 && sample_rank[j] < ix->n_item, "sample rank %d out of range", sample_rank[j]);
+        RKR_REQUIRE(j == 0 || sample_rank[j] >= sample_rank[j - 1], "sample ranks must be ascending");
+    }
+    RKR_TRY(ensure_device(ix));
+    RKR_TRY(ix->sample_rank.ensure(sizeof(int32_t) * n_sample));
+    RKR_TRY(ix->thr.ensure(sizeof(float) * (size_t) ix->n_user * n_sample));
+    RKR_CUDA(cudaMemcpyAsync(ix->sample_rank.p, sample_rank, sizeof(int32_t) * n_sample, cudaMemcpyHostToDevice, ix->stream));
+    RKR_CUDA(cudaMemcpyAsync(ix->thr.p, thresholds, sizeof(float) * (size_t) ix->n_user * n_sample, cudaMemcpyHostToDevice,
+                             ix->stream));
+    RKR_CUDA(cudaStreamSynchronize(ix->stream));
+    ix->n_sample = n_sample;
+    ix->h_sample_rank.assign(sample_rank, sample_rank + n_sample);
+    return RKR_OK;
+}
+
+int rkr_index_build_sample_search(rkr_index *ix, const int32_t *sample_rank, int32_t n_sample, float *thresholds_out) {
+    RKR_REQUIRE(ix && sample_rank, "null argument");
+    RKR_REQUIRE(n_sample > 0 && n_sample < ix->n_item && n_sample <= 0xfffe, "n_sample %d must be in (0, n_item)",
+                n_sample);
+    for (int j = 0; j < n_sample; j++) {
+        RKR_REQUIRE(sample_rank[j] >= 0 && sample_rank[j] < ix->n_item, "sample rank %d out of range", sample_rank[j]);
+        RKR_REQUIRE(j == 0 || sample_rank[j] >= sample_rank[j - 1], "sample ranks must be ascending");
+    }
+    RKR_TRY(build_sample_search(ix, sample_rank, n_sample));
+    if (thresholds_out) {
+        RKR_CUDA(cudaMemcpy(thresholds_out, ix->thr.p, sizeof(float) * (size_t) ix->n_user * n_sample,
+                            cudaMemcpyDeviceToHost));
+    }
+    return RKR_OK;
+}
+
+int rkr_index_load_regression(rkr_index *ix, const int32_t *sample_rank, int32_t n_sample, const float *records) {
+    RKR_REQUIRE(ix && sample_rank && records, "null argument");
+    RKR_REQUIRE(n_sample > 0 && n_sample <= 0xfffd, "n_sample %d out of range", n_sample);
+    for (int j = 0; j < n_sample; j++)
+        RKR_REQUIRE(sample_rank[j] >= 0 && sample_rank[j] <= ix->n_item, "regression sample rank %d out of range",
+                    sample_rank[j]);
+    RKR_TRY(ensure_device(ix));
+    std::vector<float> rec8((size_t) ix->n_user * 8, 0.0f);
+    for (int64_t u = 0; u < ix->n_user; u++) std::memcpy(&rec8[u * 8], records + u * 7, 7 * sizeof(float));
+    RKR_TRY(ix->reg_rank.ensure(sizeof(int32_t) * n_sample));
+    RKR_TRY(ix->reg.ensure(sizeof(float) * rec8.size()));
+    RKR_CUDA(cudaMemcpyAsync(ix->reg_rank.p, sample_rank, sizeof(int32_t) * n_sample, cudaMemcpyHostToDevice, ix->stream));
+    RKR_CUDA(cudaMemcpyAsync(ix->reg.p, rec8.data(), sizeof(float) * rec8.size(), cudaMemcpyHostToDevice, ix->stream));
+    RKR_CUDA(cudaStreamSynchronize(ix->stream));
+    ix->n_sample_reg = n_sample;
+    return RKR_OK;
+}
+
+int rkr_index_load_svd(rkr_index *ix, int32_t check_dim, const float *transfer_item, const float *svd_user) {
+    RKR_REQUIRE(ix && transfer_item && svd_user, "null argument");
+    RKR_REQUIRE(check_dim >= 0 && check_dim <= ix->dim, "check_dim %d outside [0, %d]", check_dim, ix->dim);
+    RKR_TRY(ensure_device(ix));
+    const size_t d = (size_t) ix->dim;
+    RKR_TRY(ix->transfer_item.ensure(sizeof(float) * d * d));
+    RKR_TRY(ix->svd_user.ensure(sizeof(float) * (size_t) ix->n_user * d));
+    RKR_CUDA(cudaMemcpyAsync(ix->transfer_item.p, transfer_item, sizeof(float) * d * d, cudaMemcpyHostToDevice, ix->stream));
+    RKR_CUDA(cudaMemcpyAsync(ix->svd_user.p, svd_user, sizeof(float) * (size_t) ix->n_user * d, cudaMemcpyHostToDevice,
+                             ix->stream));
+    ix->has_svd = true;
+    ix->check_dim = check_dim;
+    return refine_prepare_norms(ix);
+}
+
+int rkr_index_reset_state(rkr_index *ix) {
+    RKR_REQUIRE(ix, "null index");
+    RKR_TRY(ensure_device(ix));
+    RKR_CUDA(cudaMemsetAsync(ix->qip_state.p, 0, sizeof(float) * ix->n_user, ix->stream));
+    RKR_CUDA(cudaStreamSynchronize(ix->stream));
+    return RKR_OK;
+}
+
+int rkr_index_size_bytes(const rkr_index *ix, uint64_t *bytes) {
+    RKR_REQUIRE(ix && bytes, "null argument");
+    uint64_t s = 0;
+    for (const DevBuf *b : {&ix->user, &ix->item, &ix->item_sorted, &ix->item_norm, &ix->item_rnorm, &ix->user_rnorm,
+                            &ix->sample_rank, &ix->thr, &ix->reg_rank, &ix->reg, &ix->transfer_item, &ix->svd_user,
+                            &ix->svd_unorm, &ix->qip_state})
+        s += b->bytes;
+    *bytes = s;
+    return RKR_OK;
+}
+
+static int check_query_args(rkr_index *ix, int32_t method, int32_t n_query, int32_t topk, int32_t *n_answered) {
+    RKR_REQUIRE(ix, "null index");
+    RKR_REQUIRE(method == RKR_METHOD_QS || method == RKR_METHOD_QSRP_NORMAL_LP || method == RKR_METHOD_US,
+                "unknown method %d", method);
+    RKR_REQUIRE(n_query >= 0, "negative n_query");
+    // QS.hpp:116-119: "top-k is too large"; topk < 1 leaves the reference's heaps empty.
+    RKR_REQUIRE(topk >= 1 && topk <= ix->n_user, "topk %d outside [1, n_user=%lld]", topk, (long long) ix->n_user);
+    RKR_REQUIRE(topk <= 4096, "topk %d above the supported maximum of 4096", topk);
+    if (ix->n_sample <= 0) {
+        set_error("method needs the sampled-threshold index (load or build it first)");
+        return RKR_ERR_STATE;
+    }
+    if (method != RKR_METHOD_US && ix->check_dim < 0) {
+        set_error("method needs check_dim (rkr_index_set_check_dim or rkr_index_load_svd)");
+        return RKR_ERR_STATE;
+    }
+    if (method == RKR_METHOD_QSRP_NORMAL_LP && (!ix->has_svd || ix->n_sample_reg <= 0)) {
+        set_error("QSRPNormalLP needs the SVD transform and the regression models");
+        return RKR_ERR_STATE;
+    }
+    int nq = n_query;
+    if (method == RKR_METHOD_US && ix->n_sample <= 1000) {  // US.hpp:113
+        RKR_REQUIRE(n_query >= 100, "US with n_sample <= 1000 answers exactly 100 queries; got %d", n_query);
+        nq = 100;
+    }
+    if (n_answered) *n_answered = nq;
+    return RKR_OK;
+}
+
+int rkr_retrieval_device(rkr_index *ix, int32_t method, const float *d_query, int32_t n_query, int32_t topk,
+                         rkr_user_rank *d_out, rkr_query_stats *d_stats, int32_t *n_answered, void *stream) {
+    int32_t nq = 0;
+    RKR_TRY(check_query_args(ix, method, n_query, topk, &nq));
+    if (n_answered) *n_answered = nq;
+    if (nq == 0) return RKR_OK;
+    RKR_REQUIRE(d_query && d_out, "null query/output pointer");
+    RKR_TRY(ensure_device(ix));
+    cudaStream_t st = stream ? (cudaStream_t) stream : ix->stream;
+    return query_batch(ix, method, d_query, nq, topk, d_out, d_stats, st);
+}
+
+int rkr_retrieval(rkr_index *ix, int32_t method, const float *query, int32_t n_query, int32_t topk, rkr_user_rank *out,
+                  rkr_query_stats *stats, int32_t *n_answered) {
+    int32_t nq = 0;
+    RKR_TRY(check_query_args(ix, method, n_query, topk, &nq));
+    if (n_answered) *n_answered = nq;
+    if (nq == 0) return RKR_OK;
+    RKR_REQUIRE(query && out, "null query/output pointer");
+    RKR_TRY(ensure_device(ix));
+    const size_t qb = sizeof(float) * (size_t) nq * ix->dim;
+    const size_t ob = sizeof(rkr_user_rank) * (size_t) nq * topk;
+    const size_t sb = sizeof(rkr_query_stats) * (size_t) nq;
+    RKR_TRY(ix->ws_query.ensure(qb));
+    RKR_TRY(ix->ws_out.ensure(ob));
+    RKR_TRY(ix->ws_stats.ensure(sb));
+    RKR_CUDA(cudaMemcpyAsync(ix->ws_query.p, query, qb, cudaMemcpyHostToDevice, ix->stream));
+    RKR_TRY(query_batch(ix, method, ix->ws_query.as<float>(), nq, topk, ix->ws_out.as<rkr_user_rank>(),
+                        stats ? ix->ws_stats.as<rkr_query_stats>() : nullptr, ix->stream));
+    RKR_CUDA(cudaMemcpyAsync(out, ix->ws_out.p, ob, cudaMemcpyDeviceToHost, ix->stream));
+    if (stats) RKR_CUDA(cudaMemcpyAsync(stats, ix->ws_stats.p, sb, cudaMemcpyDeviceToHost, ix->stream));
+    RKR_CUDA(cudaStreamSynchronize(ix->stream));
+    return RKR_OK;
+}
+
+int rkr_score_sort_batch(rkr_index *ix, int64_t start_user, int64_t n_rows, float *rows_out) {
+    RKR_REQUIRE(ix && rows_out, "null argument");
+    RKR_REQUIRE(start_user >= 0 && n_rows >= 0 && start_user + n_rows <= ix->n_user, "user range out of bounds");
+    if (n_rows == 0) return RKR_OK;
+    return score_sort_rows(ix, start_user, n_rows, rows_out);
+}
+
+int rkr_index_query_rank_distribution(rkr_index *ix, const int32_t *sample_item, int32_t n_sample_item,
+                                      int32_t *accu_out) {
+    RKR_REQUIRE(ix && sample_item && accu_out, "null argument");
+    RKR_REQUIRE(n_sample_item > 0 && n_sample_item <= ix->n_item, "n_sample_item %d out of range", n_sample_item);
+    for (int s = 0; s < n_sample_item; s++)
+        RKR_REQUIRE(sample_item[s] >= 0 && sample_item[s] < ix->n_item, "sample item %d out of range", sample_item[s]);
+    return query_rank_distribution(ix, sample_item, n_sample_item, accu_out);
+}
+
+}  // extern "C"

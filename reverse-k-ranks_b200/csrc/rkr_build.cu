@@ -1,0 +1,374 @@
+// rkr_build.cu -- index build on the device: score rows, sampled thresholds, query-rank distribution.
+//
+// The reference sorts every user's full score row and then reads a few positions
+// (ComputeScoreTableBatch + SampleSearch::LoopPreprocess, bsibc; QueryRankCPU + lower_bound, qdibc).
+// Here a batch of users' rows is computed exactly (binary32, reference order) into device memory,
+// and one CTA per row finds only what is asked for: it bins the row by value (bins are a
+// monotone function of the score, so they keep the order), scatters it into bin order, and sorts
+// only the bins that contain a requested position.  The row is never sorted as a whole unless a
+// full sort is what the caller wants (rkr_score_sort_batch).
+#include <algorithm>
+#include <vector>
+
+#include "rkr_internal.cuh"
+
+namespace rkr {
+
+constexpr int kBins = 4096;
+constexpr int kSelThreads = 512;
+
+// Score rows of users [u0, u0 + nu) against all items: rows[u - u0][i] = InnerProduct(user, item)
+// (CPUScoreTable.hpp:372-386), stored with row stride ld.
+__global__ void __launch_bounds__(kTileThreads) score_rows_kernel(const float *__restrict__ item, int64_t n_item,
+                                                                 const float *__restrict__ user, int64_t u0, int64_t nu,
+                                                                 int dim, float *__restrict__ rows, int64_t ld) {
+    __shared__ TileSmem sm;
+    const int64_t a0 = (int64_t) blockIdx.x * kTile;  // items
+    const int64_t b0 = (int64_t) blockIdx.y * kTile;  // users (relative to u0)
+    float lo[4][4], hi[4][4];
+    exact_tile(sm, item, nullptr, n_item, dim, a0, user + u0 * dim, nu, dim, b0, dim, dim, lo, hi);
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        const int64_t u = b0 + 4 * ty + j;
+        if (u >= nu) continue;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int64_t it = a0 + 4 * tx + i;
+            if (it < n_item) rows[u * ld + it] = lo[i][j];
+        }
+    }
+}
+
+// Ascending sort of up to 32 keys held one per lane (missing lanes hold +inf).
+__device__ __forceinline__ float warp_sort32(float v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const float o = __shfl_xor_sync(0xffffffffu, v, j);
+            const bool up = (lane & k) == 0;
+            const bool lower = (lane & j) == 0;
+            v = (lower == up) ? fminf(v, o) : fmaxf(v, o);
+        }
+    return v;
+}
+
+// The l-th smallest value (0-based) of seg[0..n) for one warp; every lane returns it.
+// Values are compared as floats (the reference sorts floats with std::greater; NaNs do not occur).
+__device__ float warp_select(const float *seg, int n, int l) {
+    const int lane = threadIdx.x & 31;
+    if (n <= 32) {
+        float v = lane < n ? seg[lane] : __int_as_float(0x7f800000);
+        v = warp_sort32(v);
+        return __shfl_sync(0xffffffffu, v, l);
+    }
+    float ans = 0.0f;
+    bool found = false;
+    for (int i0 = 0; i0 < n && !__any_sync(0xffffffffu, found); i0 += 32) {
+        const int i = i0 + lane;
+        if (i < n) {
+            const float x = seg[i];
+            int lt = 0, eq = 0;
+            for (int t = 0; t < n; t++) {
+                const float y = seg[t];
+                lt += y < x;
+                eq += y == x;
+            }
+            if (lt <= l && l < lt + eq) { ans = x; found = true; }
+        }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, found);
+    return __shfl_sync(0xffffffffu, ans, __ffs(m) - 1);
+}
+
+struct SelectArgs {
+    const float *rows;       // [n_rows][ld]
+    int64_t ld;
+    int n_rows;
+    int n_item;
+    // thresholds
+    const int32_t *sample_rank;  // [S] or nullptr
+    int S;
+    float *thr_out;          // [n_rows][S]
+    // query-rank distribution
+    const int32_t *sample_item;  // [n_si] or nullptr
+    int n_si;
+    int32_t *rank_hist;      // [n_si][n_item + 1], atomically incremented
+    // full sort (descending) into sorted_out [n_rows][n_item] (or nullptr)
+    float *sorted_out;
+    // global scratch when the row does not fit in shared memory ([gridDim.x][2][n_item])
+    float *gscratch;
+};
+
+__device__ __forceinline__ int value_bin(float x, float mn, float scale) {
+    const int b = (int) __fmul_rn(__fsub_rn(x, mn), scale);
+    return min(max(b, 0), kBins - 1);
+}
+
+// One CTA per row: bins, scatter, and the requested order statistics.
+__global__ void __launch_bounds__(kSelThreads) row_select_kernel(SelectArgs a, int use_smem) {
+    extern __shared__ float dyn[];
+    __shared__ int hist[kBins];
+    __shared__ int start[kBins + 1];
+    __shared__ float red_mn[32], red_mx[32];
+    __shared__ int warp_tot[32];
+    const int n = a.n_item;
+    float *vals, *buf;
+    if (use_smem) {
+        vals = dyn;
+        buf = dyn + n;
+    } else {
+        vals = a.gscratch + (int64_t) blockIdx.x * 2 * n;
+        buf = vals + n;
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int row = blockIdx.x; row < a.n_rows; row += gridDim.x) {
+        const float *src = a.rows + (int64_t) row * a.ld;
+        float mn = __int_as_float(0x7f800000), mx = -mn;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const float x = src[i];
+            vals[i] = x;
+            mn = fminf(mn, x);
+            mx = fmaxf(mx, x);
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+            mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        }
+        if (lane == 0) { red_mn[w] = mn; red_mx[w] = mx; }
+        for (int b = threadIdx.x; b < kBins; b += blockDim.x) hist[b] = 0;
+        __syncthreads();
+        if (w == 0) {
+            mn = lane < nw ? red_mn[lane] : __int_as_float(0x7f800000);
+            mx = lane < nw ? red_mx[lane] : -__int_as_float(0x7f800000);
+            for (int o = 16; o > 0; o >>= 1) {
+                mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+                mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+            }
+            if (lane == 0) { red_mn[0] = mn; red_mx[0] = mx; }
+        }
+        __syncthreads();
+        mn = red_mn[0];
+        mx = red_mx[0];
+        const float range = __fsub_rn(mx, mn);
+        const float scale = range > 0.0f ? __fdiv_rn((float) kBins, range) : 0.0f;
+        for (int i = threadIdx.x; i < n; i += blockDim.x) atomicAdd(&hist[value_bin(vals[i], mn, scale)], 1);
+        __syncthreads();
+        // exclusive scan of hist into start (kBins / blockDim per thread)
+        {
+            const int per = kBins / kSelThreads;
+            int loc[kBins / kSelThreads];
+            int s = 0;
+            for (int t = 0; t < per; t++) { loc[t] = s; s += hist[threadIdx.x * per + t]; }
+            int incl = s;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            if (lane == 31) warp_tot[w] = incl;
+            __syncthreads();
+            if (w == 0) {
+                const int v = lane < nw ? warp_tot[lane] : 0;
+                int iv = v;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int x = __shfl_up_sync(0xffffffffu, iv, o);
+                    if (lane >= o) iv += x;
+                }
+                if (lane < nw) warp_tot[lane] = iv - v;
+            }
+            __syncthreads();
+            const int base = warp_tot[w] + incl - s;
+            for (int t = 0; t < per; t++) {
+                start[threadIdx.x * per + t] = base + loc[t];
+                hist[threadIdx.x * per + t] = base + loc[t];  // scatter cursor
+            }
+            if (threadIdx.x == 0) start[kBins] = n;
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const float x = vals[i];
+            buf[atomicAdd(&hist[value_bin(x, mn, scale)], 1)] = x;
+        }
+        __syncthreads();
+        // thresholds: position r (descending) is ascending position n - 1 - r
+        if (a.thr_out) {
+            for (int j = w; j < a.S; j += nw) {
+                const int p = n - 1 - a.sample_rank[j];
+                int lo = 0, len = kBins;  // last bin with start <= p
+                while (len > 0) {
+                    const int h = len >> 1, m = lo + h;
+                    if (start[m + 1] <= p) { lo = m + 1; len -= h + 1; } else len = h;
+                }
+                const int b = lo;
+                const float v = warp_select(buf + start[b], start[b + 1] - start[b], p - start[b]);
+                if (lane == 0) a.thr_out[(int64_t) row * a.S + j] = v;
+            }
+        }
+        // query ranks: number of items scoring strictly above each sampled item's score
+        if (a.rank_hist) {
+            for (int s = threadIdx.x; s < a.n_si; s += blockDim.x) {
+                const float sv = vals[a.sample_item[s]];
+                const int b = value_bin(sv, mn, scale);
+                int cnt = n - start[b + 1];
+                for (int t = start[b]; t < start[b + 1]; t++) cnt += buf[t] > sv;
+                atomicAdd(&a.rank_hist[(int64_t) s * (n + 1) + cnt], 1);
+            }
+        }
+        // full descending sort
+        if (a.sorted_out) {
+            float *dst = a.sorted_out + (int64_t) row * n;
+            for (int b = w; b < kBins; b += nw) {
+                const int s0 = start[b], nb = start[b + 1] - s0;
+                if (nb == 0) continue;
+                if (nb <= 32) {
+                    float v = lane < nb ? buf[s0 + lane] : __int_as_float(0x7f800000);
+                    v = warp_sort32(v);
+                    if (lane < nb) dst[n - 1 - (s0 + lane)] = v;
+                } else {
+                    for (int i = lane; i < nb; i += 32) {
+                        const float x = buf[s0 + i];
+                        int lt = 0, eq_before = 0;
+                        for (int t = 0; t < nb; t++) {
+                            const float y = buf[s0 + t];
+                            lt += y < x;
+                            eq_before += (y == x) & (t < i);
+                        }
+                        dst[n - 1 - (s0 + lt + eq_before)] = x;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void prefix_rows_kernel(int32_t *__restrict__ h, int rows, int64_t len) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    int32_t *p = h + (int64_t) r * len;
+    int32_t s = 0;
+    for (int64_t i = 0; i < len; i++) { s += p[i]; p[i] = s; }
+}
+
+// ---- host side --------------------------------------------------------------------------------------
+
+namespace {
+
+struct RowPipeline {
+    rkr_index *ix;
+    int64_t batch = 0;
+    int64_t ld = 0;
+    int grid = 0;
+    size_t smem = 0;
+    int use_smem = 1;
+};
+
+int setup_pipeline(rkr_index *ix, RowPipeline &P) {
+    P.ix = ix;
+    const int64_t n = ix->n_item;
+    P.ld = (n + 3) / 4 * 4;
+    P.batch = std::max<int64_t>(64, std::min<int64_t>(ix->n_user, (int64_t(3) << 30) / (P.ld * 4)));
+    P.batch = (P.batch + kTile - 1) / kTile * kTile;
+    int dev_smem = 0;
+    RKR_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, ix->device));
+    const size_t static_smem = sizeof(int) * (2 * kBins + 1) + 64 * sizeof(float) * 2 + 32 * sizeof(int);
+    P.smem = (size_t) 2 * n * sizeof(float);
+    P.use_smem = P.smem + static_smem + 1024 <= (size_t) dev_smem;
+    if (!P.use_smem) P.smem = 0;
+    else RKR_CUDA(cudaFuncSetAttribute(row_select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) P.smem));
+    int sms = 0;
+    RKR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ix->device));
+    P.grid = sms * (P.use_smem ? 1 : 2);
+    RKR_TRY(ix->ws_bucket.ensure((size_t) P.batch * P.ld * sizeof(float)));
+    if (!P.use_smem) RKR_TRY(ix->ws_misc.ensure((size_t) P.grid * 2 * n * sizeof(float)));
+    return RKR_OK;
+}
+
+int run_rows(RowPipeline &P, int64_t u0, int64_t nu, SelectArgs sa) {
+    rkr_index *ix = P.ix;
+    cudaStream_t st = ix->stream;
+    float *rows = ix->ws_bucket.as<float>();
+    dim3 g((unsigned) ((ix->n_item + kTile - 1) / kTile), (unsigned) ((nu + kTile - 1) / kTile));
+    score_rows_kernel<<<g, kTileThreads, 0, st>>>(ix->item.as<float>(), ix->n_item, ix->user.as<float>(), u0, nu, ix->dim,
+                                                 rows, P.ld);
+    RKR_CUDA(cudaGetLastError());
+    sa.rows = rows;
+    sa.ld = P.ld;
+    sa.n_rows = (int) nu;
+    sa.n_item = (int) ix->n_item;
+    sa.gscratch = P.use_smem ? nullptr : ix->ws_misc.as<float>();
+    row_select_kernel<<<(unsigned) std::min<int64_t>(P.grid, nu), kSelThreads, P.smem, st>>>(sa, P.use_smem);
+    RKR_CUDA(cudaGetLastError());
+    return RKR_OK;
+}
+
+}  // namespace
+
+int build_sample_search(rkr_index *ix, const int32_t *sample_rank, int n_sample) {
+    RKR_TRY(ensure_device(ix));
+    RowPipeline P;
+    RKR_TRY(setup_pipeline(ix, P));
+    RKR_TRY(ix->sample_rank.ensure(sizeof(int32_t) * n_sample));
+    RKR_TRY(ix->thr.ensure(sizeof(float) * (size_t) ix->n_user * n_sample));
+    RKR_CUDA(cudaMemcpyAsync(ix->sample_rank.p, sample_rank, sizeof(int32_t) * n_sample, cudaMemcpyHostToDevice, ix->stream));
+    ix->n_sample = n_sample;
+    ix->h_sample_rank.assign(sample_rank, sample_rank + n_sample);
+    for (int64_t u0 = 0; u0 < ix->n_user; u0 += P.batch) {
+        const int64_t nu = std::min(P.batch, ix->n_user - u0);
+        SelectArgs sa = {};
+        sa.sample_rank = ix->sample_rank.as<int32_t>();
+        sa.S = n_sample;
+        sa.thr_out = ix->thr.as<float>() + u0 * n_sample;
+        RKR_TRY(run_rows(P, u0, nu, sa));
+    }
+    RKR_CUDA(cudaStreamSynchronize(ix->stream));
+    return RKR_OK;
+}
+
+int score_sort_rows(rkr_index *ix, int64_t start, int64_t n_rows, float *h_rows) {
+    RKR_TRY(ensure_device(ix));
+    RowPipeline P;
+    RKR_TRY(setup_pipeline(ix, P));
+    const int64_t n = ix->n_item;
+    const int64_t per = std::max<int64_t>(1, std::min<int64_t>(P.batch, (int64_t(1) << 30) / (n * 4)));
+    RKR_TRY(ix->ws_out.ensure((size_t) per * n * sizeof(float)));
+    for (int64_t r0 = 0; r0 < n_rows; r0 += per) {
+        const int64_t nr = std::min(per, n_rows - r0);
+        SelectArgs sa = {};
+        sa.sorted_out = ix->ws_out.as<float>();
+        RKR_TRY(run_rows(P, start + r0, nr, sa));
+        RKR_CUDA(cudaMemcpyAsync(h_rows + r0 * n, ix->ws_out.p, (size_t) nr * n * sizeof(float), cudaMemcpyDeviceToHost,
+                                 ix->stream));
+        RKR_CUDA(cudaStreamSynchronize(ix->stream));
+    }
+    return RKR_OK;
+}
+
+int query_rank_distribution(rkr_index *ix, const int32_t *sample_item, int n_sample_item, int32_t *h_accu) {
+    RKR_TRY(ensure_device(ix));
+    RowPipeline P;
+    RKR_TRY(setup_pipeline(ix, P));
+    const int64_t n = ix->n_item;
+    RKR_TRY(ix->ws_hist.ensure(sizeof(int32_t) * (size_t) n_sample_item * (n + 1)));
+    RKR_TRY(ix->ws_res.ensure(sizeof(int32_t) * n_sample_item));
+    RKR_CUDA(cudaMemsetAsync(ix->ws_hist.p, 0, sizeof(int32_t) * (size_t) n_sample_item * (n + 1), ix->stream));
+    RKR_CUDA(cudaMemcpyAsync(ix->ws_res.p, sample_item, sizeof(int32_t) * n_sample_item, cudaMemcpyHostToDevice, ix->stream));
+    for (int64_t u0 = 0; u0 < ix->n_user; u0 += P.batch) {
+        const int64_t nu = std::min(P.batch, ix->n_user - u0);
+        SelectArgs sa = {};
+        sa.sample_item = ix->ws_res.as<int32_t>();
+        sa.n_si = n_sample_item;
+        sa.rank_hist = ix->ws_hist.as<int32_t>();
+        RKR_TRY(run_rows(P, u0, nu, sa));
+    }
+    prefix_rows_kernel<<<(n_sample_item + 63) / 64, 64, 0, ix->stream>>>(ix->ws_hist.as<int32_t>(), n_sample_item, n + 1);
+    RKR_CUDA(cudaGetLastError());
+    RKR_CUDA(cudaMemcpyAsync(h_accu, ix->ws_hist.p, sizeof(int32_t) * (size_t) n_sample_item * (n + 1),
+                             cudaMemcpyDeviceToHost, ix->stream));
+    RKR_CUDA(cudaStreamSynchronize(ix->stream));
+    return RKR_OK;
+}
+
+}  // namespace rkr

@@ -1,0 +1,413 @@
+// rkr_host.cpp -- host-side index-build steps of librkr_b200 (CPU, OpenMP).
+//
+// These steps are small next to the score passes that run on the device: choosing the sampled
+// items and sample ranks, fitting one straight line per user, and the SVD transform.  Float
+// arithmetic here follows the reference's expressions operation by operation (this file is compiled
+// with -ffp-contract=off), so the models it fits are the models the reference would fit.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <numeric>
+#include <random>
+#include <set>
+#include <vector>
+
+#include "rkr.h"
+
+namespace rkr {
+void set_error(const char *fmt, ...);
+}
+
+namespace {
+
+float dot_f32(const float *a, const float *b, int n) {
+    float r = 0.0f;
+    for (int i = 0; i < n; i++) r += a[i] * b[i];
+    return r;
+}
+
+// NormalLinearRegressionLP::CDFPhi (NormalLinearRegressionLP.hpp:123-143): float constants and
+// polynomial, t and the closing expression in double, the double ::exp; sqrt_2_ is the binary32
+// value of ReverseMIPS::sqrt(2.0) (MathUtil.hpp:10-27), i.e. the float nearest sqrt(2).
+float cdf_phi(float x) {
+    const float a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f;
+    const float a4 = -1.453152027f, a5 = 1.061405429f, p = 0.3275911f;
+    const float sqrt_2 = 1.41421354f;
+    int sign = 1;
+    if (x < 0) sign = -1;
+    x = std::fabs(x) / sqrt_2;
+    const float t = (float) (1.0 / (1.0 + (double) (p * x)));
+    const float pt = (((((a5 * t + a4) * t) + a3) * t + a2) * t + a1) * t;
+    const float y = (float) (1.0 - (double) pt * ::exp((double) (-x * x)));
+    return (float) (0.5 * (1.0 + (double) ((float) sign * y)));
+}
+
+// Minimax straight line through (x_i, y_i): minimise e = max |a x_i + b - y_i|, the optimum of
+// the LP in NormalLinearRegressionLP::LinearProgram (:181-213).  Points arrive sorted by x
+// ascending.  The optimal strip's direction is that of a convex-hull edge; each hull-edge slope is
+// tried and the narrowest vertical strip kept.  Double precision.
+void minimax_fit(const std::vector<double> &xs, const std::vector<double> &ys, double &a, double &b, double &e) {
+    const size_t n = xs.size();
+    std::vector<size_t> lo, up;
+    auto cross = [&](size_t o, size_t p, size_t q) {
+        return (xs[p] - xs[o]) * (ys[q] - ys[o]) - (ys[p] - ys[o]) * (xs[q] - xs[o]);
+    };
+    for (size_t i = 0; i < n; i++) {
+        while (lo.size() >= 2 && cross(lo[lo.size() - 2], lo.back(), i) <= 0) lo.pop_back();
+        lo.push_back(i);
+        while (up.size() >= 2 && cross(up[up.size() - 2], up.back(), i) >= 0) up.pop_back();
+        up.push_back(i);
+    }
+    double best = std::numeric_limits<double>::infinity(), ba = 0, bb = 0;
+    auto try_slope = [&](double s) {
+        double mx = -std::numeric_limits<double>::infinity(), mn = std::numeric_limits<double>::infinity();
+        for (size_t i : up) { const double r = ys[i] - s * xs[i]; mx = std::max(mx, r); mn = std::min(mn, r); }
+        for (size_t i : lo) { const double r = ys[i] - s * xs[i]; mx = std::max(mx, r); mn = std::min(mn, r); }
+        const double w = 0.5 * (mx - mn);
+        if (w < best) { best = w; ba = s; bb = 0.5 * (mx + mn); }
+    };
+    for (const auto *h : {&lo, &up})
+        for (size_t k = 0; k + 1 < h->size(); k++) {
+            const double dx = xs[(*h)[k + 1]] - xs[(*h)[k]];
+            if (dx != 0) try_slope((ys[(*h)[k + 1]] - ys[(*h)[k]]) / dx);
+        }
+    if (!(best < std::numeric_limits<double>::infinity())) {
+        double mx = -std::numeric_limits<double>::infinity(), mn = std::numeric_limits<double>::infinity();
+        for (size_t i = 0; i < n; i++) { mx = std::max(mx, ys[i]); mn = std::min(mn, ys[i]); }
+        ba = 0;
+        bb = n ? 0.5 * (mx + mn) : 0;
+        best = n ? 0.5 * (mx - mn) : 0;
+    }
+    a = ba;
+    b = bb;
+    e = best;
+}
+
+// One user's model from its descending thresholds (AssignCache :145-179, the LinearProgram
+// post-processing :194-211, and the endpoint-line fallback with CalcError :215-243, 272-296).
+void fit_user(const float *thr, int S, float *rec) {
+    float mu = 0.0f;
+    for (int s = 0; s < S; s++) mu += thr[s];
+    mu = mu / (float) S;
+    float sigma = 0.0f;
+    for (int s = 0; s < S; s++) {
+        const float m = thr[s] - mu;
+        const float t = m * m;
+        sigma += t;
+    }
+    sigma /= (float) S;
+    sigma = std::sqrt(sigma);
+    std::vector<float> cdf(S);
+    for (int s = 0; s < S; s++) cdf[s] = cdf_phi((thr[s] - mu) / sigma);
+    // points (cdf_j, j + 1) and (cdf_{j+1}, j + 1), j = 0 .. S-2; cdf is non-increasing in j, so
+    // walking j backwards gives ascending x.
+    std::vector<double> xs, ys;
+    xs.reserve(2 * S);
+    ys.reserve(2 * S);
+    for (int j = S - 2; j >= 0; j--) {
+        xs.push_back(cdf[j + 1]); ys.push_back(j + 1);
+        xs.push_back(cdf[j]); ys.push_back(j + 1);
+    }
+    // restore exact ascending order on ties/NaN-free input
+    std::vector<size_t> ord(xs.size());
+    std::iota(ord.begin(), ord.end(), 0);
+    std::stable_sort(ord.begin(), ord.end(), [&](size_t p, size_t q) {
+        return xs[p] < xs[q] || (xs[p] == xs[q] && ys[p] < ys[q]);
+    });
+    std::vector<double> sx(xs.size()), sy(ys.size());
+    for (size_t i = 0; i < ord.size(); i++) { sx[i] = xs[ord[i]]; sy[i] = ys[ord[i]]; }
+    double a = 0, b = 0, e = -1;
+    if (!sx.empty()) minimax_fit(sx, sy, a, b, e);
+    float err = (float) e;
+    const float fa = (float) a, fb = (float) b;
+    if (fa > 0 || fb < 0) err = -1;
+    else if (0 < err && err < (float) S) err += 0.01f;
+    else err = -1;
+    rec[0] = fa; rec[1] = fb; rec[2] = mu; rec[3] = sigma;
+    rec[5] = thr[0]; rec[6] = thr[S - 1];
+    if (err < 0 || (double) err > S - 1e-3) {
+        const float first = cdf[0], last = cdf[S - 1];
+        const float av = (float) (2.0f - (float) S) / (first - last);
+        const float bv = ((float) S * first - last) / (first - last);
+        rec[0] = av; rec[1] = bv;
+        err = -1;
+        for (int j = 0; j < S - 1; j++) {
+            const float p1 = cdf[j] * av + bv, p2 = cdf[j + 1] * av + bv;
+            const float e1 = std::abs((float) (j + 1) - p1), e2 = std::abs((float) (j + 1) - p2);
+            const float te = std::max(e1, e2) + 0.01f;
+            err = std::max(te, err);
+        }
+        err = std::min(err, (float) S);
+        err += 0.01f;
+    }
+    rec[4] = err;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rkr_normalize(float *v, int64_t n, int32_t dim) {
+    if (!v || n < 0 || dim <= 0) { rkr::set_error("rkr_normalize: bad argument"); return RKR_ERR_INVALID; }
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; i++) {
+        float *row = v + i * dim;
+        float l2 = 0.0f;
+        for (int j = 0; j < dim; j++) l2 += row[j] * row[j];
+        l2 = std::sqrt(l2);
+        if (l2 <= 0.001) continue;
+        for (int j = 0; j < dim; j++) row[j] /= l2;
+    }
+    return RKR_OK;
+}
+
+int rkr_sample_item(int32_t n_item, int32_t n_sample_item, int32_t *out) {
+    if (!out || n_item <= 0 || n_sample_item < 0 || n_sample_item > n_item) {
+        rkr::set_error("rkr_sample_item: bad argument");
+        return RKR_ERR_INVALID;
+    }
+    std::vector<int> idx(n_item);
+    std::iota(idx.begin(), idx.end(), 0);
+    std::mt19937 eng(0);
+    std::shuffle(idx.begin(), idx.end(), eng);
+    for (int s = 0; s < n_sample_item; s++) out[s] = idx[s];
+    return RKR_OK;
+}
+
+int rkr_sort_kth_rank(const int32_t *accu, int64_t n_item, int32_t n_sample_item, int32_t sample_topk,
+                      int32_t *sort_kth_out, int32_t *sort_sample_id_out) {
+    if (!accu || !sort_kth_out || !sort_sample_id_out || n_item <= 0 || n_sample_item <= 0 || sample_topk < 0) {
+        rkr::set_error("rkr_sort_kth_rank: bad argument");
+        return RKR_ERR_INVALID;
+    }
+    std::vector<int> kth(n_sample_item);
+    for (int s = 0; s < n_sample_item; s++) {
+        const int32_t *a = accu + (int64_t) s * (n_item + 1);
+        kth[s] = (int) (std::lower_bound(a, a + n_item + 1, sample_topk) - a);
+    }
+    std::vector<int> sid(n_sample_item);
+    std::iota(sid.begin(), sid.end(), 0);
+    std::sort(sid.begin(), sid.end(), [&kth](int i1, int i2) { return kth[i1] < kth[i2]; });
+    for (int s = 0; s < n_sample_item; s++) {
+        sort_sample_id_out[s] = sid[s];
+        sort_kth_out[s] = kth[sid[s]];
+    }
+    return RKR_OK;
+}
+
+int rkr_uniform_sample_rank(int32_t n_item, int32_t n_sample, int32_t *out) {
+    if (!out || n_item <= 1 || n_sample <= 0 || n_sample >= n_item) {
+        rkr::set_error("rkr_uniform_sample_rank: bad argument");
+        return RKR_ERR_INVALID;
+    }
+    const double delta = (n_item - 1) * 1.0 / n_sample;
+    for (int s = 0; s < n_sample; s++) out[s] = (int32_t) std::floor(s * delta);
+    return RKR_OK;
+}
+
+// The OptimalPart dynamic program: candidate ranks {kth, kth - 1}, the cost of a sample set being
+// the number of training-query users left unpruned (OptimalSampleRank.hpp:234-325), minimised over
+// n_sample ranks (OptimalSampleRankFast.hpp:330-395), then the duplicate repair (:397-448).
+int rkr_find_optimal_sample_rank(int64_t n_user, int64_t n_item, int32_t n_sample, int32_t nsq, const int32_t *kth,
+                                 const int32_t *accu, int32_t *out, int64_t *train_cost) {
+    if (!kth || !accu || !out || n_sample <= 0 || nsq <= 0 || n_item <= 0) {
+        rkr::set_error("rkr_find_optimal_sample_rank: bad argument");
+        return RKR_ERR_INVALID;
+    }
+    const int64_t W = n_item + 1;
+    std::set<int> cs;
+    for (int i = 0; i < nsq; i++) {
+        cs.insert(kth[i]);
+        if (kth[i] != 0) cs.insert(kth[i] - 1);
+    }
+    std::vector<int> cand(cs.begin(), cs.end());
+    const int R = (int) cand.size();
+    std::vector<int> this_last(R), next_first(R);
+    for (int r = 0; r < R; r++) {
+        this_last[r] = (int) (std::upper_bound(kth, kth + nsq, cand[r]) - kth);
+        next_first[r] = (int) (std::lower_bound(kth, kth + nsq, cand[r] + 1) - kth);
+    }
+    auto A = [&](int q, int64_t r) -> int64_t { return accu[(int64_t) q * W + r]; };
+    auto cost_end = [&](int r) -> int64_t {
+        const int rank = cand[r] + 1, st = next_first[r];
+        int64_t s = 0;
+        for (int q = st; q < nsq; q++) s += n_user - A(q, rank - 1);
+        return s;
+    };
+    auto cost_begin = [&](int r) -> int64_t {
+        int64_t s = 0;
+        for (int q = 0; q < this_last[r]; q++) s += A(q, cand[r]);
+        return s;
+    };
+    auto cost_between = [&](int ub, int lb) -> int64_t {
+        const int rank_ub = cand[ub] + 1, rank_lb = cand[lb];
+        const int b = next_first[ub], e = this_last[lb];
+        if (b >= nsq || b > e) return 0;
+        int64_t s = 0;
+        for (int q = b; q < e; q++) s += A(q, rank_lb) - A(q, rank_ub - 1);
+        return s;
+    };
+    auto fill = [&](std::set<int> &set, int last_sample) {
+        const int n_remain = n_sample - (int) set.size();
+        const double delta = last_sample * 1.0 / n_remain;
+        double ins = 0;
+        while ((int) set.size() < n_sample && (int) ins < last_sample) {
+            if (!set.count((int) ins)) { set.insert((int) ins); ins += delta; }
+            else ins += 1;
+        }
+        for (int i = 0; (int) set.size() < n_sample && i < n_item; i++) set.insert(i);
+    };
+    if (train_cost) *train_cost = 0;
+    if (R <= n_sample) {
+        std::set<int> set(cand.begin(), cand.end());
+        fill(set, nsq < 500 ? (int) n_item : cand[R - 1]);
+        if ((int) set.size() != n_sample) { rkr::set_error("cannot fill %d sample ranks", n_sample); return RKR_ERR_INVALID; }
+        int i = 0;
+        for (int r : set) out[i++] = r;
+        return RKR_OK;
+    }
+    std::vector<int64_t> end_cost(R);
+    for (int r = 0; r < R; r++) end_cost[r] = cost_end(r);
+    std::vector<int64_t> tr((size_t) R * R);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int lb = 1; lb < R; lb++)
+        for (int ub = 0; ub < lb; ub++) tr[(size_t) lb * R + ub] = -end_cost[ub] + cost_between(ub, lb) + end_cost[lb];
+    std::vector<int64_t> dp((size_t) n_sample * R);
+    std::vector<int32_t> pos((size_t) n_sample * R);
+    for (int r = 0; r < R; r++) { dp[r] = cost_begin(r) + end_cost[r]; pos[r] = r; }
+    for (int s = 1; s < n_sample; s++) {
+#pragma omp parallel for schedule(static)
+        for (int r = 0; r < R; r++) {
+            int64_t best = dp[(size_t) (s - 1) * R + r];
+            int32_t bp = pos[(size_t) (s - 1) * R + r];
+            for (int p = 0; p < r; p++) {
+                const int64_t c = dp[(size_t) (s - 1) * R + p] + tr[(size_t) r * R + p];
+                if (best > c) { best = c; bp = p; }
+            }
+            dp[(size_t) s * R + r] = best;
+            pos[(size_t) s * R + r] = bp;
+        }
+    }
+    uint64_t min_cost = UINT64_MAX;
+    int idx = -1;
+    for (int r = 0; r < R; r++) {
+        const uint64_t c = (uint64_t) dp[(size_t) (n_sample - 1) * R + r];
+        if (c < min_cost) { idx = r; min_cost = c; }
+    }
+    if (train_cost) *train_cost = (int64_t) min_cost;
+    for (int s = n_sample - 1; s >= 0; s--) {
+        out[s] = cand[idx];
+        idx = pos[(size_t) s * R + idx];
+    }
+    std::set<int> set(out, out + n_sample);
+    if ((int) set.size() != n_sample) {
+        fill(set, cand[R - 1]);
+        if ((int) set.size() != n_sample) { rkr::set_error("cannot fill %d sample ranks", n_sample); return RKR_ERR_INVALID; }
+        int i = 0;
+        for (int r : set) out[i++] = r;
+    }
+    return RKR_OK;
+}
+
+int rkr_fit_regression(const float *thr, int64_t n_user, int32_t S, float *rec_out) {
+    if (!thr || !rec_out || n_user < 0 || S < 2) { rkr::set_error("rkr_fit_regression: bad argument"); return RKR_ERR_INVALID; }
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t u = 0; u < n_user; u++) fit_user(thr + u * S, S, rec_out + u * 7);
+    return RKR_OK;
+}
+
+// SVD::PerformSVD (SVD.hpp:62-124) with the thin SVD from the Gram matrix: user^T user = E diag(s^2) E^T,
+// transfer_item[r][c] = s_r * E[c][r], svd_user = user E diag(1/s); check_dim from the cumulative
+// singular values (:214-226).
+int rkr_svd_build(const float *user, int64_t n_user, int32_t dim, float sigma_ratio, float *transfer_item,
+                  float *svd_user, int32_t *check_dim_out) {
+    if (!user || !transfer_item || !svd_user || !check_dim_out || n_user <= 0 || dim <= 0) {
+        rkr::set_error("rkr_svd_build: bad argument");
+        return RKR_ERR_INVALID;
+    }
+    const int d = dim;
+    std::vector<double> G((size_t) d * d, 0.0);
+#pragma omp parallel
+    {
+        std::vector<double> g((size_t) d * d, 0.0);
+#pragma omp for schedule(static)
+        for (int64_t u = 0; u < n_user; u++) {
+            const float *r = user + u * d;
+            for (int i = 0; i < d; i++) {
+                const double ri = r[i];
+                for (int j = i; j < d; j++) g[(size_t) i * d + j] += ri * r[j];
+            }
+        }
+#pragma omp critical
+        for (size_t k = 0; k < g.size(); k++) G[k] += g[k];
+    }
+    for (int i = 0; i < d; i++)
+        for (int j = 0; j < i; j++) G[(size_t) i * d + j] = G[(size_t) j * d + i];
+    std::vector<double> E((size_t) d * d, 0.0);
+    for (int i = 0; i < d; i++) E[(size_t) i * d + i] = 1.0;
+    for (int sweep = 0; sweep < 60; sweep++) {
+        double off = 0, diag = 0;
+        for (int p = 0; p < d; p++) {
+            diag += G[(size_t) p * d + p] * G[(size_t) p * d + p];
+            for (int q = p + 1; q < d; q++) off += G[(size_t) p * d + q] * G[(size_t) p * d + q];
+        }
+        if (off <= 1e-30 * diag) break;
+        for (int p = 0; p < d; p++)
+            for (int q = p + 1; q < d; q++) {
+                const double apq = G[(size_t) p * d + q];
+                if (std::fabs(apq) < 1e-300) continue;
+                const double th = (G[(size_t) q * d + q] - G[(size_t) p * d + p]) / (2 * apq);
+                const double t = (th >= 0 ? 1.0 : -1.0) / (std::fabs(th) + std::sqrt(th * th + 1));
+                const double c = 1 / std::sqrt(t * t + 1), s = t * c;
+                for (int r = 0; r < d; r++) {
+                    const double x = G[(size_t) r * d + p], y = G[(size_t) r * d + q];
+                    G[(size_t) r * d + p] = c * x - s * y;
+                    G[(size_t) r * d + q] = s * x + c * y;
+                }
+                for (int r = 0; r < d; r++) {
+                    const double x = G[(size_t) p * d + r], y = G[(size_t) q * d + r];
+                    G[(size_t) p * d + r] = c * x - s * y;
+                    G[(size_t) q * d + r] = s * x + c * y;
+                }
+                for (int r = 0; r < d; r++) {
+                    const double x = E[(size_t) r * d + p], y = E[(size_t) r * d + q];
+                    E[(size_t) r * d + p] = c * x - s * y;
+                    E[(size_t) r * d + q] = s * x + c * y;
+                }
+            }
+    }
+    std::vector<int> ord(d);
+    std::iota(ord.begin(), ord.end(), 0);
+    std::sort(ord.begin(), ord.end(), [&](int a, int b) { return G[(size_t) a * d + a] > G[(size_t) b * d + b]; });
+    std::vector<float> s(d);
+    std::vector<double> Es((size_t) d * d);
+    for (int k = 0; k < d; k++) {
+        const int e = ord[k];
+        s[k] = (float) std::sqrt(std::max(G[(size_t) e * d + e], 0.0));
+        for (int i = 0; i < d; i++) Es[(size_t) i * d + k] = E[(size_t) i * d + e];
+    }
+    for (int r = 0; r < d; r++)
+        for (int c = 0; c < d; c++) transfer_item[(size_t) r * d + c] = (float) (s[r] * (float) Es[(size_t) c * d + r]);
+#pragma omp parallel for schedule(static)
+    for (int64_t u = 0; u < n_user; u++) {
+        const float *row = user + u * d;
+        for (int k = 0; k < d; k++) {
+            double acc = 0;
+            for (int i = 0; i < d; i++) acc += (double) row[i] * Es[(size_t) i * d + k];
+            svd_user[u * d + k] = s[k] > 0 ? (float) (acc / s[k]) : 0.0f;
+        }
+    }
+    std::vector<float> cum(d);
+    cum[0] = s[0];
+    for (int c = 1; c < d; c++) cum[c] = cum[c - 1] + s[c];
+    int check_dim = 0;
+    for (int c = 0; c < d; c++)
+        if (cum[c] / cum[d - 1] >= sigma_ratio) { check_dim = c; break; }
+    *check_dim_out = check_dim;
+    return RKR_OK;
+}
+
+}  // extern "C"

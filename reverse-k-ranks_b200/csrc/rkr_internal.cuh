@@ -1,0 +1,278 @@
+// rkr_internal.cuh -- shared device code and the index handle of librkr_b200.
+//
+// Arithmetic contract: every dot product that decides a bound, a prune, a rank or a reported score
+// is evaluated exactly as the reference evaluates InnerProduct (src/include/alg/SpaceInnerProduct.hpp:14-20):
+// acc = 0; for j in order: acc = acc + a[j]*b[j], each product and sum rounded to binary32 (no FMA,
+// no reassociation).  __fmul_rn/__fadd_rn are never contracted by nvcc, so the kernels reproduce
+// the reference's float results bit for bit while running as register-tiled SIMT "GEMMs".
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "rkr.h"
+
+namespace rkr {
+
+// ---- errors ---------------------------------------------------------------------------------------
+
+void set_error(const char *fmt, ...);
+
+#define RKR_CUDA(call)                                                                       \
+    do {                                                                                     \
+        cudaError_t e_ = (call);                                                             \
+        if (e_ != cudaSuccess) {                                                             \
+            ::rkr::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+            return RKR_ERR_CUDA;                                                             \
+        }                                                                                    \
+    } while (0)
+
+#define RKR_TRY(expr)                      \
+    do {                                   \
+        int s_ = (expr);                   \
+        if (s_ != RKR_OK) return s_;       \
+    } while (0)
+
+#define RKR_REQUIRE(cond, ...)                  \
+    do {                                        \
+        if (!(cond)) {                          \
+            ::rkr::set_error(__VA_ARGS__);      \
+            return RKR_ERR_INVALID;             \
+        }                                       \
+    } while (0)
+
+// ---- device buffers -------------------------------------------------------------------------------
+
+// Grow-only device buffer owned by an index.
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t want) {
+        if (want <= bytes) return RKR_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        if (want == 0) return RKR_OK;
+        cudaError_t e = cudaMalloc(&p, want);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
+            return RKR_ERR_NOMEM;
+        }
+        bytes = want;
+        return RKR_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <typename T> T *as() const { return static_cast<T *>(p); }
+};
+
+// ---- exact register-tiled dot-product tiles ----------------------------------------------------------
+
+constexpr int kTile = 64;      // rows of A and columns of B per CTA
+constexpr int kKChunk = 32;    // k staged through shared memory per step
+constexpr int kPad = 4;        // shared-memory row padding (keeps float4 alignment)
+constexpr int kTileThreads = 256;
+
+// Shared operand tiles, k-major so four consecutive rows (or columns) load as one float4.
+struct TileSmem {
+    float a[kKChunk][kTile + kPad];
+    float b[kKChunk][kTile + kPad];
+};
+
+// Computes, for the CTA's 64 x 64 block of (row of A, row of B) pairs, the sequential binary32 dot
+// products over k in [0, k_split) into `lo` and over [k_split, k_end) into `hi` (each accumulated
+// from 0, as the reference accumulates its two partial sums).  Rows of A may be gathered through
+// a_idx.  Thread (tx, ty) owns rows a0 + 4*tx + i and columns b0 + 4*ty + j.
+__device__ __forceinline__ void exact_tile(TileSmem &sm, const float *__restrict__ A, const int32_t *__restrict__ a_idx,
+                                          int64_t n_a, int lda, int64_t a0, const float *__restrict__ B, int64_t n_b,
+                                          int ldb, int64_t b0, int k_split, int k_end, float lo[4][4],
+                                          float hi[4][4]) {
+    const int tid = threadIdx.x;
+    const int tx = tid & 15, ty = tid >> 4;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) lo[i][j] = 0.0f, hi[i][j] = 0.0f;
+    for (int k0 = 0; k0 < k_end; k0 += kKChunk) {
+        const int kc = min(kKChunk, k_end - k0);
+        __syncthreads();
+        for (int idx = tid; idx < kTile * kKChunk; idx += kTileThreads) {
+            const int r = idx / kKChunk, kk = idx % kKChunk;
+            float va = 0.0f, vb = 0.0f;
+            if (kk < kc) {
+                const int64_t ra = a0 + r, rb = b0 + r;
+                if (ra < n_a) {
+                    const int64_t row = a_idx ? (int64_t) a_idx[ra] : ra;
+                    va = __ldg(A + row * lda + k0 + kk);
+                }
+                if (rb < n_b) vb = __ldg(B + rb * ldb + k0 + kk);
+            }
+            sm.a[kk][r] = va;
+            sm.b[kk][r] = vb;
+        }
+        __syncthreads();
+        // The chunk may straddle k_split: the first part feeds `lo`, the rest `hi`.
+        const int ks = min(max(k_split - k0, 0), kc);
+        for (int kk = 0; kk < ks; kk++) {
+            const float4 a = *reinterpret_cast<const float4 *>(&sm.a[kk][4 * tx]);
+            const float4 b = *reinterpret_cast<const float4 *>(&sm.b[kk][4 * ty]);
+            const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) lo[i][j] = __fadd_rn(lo[i][j], __fmul_rn(av[i], bv[j]));
+        }
+        for (int kk = ks; kk < kc; kk++) {
+            const float4 a = *reinterpret_cast<const float4 *>(&sm.a[kk][4 * tx]);
+            const float4 b = *reinterpret_cast<const float4 *>(&sm.b[kk][4 * ty]);
+            const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) hi[i][j] = __fadd_rn(hi[i][j], __fmul_rn(av[i], bv[j]));
+        }
+    }
+}
+
+// Sequential binary32 dot product of one pair (thread-serial), same arithmetic as exact_tile.
+__device__ __forceinline__ float exact_dot(const float *__restrict__ a, const float *__restrict__ b, int n) {
+    float acc = 0.0f;
+    for (int j = 0; j < n; j++) acc = __fadd_rn(acc, __fmul_rn(__ldg(a + j), __ldg(b + j)));
+    return acc;
+}
+
+// std::lower_bound(row, row + S, q, [](float arr, float q) { return arr >= q; }) on a descending
+// row: the number of leading thresholds >= q (SampleSearch.hpp:99-102).
+__device__ __forceinline__ int bucket_of(const float *__restrict__ row, int S, float q) {
+    int lo = 0, len = S;
+    while (len > 0) {
+        const int h = len >> 1, m = lo + h;
+        if (__ldg(row + m) >= q) {
+            lo = m + 1;
+            len -= h + 1;
+        } else {
+            len = h;
+        }
+    }
+    return lo;
+}
+
+// Inclusive warp scan of an int.
+__device__ __forceinline__ int warp_incl_scan(int v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int n = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += n;
+    }
+    return v;
+}
+
+// Exclusive block scan (blockDim.x == 256); returns the exclusive prefix, *total gets the sum.
+__device__ __forceinline__ int block_excl_scan(int v, int *warp_tot, int *total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int incl = warp_incl_scan(v);
+    if (lane == 31) warp_tot[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        int t = lane < 8 ? warp_tot[lane] : 0;
+        const int ti = warp_incl_scan(t);
+        if (lane < 8) warp_tot[lane] = ti - t;
+        if (lane == 7) warp_tot[8] = ti;
+    }
+    __syncthreads();
+    const int r = warp_tot[w] + incl - v;
+    *total = warp_tot[8];
+    __syncthreads();
+    return r;
+}
+
+// Rank bounds of bucket b (SampleSearch::CoarseBinarySearch, SampleSearch.hpp:107-125).
+__device__ __host__ __forceinline__ void bucket_bounds(int b, int S, const int32_t *rank, int n_item, int &lb, int &ub) {
+    const unsigned tlb = b == S ? (unsigned) n_item : (unsigned) rank[b];
+    const unsigned tub = b == 0 ? 0u : (unsigned) rank[b - 1];
+    if (b == S) {
+        lb = n_item;
+        ub = (int) tub;
+    } else if (b == 0) {
+        lb = (int) tlb;
+        ub = 0;
+    } else if (tlb - tub <= 1) {
+        lb = (int) tlb;
+        ub = (int) tlb;
+    } else {
+        lb = (int) tlb;
+        ub = (int) tub;
+    }
+}
+
+// Per-query outcome of the pruning steps, written by the select kernels.
+struct QueryCounts {
+    int32_t n_result;        // results after pruning (the reference's n_result_user)
+    int32_t n_prune;         // pruned users (n_prune_user)
+    int32_t n_cand;          // candidates handed to refinement (0 when n_result >= topk)
+    int32_t n_res_emit;      // result users emitted (min(number flagged, topk))
+    int32_t mode;            // 0: normal, 1: k-th bounds equal, 2: refinement skipped
+    int32_t bk;              // bucket of the k-th smallest bound
+    int32_t lstar, ustar;    // k-th smallest lower / upper rank bound
+};
+
+// Pair classes produced by the pruning step (PruneCandidateByBound.hpp:83-150).
+enum : uint8_t { kClsRefine = 0, kClsResult = 1, kClsPrune = 2, kClsIdle = 3 };
+
+}  // namespace rkr
+
+// ---- the index handle --------------------------------------------------------------------------------
+
+struct rkr_index {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int64_t n_user = 0, n_item = 0;
+    int dim = 0;
+    int check_dim = -1;
+    // resident data
+    rkr::DevBuf user;          // [n_user][dim], normalised
+    rkr::DevBuf item;          // [n_item][dim], original order
+    rkr::DevBuf item_sorted;   // [n_item][dim], by norm, descending
+    rkr::DevBuf item_norm;     // [n_item], descending
+    rkr::DevBuf item_rnorm;    // [n_item], norm of dims [check_dim, dim) of item_sorted
+    rkr::DevBuf user_rnorm;    // [n_user], norm of dims [check_dim, dim) of user
+    std::vector<float> h_item_norm_sorted;
+    std::vector<int32_t> h_item_order;
+    // SampleSearch
+    int n_sample = 0;
+    rkr::DevBuf sample_rank;   // [n_sample]
+    rkr::DevBuf thr;           // [n_user][n_sample]
+    std::vector<int32_t> h_sample_rank;
+    // NormalLinearRegressionLP
+    int n_sample_reg = 0;
+    rkr::DevBuf reg_rank;      // [n_sample_reg]
+    rkr::DevBuf reg;           // [n_user][8]: a, b, mu, sigma, err, smax, smin, 0
+    // SVD
+    bool has_svd = false;
+    rkr::DevBuf transfer_item; // [dim][dim]
+    rkr::DevBuf svd_user;      // [n_user][dim]
+    rkr::DevBuf svd_unorm;     // [n_user], norm of dims [check_dim, dim) of svd_user
+    rkr::DevBuf qip_state;     // [n_user], QSRPNormalLP's carried query scores
+    // per-call workspace
+    rkr::DevBuf ws_query, ws_qtr, ws_qnorm, ws_bucket, ws_bucket2, ws_levels, ws_cls, ws_counts, ws_hist;
+    rkr::DevBuf ws_res, ws_cand, ws_cand_off, ws_refine, ws_rank, ws_out, ws_stats, ws_misc;
+    std::vector<uint8_t> h_scratch;
+};
+
+namespace rkr {
+int ensure_device(const rkr_index *ix);
+int refine_prepare_norms(rkr_index *ix);
+int query_batch(rkr_index *ix, int method, const float *d_query, int n_query, int topk, rkr_user_rank *d_out,
+                rkr_query_stats *d_stats, cudaStream_t st);
+int build_sample_search(rkr_index *ix, const int32_t *sample_rank, int n_sample);
+int score_sort_rows(rkr_index *ix, int64_t start, int64_t n_rows, float *h_rows);
+int query_rank_distribution(rkr_index *ix, const int32_t *sample_item, int n_sample_item, int32_t *h_accu);
+}  // namespace rkr

@@ -1,0 +1,593 @@
+// rkr_qsrp.cu -- QSRPNormalLP retrieval on the device (src/impl/QSRPNormalLP.hpp:116-260).
+//
+// Per query the reference runs two bound/prune rounds before refinement:
+//   1. SVD-space partial score on the first check_dim coordinates +- the product of the remaining
+//      norms (PartDimPartNorm::IPBound, PartDimPartNorm.hpp:52-74) -> regression rank bounds
+//      (NormalLinearRegressionLP::ComputeRankBound, NormalLinearRegressionLP.hpp:326-398) -> prune.
+//   2. full SVD-space score for the survivors (ComputeRemainDim, :76-95) -> sampled-threshold
+//      bounds (SampleSearch::RankBound) -> prune again.
+// Here each round is one pass over all (user, query) pairs of the batch.  The reference keeps its
+// per-user score vector across queries; users accepted in round 1 are reported with whatever that
+// vector holds for them.  The batch reproduces it: the score a user had at its latest earlier query
+// in which it reached round 2, or the index's carried state when there is none.
+#include <algorithm>
+#include <vector>
+
+#include "rkr_internal.cuh"
+
+namespace rkr {
+
+// launched from rkr_query.cu
+int refine_and_assemble_qsrp(rkr_index *ix, const float *d_query, int nq, int topk, const QueryCounts *d_counts,
+                             const int32_t *d_res_user, const int32_t *d_res_rank, const float *d_res_qip, int64_t n_cand,
+                             int32_t *d_cand_user, int32_t *d_cand_query, int32_t *d_cand_lb, int32_t *d_cand_ub,
+                             const float *d_cand_qip, const int64_t *d_cand_off, rkr_user_rank *d_out,
+                             rkr_query_stats *d_stats, cudaStream_t st);
+
+// ---- the regression model's arithmetic (NormalLinearRegressionLP.hpp) ------------------------------
+
+// float -> int64 as x86-64 converts it (cvttss2si): NaN and out-of-range values give INT64_MIN.
+__device__ __forceinline__ int64_t f2i64_x86(float v) {
+    if (!(v >= -9.2233720368547758e18f && v < 9.2233720368547758e18f)) return INT64_MIN;
+    return (int64_t) v;
+}
+
+// NormalLinearRegressionLP::CDFPhi (:123-143).  Float constants; t and the closing expression pass
+// through double; exp is the double ::exp (the query and regression apps never bring the float
+// overload into scope).  sqrt_2_ is ReverseMIPS::sqrt(2.0) (MathUtil.hpp:10-27), which equals
+// the binary32 nearest to sqrt(2).
+__device__ __forceinline__ float cdf_phi(float x) {
+    const float a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f;
+    const float a4 = -1.453152027f, a5 = 1.061405429f, p = 0.3275911f;
+    const float sqrt_2 = __int_as_float(0x3fb504f3);
+    const int sign = x < 0 ? -1 : 1;
+    x = __fdiv_rn(fabsf(x), sqrt_2);
+    const float t = __double2float_rn(__ddiv_rn(1.0, __dadd_rn(1.0, (double) __fmul_rn(p, x))));
+    float poly = __fadd_rn(__fmul_rn(a5, t), a4);
+    poly = __fmul_rn(poly, t);
+    poly = __fadd_rn(poly, a3);
+    poly = __fadd_rn(__fmul_rn(poly, t), a2);
+    poly = __fadd_rn(__fmul_rn(poly, t), a1);
+    const float pt = __fmul_rn(poly, t);
+    const double e = exp((double) __fmul_rn(-x, x));
+    const float y = __double2float_rn(__dsub_rn(1.0, __dmul_rn((double) pt, e)));
+    return __double2float_rn(__dmul_rn(0.5, __dadd_rn(1.0, (double) __fmul_rn((float) sign, y))));
+}
+
+struct RegModel {           // device view of the regression index
+    const float *rec;       // [n_user][8]
+    const int32_t *rank;    // [S]
+    int S;
+    double err_cap;         // S - 1e-3
+    int n_item;
+};
+
+// ComputeRankBound (:326-380), returning levels: 0 -> rank 0, j + 1 -> rank[j], S + 1 -> n_item.
+__device__ __forceinline__ void regression_levels(const RegModel &m, int64_t u, float qlb, float qub, int &lvl_lb,
+                                                  int &lvl_ub) {
+    const float4 r0 = __ldg(reinterpret_cast<const float4 *>(m.rec + u * 8));
+    const float4 r1 = __ldg(reinterpret_cast<const float4 *>(m.rec + u * 8 + 4));
+    const float a = r0.x, b = r0.y, mu = r0.z, sigma = r0.w, err = r1.x, smax = r1.y, smin = r1.z;
+    const int S = m.S;
+    if (qlb > smax) lvl_lb = 1;
+    else if (qlb < smin) lvl_lb = S + 1;
+    else if ((double) err >= m.err_cap) lvl_lb = S + 1;
+    else {
+        const float ix = cdf_phi(__fdiv_rn(__fsub_rn(qlb, mu), sigma));
+        const float pred = __fadd_rn(__fmul_rn(ix, a), b);
+        const int64_t pr = f2i64_x86(ceilf(__fadd_rn(pred, err)));
+        lvl_lb = pr >= S ? S + 1 : (pr < 0 ? 1 : (int) pr + 1);
+    }
+    if (qub > smax) lvl_ub = 0;
+    else if (qub < smin) lvl_ub = S;
+    else if ((double) err >= m.err_cap) lvl_ub = 0;
+    else {
+        const float ix = cdf_phi(__fdiv_rn(__fsub_rn(qub, mu), sigma));
+        const float pred = __fadd_rn(__fmul_rn(ix, a), b);
+        const int64_t pr = f2i64_x86(floorf(__fsub_rn(pred, err)));
+        lvl_ub = pr >= S ? S + 1 : (pr < 0 ? 0 : (int) pr + 1);
+    }
+}
+
+__device__ __forceinline__ int level_rank(int lvl, const int32_t *rank, int S, int n_item) {
+    return lvl == 0 ? 0 : (lvl > S ? n_item : rank[lvl - 1]);
+}
+
+// ---- kernels ---------------------------------------------------------------------------------------
+
+struct QsrpParams {
+    int32_t mode1, all1, L1, U1;         // round 1: equal-bounds mode, "all survivors accepted", k-th bounds
+    int32_t n_res1, n_pr1, n_ref1, skip2; // round-1 counts; skip2: round 1 already produced top-k results
+    int32_t mode2, all2, L2, U2;         // round 2
+    int32_t n_elig2, pad0, pad1, pad2;
+};
+
+// SVD::TransferQuery (SVD.hpp:156-164) and the query's remaining-dims norm (PartDimPartNorm.hpp:56-57).
+__global__ void transfer_query_kernel(const float *__restrict__ query, const float *__restrict__ transfer, int dim,
+                                      int check_dim, float *__restrict__ qtr, float *__restrict__ qnorm) {
+    const int q = blockIdx.x;
+    const float *qv = query + (int64_t) q * dim;
+    float *out = qtr + (int64_t) q * dim;
+    for (int t = threadIdx.x; t < dim; t += blockDim.x) out[t] = exact_dot(transfer + (int64_t) t * dim, qv, dim);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float s = 0.0f;
+        for (int j = check_dim; j < dim; j++) s = __fadd_rn(s, __fmul_rn(out[j], out[j]));
+        qnorm[q] = __fsqrt_rn(s);
+    }
+}
+
+// Round 1 for every pair: left = InnerProduct(svd_user, qtr, check_dim); bounds left -+ norms;
+// regression levels of both bounds packed as (lb | ub << 16).
+__global__ void __launch_bounds__(kTileThreads) qsrp_round1_kernel(const float *__restrict__ svd_user, int64_t n_user,
+                                                                  int dim, const float *__restrict__ unorm,
+                                                                  const float *__restrict__ qtr,
+                                                                  const float *__restrict__ qnorm, int n_query,
+                                                                  int check_dim, RegModel m, uint32_t *__restrict__ lv) {
+    __shared__ TileSmem sm;
+    const int64_t b0 = (int64_t) blockIdx.x * kTile;
+    const int64_t a0 = (int64_t) blockIdx.y * kTile;
+    float lo[4][4], hi[4][4];
+    exact_tile(sm, svd_user, nullptr, n_user, dim, a0, qtr, n_query, dim, b0, check_dim, check_dim, lo, hi);
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int64_t u = a0 + 4 * tx + i;
+        if (u >= n_user) continue;
+        const float un = __ldg(unorm + u);
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int64_t q = b0 + 4 * ty + j;
+            if (q >= n_query) continue;
+            const float right = __fmul_rn(un, __ldg(qnorm + q));
+            int l, h;
+            regression_levels(m, u, __fsub_rn(lo[i][j], right), __fadd_rn(lo[i][j], right), l, h);
+            lv[q * n_user + u] = (uint32_t) l | ((uint32_t) h << 16);
+        }
+    }
+}
+
+// Round-1 k-th smallest bounds per query (PruneCandidateByBound.hpp:36-77 with nothing excluded).
+__global__ void qsrp_select1_kernel(const uint32_t *__restrict__ lv, int64_t n_user, const int32_t *__restrict__ rank,
+                                    int S, int n_item, int topk, QsrpParams *__restrict__ par) {
+    extern __shared__ int h[];  // 2 * (S + 2)
+    const int nl = S + 2;
+    const int q = blockIdx.x;
+    for (int b = threadIdx.x; b < 2 * nl; b += blockDim.x) h[b] = 0;
+    __syncthreads();
+    const uint32_t *row = lv + (int64_t) q * n_user;
+    for (int64_t u = threadIdx.x; u < n_user; u += blockDim.x) {
+        const uint32_t v = row[u];
+        const unsigned act = __activemask();
+        const int l = v & 0xffff, hh = v >> 16;
+        unsigned peers = __match_any_sync(act, l);
+        if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&h[l], __popc(peers));
+        peers = __match_any_sync(act, hh);
+        if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&h[nl + hh], __popc(peers));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int kl = nl - 1, kh = nl - 1;
+        int64_t c = 0;
+        for (int b = 0; b < nl; b++) { c += h[b]; if (c >= topk) { kl = b; break; } }
+        c = 0;
+        for (int b = 0; b < nl; b++) { c += h[nl + b]; if (c >= topk) { kh = b; break; } }
+        QsrpParams p = {};
+        p.L1 = level_rank(kl, rank, S, n_item);
+        p.U1 = level_rank(kh, rank, S, n_item);
+        p.mode1 = p.L1 == p.U1;
+        par[q] = p;
+    }
+}
+
+__device__ __forceinline__ int class1_of(const QsrpParams &p, int lb, int ub) {
+    if (p.mode1) return (ub <= p.L1 && lb <= p.L1) ? kClsResult : kClsIdle;
+    if (lb <= p.U1) return kClsResult;
+    if (p.L1 <= ub) return kClsPrune;
+    return p.all1 ? kClsResult : kClsRefine;
+}
+
+// Round-1 class counts (the reference's reduction at PruneCandidateByBound.hpp:115-136).
+__global__ void qsrp_count1_kernel(const uint32_t *__restrict__ lv, int64_t n_user, const int32_t *__restrict__ rank,
+                                   int S, int n_item, QsrpParams *__restrict__ par) {
+    const int q = blockIdx.y;
+    const QsrpParams p = par[q];
+    if (p.mode1) return;
+    __shared__ int cnt[3];
+    if (threadIdx.x < 3) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    int c[3] = {0, 0, 0};
+    const uint32_t *row = lv + (int64_t) q * n_user;
+    for (int64_t u = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; u < n_user; u += (int64_t) gridDim.x * blockDim.x) {
+        const uint32_t v = row[u];
+        const int k = class1_of(p, level_rank(v & 0xffff, rank, S, n_item), level_rank(v >> 16, rank, S, n_item));
+        c[k == kClsResult ? 0 : (k == kClsPrune ? 1 : 2)]++;
+    }
+    for (int i = 0; i < 3; i++) {
+        int v = c[i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(&cnt[i], v);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        atomicAdd(&par[q].n_res1, cnt[0]);
+        atomicAdd(&par[q].n_pr1, cnt[1]);
+        atomicAdd(&par[q].n_ref1, cnt[2]);
+    }
+}
+
+// Round-1 closing rules (PruneCandidateByBound.hpp:93-94, 139-150).
+__global__ void qsrp_final1_kernel(QsrpParams *__restrict__ par, int nq, int topk) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    QsrpParams p = par[q];
+    if (p.mode1) {
+        p.n_res1 = topk;
+        p.n_pr1 = 0;
+        p.n_ref1 = 0;
+    } else if (p.n_res1 + p.n_ref1 == topk) {
+        p.all1 = 1;
+        p.n_res1 = topk;
+        p.n_ref1 = 0;
+    }
+    p.skip2 = p.n_res1 >= topk;
+    par[q] = p;
+}
+
+// Does the pair reach round 2 (neither pruned nor accepted in round 1)?
+__device__ __forceinline__ bool eligible2(const QsrpParams &p, uint32_t v, const int32_t *rank, int S, int n_item) {
+    const int k = class1_of(p, level_rank(v & 0xffff, rank, S, n_item), level_rank(v >> 16, rank, S, n_item));
+    return k == kClsRefine || k == kClsIdle;
+}
+
+// Round 2: full SVD-space score of each surviving pair and its sampled-threshold bucket
+// (0xffff marks pairs that did not reach round 2).
+__global__ void __launch_bounds__(kTileThreads) qsrp_round2_kernel(const float *__restrict__ svd_user, int64_t n_user,
+                                                                  int dim, const float *__restrict__ qtr, int n_query,
+                                                                  int check_dim, const uint32_t *__restrict__ lv,
+                                                                  const QsrpParams *__restrict__ par,
+                                                                  const int32_t *__restrict__ reg_rank, int S_reg,
+                                                                  int n_item, const float *__restrict__ thr, int S,
+                                                                  uint16_t *__restrict__ bucket2) {
+    __shared__ TileSmem sm;
+    const int64_t b0 = (int64_t) blockIdx.x * kTile;
+    const int64_t a0 = (int64_t) blockIdx.y * kTile;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    bool el[4][4];
+    bool any = false;
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int64_t u = a0 + 4 * tx + i, q = b0 + 4 * ty + j;
+            el[i][j] = false;
+            if (u < n_user && q < n_query) el[i][j] = eligible2(par[q], lv[q * n_user + u], reg_rank, S_reg, n_item);
+            any |= el[i][j];
+        }
+    any = __syncthreads_or(any);
+    float lo[4][4], hi[4][4];
+    if (any) exact_tile(sm, svd_user, nullptr, n_user, dim, a0, qtr, n_query, dim, b0, check_dim, dim, lo, hi);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const int64_t u = a0 + 4 * tx + i;
+        if (u >= n_user) continue;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const int64_t q = b0 + 4 * ty + j;
+            if (q >= n_query) continue;
+            uint16_t b = 0xffff;
+            if (el[i][j]) b = (uint16_t) bucket_of(thr + u * S, S, __fadd_rn(lo[i][j], hi[i][j]));
+            bucket2[q * n_user + u] = b;
+        }
+    }
+}
+
+// Round-2 pruning per query (second PruneCandidateByBound call, QSRPNormalLP.hpp:187-190): users
+// excluded in round 1 are skipped by the heap scan and the classification; the equal-bounds rule
+// looks at every user's current bounds.
+__global__ void qsrp_select2_kernel(const uint16_t *__restrict__ bucket2, int64_t n_user, int S,
+                                    const int32_t *__restrict__ rank, int n_item, int topk, QsrpParams *__restrict__ par,
+                                    uint8_t *__restrict__ cls2, QueryCounts *__restrict__ counts) {
+    extern __shared__ int hist[];  // S + 1
+    const int q = blockIdx.x;
+    QsrpParams p = par[q];
+    uint8_t *cq = cls2 + (int64_t) q * (S + 1);
+    if (p.skip2) {
+        if (threadIdx.x == 0) {
+            QueryCounts c = {};
+            c.n_result = p.n_res1;
+            c.n_prune = p.n_pr1;
+            c.n_cand = 0;
+            c.mode = 2;
+            counts[q] = c;
+        }
+        return;
+    }
+    for (int b = threadIdx.x; b <= S; b += blockDim.x) hist[b] = 0;
+    __syncthreads();
+    const uint16_t *row = bucket2 + (int64_t) q * n_user;
+    for (int64_t u = threadIdx.x; u < n_user; u += blockDim.x) {
+        const int v = row[u];
+        const unsigned act = __activemask();
+        const unsigned peers = __match_any_sync(act, v);
+        if (v != 0xffff && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[v], __popc(peers));
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    const int kp = topk - p.n_res1;
+    int64_t n_el = 0;
+    for (int b = 0; b <= S; b++) n_el += hist[b];
+    int L, U;
+    if (n_el < kp) {  // the reference's zero-filled heap: max(bounds of eligible users, 0)
+        int bmax = -1;
+        for (int b = S; b >= 0; b--) if (hist[b]) { bmax = b; break; }
+        L = 0; U = 0;
+        if (bmax >= 0) {
+            int lb, ub;
+            bucket_bounds(bmax, S, rank, n_item, lb, ub);
+            L = max(lb, 0); U = max(ub, 0);
+        }
+    } else {
+        int bk = S;
+        int64_t c = 0;
+        for (int b = 0; b <= S; b++) { c += hist[b]; if (c >= kp) { bk = b; break; } }
+        bucket_bounds(bk, S, rank, n_item, L, U);
+    }
+    p.L2 = L; p.U2 = U; p.n_elig2 = (int) n_el;
+    QueryCounts c = {};
+    c.lstar = L; c.ustar = U;
+    if (L == U) {
+        p.mode2 = 1;
+        c.mode = 1;
+        c.n_result = topk;
+        c.n_prune = p.n_pr1;
+        c.n_cand = 0;
+        for (int b = 0; b <= S; b++) cq[b] = kClsIdle;
+    } else {
+        int64_t nres = p.n_res1, npr = p.n_pr1, nref = 0;
+        for (int b = 0; b <= S; b++) {
+            int lb, ub;
+            bucket_bounds(b, S, rank, n_item, lb, ub);
+            uint8_t k;
+            if (lb <= U) { k = kClsResult; nres += hist[b]; }
+            else if (L <= ub) { k = kClsPrune; npr += hist[b]; }
+            else { k = kClsRefine; nref += hist[b]; }
+            cq[b] = k;
+        }
+        if (nres + nref == topk) {
+            for (int b = 0; b <= S; b++) if (cq[b] == kClsRefine) cq[b] = kClsResult;
+            p.all2 = 1;
+            nres = topk; nref = 0;
+        }
+        c.mode = 0;
+        c.n_result = (int) nres;
+        c.n_prune = (int) npr;
+        c.n_cand = nres >= topk ? 0 : (int) nref;
+    }
+    par[q] = p;
+    counts[q] = c;
+}
+
+// Per query, in user-id order: result users (with their reported rank and whether their score is
+// this query's or a carried one) and the refinement candidates.
+__global__ void qsrp_compact_kernel(const uint32_t *__restrict__ lv, const uint16_t *__restrict__ bucket2, int64_t n_user,
+                                    const int32_t *__restrict__ reg_rank, int S_reg, const int32_t *__restrict__ rank,
+                                    int S, int n_item, const QsrpParams *__restrict__ par, const uint8_t *__restrict__ cls2,
+                                    QueryCounts *__restrict__ counts, const int64_t *__restrict__ cand_off, int topk,
+                                    int32_t *__restrict__ res_user, int32_t *__restrict__ res_rank,
+                                    uint8_t *__restrict__ res_fresh, int32_t *__restrict__ cand_user,
+                                    int32_t *__restrict__ cand_query, int32_t *__restrict__ cand_lb,
+                                    int32_t *__restrict__ cand_ub) {
+    extern __shared__ uint8_t cls_s[];
+    __shared__ int warp_tot[9];
+    const int q = blockIdx.x;
+    const QsrpParams p = par[q];
+    const int n_cand = counts[q].n_cand;
+    for (int b = threadIdx.x; b <= S; b += blockDim.x) cls_s[b] = cls2[(int64_t) q * (S + 1) + b];
+    __syncthreads();
+    const uint32_t *lrow = lv + (int64_t) q * n_user;
+    const uint16_t *brow = bucket2 + (int64_t) q * n_user;
+    int nres = 0, ncand = 0;
+    const int64_t coff = cand_off[q];
+    for (int64_t base = 0; base < n_user; base += blockDim.x) {
+        if (nres >= topk && ncand >= n_cand) break;
+        const int64_t u = base + threadIdx.x;
+        int isres = 0, iscand = 0, rk = 0, fresh = 0, clb = 0, cub = 0;
+        if (u < n_user) {
+            const uint32_t v = lrow[u];
+            const int lb1 = level_rank(v & 0xffff, reg_rank, S_reg, n_item);
+            const int ub1 = level_rank(v >> 16, reg_rank, S_reg, n_item);
+            const int k1 = class1_of(p, lb1, ub1);
+            const uint16_t b2 = brow[u];
+            int lbc = lb1, ubc = ub1;
+            if (b2 != 0xffff) bucket_bounds(b2, S, rank, n_item, lbc, ubc);
+            if (k1 == kClsResult) {
+                isres = 1;
+            } else if (!p.skip2) {
+                if (p.mode2) {
+                    isres = ubc <= p.L2 && lbc <= p.L2;
+                } else if (b2 != 0xffff) {
+                    const uint8_t k2 = cls_s[b2];
+                    isres = k2 == kClsResult;
+                    iscand = k2 == kClsRefine && n_cand > 0;
+                }
+            }
+            rk = lbc;
+            fresh = b2 != 0xffff;
+            clb = lbc;
+            cub = ubc;
+        }
+        int tot;
+        const int pre = block_excl_scan(isres | (iscand << 16), warp_tot, &tot);
+        if (isres) {
+            const int pos = nres + (pre & 0xffff);
+            if (pos < topk) {
+                res_user[(int64_t) q * topk + pos] = (int32_t) u;
+                res_rank[(int64_t) q * topk + pos] = rk;
+                res_fresh[(int64_t) q * topk + pos] = (uint8_t) fresh;
+            }
+        } else if (iscand) {
+            const int64_t pos = coff + ncand + (pre >> 16);
+            cand_user[pos] = (int32_t) u;
+            cand_query[pos] = q;
+            cand_lb[pos] = clb;
+            cand_ub[pos] = cub;
+        }
+        nres += tot & 0xffff;
+        ncand += tot >> 16;
+    }
+    if (threadIdx.x == 0) counts[q].n_res_emit = min(nres, topk);
+}
+
+// Exact SVD-space score of (query, user): checkdim part + remaining part (PartDimPartNorm.hpp:62, 89-92).
+__device__ __forceinline__ float qsrp_score(const float *svd_user, const float *qtr, int64_t u, int q, int dim, int c) {
+    const float *uv = svd_user + u * dim;
+    const float *qv = qtr + (int64_t) q * dim;
+    return __fadd_rn(exact_dot(uv, qv, c), exact_dot(uv + c, qv + c, dim - c));
+}
+
+// Scores of the emitted result users: this query's score when the user reached round 2, else the
+// score from its latest earlier round-2 query in the batch, else the carried state.
+__global__ void qsrp_result_fill_kernel(const QueryCounts *__restrict__ counts, const int32_t *__restrict__ res_user,
+                                        const uint8_t *__restrict__ res_fresh, const uint16_t *__restrict__ bucket2,
+                                        int64_t n_user, const float *__restrict__ svd_user, const float *__restrict__ qtr,
+                                        int dim, int check_dim, const float *__restrict__ state, int topk,
+                                        float *__restrict__ res_qip) {
+    const int q = blockIdx.x;
+    const int n = counts[q].n_res_emit;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        const int64_t i = (int64_t) q * topk + k;
+        const int u = res_user[i];
+        int src = res_fresh[i] ? q : -1;
+        for (int qq = q - 1; src < 0 && qq >= 0; qq--)
+            if (bucket2[(int64_t) qq * n_user + u] != 0xffff) src = qq;
+        res_qip[i] = src >= 0 ? qsrp_score(svd_user, qtr, u, src, dim, check_dim) : state[u];
+    }
+}
+
+__global__ void qsrp_cand_fill_kernel(const int32_t *__restrict__ cand_user, const int32_t *__restrict__ cand_query,
+                                      int64_t n, const float *__restrict__ svd_user, const float *__restrict__ qtr, int dim,
+                                      int check_dim, float *__restrict__ cand_qip) {
+    const int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    cand_qip[e] = qsrp_score(svd_user, qtr, cand_user[e], cand_query[e], dim, check_dim);
+}
+
+// Carried state after the batch: each user's score at its last round-2 query of the batch.
+__global__ void qsrp_state_kernel(const uint16_t *__restrict__ bucket2, int64_t n_user, int nq,
+                                  const float *__restrict__ svd_user, const float *__restrict__ qtr, int dim, int check_dim,
+                                  float *__restrict__ state) {
+    const int64_t u = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= n_user) return;
+    for (int q = nq - 1; q >= 0; q--)
+        if (bucket2[(int64_t) q * n_user + u] != 0xffff) {
+            state[u] = qsrp_score(svd_user, qtr, u, q, dim, check_dim);
+            return;
+        }
+}
+
+// ---- host orchestration ----------------------------------------------------------------------------
+
+namespace {
+template <typename T> T *carve(uint8_t *&p, size_t n) {
+    uintptr_t v = reinterpret_cast<uintptr_t>(p);
+    v = (v + 255) & ~uintptr_t(255);
+    T *r = reinterpret_cast<T *>(v);
+    p = reinterpret_cast<uint8_t *>(v + n * sizeof(T));
+    return r;
+}
+inline size_t carve_size(size_t n, size_t elem) { return ((n * elem + 255) & ~size_t(255)) + 256; }
+}  // namespace
+
+int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_rank *d_out, rkr_query_stats *d_stats,
+               cudaStream_t st) {
+    const int64_t U = ix->n_user;
+    const int dim = ix->dim, c = ix->check_dim, S = ix->n_sample, Sr = ix->n_sample_reg;
+    const int n_item = (int) ix->n_item;
+    RKR_TRY(ix->ws_qtr.ensure(carve_size((size_t) nq * dim, 4) + carve_size(nq, 4) + carve_size(nq, sizeof(QsrpParams))));
+    uint8_t *p0 = ix->ws_qtr.as<uint8_t>();
+    float *qtr = carve<float>(p0, (size_t) nq * dim);
+    float *qnorm = carve<float>(p0, nq);
+    QsrpParams *par = carve<QsrpParams>(p0, nq);
+    RKR_TRY(ix->ws_levels.ensure((size_t) nq * U * 4));
+    RKR_TRY(ix->ws_bucket2.ensure((size_t) nq * U * 2));
+    RKR_TRY(ix->ws_cls.ensure((size_t) nq * (S + 1)));
+    RKR_TRY(ix->ws_counts.ensure(sizeof(QueryCounts) * (size_t) nq));
+    uint32_t *lv = ix->ws_levels.as<uint32_t>();
+    uint16_t *b2 = ix->ws_bucket2.as<uint16_t>();
+    QueryCounts *counts = ix->ws_counts.as<QueryCounts>();
+    RKR_CUDA(cudaMemsetAsync(par, 0, sizeof(QsrpParams) * nq, st));
+
+    transfer_query_kernel<<<nq, 128, 0, st>>>(d_query, ix->transfer_item.as<float>(), dim, c, qtr, qnorm);
+    RKR_CUDA(cudaGetLastError());
+    RegModel m;
+    m.rec = ix->reg.as<float>();
+    m.rank = ix->reg_rank.as<int32_t>();
+    m.S = Sr;
+    m.err_cap = (double) Sr - 1e-3;
+    m.n_item = n_item;
+    dim3 grid((unsigned) ((nq + kTile - 1) / kTile), (unsigned) ((U + kTile - 1) / kTile));
+    qsrp_round1_kernel<<<grid, kTileThreads, 0, st>>>(ix->svd_user.as<float>(), U, dim, ix->svd_unorm.as<float>(), qtr,
+                                                     qnorm, nq, c, m, lv);
+    RKR_CUDA(cudaGetLastError());
+    qsrp_select1_kernel<<<nq, 256, 2 * (Sr + 2) * sizeof(int), st>>>(lv, U, m.rank, Sr, n_item, topk, par);
+    RKR_CUDA(cudaGetLastError());
+    {
+        dim3 g((unsigned) std::min<int64_t>((U + 1023) / 1024, 64), (unsigned) nq);
+        qsrp_count1_kernel<<<g, 256, 0, st>>>(lv, U, m.rank, Sr, n_item, par);
+        RKR_CUDA(cudaGetLastError());
+    }
+    qsrp_final1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, topk);
+    RKR_CUDA(cudaGetLastError());
+    qsrp_round2_kernel<<<grid, kTileThreads, 0, st>>>(ix->svd_user.as<float>(), U, dim, qtr, nq, c, lv, par, m.rank, Sr,
+                                                     n_item, ix->thr.as<float>(), S, b2);
+    RKR_CUDA(cudaGetLastError());
+    qsrp_select2_kernel<<<nq, 256, (S + 1) * sizeof(int), st>>>(b2, U, S, ix->sample_rank.as<int32_t>(), n_item, topk,
+                                                               par, ix->ws_cls.as<uint8_t>(), counts);
+    RKR_CUDA(cudaGetLastError());
+
+    std::vector<QueryCounts> hc(nq);
+    RKR_CUDA(cudaMemcpyAsync(hc.data(), counts, sizeof(QueryCounts) * nq, cudaMemcpyDeviceToHost, st));
+    RKR_CUDA(cudaStreamSynchronize(st));
+    std::vector<int64_t> off(nq + 1, 0);
+    for (int q = 0; q < nq; q++) off[q + 1] = off[q] + hc[q].n_cand;
+    const int64_t n_cand = off[nq];
+    size_t need = carve_size(nq + 1, 8) + carve_size((size_t) nq * topk, 4) * 3 + carve_size((size_t) nq * topk, 1) +
+                  carve_size(n_cand, 4) * 5;
+    RKR_TRY(ix->ws_cand.ensure(need));
+    uint8_t *p = ix->ws_cand.as<uint8_t>();
+    int64_t *d_off = carve<int64_t>(p, nq + 1);
+    int32_t *res_user = carve<int32_t>(p, (size_t) nq * topk);
+    int32_t *res_rank = carve<int32_t>(p, (size_t) nq * topk);
+    float *res_qip = carve<float>(p, (size_t) nq * topk);
+    uint8_t *res_fresh = carve<uint8_t>(p, (size_t) nq * topk);
+    int32_t *cand_user = carve<int32_t>(p, n_cand);
+    int32_t *cand_query = carve<int32_t>(p, n_cand);
+    int32_t *cand_lb = carve<int32_t>(p, n_cand);
+    int32_t *cand_ub = carve<int32_t>(p, n_cand);
+    float *cand_qip = carve<float>(p, n_cand);
+    RKR_CUDA(cudaMemcpyAsync(d_off, off.data(), sizeof(int64_t) * (nq + 1), cudaMemcpyHostToDevice, st));
+    qsrp_compact_kernel<<<nq, 256, S + 1, st>>>(lv, b2, U, m.rank, Sr, ix->sample_rank.as<int32_t>(), S, n_item, par,
+                                                ix->ws_cls.as<uint8_t>(), counts, d_off, topk, res_user, res_rank,
+                                                res_fresh, cand_user, cand_query, cand_lb, cand_ub);
+    RKR_CUDA(cudaGetLastError());
+    qsrp_result_fill_kernel<<<nq, 128, 0, st>>>(counts, res_user, res_fresh, b2, U, ix->svd_user.as<float>(), qtr, dim, c,
+                                                ix->qip_state.as<float>(), topk, res_qip);
+    RKR_CUDA(cudaGetLastError());
+    if (n_cand > 0) {
+        qsrp_cand_fill_kernel<<<(unsigned) ((n_cand + 255) / 256), 256, 0, st>>>(cand_user, cand_query, n_cand,
+                                                                                 ix->svd_user.as<float>(), qtr, dim, c,
+                                                                                 cand_qip);
+        RKR_CUDA(cudaGetLastError());
+    }
+    RKR_TRY(refine_and_assemble_qsrp(ix, d_query, nq, topk, counts, res_user, res_rank, res_qip, n_cand, cand_user,
+                                     cand_query, cand_lb, cand_ub, cand_qip, d_off, d_out, d_stats, st));
+    qsrp_state_kernel<<<(unsigned) ((U + 255) / 256), 256, 0, st>>>(b2, U, nq, ix->svd_user.as<float>(), qtr, dim, c,
+                                                                    ix->qip_state.as<float>());
+    RKR_CUDA(cudaGetLastError());
+    RKR_CUDA(cudaStreamSynchronize(st));
+    return RKR_OK;
+}
+
+}  // namespace rkr

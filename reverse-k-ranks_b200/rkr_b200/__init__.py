@@ -1,0 +1,250 @@
+"""Python binding of librkr_b200.so, the B200 reverse k-ranks engine (C ABI: include/rkr.h).
+
+Mirrors the reference's index / query interface (DBGroup-SUSTech/reverse-k-ranks):
+
+* ``Index`` is the device-resident index behind ``BaseIndex``
+  (src/include/struct/MethodBase.hpp:14-27): it owns the users and items, the SampleSearch
+  thresholds, the NormalLinearRegressionLP models and the SVD transform, and answers
+  ``retrieval(method, query, topk)`` for the reference's ``QS``, ``QSRPNormalLP`` and ``US`` methods.
+* The module-level functions are the reference's host-side index-build steps
+  (normalisation, sampled items, k-th ranks, sample-rank selection, regression fit, SVD).
+
+Errors raise ``RkrError`` with the library's message (the reference exits the process instead).
+There is no CPU fallback: without the compiled library the import fails.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.environ.get("RKR_B200_LIB", os.path.join(os.path.dirname(_HERE), "librkr_b200.so"))
+
+USER_RANK = np.dtype([("user_id", np.int32), ("rank", np.int32), ("query_ip", np.float32)])
+QUERY_STATS = np.dtype([("n_prune", np.int32), ("n_result", np.int32), ("n_refine", np.int32),
+                        ("n_candidate", np.int32), ("n_compute_item", np.int64)])
+
+METHODS = {"QS": 0, "QSRPNormalLP": 1, "US": 2}
+
+RKR_OK, RKR_ERR_INVALID, RKR_ERR_CUDA, RKR_ERR_NOMEM, RKR_ERR_STATE, RKR_ERR_IO = 0, -1, -2, -3, -4, -5
+
+# Every entry point declared in include/rkr.h.
+EXPORTS = [
+    "rkr_last_error", "rkr_version", "rkr_index_create", "rkr_index_destroy", "rkr_index_set_check_dim",
+    "rkr_index_load_sample_search", "rkr_index_load_regression", "rkr_index_load_svd", "rkr_index_reset_state",
+    "rkr_index_size_bytes", "rkr_index_build_sample_search", "rkr_retrieval", "rkr_retrieval_device",
+    "rkr_score_sort_batch", "rkr_index_query_rank_distribution", "rkr_normalize", "rkr_sample_item",
+    "rkr_sort_kth_rank", "rkr_find_optimal_sample_rank", "rkr_uniform_sample_rank", "rkr_fit_regression",
+    "rkr_svd_build",
+]
+
+
+class RkrError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"rkr status {status}: {msg}")
+        self.status = status
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"librkr_b200.so not found at {LIB_PATH}; build it with `make -C reverse-k-ranks_b200` "
+                          "(or __graft_entry__.build())")
+    lib = C.CDLL(LIB_PATH)
+    lib.rkr_last_error.restype = C.c_char_p
+    lib.rkr_version.restype = C.c_int
+    return lib
+
+
+_lib = _load()
+
+
+def lib():
+    return _lib
+
+
+def _check(status):
+    if status != RKR_OK:
+        raise RkrError(status, _lib.rkr_last_error().decode(errors="replace"))
+
+
+def _p(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+# ---- host-side build steps ------------------------------------------------------------------------------
+
+def normalize(v):
+    """VectorMatrix::vectorNormalize (src/include/struct/VectorMatrix.hpp:51-66) on a copy."""
+    v = _f32(v).copy()
+    _check(_lib.rkr_normalize(_p(v), C.c_int64(v.shape[0]), C.c_int32(v.shape[1])))
+    return v
+
+
+def sample_item(n_item, n_sample_item):
+    """SampleItem (src/app/build-index/QueryRankBySample.hpp:20-37)."""
+    out = np.empty(n_sample_item, np.int32)
+    _check(_lib.rkr_sample_item(C.c_int32(n_item), C.c_int32(n_sample_item), _p(out)))
+    return out
+
+
+def sort_kth_rank(accu, sample_topk):
+    """ComputeSortKthRank (QueryRankBySample.hpp:103-134): (sorted k-th ranks, sample order)."""
+    accu = _i32(accu)
+    kth = np.empty(accu.shape[0], np.int32)
+    sid = np.empty(accu.shape[0], np.int32)
+    _check(_lib.rkr_sort_kth_rank(_p(accu), C.c_int64(accu.shape[1] - 1), C.c_int32(accu.shape[0]),
+                                  C.c_int32(sample_topk), _p(kth), _p(sid)))
+    return kth, sid
+
+
+def find_optimal_sample_rank(n_user, n_item, n_sample, sort_kth, accu_sorted):
+    """FindOptimalSampleFast, OptimalPart (OptimalSampleRankFast.hpp:269-472): (ranks, train cost)."""
+    sk, acc = _i32(sort_kth), _i32(accu_sorted)
+    out = np.empty(n_sample, np.int32)
+    cost = np.zeros(1, np.int64)
+    _check(_lib.rkr_find_optimal_sample_rank(C.c_int64(n_user), C.c_int64(n_item), C.c_int32(n_sample),
+                                             C.c_int32(sk.shape[0]), _p(sk), _p(acc), _p(out), _p(cost)))
+    return out, int(cost[0])
+
+
+def uniform_sample_rank(n_item, n_sample):
+    """FindUniformSample (UniformSample.hpp:17-56)."""
+    out = np.empty(n_sample, np.int32)
+    _check(_lib.rkr_uniform_sample_rank(C.c_int32(n_item), C.c_int32(n_sample), _p(out)))
+    return out
+
+
+def fit_regression(thresholds):
+    """NormalLinearRegressionLP fit: [n_user][7] records (a, b, mu, sigma, error, smax, smin)."""
+    thr = _f32(thresholds)
+    out = np.empty((thr.shape[0], 7), np.float32)
+    _check(_lib.rkr_fit_regression(_p(thr), C.c_int64(thr.shape[0]), C.c_int32(thr.shape[1]), _p(out)))
+    return out
+
+
+def svd_build(user, sigma=0.7):
+    """SVD::PerformSVD (src/include/alg/SVD.hpp:62-124): (transfer_item, svd_user, check_dim)."""
+    user = _f32(user)
+    d = user.shape[1]
+    ti = np.empty((d, d), np.float32)
+    su = np.empty_like(user)
+    cd = np.zeros(1, np.int32)
+    _check(_lib.rkr_svd_build(_p(user), C.c_int64(user.shape[0]), C.c_int32(d), C.c_float(sigma), _p(ti), _p(su),
+                              _p(cd)))
+    return ti, su, int(cd[0])
+
+
+# ---- the device index ---------------------------------------------------------------------------------------
+
+class Index:
+    """Device-resident reverse k-ranks index (QS / QSRPNormalLP / US)."""
+
+    def __init__(self, user, item, device: int = 0):
+        user, item = _f32(user), _f32(item)
+        if user.ndim != 2 or item.ndim != 2 or user.shape[1] != item.shape[1]:
+            raise ValueError("user and item must be 2-D with the same dimension")
+        self.n_user, self.dim = user.shape
+        self.n_item = item.shape[0]
+        h = C.c_void_p()
+        _check(_lib.rkr_index_create(C.c_int32(device), _p(user), C.c_int64(self.n_user), _p(item),
+                                     C.c_int64(self.n_item), C.c_int32(self.dim), C.byref(h)))
+        self._h = h
+        self.n_sample = 0
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.rkr_index_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_check_dim(self, check_dim):
+        _check(_lib.rkr_index_set_check_dim(self._h, C.c_int32(check_dim)))
+
+    def load_sample_search(self, sample_rank, thresholds):
+        sr, thr = _i32(sample_rank), _f32(thresholds)
+        _check(_lib.rkr_index_load_sample_search(self._h, _p(sr), C.c_int32(sr.shape[0]), _p(thr)))
+        self.n_sample = sr.shape[0]
+
+    def build_sample_search(self, sample_rank, return_thresholds=True):
+        sr = _i32(sample_rank)
+        out = np.empty((self.n_user, sr.shape[0]), np.float32) if return_thresholds else None
+        _check(_lib.rkr_index_build_sample_search(self._h, _p(sr), C.c_int32(sr.shape[0]), _p(out)))
+        self.n_sample = sr.shape[0]
+        return out
+
+    def load_regression(self, sample_rank, records):
+        sr, rec = _i32(sample_rank), _f32(records)
+        _check(_lib.rkr_index_load_regression(self._h, _p(sr), C.c_int32(sr.shape[0]), _p(rec)))
+
+    def load_svd(self, check_dim, transfer_item, svd_user):
+        ti, su = _f32(transfer_item), _f32(svd_user)
+        _check(_lib.rkr_index_load_svd(self._h, C.c_int32(check_dim), _p(ti), _p(su)))
+
+    def reset_state(self):
+        _check(_lib.rkr_index_reset_state(self._h))
+
+    def size_bytes(self):
+        v = C.c_uint64()
+        _check(_lib.rkr_index_size_bytes(self._h, C.byref(v)))
+        return v.value
+
+    def retrieval(self, method, query, topk, stats=False):
+        """BaseIndex::Retrieval: [n_answered][topk] USER_RANK records (and QUERY_STATS per query)."""
+        m = METHODS[method] if isinstance(method, str) else int(method)
+        q = _f32(query)
+        nq = q.shape[0]
+        n_rows = max(nq, 100)
+        out = np.zeros((n_rows, topk), USER_RANK)
+        st = np.zeros(n_rows, QUERY_STATS) if stats else None
+        na = C.c_int32()
+        _check(_lib.rkr_retrieval(self._h, C.c_int32(m), _p(q), C.c_int32(nq), C.c_int32(topk), _p(out), _p(st),
+                                  C.byref(na)))
+        n = na.value
+        return (out[:n], st[:n]) if stats else out[:n]
+
+    def retrieval_device(self, method, d_query, n_query, topk, d_out, d_stats=None, stream=None):
+        """Same with device pointers (ints): queries [n_query][dim] f32, out [n][topk] USER_RANK."""
+        m = METHODS[method] if isinstance(method, str) else int(method)
+        na = C.c_int32()
+        _check(_lib.rkr_retrieval_device(self._h, C.c_int32(m), C.c_void_p(d_query), C.c_int32(n_query),
+                                         C.c_int32(topk), C.c_void_p(d_out), C.c_void_p(d_stats or 0),
+                                         C.byref(na), C.c_void_p(stream or 0)))
+        return na.value
+
+    def score_sort_batch(self, start_user, n_rows):
+        """ComputeScoreTableBatch::ComputeSortItemsBatch: descending score rows of users [start, start+n)."""
+        out = np.empty((n_rows, self.n_item), np.float32)
+        _check(_lib.rkr_score_sort_batch(self._h, C.c_int64(start_user), C.c_int64(n_rows), _p(out)))
+        return out
+
+    def query_rank_distribution(self, sample_item_ids):
+        """ComputeQueryRankByComputation: accumulated user counts by rank, [n_sample_item][n_item+1]."""
+        si = _i32(sample_item_ids)
+        out = np.empty((si.shape[0], self.n_item + 1), np.int32)
+        _check(_lib.rkr_index_query_rank_distribution(self._h, _p(si), C.c_int32(si.shape[0]), _p(out)))
+        return out

@@ -1,0 +1,417 @@
+#!/usr/bin/env python
+"""Benchmark of the reverse k-ranks query path on B200 (QSRPNormalLP, exact reference ranks).
+
+Workload (default, --config config2): 480,189 users x 17,770 items, d = 150; users N(0, 1/150),
+items N(0, 1/150) scaled per item by lognormal(0, 0.3); the index holds 512 sampled thresholds per
+user (ranks chosen by the OptimalPart program over 150 sampled items, sample_topk = 100), one
+NormalLinearRegressionLP model per user and the SVD transform (sigma 0.7).  A step is one batch of
+1,000 query items drawn uniformly from the items, answered at k = 100.  Synthetic, seeded data
+stands in for the reference's matrix-factorisation datasets (not available here).
+
+value      queries/s with the queries and results resident in device memory (CUDA events on the
+           launching stream, max over ranks);
+e2e        queries/s through the public host API (rkr_retrieval), host->device copy of the queries
+           and device->host copy of the results inside every timed step;
+roofline   the dominant kernel's algorithmic throughput from live per-kernel event timing;
+cpu_baseline  the reference's own QSRPNormalLP::Retrieval (oracle/_ref) on a bounded sample of
+           the same queries, all host threads.
+--impl reference times only that reference path and prints its line.
+
+Multi-GPU (torchrun): every rank holds a replica of the index and answers its own batch of
+queries (weak scaling, no collective on the data path).
+"""
+import argparse
+import contextlib
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "reverse-k-ranks_b200"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "queries/sec and p50/p99 ms at exact ranks (k=100) vs plain FP32 GPU; index-build sec"
+
+CONFIGS = {
+    # name: n_user, n_item, dim, n_sample, n_sample_item, sample_topk, batch, topk
+    "config2": (480189, 17770, 150, 512, 150, 100, 1000, 100),
+    "config1": (1000, 5000, 30, 64, 150, 10, 100, 10),
+}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+@contextlib.contextmanager
+def quiet_stdout():
+    """Silence C-level stdout (the reference prints progress lines) so ours stays one JSON line."""
+    sys.stdout.flush()
+    fd = os.dup(1)
+    dn = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(dn, 1)
+    try:
+        yield
+    finally:
+        sys.stdout.flush()
+        os.dup2(fd, 1)
+        os.close(fd)
+        os.close(dn)
+
+
+def make_data(cfg, seed, rank_id):
+    n_user, n_item, dim = CONFIGS[cfg][:3]
+    rng = np.random.default_rng(seed)
+    user = rng.standard_normal((n_user, dim), dtype=np.float32) * np.float32(1 / np.sqrt(dim))
+    item = rng.standard_normal((n_item, dim), dtype=np.float32) * np.float32(1 / np.sqrt(dim))
+    if cfg == "config2":
+        item *= np.exp(rng.normal(0.0, 0.3, (n_item, 1))).astype(np.float32)
+    qrng = np.random.default_rng(seed + 1000 + rank_id)
+    return user, item, qrng
+
+
+def build_index(R, user_raw, item, cfg, device):
+    n_user, n_item, dim, n_sample, n_si, stopk = CONFIGS[cfg][:6]
+    stages = {}
+    t = time.perf_counter()
+    user = R.normalize(user_raw)
+    stages["normalize"] = time.perf_counter() - t
+    t = time.perf_counter()
+    ix = R.Index(user, item, device=device)
+    stages["upload"] = time.perf_counter() - t
+    t = time.perf_counter()
+    si = R.sample_item(n_item, n_si)
+    accu = ix.query_rank_distribution(si)
+    stages["query_rank_distribution"] = time.perf_counter() - t
+    t = time.perf_counter()
+    kth, sid = R.sort_kth_rank(accu, stopk)
+    rank, _ = R.find_optimal_sample_rank(n_user, n_item, n_sample, kth, accu[sid])
+    stages["sample_rank"] = time.perf_counter() - t
+    t = time.perf_counter()
+    thr = ix.build_sample_search(rank)
+    stages["thresholds"] = time.perf_counter() - t
+    t = time.perf_counter()
+    reg = R.fit_regression(thr)
+    stages["regression_fit"] = time.perf_counter() - t
+    t = time.perf_counter()
+    ti, su, cd = R.svd_build(user, 0.7)
+    ix.load_svd(cd, ti, su)
+    ix.load_regression(rank, reg)
+    stages["svd"] = time.perf_counter() - t
+    parts = dict(user=user, rank=rank, thr=thr, reg=reg, ti=ti, su=su, cd=cd)
+    return ix, parts, stages
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+        def run():
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.samples.append([x.strip() for x in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and
+                          s[3 + i].lower() in ("active", "1")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def kernel_model(name, cfg, nq, stats):
+    """Algorithmic (ops, bytes) per launch of the query kernels, from the workload's sizes."""
+    n_user, n_item, dim = CONFIGS[cfg][:3]
+    c = stats["check_dim"]
+    if name == "qsrp_round1":
+        return 2.0 * n_user * nq * c, 4.0 * n_user * c + 4.0 * n_user * nq + 36.0 * n_user + 4.0 * nq * dim
+    if name == "qsrp_round2":
+        el = stats["eligible2"]
+        return 2.0 * el * dim, 4.0 * n_user * nq + 2.0 * n_user * nq + 4.0 * el * 9
+    if name in ("qsrp_select1", "qsrp_count1"):
+        return 0.0, 4.0 * n_user * nq
+    if name == "qsrp_select2":
+        return 0.0, 2.0 * n_user * nq
+    if name == "qsrp_compact":
+        return 0.0, 6.0 * n_user * nq
+    if name == "refine_tile":
+        return 2.0 * stats["n_compute_item"] * dim, 4.0 * stats["n_compute_item"] * dim
+    return 0.0, 0.0
+
+
+class ReferenceTimer:
+    """The reference's QSRPNormalLP::Retrieval (oracle/_ref) held open on the same index; each run
+    times a bounded sample of queries with all host threads."""
+
+    def __init__(self, parts, item, n_thread):
+        from checkers import ReferenceQsrp
+        self.n_thread = n_thread
+        with quiet_stdout():
+            self.ref = ReferenceQsrp(parts["user"], parts["su"], parts["ti"], item, parts["cd"], parts["rank"],
+                                     parts["thr"], parts["rank"], parts["reg"], n_thread)
+        self.per_q = None
+
+    def run(self, queries, topk, budget_s):
+        with quiet_stdout():
+            if self.per_q is None:
+                _, _, t = self.ref.run(queries[:4], topk)
+                self.per_q = max(t / 4, 1e-6)
+            n = int(min(len(queries), max(8, budget_s / self.per_q)))
+            _, _, secs = self.ref.run(queries[:n], topk)
+        self.per_q = secs / n
+        return n, secs
+
+    def close(self):
+        self.ref.close()
+
+
+def reference_available():
+    from checkers import Reference
+    return Reference.available()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="config2", choices=sorted(CONFIGS))
+    ap.add_argument("--method", default="QSRPNormalLP", choices=["QSRPNormalLP", "QS", "US"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--single-queries", type=int, default=100)
+    args = ap.parse_args()
+
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank_id = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    n_user, n_item, dim, n_sample, n_si, stopk, batch, topk = CONFIGS[args.config]
+    n_thread = os.cpu_count() or 1
+
+    if args.impl == "reference" and rank_id != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    import rkr_b200 as R
+    log(f"[bench] rank {rank_id}/{world}: generating {args.config} data")
+    user_raw, item, qrng = make_data(args.config, args.seed, rank_id)
+    t0 = time.perf_counter()
+    ix, parts, stages = build_index(R, user_raw, item, args.config, local)
+    torch.cuda.synchronize()
+    build_sec = time.perf_counter() - t0
+    log(f"[bench] index built in {build_sec:.2f}s: " + ", ".join(f"{k} {v:.2f}s" for k, v in stages.items()))
+
+    def draw_batch():
+        return item[qrng.choice(n_item, size=batch, replace=False)].copy()
+
+    if args.impl == "reference":
+        if not reference_available():
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (needs the reference "
+                              "sources at build time)"}))
+            return
+        timer = ReferenceTimer(parts, item, n_thread)
+        runs = []
+        for s in range(args.warmup + args.steps):
+            n, secs = timer.run(draw_batch(), topk, args.cpu_seconds / 2)
+            if s >= args.warmup:
+                runs.append((n, secs))
+        timer.close()
+        secs = sum(r[1] for r in runs)
+        nqs = sum(r[0] for r in runs)
+        v = nqs / secs
+        sample = (f"{runs[-1][0]} of each step's {batch} queries through the reference's QSRPNormalLP::Retrieval "
+                  f"(oracle/_ref, the reference's unmodified headers), {n_thread} OpenMP threads")
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "queries/s", "n_gpus": 1,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / len(runs),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded numpy; index built with librkr_b200, bit-identical to the reference's)",
+                "config": {"workload": f"{args.config}: {n_user} users x {n_item} items, d={dim}, {n_sample} "
+                                       f"thresholds + regression, QSRPNormalLP, k={topk}",
+                           "sample_queries_per_step": int(round(nqs / len(runs)))},
+                "cpu_baseline": {"value": v, "unit": "queries/s", "cores": n_thread, "kind": "reference",
+                                 "sample": sample},
+                "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    # ---- device-resident timing -------------------------------------------------------------------
+    stream = torch.cuda.current_stream()
+    rec_bytes = R.USER_RANK.itemsize
+    d_out = torch.empty(batch * topk * rec_bytes, dtype=torch.uint8, device="cuda")
+    d_stats = torch.empty(batch * R.QUERY_STATS.itemsize, dtype=torch.uint8, device="cuda")
+    batches = [torch.from_numpy(draw_batch()).cuda() for _ in range(args.warmup + args.steps)]
+
+    def run_step(dq):
+        return ix.retrieval_device(args.method, dq.data_ptr(), batch, topk, d_out.data_ptr(), d_stats.data_ptr(),
+                                   stream=stream.cuda_stream)
+
+    for s in range(args.warmup):
+        run_step(batches[s])
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    step_ms = []
+    with Clocks(local) as clk:
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t_all0 = torch.cuda.Event(enable_timing=True)
+        t_all1 = torch.cuda.Event(enable_timing=True)
+        t_all0.record(stream)
+        for s in range(args.steps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            run_step(batches[args.warmup + s])
+            e1.record(stream)
+            step_ms.append((e0, e1))
+        t_all1.record(stream)
+        torch.cuda.synchronize()
+    total_ms = t_all0.elapsed_time(t_all1)
+    step_ms = [a.elapsed_time(b) for a, b in step_ms]
+    if dist:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * batch * args.steps / (total_ms / 1e3)
+
+    # ---- per-kernel profile of one more step (outside the timed region) ---------------------------------
+    ix.profile(True)
+    run_step(batches[0])
+    torch.cuda.synchronize()
+    prof = ix.profile_read()
+    ix.profile(False)
+    st = np.frombuffer(d_stats.cpu().numpy().tobytes(), dtype=R.QUERY_STATS)
+    model_stats = {"check_dim": parts["cd"], "n_compute_item": float(st["n_compute_item"].sum()),
+                   "eligible2": float(n_user * batch)}
+    launches_per_step = sum(c for _, c in prof.values())
+    dom = max(prof.items(), key=lambda kv: kv[1][0])
+    dom_name, (dom_ms, dom_n) = dom
+    ops, nbytes = kernel_model(dom_name, args.config, batch, model_stats)
+    avg_s = dom_ms / 1e3 / max(dom_n, 1)
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    sm_clock_ghz = (peaks.get("sm_max_mhz", 1965.0)) / 1e3
+    simt_peak_tops = 148 * 128 * sm_clock_ghz / 1e3  # one FP32 add or mul per lane per clock, T ops/s
+    roofline = {"kernel": dom_name, "bound": "hbm", "achieved": nbytes / avg_s / 1e9, "peak": hbm_peak,
+                "unit": "GB/s", "frac": (nbytes / avg_s / 1e9) / hbm_peak,
+                "peak_source": "MEASURED_PEAKS.json" if peaks else "fallback",
+                "traffic": None, "avg_launch_ms": avg_s * 1e3,
+                "share_of_step": dom_ms / max(sum(v[0] for v in prof.values()), 1e-9),
+                "simt_fp32": {"achieved_tops": ops / avg_s / 1e12, "peak_tops_nominal": simt_peak_tops,
+                              "frac": (ops / avg_s / 1e12) / simt_peak_tops},
+                "kernels_ms_per_step": {k: round(v[0], 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}}
+
+    # ---- latency ------------------------------------------------------------------------------------------
+    single = []
+    q1 = batches[0]
+    for i in range(args.single_queries):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ix.retrieval_device(args.method, q1[i % batch:].data_ptr(), 1, topk, d_out.data_ptr(), 0,
+                            stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        single.append(e0.elapsed_time(e1))
+
+    # ---- end to end through the host API -----------------------------------------------------------------
+    pinned = [torch.from_numpy(draw_batch()).pin_memory() for _ in range(args.steps)]
+    for s in range(min(2, args.warmup)):
+        ix.retrieval(args.method, pinned[s].numpy(), topk)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t = time.perf_counter()
+    for s in range(args.steps):
+        res = ix.retrieval(args.method, pinned[s].numpy(), topk)
+    e2e_s = time.perf_counter() - t
+    if dist:
+        tt = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    e2e = {"value": world * batch * args.steps / e2e_s, "unit": "queries/s",
+           "h2d_bytes_per_step": batch * dim * 4, "d2h_bytes_per_step": batch * topk * rec_bytes}
+
+    cpu = None
+    if rank_id == 0 and world == 1 and reference_available():
+        timer = ReferenceTimer(parts, item, n_thread)
+        n, secs = timer.run(batches[0].cpu().numpy(), topk, args.cpu_seconds)
+        timer.close()
+        cpu = {"value": n / secs, "unit": "queries/s", "cores": n_thread, "kind": "reference",
+               "sample": f"{n} of the step's {batch} queries through the reference's QSRPNormalLP::Retrieval "
+                         f"(oracle/_ref, the reference's unmodified headers) on the same index, {n_thread} threads"}
+
+    if rank_id == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded numpy N(0,1/150) users, lognormal-scaled N(0,1/150) items, queries drawn "
+                    "from the items",
+            "config": {"workload": f"{args.config}: {n_user} users x {n_item} items, d={dim}, {n_sample} sampled "
+                                   f"thresholds/user + NormalLinearRegressionLP + SVD, {args.method}, "
+                                   f"{batch} queries/step, k={topk}",
+                       "batch_per_gpu": batch, "topk": topk, "method": args.method,
+                       "l2": "inputs larger than L2 (resident index ~1.6 GB)",
+                       "parallelism": f"replica x{world} (queries split across GPUs)"},
+            "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
+            "single_query_p50_ms": float(np.percentile(single, 50)),
+            "single_query_p99_ms": float(np.percentile(single, 99)),
+            "build_sec": build_sec, "build_stages_sec": {k: round(v, 3) for k, v in stages.items()},
+            "e2e": e2e, "gpu_launches": int(launches_per_step * args.steps), "roofline": roofline,
+            "cpu_baseline": cpu, "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    ix.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

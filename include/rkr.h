@@ -117,6 +117,17 @@ int rkr_retrieval(rkr_index *index, int32_t method, const float *query, int32_t 
 int rkr_retrieval_device(rkr_index *index, int32_t method, const float *d_query, int32_t n_query, int32_t topk,
                          rkr_user_rank *d_out, rkr_query_stats *d_stats, int32_t *n_answered, void *stream);
 
+/* ---- measurement ---------------------------------------------------------------------------------- */
+
+/* Per-kernel device time: with profiling on, every kernel the index launches is bracketed by CUDA
+ * events on the stream it runs on.  rkr_profile_read returns, per kernel name, the summed time and
+ * the launch count since the previous complete read (a read with max_kernels >= *n_kernels clears
+ * them; a smaller one only reports the count); names is [max_kernels][64] chars.
+ * (The reference's counterpart is its TimeRecord per stage, src/include/util/TimeMemory.hpp:7-24.) */
+int rkr_profile_enable(rkr_index *index, int32_t on);
+int rkr_profile_read(rkr_index *index, int32_t max_kernels, char *names, double *total_ms, int64_t *launches,
+                     int32_t *n_kernels);
+
 /* ---- index build --------------------------------------------------------------------------------- */
 
 /* ComputeScoreTableBatch::ComputeSortItemsBatch (src/include/score_computation/ComputeScoreTableBatch.hpp:79-92):

@@ -37,6 +37,7 @@
 #include "alg/RankBoundRefinement/FindSampleRank/UniformSample.hpp"
 #include "QueryRankByComputation.hpp"
 
+#include <chrono>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -390,5 +391,59 @@ int ref_cdf_phi(const float *x, int64_t n, float *out) {
     NormalLinearRegressionLP lr(1, 1, "QS");
     for (int64_t i = 0; i < n; i++) out[i] = lr.CDFPhi(x[i]);
     return 0;
+}
+}
+
+// ---- persistent reference index for timing (bench.py's CPU legs) --------------------------------
+namespace {
+struct RefQsrp {
+    std::string dir;
+    VectorMatrix user, item;
+    std::unique_ptr<QSRPNormalLP::Index> idx;
+    int64_t n_user = 0;
+    int32_t dim = 0;
+};
+}  // namespace
+
+extern "C" {
+// QSRPNormalLP::BuildIndex from index files written to work_dir in the reference formats; the
+// handle keeps the reference's Index object for repeated Retrieval calls.
+void *ref_qsrp_open(const char *work_dir, const float *user, const float *svd_user, const float *transfer_item,
+                    int64_t n_user, const float *item, int64_t n_item, int32_t d, int32_t check_dim,
+                    const int32_t *sample_rank, int32_t S, const float *thr, const int32_t *reg_rank, const float *reg,
+                    int32_t n_thread) {
+    RefQsrp *h = new RefQsrp();
+    h->dir = work_dir;
+    ensure_index_dirs(h->dir);
+    write_sample_index(h->dir, "h", "QS", sample_rank, S, thr, n_user, n_item, 1, 1, true);
+    write_svd_index(h->dir, "h", n_user, n_item, d, check_dim, transfer_item, svd_user);
+    write_regression_index(h->dir, "h", n_user, n_item, reg_rank, S, reg, 1, 1);
+    fill_vm(h->user, user, n_user, d);
+    fill_vm(h->item, item, n_item, d);
+    h->idx = QSRPNormalLP::BuildIndex(h->item, h->user, "h", S, 1, 1, n_thread, h->dir.c_str());
+    h->n_user = n_user;
+    h->dim = d;
+    return h;
+}
+
+// Index::Retrieval on n_query queries; *seconds = wall time of the Retrieval call alone.
+int ref_qsrp_run(void *handle, const float *query, int32_t n_query, int32_t topk, RefUserRank *out, RefStats *st,
+                 double *seconds) {
+    RefQsrp *h = static_cast<RefQsrp *>(handle);
+    VectorMatrix qv;
+    fill_vm(qv, query, n_query, h->dim);
+    std::vector<SingleQueryPerformance> perf(n_query);
+    const auto t0 = std::chrono::steady_clock::now();
+    auto res = h->idx->Retrieval(qv, topk, n_query, perf);
+    const auto t1 = std::chrono::steady_clock::now();
+    if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+    if (out) copy_results(res, perf, topk, out, st);
+    return 0;
+}
+
+void ref_qsrp_close(void *handle) {
+    RefQsrp *h = static_cast<RefQsrp *>(handle);
+    std::filesystem::remove_all(h->dir);
+    delete h;
 }
 }

@@ -157,6 +157,7 @@ int rkr_index_destroy(rkr_index *ix) {
                       &ix->ws_cand, &ix->ws_cand_off, &ix->ws_refine, &ix->ws_rank, &ix->ws_out, &ix->ws_stats,
                       &ix->ws_misc})
         b->release();
+    ix->prof.release();
     if (ix->stream) cudaStreamDestroy(ix->stream);
     delete ix;
     return RKR_OK;
@@ -337,6 +338,34 @@ int rkr_index_query_rank_distribution(rkr_index *ix, const int32_t *sample_item,
     for (int s = 0; s < n_sample_item; s++)
         RKR_REQUIRE(sample_item[s] >= 0 && sample_item[s] < ix->n_item, "sample item %d out of range", sample_item[s]);
     return query_rank_distribution(ix, sample_item, n_sample_item, accu_out);
+}
+
+int rkr_profile_enable(rkr_index *ix, int32_t on) {
+    RKR_REQUIRE(ix, "null index");
+    RKR_TRY(ensure_device(ix));
+    ix->prof.resolve();
+    ix->prof.on = on != 0;
+    return RKR_OK;
+}
+
+int rkr_profile_read(rkr_index *ix, int32_t max_kernels, char *names, double *total_ms, int64_t *launches,
+                     int32_t *n_kernels) {
+    RKR_REQUIRE(ix && n_kernels, "null argument");
+    RKR_TRY(ensure_device(ix));
+    ix->prof.resolve();
+    const int n = (int) ix->prof.names.size();
+    *n_kernels = n;
+    for (int i = 0; i < n && i < max_kernels; i++) {
+        if (names) {
+            std::strncpy(names + (size_t) i * 64, ix->prof.names[i].c_str(), 63);
+            names[(size_t) i * 64 + 63] = 0;
+        }
+        if (total_ms) total_ms[i] = ix->prof.total_ms[i];
+        if (launches) launches[i] = ix->prof.launches[i];
+    }
+    if (max_kernels >= n)  // a size query (max_kernels < n) leaves the counters in place
+        for (int i = 0; i < n; i++) { ix->prof.total_ms[i] = 0; ix->prof.launches[i] = 0; }
+    return RKR_OK;
 }
 
 }  // extern "C"

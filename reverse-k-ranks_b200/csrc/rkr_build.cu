@@ -291,15 +291,15 @@ int run_rows(RowPipeline &P, int64_t u0, int64_t nu, SelectArgs sa) {
     cudaStream_t st = ix->stream;
     float *rows = ix->ws_bucket.as<float>();
     dim3 g((unsigned) ((ix->n_item + kTile - 1) / kTile), (unsigned) ((nu + kTile - 1) / kTile));
-    score_rows_kernel<<<g, kTileThreads, 0, st>>>(ix->item.as<float>(), ix->n_item, ix->user.as<float>(), u0, nu, ix->dim,
-                                                 rows, P.ld);
+    timed(ix, st, "score_rows", [&] { score_rows_kernel<<<g, kTileThreads, 0, st>>>(ix->item.as<float>(), ix->n_item, ix->user.as<float>(), u0, nu, ix->dim,
+                                                 rows, P.ld); });
     RKR_CUDA(cudaGetLastError());
     sa.rows = rows;
     sa.ld = P.ld;
     sa.n_rows = (int) nu;
     sa.n_item = (int) ix->n_item;
     sa.gscratch = P.use_smem ? nullptr : ix->ws_misc.as<float>();
-    row_select_kernel<<<(unsigned) std::min<int64_t>(P.grid, nu), kSelThreads, P.smem, st>>>(sa, P.use_smem);
+    timed(ix, st, "row_select", [&] { row_select_kernel<<<(unsigned) std::min<int64_t>(P.grid, nu), kSelThreads, P.smem, st>>>(sa, P.use_smem); });
     RKR_CUDA(cudaGetLastError());
     return RKR_OK;
 }
@@ -363,7 +363,7 @@ int query_rank_distribution(rkr_index *ix, const int32_t *sample_item, int n_sam
         sa.rank_hist = ix->ws_hist.as<int32_t>();
         RKR_TRY(run_rows(P, u0, nu, sa));
     }
-    prefix_rows_kernel<<<(n_sample_item + 63) / 64, 64, 0, ix->stream>>>(ix->ws_hist.as<int32_t>(), n_sample_item, n + 1);
+    timed(ix, ix->stream, "prefix_rows", [&] { prefix_rows_kernel<<<(n_sample_item + 63) / 64, 64, 0, ix->stream>>>(ix->ws_hist.as<int32_t>(), n_sample_item, n + 1); });
     RKR_CUDA(cudaGetLastError());
     RKR_CUDA(cudaMemcpyAsync(h_accu, ix->ws_hist.p, sizeof(int32_t) * (size_t) n_sample_item * (n + 1),
                              cudaMemcpyDeviceToHost, ix->stream));

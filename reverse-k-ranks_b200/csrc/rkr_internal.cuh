@@ -229,6 +229,51 @@ enum : uint8_t { kClsRefine = 0, kClsResult = 1, kClsPrune = 2, kClsIdle = 3 };
 
 }  // namespace rkr
 
+// ---- per-kernel timing (opt-in) -------------------------------------------------------------------
+
+namespace rkr {
+// CUDA-event pairs around each kernel launch on its own stream, resolved when read.
+struct Profiler {
+    bool on = false;
+    std::vector<std::string> names;
+    std::vector<double> total_ms;
+    std::vector<int64_t> launches;
+    struct Pending { int id; cudaEvent_t a, b; };
+    std::vector<Pending> pending;
+    std::vector<cudaEvent_t> pool;
+    cudaEvent_t get_event() {
+        if (!pool.empty()) { cudaEvent_t e = pool.back(); pool.pop_back(); return e; }
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        return e;
+    }
+    int id_of(const char *n) {
+        for (size_t i = 0; i < names.size(); i++) if (names[i] == n) return (int) i;
+        names.emplace_back(n);
+        total_ms.push_back(0);
+        launches.push_back(0);
+        return (int) names.size() - 1;
+    }
+    void resolve() {
+        for (auto &p : pending) {
+            float ms = 0;
+            if (cudaEventSynchronize(p.b) == cudaSuccess && cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess) {
+                total_ms[p.id] += ms;
+                launches[p.id] += 1;
+            }
+            pool.push_back(p.a);
+            pool.push_back(p.b);
+        }
+        pending.clear();
+    }
+    void release() {
+        resolve();
+        for (auto e : pool) cudaEventDestroy(e);
+        pool.clear();
+    }
+};
+}  // namespace rkr
+
 // ---- the index handle --------------------------------------------------------------------------------
 
 struct rkr_index {
@@ -265,9 +310,22 @@ struct rkr_index {
     rkr::DevBuf ws_query, ws_qtr, ws_qnorm, ws_bucket, ws_bucket2, ws_levels, ws_cls, ws_counts, ws_hist;
     rkr::DevBuf ws_res, ws_cand, ws_cand_off, ws_refine, ws_rank, ws_out, ws_stats, ws_misc;
     std::vector<uint8_t> h_scratch;
+    rkr::Profiler prof;
 };
 
 namespace rkr {
+// Runs `launch` (one kernel launch on stream st) and, when profiling is on, times it with events.
+template <typename F> inline void timed(rkr_index *ix, cudaStream_t st, const char *name, F &&launch) {
+    if (!ix->prof.on) { launch(); return; }
+    Profiler::Pending p;
+    p.id = ix->prof.id_of(name);
+    p.a = ix->prof.get_event();
+    p.b = ix->prof.get_event();
+    cudaEventRecord(p.a, st);
+    launch();
+    cudaEventRecord(p.b, st);
+    ix->prof.pending.push_back(p);
+}
 int ensure_device(const rkr_index *ix);
 int refine_prepare_norms(rkr_index *ix);
 int query_batch(rkr_index *ix, int method, const float *d_query, int n_query, int topk, rkr_user_rank *d_out,

@@ -519,7 +519,7 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     QueryCounts *counts = ix->ws_counts.as<QueryCounts>();
     RKR_CUDA(cudaMemsetAsync(par, 0, sizeof(QsrpParams) * nq, st));
 
-    transfer_query_kernel<<<nq, 128, 0, st>>>(d_query, ix->transfer_item.as<float>(), dim, c, qtr, qnorm);
+    timed(ix, st, "transfer_query", [&] { transfer_query_kernel<<<nq, 128, 0, st>>>(d_query, ix->transfer_item.as<float>(), dim, c, qtr, qnorm); });
     RKR_CUDA(cudaGetLastError());
     RegModel m;
     m.rec = ix->reg.as<float>();
@@ -528,23 +528,23 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     m.err_cap = (double) Sr - 1e-3;
     m.n_item = n_item;
     dim3 grid((unsigned) ((nq + kTile - 1) / kTile), (unsigned) ((U + kTile - 1) / kTile));
-    qsrp_round1_kernel<<<grid, kTileThreads, 0, st>>>(ix->svd_user.as<float>(), U, dim, ix->svd_unorm.as<float>(), qtr,
-                                                     qnorm, nq, c, m, lv);
+    timed(ix, st, "qsrp_round1", [&] { qsrp_round1_kernel<<<grid, kTileThreads, 0, st>>>(ix->svd_user.as<float>(), U, dim, ix->svd_unorm.as<float>(), qtr,
+                                                     qnorm, nq, c, m, lv); });
     RKR_CUDA(cudaGetLastError());
-    qsrp_select1_kernel<<<nq, 256, 2 * (Sr + 2) * sizeof(int), st>>>(lv, U, m.rank, Sr, n_item, topk, par);
+    timed(ix, st, "qsrp_select1", [&] { qsrp_select1_kernel<<<nq, 256, 2 * (Sr + 2) * sizeof(int), st>>>(lv, U, m.rank, Sr, n_item, topk, par); });
     RKR_CUDA(cudaGetLastError());
     {
         dim3 g((unsigned) std::min<int64_t>((U + 1023) / 1024, 64), (unsigned) nq);
-        qsrp_count1_kernel<<<g, 256, 0, st>>>(lv, U, m.rank, Sr, n_item, par);
+        timed(ix, st, "qsrp_count1", [&] { qsrp_count1_kernel<<<g, 256, 0, st>>>(lv, U, m.rank, Sr, n_item, par); });
         RKR_CUDA(cudaGetLastError());
     }
-    qsrp_final1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, topk);
+    timed(ix, st, "qsrp_final1", [&] { qsrp_final1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, topk); });
     RKR_CUDA(cudaGetLastError());
-    qsrp_round2_kernel<<<grid, kTileThreads, 0, st>>>(ix->svd_user.as<float>(), U, dim, qtr, nq, c, lv, par, m.rank, Sr,
-                                                     n_item, ix->thr.as<float>(), S, b2);
+    timed(ix, st, "qsrp_round2", [&] { qsrp_round2_kernel<<<grid, kTileThreads, 0, st>>>(ix->svd_user.as<float>(), U, dim, qtr, nq, c, lv, par, m.rank, Sr,
+                                                     n_item, ix->thr.as<float>(), S, b2); });
     RKR_CUDA(cudaGetLastError());
-    qsrp_select2_kernel<<<nq, 256, (S + 1) * sizeof(int), st>>>(b2, U, S, ix->sample_rank.as<int32_t>(), n_item, topk,
-                                                               par, ix->ws_cls.as<uint8_t>(), counts);
+    timed(ix, st, "qsrp_select2", [&] { qsrp_select2_kernel<<<nq, 256, (S + 1) * sizeof(int), st>>>(b2, U, S, ix->sample_rank.as<int32_t>(), n_item, topk,
+                                                               par, ix->ws_cls.as<uint8_t>(), counts); });
     RKR_CUDA(cudaGetLastError());
 
     std::vector<QueryCounts> hc(nq);
@@ -568,23 +568,23 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     int32_t *cand_ub = carve<int32_t>(p, n_cand);
     float *cand_qip = carve<float>(p, n_cand);
     RKR_CUDA(cudaMemcpyAsync(d_off, off.data(), sizeof(int64_t) * (nq + 1), cudaMemcpyHostToDevice, st));
-    qsrp_compact_kernel<<<nq, 256, S + 1, st>>>(lv, b2, U, m.rank, Sr, ix->sample_rank.as<int32_t>(), S, n_item, par,
+    timed(ix, st, "qsrp_compact", [&] { qsrp_compact_kernel<<<nq, 256, S + 1, st>>>(lv, b2, U, m.rank, Sr, ix->sample_rank.as<int32_t>(), S, n_item, par,
                                                 ix->ws_cls.as<uint8_t>(), counts, d_off, topk, res_user, res_rank,
-                                                res_fresh, cand_user, cand_query, cand_lb, cand_ub);
+                                                res_fresh, cand_user, cand_query, cand_lb, cand_ub); });
     RKR_CUDA(cudaGetLastError());
-    qsrp_result_fill_kernel<<<nq, 128, 0, st>>>(counts, res_user, res_fresh, b2, U, ix->svd_user.as<float>(), qtr, dim, c,
-                                                ix->qip_state.as<float>(), topk, res_qip);
+    timed(ix, st, "qsrp_result_fill", [&] { qsrp_result_fill_kernel<<<nq, 128, 0, st>>>(counts, res_user, res_fresh, b2, U, ix->svd_user.as<float>(), qtr, dim, c,
+                                                ix->qip_state.as<float>(), topk, res_qip); });
     RKR_CUDA(cudaGetLastError());
     if (n_cand > 0) {
-        qsrp_cand_fill_kernel<<<(unsigned) ((n_cand + 255) / 256), 256, 0, st>>>(cand_user, cand_query, n_cand,
+        timed(ix, st, "qsrp_cand_fill", [&] { qsrp_cand_fill_kernel<<<(unsigned) ((n_cand + 255) / 256), 256, 0, st>>>(cand_user, cand_query, n_cand,
                                                                                  ix->svd_user.as<float>(), qtr, dim, c,
-                                                                                 cand_qip);
+                                                                                 cand_qip); });
         RKR_CUDA(cudaGetLastError());
     }
     RKR_TRY(refine_and_assemble_qsrp(ix, d_query, nq, topk, counts, res_user, res_rank, res_qip, n_cand, cand_user,
                                      cand_query, cand_lb, cand_ub, cand_qip, d_off, d_out, d_stats, st));
-    qsrp_state_kernel<<<(unsigned) ((U + 255) / 256), 256, 0, st>>>(b2, U, nq, ix->svd_user.as<float>(), qtr, dim, c,
-                                                                    ix->qip_state.as<float>());
+    timed(ix, st, "qsrp_state", [&] { qsrp_state_kernel<<<(unsigned) ((U + 255) / 256), 256, 0, st>>>(b2, U, nq, ix->svd_user.as<float>(), qtr, dim, c,
+                                                                    ix->qip_state.as<float>()); });
     RKR_CUDA(cudaGetLastError());
     RKR_CUDA(cudaStreamSynchronize(st));
     return RKR_OK;

@@ -552,13 +552,13 @@ static int refine_and_assemble(rkr_index *ix, int method, const float *d_query, 
         ra.ref_idx = ref_idx;
         ra.ref_user = ref_user;
         ra.n_ref = n_ref;
-        refine_prep_kernel<<<(unsigned) ((n_cand + 255) / 256), 256, 0, st>>>(ra);
+        timed(ix, st, "refine_prep", [&] { refine_prep_kernel<<<(unsigned) ((n_cand + 255) / 256), 256, 0, st>>>(ra); });
         RKR_CUDA(cudaGetLastError());
         const float *items = ipbound ? ix->item_sorted.as<float>() : ix->item.as<float>();
         dim3 grid((unsigned) ((ix->n_item + kTile - 1) / kTile),
                   (unsigned) std::min<int64_t>((n_cand + kTile - 1) / kTile, 65535));
-        refine_tile_kernel<<<grid, kTileThreads, 0, st>>>(ra, items, ix->item_rnorm.as<float>(),
-                                                         ix->user_rnorm.as<float>(), ipbound ? ix->check_dim : ix->dim);
+        timed(ix, st, "refine_tile", [&] { refine_tile_kernel<<<grid, kTileThreads, 0, st>>>(ra, items, ix->item_rnorm.as<float>(),
+                                                         ix->user_rnorm.as<float>(), ipbound ? ix->check_dim : ix->dim); });
         RKR_CUDA(cudaGetLastError());
     }
     AssembleArgs aa;
@@ -577,7 +577,7 @@ static int refine_and_assemble(rkr_index *ix, int method, const float *d_query, 
     aa.out = d_out;
     aa.stats = d_stats;
     aa.scratch = nullptr;
-    assemble_kernel<<<nq, 256, 0, st>>>(aa);
+    timed(ix, st, "assemble", [&] { assemble_kernel<<<nq, 256, 0, st>>>(aa); });
     RKR_CUDA(cudaGetLastError());
     (void) h_counts;
     return RKR_OK;
@@ -596,12 +596,12 @@ static int qs_chunk(rkr_index *ix, int method, const float *d_query, int nq, int
     QueryCounts *counts = ix->ws_counts.as<QueryCounts>();
     {
         dim3 grid((unsigned) ((nq + kTile - 1) / kTile), (unsigned) ((U + kTile - 1) / kTile));
-        score_bucket_kernel<<<grid, kTileThreads, 0, st>>>(ix->user.as<float>(), U, dim, d_query, nq,
-                                                          ix->thr.as<float>(), S, bucket);
+        timed(ix, st, "score_bucket", [&] { score_bucket_kernel<<<grid, kTileThreads, 0, st>>>(ix->user.as<float>(), U, dim, d_query, nq,
+                                                          ix->thr.as<float>(), S, bucket); });
         RKR_CUDA(cudaGetLastError());
-        select_bucket_kernel<<<nq, 256, (S + 1) * sizeof(int), st>>>(bucket, U, S, ix->sample_rank.as<int32_t>(),
+        timed(ix, st, "select_bucket", [&] { select_bucket_kernel<<<nq, 256, (S + 1) * sizeof(int), st>>>(bucket, U, S, ix->sample_rank.as<int32_t>(),
                                                                      (int) ix->n_item, topk, ix->ws_cls.as<uint8_t>(),
-                                                                     counts);
+                                                                     counts); });
         RKR_CUDA(cudaGetLastError());
     }
     std::vector<QueryCounts> hc(nq);
@@ -624,15 +624,15 @@ static int qs_chunk(rkr_index *ix, int method, const float *d_query, int nq, int
     int32_t *cand_ub = carve<int32_t>(p, n_cand);
     uint16_t *cand_bucket = carve<uint16_t>(p, n_cand);
     RKR_CUDA(cudaMemcpyAsync(d_off, off.data(), sizeof(int64_t) * (nq + 1), cudaMemcpyHostToDevice, st));
-    compact_kernel<<<nq, 256, S + 1, st>>>(bucket, U, S, ix->ws_cls.as<uint8_t>(), counts, d_off, topk, res_user,
-                                           cand_user, cand_query, cand_bucket);
+    timed(ix, st, "compact", [&] { compact_kernel<<<nq, 256, S + 1, st>>>(bucket, U, S, ix->ws_cls.as<uint8_t>(), counts, d_off, topk, res_user,
+                                           cand_user, cand_query, cand_bucket); });
     RKR_CUDA(cudaGetLastError());
-    result_fill_kernel<<<nq, 128, 0, st>>>(counts, res_user, bucket, U, ix->user.as<float>(), d_query, dim, S,
-                                            ix->sample_rank.as<int32_t>(), (int) ix->n_item, topk, res_rank, res_qip);
+    timed(ix, st, "result_fill", [&] { result_fill_kernel<<<nq, 128, 0, st>>>(counts, res_user, bucket, U, ix->user.as<float>(), d_query, dim, S,
+                                            ix->sample_rank.as<int32_t>(), (int) ix->n_item, topk, res_rank, res_qip); });
     RKR_CUDA(cudaGetLastError());
     if (n_cand > 0) {
-        cand_bounds_kernel<<<(unsigned) ((n_cand + 255) / 256), 256, 0, st>>>(
-            cand_bucket, n_cand, S, ix->sample_rank.as<int32_t>(), (int) ix->n_item, cand_lb, cand_ub);
+        timed(ix, st, "cand_bounds", [&] { cand_bounds_kernel<<<(unsigned) ((n_cand + 255) / 256), 256, 0, st>>>(
+            cand_bucket, n_cand, S, ix->sample_rank.as<int32_t>(), (int) ix->n_item, cand_lb, cand_ub); });
         RKR_CUDA(cudaGetLastError());
     }
     RKR_TRY(refine_and_assemble(ix, method, d_query, nq, topk, counts, hc, res_user, res_rank, res_qip, n_cand,

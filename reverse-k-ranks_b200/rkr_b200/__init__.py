@@ -37,7 +37,7 @@ EXPORTS = [
     "rkr_index_size_bytes", "rkr_index_build_sample_search", "rkr_retrieval", "rkr_retrieval_device",
     "rkr_score_sort_batch", "rkr_index_query_rank_distribution", "rkr_normalize", "rkr_sample_item",
     "rkr_sort_kth_rank", "rkr_find_optimal_sample_rank", "rkr_uniform_sample_rank", "rkr_fit_regression",
-    "rkr_svd_build",
+    "rkr_svd_build", "rkr_profile_enable", "rkr_profile_read",
 ]
 
 
@@ -235,6 +235,21 @@ class Index:
                                          C.c_int32(topk), C.c_void_p(d_out), C.c_void_p(d_stats or 0),
                                          C.byref(na), C.c_void_p(stream or 0)))
         return na.value
+
+    def profile(self, on=True):
+        """Turn per-kernel event timing on or off (rkr_profile_enable)."""
+        _check(_lib.rkr_profile_enable(self._h, C.c_int32(1 if on else 0)))
+
+    def profile_read(self):
+        """{kernel name: (total ms, launches)} since the previous read."""
+        n = C.c_int32()
+        _check(_lib.rkr_profile_read(self._h, C.c_int32(0), None, None, None, C.byref(n)))
+        k = n.value
+        names = C.create_string_buffer(64 * max(k, 1))
+        ms = np.zeros(max(k, 1), np.float64)
+        cnt = np.zeros(max(k, 1), np.int64)
+        _check(_lib.rkr_profile_read(self._h, C.c_int32(k), names, _p(ms), _p(cnt), C.byref(n)))
+        return {names.raw[64 * i:64 * i + 64].split(b"\0")[0].decode(): (float(ms[i]), int(cnt[i])) for i in range(k)}
 
     def score_sort_batch(self, start_user, n_rows):
         """ComputeScoreTableBatch::ComputeSortItemsBatch: descending score rows of users [start, start+n)."""

@@ -322,3 +322,34 @@ class Reference:
                                         _p(reg), _p(query), C.c_int32(nq), C.c_int32(topk),
                                         C.c_int32(self.n_thread), _p(out), _p(st))
         return out, st
+
+
+class ReferenceQsrp:
+    """The reference's QSRPNormalLP index held open for repeated Retrieval timing (oracle/_ref)."""
+
+    def __init__(self, user, svd_user, transfer_item, item, check_dim, sample_rank, thr, reg_rank, reg, n_thread):
+        self.lib = C.CDLL(REF_SO)
+        self.lib.ref_qsrp_open.restype = C.c_void_p
+        self.lib.ref_set_threads(C.c_int(n_thread))
+        self._keep = [_f32(user), _f32(svd_user), _f32(transfer_item), _f32(item), _i32(sample_rank), _f32(thr),
+                      _i32(reg_rank), _f32(reg)]
+        u, su, ti, it, sr, th, rr, rg = self._keep
+        self.dir = tempfile.mkdtemp(prefix="rkr_ref_qsrp_")
+        self.h = self.lib.ref_qsrp_open(self.dir.encode(), _p(u), _p(su), _p(ti), C.c_int64(u.shape[0]), _p(it),
+                                        C.c_int64(it.shape[0]), C.c_int32(u.shape[1]), C.c_int32(check_dim), _p(sr),
+                                        C.c_int32(sr.shape[0]), _p(th), _p(rr), _p(rg), C.c_int32(n_thread))
+        self._keep = None
+
+    def run(self, query, topk):
+        q = _f32(query)
+        out = np.zeros((q.shape[0], topk), USER_RANK)
+        st = np.zeros(q.shape[0], STATS)
+        secs = C.c_double()
+        self.lib.ref_qsrp_run(C.c_void_p(self.h), _p(q), C.c_int32(q.shape[0]), C.c_int32(topk), _p(out), _p(st),
+                              C.byref(secs))
+        return out, st, secs.value
+
+    def close(self):
+        if self.h:
+            self.lib.ref_qsrp_close(C.c_void_p(self.h))
+            self.h = None

@@ -128,7 +128,7 @@ class Clocks:
                                           "--format=csv,noheader,nounits"], capture_output=True, text=True,
                                          timeout=5).stdout.strip()
                     if out:
-                        self.samples.append([x.strip() for x in out.split(",")])
+                        self.samples.append((time.perf_counter(), [x.strip() for x in out.split(",")]))
                 except Exception:
                     pass
                 self._stop.wait(0.2)
@@ -141,7 +141,16 @@ class Clocks:
         self._stop.set()
         self._t.join(timeout=10)
 
+    def mark(self, t0, t1):
+        """Restrict the summary to samples taken between t0 and t1 (perf_counter seconds)."""
+        self.window = (t0, t1)
+
     def summary(self):
+        w = getattr(self, "window", None)
+        samples = [s for t, s in self.samples if w is None or w[0] - 0.25 <= t <= w[1] + 0.25]
+        if not samples:
+            samples = [s for _, s in self.samples[-3:]]
+        self.samples = samples
         if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
@@ -215,6 +224,7 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--single-queries", type=int, default=100)
+    ap.add_argument("--batch", type=int, default=0, help="queries per step (default: the workload's)")
     args = ap.parse_args()
 
     import torch
@@ -229,6 +239,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     torch.cuda.set_device(local)
     n_user, n_item, dim, n_sample, n_si, stopk, batch, topk = CONFIGS[args.config]
+    if args.batch:
+        batch = args.batch
     n_thread = os.cpu_count() or 1
 
     if args.impl == "reference" and rank_id != 0:
@@ -289,16 +301,15 @@ def main():
         return ix.retrieval_device(args.method, dq.data_ptr(), batch, topk, d_out.data_ptr(), d_stats.data_ptr(),
                                    stream=stream.cuda_stream)
 
-    for s in range(args.warmup):
-        run_step(batches[s])
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    step_ms = []
     with Clocks(local) as clk:
+        time.sleep(0.5)  # the sampler's first nvidia-smi call lands before the timed region
+        for s in range(args.warmup):
+            run_step(batches[s])
         torch.cuda.synchronize()
         if dist:
             dist.barrier()
+        step_ms = []
+        wall0 = time.perf_counter()
         t_all0 = torch.cuda.Event(enable_timing=True)
         t_all1 = torch.cuda.Event(enable_timing=True)
         t_all0.record(stream)
@@ -311,8 +322,10 @@ def main():
             step_ms.append((e0, e1))
         t_all1.record(stream)
         torch.cuda.synchronize()
+        clk.mark(wall0, time.perf_counter())
     total_ms = t_all0.elapsed_time(t_all1)
     step_ms = [a.elapsed_time(b) for a, b in step_ms]
+    log("[bench] step ms: " + " ".join(f"{v:.2f}" for v in step_ms))
     if dist:
         t = torch.tensor([total_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

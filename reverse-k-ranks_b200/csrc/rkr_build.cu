@@ -26,7 +26,7 @@ __global__ void __launch_bounds__(kTileThreads) score_rows_kernel(const float *_
     const int64_t a0 = (int64_t) blockIdx.x * kTile;  // items
     const int64_t b0 = (int64_t) blockIdx.y * kTile;  // users (relative to u0)
     float lo[4][4], hi[4][4];
-    exact_tile(sm, item, nullptr, n_item, dim, a0, user + u0 * dim, nu, dim, b0, dim, dim, lo, hi);
+    exact_tile(sm, item, nullptr, n_item, dim, a0, user + u0 * dim, nu, dim, b0, 0, dim, dim, lo, hi);
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
 #pragma unroll
     for (int j = 0; j < 4; j++) {

@@ -87,12 +87,12 @@ struct TileSmem {
 };
 
 // Computes, for the CTA's 64 x 64 block of (row of A, row of B) pairs, the sequential binary32 dot
-// products over k in [0, k_split) into `lo` and over [k_split, k_end) into `hi` (each accumulated
-// from 0, as the reference accumulates its two partial sums).  Rows of A may be gathered through
+// products over k in [k_begin, k_split) into `lo` and over [k_split, k_end) into `hi` (each
+// accumulated from 0, as the reference accumulates its partial sums).  Rows of A may be gathered through
 // a_idx.  Thread (tx, ty) owns rows a0 + 4*tx + i and columns b0 + 4*ty + j.
 __device__ __forceinline__ void exact_tile(TileSmem &sm, const float *__restrict__ A, const int32_t *__restrict__ a_idx,
                                           int64_t n_a, int lda, int64_t a0, const float *__restrict__ B, int64_t n_b,
-                                          int ldb, int64_t b0, int k_split, int k_end, float lo[4][4],
+                                          int ldb, int64_t b0, int k_begin, int k_split, int k_end, float lo[4][4],
                                           float hi[4][4]) {
     const int tid = threadIdx.x;
     const int tx = tid & 15, ty = tid >> 4;
@@ -100,7 +100,7 @@ __device__ __forceinline__ void exact_tile(TileSmem &sm, const float *__restrict
     for (int i = 0; i < 4; i++)
 #pragma unroll
         for (int j = 0; j < 4; j++) lo[i][j] = 0.0f, hi[i][j] = 0.0f;
-    for (int k0 = 0; k0 < k_end; k0 += kKChunk) {
+    for (int k0 = k_begin; k0 < k_end; k0 += kKChunk) {
         const int kc = min(kKChunk, k_end - k0);
         __syncthreads();
         for (int idx = tid; idx < kTile * kKChunk; idx += kTileThreads) {
@@ -194,6 +194,53 @@ __device__ __forceinline__ int block_excl_scan(int v, int *warp_tot, int *total)
     return r;
 }
 
+// Two-level form of bucket_of for a block of users: the CTA keeps every g-th threshold of each of
+// its users in shared memory (the last element of each group of g), finds the first group whose
+// last (smallest) threshold is below q there, and counts the thresholds >= q inside that group
+// with independent loads.  On a descending row this is the same count std::lower_bound returns.
+struct ThrSummary {
+    static constexpr int kMaxGroups = 64;
+    float v[kTile][kMaxGroups];
+};
+
+__host__ __device__ __forceinline__ int thr_group(int S) {
+    const int g = (S + ThrSummary::kMaxGroups - 1) / ThrSummary::kMaxGroups;
+    return g < 16 ? 16 : g;
+}
+
+__device__ __forceinline__ void load_thr_summary(ThrSummary &ts, const float *__restrict__ thr, int64_t n_user,
+                                                 int64_t a0, int S) {
+    const int g = thr_group(S), nb = (S + g - 1) / g;
+    for (int idx = threadIdx.x; idx < kTile * nb; idx += blockDim.x) {
+        const int r = idx / nb, j = idx % nb;
+        const int64_t u = a0 + r;
+        ts.v[r][j] = u < n_user ? __ldg(thr + u * S + min(g * j + g - 1, S - 1)) : 0.0f;
+    }
+}
+
+__device__ __forceinline__ int bucket_of_2level(const float *__restrict__ summ, const float *__restrict__ row, int S,
+                                                float q) {
+    const int g = thr_group(S), nb = (S + g - 1) / g;
+    int lo = 0, len = nb;
+    while (len > 0) {
+        const int h = len >> 1, m = lo + h;
+        if (summ[m] >= q) { lo = m + 1; len -= h + 1; } else len = h;
+    }
+    if (lo == nb) return S;
+    const int base = g * lo, end = min(base + g, S);
+    int c = 0;
+    if (g == 16 && end - base == 16 && (S & 3) == 0) {
+        const float4 *p = reinterpret_cast<const float4 *>(row + base);
+        const float4 x0 = __ldg(p), x1 = __ldg(p + 1), x2 = __ldg(p + 2), x3 = __ldg(p + 3);
+        c = (x0.x >= q) + (x0.y >= q) + (x0.z >= q) + (x0.w >= q) + (x1.x >= q) + (x1.y >= q) + (x1.z >= q) +
+            (x1.w >= q) + (x2.x >= q) + (x2.y >= q) + (x2.z >= q) + (x2.w >= q) + (x3.x >= q) + (x3.y >= q) +
+            (x3.z >= q) + (x3.w >= q);
+    } else {
+        for (int i = base; i < end; i++) c += __ldg(row + i) >= q;
+    }
+    return base + c;
+}
+
 // Rank bounds of bucket b (SampleSearch::CoarseBinarySearch, SampleSearch.hpp:107-125).
 __device__ __host__ __forceinline__ void bucket_bounds(int b, int S, const int32_t *rank, int n_item, int &lb, int &ub) {
     const unsigned tlb = b == S ? (unsigned) n_item : (unsigned) rank[b];
@@ -226,6 +273,140 @@ struct QueryCounts {
 
 // Pair classes produced by the pruning step (PruneCandidateByBound.hpp:83-150).
 enum : uint8_t { kClsRefine = 0, kClsResult = 1, kClsPrune = 2, kClsIdle = 3 };
+
+// Histogram of small unsigned values per query (values >= n_bins are skipped), one CTA per
+// (user chunk, query).  Each warp counts into its own shared-memory copy (plain atomics, no warp
+// matching), the copies are summed, and the non-zero bins are added to the global histogram.
+constexpr int kHistThreads = 256;
+
+__host__ __device__ inline int hist_copies(int n_bins) {
+    int c = 98304 / (4 * n_bins);
+    return c < 1 ? 1 : (c > 8 ? 8 : c);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kHistThreads) bucket_hist_kernel(const T *__restrict__ vals, int64_t n_user,
+                                                                  int n_bins, int64_t chunk, int *__restrict__ hist) {
+    extern __shared__ int h[];
+    const int copies = hist_copies(n_bins);
+    const int q = blockIdx.y;
+    for (int b = threadIdx.x; b < copies * n_bins; b += blockDim.x) h[b] = 0;
+    __syncthreads();
+    int *mine = h + ((threadIdx.x >> 5) % copies) * n_bins;
+    const T *row = vals + (int64_t) q * n_user;
+    const int64_t u0 = (int64_t) blockIdx.x * chunk, u1 = min(u0 + chunk, n_user);
+    int64_t u = u0 + threadIdx.x;
+    for (; u + 3 * kHistThreads < u1; u += 4 * kHistThreads) {
+        const unsigned v0 = row[u], v1 = row[u + kHistThreads], v2 = row[u + 2 * kHistThreads],
+                       v3 = row[u + 3 * kHistThreads];
+        if (v0 < (unsigned) n_bins) atomicAdd(mine + v0, 1);
+        if (v1 < (unsigned) n_bins) atomicAdd(mine + v1, 1);
+        if (v2 < (unsigned) n_bins) atomicAdd(mine + v2, 1);
+        if (v3 < (unsigned) n_bins) atomicAdd(mine + v3, 1);
+    }
+    for (; u < u1; u += kHistThreads) {
+        const unsigned v = row[u];
+        if (v < (unsigned) n_bins) atomicAdd(mine + v, 1);
+    }
+    __syncthreads();
+    int *g = hist + (int64_t) q * n_bins;
+    for (int b = threadIdx.x; b < n_bins; b += blockDim.x) {
+        int s = 0;
+        for (int c = 0; c < copies; c++) s += h[c * n_bins + b];
+        if (s) atomicAdd(g + b, s);
+    }
+}
+
+// ---- ordered compaction of result users and candidates ---------------------------------------------
+//
+// Per query the reference lists result users in user-id order (QS.hpp:185-194) and collects the
+// refinement candidates (ComputeAllIPBound.hpp:306-313).  Users are cut into chunks of
+// kCompactChunk; pass 1 counts per (query, chunk), a scan turns the counts into offsets, pass 2
+// writes each chunk's entries at its offset -- so the lists come out in user-id order while every
+// chunk runs in parallel.  A policy P classifies a (query, user) pair (0 none, 1 result,
+// 2 candidate) and writes the entries.
+
+constexpr int kCompactThreads = 256;
+constexpr int kCompactPer = 16;
+constexpr int64_t kCompactChunk = (int64_t) kCompactThreads * kCompactPer;
+
+template <class P>
+__global__ void __launch_bounds__(kCompactThreads) compact_count_kernel(P p, int64_t n_user, int nchunks,
+                                                                      int2 *__restrict__ cnt) {
+    __shared__ int warp_tot[9];
+    const int q = blockIdx.y;
+    const int64_t u0 = (int64_t) blockIdx.x * kCompactChunk;
+    int r = 0, c = 0;
+    if (p.query_active(q)) {
+#pragma unroll 4
+        for (int e = 0; e < kCompactPer; e++) {
+            const int64_t u = u0 + (int64_t) e * kCompactThreads + threadIdx.x;
+            if (u >= n_user) break;
+            typename P::Aux aux;
+            const int k = p.classify(q, u, aux);
+            r += k == 1;
+            c += k == 2;
+        }
+    }
+    int tot;
+    block_excl_scan(r | (c << 16), warp_tot, &tot);
+    if (threadIdx.x == 0) cnt[(int64_t) q * nchunks + blockIdx.x] = make_int2(tot & 0xffff, tot >> 16);
+}
+
+// Offsets per (query, chunk); n_res_emit = min(results, topk); flags a candidate-count mismatch.
+static __global__ void compact_scan_kernel(const int2 *__restrict__ cnt, int nchunks, int nq, int topk, int2 *__restrict__ off,
+                                    QueryCounts *__restrict__ counts, int *__restrict__ err) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    int r = 0, c = 0;
+    for (int i = 0; i < nchunks; i++) {
+        const int2 v = cnt[(int64_t) q * nchunks + i];
+        off[(int64_t) q * nchunks + i] = make_int2(r, c);
+        r += v.x;
+        c += v.y;
+    }
+    counts[q].n_res_emit = r < topk ? r : topk;
+    if (c != counts[q].n_cand) atomicAdd(err, 1);
+}
+
+template <class P>
+__global__ void __launch_bounds__(kCompactThreads) compact_write_kernel(P p, int64_t n_user, int nchunks,
+                                                                      const int2 *__restrict__ cnt,
+                                                                      const int2 *__restrict__ off, int topk) {
+    __shared__ int warp_tot[9];
+    const int q = blockIdx.y;
+    const int2 cc = cnt[(int64_t) q * nchunks + blockIdx.x];
+    const int2 oo = off[(int64_t) q * nchunks + blockIdx.x];
+    if ((cc.x == 0 || oo.x >= topk) && cc.y == 0) return;
+    // thread t owns users u0 + t*kCompactPer .. + kCompactPer - 1, so prefix order is user-id order
+    const int64_t u0 = (int64_t) blockIdx.x * kCompactChunk + (int64_t) threadIdx.x * kCompactPer;
+    int r = 0, c = 0;
+    for (int e = 0; e < kCompactPer; e++) {
+        const int64_t u = u0 + e;
+        if (u >= n_user) break;
+        typename P::Aux aux;
+        const int k = p.classify(q, u, aux);
+        r += k == 1;
+        c += k == 2;
+    }
+    int tot;
+    const int pre = block_excl_scan(r | (c << 16), warp_tot, &tot);
+    if (r == 0 && c == 0) return;
+    int pr = oo.x + (pre & 0xffff), pc = oo.y + (pre >> 16);
+    for (int e = 0; e < kCompactPer; e++) {
+        const int64_t u = u0 + e;
+        if (u >= n_user) break;
+        typename P::Aux aux;
+        const int k = p.classify(q, u, aux);
+        if (k == 1) {
+            if (pr < topk) p.emit_result(q, pr, u, aux);
+            pr++;
+        } else if (k == 2) {
+            p.emit_cand(q, pc, u, aux);
+            pc++;
+        }
+    }
+}
 
 }  // namespace rkr
 
@@ -326,6 +507,33 @@ template <typename F> inline void timed(rkr_index *ix, cudaStream_t st, const ch
     cudaEventRecord(p.b, st);
     ix->prof.pending.push_back(p);
 }
+// Ordered compaction driver shared by QS and QSRP (pass 1, scan, pass 2).
+template <class P>
+inline int run_compaction(rkr_index *ix, P p, int nq, int topk, QueryCounts *counts, cudaStream_t st) {
+    const int64_t U = ix->n_user;
+    const int nchunks = (int) ((U + kCompactChunk - 1) / kCompactChunk);
+    RKR_TRY(ix->ws_cand_off.ensure(sizeof(int2) * 2 * (size_t) nq * nchunks + 256));
+    int2 *cnt = ix->ws_cand_off.as<int2>();
+    int2 *off = cnt + (size_t) nq * nchunks;
+    int *err = reinterpret_cast<int *>(off + (size_t) nq * nchunks);
+    RKR_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+    dim3 g((unsigned) nchunks, (unsigned) nq);
+    timed(ix, st, "compact_count", [&] { compact_count_kernel<P><<<g, kCompactThreads, 0, st>>>(p, U, nchunks, cnt); });
+    RKR_CUDA(cudaGetLastError());
+    timed(ix, st, "compact_scan", [&] { compact_scan_kernel<<<(nq + 127) / 128, 128, 0, st>>>(cnt, nchunks, nq, topk, off, counts, err); });
+    RKR_CUDA(cudaGetLastError());
+    timed(ix, st, "compact_write", [&] { compact_write_kernel<P><<<g, kCompactThreads, 0, st>>>(p, U, nchunks, cnt, off, topk); });
+    RKR_CUDA(cudaGetLastError());
+    int h_err = 0;
+    RKR_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    RKR_CUDA(cudaStreamSynchronize(st));
+    if (h_err) {
+        set_error("internal: candidate count mismatch in %d queries", h_err);
+        return RKR_ERR_STATE;
+    }
+    return RKR_OK;
+}
+
 int ensure_device(const rkr_index *ix);
 int refine_prepare_norms(rkr_index *ix);
 int query_batch(rkr_index *ix, int method, const float *d_query, int n_query, int topk, rkr_user_rank *d_out,

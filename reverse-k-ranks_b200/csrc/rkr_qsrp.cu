@@ -95,6 +95,8 @@ __device__ __forceinline__ int level_rank(int lvl, const int32_t *rank, int S, i
 
 // ---- kernels ---------------------------------------------------------------------------------------
 
+constexpr uint16_t kStateResult1 = 0xfffe, kStatePruned1 = 0xffff;
+
 struct QsrpParams {
     int32_t mode1, all1, L1, U1;         // round 1: equal-bounds mode, "all survivors accepted", k-th bounds
     int32_t n_res1, n_pr1, n_ref1, skip2; // round-1 counts; skip2: round 1 already produced top-k results
@@ -117,18 +119,19 @@ __global__ void transfer_query_kernel(const float *__restrict__ query, const flo
     }
 }
 
-// Round 1 for every pair: left = InnerProduct(svd_user, qtr, check_dim); bounds left -+ norms;
-// regression levels of both bounds packed as (lb | ub << 16).
+// Round 1 for every pair: left = InnerProduct(svd_user, qtr, check_dim) (kept for round 2);
+// bounds left -+ norms; regression levels of both bounds packed as (lb | ub << 16).
 __global__ void __launch_bounds__(kTileThreads) qsrp_round1_kernel(const float *__restrict__ svd_user, int64_t n_user,
                                                                   int dim, const float *__restrict__ unorm,
                                                                   const float *__restrict__ qtr,
                                                                   const float *__restrict__ qnorm, int n_query,
-                                                                  int check_dim, RegModel m, uint32_t *__restrict__ lv) {
+                                                                  int check_dim, RegModel m, uint32_t *__restrict__ lv,
+                                                                  float *__restrict__ left) {
     __shared__ TileSmem sm;
     const int64_t b0 = (int64_t) blockIdx.x * kTile;
     const int64_t a0 = (int64_t) blockIdx.y * kTile;
     float lo[4][4], hi[4][4];
-    exact_tile(sm, svd_user, nullptr, n_user, dim, a0, qtr, n_query, dim, b0, check_dim, check_dim, lo, hi);
+    exact_tile(sm, svd_user, nullptr, n_user, dim, a0, qtr, n_query, dim, b0, 0, check_dim, check_dim, lo, hi);
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
@@ -143,41 +146,84 @@ __global__ void __launch_bounds__(kTileThreads) qsrp_round1_kernel(const float *
             int l, h;
             regression_levels(m, u, __fsub_rn(lo[i][j], right), __fadd_rn(lo[i][j], right), l, h);
             lv[q * n_user + u] = (uint32_t) l | ((uint32_t) h << 16);
+            left[q * n_user + u] = lo[i][j];
         }
     }
 }
 
-// Round-1 k-th smallest bounds per query (PruneCandidateByBound.hpp:36-77 with nothing excluded).
-__global__ void qsrp_select1_kernel(const uint32_t *__restrict__ lv, int64_t n_user, const int32_t *__restrict__ rank,
-                                    int S, int n_item, int topk, QsrpParams *__restrict__ par) {
-    extern __shared__ int h[];  // 2 * (S + 2)
-    const int nl = S + 2;
-    const int q = blockIdx.x;
-    for (int b = threadIdx.x; b < 2 * nl; b += blockDim.x) h[b] = 0;
+// Histograms of the round-1 lower- and upper-bound levels per query, one CTA per (user chunk,
+// query), counted in per-warp shared-memory copies; also counts pairs whose upper bound exceeds
+// their lower bound (never expected, but it would void the shortcut qsrp_select1 takes for the
+// class counts).
+__global__ void __launch_bounds__(kHistThreads) level_hist_kernel(const uint32_t *__restrict__ lv, int64_t n_user,
+                                                                 const int32_t *__restrict__ rank, int S, int n_item,
+                                                                 int64_t chunk, int *__restrict__ hist,
+                                                                 int *__restrict__ anomaly) {
+    extern __shared__ int h[];
+    __shared__ int anom;
+    const int nl = S + 2, nb = 2 * nl;
+    const int copies = hist_copies(nb);
+    const int q = blockIdx.y;
+    for (int b = threadIdx.x; b < copies * nb; b += blockDim.x) h[b] = 0;
+    if (threadIdx.x == 0) anom = 0;
     __syncthreads();
+    int *mine = h + ((threadIdx.x >> 5) % copies) * nb;
     const uint32_t *row = lv + (int64_t) q * n_user;
-    for (int64_t u = threadIdx.x; u < n_user; u += blockDim.x) {
+    const int64_t u0 = (int64_t) blockIdx.x * chunk, u1 = min(u0 + chunk, n_user);
+    int my_anom = 0;
+    for (int64_t u = u0 + threadIdx.x; u < u1; u += kHistThreads) {
         const uint32_t v = row[u];
-        const unsigned act = __activemask();
         const int l = v & 0xffff, hh = v >> 16;
-        unsigned peers = __match_any_sync(act, l);
-        if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&h[l], __popc(peers));
-        peers = __match_any_sync(act, hh);
-        if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&h[nl + hh], __popc(peers));
+        atomicAdd(mine + l, 1);
+        atomicAdd(mine + nl + hh, 1);
+        my_anom += hh > l && level_rank(hh, rank, S, n_item) > level_rank(l, rank, S, n_item);
     }
+    if (my_anom) atomicAdd(&anom, my_anom);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        int kl = nl - 1, kh = nl - 1;
-        int64_t c = 0;
-        for (int b = 0; b < nl; b++) { c += h[b]; if (c >= topk) { kl = b; break; } }
-        c = 0;
-        for (int b = 0; b < nl; b++) { c += h[nl + b]; if (c >= topk) { kh = b; break; } }
-        QsrpParams p = {};
-        p.L1 = level_rank(kl, rank, S, n_item);
-        p.U1 = level_rank(kh, rank, S, n_item);
-        p.mode1 = p.L1 == p.U1;
-        par[q] = p;
+    int *g = hist + (int64_t) q * nb;
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+        int sum = 0;
+        for (int c = 0; c < copies; c++) sum += h[c * nb + b];
+        if (sum) atomicAdd(g + b, sum);
     }
+    if (threadIdx.x == 0 && anom) atomicAdd(anomaly + q, anom);
+}
+
+// Round-1 k-th smallest bounds per query (PruneCandidateByBound.hpp:36-77 with nothing excluded)
+// and the class counts.  While every pair has ub <= lb, a result (lb <= U*) and a prune
+// (ub >= L*) cannot coincide unless L* == U*, so the counts follow from the two histograms;
+// otherwise qsrp_count1 counts pair by pair.
+__global__ void qsrp_select1_kernel(const int *__restrict__ hist_all, const int *__restrict__ anomaly, int64_t n_user,
+                                    const int32_t *__restrict__ rank, int S, int n_item, int topk, int nq,
+                                    QsrpParams *__restrict__ par) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    const int nl = S + 2;
+    const int *h = hist_all + (int64_t) q * 2 * nl;
+    int kl = nl - 1, kh = nl - 1;
+    int64_t c = 0;
+    for (int b = 0; b < nl; b++) { c += h[b]; if (c >= topk) { kl = b; break; } }
+    c = 0;
+    for (int b = 0; b < nl; b++) { c += h[nl + b]; if (c >= topk) { kh = b; break; } }
+    QsrpParams p = {};
+    p.L1 = level_rank(kl, rank, S, n_item);
+    p.U1 = level_rank(kh, rank, S, n_item);
+    p.mode1 = p.L1 == p.U1;
+    if (!p.mode1) {
+        if (anomaly[q]) {
+            p.pad0 = 1;  // exact counting needed
+        } else {
+            int64_t nres = 0, npr = 0;
+            for (int b = 0; b < nl; b++) {
+                if (level_rank(b, rank, S, n_item) <= p.U1) nres += h[b];
+                if (level_rank(b, rank, S, n_item) >= p.L1) npr += h[nl + b];
+            }
+            p.n_res1 = (int) nres;
+            p.n_pr1 = (int) npr;
+            p.n_ref1 = (int) (n_user - nres - npr);
+        }
+    }
+    par[q] = p;
 }
 
 __device__ __forceinline__ int class1_of(const QsrpParams &p, int lb, int ub) {
@@ -187,12 +233,13 @@ __device__ __forceinline__ int class1_of(const QsrpParams &p, int lb, int ub) {
     return p.all1 ? kClsResult : kClsRefine;
 }
 
-// Round-1 class counts (the reference's reduction at PruneCandidateByBound.hpp:115-136).
+// Round-1 class counts pair by pair (the reduction at PruneCandidateByBound.hpp:115-136), for
+// queries where the histogram shortcut does not apply.
 __global__ void qsrp_count1_kernel(const uint32_t *__restrict__ lv, int64_t n_user, const int32_t *__restrict__ rank,
                                    int S, int n_item, QsrpParams *__restrict__ par) {
     const int q = blockIdx.y;
     const QsrpParams p = par[q];
-    if (p.mode1) return;
+    if (p.mode1 || !p.pad0) return;
     __shared__ int cnt[3];
     if (threadIdx.x < 3) cnt[threadIdx.x] = 0;
     __syncthreads();
@@ -241,33 +288,45 @@ __device__ __forceinline__ bool eligible2(const QsrpParams &p, uint32_t v, const
     return k == kClsRefine || k == kClsIdle;
 }
 
-// Round 2: full SVD-space score of each surviving pair and its sampled-threshold bucket
-// (0xffff marks pairs that did not reach round 2).
+// Round 2: full SVD-space score of each surviving pair, left (round 1) + the remaining dims
+// (ComputeRemainDim, PartDimPartNorm.hpp:76-95), and its sampled-threshold bucket.  Pairs that did
+// not reach round 2 get a state code instead: kStateResult1 (accepted in round 1) or kStatePruned1.
 __global__ void __launch_bounds__(kTileThreads) qsrp_round2_kernel(const float *__restrict__ svd_user, int64_t n_user,
                                                                   int dim, const float *__restrict__ qtr, int n_query,
                                                                   int check_dim, const uint32_t *__restrict__ lv,
+                                                                  const float *__restrict__ left,
                                                                   const QsrpParams *__restrict__ par,
                                                                   const int32_t *__restrict__ reg_rank, int S_reg,
                                                                   int n_item, const float *__restrict__ thr, int S,
                                                                   uint16_t *__restrict__ bucket2) {
     __shared__ TileSmem sm;
+    __shared__ ThrSummary ts;
+    __shared__ QsrpParams par_s[kTile];
     const int64_t b0 = (int64_t) blockIdx.x * kTile;
     const int64_t a0 = (int64_t) blockIdx.y * kTile;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    bool el[4][4];
-    bool any = false;
+    if (threadIdx.x < kTile && b0 + threadIdx.x < n_query) par_s[threadIdx.x] = par[b0 + threadIdx.x];
+    __syncthreads();
+    uint32_t el = 0, r1 = 0;  // bit 4*i + j: reached round 2 / accepted in round 1
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             const int64_t u = a0 + 4 * tx + i, q = b0 + 4 * ty + j;
-            el[i][j] = false;
-            if (u < n_user && q < n_query) el[i][j] = eligible2(par[q], lv[q * n_user + u], reg_rank, S_reg, n_item);
-            any |= el[i][j];
+            if (u < n_user && q < n_query) {
+                const uint32_t v = lv[q * n_user + u];
+                const int k = class1_of(par_s[4 * ty + j], level_rank(v & 0xffff, reg_rank, S_reg, n_item),
+                                        level_rank(v >> 16, reg_rank, S_reg, n_item));
+                if (k == kClsRefine || k == kClsIdle) el |= 1u << (4 * i + j);
+                else if (k == kClsResult) r1 |= 1u << (4 * i + j);
+            }
         }
-    any = __syncthreads_or(any);
+    const bool any = __syncthreads_or(el != 0);
     float lo[4][4], hi[4][4];
-    if (any) exact_tile(sm, svd_user, nullptr, n_user, dim, a0, qtr, n_query, dim, b0, check_dim, dim, lo, hi);
+    if (any) {
+        load_thr_summary(ts, thr, n_user, a0, S);
+        exact_tile(sm, svd_user, nullptr, n_user, dim, a0, qtr, n_query, dim, b0, check_dim, dim, dim, lo, hi);
+    }
 #pragma unroll
     for (int i = 0; i < 4; i++) {
         const int64_t u = a0 + 4 * tx + i;
@@ -276,8 +335,11 @@ __global__ void __launch_bounds__(kTileThreads) qsrp_round2_kernel(const float *
         for (int j = 0; j < 4; j++) {
             const int64_t q = b0 + 4 * ty + j;
             if (q >= n_query) continue;
-            uint16_t b = 0xffff;
-            if (el[i][j]) b = (uint16_t) bucket_of(thr + u * S, S, __fadd_rn(lo[i][j], hi[i][j]));
+            uint16_t b = (r1 >> (4 * i + j) & 1) ? kStateResult1 : kStatePruned1;
+            if (el >> (4 * i + j) & 1) {
+                const float qip = __fadd_rn(left[q * n_user + u], lo[i][j]);
+                b = (uint16_t) bucket_of_2level(ts.v[4 * tx + i], thr + u * S, S, qip);
+            }
             bucket2[q * n_user + u] = b;
         }
     }
@@ -286,35 +348,23 @@ __global__ void __launch_bounds__(kTileThreads) qsrp_round2_kernel(const float *
 // Round-2 pruning per query (second PruneCandidateByBound call, QSRPNormalLP.hpp:187-190): users
 // excluded in round 1 are skipped by the heap scan and the classification; the equal-bounds rule
 // looks at every user's current bounds.
-__global__ void qsrp_select2_kernel(const uint16_t *__restrict__ bucket2, int64_t n_user, int S,
-                                    const int32_t *__restrict__ rank, int n_item, int topk, QsrpParams *__restrict__ par,
+__global__ void qsrp_select2_kernel(const int *__restrict__ hist_all, int S, const int32_t *__restrict__ rank,
+                                    int n_item, int topk, int nq, QsrpParams *__restrict__ par,
                                     uint8_t *__restrict__ cls2, QueryCounts *__restrict__ counts) {
-    extern __shared__ int hist[];  // S + 1
-    const int q = blockIdx.x;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
     QsrpParams p = par[q];
     uint8_t *cq = cls2 + (int64_t) q * (S + 1);
     if (p.skip2) {
-        if (threadIdx.x == 0) {
-            QueryCounts c = {};
-            c.n_result = p.n_res1;
-            c.n_prune = p.n_pr1;
-            c.n_cand = 0;
-            c.mode = 2;
-            counts[q] = c;
-        }
+        QueryCounts c = {};
+        c.n_result = p.n_res1;
+        c.n_prune = p.n_pr1;
+        c.n_cand = 0;
+        c.mode = 2;
+        counts[q] = c;
         return;
     }
-    for (int b = threadIdx.x; b <= S; b += blockDim.x) hist[b] = 0;
-    __syncthreads();
-    const uint16_t *row = bucket2 + (int64_t) q * n_user;
-    for (int64_t u = threadIdx.x; u < n_user; u += blockDim.x) {
-        const int v = row[u];
-        const unsigned act = __activemask();
-        const unsigned peers = __match_any_sync(act, v);
-        if (v != 0xffff && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[v], __popc(peers));
-    }
-    __syncthreads();
-    if (threadIdx.x != 0) return;
+    const int *hist = hist_all + (int64_t) q * (S + 1);
     const int kp = topk - p.n_res1;
     int64_t n_el = 0;
     for (int b = 0; b <= S; b++) n_el += hist[b];
@@ -369,76 +419,64 @@ __global__ void qsrp_select2_kernel(const uint16_t *__restrict__ bucket2, int64_
     counts[q] = c;
 }
 
-// Per query, in user-id order: result users (with their reported rank and whether their score is
-// this query's or a carried one) and the refinement candidates.
-__global__ void qsrp_compact_kernel(const uint32_t *__restrict__ lv, const uint16_t *__restrict__ bucket2, int64_t n_user,
-                                    const int32_t *__restrict__ reg_rank, int S_reg, const int32_t *__restrict__ rank,
-                                    int S, int n_item, const QsrpParams *__restrict__ par, const uint8_t *__restrict__ cls2,
-                                    QueryCounts *__restrict__ counts, const int64_t *__restrict__ cand_off, int topk,
-                                    int32_t *__restrict__ res_user, int32_t *__restrict__ res_rank,
-                                    uint8_t *__restrict__ res_fresh, int32_t *__restrict__ cand_user,
-                                    int32_t *__restrict__ cand_query, int32_t *__restrict__ cand_lb,
-                                    int32_t *__restrict__ cand_ub) {
-    extern __shared__ uint8_t cls_s[];
-    __shared__ int warp_tot[9];
-    const int q = blockIdx.x;
-    const QsrpParams p = par[q];
-    const int n_cand = counts[q].n_cand;
-    for (int b = threadIdx.x; b <= S; b += blockDim.x) cls_s[b] = cls2[(int64_t) q * (S + 1) + b];
-    __syncthreads();
-    const uint32_t *lrow = lv + (int64_t) q * n_user;
-    const uint16_t *brow = bucket2 + (int64_t) q * n_user;
-    int nres = 0, ncand = 0;
-    const int64_t coff = cand_off[q];
-    for (int64_t base = 0; base < n_user; base += blockDim.x) {
-        if (nres >= topk && ncand >= n_cand) break;
-        const int64_t u = base + threadIdx.x;
-        int isres = 0, iscand = 0, rk = 0, fresh = 0, clb = 0, cub = 0;
-        if (u < n_user) {
-            const uint32_t v = lrow[u];
+// Classification of a pair after both rounds for the ordered compaction: result users carry their
+// reported rank (the lower bound in force) and whether their score is this query's; candidates
+// carry their round-2 bounds.
+struct QsrpCompactPolicy {
+    struct Aux { int rank, fresh, lb, ub; };
+    const uint32_t *lv;
+    const uint16_t *b2;
+    int64_t n_user;
+    const int32_t *reg_rank, *rank;
+    int S_reg, S, n_item;
+    const QsrpParams *par;
+    const uint8_t *cls2;
+    const QueryCounts *counts;
+    const int64_t *cand_off;
+    int topk;
+    int32_t *res_user, *res_rank;
+    uint8_t *res_fresh;
+    int32_t *cand_user, *cand_query, *cand_lb, *cand_ub;
+    __device__ bool query_active(int q) const { return true; }
+    __device__ int classify(int q, int64_t u, Aux &aux) const {
+        const QsrpParams &p = par[q];
+        const uint16_t code = b2[(int64_t) q * n_user + u];
+        if (code <= S) {  // reached round 2
+            int lb, ub;
+            bucket_bounds(code, S, rank, n_item, lb, ub);
+            aux.rank = lb; aux.fresh = 1; aux.lb = lb; aux.ub = ub;
+            if (p.skip2) return 0;
+            if (p.mode2) return (ub <= p.L2 && lb <= p.L2) ? 1 : 0;
+            const uint8_t k2 = __ldg(cls2 + (int64_t) q * (S + 1) + code);
+            if (k2 == kClsResult) return 1;
+            return (k2 == kClsRefine && counts[q].n_cand > 0) ? 2 : 0;
+        }
+        aux.fresh = 0;
+        if (code == kStateResult1 || (!p.skip2 && p.mode2)) {
+            const uint32_t v = lv[(int64_t) q * n_user + u];
             const int lb1 = level_rank(v & 0xffff, reg_rank, S_reg, n_item);
             const int ub1 = level_rank(v >> 16, reg_rank, S_reg, n_item);
-            const int k1 = class1_of(p, lb1, ub1);
-            const uint16_t b2 = brow[u];
-            int lbc = lb1, ubc = ub1;
-            if (b2 != 0xffff) bucket_bounds(b2, S, rank, n_item, lbc, ubc);
-            if (k1 == kClsResult) {
-                isres = 1;
-            } else if (!p.skip2) {
-                if (p.mode2) {
-                    isres = ubc <= p.L2 && lbc <= p.L2;
-                } else if (b2 != 0xffff) {
-                    const uint8_t k2 = cls_s[b2];
-                    isres = k2 == kClsResult;
-                    iscand = k2 == kClsRefine && n_cand > 0;
-                }
-            }
-            rk = lbc;
-            fresh = b2 != 0xffff;
-            clb = lbc;
-            cub = ubc;
+            aux.rank = lb1; aux.lb = lb1; aux.ub = ub1;
+            if (code == kStateResult1) return 1;
+            return (ub1 <= p.L2 && lb1 <= p.L2) ? 1 : 0;  // the equal-bounds rule scans every user
         }
-        int tot;
-        const int pre = block_excl_scan(isres | (iscand << 16), warp_tot, &tot);
-        if (isres) {
-            const int pos = nres + (pre & 0xffff);
-            if (pos < topk) {
-                res_user[(int64_t) q * topk + pos] = (int32_t) u;
-                res_rank[(int64_t) q * topk + pos] = rk;
-                res_fresh[(int64_t) q * topk + pos] = (uint8_t) fresh;
-            }
-        } else if (iscand) {
-            const int64_t pos = coff + ncand + (pre >> 16);
-            cand_user[pos] = (int32_t) u;
-            cand_query[pos] = q;
-            cand_lb[pos] = clb;
-            cand_ub[pos] = cub;
-        }
-        nres += tot & 0xffff;
-        ncand += tot >> 16;
+        return 0;
     }
-    if (threadIdx.x == 0) counts[q].n_res_emit = min(nres, topk);
-}
+    __device__ void emit_result(int q, int pos, int64_t u, const Aux &aux) const {
+        const int64_t i = (int64_t) q * topk + pos;
+        res_user[i] = (int32_t) u;
+        res_rank[i] = aux.rank;
+        res_fresh[i] = (uint8_t) aux.fresh;
+    }
+    __device__ void emit_cand(int q, int pos, int64_t u, const Aux &aux) const {
+        if (pos >= counts[q].n_cand) return;  // the count pass disagrees; reported by compact_scan
+        const int64_t e = cand_off[q] + pos;
+        cand_user[e] = (int32_t) u;
+        cand_query[e] = q;
+        cand_lb[e] = aux.lb;
+        cand_ub[e] = aux.ub;
+    }
+};
 
 // Exact SVD-space score of (query, user): checkdim part + remaining part (PartDimPartNorm.hpp:62, 89-92).
 __device__ __forceinline__ float qsrp_score(const float *svd_user, const float *qtr, int64_t u, int q, int dim, int c) {
@@ -461,7 +499,7 @@ __global__ void qsrp_result_fill_kernel(const QueryCounts *__restrict__ counts, 
         const int u = res_user[i];
         int src = res_fresh[i] ? q : -1;
         for (int qq = q - 1; src < 0 && qq >= 0; qq--)
-            if (bucket2[(int64_t) qq * n_user + u] != 0xffff) src = qq;
+            if (bucket2[(int64_t) qq * n_user + u] < kStateResult1) src = qq;
         res_qip[i] = src >= 0 ? qsrp_score(svd_user, qtr, u, src, dim, check_dim) : state[u];
     }
 }
@@ -481,7 +519,7 @@ __global__ void qsrp_state_kernel(const uint16_t *__restrict__ bucket2, int64_t 
     const int64_t u = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= n_user) return;
     for (int q = nq - 1; q >= 0; q--)
-        if (bucket2[(int64_t) q * n_user + u] != 0xffff) {
+        if (bucket2[(int64_t) q * n_user + u] < kStateResult1) {
             state[u] = qsrp_score(svd_user, qtr, u, q, dim, check_dim);
             return;
         }
@@ -505,21 +543,29 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     const int64_t U = ix->n_user;
     const int dim = ix->dim, c = ix->check_dim, S = ix->n_sample, Sr = ix->n_sample_reg;
     const int n_item = (int) ix->n_item;
-    RKR_TRY(ix->ws_qtr.ensure(carve_size((size_t) nq * dim, 4) + carve_size(nq, 4) + carve_size(nq, sizeof(QsrpParams))));
+    const int nl = Sr + 2;
+    RKR_TRY(ix->ws_qtr.ensure(carve_size((size_t) nq * dim, 4) + carve_size(nq, 4) + carve_size(nq, sizeof(QsrpParams)) +
+                              carve_size(nq, 4)));
     uint8_t *p0 = ix->ws_qtr.as<uint8_t>();
     float *qtr = carve<float>(p0, (size_t) nq * dim);
     float *qnorm = carve<float>(p0, nq);
     QsrpParams *par = carve<QsrpParams>(p0, nq);
-    RKR_TRY(ix->ws_levels.ensure((size_t) nq * U * 4));
+    int *anomaly = carve<int>(p0, nq);
+    RKR_TRY(ix->ws_levels.ensure((size_t) nq * U * 8));
     RKR_TRY(ix->ws_bucket2.ensure((size_t) nq * U * 2));
     RKR_TRY(ix->ws_cls.ensure((size_t) nq * (S + 1)));
     RKR_TRY(ix->ws_counts.ensure(sizeof(QueryCounts) * (size_t) nq));
+    RKR_TRY(ix->ws_hist.ensure(sizeof(int) * (size_t) nq * std::max(2 * nl, S + 1)));
     uint32_t *lv = ix->ws_levels.as<uint32_t>();
+    float *left = reinterpret_cast<float *>(lv + (size_t) nq * U);
     uint16_t *b2 = ix->ws_bucket2.as<uint16_t>();
     QueryCounts *counts = ix->ws_counts.as<QueryCounts>();
-    RKR_CUDA(cudaMemsetAsync(par, 0, sizeof(QsrpParams) * nq, st));
+    int *hist = ix->ws_hist.as<int>();
+    RKR_CUDA(cudaMemsetAsync(anomaly, 0, sizeof(int) * nq, st));
 
-    timed(ix, st, "transfer_query", [&] { transfer_query_kernel<<<nq, 128, 0, st>>>(d_query, ix->transfer_item.as<float>(), dim, c, qtr, qnorm); });
+    timed(ix, st, "transfer_query", [&] {
+        transfer_query_kernel<<<nq, 128, 0, st>>>(d_query, ix->transfer_item.as<float>(), dim, c, qtr, qnorm);
+    });
     RKR_CUDA(cudaGetLastError());
     RegModel m;
     m.rec = ix->reg.as<float>();
@@ -528,10 +574,22 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     m.err_cap = (double) Sr - 1e-3;
     m.n_item = n_item;
     dim3 grid((unsigned) ((nq + kTile - 1) / kTile), (unsigned) ((U + kTile - 1) / kTile));
-    timed(ix, st, "qsrp_round1", [&] { qsrp_round1_kernel<<<grid, kTileThreads, 0, st>>>(ix->svd_user.as<float>(), U, dim, ix->svd_unorm.as<float>(), qtr,
-                                                     qnorm, nq, c, m, lv); });
+    timed(ix, st, "qsrp_round1", [&] {
+        qsrp_round1_kernel<<<grid, kTileThreads, 0, st>>>(ix->svd_user.as<float>(), U, dim, ix->svd_unorm.as<float>(),
+                                                         qtr, qnorm, nq, c, m, lv, left);
+    });
     RKR_CUDA(cudaGetLastError());
-    timed(ix, st, "qsrp_select1", [&] { qsrp_select1_kernel<<<nq, 256, 2 * (Sr + 2) * sizeof(int), st>>>(lv, U, m.rank, Sr, n_item, topk, par); });
+    const int64_t chunk = 16384;
+    dim3 hg((unsigned) ((U + chunk - 1) / chunk), (unsigned) nq);
+    RKR_CUDA(cudaMemsetAsync(hist, 0, sizeof(int) * (size_t) nq * 2 * nl, st));
+    timed(ix, st, "level_hist", [&] {
+        level_hist_kernel<<<hg, kHistThreads, hist_copies(2 * nl) * 2 * nl * sizeof(int), st>>>(lv, U, m.rank, Sr, n_item,
+                                                                                               chunk, hist, anomaly);
+    });
+    RKR_CUDA(cudaGetLastError());
+    timed(ix, st, "qsrp_select1", [&] {
+        qsrp_select1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(hist, anomaly, U, m.rank, Sr, n_item, topk, nq, par);
+    });
     RKR_CUDA(cudaGetLastError());
     {
         dim3 g((unsigned) std::min<int64_t>((U + 1023) / 1024, 64), (unsigned) nq);
@@ -540,11 +598,20 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     }
     timed(ix, st, "qsrp_final1", [&] { qsrp_final1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, topk); });
     RKR_CUDA(cudaGetLastError());
-    timed(ix, st, "qsrp_round2", [&] { qsrp_round2_kernel<<<grid, kTileThreads, 0, st>>>(ix->svd_user.as<float>(), U, dim, qtr, nq, c, lv, par, m.rank, Sr,
-                                                     n_item, ix->thr.as<float>(), S, b2); });
+    timed(ix, st, "qsrp_round2", [&] {
+        qsrp_round2_kernel<<<grid, kTileThreads, 0, st>>>(ix->svd_user.as<float>(), U, dim, qtr, nq, c, lv, left, par,
+                                                         m.rank, Sr, n_item, ix->thr.as<float>(), S, b2);
+    });
     RKR_CUDA(cudaGetLastError());
-    timed(ix, st, "qsrp_select2", [&] { qsrp_select2_kernel<<<nq, 256, (S + 1) * sizeof(int), st>>>(b2, U, S, ix->sample_rank.as<int32_t>(), n_item, topk,
-                                                               par, ix->ws_cls.as<uint8_t>(), counts); });
+    RKR_CUDA(cudaMemsetAsync(hist, 0, sizeof(int) * (size_t) nq * (S + 1), st));
+    timed(ix, st, "bucket_hist", [&] {
+        bucket_hist_kernel<<<hg, kHistThreads, hist_copies(S + 1) * (S + 1) * sizeof(int), st>>>(b2, U, S + 1, chunk, hist);
+    });
+    RKR_CUDA(cudaGetLastError());
+    timed(ix, st, "qsrp_select2", [&] {
+        qsrp_select2_kernel<<<(nq + 127) / 128, 128, 0, st>>>(hist, S, ix->sample_rank.as<int32_t>(), n_item, topk, nq,
+                                                             par, ix->ws_cls.as<uint8_t>(), counts);
+    });
     RKR_CUDA(cudaGetLastError());
 
     std::vector<QueryCounts> hc(nq);
@@ -568,23 +635,46 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     int32_t *cand_ub = carve<int32_t>(p, n_cand);
     float *cand_qip = carve<float>(p, n_cand);
     RKR_CUDA(cudaMemcpyAsync(d_off, off.data(), sizeof(int64_t) * (nq + 1), cudaMemcpyHostToDevice, st));
-    timed(ix, st, "qsrp_compact", [&] { qsrp_compact_kernel<<<nq, 256, S + 1, st>>>(lv, b2, U, m.rank, Sr, ix->sample_rank.as<int32_t>(), S, n_item, par,
-                                                ix->ws_cls.as<uint8_t>(), counts, d_off, topk, res_user, res_rank,
-                                                res_fresh, cand_user, cand_query, cand_lb, cand_ub); });
-    RKR_CUDA(cudaGetLastError());
-    timed(ix, st, "qsrp_result_fill", [&] { qsrp_result_fill_kernel<<<nq, 128, 0, st>>>(counts, res_user, res_fresh, b2, U, ix->svd_user.as<float>(), qtr, dim, c,
-                                                ix->qip_state.as<float>(), topk, res_qip); });
+    QsrpCompactPolicy pol;
+    pol.lv = lv;
+    pol.b2 = b2;
+    pol.n_user = U;
+    pol.reg_rank = m.rank;
+    pol.rank = ix->sample_rank.as<int32_t>();
+    pol.S_reg = Sr;
+    pol.S = S;
+    pol.n_item = n_item;
+    pol.par = par;
+    pol.cls2 = ix->ws_cls.as<uint8_t>();
+    pol.counts = counts;
+    pol.cand_off = d_off;
+    pol.topk = topk;
+    pol.res_user = res_user;
+    pol.res_rank = res_rank;
+    pol.res_fresh = res_fresh;
+    pol.cand_user = cand_user;
+    pol.cand_query = cand_query;
+    pol.cand_lb = cand_lb;
+    pol.cand_ub = cand_ub;
+    RKR_TRY(run_compaction(ix, pol, nq, topk, counts, st));
+    timed(ix, st, "qsrp_result_fill", [&] {
+        qsrp_result_fill_kernel<<<nq, 128, 0, st>>>(counts, res_user, res_fresh, b2, U, ix->svd_user.as<float>(), qtr,
+                                                    dim, c, ix->qip_state.as<float>(), topk, res_qip);
+    });
     RKR_CUDA(cudaGetLastError());
     if (n_cand > 0) {
-        timed(ix, st, "qsrp_cand_fill", [&] { qsrp_cand_fill_kernel<<<(unsigned) ((n_cand + 255) / 256), 256, 0, st>>>(cand_user, cand_query, n_cand,
-                                                                                 ix->svd_user.as<float>(), qtr, dim, c,
-                                                                                 cand_qip); });
+        timed(ix, st, "qsrp_cand_fill", [&] {
+            qsrp_cand_fill_kernel<<<(unsigned) ((n_cand + 255) / 256), 256, 0, st>>>(
+                cand_user, cand_query, n_cand, ix->svd_user.as<float>(), qtr, dim, c, cand_qip);
+        });
         RKR_CUDA(cudaGetLastError());
     }
     RKR_TRY(refine_and_assemble_qsrp(ix, d_query, nq, topk, counts, res_user, res_rank, res_qip, n_cand, cand_user,
                                      cand_query, cand_lb, cand_ub, cand_qip, d_off, d_out, d_stats, st));
-    timed(ix, st, "qsrp_state", [&] { qsrp_state_kernel<<<(unsigned) ((U + 255) / 256), 256, 0, st>>>(b2, U, nq, ix->svd_user.as<float>(), qtr, dim, c,
-                                                                    ix->qip_state.as<float>()); });
+    timed(ix, st, "qsrp_state", [&] {
+        qsrp_state_kernel<<<(unsigned) ((U + 255) / 256), 256, 0, st>>>(b2, U, nq, ix->svd_user.as<float>(), qtr, dim,
+                                                                        c, ix->qip_state.as<float>());
+    });
     RKR_CUDA(cudaGetLastError());
     RKR_CUDA(cudaStreamSynchronize(st));
     return RKR_OK;

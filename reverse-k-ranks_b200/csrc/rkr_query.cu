@@ -38,10 +38,12 @@ __global__ void __launch_bounds__(kTileThreads) score_bucket_kernel(const float 
                                                                    int n_query, const float *__restrict__ thr, int S,
                                                                    uint16_t *__restrict__ bucket) {
     __shared__ TileSmem sm;
+    __shared__ ThrSummary ts;
     const int64_t b0 = (int64_t) blockIdx.x * kTile;  // queries
     const int64_t a0 = (int64_t) blockIdx.y * kTile;  // users
+    load_thr_summary(ts, thr, n_user, a0, S);
     float lo[4][4], hi[4][4];
-    exact_tile(sm, user, nullptr, n_user, dim, a0, query, n_query, dim, b0, dim, dim, lo, hi);
+    exact_tile(sm, user, nullptr, n_user, dim, a0, query, n_query, dim, b0, 0, dim, dim, lo, hi);
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
 #pragma unroll
     for (int i = 0; i < 4; i++) {
@@ -52,30 +54,15 @@ __global__ void __launch_bounds__(kTileThreads) score_bucket_kernel(const float 
         for (int j = 0; j < 4; j++) {
             const int64_t q = b0 + 4 * ty + j;
             if (q >= n_query) continue;
-            bucket[q * n_user + u] = (uint16_t) bucket_of(row, S, lo[i][j]);
+            bucket[q * n_user + u] = (uint16_t) bucket_of_2level(ts.v[4 * tx + i], row, S, lo[i][j]);
         }
     }
 }
 
-// Per query: histogram of buckets, the k-th smallest bounds and the class of every bucket value
-// (PruneCandidateByBound.hpp:36-150 with n_result_user = 0 and no user excluded).  Both bounds are
-// non-decreasing functions of the bucket, so the k-th smallest lower bound and the k-th smallest
-// upper bound both sit at the k-th smallest bucket.
-__global__ void select_bucket_kernel(const uint16_t *__restrict__ bucket, int64_t n_user, int S,
-                                     const int32_t *__restrict__ rank, int n_item, int topk,
-                                     uint8_t *__restrict__ cls, QueryCounts *__restrict__ counts) {
-    extern __shared__ int hist[];  // S + 1
+__global__ void select_bucket_kernel(const int *__restrict__ hist_all, int S, const int32_t *__restrict__ rank,
+                                     int n_item, int topk, uint8_t *__restrict__ cls, QueryCounts *__restrict__ counts) {
     const int q = blockIdx.x;
-    for (int b = threadIdx.x; b <= S; b += blockDim.x) hist[b] = 0;
-    __syncthreads();
-    const uint16_t *row = bucket + (int64_t) q * n_user;
-    for (int64_t u = threadIdx.x; u < n_user; u += blockDim.x) {
-        const int v = row[u];
-        const unsigned act = __activemask();
-        const unsigned peers = __match_any_sync(act, v);
-        if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[v], __popc(peers));
-    }
-    __syncthreads();
+    const int *hist = hist_all + (int64_t) q * (S + 1);
     if (threadIdx.x == 0) {
         int bk = S;
         int64_t cum = 0;
@@ -123,54 +110,37 @@ __global__ void select_bucket_kernel(const uint16_t *__restrict__ bucket, int64_
     }
 }
 
-// Per query, in user-id order: the first n_res_emit result users and every candidate.
-__global__ void compact_kernel(const uint16_t *__restrict__ bucket, int64_t n_user, int S, const uint8_t *__restrict__ cls,
-                               const QueryCounts *__restrict__ counts, const int64_t *__restrict__ cand_off, int topk,
-                               int32_t *__restrict__ res_user, int32_t *__restrict__ cand_user,
-                               int32_t *__restrict__ cand_query, uint16_t *__restrict__ cand_bucket) {
-    extern __shared__ uint8_t cls_s[];  // S + 1
-    __shared__ int warp_tot[9];
-    const int q = blockIdx.x;
-    const QueryCounts c = counts[q];
-    for (int b = threadIdx.x; b <= S; b += blockDim.x) cls_s[b] = cls[(int64_t) q * (S + 1) + b];
-    __syncthreads();
-    const uint16_t *row = bucket + (int64_t) q * n_user;
-    const bool want_cand = c.n_cand > 0;
-    int nres = 0, ncand = 0;
-    int64_t coff = cand_off[q];
-    for (int64_t base = 0; base < n_user; base += 4 * blockDim.x) {
-        if (nres >= c.n_res_emit && (!want_cand || ncand >= c.n_cand)) break;
-        uint16_t bv[4];
-        uint8_t kv[4];
-        int mr = 0, mc = 0;
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            const int64_t u = base + 4 * threadIdx.x + e;
-            bv[e] = u < n_user ? row[u] : 0;
-            kv[e] = u < n_user ? cls_s[bv[e]] : kClsPrune;
-            mr += kv[e] == kClsResult;
-            mc += (kv[e] == kClsRefine) & want_cand;
-        }
-        int tot;
-        const int pre = block_excl_scan(mr | (mc << 16), warp_tot, &tot);
-        int pr = nres + (pre & 0xffff), pc = ncand + (pre >> 16);
-#pragma unroll
-        for (int e = 0; e < 4; e++) {
-            const int64_t u = base + 4 * threadIdx.x + e;
-            if (kv[e] == kClsResult) {
-                if (pr < c.n_res_emit) res_user[(int64_t) q * topk + pr] = (int32_t) u;
-                pr++;
-            } else if (kv[e] == kClsRefine && want_cand) {
-                cand_user[coff + pc] = (int32_t) u;
-                cand_query[coff + pc] = q;
-                cand_bucket[coff + pc] = bv[e];
-                pc++;
-            }
-        }
-        nres += tot & 0xffff;
-        ncand += tot >> 16;
+// QS / US classification of a pair for the ordered compaction: the class of its bucket.
+struct QsCompactPolicy {
+    struct Aux { uint16_t b; };
+    const uint16_t *bucket;
+    int64_t n_user;
+    const uint8_t *cls;
+    int S;
+    const QueryCounts *counts;
+    const int64_t *cand_off;
+    int topk;
+    int32_t *res_user, *cand_user, *cand_query;
+    uint16_t *cand_bucket;
+    __device__ bool query_active(int q) const { return true; }
+    __device__ int classify(int q, int64_t u, Aux &aux) const {
+        const uint16_t b = bucket[(int64_t) q * n_user + u];
+        aux.b = b;
+        const uint8_t k = __ldg(cls + (int64_t) q * (S + 1) + b);
+        if (k == kClsResult) return 1;
+        return (k == kClsRefine && counts[q].n_cand > 0) ? 2 : 0;
     }
-}
+    __device__ void emit_result(int q, int pos, int64_t u, const Aux &) const {
+        res_user[(int64_t) q * topk + pos] = (int32_t) u;
+    }
+    __device__ void emit_cand(int q, int pos, int64_t u, const Aux &aux) const {
+        if (pos >= counts[q].n_cand) return;  // the count pass disagrees; reported by compact_scan
+        const int64_t e = cand_off[q] + pos;
+        cand_user[e] = (int32_t) u;
+        cand_query[e] = q;
+        cand_bucket[e] = aux.b;
+    }
+};
 
 // ============================================================================================
 // refinement
@@ -270,7 +240,7 @@ __global__ void __launch_bounds__(kTileThreads) refine_tile_kernel(RefineArgs a,
         __syncthreads();
         if (b0 >= max_np) continue;
         float lo[4][4], hi[4][4];
-        exact_tile(sm, a.user, a.ref_user, n_ref, a.dim, a0, items, a.n_item, a.dim, b0, ks, a.dim, lo, hi);
+        exact_tile(sm, a.user, a.ref_user, n_ref, a.dim, a0, items, a.n_item, a.dim, b0, 0, ks, a.dim, lo, hi);
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             const int r = 4 * tx + i;
@@ -593,15 +563,28 @@ static int qs_chunk(rkr_index *ix, int method, const float *d_query, int nq, int
     uint16_t *bucket = ix->ws_bucket.as<uint16_t>();
     RKR_TRY(ix->ws_cls.ensure((size_t) nq * (S + 1)));
     RKR_TRY(ix->ws_counts.ensure(sizeof(QueryCounts) * (size_t) nq));
+    RKR_TRY(ix->ws_hist.ensure(sizeof(int) * (size_t) nq * (S + 1)));
     QueryCounts *counts = ix->ws_counts.as<QueryCounts>();
+    int *hist = ix->ws_hist.as<int>();
     {
         dim3 grid((unsigned) ((nq + kTile - 1) / kTile), (unsigned) ((U + kTile - 1) / kTile));
-        timed(ix, st, "score_bucket", [&] { score_bucket_kernel<<<grid, kTileThreads, 0, st>>>(ix->user.as<float>(), U, dim, d_query, nq,
-                                                          ix->thr.as<float>(), S, bucket); });
+        timed(ix, st, "score_bucket", [&] {
+            score_bucket_kernel<<<grid, kTileThreads, 0, st>>>(ix->user.as<float>(), U, dim, d_query, nq,
+                                                              ix->thr.as<float>(), S, bucket);
+        });
         RKR_CUDA(cudaGetLastError());
-        timed(ix, st, "select_bucket", [&] { select_bucket_kernel<<<nq, 256, (S + 1) * sizeof(int), st>>>(bucket, U, S, ix->sample_rank.as<int32_t>(),
-                                                                     (int) ix->n_item, topk, ix->ws_cls.as<uint8_t>(),
-                                                                     counts); });
+        RKR_CUDA(cudaMemsetAsync(hist, 0, sizeof(int) * (size_t) nq * (S + 1), st));
+        const int64_t chunk = 16384;
+        dim3 hg((unsigned) ((U + chunk - 1) / chunk), (unsigned) nq);
+        timed(ix, st, "bucket_hist", [&] {
+            bucket_hist_kernel<<<hg, kHistThreads, hist_copies(S + 1) * (S + 1) * sizeof(int), st>>>(bucket, U, S + 1,
+                                                                                                  chunk, hist);
+        });
+        RKR_CUDA(cudaGetLastError());
+        timed(ix, st, "select_bucket", [&] {
+            select_bucket_kernel<<<nq, 32, 0, st>>>(hist, S, ix->sample_rank.as<int32_t>(), (int) ix->n_item, topk,
+                                                   ix->ws_cls.as<uint8_t>(), counts);
+        });
         RKR_CUDA(cudaGetLastError());
     }
     std::vector<QueryCounts> hc(nq);
@@ -624,20 +607,33 @@ static int qs_chunk(rkr_index *ix, int method, const float *d_query, int nq, int
     int32_t *cand_ub = carve<int32_t>(p, n_cand);
     uint16_t *cand_bucket = carve<uint16_t>(p, n_cand);
     RKR_CUDA(cudaMemcpyAsync(d_off, off.data(), sizeof(int64_t) * (nq + 1), cudaMemcpyHostToDevice, st));
-    timed(ix, st, "compact", [&] { compact_kernel<<<nq, 256, S + 1, st>>>(bucket, U, S, ix->ws_cls.as<uint8_t>(), counts, d_off, topk, res_user,
-                                           cand_user, cand_query, cand_bucket); });
-    RKR_CUDA(cudaGetLastError());
-    timed(ix, st, "result_fill", [&] { result_fill_kernel<<<nq, 128, 0, st>>>(counts, res_user, bucket, U, ix->user.as<float>(), d_query, dim, S,
-                                            ix->sample_rank.as<int32_t>(), (int) ix->n_item, topk, res_rank, res_qip); });
+    QsCompactPolicy pol;
+    pol.bucket = bucket;
+    pol.n_user = U;
+    pol.cls = ix->ws_cls.as<uint8_t>();
+    pol.S = S;
+    pol.counts = counts;
+    pol.cand_off = d_off;
+    pol.topk = topk;
+    pol.res_user = res_user;
+    pol.cand_user = cand_user;
+    pol.cand_query = cand_query;
+    pol.cand_bucket = cand_bucket;
+    RKR_TRY(run_compaction(ix, pol, nq, topk, counts, st));
+    timed(ix, st, "result_fill", [&] {
+        result_fill_kernel<<<nq, 128, 0, st>>>(counts, res_user, bucket, U, ix->user.as<float>(), d_query, dim, S,
+                                               ix->sample_rank.as<int32_t>(), (int) ix->n_item, topk, res_rank, res_qip);
+    });
     RKR_CUDA(cudaGetLastError());
     if (n_cand > 0) {
-        timed(ix, st, "cand_bounds", [&] { cand_bounds_kernel<<<(unsigned) ((n_cand + 255) / 256), 256, 0, st>>>(
-            cand_bucket, n_cand, S, ix->sample_rank.as<int32_t>(), (int) ix->n_item, cand_lb, cand_ub); });
+        timed(ix, st, "cand_bounds", [&] {
+            cand_bounds_kernel<<<(unsigned) ((n_cand + 255) / 256), 256, 0, st>>>(
+                cand_bucket, n_cand, S, ix->sample_rank.as<int32_t>(), (int) ix->n_item, cand_lb, cand_ub);
+        });
         RKR_CUDA(cudaGetLastError());
     }
     RKR_TRY(refine_and_assemble(ix, method, d_query, nq, topk, counts, hc, res_user, res_rank, res_qip, n_cand,
                                 cand_user, cand_query, cand_lb, cand_ub, nullptr, d_off, d_out, d_stats, st));
-    // keep the host vector alive until the stream passes the copies
     RKR_CUDA(cudaStreamSynchronize(st));
     return RKR_OK;
 }

@@ -41,14 +41,16 @@ typedef struct {
     float query_ip;
 } rkr_user_rank;
 
-/* Per-query counters: the reference's SingleQueryPerformance fields (src/include/util/FileIO.hpp:255-277)
- * plus the candidate count and the number of items examined during refinement. */
+/* Per-query counters: the reference's SingleQueryPerformance fields (src/include/util/FileIO.hpp:255-277:
+ * n_prune_user, n_result_user, n_refine_user, ip_cost), the number of refinement candidates and
+ * the number of items refinement examined (the reference's n_compute_item). */
 typedef struct {
     int32_t n_prune;
     int32_t n_result;
     int32_t n_refine;
     int32_t n_candidate;
     int64_t n_compute_item;
+    int64_t ip_cost;
 } rkr_query_stats;
 
 typedef struct rkr_index rkr_index;

@@ -120,7 +120,7 @@ void write_regression_index(const std::string &dir, const char *ds, int64_t n_us
 }
 
 struct RefUserRank { int32_t user_id, rank; float query_ip; };
-struct RefStats { int32_t n_prune, n_result, n_refine, n_candidate; int64_t n_compute_item; };
+struct RefStats { int32_t n_prune, n_result, n_refine, n_candidate; int64_t n_compute_item, ip_cost; };
 
 void copy_results(const std::vector<std::vector<UserRankElement>> &res, const std::vector<SingleQueryPerformance> &perf,
                   int32_t topk, RefUserRank *out, RefStats *st) {
@@ -136,6 +136,7 @@ void copy_results(const std::vector<std::vector<UserRankElement>> &res, const st
             st[q].n_refine = perf[q].n_refine_user_;
             st[q].n_candidate = 0;
             st[q].n_compute_item = 0;
+            st[q].ip_cost = (int64_t) perf[q].ip_cost_;
         }
     }
 }

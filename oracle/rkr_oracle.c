@@ -557,7 +557,8 @@ static void refine_free(refine_t *r) {
 
 /* RefineCPUIPBound::RefineRank, RefineCPUIPBound.hpp:93-150 (with RefineCPUPartDimPartNorm's
  * IPBoundNoParallel :83-107 and ComputeRemainDimNoParallel :131-152). */
-static int32_t refine_rank_ipbound(const refine_t *r, float qip, int64_t uid, int64_t *n_compute_item) {
+static int32_t refine_rank_ipbound(const refine_t *r, float qip, int64_t uid, int64_t *n_compute_item,
+                                   int64_t *ip_cost) {
     const float lowq = qip - 8e-3f, highq = qip + 8e-3f;
     int64_t lo = 0, len = r->n_item; /* lower_bound(norms, lowq, arr > q) */
     while (len > 0) { int64_t h = len >> 1, m = lo + h; if (r->item_norm[m] > lowq) { lo = m + 1; len -= h + 1; } else len = h; }
@@ -567,6 +568,7 @@ static int32_t refine_rank_ipbound(const refine_t *r, float qip, int64_t uid, in
     const float *uv = r->user + uid * d;
     const float unorm = r->user_rnorm[uid];
     int32_t rank = 0;
+    int64_t cost = (int) (n_proc * 1.0 * (c + 1) / (int) d);  /* RefineCPUIPBound.hpp:491 */
     for (int64_t i = 0; i < n_proc; i++) {
         const float *iv = r->item_sorted + i * d;
         const float left = ip_f32(uv, iv, c);
@@ -575,8 +577,10 @@ static int32_t refine_rank_ipbound(const refine_t *r, float qip, int64_t uid, in
         if (lowq > ubv) continue;
         if (highq < lbv) { rank++; continue; }
         const float ip = left + ip_f32(uv + c, iv + c, d - c);
+        cost++;  /* RefineCPUIPBound.hpp:518 */
         if (ip >= qip) rank++;
     }
+    if (ip_cost) *ip_cost = cost;
     return rank;
 }
 
@@ -594,7 +598,7 @@ static int cmp_user_rank(const void *a, const void *b) { /* UserRankElement::ope
     return (x->user_id > y->user_id) - (x->user_id < y->user_id);
 }
 
-typedef struct { int32_t n_prune, n_result, n_refine, n_candidate; int64_t n_compute_item; } orc_query_stats;
+typedef struct { int32_t n_prune, n_result, n_refine, n_candidate; int64_t n_compute_item, ip_cost; } orc_query_stats;
 
 /* ComputeAllIPBound::GetRank (ComputeAllIPBound.hpp:57-137) and ComputeAll::GetRank
  * (ComputeAll.hpp:54-125), then the result assembly of QS.hpp:185-198 / QSRPNormalLP.hpp:213-226 /
@@ -605,7 +609,7 @@ static void refine_and_assemble(const refine_t *rf, int use_ipbound, const float
                                 orc_user_rank *out, orc_query_stats *st) {
     const int32_t n_remain = topk - n_result > 0 ? topk - n_result : 0;
     int32_t n_refine = 0, n_cand = 0;
-    int64_t n_compute = 0;
+    int64_t n_compute = 0, refine_ip_cost = 0;
     if (n_remain != 0) {
         for (int64_t u = 0; u < n_user; u++) {
             if (prune[u] || result[u]) continue;
@@ -614,12 +618,14 @@ static void refine_and_assemble(const refine_t *rf, int use_ipbound, const float
             else {
                 n_refine++;
                 if (use_ipbound) {
-                    int64_t nc = 0;
-                    rank = refine_rank_ipbound(rf, qip[u], u, &nc);
+                    int64_t nc = 0, ic = 0;
+                    rank = refine_rank_ipbound(rf, qip[u], u, &nc, &ic);
                     n_compute += nc;
+                    refine_ip_cost += ic;
                 } else {
                     rank = refine_rank_all(rf->user + u * rf->d, item, rf->n_item, rf->d, qip[u]);
                     n_compute += rf->n_item;
+                    refine_ip_cost += rf->n_item;  /* ComputeAll.hpp:112-116 */
                 }
             }
             cache[n_cand].user_id = (int32_t) u; cache[n_cand].rank = rank; cache[n_cand].query_ip = qip[u];
@@ -633,7 +639,7 @@ static void refine_and_assemble(const refine_t *rf, int use_ipbound, const float
         if (nc == topk) break;
     }
     for (int c = nc; c < topk; c++) out[c] = cache[c - nc];
-    if (st) { st->n_refine = n_refine; st->n_candidate = n_cand; st->n_compute_item = n_compute; }
+    if (st) { st->n_refine = n_refine; st->n_candidate = n_cand; st->n_compute_item = n_compute; st->ip_cost = refine_ip_cost; }
 }
 
 /* QS::Index::Retrieval, src/impl/QS.hpp:106-230.
@@ -663,6 +669,7 @@ int orc_qs_retrieval(const float *user, int64_t n_user, const float *item, int64
         refine_and_assemble(&rf, 1, item, qip, lb, ub, prune, result, n_user, topk, n_result, cache,
                             out + (int64_t) q * topk, &s);
         s.n_prune = n_prune; s.n_result = n_result;
+        s.ip_cost += n_user;  /* QS.hpp:146, 221 */
         if (st) st[q] = s;
     }
     free(qip); free(lb); free(ub); free(prune); free(result); free(cache);
@@ -698,6 +705,7 @@ int orc_us_retrieval(const float *user, int64_t n_user, const float *item, int64
         refine_and_assemble(&rf, 0, item, qip, lb, ub, prune, result, n_user, topk, n_result, cache,
                             out + (int64_t) q * topk, &s);
         s.n_prune = n_prune; s.n_result = n_result;
+        s.ip_cost += n_user;  /* US.hpp:134, 188 */
         if (st) st[q] = s;
     }
     free(qip); free(lb); free(ub); free(prune); free(result); free(cache);
@@ -743,6 +751,7 @@ int orc_qsrp_retrieval(const float *user, const float *svd_user, const float *tr
         }
         int32_t refine_size = (int32_t) n_user, n_result = 0, n_prune = 0;
         orc_prune_candidate_by_bound(lb, ub, n_user, topk, &refine_size, &n_result, &n_prune, prune, result);
+        const int32_t ip_cost = refine_size;                                                 /* QSRPNormalLP.hpp:177 */
         for (int64_t u = 0; u < n_user; u++) {                                               /* ComputeRemainDim :76-95 */
             if (prune[u] || result[u]) continue;
             qip_state[u] = left[u] + ip_f32(svd_user + u * d + c, qtr + c, rd);
@@ -756,6 +765,7 @@ int orc_qsrp_retrieval(const float *user, const float *svd_user, const float *tr
         refine_and_assemble(&rf, 1, item, qip_state, lb, ub, prune, result, n_user, topk, n_result, cache,
                             out + (int64_t) q * topk, &s);
         s.n_prune = n_prune; s.n_result = n_result;
+        s.ip_cost += ip_cost;
         if (st) st[q] = s;
     }
     free(unorm); free(left); free(qtr); free(lb); free(ub); free(prune); free(result); free(cache);

@@ -269,6 +269,8 @@ struct QueryCounts {
     int32_t mode;            // 0: normal, 1: k-th bounds equal, 2: refinement skipped
     int32_t bk;              // bucket of the k-th smallest bound
     int32_t lstar, ustar;    // k-th smallest lower / upper rank bound
+    int32_t ip_base;         // the reference's ip_cost before refinement (QS/US: n_user; QSRP: round-2 users)
+    int32_t pad;
 };
 
 // Pair classes produced by the pruning step (PruneCandidateByBound.hpp:83-150).

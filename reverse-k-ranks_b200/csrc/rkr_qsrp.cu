@@ -62,6 +62,40 @@ struct RegModel {           // device view of the regression index
     int n_item;
 };
 
+// The same CDF with every step in binary32 and expf: within 1e-6 of cdf_phi for every input
+// (the two differ only in where the last bits of t, the product and the closing sum are rounded).
+__device__ __forceinline__ float cdf_phi_f32(float x) {
+    const float a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f;
+    const float a4 = -1.453152027f, a5 = 1.061405429f, p = 0.3275911f;
+    const float sign = x < 0 ? -1.0f : 1.0f;
+    x = __fdiv_rn(fabsf(x), __int_as_float(0x3fb504f3));
+    const float t = __fdiv_rn(1.0f, __fadd_rn(1.0f, __fmul_rn(p, x)));
+    const float pt = (((((a5 * t + a4) * t) + a3) * t + a2) * t + a1) * t;
+    const float y = 1.0f - pt * expf(-x * x);
+    return 0.5f * (1.0f + sign * y);
+}
+
+// The reference's float/double evaluation of one side of ComputeRankBound's index arithmetic
+// (kept out of line: the float screen below rarely needs it).
+__device__ __noinline__ int64_t regression_index_exact(float nx, float a, float b, float err, bool upper) {
+    const float ix = cdf_phi(nx);
+    const float pred = __fadd_rn(__fmul_rn(ix, a), b);
+    return upper ? f2i64_x86(floorf(__fsub_rn(pred, err))) : f2i64_x86(ceilf(__fadd_rn(pred, err)));
+}
+
+// One side of ComputeRankBound's index arithmetic: pr = ceil(pred + err) (upper = 0) or
+// floor(pred - err) (upper = 1), pred = cdf(nx) * a + b.  The float-only CDF decides it whenever
+// pred -+ err lies farther from an integer than that CDF's error can move it (|a| * 4e-6 plus a
+// few ulps of the sum); otherwise the reference's own float/double evaluation decides.
+__device__ __forceinline__ int64_t regression_index(float nx, float a, float b, float err, bool upper) {
+    const float ixf = cdf_phi_f32(nx);
+    const float vf = upper ? __fsub_rn(__fadd_rn(__fmul_rn(ixf, a), b), err) : __fadd_rn(__fadd_rn(__fmul_rn(ixf, a), b), err);
+    const float margin = fabsf(a) * 4e-6f + 8.0f * fabsf(vf) * 1.2e-7f + 1e-6f;
+    const float r = rintf(vf);
+    if (isfinite(vf) && fabsf(vf - r) > margin) return (int64_t) (upper ? floorf(vf) : ceilf(vf));
+    return regression_index_exact(nx, a, b, err, upper);
+}
+
 // ComputeRankBound (:326-380), returning levels: 0 -> rank 0, j + 1 -> rank[j], S + 1 -> n_item.
 __device__ __forceinline__ void regression_levels(const RegModel &m, int64_t u, float qlb, float qub, int &lvl_lb,
                                                   int &lvl_ub) {
@@ -73,18 +107,14 @@ __device__ __forceinline__ void regression_levels(const RegModel &m, int64_t u, 
     else if (qlb < smin) lvl_lb = S + 1;
     else if ((double) err >= m.err_cap) lvl_lb = S + 1;
     else {
-        const float ix = cdf_phi(__fdiv_rn(__fsub_rn(qlb, mu), sigma));
-        const float pred = __fadd_rn(__fmul_rn(ix, a), b);
-        const int64_t pr = f2i64_x86(ceilf(__fadd_rn(pred, err)));
+        const int64_t pr = regression_index(__fdiv_rn(__fsub_rn(qlb, mu), sigma), a, b, err, false);
         lvl_lb = pr >= S ? S + 1 : (pr < 0 ? 1 : (int) pr + 1);
     }
     if (qub > smax) lvl_ub = 0;
     else if (qub < smin) lvl_ub = S;
     else if ((double) err >= m.err_cap) lvl_ub = 0;
     else {
-        const float ix = cdf_phi(__fdiv_rn(__fsub_rn(qub, mu), sigma));
-        const float pred = __fadd_rn(__fmul_rn(ix, a), b);
-        const int64_t pr = f2i64_x86(floorf(__fsub_rn(pred, err)));
+        const int64_t pr = regression_index(__fdiv_rn(__fsub_rn(qub, mu), sigma), a, b, err, true);
         lvl_ub = pr >= S ? S + 1 : (pr < 0 ? 0 : (int) pr + 1);
     }
 }
@@ -291,22 +321,25 @@ __device__ __forceinline__ bool eligible2(const QsrpParams &p, uint32_t v, const
 // Round 2: full SVD-space score of each surviving pair, left (round 1) + the remaining dims
 // (ComputeRemainDim, PartDimPartNorm.hpp:76-95), and its sampled-threshold bucket.  Pairs that did
 // not reach round 2 get a state code instead: kStateResult1 (accepted in round 1) or kStatePruned1.
-__global__ void __launch_bounds__(kTileThreads) qsrp_round2_kernel(const float *__restrict__ svd_user, int64_t n_user,
+__global__ void __launch_bounds__(kTileThreads, 3) qsrp_round2_kernel(const float *__restrict__ svd_user, int64_t n_user,
                                                                   int dim, const float *__restrict__ qtr, int n_query,
                                                                   int check_dim, const uint32_t *__restrict__ lv,
                                                                   const float *__restrict__ left,
                                                                   const QsrpParams *__restrict__ par,
-                                                                  const int32_t *__restrict__ reg_rank, int S_reg,
+                                                                  const int32_t *reg_rank, int S_reg,
                                                                   int n_item, const float *__restrict__ thr, int S,
                                                                   uint16_t *__restrict__ bucket2) {
     __shared__ TileSmem sm;
     __shared__ ThrSummary ts;
     __shared__ QsrpParams par_s[kTile];
+    extern __shared__ int32_t rank_s[];  // the regression model's sample ranks
     const int64_t b0 = (int64_t) blockIdx.x * kTile;
     const int64_t a0 = (int64_t) blockIdx.y * kTile;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     if (threadIdx.x < kTile && b0 + threadIdx.x < n_query) par_s[threadIdx.x] = par[b0 + threadIdx.x];
+    for (int i = threadIdx.x; i < S_reg; i += blockDim.x) rank_s[i] = reg_rank[i];
     __syncthreads();
+    reg_rank = rank_s;
     uint32_t el = 0, r1 = 0;  // bit 4*i + j: reached round 2 / accepted in round 1
 #pragma unroll
     for (int i = 0; i < 4; i++)
@@ -361,6 +394,7 @@ __global__ void qsrp_select2_kernel(const int *__restrict__ hist_all, int S, con
         c.n_prune = p.n_pr1;
         c.n_cand = 0;
         c.mode = 2;
+        c.ip_base = p.n_ref1;
         counts[q] = c;
         return;
     }
@@ -387,6 +421,7 @@ __global__ void qsrp_select2_kernel(const int *__restrict__ hist_all, int S, con
     p.L2 = L; p.U2 = U; p.n_elig2 = (int) n_el;
     QueryCounts c = {};
     c.lstar = L; c.ustar = U;
+    c.ip_base = p.n_ref1;  // QSRPNormalLP.hpp:177: refine_user_size after the first prune
     if (L == U) {
         p.mode2 = 1;
         c.mode = 1;
@@ -599,7 +634,7 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     timed(ix, st, "qsrp_final1", [&] { qsrp_final1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, topk); });
     RKR_CUDA(cudaGetLastError());
     timed(ix, st, "qsrp_round2", [&] {
-        qsrp_round2_kernel<<<grid, kTileThreads, 0, st>>>(ix->svd_user.as<float>(), U, dim, qtr, nq, c, lv, left, par,
+        qsrp_round2_kernel<<<grid, kTileThreads, Sr * sizeof(int32_t), st>>>(ix->svd_user.as<float>(), U, dim, qtr, nq, c, lv, left, par,
                                                          m.rank, Sr, n_item, ix->thr.as<float>(), S, b2);
     });
     RKR_CUDA(cudaGetLastError());

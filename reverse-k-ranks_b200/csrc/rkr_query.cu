@@ -60,7 +60,8 @@ __global__ void __launch_bounds__(kTileThreads) score_bucket_kernel(const float 
 }
 
 __global__ void select_bucket_kernel(const int *__restrict__ hist_all, int S, const int32_t *__restrict__ rank,
-                                     int n_item, int topk, uint8_t *__restrict__ cls, QueryCounts *__restrict__ counts) {
+                                     int n_item, int topk, int n_user, uint8_t *__restrict__ cls,
+                                     QueryCounts *__restrict__ counts) {
     const int q = blockIdx.x;
     const int *hist = hist_all + (int64_t) q * (S + 1);
     if (threadIdx.x == 0) {
@@ -72,8 +73,9 @@ __global__ void select_bucket_kernel(const int *__restrict__ hist_all, int S, co
         }
         int L, U;
         bucket_bounds(bk, S, rank, n_item, L, U);
-        QueryCounts c;
+        QueryCounts c = {};
         c.bk = bk; c.lstar = L; c.ustar = U;
+        c.ip_base = n_user;
         uint8_t *cq = cls + (int64_t) q * (S + 1);
         if (L == U) {
             int64_t nres = 0;
@@ -165,6 +167,7 @@ struct RefineArgs {
     int32_t *ref_idx;         // refined candidates (compacted)
     int32_t *ref_user;        // their users
     int32_t *n_ref;           // device counter
+    int32_t *undecided;       // [n_cand] items whose score had to be computed in full
 };
 
 // Score of each candidate and its rank when the bounds agree (ComputeAllIPBound.hpp:319-341;
@@ -182,6 +185,7 @@ __global__ void refine_prep_kernel(RefineArgs a) {
     if (lb == ub) {
         a.rank[e] = lb;
         a.nproc[e] = 0;
+        a.undecided[e] = 0;
         return;
     }
     int np = (int) a.n_item;
@@ -196,6 +200,7 @@ __global__ void refine_prep_kernel(RefineArgs a) {
     }
     a.rank[e] = 0;
     a.nproc[e] = np;
+    a.undecided[e] = 0;
     const int slot = atomicAdd(a.n_ref, 1);
     a.ref_idx[slot] = (int32_t) e;
     a.ref_user[slot] = u;
@@ -211,7 +216,7 @@ __global__ void __launch_bounds__(kTileThreads) refine_tile_kernel(RefineArgs a,
     __shared__ TileSmem sm;
     __shared__ int nproc_s[kTile];
     __shared__ float qip_s[kTile], urn_s[kTile];
-    __shared__ int cnt_s[kTile];
+    __shared__ int cnt_s[kTile], und_s[kTile];
     __shared__ int max_np;
     const int n_ref = *a.n_ref;
     const int64_t b0 = (int64_t) blockIdx.x * kTile;  // items
@@ -235,6 +240,7 @@ __global__ void __launch_bounds__(kTileThreads) refine_tile_kernel(RefineArgs a,
             qip_s[threadIdx.x] = qv;
             urn_s[threadIdx.x] = un;
             cnt_s[threadIdx.x] = 0;
+            und_s[threadIdx.x] = 0;
             atomicMax(&max_np, np);
         }
         __syncthreads();
@@ -246,7 +252,7 @@ __global__ void __launch_bounds__(kTileThreads) refine_tile_kernel(RefineArgs a,
             const int r = 4 * tx + i;
             const float qv = qip_s[r];
             const int np = nproc_s[r];
-            int c = 0;
+            int c = 0, und = 0;
 #pragma unroll
             for (int j = 0; j < 4; j++) {
                 const int64_t it = b0 + 4 * ty + j;
@@ -257,16 +263,20 @@ __global__ void __launch_bounds__(kTileThreads) refine_tile_kernel(RefineArgs a,
                     const float lbv = __fsub_rn(lo[i][j], right), ubv = __fadd_rn(lo[i][j], right);
                     if (lowq > ubv) continue;
                     if (highq < lbv) { c++; continue; }
+                    und++;
                     c += __fadd_rn(lo[i][j], hi[i][j]) >= qv;
                 } else {
                     c += lo[i][j] > qv;
                 }
             }
             if (c) atomicAdd(&cnt_s[r], c);
+            if (und) atomicAdd(&und_s[r], und);
         }
         __syncthreads();
-        if (threadIdx.x < kTile && a0 + threadIdx.x < n_ref && cnt_s[threadIdx.x])
-            atomicAdd(a.rank + a.ref_idx[a0 + threadIdx.x], cnt_s[threadIdx.x]);
+        if (threadIdx.x < kTile && a0 + threadIdx.x < n_ref) {
+            if (cnt_s[threadIdx.x]) atomicAdd(a.rank + a.ref_idx[a0 + threadIdx.x], cnt_s[threadIdx.x]);
+            if (und_s[threadIdx.x]) atomicAdd(a.undecided + a.ref_idx[a0 + threadIdx.x], und_s[threadIdx.x]);
+        }
     }
 }
 
@@ -286,8 +296,10 @@ struct AssembleArgs {
     const int32_t *cand_rank;
     const float *cand_qip;
     const int32_t *cand_nproc;
+    const int32_t *cand_undecided;
     const int32_t *cand_lb, *cand_ub;
     int topk;
+    int ipbound, dim, check_dim;
     rkr_user_rank *out;          // [n_query][topk]
     rkr_query_stats *stats;      // [n_query] or nullptr
     uint64_t *scratch;           // keys for candidates beyond kSortCap (indexed by candidate)
@@ -303,7 +315,7 @@ __device__ __forceinline__ uint64_t cand_key(int rank, int user) {
 __global__ void assemble_kernel(AssembleArgs a) {
     __shared__ uint64_t keys[kSortCap];
     __shared__ int n_refined, warp_tot[9];
-    __shared__ int64_t n_items;
+    __shared__ int64_t n_items, ip_refine;
     __shared__ uint64_t thresh;
     const int q = blockIdx.x;
     const QueryCounts c = a.counts[q];
@@ -319,12 +331,17 @@ __global__ void assemble_kernel(AssembleArgs a) {
     const int64_t off = a.cand_off[q];
     const int nc = c.n_cand;
     const int m = min(topk - nres, nc);
-    if (threadIdx.x == 0) { n_refined = 0; n_items = 0; }
+    if (threadIdx.x == 0) { n_refined = 0; n_items = 0; ip_refine = 0; }
     __syncthreads();
     for (int e = threadIdx.x; e < nc; e += blockDim.x) {
         if (a.cand_lb[off + e] != a.cand_ub[off + e]) {
+            const int np = a.cand_nproc[off + e];
             atomicAdd(&n_refined, 1);
-            atomicAdd((unsigned long long *) &n_items, (unsigned long long) a.cand_nproc[off + e]);
+            atomicAdd((unsigned long long *) &n_items, (unsigned long long) np);
+            // RefineCPUIPBound.hpp:491,518 (bound pass plus items scored in full); ComputeAll.hpp:112-116
+            const int64_t cost = a.ipbound ? (int64_t) (int) (np * 1.0 * (a.check_dim + 1) / a.dim) + a.cand_undecided[off + e]
+                                           : (int64_t) np;
+            atomicAdd((unsigned long long *) &ip_refine, (unsigned long long) cost);
         }
     }
     if (m > 0) {
@@ -432,6 +449,7 @@ __global__ void assemble_kernel(AssembleArgs a) {
         s.n_refine = n_refined;
         s.n_candidate = nc;
         s.n_compute_item = n_items;
+        s.ip_cost = (int64_t) c.ip_base + ip_refine;
         a.stats[q] = s;
     }
 }
@@ -492,7 +510,7 @@ static int refine_and_assemble(rkr_index *ix, int method, const float *d_query, 
                                int32_t *d_cand_ub, const float *d_cand_qip_given, const int64_t *d_cand_off,
                                rkr_user_rank *d_out, rkr_query_stats *d_stats, cudaStream_t st) {
     const bool ipbound = method != RKR_METHOD_US;
-    size_t need = carve_size(n_cand, 4) * 6 + carve_size(1, 4);
+    size_t need = carve_size(n_cand, 4) * 7 + carve_size(1, 4);
     RKR_TRY(ix->ws_refine.ensure(need));
     uint8_t *p = ix->ws_refine.as<uint8_t>();
     float *qip = carve<float>(p, n_cand);
@@ -500,6 +518,7 @@ static int refine_and_assemble(rkr_index *ix, int method, const float *d_query, 
     int32_t *nproc = carve<int32_t>(p, n_cand);
     int32_t *ref_idx = carve<int32_t>(p, n_cand);
     int32_t *ref_user = carve<int32_t>(p, n_cand);
+    int32_t *undecided = carve<int32_t>(p, n_cand);
     int32_t *n_ref = carve<int32_t>(p, 1);
     RKR_CUDA(cudaMemsetAsync(n_ref, 0, sizeof(int32_t), st));
     if (n_cand > 0) {
@@ -522,6 +541,7 @@ static int refine_and_assemble(rkr_index *ix, int method, const float *d_query, 
         ra.ref_idx = ref_idx;
         ra.ref_user = ref_user;
         ra.n_ref = n_ref;
+        ra.undecided = undecided;
         timed(ix, st, "refine_prep", [&] { refine_prep_kernel<<<(unsigned) ((n_cand + 255) / 256), 256, 0, st>>>(ra); });
         RKR_CUDA(cudaGetLastError());
         const float *items = ipbound ? ix->item_sorted.as<float>() : ix->item.as<float>();
@@ -541,6 +561,10 @@ static int refine_and_assemble(rkr_index *ix, int method, const float *d_query, 
     aa.cand_rank = rank;
     aa.cand_qip = qip;
     aa.cand_nproc = nproc;
+    aa.cand_undecided = undecided;
+    aa.ipbound = ipbound ? 1 : 0;
+    aa.dim = ix->dim;
+    aa.check_dim = ix->check_dim;
     aa.cand_lb = d_cand_lb;
     aa.cand_ub = d_cand_ub;
     aa.topk = topk;
@@ -583,7 +607,7 @@ static int qs_chunk(rkr_index *ix, int method, const float *d_query, int nq, int
         RKR_CUDA(cudaGetLastError());
         timed(ix, st, "select_bucket", [&] {
             select_bucket_kernel<<<nq, 32, 0, st>>>(hist, S, ix->sample_rank.as<int32_t>(), (int) ix->n_item, topk,
-                                                   ix->ws_cls.as<uint8_t>(), counts);
+                                                   (int) U, ix->ws_cls.as<uint8_t>(), counts);
         });
         RKR_CUDA(cudaGetLastError());
     }

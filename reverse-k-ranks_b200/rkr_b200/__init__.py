@@ -24,7 +24,7 @@ LIB_PATH = os.environ.get("RKR_B200_LIB", os.path.join(os.path.dirname(_HERE), "
 
 USER_RANK = np.dtype([("user_id", np.int32), ("rank", np.int32), ("query_ip", np.float32)])
 QUERY_STATS = np.dtype([("n_prune", np.int32), ("n_result", np.int32), ("n_refine", np.int32),
-                        ("n_candidate", np.int32), ("n_compute_item", np.int64)])
+                        ("n_candidate", np.int32), ("n_compute_item", np.int64), ("ip_cost", np.int64)])
 
 METHODS = {"QS": 0, "QSRPNormalLP": 1, "US": 2}
 

@@ -22,7 +22,7 @@ REF_SO = os.path.join(ORACLE_DIR, "_ref", "librkr_ref.so")
 
 USER_RANK = np.dtype([("user_id", np.int32), ("rank", np.int32), ("query_ip", np.float32)])
 STATS = np.dtype([("n_prune", np.int32), ("n_result", np.int32), ("n_refine", np.int32),
-                  ("n_candidate", np.int32), ("n_compute_item", np.int64)])
+                  ("n_candidate", np.int32), ("n_compute_item", np.int64), ("ip_cost", np.int64)])
 
 
 def _p(a):

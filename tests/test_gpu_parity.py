@@ -55,6 +55,7 @@ def test_qs_matches_golden(case):
     assert np.array_equal(st["n_refine"], g["qs_stats"]["n_refine"])
     assert np.array_equal(st["n_prune"], g["qs_stats"]["n_prune"])
     assert np.array_equal(st["n_result"], g["qs_stats"]["n_result"])
+    assert np.array_equal(st["ip_cost"], g["qs_stats"]["ip_cost"])
 
 
 @pytest.mark.parametrize("case", ["small", "fakenormal"])
@@ -67,6 +68,7 @@ def test_qsrp_matches_golden(case):
     assert same(out, g["qsrp"]), first_diff(out, g["qsrp"])
     assert np.array_equal(st["n_result"], g["qsrp_stats"]["n_result"])
     assert np.array_equal(st["n_prune"], g["qsrp_stats"]["n_prune"])
+    assert np.array_equal(st["ip_cost"], g["qsrp_stats"]["ip_cost"])
 
 
 @pytest.mark.parametrize("case", ["small", "fakenormal"])
@@ -75,8 +77,10 @@ def test_us_matches_golden(case):
     q100 = np.concatenate([g["query"]] * (100 // g["query"].shape[0] + 1))[:100]
     with rkr_b200.Index(g["user_norm"], g["item"]) as ix:
         ix.load_sample_search(g["uni_rank"], g["thr_uni"])
-        out = ix.retrieval("US", q100, int(g["topk"]))
+        out, st = ix.retrieval("US", q100, int(g["topk"]), stats=True)
     assert same(out, g["us"]), first_diff(out, g["us"])
+    assert np.array_equal(st["ip_cost"], g["us_stats"]["ip_cost"])
+    assert np.array_equal(st["n_refine"], g["us_stats"]["n_refine"])
 
 
 @pytest.mark.parametrize("case", ["small", "fakenormal"])
@@ -119,12 +123,16 @@ def test_random_qs_qsrp_us_match_oracle(shape, orc):
         ix.load_regression(rank, reg)
         state = np.zeros(n_user, np.float32)
         for k in (1, 10, 57):
-            a = ix.retrieval("QS", query, k)
-            b, _ = orc.qs_retrieval(un, item, cd, rank, thr, query, k)
+            a, sa = ix.retrieval("QS", query, k, stats=True)
+            b, sb = orc.qs_retrieval(un, item, cd, rank, thr, query, k)
             assert same(a, b), ("QS", k, first_diff(a, b))
-            a = ix.retrieval("QSRPNormalLP", query, k)
-            b, _ = orc.qsrp_retrieval(un, su, ti, item, cd, rank, thr, rank, reg, query, k, qip_state=state)
+            for f in ("n_prune", "n_result", "n_refine", "ip_cost", "n_compute_item"):
+                assert np.array_equal(sa[f], sb[f]), ("QS", k, f)
+            a, sa = ix.retrieval("QSRPNormalLP", query, k, stats=True)
+            b, sb = orc.qsrp_retrieval(un, su, ti, item, cd, rank, thr, rank, reg, query, k, qip_state=state)
             assert same(a, b), ("QSRP", k, first_diff(a, b))
+            for f in ("n_prune", "n_result", "n_refine", "ip_cost", "n_compute_item"):
+                assert np.array_equal(sa[f], sb[f]), ("QSRP", k, f)
         q100 = np.concatenate([query] * 2)[:100]
         a = ix.retrieval("US", q100, 10)
         b, _ = orc.us_retrieval(un, item, rank, thr, q100, 10)

@@ -66,13 +66,16 @@ def test_query_methods_match_golden(orc, case):
     assert same_results(qs, g["qs"])
     assert np.array_equal(st["n_refine"], g["qs_stats"]["n_refine"])
     assert np.array_equal(st["n_prune"], g["qs_stats"]["n_prune"])
+    assert np.array_equal(st["ip_cost"], g["qs_stats"]["ip_cost"])
     qsrp, st = orc.qsrp_retrieval(g["user_norm"], g["svd_user"], g["transfer_item"], g["item"], int(g["check_dim"]),
                                   g["opt_rank"], g["thr"], g["opt_rank"], g["reg"], g["query"], k)
     assert same_results(qsrp, g["qsrp"])
     assert np.array_equal(st["n_result"], g["qsrp_stats"]["n_result"])
+    assert np.array_equal(st["ip_cost"], g["qsrp_stats"]["ip_cost"])
     q100 = np.concatenate([g["query"]] * (100 // g["query"].shape[0] + 1))[:100]
-    us, _ = orc.us_retrieval(g["user_norm"], g["item"], g["uni_rank"], g["thr_uni"], q100, k)
+    us, st = orc.us_retrieval(g["user_norm"], g["item"], g["uni_rank"], g["thr_uni"], q100, k)
     assert same_results(us, g["us"])
+    assert np.array_equal(st["ip_cost"], g["us_stats"]["ip_cost"])
 
 
 @pytest.mark.parametrize("case", CASES)

@@ -108,58 +108,63 @@ def build_index(R, user_raw, item, cfg, device):
 
 
 class Clocks:
-    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+    """SM clock and throttle reasons while the timed region runs: one `nvidia-smi -lms 200` process
+    started before warm-up and stopped after the timed steps; only samples inside the timed
+    window (plus a margin) are summarised."""
+
+    QUERY = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device):
         self.device = device
         self.samples = []
-        self._stop = threading.Event()
-        self._t = None
+        self.window = None
 
     def __enter__(self):
-        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
-             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-             "clocks_event_reasons.sw_power_cap")
-
-        def run():
-            while not self._stop.is_set():
-                try:
-                    out = subprocess.run(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                         timeout=5).stdout.strip()
-                    if out:
-                        self.samples.append((time.perf_counter(), [x.strip() for x in out.split(",")]))
-                except Exception:
-                    pass
-                self._stop.wait(0.2)
-
-        self._t = threading.Thread(target=run, daemon=True)
-        self._t.start()
+        self.t0 = time.perf_counter()
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.lines = []
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        except Exception:
+            self.proc = None
         return self
 
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append((time.perf_counter(), line.strip()))
+
     def __exit__(self, *exc):
-        self._stop.set()
-        self._t.join(timeout=10)
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.reader.join(timeout=5)
+            self.samples = [(t, [x.strip() for x in l.split(",")]) for t, l in self.lines if l]
 
     def mark(self, t0, t1):
-        """Restrict the summary to samples taken between t0 and t1 (perf_counter seconds)."""
         self.window = (t0, t1)
 
     def summary(self):
-        w = getattr(self, "window", None)
-        samples = [s for t, s in self.samples if w is None or w[0] - 0.25 <= t <= w[1] + 0.25]
+        w = self.window
+        samples = [s for t, s in self.samples if w is None or w[0] - 0.3 <= t <= w[1] + 0.3]
         if not samples:
             samples = [s for _, s in self.samples[-3:]]
-        self.samples = samples
-        if not self.samples:
+        if not samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        sm = [float(s[0]) for s in samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in samples if s[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if len(s) > 3 + i and
+        reasons = sorted({names[i] for s in samples for i in range(4) if len(s) > 3 + i and
                           s[3 + i].lower() in ("active", "1")})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(samples)}
 
 
 def kernel_model(name, cfg, nq, stats):
@@ -342,6 +347,7 @@ def main():
     model_stats = {"check_dim": parts["cd"], "n_compute_item": float(st["n_compute_item"].sum()),
                    "eligible2": float(n_user * batch)}
     launches_per_step = sum(c for _, c in prof.values())
+    stats_mean = {f: float(st[f].mean()) for f in R.QUERY_STATS.names}
     dom = max(prof.items(), key=lambda kv: kv[1][0])
     dom_name, (dom_ms, dom_n) = dom
     ops, nbytes = kernel_model(dom_name, args.config, batch, model_stats)
@@ -418,7 +424,7 @@ def main():
             "single_query_p99_ms": float(np.percentile(single, 99)),
             "build_sec": build_sec, "build_stages_sec": {k: round(v, 3) for k, v in stages.items()},
             "e2e": e2e, "gpu_launches": int(launches_per_step * args.steps), "roofline": roofline,
-            "cpu_baseline": cpu, "clocks": clk.summary(),
+            "cpu_baseline": cpu, "clocks": clk.summary(), "query_stats_mean": stats_mean,
         }
         print(json.dumps(line))
     ix.close()

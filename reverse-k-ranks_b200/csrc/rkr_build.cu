@@ -40,6 +40,26 @@ __global__ void __launch_bounds__(kTileThreads) score_rows_kernel(const float *_
     }
 }
 
+// score_rows on 128 x 128 tiles (items x users): rows[u - u0][i] = InnerProduct(user, item).
+struct ScoreRowsEpi {
+    static constexpr size_t kExtra = 0;
+    float *rows;
+    int64_t ld, n_item, n_rows;
+    __device__ void prologue(char *, int64_t, int64_t) const {}
+    __device__ bool active(char *, int64_t, int64_t) const { return true; }
+    __device__ void finish(char *, const BigResult &res, int64_t a0, int64_t b0, bool) const {
+        const int ra = threadIdx.x & (kBig - 1), half = threadIdx.x >> 7;
+        const int64_t it = a0 + ra;
+        if (it >= n_item) return;
+#pragma unroll 8
+        for (int i = 0; i < kBig / 2; i++) {
+            const int rb = half + 2 * i;
+            if (b0 + rb >= n_rows) break;
+            rows[(b0 + rb) * ld + it] = res.v[rb][ra];
+        }
+    }
+};
+
 // Ascending sort of up to 32 keys held one per lane (missing lanes hold +inf).
 __device__ __forceinline__ float warp_sort32(float v) {
     const int lane = threadIdx.x & 31;
@@ -290,10 +310,17 @@ int run_rows(RowPipeline &P, int64_t u0, int64_t nu, SelectArgs sa) {
     rkr_index *ix = P.ix;
     cudaStream_t st = ix->stream;
     float *rows = ix->ws_bucket.as<float>();
-    dim3 g((unsigned) ((ix->n_item + kTile - 1) / kTile), (unsigned) ((nu + kTile - 1) / kTile));
-    timed(ix, st, "score_rows", [&] { score_rows_kernel<<<g, kTileThreads, 0, st>>>(ix->item.as<float>(), ix->n_item, ix->user.as<float>(), u0, nu, ix->dim,
-                                                 rows, P.ld); });
-    RKR_CUDA(cudaGetLastError());
+    ScoreRowsEpi epi;
+    epi.rows = rows;
+    epi.ld = P.ld;
+    epi.n_item = ix->n_item;
+    epi.n_rows = nu;
+    cudaError_t ce = cudaSuccess;
+    timed(ix, st, "score_rows", [&] {
+        ce = launch_big(ix->item.as<float>(), nullptr, ix->n_item, ix->dim, ix->user.as<float>() + u0 * ix->dim, nu,
+                        ix->dim, 0, ix->dim, epi, st);
+    });
+    RKR_CUDA(ce);
     sa.rows = rows;
     sa.ld = P.ld;
     sa.n_rows = (int) nu;

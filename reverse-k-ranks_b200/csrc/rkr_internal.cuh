@@ -50,12 +50,15 @@ void set_error(const char *fmt, ...);
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
+    // Grows with 25% headroom so batches of slightly varying size do not reallocate (each
+    // reallocation synchronises the device).
     int ensure(size_t want) {
         if (want <= bytes) return RKR_OK;
         if (p) cudaFree(p);
         p = nullptr;
         bytes = 0;
         if (want == 0) return RKR_OK;
+        want += want / 4 + 4096;
         cudaError_t e = cudaMalloc(&p, want);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -141,6 +144,138 @@ __device__ __forceinline__ void exact_tile(TileSmem &sm, const float *__restrict
     }
 }
 
+// ---- 128 x 128 exact tiles ------------------------------------------------------------------------
+//
+// The bulk form of exact_tile: each CTA computes a 128 x 128 block of dot products over
+// k in [k_begin, k_end), each thread an 8 x 8 register block, with the k range staged through a
+// double-buffered shared-memory pipeline (cp.async).  Products and sums stay separately rounded and
+// in k order, so every value is the reference's InnerProduct bit for bit; zero-filled padding k
+// adds +0.0, which leaves a sum that starts at +0.0 unchanged.  The finished block goes through
+// shared memory to an epilogue functor that visits the pairs with consecutive threads on
+// consecutive A rows, so outputs indexed [b][a] are written coalesced.
+
+constexpr int kBig = 128, kBigK = 16, kBigPad = 4, kBigThreads = 256;
+
+struct BigOperands {
+    float a[2][kBigK][kBig + kBigPad];
+    float b[2][kBigK][kBig + kBigPad];
+};
+struct BigResult {
+    float v[kBig][kBig + kBigPad];  // [b row][a row]
+};
+constexpr size_t kBigSmem = sizeof(BigResult) > sizeof(BigOperands) ? sizeof(BigResult) : sizeof(BigOperands);
+
+__device__ __forceinline__ void cp_async4(float *smem, const float *gmem, bool valid) {
+    const unsigned s = (unsigned) __cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 4 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void big_load_stage(BigOperands &op, int buf, const float *__restrict__ A,
+                                               const int32_t *__restrict__ a_idx, int64_t n_a, int lda, int64_t a0,
+                                               const float *__restrict__ B, int64_t n_b, int ldb, int64_t b0, int k0,
+                                               int k_end) {
+#pragma unroll 1
+    for (int t = 0; t < (kBig * kBigK) / kBigThreads; t++) {
+        const int idx = threadIdx.x + t * kBigThreads;
+        const int r = idx / kBigK, kk = idx % kBigK;
+        const int k = k0 + kk;
+        const int64_t ra = a0 + r, rb = b0 + r;
+        const bool va = ra < n_a && k < k_end, vb = rb < n_b && k < k_end;
+        const int64_t row = va ? (a_idx ? (int64_t) a_idx[ra] : ra) : 0;
+        cp_async4(&op.a[buf][kk][r], va ? A + row * lda + k : A, va);
+        cp_async4(&op.b[buf][kk][r], vb ? B + rb * ldb + k : B, vb);
+    }
+}
+
+// Fills res with the 128 x 128 block of dot products (A rows a0.., B rows b0..) over [k_begin, k_end).
+__device__ __forceinline__ void exact_big_tile(char *smem, const float *__restrict__ A, const int32_t *__restrict__ a_idx,
+                                              int64_t n_a, int lda, int64_t a0, const float *__restrict__ B,
+                                              int64_t n_b, int ldb, int64_t b0, int k_begin, int k_end) {
+    BigOperands &op = *reinterpret_cast<BigOperands *>(smem);
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    float acc[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] = 0.0f;
+    const int ns = (k_end - k_begin + kBigK - 1) / kBigK;
+    if (ns > 0) {
+        big_load_stage(op, 0, A, a_idx, n_a, lda, a0, B, n_b, ldb, b0, k_begin, k_end);
+        cp_async_commit();
+    }
+    for (int s = 0; s < ns; s++) {
+        if (s + 1 < ns) {
+            big_load_stage(op, (s + 1) & 1, A, a_idx, n_a, lda, a0, B, n_b, ldb, b0, k_begin + (s + 1) * kBigK, k_end);
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const int buf = s & 1;
+#pragma unroll
+        for (int kk = 0; kk < kBigK; kk++) {
+            const float4 a_lo = *reinterpret_cast<const float4 *>(&op.a[buf][kk][4 * tx]);
+            const float4 a_hi = *reinterpret_cast<const float4 *>(&op.a[buf][kk][64 + 4 * tx]);
+            const float4 b_lo = *reinterpret_cast<const float4 *>(&op.b[buf][kk][4 * ty]);
+            const float4 b_hi = *reinterpret_cast<const float4 *>(&op.b[buf][kk][64 + 4 * ty]);
+            const float av[8] = {a_lo.x, a_lo.y, a_lo.z, a_lo.w, a_hi.x, a_hi.y, a_hi.z, a_hi.w};
+            const float bv[8] = {b_lo.x, b_lo.y, b_lo.z, b_lo.w, b_hi.x, b_hi.y, b_hi.z, b_hi.w};
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+#pragma unroll
+                for (int j = 0; j < 8; j++) acc[i][j] = __fadd_rn(acc[i][j], __fmul_rn(av[i], bv[j]));
+        }
+        __syncthreads();
+    }
+    BigResult &res = *reinterpret_cast<BigResult *>(smem);
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        const int cb = (j < 4 ? 0 : 64) + 4 * ty + (j & 3);
+        *reinterpret_cast<float4 *>(&res.v[cb][4 * tx]) = make_float4(acc[0][j], acc[1][j], acc[2][j], acc[3][j]);
+        *reinterpret_cast<float4 *>(&res.v[cb][64 + 4 * tx]) = make_float4(acc[4][j], acc[5][j], acc[6][j], acc[7][j]);
+    }
+    __syncthreads();
+}
+
+// Grid: x over B tiles, y over A tiles.  Epi provides: static constexpr size_t kExtra (extra shared
+// bytes), prologue(extra, a0, b0), active(extra, a0, b0) (false skips the dot products) and
+// finish(extra, res, a0, b0, live), which reads the block from res.v[b - b0][a - a0].  The usual
+// finish is row-owned: thread t takes A row a0 + (t % 128) and B rows b0 + t / 128 + 2 i, so a
+// warp writes 32 consecutive A rows of one B row at a time.
+template <class Epi>
+__global__ void __launch_bounds__(kBigThreads, 2) exact_big_kernel(const float *__restrict__ A,
+                                                                   const int32_t *__restrict__ a_idx, int64_t n_a,
+                                                                   int lda, const float *__restrict__ B, int64_t n_b,
+                                                                   int ldb, int k_begin, int k_end, Epi epi) {
+    extern __shared__ __align__(16) char big_smem[];
+    char *extra = big_smem + kBigSmem;
+    const int64_t b0 = (int64_t) blockIdx.x * kBig;
+    const int64_t a0 = (int64_t) blockIdx.y * kBig;
+    epi.prologue(extra, a0, b0);
+    __syncthreads();
+    const bool live = epi.active(extra, a0, b0);
+    if (live) exact_big_tile(big_smem, A, a_idx, n_a, lda, a0, B, n_b, ldb, b0, k_begin, k_end);
+    epi.finish(extra, *reinterpret_cast<const BigResult *>(big_smem), a0, b0, live);
+}
+
+template <class Epi>
+inline size_t big_kernel_smem() { return kBigSmem + Epi::kExtra; }
+
+// Launches exact_big_kernel<Epi> over n_a x n_b pairs on stream st.
+template <class Epi>
+inline cudaError_t launch_big(const float *A, const int32_t *a_idx, int64_t n_a, int lda, const float *B, int64_t n_b,
+                              int ldb, int k_begin, int k_end, const Epi &epi, cudaStream_t st) {
+    const size_t smem = big_kernel_smem<Epi>();
+    cudaError_t e = cudaFuncSetAttribute(exact_big_kernel<Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid((unsigned) ((n_b + kBig - 1) / kBig), (unsigned) ((n_a + kBig - 1) / kBig));
+    exact_big_kernel<Epi><<<grid, kBigThreads, smem, st>>>(A, a_idx, n_a, lda, B, n_b, ldb, k_begin, k_end, epi);
+    return cudaGetLastError();
+}
+
 // Sequential binary32 dot product of one pair (thread-serial), same arithmetic as exact_tile.
 __device__ __forceinline__ float exact_dot(const float *__restrict__ a, const float *__restrict__ b, int n) {
     float acc = 0.0f;
@@ -199,7 +334,7 @@ __device__ __forceinline__ int block_excl_scan(int v, int *warp_tot, int *total)
 // last (smallest) threshold is below q there, and counts the thresholds >= q inside that group
 // with independent loads.  On a descending row this is the same count std::lower_bound returns.
 struct ThrSummary {
-    static constexpr int kMaxGroups = 64;
+    static constexpr int kMaxGroups = 32;
     float v[kTile][kMaxGroups];
 };
 
@@ -218,6 +353,17 @@ __device__ __forceinline__ void load_thr_summary(ThrSummary &ts, const float *__
     }
 }
 
+// Threshold summaries for `rows` users starting at a0 into dst[rows][kMaxGroups].
+__device__ __forceinline__ void load_thr_summary_rows(float *dst, int rows, const float *__restrict__ thr,
+                                                      int64_t n_user, int64_t a0, int S) {
+    const int g = thr_group(S), nb = (S + g - 1) / g;
+    for (int idx = threadIdx.x; idx < rows * nb; idx += blockDim.x) {
+        const int r = idx / nb, j = idx % nb;
+        const int64_t u = a0 + r;
+        dst[r * ThrSummary::kMaxGroups + j] = u < n_user ? __ldg(thr + u * S + min(g * j + g - 1, S - 1)) : 0.0f;
+    }
+}
+
 __device__ __forceinline__ int bucket_of_2level(const float *__restrict__ summ, const float *__restrict__ row, int S,
                                                 float q) {
     const int g = thr_group(S), nb = (S + g - 1) / g;
@@ -229,12 +375,14 @@ __device__ __forceinline__ int bucket_of_2level(const float *__restrict__ summ, 
     if (lo == nb) return S;
     const int base = g * lo, end = min(base + g, S);
     int c = 0;
-    if (g == 16 && end - base == 16 && (S & 3) == 0) {
+    if ((g & 15) == 0 && end - base == g && (S & 3) == 0) {
         const float4 *p = reinterpret_cast<const float4 *>(row + base);
-        const float4 x0 = __ldg(p), x1 = __ldg(p + 1), x2 = __ldg(p + 2), x3 = __ldg(p + 3);
-        c = (x0.x >= q) + (x0.y >= q) + (x0.z >= q) + (x0.w >= q) + (x1.x >= q) + (x1.y >= q) + (x1.z >= q) +
-            (x1.w >= q) + (x2.x >= q) + (x2.y >= q) + (x2.z >= q) + (x2.w >= q) + (x3.x >= q) + (x3.y >= q) +
-            (x3.z >= q) + (x3.w >= q);
+        for (int t = 0; t < g / 16; t++, p += 4) {
+            const float4 x0 = __ldg(p), x1 = __ldg(p + 1), x2 = __ldg(p + 2), x3 = __ldg(p + 3);
+            c += (x0.x >= q) + (x0.y >= q) + (x0.z >= q) + (x0.w >= q) + (x1.x >= q) + (x1.y >= q) + (x1.z >= q) +
+                 (x1.w >= q) + (x2.x >= q) + (x2.y >= q) + (x2.z >= q) + (x2.w >= q) + (x3.x >= q) + (x3.y >= q) +
+                 (x3.z >= q) + (x3.w >= q);
+        }
     } else {
         for (int i = base; i < end; i++) c += __ldg(row + i) >= q;
     }

@@ -97,10 +97,9 @@ __device__ __forceinline__ int64_t regression_index(float nx, float a, float b, 
 }
 
 // ComputeRankBound (:326-380), returning levels: 0 -> rank 0, j + 1 -> rank[j], S + 1 -> n_item.
-__device__ __forceinline__ void regression_levels(const RegModel &m, int64_t u, float qlb, float qub, int &lvl_lb,
-                                                  int &lvl_ub) {
-    const float4 r0 = __ldg(reinterpret_cast<const float4 *>(m.rec + u * 8));
-    const float4 r1 = __ldg(reinterpret_cast<const float4 *>(m.rec + u * 8 + 4));
+// r0 = (a, b, mu, sigma), r1 = (err, smax, smin, -) is the user's model record.
+__device__ __forceinline__ void regression_levels_rec(const RegModel &m, float4 r0, float4 r1, float qlb, float qub,
+                                                      int &lvl_lb, int &lvl_ub) {
     const float a = r0.x, b = r0.y, mu = r0.z, sigma = r0.w, err = r1.x, smax = r1.y, smin = r1.z;
     const int S = m.S;
     if (qlb > smax) lvl_lb = 1;
@@ -117,6 +116,12 @@ __device__ __forceinline__ void regression_levels(const RegModel &m, int64_t u, 
         const int64_t pr = regression_index(__fdiv_rn(__fsub_rn(qub, mu), sigma), a, b, err, true);
         lvl_ub = pr >= S ? S + 1 : (pr < 0 ? 0 : (int) pr + 1);
     }
+}
+
+__device__ __forceinline__ void regression_levels(const RegModel &m, int64_t u, float qlb, float qub, int &lvl_lb,
+                                                  int &lvl_ub) {
+    regression_levels_rec(m, __ldg(reinterpret_cast<const float4 *>(m.rec + u * 8)),
+                          __ldg(reinterpret_cast<const float4 *>(m.rec + u * 8 + 4)), qlb, qub, lvl_lb, lvl_ub);
 }
 
 __device__ __forceinline__ int level_rank(int lvl, const int32_t *rank, int S, int n_item) {
@@ -218,6 +223,39 @@ __global__ void __launch_bounds__(kHistThreads) level_hist_kernel(const uint32_t
     }
     if (threadIdx.x == 0 && anom) atomicAdd(anomaly + q, anom);
 }
+
+// Round 1 on 128 x 128 tiles (users x queries): left over the first check_dim coordinates, the
+// bounds left -+ norms and their regression levels.
+struct Round1Epi {
+    static constexpr size_t kExtra = 0;
+    const float *unorm, *qnorm;
+    RegModel m;
+    uint32_t *lv;
+    float *left;
+    int64_t n_user, n_query;
+    __device__ void prologue(char *, int64_t, int64_t) const {}
+    __device__ bool active(char *, int64_t, int64_t) const { return true; }
+    __device__ void finish(char *, const BigResult &res, int64_t a0, int64_t b0, bool) const {
+        const int ra = threadIdx.x & (kBig - 1), half = threadIdx.x >> 7;
+        const int64_t u = a0 + ra;
+        if (u >= n_user) return;
+        const float4 r0 = __ldg(reinterpret_cast<const float4 *>(m.rec + u * 8));
+        const float4 r1 = __ldg(reinterpret_cast<const float4 *>(m.rec + u * 8 + 4));
+        const float un = __ldg(unorm + u);
+#pragma unroll 2
+        for (int i = 0; i < kBig / 2; i++) {
+            const int rb = half + 2 * i;
+            const int64_t q = b0 + rb;
+            if (q >= n_query) break;
+            const float v = res.v[rb][ra];
+            const float right = __fmul_rn(un, __ldg(qnorm + q));
+            int l, h;
+            regression_levels_rec(m, r0, r1, __fsub_rn(v, right), __fadd_rn(v, right), l, h);
+            lv[q * n_user + u] = (uint32_t) l | ((uint32_t) h << 16);
+            left[q * n_user + u] = v;
+        }
+    }
+};
 
 // Round-1 k-th smallest bounds per query (PruneCandidateByBound.hpp:36-77 with nothing excluded)
 // and the class counts.  While every pair has ub <= lb, a result (lb <= U*) and a prune
@@ -377,6 +415,95 @@ __global__ void __launch_bounds__(kTileThreads, 3) qsrp_round2_kernel(const floa
         }
     }
 }
+
+// Round 2 on 128 x 128 tiles: pairs that reached round 2 get left + the remaining coordinates and
+// their sampled-threshold bucket; the others their round-1 state code.  Tiles without a surviving
+// pair skip the dot products.
+struct Round2Epi {
+    static constexpr int kMaxRank = 1024;
+    static constexpr size_t kExtra = sizeof(float) * kBig * ThrSummary::kMaxGroups + sizeof(QsrpParams) * kBig +
+                                     sizeof(int32_t) * kMaxRank;
+    const uint32_t *lv;
+    const float *left;
+    const QsrpParams *par;
+    const int32_t *reg_rank;
+    int S_reg, n_item;
+    const float *thr;
+    int S;
+    int64_t n_user;
+    int n_query;
+    uint16_t *bucket2;
+    __device__ float *summ(char *x) const { return reinterpret_cast<float *>(x); }
+    __device__ QsrpParams *pars(char *x) const {
+        return reinterpret_cast<QsrpParams *>(x + sizeof(float) * kBig * ThrSummary::kMaxGroups);
+    }
+    __device__ const int32_t *ranks(char *x) const {
+        return S_reg <= kMaxRank ? reinterpret_cast<const int32_t *>(x + sizeof(float) * kBig * ThrSummary::kMaxGroups +
+                                                                    sizeof(QsrpParams) * kBig)
+                                 : reg_rank;
+    }
+    __device__ int klass(char *x, int64_t u, int64_t q, int rb) const {
+        const uint32_t v = lv[q * n_user + u];
+        const int32_t *rk = ranks(x);
+        return class1_of(pars(x)[rb], level_rank(v & 0xffff, rk, S_reg, n_item), level_rank(v >> 16, rk, S_reg, n_item));
+    }
+    __device__ void prologue(char *x, int64_t a0, int64_t b0) const {
+        if (threadIdx.x < kBig && b0 + threadIdx.x < n_query) pars(x)[threadIdx.x] = par[b0 + threadIdx.x];
+        if (S_reg <= kMaxRank) {
+            int32_t *rk = reinterpret_cast<int32_t *>(x + sizeof(float) * kBig * ThrSummary::kMaxGroups +
+                                                      sizeof(QsrpParams) * kBig);
+            for (int i = threadIdx.x; i < S_reg; i += blockDim.x) rk[i] = reg_rank[i];
+        }
+        load_thr_summary_rows(summ(x), kBig, thr, n_user, a0, S);
+    }
+    __device__ bool active(char *x, int64_t a0, int64_t b0) const {
+        bool any = false;
+        for (int idx = threadIdx.x; idx < kBig * kBig && !any; idx += kBigThreads) {
+            const int rb = idx / kBig, ra = idx % kBig;
+            const int64_t u = a0 + ra, q = b0 + rb;
+            if (u < n_user && q < n_query) {
+                const int k = klass(x, u, q, rb);
+                any = k == kClsRefine || k == kClsIdle;
+            }
+        }
+        return __syncthreads_or(any);
+    }
+    __device__ void finish(char *x, const BigResult &res, int64_t a0, int64_t b0, bool live) const {
+        const int ra = threadIdx.x & (kBig - 1), half = threadIdx.x >> 7;
+        const int64_t u = a0 + ra;
+        if (u >= n_user) return;
+        const float *sm = summ(x) + ra * ThrSummary::kMaxGroups;
+        const float *row = thr + u * S;
+        const int32_t *rk = ranks(x);
+        const QsrpParams *ps = pars(x);
+        constexpr int G = 8;
+        for (int i0 = 0; i0 < kBig / 2; i0 += G) {
+            uint32_t v[G];
+            float lf[G];
+#pragma unroll
+            for (int g = 0; g < G; g++) {
+                const int64_t q = b0 + half + 2 * (i0 + g);
+                v[g] = q < n_query ? lv[q * n_user + u] : 0u;
+                lf[g] = q < n_query ? left[q * n_user + u] : 0.0f;
+            }
+#pragma unroll
+            for (int g = 0; g < G; g++) {
+                const int rb = half + 2 * (i0 + g);
+                const int64_t q = b0 + rb;
+                if (q >= n_query) break;
+                const int k = class1_of(ps[rb], level_rank(v[g] & 0xffff, rk, S_reg, n_item),
+                                        level_rank(v[g] >> 16, rk, S_reg, n_item));
+                uint16_t b;
+                if (k == kClsRefine || k == kClsIdle) {
+                    b = (uint16_t) bucket_of_2level(sm, row, S, __fadd_rn(lf[g], live ? res.v[rb][ra] : 0.0f));
+                } else {
+                    b = k == kClsResult ? kStateResult1 : kStatePruned1;
+                }
+                bucket2[q * n_user + u] = b;
+            }
+        }
+    }
+};
 
 // Round-2 pruning per query (second PruneCandidateByBound call, QSRPNormalLP.hpp:187-190): users
 // excluded in round 1 are skipped by the heap scan and the classification; the equal-bounds rule
@@ -608,12 +735,17 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     m.S = Sr;
     m.err_cap = (double) Sr - 1e-3;
     m.n_item = n_item;
-    dim3 grid((unsigned) ((nq + kTile - 1) / kTile), (unsigned) ((U + kTile - 1) / kTile));
-    timed(ix, st, "qsrp_round1", [&] {
-        qsrp_round1_kernel<<<grid, kTileThreads, 0, st>>>(ix->svd_user.as<float>(), U, dim, ix->svd_unorm.as<float>(),
-                                                         qtr, qnorm, nq, c, m, lv, left);
-    });
-    RKR_CUDA(cudaGetLastError());
+    Round1Epi e1;
+    e1.unorm = ix->svd_unorm.as<float>();
+    e1.qnorm = qnorm;
+    e1.m = m;
+    e1.lv = lv;
+    e1.left = left;
+    e1.n_user = U;
+    e1.n_query = nq;
+    cudaError_t ce = cudaSuccess;
+    timed(ix, st, "qsrp_round1", [&] { ce = launch_big(ix->svd_user.as<float>(), nullptr, U, dim, qtr, nq, dim, 0, c, e1, st); });
+    RKR_CUDA(ce);
     const int64_t chunk = 16384;
     dim3 hg((unsigned) ((U + chunk - 1) / chunk), (unsigned) nq);
     RKR_CUDA(cudaMemsetAsync(hist, 0, sizeof(int) * (size_t) nq * 2 * nl, st));
@@ -633,11 +765,20 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     }
     timed(ix, st, "qsrp_final1", [&] { qsrp_final1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, topk); });
     RKR_CUDA(cudaGetLastError());
-    timed(ix, st, "qsrp_round2", [&] {
-        qsrp_round2_kernel<<<grid, kTileThreads, Sr * sizeof(int32_t), st>>>(ix->svd_user.as<float>(), U, dim, qtr, nq, c, lv, left, par,
-                                                         m.rank, Sr, n_item, ix->thr.as<float>(), S, b2);
-    });
-    RKR_CUDA(cudaGetLastError());
+    Round2Epi e2;
+    e2.lv = lv;
+    e2.left = left;
+    e2.par = par;
+    e2.reg_rank = m.rank;
+    e2.S_reg = Sr;
+    e2.n_item = n_item;
+    e2.thr = ix->thr.as<float>();
+    e2.S = S;
+    e2.n_user = U;
+    e2.n_query = nq;
+    e2.bucket2 = b2;
+    timed(ix, st, "qsrp_round2", [&] { ce = launch_big(ix->svd_user.as<float>(), nullptr, U, dim, qtr, nq, dim, c, dim, e2, st); });
+    RKR_CUDA(ce);
     RKR_CUDA(cudaMemsetAsync(hist, 0, sizeof(int) * (size_t) nq * (S + 1), st));
     timed(ix, st, "bucket_hist", [&] {
         bucket_hist_kernel<<<hg, kHistThreads, hist_copies(S + 1) * (S + 1) * sizeof(int), st>>>(b2, U, S + 1, chunk, hist);

@@ -59,6 +59,33 @@ __global__ void __launch_bounds__(kTileThreads) score_bucket_kernel(const float 
     }
 }
 
+// score_bucket on 128 x 128 tiles: the exact score of each (user, query) pair and its bucket.
+struct QsBucketEpi {
+    static constexpr size_t kExtra = sizeof(float) * kBig * ThrSummary::kMaxGroups;
+    const float *thr;
+    int64_t n_user, n_query;
+    int S;
+    uint16_t *bucket;
+    __device__ void prologue(char *extra, int64_t a0, int64_t) const {
+        load_thr_summary_rows(reinterpret_cast<float *>(extra), kBig, thr, n_user, a0, S);
+    }
+    __device__ bool active(char *, int64_t, int64_t) const { return true; }
+    __device__ void finish(char *extra, const BigResult &res, int64_t a0, int64_t b0, bool) const {
+        const int ra = threadIdx.x & (kBig - 1), half = threadIdx.x >> 7;
+        const int64_t u = a0 + ra;
+        if (u >= n_user) return;
+        const float *summ = reinterpret_cast<const float *>(extra) + ra * ThrSummary::kMaxGroups;
+        const float *row = thr + u * S;
+#pragma unroll 4
+        for (int i = 0; i < kBig / 2; i++) {
+            const int rb = half + 2 * i;
+            const int64_t q = b0 + rb;
+            if (q >= n_query) break;
+            bucket[q * n_user + u] = (uint16_t) bucket_of_2level(summ, row, S, res.v[rb][ra]);
+        }
+    }
+};
+
 __global__ void select_bucket_kernel(const int *__restrict__ hist_all, int S, const int32_t *__restrict__ rank,
                                      int n_item, int topk, int n_user, uint8_t *__restrict__ cls,
                                      QueryCounts *__restrict__ counts) {
@@ -591,12 +618,17 @@ static int qs_chunk(rkr_index *ix, int method, const float *d_query, int nq, int
     QueryCounts *counts = ix->ws_counts.as<QueryCounts>();
     int *hist = ix->ws_hist.as<int>();
     {
-        dim3 grid((unsigned) ((nq + kTile - 1) / kTile), (unsigned) ((U + kTile - 1) / kTile));
+        QsBucketEpi epi;
+        epi.thr = ix->thr.as<float>();
+        epi.n_user = U;
+        epi.n_query = nq;
+        epi.S = S;
+        epi.bucket = bucket;
+        cudaError_t e = cudaSuccess;
         timed(ix, st, "score_bucket", [&] {
-            score_bucket_kernel<<<grid, kTileThreads, 0, st>>>(ix->user.as<float>(), U, dim, d_query, nq,
-                                                              ix->thr.as<float>(), S, bucket);
+            e = launch_big(ix->user.as<float>(), nullptr, U, dim, d_query, nq, dim, 0, dim, epi, st);
         });
-        RKR_CUDA(cudaGetLastError());
+        RKR_CUDA(e);
         RKR_CUDA(cudaMemsetAsync(hist, 0, sizeof(int) * (size_t) nq * (S + 1), st));
         const int64_t chunk = 16384;
         dim3 hg((unsigned) ((U + chunk - 1) / chunk), (unsigned) nq);

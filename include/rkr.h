@@ -143,6 +143,25 @@ int rkr_score_sort_batch(rkr_index *index, int64_t start_user, int64_t n_rows, f
 int rkr_index_query_rank_distribution(rkr_index *index, const int32_t *sample_item, int32_t n_sample_item,
                                       int32_t *accu_out);
 
+/* Threshold build that allocates nothing.  Some callers cannot let a library call cudaMalloc:
+ * services that fix their device footprint at start-up, code running under a caching allocator
+ * or a carved-up memory pool, callers inside allocation-sensitive sections.  This entry point
+ * computes the same thresholds as rkr_index_build_sample_search, for users and items already in
+ * device memory of the current device (d_user [n_user][dim], d_item [n_item][dim], d_thresholds
+ * [n_user][n_sample] written), with host sample ranks (ascending, in [0, n_item)).  Its only
+ * scratch is a fixed 32 MiB array compiled into the library, which every GPU that loads the
+ * library keeps until the process exits; it holds at most 16384 sample ranks and batches of
+ * (32 MiB - 64 KiB) / (4 * round_up(n_item, 4)) score rows, and n_item must also fit the
+ * shared-memory row selection (about 24,000 items on B200); larger sizes are RKR_ERR_INVALID.
+ * The first call on a device looks the array's device address up (cudaGetSymbolAddress), so
+ * make that first call before any stream capture.  Calls share the array: calls that overlap on
+ * the GPU (other streams, other host threads) race; the call returns after its work on `stream`
+ * (a cudaStream_t, NULL for the legacy default stream) has finished.  There is no counterpart in
+ * the reference, which always allocates its score-table buffers. */
+int rkr_build_thresholds_static(const float *d_user, int64_t n_user, const float *d_item, int64_t n_item,
+                                int32_t dim, const int32_t *sample_rank, int32_t n_sample, float *d_thresholds,
+                                void *stream);
+
 /* Host-side build steps (CPU; no device needed). */
 
 /* VectorMatrix::vectorNormalize (src/include/struct/VectorMatrix.hpp:51-66), in place. */

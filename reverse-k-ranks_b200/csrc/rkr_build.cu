@@ -8,6 +8,7 @@
 // only the bins that contain a requested position.  The row is never sorted as a whole unless a
 // full sort is what the caller wants (rkr_score_sort_batch).
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "rkr_internal.cuh"
@@ -398,4 +399,103 @@ int query_rank_distribution(rkr_index *ix, const int32_t *sample_item, int n_sam
     return RKR_OK;
 }
 
+// ---- threshold build without device allocation ------------------------------------------------------
+//
+// rkr_build_thresholds_static serves callers that must not allocate device memory themselves or
+// through the library: code running where cudaMalloc is not allowed or not wanted (inside a
+// memory pool that has already been carved up, an allocator hook, a real-time service that fixes
+// its footprint at start-up).  Its only scratch is this fixed array, which every GPU that loads the
+// library holds until the process exits: the sampled ranks (first 64 KiB) and one batch of score
+// rows (the rest).  In host code g_static_scratch names a host-side stand-in, not device memory,
+// so the kernels receive the address cudaGetSymbolAddress returns for the current device.
+
+constexpr size_t kStaticScratchBytes = size_t(32) << 20;
+constexpr size_t kStaticRankBytes = size_t(64) << 10;
+constexpr int kStaticMaxSample = (int) (kStaticRankBytes / sizeof(int32_t));
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+namespace {
+std::mutex g_static_mu;
+void *g_static_addr[256];  // per device, filled on the first call on that device
+}  // namespace
+
+static int static_scratch_address(int dev, unsigned char **out) {
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (dev < 0 || dev >= 256) {
+        set_error("rkr_build_thresholds_static: device ordinal %d out of range", dev);
+        return RKR_ERR_INVALID;
+    }
+    if (!g_static_addr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess) {
+            set_error("rkr_build_thresholds_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+            return RKR_ERR_CUDA;
+        }
+        g_static_addr[dev] = p;
+    }
+    *out = static_cast<unsigned char *>(g_static_addr[dev]);
+    return RKR_OK;
+}
+
 }  // namespace rkr
+
+extern "C" int rkr_build_thresholds_static(const float *d_user, int64_t n_user, const float *d_item, int64_t n_item,
+                                           int32_t dim, const int32_t *sample_rank, int32_t n_sample,
+                                           float *d_thresholds, void *stream) {
+    using namespace rkr;
+    RKR_REQUIRE(d_user && d_item && sample_rank && d_thresholds, "rkr_build_thresholds_static: null argument");
+    RKR_REQUIRE(n_user > 0 && n_item > 1 && dim > 0 && dim <= 4096, "rkr_build_thresholds_static: bad sizes");
+    RKR_REQUIRE(n_sample > 0 && n_sample < n_item, "rkr_build_thresholds_static: n_sample %d must be in (0, n_item)",
+                n_sample);
+    RKR_REQUIRE(n_sample <= kStaticMaxSample, "rkr_build_thresholds_static: n_sample %d above the maximum %d",
+                n_sample, kStaticMaxSample);
+    for (int j = 0; j < n_sample; j++) {
+        RKR_REQUIRE(sample_rank[j] >= 0 && sample_rank[j] < n_item, "sample rank %d out of range", sample_rank[j]);
+        RKR_REQUIRE(j == 0 || sample_rank[j] >= sample_rank[j - 1], "sample ranks must be ascending");
+    }
+    const int64_t ld = (n_item + 3) / 4 * 4;
+    const int64_t row_bytes = ld * (int64_t) sizeof(float);
+    const int64_t batch = (int64_t) (kStaticScratchBytes - kStaticRankBytes) / row_bytes;
+    RKR_REQUIRE(batch >= 1, "rkr_build_thresholds_static: n_item %lld exceeds the %zu-byte scratch",
+                (long long) n_item, kStaticScratchBytes - kStaticRankBytes);
+    int dev = 0;
+    RKR_CUDA(cudaGetDevice(&dev));
+    int dev_smem = 0;
+    RKR_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t smem = (size_t) 2 * n_item * sizeof(float);
+    const size_t static_smem = sizeof(int) * (2 * kBins + 1) + 64 * sizeof(float) * 2 + 32 * sizeof(int);
+    RKR_REQUIRE(smem + static_smem + 1024 <= (size_t) dev_smem,
+                "rkr_build_thresholds_static: n_item %lld too large for the shared-memory row selection",
+                (long long) n_item);
+    unsigned char *scratch = nullptr;
+    RKR_TRY(static_scratch_address(dev, &scratch));
+    int32_t *d_rank = reinterpret_cast<int32_t *>(scratch);
+    float *rows = reinterpret_cast<float *>(scratch + kStaticRankBytes);
+    cudaStream_t st = (cudaStream_t) stream;
+    RKR_CUDA(cudaMemcpyAsync(d_rank, sample_rank, sizeof(int32_t) * n_sample, cudaMemcpyHostToDevice, st));
+    RKR_CUDA(cudaFuncSetAttribute(row_select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    int sms = 0;
+    RKR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    for (int64_t u0 = 0; u0 < n_user; u0 += batch) {
+        const int64_t nu = std::min(batch, n_user - u0);
+        ScoreRowsEpi epi;
+        epi.rows = rows;
+        epi.ld = ld;
+        epi.n_item = n_item;
+        epi.n_rows = nu;
+        RKR_CUDA(launch_big(d_item, nullptr, n_item, dim, d_user + u0 * dim, nu, dim, 0, dim, epi, st));
+        SelectArgs sa = {};
+        sa.rows = rows;
+        sa.ld = ld;
+        sa.n_rows = (int) nu;
+        sa.n_item = (int) n_item;
+        sa.sample_rank = d_rank;
+        sa.S = n_sample;
+        sa.thr_out = d_thresholds + u0 * n_sample;
+        row_select_kernel<<<(unsigned) std::min<int64_t>(sms, nu), kSelThreads, smem, st>>>(sa, 1);
+        RKR_CUDA(cudaGetLastError());
+    }
+    RKR_CUDA(cudaStreamSynchronize(st));
+    return RKR_OK;
+}

@@ -37,7 +37,7 @@ EXPORTS = [
     "rkr_index_size_bytes", "rkr_index_build_sample_search", "rkr_retrieval", "rkr_retrieval_device",
     "rkr_score_sort_batch", "rkr_index_query_rank_distribution", "rkr_normalize", "rkr_sample_item",
     "rkr_sort_kth_rank", "rkr_find_optimal_sample_rank", "rkr_uniform_sample_rank", "rkr_fit_regression",
-    "rkr_svd_build", "rkr_profile_enable", "rkr_profile_read",
+    "rkr_svd_build", "rkr_profile_enable", "rkr_profile_read", "rkr_build_thresholds_static",
 ]
 
 
@@ -142,6 +142,15 @@ def svd_build(user, sigma=0.7):
     _check(_lib.rkr_svd_build(_p(user), C.c_int64(user.shape[0]), C.c_int32(d), C.c_float(sigma), _p(ti), _p(su),
                               _p(cd)))
     return ti, su, int(cd[0])
+
+
+def build_thresholds_static(d_user, n_user, d_item, n_item, dim, sample_rank, d_thresholds, stream=None):
+    """rkr_build_thresholds_static: thresholds for users/items already on the current device
+    (device pointers as ints), without any device allocation by the library; see include/rkr.h."""
+    sr = _i32(sample_rank)
+    _check(_lib.rkr_build_thresholds_static(C.c_void_p(d_user), C.c_int64(n_user), C.c_void_p(d_item),
+                                            C.c_int64(n_item), C.c_int32(dim), _p(sr), C.c_int32(sr.shape[0]),
+                                            C.c_void_p(d_thresholds), C.c_void_p(stream or 0)))
 
 
 # ---- the device index ---------------------------------------------------------------------------------------

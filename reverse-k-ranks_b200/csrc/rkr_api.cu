@@ -32,6 +32,17 @@ __global__ void row_norm_kernel(const float *__restrict__ v, int64_t n, int dim,
     out[r] = __fsqrt_rn(exact_dot(p, p, dim - off));
 }
 
+// Per user, the last (smallest) threshold of each group of thr_group(S) consecutive thresholds;
+// unused slots hold -inf.
+__global__ void thr_summary_kernel(const float *__restrict__ thr, int64_t n_user, int S, float *__restrict__ summ) {
+    const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_user * ThrSummary::kMaxGroups) return;
+    const int64_t u = i / ThrSummary::kMaxGroups;
+    const int j = (int) (i % ThrSummary::kMaxGroups);
+    const int g = thr_group(S), nb = (S + g - 1) / g;
+    summ[i] = j < nb ? thr[u * S + min(g * j + g - 1, S - 1)] : -INFINITY;
+}
+
 __global__ void gather_rows_kernel(const float *__restrict__ src, const int32_t *__restrict__ idx, int64_t n, int dim,
                                    float *__restrict__ dst) {
     const int64_t r = blockIdx.x;
@@ -58,6 +69,16 @@ int refine_prepare_norms(rkr_index *ix) {
         RKR_CUDA(cudaGetLastError());
     }
     RKR_CUDA(cudaStreamSynchronize(ix->stream));
+    return RKR_OK;
+}
+
+// Group summaries of the current thresholds (enqueued on the index stream).
+int thr_summary_build(rkr_index *ix) {
+    const int64_t n = ix->n_user * ThrSummary::kMaxGroups;
+    RKR_TRY(ix->thr_summ.ensure(sizeof(float) * (size_t) n));
+    thr_summary_kernel<<<(unsigned) ((n + 255) / 256), 256, 0, ix->stream>>>(ix->thr.as<float>(), ix->n_user,
+                                                                            ix->n_sample, ix->thr_summ.as<float>());
+    RKR_CUDA(cudaGetLastError());
     return RKR_OK;
 }
 
@@ -151,11 +172,11 @@ int rkr_index_destroy(rkr_index *ix) {
     cudaSetDevice(ix->device);
     if (ix->stream) cudaStreamSynchronize(ix->stream);
     for (DevBuf *b : {&ix->user, &ix->item, &ix->item_sorted, &ix->item_norm, &ix->item_rnorm, &ix->user_rnorm,
-                      &ix->sample_rank, &ix->thr, &ix->reg_rank, &ix->reg, &ix->transfer_item, &ix->svd_user,
+                      &ix->sample_rank, &ix->thr, &ix->thr_summ, &ix->reg_rank, &ix->reg, &ix->transfer_item, &ix->svd_user,
                       &ix->svd_unorm, &ix->qip_state, &ix->ws_query, &ix->ws_qtr, &ix->ws_qnorm, &ix->ws_bucket,
                       &ix->ws_bucket2, &ix->ws_levels, &ix->ws_cls, &ix->ws_counts, &ix->ws_hist, &ix->ws_res,
                       &ix->ws_cand, &ix->ws_cand_off, &ix->ws_refine, &ix->ws_rank, &ix->ws_out, &ix->ws_stats,
-                      &ix->ws_misc})
+                      &ix->ws_misc, &ix->ws_fix})
         b->release();
     ix->prof.release();
     if (ix->stream) cudaStreamDestroy(ix->stream);
@@ -186,8 +207,9 @@ int rkr_index_load_sample_search(rkr_index *ix, const int32_t *sample_rank, int3
     RKR_CUDA(cudaMemcpyAsync(ix->sample_rank.p, sample_rank, sizeof(int32_t) * n_sample, cudaMemcpyHostToDevice, ix->stream));
     RKR_CUDA(cudaMemcpyAsync(ix->thr.p, thresholds, sizeof(float) * (size_t) ix->n_user * n_sample, cudaMemcpyHostToDevice,
                              ix->stream));
-    RKR_CUDA(cudaStreamSynchronize(ix->stream));
     ix->n_sample = n_sample;
+    RKR_TRY(thr_summary_build(ix));
+    RKR_CUDA(cudaStreamSynchronize(ix->stream));
     ix->h_sample_rank.assign(sample_rank, sample_rank + n_sample);
     return RKR_OK;
 }
@@ -211,9 +233,11 @@ int rkr_index_build_sample_search(rkr_index *ix, const int32_t *sample_rank, int
 int rkr_index_load_regression(rkr_index *ix, const int32_t *sample_rank, int32_t n_sample, const float *records) {
     RKR_REQUIRE(ix && sample_rank && records, "null argument");
     RKR_REQUIRE(n_sample > 0 && n_sample <= 0xfffd, "n_sample %d out of range", n_sample);
-    for (int j = 0; j < n_sample; j++)
+    for (int j = 0; j < n_sample; j++) {
         RKR_REQUIRE(sample_rank[j] >= 0 && sample_rank[j] <= ix->n_item, "regression sample rank %d out of range",
                     sample_rank[j]);
+        RKR_REQUIRE(j == 0 || sample_rank[j] >= sample_rank[j - 1], "regression sample ranks must be ascending");
+    }
     RKR_TRY(ensure_device(ix));
     std::vector<float> rec8((size_t) ix->n_user * 8, 0.0f);
     for (int64_t u = 0; u < ix->n_user; u++) std::memcpy(&rec8[u * 8], records + u * 7, 7 * sizeof(float));
@@ -253,7 +277,7 @@ int rkr_index_size_bytes(const rkr_index *ix, uint64_t *bytes) {
     RKR_REQUIRE(ix && bytes, "null argument");
     uint64_t s = 0;
     for (const DevBuf *b : {&ix->user, &ix->item, &ix->item_sorted, &ix->item_norm, &ix->item_rnorm, &ix->user_rnorm,
-                            &ix->sample_rank, &ix->thr, &ix->reg_rank, &ix->reg, &ix->transfer_item, &ix->svd_user,
+                            &ix->sample_rank, &ix->thr, &ix->thr_summ, &ix->reg_rank, &ix->reg, &ix->transfer_item, &ix->svd_user,
                             &ix->svd_unorm, &ix->qip_state})
         s += b->bytes;
     *bytes = s;

@@ -351,6 +351,7 @@ int build_sample_search(rkr_index *ix, const int32_t *sample_rank, int n_sample)
         sa.thr_out = ix->thr.as<float>() + u0 * n_sample;
         RKR_TRY(run_rows(P, u0, nu, sa));
     }
+    RKR_TRY(thr_summary_build(ix));
     RKR_CUDA(cudaStreamSynchronize(ix->stream));
     return RKR_OK;
 }

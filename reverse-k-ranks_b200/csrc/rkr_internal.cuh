@@ -189,6 +189,70 @@ __device__ __forceinline__ void big_load_stage(BigOperands &op, int buf, const f
     }
 }
 
+// Accumulates into acc (zeroed here) the thread's 8 x 8 block of dot products over [k_begin, k_end):
+// A rows a0 + 4 tx + {0..3, 64..67}, B rows b0 + 4 ty + {0..3, 64..67}.  Returns after a barrier,
+// with the operand buffers free.  Returns false (no barrier, acc zero) for an empty range.
+__device__ __forceinline__ bool big_accumulate(BigOperands &op, float acc[8][8], const float *__restrict__ A,
+                                              const int32_t *__restrict__ a_idx, int64_t n_a, int lda, int64_t a0,
+                                              const float *__restrict__ B, int64_t n_b, int ldb, int64_t b0, int k_begin,
+                                              int k_end) {
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] = 0.0f;
+    const int ns = (k_end - k_begin + kBigK - 1) / kBigK;
+    if (ns <= 0) return false;
+    big_load_stage(op, 0, A, a_idx, n_a, lda, a0, B, n_b, ldb, b0, k_begin, k_end);
+    cp_async_commit();
+    for (int s = 0; s < ns; s++) {
+        if (s + 1 < ns) {
+            big_load_stage(op, (s + 1) & 1, A, a_idx, n_a, lda, a0, B, n_b, ldb, b0, k_begin + (s + 1) * kBigK, k_end);
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const int buf = s & 1;
+#pragma unroll
+        for (int kk = 0; kk < kBigK; kk++) {
+            const float4 a_lo = *reinterpret_cast<const float4 *>(&op.a[buf][kk][4 * tx]);
+            const float4 a_hi = *reinterpret_cast<const float4 *>(&op.a[buf][kk][64 + 4 * tx]);
+            const float4 b_lo = *reinterpret_cast<const float4 *>(&op.b[buf][kk][4 * ty]);
+            const float4 b_hi = *reinterpret_cast<const float4 *>(&op.b[buf][kk][64 + 4 * ty]);
+            const float av[8] = {a_lo.x, a_lo.y, a_lo.z, a_lo.w, a_hi.x, a_hi.y, a_hi.z, a_hi.w};
+            const float bv[8] = {b_lo.x, b_lo.y, b_lo.z, b_lo.w, b_hi.x, b_hi.y, b_hi.z, b_hi.w};
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+#pragma unroll
+                for (int j = 0; j < 8; j++) acc[i][j] = __fadd_rn(acc[i][j], __fmul_rn(av[i], bv[j]));
+        }
+        __syncthreads();
+    }
+    return true;
+}
+
+// Writes (add = false) or adds with one binary32 rounding (add = true) the thread's block into res.
+__device__ __forceinline__ void big_store(BigResult &res, const float acc[8][8], bool add) {
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+    for (int j = 0; j < 8; j++) {
+        const int cb = (j < 4 ? 0 : 64) + 4 * ty + (j & 3);
+        float4 *lo = reinterpret_cast<float4 *>(&res.v[cb][4 * tx]);
+        float4 *hi = reinterpret_cast<float4 *>(&res.v[cb][64 + 4 * tx]);
+        float4 l = make_float4(acc[0][j], acc[1][j], acc[2][j], acc[3][j]);
+        float4 h = make_float4(acc[4][j], acc[5][j], acc[6][j], acc[7][j]);
+        if (add) {
+            const float4 l0 = *lo, h0 = *hi;
+            l = make_float4(__fadd_rn(l0.x, l.x), __fadd_rn(l0.y, l.y), __fadd_rn(l0.z, l.z), __fadd_rn(l0.w, l.w));
+            h = make_float4(__fadd_rn(h0.x, h.x), __fadd_rn(h0.y, h.y), __fadd_rn(h0.z, h.z), __fadd_rn(h0.w, h.w));
+        }
+        *lo = l;
+        *hi = h;
+    }
+}
+
 // Fills res with the 128 x 128 block of dot products (A rows a0.., B rows b0..) over [k_begin, k_end).
 __device__ __forceinline__ void exact_big_tile(char *smem, const float *__restrict__ A, const int32_t *__restrict__ a_idx,
                                               int64_t n_a, int lda, int64_t a0, const float *__restrict__ B,
@@ -263,6 +327,47 @@ __global__ void __launch_bounds__(kBigThreads, 2) exact_big_kernel(const float *
 
 template <class Epi>
 inline size_t big_kernel_smem() { return kBigSmem + Epi::kExtra; }
+
+// Split form: the block of partial sums over [0, k_split) goes to epi.finish_lo(extra, res, a0, b0),
+// then the sums over [k_split, k_end) -- each accumulated from 0, as the reference keeps a partial
+// score and its remainder apart -- are added to them with one rounding and epi.finish_hi sees the
+// totals.  Operands and result have separate shared memory, so the second range's loads do not
+// wait for finish_lo.  Epi also provides kExtra and prologue(extra, a0, b0).
+template <class Epi>
+__global__ void __launch_bounds__(kBigThreads, 2) exact_big_split_kernel(const float *__restrict__ A, int64_t n_a,
+                                                                         int lda, const float *__restrict__ B,
+                                                                         int64_t n_b, int ldb, int k_split, int k_end,
+                                                                         Epi epi) {
+    extern __shared__ __align__(16) char big_smem[];
+    BigOperands &op = *reinterpret_cast<BigOperands *>(big_smem);
+    BigResult &res = *reinterpret_cast<BigResult *>(big_smem + sizeof(BigOperands));
+    char *extra = big_smem + sizeof(BigOperands) + sizeof(BigResult);
+    const int64_t b0 = (int64_t) blockIdx.x * kBig;
+    const int64_t a0 = (int64_t) blockIdx.y * kBig;
+    epi.prologue(extra, a0, b0);
+    float acc[8][8];
+    big_accumulate(op, acc, A, nullptr, n_a, lda, a0, B, n_b, ldb, b0, 0, k_split);
+    big_store(res, acc, false);
+    __syncthreads();
+    epi.finish_lo(extra, res, a0, b0);
+    // big_accumulate's first barrier orders finish_lo's reads of res before the adds below
+    if (!big_accumulate(op, acc, A, nullptr, n_a, lda, a0, B, n_b, ldb, b0, k_split, k_end)) __syncthreads();
+    big_store(res, acc, true);
+    __syncthreads();
+    epi.finish_hi(extra, res, a0, b0);
+}
+
+template <class Epi>
+inline cudaError_t launch_big_split(const float *A, int64_t n_a, int lda, const float *B, int64_t n_b, int ldb,
+                                    int k_split, int k_end, const Epi &epi, cudaStream_t st) {
+    const size_t smem = sizeof(BigOperands) + sizeof(BigResult) + Epi::kExtra;
+    cudaError_t e =
+        cudaFuncSetAttribute(exact_big_split_kernel<Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    if (e != cudaSuccess) return e;
+    dim3 grid((unsigned) ((n_b + kBig - 1) / kBig), (unsigned) ((n_a + kBig - 1) / kBig));
+    exact_big_split_kernel<Epi><<<grid, kBigThreads, smem, st>>>(A, n_a, lda, B, n_b, ldb, k_split, k_end, epi);
+    return cudaGetLastError();
+}
 
 // Launches exact_big_kernel<Epi> over n_a x n_b pairs on stream st.
 template <class Epi>
@@ -626,6 +731,7 @@ struct rkr_index {
     int n_sample = 0;
     rkr::DevBuf sample_rank;   // [n_sample]
     rkr::DevBuf thr;           // [n_user][n_sample]
+    rkr::DevBuf thr_summ;      // [n_user][ThrSummary::kMaxGroups]: last (smallest) threshold of each group
     std::vector<int32_t> h_sample_rank;
     // NormalLinearRegressionLP
     int n_sample_reg = 0;
@@ -639,7 +745,7 @@ struct rkr_index {
     rkr::DevBuf qip_state;     // [n_user], QSRPNormalLP's carried query scores
     // per-call workspace
     rkr::DevBuf ws_query, ws_qtr, ws_qnorm, ws_bucket, ws_bucket2, ws_levels, ws_cls, ws_counts, ws_hist;
-    rkr::DevBuf ws_res, ws_cand, ws_cand_off, ws_refine, ws_rank, ws_out, ws_stats, ws_misc;
+    rkr::DevBuf ws_res, ws_cand, ws_cand_off, ws_refine, ws_rank, ws_out, ws_stats, ws_misc, ws_fix;
     std::vector<uint8_t> h_scratch;
     rkr::Profiler prof;
 };
@@ -685,6 +791,7 @@ inline int run_compaction(rkr_index *ix, P p, int nq, int topk, QueryCounts *cou
 }
 
 int ensure_device(const rkr_index *ix);
+int thr_summary_build(rkr_index *ix);
 int refine_prepare_norms(rkr_index *ix);
 int query_batch(rkr_index *ix, int method, const float *d_query, int n_query, int topk, rkr_user_rank *d_out,
                 rkr_query_stats *d_stats, cudaStream_t st);

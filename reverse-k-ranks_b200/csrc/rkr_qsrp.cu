@@ -6,10 +6,18 @@
 //      (NormalLinearRegressionLP::ComputeRankBound, NormalLinearRegressionLP.hpp:326-398) -> prune.
 //   2. full SVD-space score for the survivors (ComputeRemainDim, :76-95) -> sampled-threshold
 //      bounds (SampleSearch::RankBound) -> prune again.
-// Here each round is one pass over all (user, query) pairs of the batch.  The reference keeps its
-// per-user score vector across queries; users accepted in round 1 are reported with whatever that
-// vector holds for them.  The batch reproduces it: the score a user had at its latest earlier query
-// in which it reached round 2, or the index's carried state when there is none.
+// Here a batch of queries runs as passes over all (query, user) pairs:
+//   * one tile kernel computes, for every pair, the partial score, its round-1 levels and the full
+//     score (partial + remainder, two separately accumulated sums added once, as the reference adds
+//     them);
+//   * round 2 is a streaming pass that gives each surviving pair the coarse group of its sampled-
+//     threshold bucket from a per-user summary held in shared memory;
+//   * the exact bucket is resolved only where the k-th bound and the class counts need it: for the
+//     pairs in the critical group(s) of each query, and for the users that end up reported.
+// The reference keeps its per-user score vector across queries; users accepted in round 1 are
+// reported with whatever that vector holds for them.  The batch reproduces it: the score a user had
+// at its latest earlier query in which it reached round 2, or the index's carried state when there
+// is none.
 #include <algorithm>
 #include <vector>
 
@@ -54,6 +62,23 @@ __device__ __forceinline__ float cdf_phi(float x) {
     return __double2float_rn(__dmul_rn(0.5, __dadd_rn(1.0, (double) __fmul_rn((float) sign, y))));
 }
 
+// The same formula in binary32 with the hardware reciprocal and exponential, for screening.
+// Against cdf_phi, with z given as (q - mu) * (1 / sigma) instead of (q - mu) / sigma, it differs
+// by less than kCdfFastErr: the argument and x differ by a few ulps (< 1e-7 after the slope of
+// the CDF), t by a few ulps (< 4e-7 on pt * e), the fused polynomial and the approximate exp by a
+// few ulps more (< 3e-7), and the closing steps by one rounding each.
+constexpr float kCdfFastErr = 2.0e-6f;
+
+__device__ __forceinline__ float cdf_phi_fast(float z) {
+    const float a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f;
+    const float a4 = -1.453152027f, a5 = 1.061405429f, p = 0.3275911f;
+    const float x = fabsf(z) * 0.70710677f;
+    const float t = __fdividef(1.0f, fmaf(p, x, 1.0f));
+    const float pt = fmaf(fmaf(fmaf(fmaf(a5, t, a4), t, a3), t, a2), t, a1) * t;
+    const float y = fmaf(-pt, __expf(-x * x), 1.0f);
+    return fmaf(z < 0.0f ? -0.5f : 0.5f, y, 0.5f);
+}
+
 struct RegModel {           // device view of the regression index
     const float *rec;       // [n_user][8]
     const int32_t *rank;    // [S]
@@ -62,82 +87,119 @@ struct RegModel {           // device view of the regression index
     int n_item;
 };
 
-// The same CDF with every step in binary32 and expf: within 1e-6 of cdf_phi for every input
-// (the two differ only in where the last bits of t, the product and the closing sum are rounded).
-__device__ __forceinline__ float cdf_phi_f32(float x) {
-    const float a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f;
-    const float a4 = -1.453152027f, a5 = 1.061405429f, p = 0.3275911f;
-    const float sign = x < 0 ? -1.0f : 1.0f;
-    x = __fdiv_rn(fabsf(x), __int_as_float(0x3fb504f3));
-    const float t = __fdiv_rn(1.0f, __fadd_rn(1.0f, __fmul_rn(p, x)));
-    const float pt = (((((a5 * t + a4) * t) + a3) * t + a2) * t + a1) * t;
-    const float y = 1.0f - pt * expf(-x * x);
-    return 0.5f * (1.0f + sign * y);
-}
-
-// The reference's float/double evaluation of one side of ComputeRankBound's index arithmetic
-// (kept out of line: the float screen below rarely needs it).
-__device__ __noinline__ int64_t regression_index_exact(float nx, float a, float b, float err, bool upper) {
+// The reference's float/double evaluation of one side of ComputeRankBound's index arithmetic:
+// pr = ceil(pred + err) (upper = 0) or floor(pred - err) (upper = 1), pred = cdf(nx) * a + b.
+__device__ __forceinline__ int64_t regression_index_exact(float nx, float a, float b, float err, bool upper) {
     const float ix = cdf_phi(nx);
     const float pred = __fadd_rn(__fmul_rn(ix, a), b);
     return upper ? f2i64_x86(floorf(__fsub_rn(pred, err))) : f2i64_x86(ceilf(__fadd_rn(pred, err)));
 }
 
-// One side of ComputeRankBound's index arithmetic: pr = ceil(pred + err) (upper = 0) or
-// floor(pred - err) (upper = 1), pred = cdf(nx) * a + b.  The float-only CDF decides it whenever
-// pred -+ err lies farther from an integer than that CDF's error can move it (|a| * 4e-6 plus a
-// few ulps of the sum); otherwise the reference's own float/double evaluation decides.
-__device__ __forceinline__ int64_t regression_index(float nx, float a, float b, float err, bool upper) {
-    const float ixf = cdf_phi_f32(nx);
-    const float vf = upper ? __fsub_rn(__fadd_rn(__fmul_rn(ixf, a), b), err) : __fadd_rn(__fadd_rn(__fmul_rn(ixf, a), b), err);
-    const float margin = fabsf(a) * 4e-6f + 8.0f * fabsf(vf) * 1.2e-7f + 1e-6f;
-    const float r = rintf(vf);
-    if (isfinite(vf) && fabsf(vf - r) > margin) return (int64_t) (upper ? floorf(vf) : ceilf(vf));
-    return regression_index_exact(nx, a, b, err, upper);
-}
-
-// ComputeRankBound (:326-380), returning levels: 0 -> rank 0, j + 1 -> rank[j], S + 1 -> n_item.
-// r0 = (a, b, mu, sigma), r1 = (err, smax, smin, -) is the user's model record.
-__device__ __forceinline__ void regression_levels_rec(const RegModel &m, float4 r0, float4 r1, float qlb, float qub,
-                                                      int &lvl_lb, int &lvl_ub) {
+// ComputeRankBound (:326-380) with the reference's arithmetic, returning levels: 0 -> rank 0,
+// j + 1 -> rank[j], S + 1 -> n_item.
+__device__ __noinline__ void regression_levels_exact(const RegModel &m, int64_t u, float qlb, float qub, int &lvl_lb,
+                                                     int &lvl_ub) {
+    const float4 r0 = __ldg(reinterpret_cast<const float4 *>(m.rec + u * 8));
+    const float4 r1 = __ldg(reinterpret_cast<const float4 *>(m.rec + u * 8 + 4));
     const float a = r0.x, b = r0.y, mu = r0.z, sigma = r0.w, err = r1.x, smax = r1.y, smin = r1.z;
     const int S = m.S;
     if (qlb > smax) lvl_lb = 1;
     else if (qlb < smin) lvl_lb = S + 1;
     else if ((double) err >= m.err_cap) lvl_lb = S + 1;
     else {
-        const int64_t pr = regression_index(__fdiv_rn(__fsub_rn(qlb, mu), sigma), a, b, err, false);
+        const int64_t pr = regression_index_exact(__fdiv_rn(__fsub_rn(qlb, mu), sigma), a, b, err, false);
         lvl_lb = pr >= S ? S + 1 : (pr < 0 ? 1 : (int) pr + 1);
     }
     if (qub > smax) lvl_ub = 0;
     else if (qub < smin) lvl_ub = S;
     else if ((double) err >= m.err_cap) lvl_ub = 0;
     else {
-        const int64_t pr = regression_index(__fdiv_rn(__fsub_rn(qub, mu), sigma), a, b, err, true);
+        const int64_t pr = regression_index_exact(__fdiv_rn(__fsub_rn(qub, mu), sigma), a, b, err, true);
         lvl_ub = pr >= S ? S + 1 : (pr < 0 ? 0 : (int) pr + 1);
     }
 }
 
-__device__ __forceinline__ void regression_levels(const RegModel &m, int64_t u, float qlb, float qub, int &lvl_lb,
-                                                  int &lvl_ub) {
-    regression_levels_rec(m, __ldg(reinterpret_cast<const float4 *>(m.rec + u * 8)),
-                          __ldg(reinterpret_cast<const float4 *>(m.rec + u * 8 + 4)), qlb, qub, lvl_lb, lvl_ub);
+// One user's model prepared for the screen.
+struct RegUser {
+    float a, b, mu, inv_sigma, err, smax, smin, margin;
+    bool err_big;
+};
+
+__device__ __forceinline__ RegUser reg_user(const RegModel &m, int64_t u) {
+    const float4 r0 = __ldg(reinterpret_cast<const float4 *>(m.rec + u * 8));
+    const float4 r1 = __ldg(reinterpret_cast<const float4 *>(m.rec + u * 8 + 4));
+    RegUser r;
+    r.a = r0.x; r.b = r0.y; r.mu = r0.z; r.inv_sigma = __frcp_rn(r0.w);
+    r.err = r1.x; r.smax = r1.y; r.smin = r1.z;
+    r.err_big = (double) r1.x >= m.err_cap;
+    // |pred -+ err| moves by at most |a| * kCdfFastErr through the CDF, plus a few roundings of
+    // values no larger than |a| + |b| + |err| in either evaluation.
+    r.margin = fabsf(r.a) * kCdfFastErr + (fabsf(r.a) + fabsf(r.b) + fabsf(r.err)) * 4.8e-7f + 1e-6f;
+    return r;
+}
+
+// Screened ComputeRankBound: the fast CDF decides a side whenever pred -+ err lies farther than
+// the margin from an integer, so that the reference's ceil / floor cannot differ.  Returns false
+// when a side is undecided (its level is then not meaningful).
+__device__ __forceinline__ bool regression_levels_fast(const RegUser &r, int S, float qlb, float qub, int &lvl_lb,
+                                                       int &lvl_ub) {
+    bool ok = true;
+    if (qlb > r.smax) lvl_lb = 1;
+    else if (qlb < r.smin || r.err_big) lvl_lb = S + 1;
+    else {
+        const float v = fmaf(cdf_phi_fast(__fsub_rn(qlb, r.mu) * r.inv_sigma), r.a, r.b) + r.err;
+        ok = fabsf(v - rintf(v)) > r.margin && fabsf(v) < 1e18f;
+        const int64_t pr = ok ? (int64_t) ceilf(v) : 0;
+        lvl_lb = pr >= S ? S + 1 : (pr < 0 ? 1 : (int) pr + 1);
+    }
+    if (qub > r.smax) lvl_ub = 0;
+    else if (qub < r.smin) lvl_ub = S;
+    else if (r.err_big) lvl_ub = 0;
+    else {
+        const float v = fmaf(cdf_phi_fast(__fsub_rn(qub, r.mu) * r.inv_sigma), r.a, r.b) - r.err;
+        const bool ok2 = fabsf(v - rintf(v)) > r.margin && fabsf(v) < 1e18f;
+        const int64_t pr = ok2 ? (int64_t) floorf(v) : 0;
+        lvl_ub = pr >= S ? S + 1 : (pr < 0 ? 0 : (int) pr + 1);
+        ok = ok && ok2;
+    }
+    return ok;
 }
 
 __device__ __forceinline__ int level_rank(int lvl, const int32_t *rank, int S, int n_item) {
     return lvl == 0 ? 0 : (lvl > S ? n_item : rank[lvl - 1]);
 }
 
-// ---- kernels ---------------------------------------------------------------------------------------
+// ---- per-query state ---------------------------------------------------------------------------------
 
-constexpr uint16_t kStateResult1 = 0xfffe, kStatePruned1 = 0xffff;
+// Round-2 codes per pair: 0..nb a coarse threshold group (nb: bucket S); otherwise the round-1 state.
+constexpr uint8_t kCodeResult1 = 0xfe, kCodePruned1 = 0xff;
+constexpr uint8_t kClsMixed = 0xff;  // a group whose buckets fall in more than one class
 
 struct QsrpParams {
-    int32_t mode1, all1, L1, U1;         // round 1: equal-bounds mode, "all survivors accepted", k-th bounds
-    int32_t n_res1, n_pr1, n_ref1, skip2; // round-1 counts; skip2: round 1 already produced top-k results
-    int32_t mode2, all2, L2, U2;         // round 2
-    int32_t n_elig2, pad0, pad1, pad2;
+    int32_t mode1, all1, L1, U1;           // round 1: equal-bounds mode, "all survivors accepted", k-th bounds
+    int32_t n_res1, n_pr1, n_ref1, skip2;  // round-1 counts; skip2: round 1 already produced top-k results
+    int32_t mode2, L2, U2, n_elig2;        // round 2
+    int32_t exact1, lv_res, lv_pr, lv_m1;  // exact1: count round-1 classes pair by pair; level thresholds
+    int32_t crit, cum_before, mask1, mask2;  // critical coarse group, users below it, groups to resolve
 };
+
+// Round-1 class in level space: rank(level) is non-decreasing in the level, so lb <= U1 is
+// lvl_lb <= lv_res, L1 <= ub is lvl_ub >= lv_pr and the equal-bounds test is a test against lv_m1.
+__device__ __forceinline__ int class1_lv(const QsrpParams &p, int l, int h) {
+    if (p.mode1) return (h <= p.lv_m1 && l <= p.lv_m1) ? kClsResult : kClsIdle;
+    if (l <= p.lv_res) return kClsResult;
+    if (h >= p.lv_pr) return kClsPrune;
+    return p.all1 ? kClsResult : kClsRefine;
+}
+
+__device__ __forceinline__ int class1_of(const QsrpParams &p, int lb, int ub) {
+    if (p.mode1) return (ub <= p.L1 && lb <= p.L1) ? kClsResult : kClsIdle;
+    if (lb <= p.U1) return kClsResult;
+    if (p.L1 <= ub) return kClsPrune;
+    return p.all1 ? kClsResult : kClsRefine;
+}
+
+// ---- round 1 + full scores -------------------------------------------------------------------------
 
 // SVD::TransferQuery (SVD.hpp:156-164) and the query's remaining-dims norm (PartDimPartNorm.hpp:56-57).
 __global__ void transfer_query_kernel(const float *__restrict__ query, const float *__restrict__ transfer, int dim,
@@ -154,35 +216,83 @@ __global__ void transfer_query_kernel(const float *__restrict__ query, const flo
     }
 }
 
-// Round 1 for every pair: left = InnerProduct(svd_user, qtr, check_dim) (kept for round 2);
-// bounds left -+ norms; regression levels of both bounds packed as (lb | ub << 16).
-__global__ void __launch_bounds__(kTileThreads) qsrp_round1_kernel(const float *__restrict__ svd_user, int64_t n_user,
-                                                                  int dim, const float *__restrict__ unorm,
-                                                                  const float *__restrict__ qtr,
-                                                                  const float *__restrict__ qnorm, int n_query,
-                                                                  int check_dim, RegModel m, uint32_t *__restrict__ lv,
-                                                                  float *__restrict__ left) {
-    __shared__ TileSmem sm;
-    const int64_t b0 = (int64_t) blockIdx.x * kTile;
-    const int64_t a0 = (int64_t) blockIdx.y * kTile;
-    float lo[4][4], hi[4][4];
-    exact_tile(sm, svd_user, nullptr, n_user, dim, a0, qtr, n_query, dim, b0, 0, check_dim, check_dim, lo, hi);
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const int64_t u = a0 + 4 * tx + i;
-        if (u >= n_user) continue;
+// Pairs the screen left undecided, resolved by qsrp_fix1_kernel: (query, user, partial score).
+struct FixList {
+    int4 *e;
+    int *count;
+    int cap;
+};
+
+// Tiles of 128 users x 128 queries: the partial score over the first check_dim coordinates, the
+// bounds partial -+ norms and their regression levels (lb | ub << 16), then the full score.
+struct Round1Epi {
+    static constexpr size_t kExtra = sizeof(float) * kBig;
+    const float *unorm, *qnorm;
+    RegModel m;
+    uint32_t *lv;
+    float *qip;
+    int64_t n_user, n_query;
+    FixList fix;
+    __device__ void prologue(char *x, int64_t, int64_t b0) const {
+        float *qn = reinterpret_cast<float *>(x);
+        if (threadIdx.x < kBig) qn[threadIdx.x] = b0 + threadIdx.x < n_query ? __ldg(qnorm + b0 + threadIdx.x) : 0.0f;
+    }
+    __device__ void finish_lo(char *x, const BigResult &res, int64_t a0, int64_t b0) const {
+        const float *qn = reinterpret_cast<const float *>(x);
+        const int ra = threadIdx.x & (kBig - 1), half = threadIdx.x >> 7, lane = threadIdx.x & 31;
+        const int64_t u = a0 + ra;
+        const unsigned alive = __ballot_sync(0xffffffffu, u < n_user);
+        if (u >= n_user) return;
+        const RegUser r = reg_user(m, u);
         const float un = __ldg(unorm + u);
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int64_t q = b0 + 4 * ty + j;
-            if (q >= n_query) continue;
-            const float right = __fmul_rn(un, __ldg(qnorm + q));
+        for (int i = 0; i < kBig / 2; i++) {
+            const int rb = half + 2 * i;
+            const int64_t q = b0 + rb;
+            if (q >= n_query) break;
+            const float left = res.v[rb][ra];
+            const float right = __fmul_rn(un, qn[rb]);
             int l, h;
-            regression_levels(m, u, __fsub_rn(lo[i][j], right), __fadd_rn(lo[i][j], right), l, h);
+            const bool ok = regression_levels_fast(r, m.S, __fsub_rn(left, right), __fadd_rn(left, right), l, h);
+            const unsigned need = __ballot_sync(alive, !ok);
+            if (need) {
+                const int leader = __ffs(need) - 1;
+                int base = 0;
+                if (lane == leader) base = atomicAdd(fix.count, __popc(need));
+                base = __shfl_sync(alive, base, leader);
+                if (!ok) {
+                    const int idx = base + __popc(need & ((1u << lane) - 1));
+                    if (idx < fix.cap) fix.e[idx] = make_int4((int) q, (int) u, __float_as_int(left), 0);
+                    else regression_levels_exact(m, u, __fsub_rn(left, right), __fadd_rn(left, right), l, h);
+                }
+            }
             lv[q * n_user + u] = (uint32_t) l | ((uint32_t) h << 16);
-            left[q * n_user + u] = lo[i][j];
         }
+    }
+    __device__ void finish_hi(char *, const BigResult &res, int64_t a0, int64_t b0) const {
+        const int ra = threadIdx.x & (kBig - 1), half = threadIdx.x >> 7;
+        const int64_t u = a0 + ra;
+        if (u >= n_user) return;
+        for (int i = 0; i < kBig / 2; i++) {
+            const int rb = half + 2 * i;
+            const int64_t q = b0 + rb;
+            if (q >= n_query) break;
+            qip[q * n_user + u] = res.v[rb][ra];
+        }
+    }
+};
+
+// The reference's arithmetic for the pairs the screen left undecided (listed ones; pairs beyond
+// the list's capacity were resolved in place).
+__global__ void qsrp_fix1_kernel(FixList fix, RegModel m, const float *__restrict__ unorm,
+                                 const float *__restrict__ qnorm, int64_t n_user, uint32_t *__restrict__ lv) {
+    const int n = min(*fix.count, fix.cap);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int4 e = fix.e[i];
+        const float left = __int_as_float(e.z);
+        const float right = __fmul_rn(__ldg(unorm + e.y), __ldg(qnorm + e.x));
+        int l, h;
+        regression_levels_exact(m, e.y, __fsub_rn(left, right), __fadd_rn(left, right), l, h);
+        lv[(int64_t) e.x * n_user + e.y] = (uint32_t) l | ((uint32_t) h << 16);
     }
 }
 
@@ -224,39 +334,6 @@ __global__ void __launch_bounds__(kHistThreads) level_hist_kernel(const uint32_t
     if (threadIdx.x == 0 && anom) atomicAdd(anomaly + q, anom);
 }
 
-// Round 1 on 128 x 128 tiles (users x queries): left over the first check_dim coordinates, the
-// bounds left -+ norms and their regression levels.
-struct Round1Epi {
-    static constexpr size_t kExtra = 0;
-    const float *unorm, *qnorm;
-    RegModel m;
-    uint32_t *lv;
-    float *left;
-    int64_t n_user, n_query;
-    __device__ void prologue(char *, int64_t, int64_t) const {}
-    __device__ bool active(char *, int64_t, int64_t) const { return true; }
-    __device__ void finish(char *, const BigResult &res, int64_t a0, int64_t b0, bool) const {
-        const int ra = threadIdx.x & (kBig - 1), half = threadIdx.x >> 7;
-        const int64_t u = a0 + ra;
-        if (u >= n_user) return;
-        const float4 r0 = __ldg(reinterpret_cast<const float4 *>(m.rec + u * 8));
-        const float4 r1 = __ldg(reinterpret_cast<const float4 *>(m.rec + u * 8 + 4));
-        const float un = __ldg(unorm + u);
-#pragma unroll 2
-        for (int i = 0; i < kBig / 2; i++) {
-            const int rb = half + 2 * i;
-            const int64_t q = b0 + rb;
-            if (q >= n_query) break;
-            const float v = res.v[rb][ra];
-            const float right = __fmul_rn(un, __ldg(qnorm + q));
-            int l, h;
-            regression_levels_rec(m, r0, r1, __fsub_rn(v, right), __fadd_rn(v, right), l, h);
-            lv[q * n_user + u] = (uint32_t) l | ((uint32_t) h << 16);
-            left[q * n_user + u] = v;
-        }
-    }
-};
-
 // Round-1 k-th smallest bounds per query (PruneCandidateByBound.hpp:36-77 with nothing excluded)
 // and the class counts.  While every pair has ub <= lb, a result (lb <= U*) and a prune
 // (ub >= L*) cannot coincide unless L* == U*, so the counts follow from the two histograms;
@@ -277,14 +354,21 @@ __global__ void qsrp_select1_kernel(const int *__restrict__ hist_all, const int 
     p.L1 = level_rank(kl, rank, S, n_item);
     p.U1 = level_rank(kh, rank, S, n_item);
     p.mode1 = p.L1 == p.U1;
+    p.lv_res = -1; p.lv_pr = nl; p.lv_m1 = -1;
+    for (int l = 0; l < nl; l++) {
+        const int rl = level_rank(l, rank, S, n_item);
+        if (rl <= p.U1) p.lv_res = l;
+        if (rl <= p.L1) p.lv_m1 = l;
+        if (rl >= p.L1 && p.lv_pr == nl) p.lv_pr = l;
+    }
     if (!p.mode1) {
         if (anomaly[q]) {
-            p.pad0 = 1;  // exact counting needed
+            p.exact1 = 1;
         } else {
             int64_t nres = 0, npr = 0;
             for (int b = 0; b < nl; b++) {
-                if (level_rank(b, rank, S, n_item) <= p.U1) nres += h[b];
-                if (level_rank(b, rank, S, n_item) >= p.L1) npr += h[nl + b];
+                if (b <= p.lv_res) nres += h[b];
+                if (b >= p.lv_pr) npr += h[nl + b];
             }
             p.n_res1 = (int) nres;
             p.n_pr1 = (int) npr;
@@ -294,20 +378,12 @@ __global__ void qsrp_select1_kernel(const int *__restrict__ hist_all, const int 
     par[q] = p;
 }
 
-__device__ __forceinline__ int class1_of(const QsrpParams &p, int lb, int ub) {
-    if (p.mode1) return (ub <= p.L1 && lb <= p.L1) ? kClsResult : kClsIdle;
-    if (lb <= p.U1) return kClsResult;
-    if (p.L1 <= ub) return kClsPrune;
-    return p.all1 ? kClsResult : kClsRefine;
-}
-
 // Round-1 class counts pair by pair (the reduction at PruneCandidateByBound.hpp:115-136), for
 // queries where the histogram shortcut does not apply.
-__global__ void qsrp_count1_kernel(const uint32_t *__restrict__ lv, int64_t n_user, const int32_t *__restrict__ rank,
-                                   int S, int n_item, QsrpParams *__restrict__ par) {
+__global__ void qsrp_count1_kernel(const uint32_t *__restrict__ lv, int64_t n_user, QsrpParams *__restrict__ par) {
     const int q = blockIdx.y;
     const QsrpParams p = par[q];
-    if (p.mode1 || !p.pad0) return;
+    if (p.mode1 || !p.exact1) return;
     __shared__ int cnt[3];
     if (threadIdx.x < 3) cnt[threadIdx.x] = 0;
     __syncthreads();
@@ -315,7 +391,7 @@ __global__ void qsrp_count1_kernel(const uint32_t *__restrict__ lv, int64_t n_us
     const uint32_t *row = lv + (int64_t) q * n_user;
     for (int64_t u = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; u < n_user; u += (int64_t) gridDim.x * blockDim.x) {
         const uint32_t v = row[u];
-        const int k = class1_of(p, level_rank(v & 0xffff, rank, S, n_item), level_rank(v >> 16, rank, S, n_item));
+        const int k = class1_lv(p, v & 0xffff, v >> 16);
         c[k == kClsResult ? 0 : (k == kClsPrune ? 1 : 2)]++;
     }
     for (int i = 0; i < 3; i++) {
@@ -350,171 +426,101 @@ __global__ void qsrp_final1_kernel(QsrpParams *__restrict__ par, int nq, int top
     par[q] = p;
 }
 
-// Does the pair reach round 2 (neither pruned nor accepted in round 1)?
-__device__ __forceinline__ bool eligible2(const QsrpParams &p, uint32_t v, const int32_t *rank, int S, int n_item) {
-    const int k = class1_of(p, level_rank(v & 0xffff, rank, S, n_item), level_rank(v >> 16, rank, S, n_item));
-    return k == kClsRefine || k == kClsIdle;
+// ---- round 2 -------------------------------------------------------------------------------------
+
+// Number of groups whose last (smallest) threshold is >= s: the coarse group of s's bucket.
+__device__ __forceinline__ int coarse_group(const float *summ, int nb, float s) {
+    int lo = 0, len = nb;
+    while (len > 0) {
+        const int h = len >> 1, m = lo + h;
+        if (summ[m] >= s) { lo = m + 1; len -= h + 1; } else len = h;
+    }
+    return lo;
 }
 
-// Round 2: full SVD-space score of each surviving pair, left (round 1) + the remaining dims
-// (ComputeRemainDim, PartDimPartNorm.hpp:76-95), and its sampled-threshold bucket.  Pairs that did
-// not reach round 2 get a state code instead: kStateResult1 (accepted in round 1) or kStatePruned1.
-__global__ void __launch_bounds__(kTileThreads, 3) qsrp_round2_kernel(const float *__restrict__ svd_user, int64_t n_user,
-                                                                  int dim, const float *__restrict__ qtr, int n_query,
-                                                                  int check_dim, const uint32_t *__restrict__ lv,
-                                                                  const float *__restrict__ left,
-                                                                  const QsrpParams *__restrict__ par,
-                                                                  const int32_t *reg_rank, int S_reg,
-                                                                  int n_item, const float *__restrict__ thr, int S,
-                                                                  uint16_t *__restrict__ bucket2) {
-    __shared__ TileSmem sm;
-    __shared__ ThrSummary ts;
-    __shared__ QsrpParams par_s[kTile];
-    extern __shared__ int32_t rank_s[];  // the regression model's sample ranks
-    const int64_t b0 = (int64_t) blockIdx.x * kTile;
-    const int64_t a0 = (int64_t) blockIdx.y * kTile;
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    if (threadIdx.x < kTile && b0 + threadIdx.x < n_query) par_s[threadIdx.x] = par[b0 + threadIdx.x];
-    for (int i = threadIdx.x; i < S_reg; i += blockDim.x) rank_s[i] = reg_rank[i];
+// The bucket of s inside coarse group g (< nb): g * gs + the group's thresholds >= s.
+__device__ __forceinline__ int fine_bucket(const float *__restrict__ row, int S, int gs, int g, float s) {
+    const int base = g * gs, end = min(base + gs, S);
+    int c = 0;
+    if ((gs & 15) == 0 && end - base == gs && (S & 3) == 0) {
+        const float4 *p = reinterpret_cast<const float4 *>(row + base);
+        for (int t = 0; t < gs / 16; t++, p += 4) {
+            const float4 x0 = __ldg(p), x1 = __ldg(p + 1), x2 = __ldg(p + 2), x3 = __ldg(p + 3);
+            c += (x0.x >= s) + (x0.y >= s) + (x0.z >= s) + (x0.w >= s) + (x1.x >= s) + (x1.y >= s) + (x1.z >= s) +
+                 (x1.w >= s) + (x2.x >= s) + (x2.y >= s) + (x2.z >= s) + (x2.w >= s) + (x3.x >= s) + (x3.y >= s) +
+                 (x3.z >= s) + (x3.w >= s);
+        }
+    } else {
+        for (int i = base; i < end; i++) c += __ldg(row + i) >= s;
+    }
+    return base + c;
+}
+
+constexpr int kScreenUsers = 256, kScreenQueries = 256;
+
+// Round 2 for a block of 256 users x up to 256 queries: pairs that reached round 2 (neither pruned
+// nor accepted in round 1) get the coarse group of their full score's bucket, the others their
+// round-1 state code.  The users' group summaries stay in shared memory.
+__global__ void __launch_bounds__(kScreenUsers) qsrp_screen2_kernel(const uint32_t *__restrict__ lv,
+                                                                   const float *__restrict__ qip, int64_t n_user, int nq,
+                                                                   const QsrpParams *__restrict__ par,
+                                                                   const float *__restrict__ thr_summ, int nb,
+                                                                   uint8_t *__restrict__ code) {
+    __shared__ float summ[kScreenUsers][ThrSummary::kMaxGroups + 1];
+    __shared__ int4 pp[kScreenQueries];
+    const int64_t u0 = (int64_t) blockIdx.x * kScreenUsers;
+    const int q0 = blockIdx.y * kScreenQueries, nqc = min(kScreenQueries, nq - q0);
+    for (int idx = threadIdx.x; idx < kScreenUsers * ThrSummary::kMaxGroups; idx += kScreenUsers) {
+        const int r = idx / ThrSummary::kMaxGroups, j = idx % ThrSummary::kMaxGroups;
+        const int64_t u = u0 + r;
+        summ[r][j] = u < n_user ? __ldg(thr_summ + u * ThrSummary::kMaxGroups + j) : 0.0f;
+    }
+    for (int i = threadIdx.x; i < nqc; i += kScreenUsers) {
+        const QsrpParams &p = par[q0 + i];
+        pp[i] = make_int4(p.mode1 | (p.all1 << 1), p.lv_res, p.lv_pr, p.lv_m1);
+    }
     __syncthreads();
-    reg_rank = rank_s;
-    uint32_t el = 0, r1 = 0;  // bit 4*i + j: reached round 2 / accepted in round 1
+    const int64_t u = u0 + threadIdx.x;
+    if (u >= n_user) return;
+    const float *sm = summ[threadIdx.x];
+    // four queries at a time: their level loads, then the score loads of the survivors, are in flight together
+    constexpr int G = 4;
+    for (int i0 = 0; i0 < nqc; i0 += G) {
+        uint32_t v[G];
+        int k[G];
+        float s[G];
 #pragma unroll
-    for (int i = 0; i < 4; i++)
+        for (int g = 0; g < G; g++) v[g] = i0 + g < nqc ? __ldg(lv + (int64_t) (q0 + i0 + g) * n_user + u) : 0u;
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int64_t u = a0 + 4 * tx + i, q = b0 + 4 * ty + j;
-            if (u < n_user && q < n_query) {
-                const uint32_t v = lv[q * n_user + u];
-                const int k = class1_of(par_s[4 * ty + j], level_rank(v & 0xffff, reg_rank, S_reg, n_item),
-                                        level_rank(v >> 16, reg_rank, S_reg, n_item));
-                if (k == kClsRefine || k == kClsIdle) el |= 1u << (4 * i + j);
-                else if (k == kClsResult) r1 |= 1u << (4 * i + j);
-            }
+        for (int g = 0; g < G; g++) {
+            const int4 c = pp[min(i0 + g, nqc - 1)];
+            QsrpParams p;
+            p.mode1 = c.x & 1; p.all1 = c.x >> 1; p.lv_res = c.y; p.lv_pr = c.z; p.lv_m1 = c.w;
+            k[g] = class1_lv(p, v[g] & 0xffff, v[g] >> 16);
+            const bool el = i0 + g < nqc && (k[g] == kClsRefine || k[g] == kClsIdle);
+            s[g] = el ? __ldg(qip + (int64_t) (q0 + i0 + g) * n_user + u) : 0.0f;
+            if (!el && k[g] != kClsResult) k[g] = kClsPrune;
         }
-    const bool any = __syncthreads_or(el != 0);
-    float lo[4][4], hi[4][4];
-    if (any) {
-        load_thr_summary(ts, thr, n_user, a0, S);
-        exact_tile(sm, svd_user, nullptr, n_user, dim, a0, qtr, n_query, dim, b0, check_dim, dim, dim, lo, hi);
-    }
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const int64_t u = a0 + 4 * tx + i;
-        if (u >= n_user) continue;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int64_t q = b0 + 4 * ty + j;
-            if (q >= n_query) continue;
-            uint16_t b = (r1 >> (4 * i + j) & 1) ? kStateResult1 : kStatePruned1;
-            if (el >> (4 * i + j) & 1) {
-                const float qip = __fadd_rn(left[q * n_user + u], lo[i][j]);
-                b = (uint16_t) bucket_of_2level(ts.v[4 * tx + i], thr + u * S, S, qip);
-            }
-            bucket2[q * n_user + u] = b;
+        for (int g = 0; g < G; g++) {
+            if (i0 + g >= nqc) break;
+            uint8_t out;
+            if (k[g] == kClsRefine || k[g] == kClsIdle) out = (uint8_t) coarse_group(sm, nb, s[g]);
+            else out = k[g] == kClsResult ? kCodeResult1 : kCodePruned1;
+            code[(int64_t) (q0 + i0 + g) * n_user + u] = out;
         }
     }
 }
 
-// Round 2 on 128 x 128 tiles: pairs that reached round 2 get left + the remaining coordinates and
-// their sampled-threshold bucket; the others their round-1 state code.  Tiles without a surviving
-// pair skip the dot products.
-struct Round2Epi {
-    static constexpr int kMaxRank = 1024;
-    static constexpr size_t kExtra = sizeof(float) * kBig * ThrSummary::kMaxGroups + sizeof(QsrpParams) * kBig +
-                                     sizeof(int32_t) * kMaxRank;
-    const uint32_t *lv;
-    const float *left;
-    const QsrpParams *par;
-    const int32_t *reg_rank;
-    int S_reg, n_item;
-    const float *thr;
-    int S;
-    int64_t n_user;
-    int n_query;
-    uint16_t *bucket2;
-    __device__ float *summ(char *x) const { return reinterpret_cast<float *>(x); }
-    __device__ QsrpParams *pars(char *x) const {
-        return reinterpret_cast<QsrpParams *>(x + sizeof(float) * kBig * ThrSummary::kMaxGroups);
-    }
-    __device__ const int32_t *ranks(char *x) const {
-        return S_reg <= kMaxRank ? reinterpret_cast<const int32_t *>(x + sizeof(float) * kBig * ThrSummary::kMaxGroups +
-                                                                    sizeof(QsrpParams) * kBig)
-                                 : reg_rank;
-    }
-    __device__ int klass(char *x, int64_t u, int64_t q, int rb) const {
-        const uint32_t v = lv[q * n_user + u];
-        const int32_t *rk = ranks(x);
-        return class1_of(pars(x)[rb], level_rank(v & 0xffff, rk, S_reg, n_item), level_rank(v >> 16, rk, S_reg, n_item));
-    }
-    __device__ void prologue(char *x, int64_t a0, int64_t b0) const {
-        if (threadIdx.x < kBig && b0 + threadIdx.x < n_query) pars(x)[threadIdx.x] = par[b0 + threadIdx.x];
-        if (S_reg <= kMaxRank) {
-            int32_t *rk = reinterpret_cast<int32_t *>(x + sizeof(float) * kBig * ThrSummary::kMaxGroups +
-                                                      sizeof(QsrpParams) * kBig);
-            for (int i = threadIdx.x; i < S_reg; i += blockDim.x) rk[i] = reg_rank[i];
-        }
-        load_thr_summary_rows(summ(x), kBig, thr, n_user, a0, S);
-    }
-    __device__ bool active(char *x, int64_t a0, int64_t b0) const {
-        bool any = false;
-        for (int idx = threadIdx.x; idx < kBig * kBig && !any; idx += kBigThreads) {
-            const int rb = idx / kBig, ra = idx % kBig;
-            const int64_t u = a0 + ra, q = b0 + rb;
-            if (u < n_user && q < n_query) {
-                const int k = klass(x, u, q, rb);
-                any = k == kClsRefine || k == kClsIdle;
-            }
-        }
-        return __syncthreads_or(any);
-    }
-    __device__ void finish(char *x, const BigResult &res, int64_t a0, int64_t b0, bool live) const {
-        const int ra = threadIdx.x & (kBig - 1), half = threadIdx.x >> 7;
-        const int64_t u = a0 + ra;
-        if (u >= n_user) return;
-        const float *sm = summ(x) + ra * ThrSummary::kMaxGroups;
-        const float *row = thr + u * S;
-        const int32_t *rk = ranks(x);
-        const QsrpParams *ps = pars(x);
-        constexpr int G = 8;
-        for (int i0 = 0; i0 < kBig / 2; i0 += G) {
-            uint32_t v[G];
-            float lf[G];
-#pragma unroll
-            for (int g = 0; g < G; g++) {
-                const int64_t q = b0 + half + 2 * (i0 + g);
-                v[g] = q < n_query ? lv[q * n_user + u] : 0u;
-                lf[g] = q < n_query ? left[q * n_user + u] : 0.0f;
-            }
-#pragma unroll
-            for (int g = 0; g < G; g++) {
-                const int rb = half + 2 * (i0 + g);
-                const int64_t q = b0 + rb;
-                if (q >= n_query) break;
-                const int k = class1_of(ps[rb], level_rank(v[g] & 0xffff, rk, S_reg, n_item),
-                                        level_rank(v[g] >> 16, rk, S_reg, n_item));
-                uint16_t b;
-                if (k == kClsRefine || k == kClsIdle) {
-                    b = (uint16_t) bucket_of_2level(sm, row, S, __fadd_rn(lf[g], live ? res.v[rb][ra] : 0.0f));
-                } else {
-                    b = k == kClsResult ? kStateResult1 : kStatePruned1;
-                }
-                bucket2[q * n_user + u] = b;
-            }
-        }
-    }
-};
-
-// Round-2 pruning per query (second PruneCandidateByBound call, QSRPNormalLP.hpp:187-190): users
-// excluded in round 1 are skipped by the heap scan and the classification; the equal-bounds rule
-// looks at every user's current bounds.
-__global__ void qsrp_select2_kernel(const int *__restrict__ hist_all, int S, const int32_t *__restrict__ rank,
-                                    int n_item, int topk, int nq, QsrpParams *__restrict__ par,
-                                    uint8_t *__restrict__ cls2, QueryCounts *__restrict__ counts) {
+// Round-2 selection, coarse step (second PruneCandidateByBound call, QSRPNormalLP.hpp:187-190):
+// the coarse group holding the kp-th smallest bucket among the users that reached round 2
+// (kp = topk - round-1 results), or, with fewer such users than kp, the highest occupied group.
+__global__ void qsrp_select2c_kernel(const int *__restrict__ hist_c, int nb, int topk, int nq,
+                                     QsrpParams *__restrict__ par, QueryCounts *__restrict__ counts) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nq) return;
     QsrpParams p = par[q];
-    uint8_t *cq = cls2 + (int64_t) q * (S + 1);
+    p.crit = -1; p.cum_before = -1; p.mask1 = 0; p.mask2 = 0;
     if (p.skip2) {
         QueryCounts c = {};
         c.n_result = p.n_res1;
@@ -523,17 +529,77 @@ __global__ void qsrp_select2_kernel(const int *__restrict__ hist_all, int S, con
         c.mode = 2;
         c.ip_base = p.n_ref1;
         counts[q] = c;
+        par[q] = p;
         return;
     }
-    const int *hist = hist_all + (int64_t) q * (S + 1);
+    const int *h = hist_c + (int64_t) q * (nb + 1);
     const int kp = topk - p.n_res1;
     int64_t n_el = 0;
-    for (int b = 0; b <= S; b++) n_el += hist[b];
-    int L, U;
-    if (n_el < kp) {  // the reference's zero-filled heap: max(bounds of eligible users, 0)
+    for (int g = 0; g <= nb; g++) n_el += h[g];
+    p.n_elig2 = (int) n_el;
+    if (n_el < kp) {
+        for (int g = nb; g >= 0; g--) if (h[g]) { p.crit = g; break; }
+    } else {
+        int64_t cum = 0;
+        for (int g = 0; g <= nb; g++) {
+            if (cum + h[g] >= kp) { p.crit = g; p.cum_before = (int) cum; break; }
+            cum += h[g];
+        }
+    }
+    if (p.crit >= 0 && p.crit < nb) p.mask1 = (int32_t) (1u << p.crit);
+    par[q] = p;
+}
+
+// Exact bucket histogram of the pairs whose coarse group is flagged for their query (mask1 or
+// mask2), one CTA per (user chunk, query).
+__global__ void __launch_bounds__(kHistThreads) qsrp_fine2_kernel(const uint8_t *__restrict__ code,
+                                                                 const float *__restrict__ qip, int64_t n_user,
+                                                                 const float *__restrict__ thr, int S, int gs,
+                                                                 const QsrpParams *__restrict__ par, int second,
+                                                                 int64_t chunk, int *__restrict__ hist_f) {
+    const int q = blockIdx.y;
+    const uint32_t mask = (uint32_t) (second ? par[q].mask2 : par[q].mask1);
+    if (!mask) return;
+    const uint8_t *row = code + (int64_t) q * n_user;
+    const int64_t u0 = (int64_t) blockIdx.x * chunk, u1 = min(u0 + chunk, n_user);
+    int *hq = hist_f + (int64_t) q * (S + 1);
+    for (int64_t u = u0 + threadIdx.x; u < u1; u += kHistThreads) {
+        const unsigned c = row[u];
+        if (c < 32 && (mask >> c & 1u)) {
+            const float s = __ldg(qip + (int64_t) q * n_user + u);
+            atomicAdd(hq + fine_bucket(thr + u * S, S, gs, (int) c, s), 1);
+        }
+    }
+}
+
+// Class of bucket b for the round-2 bounds (L, U): mode2 (L == U) marks results only.
+__device__ __forceinline__ uint8_t class2_of(int b, int S, const int32_t *rank, int n_item, int L, int U, bool mode2) {
+    int lb, ub;
+    bucket_bounds(b, S, rank, n_item, lb, ub);
+    if (mode2) return (ub <= L && lb <= L) ? kClsResult : kClsIdle;
+    if (lb <= U) return kClsResult;
+    if (L <= ub) return kClsPrune;
+    return kClsRefine;
+}
+
+// Round-2 selection, exact step: the k-th bucket from the critical group's exact histogram, the
+// bounds (L2, U2), each bucket's and each group's class, and the mixed groups still without an
+// exact histogram (mask2).
+__global__ void qsrp_select2f_kernel(const int *__restrict__ hist_f, int nb, int gs, int S,
+                                     const int32_t *__restrict__ rank, int n_item, int topk, int nq,
+                                     QsrpParams *__restrict__ par, uint8_t *__restrict__ cls2,
+                                     uint8_t *__restrict__ clsg) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    QsrpParams p = par[q];
+    if (p.skip2) return;
+    const int *hf = hist_f + (int64_t) q * (S + 1);
+    int L = 0, U = 0;
+    if (p.cum_before < 0) {  // the reference's zero-filled heap: max(bounds of the highest bucket, 0)
         int bmax = -1;
-        for (int b = S; b >= 0; b--) if (hist[b]) { bmax = b; break; }
-        L = 0; U = 0;
+        if (p.crit == nb) bmax = S;
+        else if (p.crit >= 0)
+            for (int b = min(p.crit * gs + gs, S) - 1; b >= p.crit * gs; b--) if (hf[b]) { bmax = b; break; }
         if (bmax >= 0) {
             int lb, ub;
             bucket_bounds(bmax, S, rank, n_item, lb, ub);
@@ -541,58 +607,91 @@ __global__ void qsrp_select2_kernel(const int *__restrict__ hist_all, int S, con
         }
     } else {
         int bk = S;
-        int64_t c = 0;
-        for (int b = 0; b <= S; b++) { c += hist[b]; if (c >= kp) { bk = b; break; } }
+        if (p.crit < nb) {
+            const int need = topk - p.n_res1 - p.cum_before;
+            const int end = min(p.crit * gs + gs, S);
+            int c = 0;
+            bk = end - 1;
+            for (int b = p.crit * gs; b < end; b++) { c += hf[b]; if (c >= need) { bk = b; break; } }
+        }
         bucket_bounds(bk, S, rank, n_item, L, U);
     }
-    p.L2 = L; p.U2 = U; p.n_elig2 = (int) n_el;
+    p.L2 = L; p.U2 = U; p.mode2 = L == U;
+    uint8_t *cq = cls2 + (int64_t) q * (S + 1);
+    uint8_t *cg = clsg + (int64_t) q * (nb + 1);
+    for (int b = 0; b <= S; b++) cq[b] = class2_of(b, S, rank, n_item, L, U, p.mode2);
+    uint32_t mask2 = 0;
+    for (int g = 0; g < nb; g++) {
+        const int b0 = g * gs, b1 = min(b0 + gs, S);
+        uint8_t k = cq[b0];
+        for (int b = b0 + 1; b < b1; b++) if (cq[b] != k) { k = kClsMixed; break; }
+        cg[g] = k;
+        if (k == kClsMixed && !p.mode2 && !(p.mask1 >> g & 1)) mask2 |= 1u << g;
+    }
+    cg[nb] = cq[S];
+    p.mask2 = (int32_t) mask2;
+    par[q] = p;
+}
+
+// Round-2 class counts (PruneCandidateByBound.hpp:83-150): pure groups count whole from the
+// coarse histogram, mixed groups bucket by bucket; then the "all survivors are results" rule.
+__global__ void qsrp_final2_kernel(const int *__restrict__ hist_c, const int *__restrict__ hist_f, int nb, int gs, int S,
+                                   int topk, int nq, QsrpParams *__restrict__ par, uint8_t *__restrict__ cls2,
+                                   uint8_t *__restrict__ clsg, QueryCounts *__restrict__ counts) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    const QsrpParams p = par[q];
+    if (p.skip2) return;
     QueryCounts c = {};
-    c.lstar = L; c.ustar = U;
+    c.lstar = p.L2;
+    c.ustar = p.U2;
     c.ip_base = p.n_ref1;  // QSRPNormalLP.hpp:177: refine_user_size after the first prune
-    if (L == U) {
-        p.mode2 = 1;
+    if (p.mode2) {
         c.mode = 1;
         c.n_result = topk;
         c.n_prune = p.n_pr1;
         c.n_cand = 0;
-        for (int b = 0; b <= S; b++) cq[b] = kClsIdle;
     } else {
-        int64_t nres = p.n_res1, npr = p.n_pr1, nref = 0;
-        for (int b = 0; b <= S; b++) {
-            int lb, ub;
-            bucket_bounds(b, S, rank, n_item, lb, ub);
-            uint8_t k;
-            if (lb <= U) { k = kClsResult; nres += hist[b]; }
-            else if (L <= ub) { k = kClsPrune; npr += hist[b]; }
-            else { k = kClsRefine; nref += hist[b]; }
-            cq[b] = k;
+        const int *hc = hist_c + (int64_t) q * (nb + 1);
+        const int *hf = hist_f + (int64_t) q * (S + 1);
+        uint8_t *cq = cls2 + (int64_t) q * (S + 1);
+        uint8_t *cg = clsg + (int64_t) q * (nb + 1);
+        int64_t n[4] = {0, 0, 0, 0};
+        for (int g = 0; g <= nb; g++) {
+            if (cg[g] != kClsMixed) {
+                n[cg[g]] += hc[g];
+            } else {
+                for (int b = g * gs; b < min(g * gs + gs, S); b++) n[cq[b]] += hf[b];
+            }
         }
+        int64_t nres = p.n_res1 + n[kClsResult], npr = p.n_pr1 + n[kClsPrune], nref = n[kClsRefine];
         if (nres + nref == topk) {
             for (int b = 0; b <= S; b++) if (cq[b] == kClsRefine) cq[b] = kClsResult;
-            p.all2 = 1;
-            nres = topk; nref = 0;
+            for (int g = 0; g <= nb; g++) if (cg[g] == kClsRefine) cg[g] = kClsResult;
+            nres = topk;
+            nref = 0;
         }
         c.mode = 0;
         c.n_result = (int) nres;
         c.n_prune = (int) npr;
         c.n_cand = nres >= topk ? 0 : (int) nref;
     }
-    par[q] = p;
     counts[q] = c;
 }
 
 // Classification of a pair after both rounds for the ordered compaction: result users carry their
 // reported rank (the lower bound in force) and whether their score is this query's; candidates
-// carry their round-2 bounds.
+// carry their round-2 bounds.  Exact buckets are resolved here for the few pairs that need one.
 struct QsrpCompactPolicy {
     struct Aux { int rank, fresh, lb, ub; };
     const uint32_t *lv;
-    const uint16_t *b2;
+    const uint8_t *code;
+    const float *qip, *thr;
     int64_t n_user;
     const int32_t *reg_rank, *rank;
-    int S_reg, S, n_item;
+    int S_reg, S, n_item, nb, gs;
     const QsrpParams *par;
-    const uint8_t *cls2;
+    const uint8_t *cls2, *clsg;
     const QueryCounts *counts;
     const int64_t *cand_off;
     int topk;
@@ -601,25 +700,28 @@ struct QsrpCompactPolicy {
     int32_t *cand_user, *cand_query, *cand_lb, *cand_ub;
     __device__ bool query_active(int q) const { return true; }
     __device__ int classify(int q, int64_t u, Aux &aux) const {
-        const QsrpParams &p = par[q];
-        const uint16_t code = b2[(int64_t) q * n_user + u];
-        if (code <= S) {  // reached round 2
+        const int64_t at = (int64_t) q * n_user + u;
+        const unsigned c = code[at];
+        if (c <= (unsigned) nb) {  // reached round 2
+            if (par[q].skip2) return 0;
+            const uint8_t kg = clsg[(int64_t) q * (nb + 1) + c];
+            if (kg == kClsPrune || kg == kClsIdle) return 0;
+            const int b = c == (unsigned) nb ? S : fine_bucket(thr + u * S, S, gs, (int) c, __ldg(qip + at));
+            const uint8_t k2 = cls2[(int64_t) q * (S + 1) + b];
             int lb, ub;
-            bucket_bounds(code, S, rank, n_item, lb, ub);
+            bucket_bounds(b, S, rank, n_item, lb, ub);
             aux.rank = lb; aux.fresh = 1; aux.lb = lb; aux.ub = ub;
-            if (p.skip2) return 0;
-            if (p.mode2) return (ub <= p.L2 && lb <= p.L2) ? 1 : 0;
-            const uint8_t k2 = __ldg(cls2 + (int64_t) q * (S + 1) + code);
             if (k2 == kClsResult) return 1;
             return (k2 == kClsRefine && counts[q].n_cand > 0) ? 2 : 0;
         }
         aux.fresh = 0;
-        if (code == kStateResult1 || (!p.skip2 && p.mode2)) {
-            const uint32_t v = lv[(int64_t) q * n_user + u];
+        const QsrpParams &p = par[q];
+        if (c == kCodeResult1 || (!p.skip2 && p.mode2)) {
+            const uint32_t v = lv[at];
             const int lb1 = level_rank(v & 0xffff, reg_rank, S_reg, n_item);
             const int ub1 = level_rank(v >> 16, reg_rank, S_reg, n_item);
             aux.rank = lb1; aux.lb = lb1; aux.ub = ub1;
-            if (code == kStateResult1) return 1;
+            if (c == kCodeResult1) return 1;
             return (ub1 <= p.L2 && lb1 <= p.L2) ? 1 : 0;  // the equal-bounds rule scans every user
         }
         return 0;
@@ -640,20 +742,12 @@ struct QsrpCompactPolicy {
     }
 };
 
-// Exact SVD-space score of (query, user): checkdim part + remaining part (PartDimPartNorm.hpp:62, 89-92).
-__device__ __forceinline__ float qsrp_score(const float *svd_user, const float *qtr, int64_t u, int q, int dim, int c) {
-    const float *uv = svd_user + u * dim;
-    const float *qv = qtr + (int64_t) q * dim;
-    return __fadd_rn(exact_dot(uv, qv, c), exact_dot(uv + c, qv + c, dim - c));
-}
-
 // Scores of the emitted result users: this query's score when the user reached round 2, else the
 // score from its latest earlier round-2 query in the batch, else the carried state.
 __global__ void qsrp_result_fill_kernel(const QueryCounts *__restrict__ counts, const int32_t *__restrict__ res_user,
-                                        const uint8_t *__restrict__ res_fresh, const uint16_t *__restrict__ bucket2,
-                                        int64_t n_user, const float *__restrict__ svd_user, const float *__restrict__ qtr,
-                                        int dim, int check_dim, const float *__restrict__ state, int topk,
-                                        float *__restrict__ res_qip) {
+                                        const uint8_t *__restrict__ res_fresh, const uint8_t *__restrict__ code,
+                                        const float *__restrict__ qip, int64_t n_user, const float *__restrict__ state,
+                                        int topk, float *__restrict__ res_qip) {
     const int q = blockIdx.x;
     const int n = counts[q].n_res_emit;
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
@@ -661,28 +755,27 @@ __global__ void qsrp_result_fill_kernel(const QueryCounts *__restrict__ counts, 
         const int u = res_user[i];
         int src = res_fresh[i] ? q : -1;
         for (int qq = q - 1; src < 0 && qq >= 0; qq--)
-            if (bucket2[(int64_t) qq * n_user + u] < kStateResult1) src = qq;
-        res_qip[i] = src >= 0 ? qsrp_score(svd_user, qtr, u, src, dim, check_dim) : state[u];
+            if (code[(int64_t) qq * n_user + u] < kCodeResult1) src = qq;
+        res_qip[i] = src >= 0 ? qip[(int64_t) src * n_user + u] : state[u];
     }
 }
 
 __global__ void qsrp_cand_fill_kernel(const int32_t *__restrict__ cand_user, const int32_t *__restrict__ cand_query,
-                                      int64_t n, const float *__restrict__ svd_user, const float *__restrict__ qtr, int dim,
-                                      int check_dim, float *__restrict__ cand_qip) {
+                                      int64_t n, const float *__restrict__ qip, int64_t n_user,
+                                      float *__restrict__ cand_qip) {
     const int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n) return;
-    cand_qip[e] = qsrp_score(svd_user, qtr, cand_user[e], cand_query[e], dim, check_dim);
+    cand_qip[e] = qip[(int64_t) cand_query[e] * n_user + cand_user[e]];
 }
 
 // Carried state after the batch: each user's score at its last round-2 query of the batch.
-__global__ void qsrp_state_kernel(const uint16_t *__restrict__ bucket2, int64_t n_user, int nq,
-                                  const float *__restrict__ svd_user, const float *__restrict__ qtr, int dim, int check_dim,
-                                  float *__restrict__ state) {
+__global__ void qsrp_state_kernel(const uint8_t *__restrict__ code, const float *__restrict__ qip, int64_t n_user,
+                                  int nq, float *__restrict__ state) {
     const int64_t u = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= n_user) return;
     for (int q = nq - 1; q >= 0; q--)
-        if (bucket2[(int64_t) q * n_user + u] < kStateResult1) {
-            state[u] = qsrp_score(svd_user, qtr, u, q, dim, check_dim);
+        if (code[(int64_t) q * n_user + u] < kCodeResult1) {
+            state[u] = qip[(int64_t) q * n_user + u];
             return;
         }
 }
@@ -698,6 +791,7 @@ template <typename T> T *carve(uint8_t *&p, size_t n) {
     return r;
 }
 inline size_t carve_size(size_t n, size_t elem) { return ((n * elem + 255) & ~size_t(255)) + 256; }
+constexpr int kFixCap = 1 << 22;
 }  // namespace
 
 int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_rank *d_out, rkr_query_stats *d_stats,
@@ -706,24 +800,41 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     const int dim = ix->dim, c = ix->check_dim, S = ix->n_sample, Sr = ix->n_sample_reg;
     const int n_item = (int) ix->n_item;
     const int nl = Sr + 2;
+    const int gs = thr_group(S), nb = (S + gs - 1) / gs;
     RKR_TRY(ix->ws_qtr.ensure(carve_size((size_t) nq * dim, 4) + carve_size(nq, 4) + carve_size(nq, sizeof(QsrpParams)) +
-                              carve_size(nq, 4)));
+                              carve_size(nq, 4) + carve_size(1, 4)));
     uint8_t *p0 = ix->ws_qtr.as<uint8_t>();
     float *qtr = carve<float>(p0, (size_t) nq * dim);
     float *qnorm = carve<float>(p0, nq);
     QsrpParams *par = carve<QsrpParams>(p0, nq);
     int *anomaly = carve<int>(p0, nq);
+    int *fix_count = carve<int>(p0, 1);
     RKR_TRY(ix->ws_levels.ensure((size_t) nq * U * 8));
-    RKR_TRY(ix->ws_bucket2.ensure((size_t) nq * U * 2));
-    RKR_TRY(ix->ws_cls.ensure((size_t) nq * (S + 1)));
+    RKR_TRY(ix->ws_bucket2.ensure((size_t) nq * U));
+    RKR_TRY(ix->ws_cls.ensure(carve_size((size_t) nq * (S + 1), 1) + carve_size((size_t) nq * (nb + 1), 1)));
     RKR_TRY(ix->ws_counts.ensure(sizeof(QueryCounts) * (size_t) nq));
-    RKR_TRY(ix->ws_hist.ensure(sizeof(int) * (size_t) nq * std::max(2 * nl, S + 1)));
+    const size_t n_hist_l = (size_t) nq * 2 * nl, n_hist_c = (size_t) nq * (nb + 1), n_hist_f = (size_t) nq * (S + 1);
+    RKR_TRY(ix->ws_hist.ensure(carve_size(n_hist_l, 4) + carve_size(n_hist_c, 4) + carve_size(n_hist_f, 4)));
+    RKR_TRY(ix->ws_fix.ensure(carve_size(kFixCap, sizeof(int4))));
     uint32_t *lv = ix->ws_levels.as<uint32_t>();
-    float *left = reinterpret_cast<float *>(lv + (size_t) nq * U);
-    uint16_t *b2 = ix->ws_bucket2.as<uint16_t>();
+    float *qip = reinterpret_cast<float *>(lv + (size_t) nq * U);
+    uint8_t *code = ix->ws_bucket2.as<uint8_t>();
+    uint8_t *pc = ix->ws_cls.as<uint8_t>();
+    uint8_t *cls2 = carve<uint8_t>(pc, (size_t) nq * (S + 1));
+    uint8_t *clsg = carve<uint8_t>(pc, (size_t) nq * (nb + 1));
     QueryCounts *counts = ix->ws_counts.as<QueryCounts>();
-    int *hist = ix->ws_hist.as<int>();
+    uint8_t *ph = ix->ws_hist.as<uint8_t>();
+    int *hist_l = carve<int>(ph, n_hist_l);
+    int *hist_c = carve<int>(ph, n_hist_c);
+    int *hist_f = carve<int>(ph, n_hist_f);
+    uint8_t *pm = ix->ws_fix.as<uint8_t>();
+    FixList fix;
+    fix.e = carve<int4>(pm, kFixCap);
+    fix.count = fix_count;
+    fix.cap = kFixCap;
     RKR_CUDA(cudaMemsetAsync(anomaly, 0, sizeof(int) * nq, st));
+    RKR_CUDA(cudaMemsetAsync(fix_count, 0, sizeof(int), st));
+    RKR_CUDA(cudaMemsetAsync(ix->ws_hist.p, 0, (size_t) (ph - ix->ws_hist.as<uint8_t>()), st));
 
     timed(ix, st, "transfer_query", [&] {
         transfer_query_kernel<<<nq, 128, 0, st>>>(d_query, ix->transfer_item.as<float>(), dim, c, qtr, qnorm);
@@ -740,53 +851,67 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     e1.qnorm = qnorm;
     e1.m = m;
     e1.lv = lv;
-    e1.left = left;
+    e1.qip = qip;
     e1.n_user = U;
     e1.n_query = nq;
+    e1.fix = fix;
     cudaError_t ce = cudaSuccess;
-    timed(ix, st, "qsrp_round1", [&] { ce = launch_big(ix->svd_user.as<float>(), nullptr, U, dim, qtr, nq, dim, 0, c, e1, st); });
+    timed(ix, st, "qsrp_scores", [&] { ce = launch_big_split(ix->svd_user.as<float>(), U, dim, qtr, nq, dim, c, dim, e1, st); });
     RKR_CUDA(ce);
+    timed(ix, st, "qsrp_fix1", [&] {
+        qsrp_fix1_kernel<<<148 * 4, 256, 0, st>>>(fix, m, e1.unorm, qnorm, U, lv);
+    });
+    RKR_CUDA(cudaGetLastError());
     const int64_t chunk = 16384;
     dim3 hg((unsigned) ((U + chunk - 1) / chunk), (unsigned) nq);
-    RKR_CUDA(cudaMemsetAsync(hist, 0, sizeof(int) * (size_t) nq * 2 * nl, st));
     timed(ix, st, "level_hist", [&] {
         level_hist_kernel<<<hg, kHistThreads, hist_copies(2 * nl) * 2 * nl * sizeof(int), st>>>(lv, U, m.rank, Sr, n_item,
-                                                                                               chunk, hist, anomaly);
+                                                                                               chunk, hist_l, anomaly);
     });
     RKR_CUDA(cudaGetLastError());
     timed(ix, st, "qsrp_select1", [&] {
-        qsrp_select1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(hist, anomaly, U, m.rank, Sr, n_item, topk, nq, par);
+        qsrp_select1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(hist_l, anomaly, U, m.rank, Sr, n_item, topk, nq, par);
     });
     RKR_CUDA(cudaGetLastError());
     {
         dim3 g((unsigned) std::min<int64_t>((U + 1023) / 1024, 64), (unsigned) nq);
-        timed(ix, st, "qsrp_count1", [&] { qsrp_count1_kernel<<<g, 256, 0, st>>>(lv, U, m.rank, Sr, n_item, par); });
+        timed(ix, st, "qsrp_count1", [&] { qsrp_count1_kernel<<<g, 256, 0, st>>>(lv, U, par); });
         RKR_CUDA(cudaGetLastError());
     }
     timed(ix, st, "qsrp_final1", [&] { qsrp_final1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, topk); });
     RKR_CUDA(cudaGetLastError());
-    Round2Epi e2;
-    e2.lv = lv;
-    e2.left = left;
-    e2.par = par;
-    e2.reg_rank = m.rank;
-    e2.S_reg = Sr;
-    e2.n_item = n_item;
-    e2.thr = ix->thr.as<float>();
-    e2.S = S;
-    e2.n_user = U;
-    e2.n_query = nq;
-    e2.bucket2 = b2;
-    timed(ix, st, "qsrp_round2", [&] { ce = launch_big(ix->svd_user.as<float>(), nullptr, U, dim, qtr, nq, dim, c, dim, e2, st); });
-    RKR_CUDA(ce);
-    RKR_CUDA(cudaMemsetAsync(hist, 0, sizeof(int) * (size_t) nq * (S + 1), st));
-    timed(ix, st, "bucket_hist", [&] {
-        bucket_hist_kernel<<<hg, kHistThreads, hist_copies(S + 1) * (S + 1) * sizeof(int), st>>>(b2, U, S + 1, chunk, hist);
+    {
+        dim3 g((unsigned) ((U + kScreenUsers - 1) / kScreenUsers), (unsigned) ((nq + kScreenQueries - 1) / kScreenQueries));
+        timed(ix, st, "qsrp_screen2", [&] {
+            qsrp_screen2_kernel<<<g, kScreenUsers, 0, st>>>(lv, qip, U, nq, par, ix->thr_summ.as<float>(), nb, code);
+        });
+        RKR_CUDA(cudaGetLastError());
+    }
+    timed(ix, st, "group_hist", [&] {
+        bucket_hist_kernel<<<hg, kHistThreads, hist_copies(nb + 1) * (nb + 1) * sizeof(int), st>>>(code, U, nb + 1, chunk,
+                                                                                                  hist_c);
     });
     RKR_CUDA(cudaGetLastError());
-    timed(ix, st, "qsrp_select2", [&] {
-        qsrp_select2_kernel<<<(nq + 127) / 128, 128, 0, st>>>(hist, S, ix->sample_rank.as<int32_t>(), n_item, topk, nq,
-                                                             par, ix->ws_cls.as<uint8_t>(), counts);
+    timed(ix, st, "qsrp_select2c", [&] {
+        qsrp_select2c_kernel<<<(nq + 127) / 128, 128, 0, st>>>(hist_c, nb, topk, nq, par, counts);
+    });
+    RKR_CUDA(cudaGetLastError());
+    const float *thr = ix->thr.as<float>();
+    const int32_t *srank = ix->sample_rank.as<int32_t>();
+    timed(ix, st, "qsrp_fine2", [&] {
+        qsrp_fine2_kernel<<<hg, kHistThreads, 0, st>>>(code, qip, U, thr, S, gs, par, 0, chunk, hist_f);
+    });
+    RKR_CUDA(cudaGetLastError());
+    timed(ix, st, "qsrp_select2f", [&] {
+        qsrp_select2f_kernel<<<(nq + 127) / 128, 128, 0, st>>>(hist_f, nb, gs, S, srank, n_item, topk, nq, par, cls2, clsg);
+    });
+    RKR_CUDA(cudaGetLastError());
+    timed(ix, st, "qsrp_fine2", [&] {
+        qsrp_fine2_kernel<<<hg, kHistThreads, 0, st>>>(code, qip, U, thr, S, gs, par, 1, chunk, hist_f);
+    });
+    RKR_CUDA(cudaGetLastError());
+    timed(ix, st, "qsrp_final2", [&] {
+        qsrp_final2_kernel<<<(nq + 127) / 128, 128, 0, st>>>(hist_c, hist_f, nb, gs, S, topk, nq, par, cls2, clsg, counts);
     });
     RKR_CUDA(cudaGetLastError());
 
@@ -813,15 +938,20 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     RKR_CUDA(cudaMemcpyAsync(d_off, off.data(), sizeof(int64_t) * (nq + 1), cudaMemcpyHostToDevice, st));
     QsrpCompactPolicy pol;
     pol.lv = lv;
-    pol.b2 = b2;
+    pol.code = code;
+    pol.qip = qip;
+    pol.thr = thr;
     pol.n_user = U;
     pol.reg_rank = m.rank;
-    pol.rank = ix->sample_rank.as<int32_t>();
+    pol.rank = srank;
     pol.S_reg = Sr;
     pol.S = S;
     pol.n_item = n_item;
+    pol.nb = nb;
+    pol.gs = gs;
     pol.par = par;
-    pol.cls2 = ix->ws_cls.as<uint8_t>();
+    pol.cls2 = cls2;
+    pol.clsg = clsg;
     pol.counts = counts;
     pol.cand_off = d_off;
     pol.topk = topk;
@@ -834,22 +964,21 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     pol.cand_ub = cand_ub;
     RKR_TRY(run_compaction(ix, pol, nq, topk, counts, st));
     timed(ix, st, "qsrp_result_fill", [&] {
-        qsrp_result_fill_kernel<<<nq, 128, 0, st>>>(counts, res_user, res_fresh, b2, U, ix->svd_user.as<float>(), qtr,
-                                                    dim, c, ix->qip_state.as<float>(), topk, res_qip);
+        qsrp_result_fill_kernel<<<nq, 128, 0, st>>>(counts, res_user, res_fresh, code, qip, U, ix->qip_state.as<float>(),
+                                                    topk, res_qip);
     });
     RKR_CUDA(cudaGetLastError());
     if (n_cand > 0) {
         timed(ix, st, "qsrp_cand_fill", [&] {
-            qsrp_cand_fill_kernel<<<(unsigned) ((n_cand + 255) / 256), 256, 0, st>>>(
-                cand_user, cand_query, n_cand, ix->svd_user.as<float>(), qtr, dim, c, cand_qip);
+            qsrp_cand_fill_kernel<<<(unsigned) ((n_cand + 255) / 256), 256, 0, st>>>(cand_user, cand_query, n_cand, qip, U,
+                                                                                    cand_qip);
         });
         RKR_CUDA(cudaGetLastError());
     }
     RKR_TRY(refine_and_assemble_qsrp(ix, d_query, nq, topk, counts, res_user, res_rank, res_qip, n_cand, cand_user,
                                      cand_query, cand_lb, cand_ub, cand_qip, d_off, d_out, d_stats, st));
     timed(ix, st, "qsrp_state", [&] {
-        qsrp_state_kernel<<<(unsigned) ((U + 255) / 256), 256, 0, st>>>(b2, U, nq, ix->svd_user.as<float>(), qtr, dim,
-                                                                        c, ix->qip_state.as<float>());
+        qsrp_state_kernel<<<(unsigned) ((U + 255) / 256), 256, 0, st>>>(code, qip, U, nq, ix->qip_state.as<float>());
     });
     RKR_CUDA(cudaGetLastError());
     RKR_CUDA(cudaStreamSynchronize(st));

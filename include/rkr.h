@@ -124,7 +124,10 @@ int rkr_retrieval_device(rkr_index *index, int32_t method, const float *d_query,
 /* Per-kernel device time: with profiling on, every kernel the index launches is bracketed by CUDA
  * events on the stream it runs on.  rkr_profile_read returns, per kernel name, the summed time and
  * the launch count since the previous complete read (a read with max_kernels >= *n_kernels clears
- * them; a smaller one only reports the count); names is [max_kernels][64] chars.
+ * them; a smaller one only reports the count); names is [max_kernels][64] chars.  Entries whose
+ * name ends in "_pairs" are counters rather than kernels (time 0, `launches` holds the count):
+ * screen_undecided_pairs counts the QSRPNormalLP (query, user) pairs whose regression bound the
+ * fast binary32 screen left to the reference's own float/double arithmetic.
  * (The reference's counterpart is its TimeRecord per stage, src/include/util/TimeMemory.hpp:7-24.) */
 int rkr_profile_enable(rkr_index *index, int32_t on);
 int rkr_profile_read(rkr_index *index, int32_t max_kernels, char *names, double *total_ms, int64_t *launches,

@@ -330,9 +330,11 @@ inline size_t big_kernel_smem() { return kBigSmem + Epi::kExtra; }
 
 // Split form: the block of partial sums over [0, k_split) goes to epi.finish_lo(extra, res, a0, b0),
 // then the sums over [k_split, k_end) -- each accumulated from 0, as the reference keeps a partial
-// score and its remainder apart -- are added to them with one rounding and epi.finish_hi sees the
-// totals.  Operands and result have separate shared memory, so the second range's loads do not
-// wait for finish_lo.  Epi also provides kExtra and prologue(extra, a0, b0).
+// score and its remainder apart -- are added to them with one rounding and
+// epi.finish_hi(extra, res, a0, b0, spare) sees the totals; spare is the operand buffers'
+// sizeof(BigOperands) bytes, free by then.  Operands and result have separate shared memory, so the
+// second range's loads do not wait for finish_lo.  Epi also provides kExtra and
+// prologue(extra, a0, b0).  Every thread calls each hook (they may synchronise the block).
 template <class Epi>
 __global__ void __launch_bounds__(kBigThreads, 2) exact_big_split_kernel(const float *__restrict__ A, int64_t n_a,
                                                                          int lda, const float *__restrict__ B,
@@ -354,7 +356,7 @@ __global__ void __launch_bounds__(kBigThreads, 2) exact_big_split_kernel(const f
     if (!big_accumulate(op, acc, A, nullptr, n_a, lda, a0, B, n_b, ldb, b0, k_split, k_end)) __syncthreads();
     big_store(res, acc, true);
     __syncthreads();
-    epi.finish_hi(extra, res, a0, b0);
+    epi.finish_hi(extra, res, a0, b0, big_smem);
 }
 
 template <class Epi>
@@ -578,27 +580,44 @@ __global__ void __launch_bounds__(kHistThreads) bucket_hist_kernel(const T *__re
 // refinement candidates (ComputeAllIPBound.hpp:306-313).  Users are cut into chunks of
 // kCompactChunk; pass 1 counts per (query, chunk), a scan turns the counts into offsets, pass 2
 // writes each chunk's entries at its offset -- so the lists come out in user-id order while every
-// chunk runs in parallel.  A policy P classifies a (query, user) pair (0 none, 1 result,
-// 2 candidate) and writes the entries.
+// chunk runs in parallel.  Thread t of a chunk owns kCompactPer consecutive users.  A policy P
+// gives, for a thread's users, the mask of those that can be a result or a candidate
+// (need_mask(q, u, n)), classifies such a (query, user) pair (0 none, 1 result, 2 candidate;
+// with_aux asks for the entry's fields too, which only the emitting pass needs) and writes the
+// entries.
 
 constexpr int kCompactThreads = 256;
 constexpr int kCompactPer = 16;
 constexpr int64_t kCompactChunk = (int64_t) kCompactThreads * kCompactPer;
+
+// The 16 bytes p[0..15] as four words (little-endian order), from five aligned 4-byte loads; bytes
+// past the buffer's end are read only inside its allocation slack and must be masked by the caller.
+__device__ __forceinline__ void load16_bytes(const uint8_t *p, uint32_t w[4]) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    const uint32_t *base = reinterpret_cast<const uint32_t *>(a & ~uintptr_t(3));
+    const unsigned sh = (unsigned) (a & 3) * 8;
+    uint32_t x[5];
+#pragma unroll
+    for (int i = 0; i < 5; i++) x[i] = __ldg(base + i);
+#pragma unroll
+    for (int i = 0; i < 4; i++) w[i] = __funnelshift_r(x[i], x[i + 1], sh);
+}
 
 template <class P>
 __global__ void __launch_bounds__(kCompactThreads) compact_count_kernel(P p, int64_t n_user, int nchunks,
                                                                       int2 *__restrict__ cnt) {
     __shared__ int warp_tot[9];
     const int q = blockIdx.y;
-    const int64_t u0 = (int64_t) blockIdx.x * kCompactChunk;
+    const int64_t u0 = (int64_t) blockIdx.x * kCompactChunk + (int64_t) threadIdx.x * kCompactPer;
     int r = 0, c = 0;
-    if (p.query_active(q)) {
-#pragma unroll 4
-        for (int e = 0; e < kCompactPer; e++) {
-            const int64_t u = u0 + (int64_t) e * kCompactThreads + threadIdx.x;
-            if (u >= n_user) break;
+    if (u0 < n_user) {
+        const int n = (int) (n_user - u0 < kCompactPer ? n_user - u0 : kCompactPer);
+        uint32_t need = p.need_mask(q, u0, n);
+        while (need) {
+            const int e = __ffs(need) - 1;
+            need &= need - 1;
             typename P::Aux aux;
-            const int k = p.classify(q, u, aux);
+            const int k = p.classify(q, u0 + e, aux, false);
             r += k == 1;
             c += k == 2;
         }
@@ -635,29 +654,33 @@ __global__ void __launch_bounds__(kCompactThreads) compact_write_kernel(P p, int
     if ((cc.x == 0 || oo.x >= topk) && cc.y == 0) return;
     // thread t owns users u0 + t*kCompactPer .. + kCompactPer - 1, so prefix order is user-id order
     const int64_t u0 = (int64_t) blockIdx.x * kCompactChunk + (int64_t) threadIdx.x * kCompactPer;
+    uint32_t need = 0;
+    if (u0 < n_user) need = p.need_mask(q, u0, (int) (n_user - u0 < kCompactPer ? n_user - u0 : kCompactPer));
     int r = 0, c = 0;
-    for (int e = 0; e < kCompactPer; e++) {
-        const int64_t u = u0 + e;
-        if (u >= n_user) break;
+    uint32_t hit = 0, is_res = 0;
+    for (uint32_t m = need; m; m &= m - 1) {
+        const int e = __ffs(m) - 1;
         typename P::Aux aux;
-        const int k = p.classify(q, u, aux);
+        const int k = p.classify(q, u0 + e, aux, false);
         r += k == 1;
         c += k == 2;
+        if (k) hit |= 1u << e;
+        if (k == 1) is_res |= 1u << e;
     }
     int tot;
     const int pre = block_excl_scan(r | (c << 16), warp_tot, &tot);
-    if (r == 0 && c == 0) return;
+    if (!hit) return;
     int pr = oo.x + (pre & 0xffff), pc = oo.y + (pre >> 16);
-    for (int e = 0; e < kCompactPer; e++) {
-        const int64_t u = u0 + e;
-        if (u >= n_user) break;
+    for (uint32_t m = hit; m; m &= m - 1) {
+        const int e = __ffs(m) - 1;
+        if ((is_res >> e & 1) && pr >= topk) { pr++; continue; }
         typename P::Aux aux;
-        const int k = p.classify(q, u, aux);
+        const int k = p.classify(q, u0 + e, aux, true);
         if (k == 1) {
-            if (pr < topk) p.emit_result(q, pr, u, aux);
+            if (pr < topk) p.emit_result(q, pr, u0 + e, aux);
             pr++;
         } else if (k == 2) {
-            p.emit_cand(q, pc, u, aux);
+            p.emit_cand(q, pc, u0 + e, aux);
             pc++;
         }
     }
@@ -683,6 +706,8 @@ struct Profiler {
         cudaEventCreate(&e);
         return e;
     }
+    // A counter reported beside the kernels (no time; `launches` carries the count).
+    void add_count(const char *n, int64_t v) { launches[id_of(n)] += v; }
     int id_of(const char *n) {
         for (size_t i = 0; i < names.size(); i++) if (names[i] == n) return (int) i;
         names.emplace_back(n);

@@ -7,13 +7,16 @@
 //   2. full SVD-space score for the survivors (ComputeRemainDim, :76-95) -> sampled-threshold
 //      bounds (SampleSearch::RankBound) -> prune again.
 // Here a batch of queries runs as passes over all (query, user) pairs:
-//   * one tile kernel computes, for every pair, the partial score, its round-1 levels and the full
-//     score (partial + remainder, two separately accumulated sums added once, as the reference adds
-//     them);
-//   * round 2 is a streaming pass that gives each surviving pair the coarse group of its sampled-
-//     threshold bucket from a per-user summary held in shared memory;
+//   * one tile kernel computes, for every pair, the partial score and its round-1 levels (a fast
+//     binary32 screen of the regression arithmetic; undecided pairs go to the reference's own
+//     arithmetic in a fix-up kernel), then the full score (partial + remainder, two separately
+//     accumulated sums added once, as the reference adds them) and the coarse group of its
+//     sampled-threshold bucket from a per-user summary of every 16th threshold;
+//   * round 2 is a streaming pass that marks the pairs that did not survive round 1 and counts the
+//     survivors by group;
 //   * the exact bucket is resolved only where the k-th bound and the class counts need it: for the
-//     pairs in the critical group(s) of each query, and for the users that end up reported.
+//     pairs in the critical group(s) of each query, and for the users that end up reported, from
+//     recomputed scores.
 // The reference keeps its per-user score vector across queries; users accepted in round 1 are
 // reported with whatever that vector holds for them.  The batch reproduces it: the score a user had
 // at its latest earlier query in which it reached round 2, or the index's carried state when there
@@ -138,31 +141,27 @@ __device__ __forceinline__ RegUser reg_user(const RegModel &m, int64_t u) {
     return r;
 }
 
+// Level of one side from the integral-valued c = ceil (lower bound) or floor (upper bound) of
+// pred -+ err: c >= S -> S + 1, c < 0 -> low, else c + 1.
+__device__ __forceinline__ int level_of(float c, int S, int low) {
+    return c >= (float) S ? S + 1 : (c < 0.0f ? low : (int) c + 1);
+}
+
 // Screened ComputeRankBound: the fast CDF decides a side whenever pred -+ err lies farther than
-// the margin from an integer, so that the reference's ceil / floor cannot differ.  Returns false
+// the margin from an integer, so that the reference's ceil / floor cannot differ (values beyond
+// 1e18, where the reference's int64 conversion saturates, are left undecided too).  Returns false
 // when a side is undecided (its level is then not meaningful).
 __device__ __forceinline__ bool regression_levels_fast(const RegUser &r, int S, float qlb, float qub, int &lvl_lb,
                                                        int &lvl_ub) {
-    bool ok = true;
-    if (qlb > r.smax) lvl_lb = 1;
-    else if (qlb < r.smin || r.err_big) lvl_lb = S + 1;
-    else {
-        const float v = fmaf(cdf_phi_fast(__fsub_rn(qlb, r.mu) * r.inv_sigma), r.a, r.b) + r.err;
-        ok = fabsf(v - rintf(v)) > r.margin && fabsf(v) < 1e18f;
-        const int64_t pr = ok ? (int64_t) ceilf(v) : 0;
-        lvl_lb = pr >= S ? S + 1 : (pr < 0 ? 1 : (int) pr + 1);
-    }
-    if (qub > r.smax) lvl_ub = 0;
-    else if (qub < r.smin) lvl_ub = S;
-    else if (r.err_big) lvl_ub = 0;
-    else {
-        const float v = fmaf(cdf_phi_fast(__fsub_rn(qub, r.mu) * r.inv_sigma), r.a, r.b) - r.err;
-        const bool ok2 = fabsf(v - rintf(v)) > r.margin && fabsf(v) < 1e18f;
-        const int64_t pr = ok2 ? (int64_t) floorf(v) : 0;
-        lvl_ub = pr >= S ? S + 1 : (pr < 0 ? 0 : (int) pr + 1);
-        ok = ok && ok2;
-    }
-    return ok;
+    const float vl = fmaf(cdf_phi_fast(__fsub_rn(qlb, r.mu) * r.inv_sigma), r.a, r.b) + r.err;
+    const float vu = fmaf(cdf_phi_fast(__fsub_rn(qub, r.mu) * r.inv_sigma), r.a, r.b) - r.err;
+    const bool in_l = !(qlb > r.smax) && !(qlb < r.smin) && !r.err_big;
+    const bool in_u = !(qub > r.smax) && !(qub < r.smin) && !r.err_big;
+    const bool ok_l = fabsf(vl - rintf(vl)) > r.margin && fabsf(vl) < 1e18f;
+    const bool ok_u = fabsf(vu - rintf(vu)) > r.margin && fabsf(vu) < 1e18f;
+    lvl_lb = qlb > r.smax ? 1 : (in_l ? level_of(ceilf(vl), S, 1) : S + 1);
+    lvl_ub = qub > r.smax ? 0 : (qub < r.smin ? S : (r.err_big ? 0 : level_of(floorf(vu), S, 0)));
+    return (!in_l || ok_l) && (!in_u || ok_u);
 }
 
 __device__ __forceinline__ int level_rank(int lvl, const int32_t *rank, int S, int n_item) {
@@ -181,6 +180,7 @@ struct QsrpParams {
     int32_t mode2, L2, U2, n_elig2;        // round 2
     int32_t exact1, lv_res, lv_pr, lv_m1;  // exact1: count round-1 classes pair by pair; level thresholds
     int32_t crit, cum_before, mask1, mask2;  // critical coarse group, users below it, groups to resolve
+    int32_t gneed_lo, gneed_hi, pad0, pad1;  // groups 0..31 / 32 whose pairs the compaction must classify
 };
 
 // Round-1 class in level space: rank(level) is non-decreasing in the level, so lb <= U1 is
@@ -216,21 +216,43 @@ __global__ void transfer_query_kernel(const float *__restrict__ query, const flo
     }
 }
 
+// Exact SVD-space partial score of (query, user) over the first check_dim coordinates
+// (PartDimPartNorm.hpp:62).
+struct ScoreSrc {
+    const float *svd_user, *qtr;
+    int dim, c;
+    __device__ float left(int64_t u, int64_t q) const { return exact_dot(svd_user + u * dim, qtr + q * dim, c); }
+};
+
+// The batch's full scores as the tile kernel stored them ([query][user]).
+struct QipView {
+    const float *qip;
+    int64_t n_user;
+    __device__ float operator()(int64_t u, int64_t q) const { return __ldg(qip + q * n_user + u); }
+};
+
 // Pairs the screen left undecided, resolved by qsrp_fix1_kernel: (query, user, partial score).
+// Past the list's capacity the pair's levels are written as kLvUndecided and count keeps growing,
+// which sends qsrp_fix1_scan_kernel over the whole batch.
 struct FixList {
     int4 *e;
     int *count;
     int cap;
 };
+constexpr uint32_t kLvUndecided = 0xffffffffu;
 
 // Tiles of 128 users x 128 queries: the partial score over the first check_dim coordinates, the
-// bounds partial -+ norms and their regression levels (lb | ub << 16), then the full score.
+// bounds partial -+ norms and their regression levels (lb | ub << 16); then the full score and the
+// coarse group of its sampled-threshold bucket (the round-2 code of the pair if it reaches round 2).
 struct Round1Epi {
     static constexpr size_t kExtra = sizeof(float) * kBig;
-    const float *unorm, *qnorm;
+    static constexpr int kSummStride = ThrSummary::kMaxGroups + 1;
+    const float *unorm, *qnorm, *thr_summ;
     RegModel m;
     uint32_t *lv;
+    uint8_t *code;
     float *qip;
+    int nb;
     int64_t n_user, n_query;
     FixList fix;
     __device__ void prologue(char *x, int64_t, int64_t b0) const {
@@ -245,14 +267,17 @@ struct Round1Epi {
         if (u >= n_user) return;
         const RegUser r = reg_user(m, u);
         const float un = __ldg(unorm + u);
-        for (int i = 0; i < kBig / 2; i++) {
+        uint32_t *out = lv + (b0 + half) * n_user + u;
+        const int64_t step = 2 * n_user;
+        const int64_t left_rows = (n_query - b0 - half + 1) / 2;
+        const int nrow = left_rows < kBig / 2 ? (int) left_rows : kBig / 2;
+        for (int i = 0; i < nrow; i++, out += step) {
             const int rb = half + 2 * i;
-            const int64_t q = b0 + rb;
-            if (q >= n_query) break;
             const float left = res.v[rb][ra];
             const float right = __fmul_rn(un, qn[rb]);
             int l, h;
             const bool ok = regression_levels_fast(r, m.S, __fsub_rn(left, right), __fadd_rn(left, right), l, h);
+            uint32_t packed = (uint32_t) l | ((uint32_t) h << 16);
             const unsigned need = __ballot_sync(alive, !ok);
             if (need) {
                 const int leader = __ffs(need) - 1;
@@ -261,28 +286,56 @@ struct Round1Epi {
                 base = __shfl_sync(alive, base, leader);
                 if (!ok) {
                     const int idx = base + __popc(need & ((1u << lane) - 1));
-                    if (idx < fix.cap) fix.e[idx] = make_int4((int) q, (int) u, __float_as_int(left), 0);
-                    else regression_levels_exact(m, u, __fsub_rn(left, right), __fadd_rn(left, right), l, h);
+                    if (idx < fix.cap) fix.e[idx] = make_int4((int) (b0 + rb), (int) u, __float_as_int(left), 0);
+                    else packed = kLvUndecided;
                 }
             }
-            lv[q * n_user + u] = (uint32_t) l | ((uint32_t) h << 16);
+            *out = packed;
         }
     }
-    __device__ void finish_hi(char *, const BigResult &res, int64_t a0, int64_t b0) const {
+    __device__ void finish_hi(char *, const BigResult &res, int64_t a0, int64_t b0, char *spare) const {
+        float *summ = reinterpret_cast<float *>(spare);  // [128][kSummStride]
+        for (int idx = threadIdx.x; idx < kBig * ThrSummary::kMaxGroups; idx += kBigThreads) {
+            const int rr = idx / ThrSummary::kMaxGroups, j = idx % ThrSummary::kMaxGroups;
+            summ[rr * kSummStride + j] =
+                a0 + rr < n_user ? __ldg(thr_summ + (a0 + rr) * ThrSummary::kMaxGroups + j) : 0.0f;
+        }
+        __syncthreads();
         const int ra = threadIdx.x & (kBig - 1), half = threadIdx.x >> 7;
         const int64_t u = a0 + ra;
         if (u >= n_user) return;
-        for (int i = 0; i < kBig / 2; i++) {
-            const int rb = half + 2 * i;
-            const int64_t q = b0 + rb;
-            if (q >= n_query) break;
-            qip[q * n_user + u] = res.v[rb][ra];
+        const float *sm = summ + ra * kSummStride;
+        const int64_t base = (b0 + half) * n_user + u, step = 2 * n_user;
+        const int64_t left_rows = (n_query - b0 - half + 1) / 2;
+        const int nrow = left_rows < kBig / 2 ? (int) left_rows : kBig / 2;
+        // Groups are the summary entries >= s (the summary descends; unused entries are -inf):
+        // a fixed five-step search plus one compare, four queries at a time.
+        constexpr int G = 4;
+        for (int i0 = 0; i0 < nrow; i0 += G) {
+            float sv[G];
+            int lo[G];
+#pragma unroll
+            for (int g = 0; g < G; g++) {
+                sv[g] = res.v[half + 2 * min(i0 + g, nrow - 1)][ra];
+                lo[g] = 0;
+            }
+#pragma unroll
+            for (int st = 16; st >= 1; st >>= 1)
+#pragma unroll
+                for (int g = 0; g < G; g++) lo[g] += sm[lo[g] + st - 1] >= sv[g] ? st : 0;
+#pragma unroll
+            for (int g = 0; g < G; g++) {
+                lo[g] = min(lo[g] + (sm[lo[g]] >= sv[g]), nb);  // a score of -inf passes the padding too
+                if (i0 + g < nrow) {
+                    code[base + (i0 + g) * step] = (uint8_t) lo[g];
+                    qip[base + (i0 + g) * step] = sv[g];
+                }
+            }
         }
     }
 };
 
-// The reference's arithmetic for the pairs the screen left undecided (listed ones; pairs beyond
-// the list's capacity were resolved in place).
+// The reference's arithmetic for the pairs the screen left undecided (the listed ones).
 __global__ void qsrp_fix1_kernel(FixList fix, RegModel m, const float *__restrict__ unorm,
                                  const float *__restrict__ qnorm, int64_t n_user, uint32_t *__restrict__ lv) {
     const int n = min(*fix.count, fix.cap);
@@ -293,6 +346,24 @@ __global__ void qsrp_fix1_kernel(FixList fix, RegModel m, const float *__restric
         int l, h;
         regression_levels_exact(m, e.y, __fsub_rn(left, right), __fadd_rn(left, right), l, h);
         lv[(int64_t) e.x * n_user + e.y] = (uint32_t) l | ((uint32_t) h << 16);
+    }
+}
+
+// Undecided pairs beyond the list's capacity: a scan of the batch's levels for kLvUndecided, with the
+// partial score recomputed.  Returns at once when the list held them all.
+__global__ void qsrp_fix1_scan_kernel(const int *__restrict__ count, int cap, RegModel m, ScoreSrc sc,
+                                      const float *__restrict__ unorm, const float *__restrict__ qnorm, int64_t n_user,
+                                      int nq, uint32_t *__restrict__ lv) {
+    if (*count <= cap) return;
+    const int64_t n = n_user * nq;
+    for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
+        if (lv[i] != kLvUndecided) continue;
+        const int64_t q = i / n_user, u = i % n_user;
+        const float left = sc.left(u, q);
+        const float right = __fmul_rn(__ldg(unorm + u), __ldg(qnorm + q));
+        int l, h;
+        regression_levels_exact(m, u, __fsub_rn(left, right), __fadd_rn(left, right), l, h);
+        lv[i] = (uint32_t) l | ((uint32_t) h << 16);
     }
 }
 
@@ -428,16 +499,6 @@ __global__ void qsrp_final1_kernel(QsrpParams *__restrict__ par, int nq, int top
 
 // ---- round 2 -------------------------------------------------------------------------------------
 
-// Number of groups whose last (smallest) threshold is >= s: the coarse group of s's bucket.
-__device__ __forceinline__ int coarse_group(const float *summ, int nb, float s) {
-    int lo = 0, len = nb;
-    while (len > 0) {
-        const int h = len >> 1, m = lo + h;
-        if (summ[m] >= s) { lo = m + 1; len -= h + 1; } else len = h;
-    }
-    return lo;
-}
-
 // The bucket of s inside coarse group g (< nb): g * gs + the group's thresholds >= s.
 __device__ __forceinline__ int fine_bucket(const float *__restrict__ row, int S, int gs, int g, float s) {
     const int base = g * gs, end = min(base + gs, S);
@@ -456,59 +517,53 @@ __device__ __forceinline__ int fine_bucket(const float *__restrict__ row, int S,
     return base + c;
 }
 
-constexpr int kScreenUsers = 256, kScreenQueries = 256;
-
-// Round 2 for a block of 256 users x up to 256 queries: pairs that reached round 2 (neither pruned
-// nor accepted in round 1) get the coarse group of their full score's bucket, the others their
-// round-1 state code.  The users' group summaries stay in shared memory.
-__global__ void __launch_bounds__(kScreenUsers) qsrp_screen2_kernel(const uint32_t *__restrict__ lv,
-                                                                   const float *__restrict__ qip, int64_t n_user, int nq,
-                                                                   const QsrpParams *__restrict__ par,
-                                                                   const float *__restrict__ thr_summ, int nb,
-                                                                   uint8_t *__restrict__ code) {
-    __shared__ float summ[kScreenUsers][ThrSummary::kMaxGroups + 1];
-    __shared__ int4 pp[kScreenQueries];
-    const int64_t u0 = (int64_t) blockIdx.x * kScreenUsers;
-    const int q0 = blockIdx.y * kScreenQueries, nqc = min(kScreenQueries, nq - q0);
-    for (int idx = threadIdx.x; idx < kScreenUsers * ThrSummary::kMaxGroups; idx += kScreenUsers) {
-        const int r = idx / ThrSummary::kMaxGroups, j = idx % ThrSummary::kMaxGroups;
-        const int64_t u = u0 + r;
-        summ[r][j] = u < n_user ? __ldg(thr_summ + u * ThrSummary::kMaxGroups + j) : 0.0f;
+// Round 2 per (user chunk, query): pairs that did not reach round 2 get their round-1 state code in
+// place of the group code; the others are counted by group (per-warp shared-memory copies).
+__global__ void __launch_bounds__(kHistThreads) qsrp_round2_kernel(const uint32_t *__restrict__ lv,
+                                                                  uint8_t *__restrict__ code, int64_t n_user,
+                                                                  const QsrpParams *__restrict__ par, int nb,
+                                                                  int64_t chunk, int *__restrict__ hist_c) {
+    extern __shared__ int h[];
+    const int nbin = nb + 1, copies = hist_copies(nbin);
+    const int q = blockIdx.y;
+    QsrpParams p;
+    {
+        const QsrpParams &g = par[q];
+        p.mode1 = g.mode1; p.all1 = g.all1; p.lv_res = g.lv_res; p.lv_pr = g.lv_pr; p.lv_m1 = g.lv_m1;
     }
-    for (int i = threadIdx.x; i < nqc; i += kScreenUsers) {
-        const QsrpParams &p = par[q0 + i];
-        pp[i] = make_int4(p.mode1 | (p.all1 << 1), p.lv_res, p.lv_pr, p.lv_m1);
+    for (int b = threadIdx.x; b < copies * nbin; b += blockDim.x) h[b] = 0;
+    __syncthreads();
+    int *mine = h + ((threadIdx.x >> 5) % copies) * nbin;
+    const uint32_t *lrow = lv + (int64_t) q * n_user;
+    uint8_t *crow = code + (int64_t) q * n_user;
+    const int64_t u0 = (int64_t) blockIdx.x * chunk, u1 = min(u0 + chunk, n_user);
+    constexpr int G = 4;
+    for (int64_t ub = u0 + threadIdx.x; ub < u1; ub += G * kHistThreads) {
+        uint32_t v[G];
+        bool el[G];
+#pragma unroll
+        for (int g = 0; g < G; g++) v[g] = ub + g * kHistThreads < u1 ? lrow[ub + g * kHistThreads] : 0u;
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            const int64_t u = ub + g * kHistThreads;
+            if (u >= u1) break;
+            const int k = class1_lv(p, v[g] & 0xffff, v[g] >> 16);
+            el[g] = k == kClsRefine || k == kClsIdle;
+            if (!el[g]) crow[u] = k == kClsResult ? kCodeResult1 : kCodePruned1;
+        }
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            const int64_t u = ub + g * kHistThreads;
+            if (u >= u1) break;
+            if (el[g]) atomicAdd(mine + crow[u], 1);
+        }
     }
     __syncthreads();
-    const int64_t u = u0 + threadIdx.x;
-    if (u >= n_user) return;
-    const float *sm = summ[threadIdx.x];
-    // four queries at a time: their level loads, then the score loads of the survivors, are in flight together
-    constexpr int G = 4;
-    for (int i0 = 0; i0 < nqc; i0 += G) {
-        uint32_t v[G];
-        int k[G];
-        float s[G];
-#pragma unroll
-        for (int g = 0; g < G; g++) v[g] = i0 + g < nqc ? __ldg(lv + (int64_t) (q0 + i0 + g) * n_user + u) : 0u;
-#pragma unroll
-        for (int g = 0; g < G; g++) {
-            const int4 c = pp[min(i0 + g, nqc - 1)];
-            QsrpParams p;
-            p.mode1 = c.x & 1; p.all1 = c.x >> 1; p.lv_res = c.y; p.lv_pr = c.z; p.lv_m1 = c.w;
-            k[g] = class1_lv(p, v[g] & 0xffff, v[g] >> 16);
-            const bool el = i0 + g < nqc && (k[g] == kClsRefine || k[g] == kClsIdle);
-            s[g] = el ? __ldg(qip + (int64_t) (q0 + i0 + g) * n_user + u) : 0.0f;
-            if (!el && k[g] != kClsResult) k[g] = kClsPrune;
-        }
-#pragma unroll
-        for (int g = 0; g < G; g++) {
-            if (i0 + g >= nqc) break;
-            uint8_t out;
-            if (k[g] == kClsRefine || k[g] == kClsIdle) out = (uint8_t) coarse_group(sm, nb, s[g]);
-            else out = k[g] == kClsResult ? kCodeResult1 : kCodePruned1;
-            code[(int64_t) (q0 + i0 + g) * n_user + u] = out;
-        }
+    int *gh = hist_c + (int64_t) q * nbin;
+    for (int b = threadIdx.x; b < nbin; b += blockDim.x) {
+        int sum = 0;
+        for (int c = 0; c < copies; c++) sum += h[c * nbin + b];
+        if (sum) atomicAdd(gh + b, sum);
     }
 }
 
@@ -520,7 +575,7 @@ __global__ void qsrp_select2c_kernel(const int *__restrict__ hist_c, int nb, int
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nq) return;
     QsrpParams p = par[q];
-    p.crit = -1; p.cum_before = -1; p.mask1 = 0; p.mask2 = 0;
+    p.crit = -1; p.cum_before = -1; p.mask1 = 0; p.mask2 = 0; p.gneed_lo = 0; p.gneed_hi = 0;
     if (p.skip2) {
         QueryCounts c = {};
         c.n_result = p.n_res1;
@@ -551,23 +606,26 @@ __global__ void qsrp_select2c_kernel(const int *__restrict__ hist_c, int nb, int
 }
 
 // Exact bucket histogram of the pairs whose coarse group is flagged for their query (mask1 or
-// mask2), one CTA per (user chunk, query).
-__global__ void __launch_bounds__(kHistThreads) qsrp_fine2_kernel(const uint8_t *__restrict__ code,
-                                                                 const float *__restrict__ qip, int64_t n_user,
-                                                                 const float *__restrict__ thr, int S, int gs,
-                                                                 const QsrpParams *__restrict__ par, int second,
-                                                                 int64_t chunk, int *__restrict__ hist_f) {
+// mask2); grid (users / (256 x 16), queries), each thread 16 consecutive users.
+__global__ void __launch_bounds__(256) qsrp_fine2_kernel(const uint8_t *__restrict__ code, QipView sc, int64_t n_user,
+                                                        const float *__restrict__ thr, int S, int gs,
+                                                        const QsrpParams *__restrict__ par, int second,
+                                                        int *__restrict__ hist_f) {
     const int q = blockIdx.y;
     const uint32_t mask = (uint32_t) (second ? par[q].mask2 : par[q].mask1);
     if (!mask) return;
-    const uint8_t *row = code + (int64_t) q * n_user;
-    const int64_t u0 = (int64_t) blockIdx.x * chunk, u1 = min(u0 + chunk, n_user);
+    const int64_t u0 = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) * 16;
+    if (u0 >= n_user) return;
+    const int n = (int) (n_user - u0 < 16 ? n_user - u0 : 16);
+    uint32_t w[4];
+    load16_bytes(code + (int64_t) q * n_user + u0, w);
     int *hq = hist_f + (int64_t) q * (S + 1);
-    for (int64_t u = u0 + threadIdx.x; u < u1; u += kHistThreads) {
-        const unsigned c = row[u];
-        if (c < 32 && (mask >> c & 1u)) {
-            const float s = __ldg(qip + (int64_t) q * n_user + u);
-            atomicAdd(hq + fine_bucket(thr + u * S, S, gs, (int) c, s), 1);
+#pragma unroll
+    for (int e = 0; e < 16; e++) {
+        const unsigned c = (w[e >> 2] >> (8 * (e & 3))) & 0xff;
+        if (e < n && c < 32 && (mask >> c & 1u)) {
+            const int64_t u = u0 + e;
+            atomicAdd(hq + fine_bucket(thr + u * S, S, gs, (int) c, sc(u, q)), 1);
         }
     }
 }
@@ -640,7 +698,7 @@ __global__ void qsrp_final2_kernel(const int *__restrict__ hist_c, const int *__
                                    uint8_t *__restrict__ clsg, QueryCounts *__restrict__ counts) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nq) return;
-    const QsrpParams p = par[q];
+    QsrpParams p = par[q];
     if (p.skip2) return;
     QueryCounts c = {};
     c.lstar = p.L2;
@@ -676,17 +734,28 @@ __global__ void qsrp_final2_kernel(const int *__restrict__ hist_c, const int *__
         c.n_prune = (int) npr;
         c.n_cand = nres >= topk ? 0 : (int) nref;
     }
+    const uint8_t *cg = clsg + (int64_t) q * (nb + 1);
+    uint64_t need = 0;
+    for (int g = 0; g <= nb; g++) {
+        const uint8_t k = cg[g];
+        if (k == kClsResult || k == kClsMixed || (k == kClsRefine && c.n_cand > 0)) need |= uint64_t(1) << g;
+    }
+    p.gneed_lo = (int32_t) (uint32_t) need;
+    p.gneed_hi = (int32_t) (uint32_t) (need >> 32);
+    par[q] = p;
     counts[q] = c;
 }
 
 // Classification of a pair after both rounds for the ordered compaction: result users carry their
 // reported rank (the lower bound in force) and whether their score is this query's; candidates
-// carry their round-2 bounds.  Exact buckets are resolved here for the few pairs that need one.
+// carry their round-2 bounds.  Exact buckets are resolved only where the group does not settle the
+// class or the entry's fields are asked for.
 struct QsrpCompactPolicy {
     struct Aux { int rank, fresh, lb, ub; };
     const uint32_t *lv;
     const uint8_t *code;
-    const float *qip, *thr;
+    const float *thr;
+    QipView sc;
     int64_t n_user;
     const int32_t *reg_rank, *rank;
     int S_reg, S, n_item, nb, gs;
@@ -699,20 +768,40 @@ struct QsrpCompactPolicy {
     uint8_t *res_fresh;
     int32_t *cand_user, *cand_query, *cand_lb, *cand_ub;
     __device__ bool query_active(int q) const { return true; }
-    __device__ int classify(int q, int64_t u, Aux &aux) const {
+    // Users whose code can make them a result or a candidate: a group the compaction must
+    // classify, a round-1 result, or any non-survivor under the equal-bounds rule.
+    __device__ uint32_t need_mask(int q, int64_t u, int n) const {
+        const QsrpParams &p = par[q];
+        const uint64_t gneed = (uint64_t) (uint32_t) p.gneed_lo | ((uint64_t) (uint32_t) p.gneed_hi << 32);
+        const bool state_any = !p.skip2 && p.mode2;
+        uint32_t w[4];
+        load16_bytes(code + (int64_t) q * n_user + u, w);
+        uint32_t m = 0;
+#pragma unroll
+        for (int e = 0; e < kCompactPer; e++) {
+            const unsigned c = (w[e >> 2] >> (8 * (e & 3))) & 0xff;
+            const bool nd = c <= (unsigned) nb ? (bool) (gneed >> c & 1) : (c == kCodeResult1 || state_any);
+            m |= (uint32_t) nd << e;
+        }
+        return n >= 32 ? m : m & ((1u << n) - 1);
+    }
+    __device__ int classify(int q, int64_t u, Aux &aux, bool with_aux) const {
         const int64_t at = (int64_t) q * n_user + u;
         const unsigned c = code[at];
         if (c <= (unsigned) nb) {  // reached round 2
             if (par[q].skip2) return 0;
             const uint8_t kg = clsg[(int64_t) q * (nb + 1) + c];
             if (kg == kClsPrune || kg == kClsIdle) return 0;
-            const int b = c == (unsigned) nb ? S : fine_bucket(thr + u * S, S, gs, (int) c, __ldg(qip + at));
+            const bool cand_ok = counts[q].n_cand > 0;
+            if (kg == kClsRefine && !cand_ok) return 0;
+            if (!with_aux && kg != kClsMixed) return kg == kClsResult ? 1 : 2;
+            const int b = c == (unsigned) nb ? S : fine_bucket(thr + u * S, S, gs, (int) c, sc(u, q));
             const uint8_t k2 = cls2[(int64_t) q * (S + 1) + b];
             int lb, ub;
             bucket_bounds(b, S, rank, n_item, lb, ub);
             aux.rank = lb; aux.fresh = 1; aux.lb = lb; aux.ub = ub;
             if (k2 == kClsResult) return 1;
-            return (k2 == kClsRefine && counts[q].n_cand > 0) ? 2 : 0;
+            return (k2 == kClsRefine && cand_ok) ? 2 : 0;
         }
         aux.fresh = 0;
         const QsrpParams &p = par[q];
@@ -746,8 +835,8 @@ struct QsrpCompactPolicy {
 // score from its latest earlier round-2 query in the batch, else the carried state.
 __global__ void qsrp_result_fill_kernel(const QueryCounts *__restrict__ counts, const int32_t *__restrict__ res_user,
                                         const uint8_t *__restrict__ res_fresh, const uint8_t *__restrict__ code,
-                                        const float *__restrict__ qip, int64_t n_user, const float *__restrict__ state,
-                                        int topk, float *__restrict__ res_qip) {
+                                        QipView sc, int64_t n_user, const float *__restrict__ state, int topk,
+                                        float *__restrict__ res_qip) {
     const int q = blockIdx.x;
     const int n = counts[q].n_res_emit;
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
@@ -756,26 +845,25 @@ __global__ void qsrp_result_fill_kernel(const QueryCounts *__restrict__ counts, 
         int src = res_fresh[i] ? q : -1;
         for (int qq = q - 1; src < 0 && qq >= 0; qq--)
             if (code[(int64_t) qq * n_user + u] < kCodeResult1) src = qq;
-        res_qip[i] = src >= 0 ? qip[(int64_t) src * n_user + u] : state[u];
+        res_qip[i] = src >= 0 ? sc(u, src) : state[u];
     }
 }
 
 __global__ void qsrp_cand_fill_kernel(const int32_t *__restrict__ cand_user, const int32_t *__restrict__ cand_query,
-                                      int64_t n, const float *__restrict__ qip, int64_t n_user,
-                                      float *__restrict__ cand_qip) {
+                                      int64_t n, QipView sc, float *__restrict__ cand_qip) {
     const int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n) return;
-    cand_qip[e] = qip[(int64_t) cand_query[e] * n_user + cand_user[e]];
+    cand_qip[e] = sc(cand_user[e], cand_query[e]);
 }
 
 // Carried state after the batch: each user's score at its last round-2 query of the batch.
-__global__ void qsrp_state_kernel(const uint8_t *__restrict__ code, const float *__restrict__ qip, int64_t n_user,
-                                  int nq, float *__restrict__ state) {
+__global__ void qsrp_state_kernel(const uint8_t *__restrict__ code, QipView sc, int64_t n_user, int nq,
+                                  float *__restrict__ state) {
     const int64_t u = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= n_user) return;
     for (int q = nq - 1; q >= 0; q--)
         if (code[(int64_t) q * n_user + u] < kCodeResult1) {
-            state[u] = qip[(int64_t) q * n_user + u];
+            state[u] = sc(u, q);
             return;
         }
 }
@@ -791,7 +879,6 @@ template <typename T> T *carve(uint8_t *&p, size_t n) {
     return r;
 }
 inline size_t carve_size(size_t n, size_t elem) { return ((n * elem + 255) & ~size_t(255)) + 256; }
-constexpr int kFixCap = 1 << 22;
 }  // namespace
 
 int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_rank *d_out, rkr_query_stats *d_stats,
@@ -815,7 +902,8 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     RKR_TRY(ix->ws_counts.ensure(sizeof(QueryCounts) * (size_t) nq));
     const size_t n_hist_l = (size_t) nq * 2 * nl, n_hist_c = (size_t) nq * (nb + 1), n_hist_f = (size_t) nq * (S + 1);
     RKR_TRY(ix->ws_hist.ensure(carve_size(n_hist_l, 4) + carve_size(n_hist_c, 4) + carve_size(n_hist_f, 4)));
-    RKR_TRY(ix->ws_fix.ensure(carve_size(kFixCap, sizeof(int4))));
+    const int fix_cap = (int) std::min<int64_t>(int64_t(1) << 26, std::max<int64_t>(int64_t(1) << 20, U * nq / 64));
+    RKR_TRY(ix->ws_fix.ensure(carve_size(fix_cap, sizeof(int4))));
     uint32_t *lv = ix->ws_levels.as<uint32_t>();
     float *qip = reinterpret_cast<float *>(lv + (size_t) nq * U);
     uint8_t *code = ix->ws_bucket2.as<uint8_t>();
@@ -829,9 +917,9 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     int *hist_f = carve<int>(ph, n_hist_f);
     uint8_t *pm = ix->ws_fix.as<uint8_t>();
     FixList fix;
-    fix.e = carve<int4>(pm, kFixCap);
+    fix.e = carve<int4>(pm, fix_cap);
     fix.count = fix_count;
-    fix.cap = kFixCap;
+    fix.cap = fix_cap;
     RKR_CUDA(cudaMemsetAsync(anomaly, 0, sizeof(int) * nq, st));
     RKR_CUDA(cudaMemsetAsync(fix_count, 0, sizeof(int), st));
     RKR_CUDA(cudaMemsetAsync(ix->ws_hist.p, 0, (size_t) (ph - ix->ws_hist.as<uint8_t>()), st));
@@ -840,26 +928,39 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
         transfer_query_kernel<<<nq, 128, 0, st>>>(d_query, ix->transfer_item.as<float>(), dim, c, qtr, qnorm);
     });
     RKR_CUDA(cudaGetLastError());
+    ScoreSrc sc;
+    sc.svd_user = ix->svd_user.as<float>();
+    sc.qtr = qtr;
+    sc.dim = dim;
+    sc.c = c;
     RegModel m;
     m.rec = ix->reg.as<float>();
     m.rank = ix->reg_rank.as<int32_t>();
     m.S = Sr;
     m.err_cap = (double) Sr - 1e-3;
     m.n_item = n_item;
+    QipView qv;
+    qv.qip = qip;
+    qv.n_user = U;
     Round1Epi e1;
     e1.unorm = ix->svd_unorm.as<float>();
     e1.qnorm = qnorm;
+    e1.thr_summ = ix->thr_summ.as<float>();
     e1.m = m;
     e1.lv = lv;
+    e1.code = code;
     e1.qip = qip;
+    e1.nb = nb;
     e1.n_user = U;
     e1.n_query = nq;
     e1.fix = fix;
     cudaError_t ce = cudaSuccess;
     timed(ix, st, "qsrp_scores", [&] { ce = launch_big_split(ix->svd_user.as<float>(), U, dim, qtr, nq, dim, c, dim, e1, st); });
     RKR_CUDA(ce);
-    timed(ix, st, "qsrp_fix1", [&] {
-        qsrp_fix1_kernel<<<148 * 4, 256, 0, st>>>(fix, m, e1.unorm, qnorm, U, lv);
+    timed(ix, st, "qsrp_fix1", [&] { qsrp_fix1_kernel<<<148 * 4, 256, 0, st>>>(fix, m, e1.unorm, qnorm, U, lv); });
+    RKR_CUDA(cudaGetLastError());
+    timed(ix, st, "qsrp_fix1_scan", [&] {
+        qsrp_fix1_scan_kernel<<<148 * 8, 256, 0, st>>>(fix_count, fix_cap, m, sc, e1.unorm, qnorm, U, nq, lv);
     });
     RKR_CUDA(cudaGetLastError());
     const int64_t chunk = 16384;
@@ -880,16 +981,9 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     }
     timed(ix, st, "qsrp_final1", [&] { qsrp_final1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, topk); });
     RKR_CUDA(cudaGetLastError());
-    {
-        dim3 g((unsigned) ((U + kScreenUsers - 1) / kScreenUsers), (unsigned) ((nq + kScreenQueries - 1) / kScreenQueries));
-        timed(ix, st, "qsrp_screen2", [&] {
-            qsrp_screen2_kernel<<<g, kScreenUsers, 0, st>>>(lv, qip, U, nq, par, ix->thr_summ.as<float>(), nb, code);
-        });
-        RKR_CUDA(cudaGetLastError());
-    }
-    timed(ix, st, "group_hist", [&] {
-        bucket_hist_kernel<<<hg, kHistThreads, hist_copies(nb + 1) * (nb + 1) * sizeof(int), st>>>(code, U, nb + 1, chunk,
-                                                                                                  hist_c);
+    timed(ix, st, "qsrp_round2", [&] {
+        qsrp_round2_kernel<<<hg, kHistThreads, hist_copies(nb + 1) * (nb + 1) * sizeof(int), st>>>(lv, code, U, par, nb,
+                                                                                                  chunk, hist_c);
     });
     RKR_CUDA(cudaGetLastError());
     timed(ix, st, "qsrp_select2c", [&] {
@@ -898,8 +992,9 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     RKR_CUDA(cudaGetLastError());
     const float *thr = ix->thr.as<float>();
     const int32_t *srank = ix->sample_rank.as<int32_t>();
+    const dim3 fg((unsigned) ((U + 256 * 16 - 1) / (256 * 16)), (unsigned) nq);
     timed(ix, st, "qsrp_fine2", [&] {
-        qsrp_fine2_kernel<<<hg, kHistThreads, 0, st>>>(code, qip, U, thr, S, gs, par, 0, chunk, hist_f);
+        qsrp_fine2_kernel<<<fg, 256, 0, st>>>(code, qv, U, thr, S, gs, par, 0, hist_f);
     });
     RKR_CUDA(cudaGetLastError());
     timed(ix, st, "qsrp_select2f", [&] {
@@ -907,7 +1002,7 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     });
     RKR_CUDA(cudaGetLastError());
     timed(ix, st, "qsrp_fine2", [&] {
-        qsrp_fine2_kernel<<<hg, kHistThreads, 0, st>>>(code, qip, U, thr, S, gs, par, 1, chunk, hist_f);
+        qsrp_fine2_kernel<<<fg, 256, 0, st>>>(code, qv, U, thr, S, gs, par, 1, hist_f);
     });
     RKR_CUDA(cudaGetLastError());
     timed(ix, st, "qsrp_final2", [&] {
@@ -916,8 +1011,11 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     RKR_CUDA(cudaGetLastError());
 
     std::vector<QueryCounts> hc(nq);
+    int h_fix = 0;
     RKR_CUDA(cudaMemcpyAsync(hc.data(), counts, sizeof(QueryCounts) * nq, cudaMemcpyDeviceToHost, st));
+    RKR_CUDA(cudaMemcpyAsync(&h_fix, fix_count, sizeof(int), cudaMemcpyDeviceToHost, st));
     RKR_CUDA(cudaStreamSynchronize(st));
+    if (ix->prof.on) ix->prof.add_count("screen_undecided_pairs", h_fix);
     std::vector<int64_t> off(nq + 1, 0);
     for (int q = 0; q < nq; q++) off[q + 1] = off[q] + hc[q].n_cand;
     const int64_t n_cand = off[nq];
@@ -939,8 +1037,8 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     QsrpCompactPolicy pol;
     pol.lv = lv;
     pol.code = code;
-    pol.qip = qip;
     pol.thr = thr;
+    pol.sc = qv;
     pol.n_user = U;
     pol.reg_rank = m.rank;
     pol.rank = srank;
@@ -964,13 +1062,13 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     pol.cand_ub = cand_ub;
     RKR_TRY(run_compaction(ix, pol, nq, topk, counts, st));
     timed(ix, st, "qsrp_result_fill", [&] {
-        qsrp_result_fill_kernel<<<nq, 128, 0, st>>>(counts, res_user, res_fresh, code, qip, U, ix->qip_state.as<float>(),
+        qsrp_result_fill_kernel<<<nq, 128, 0, st>>>(counts, res_user, res_fresh, code, qv, U, ix->qip_state.as<float>(),
                                                     topk, res_qip);
     });
     RKR_CUDA(cudaGetLastError());
     if (n_cand > 0) {
         timed(ix, st, "qsrp_cand_fill", [&] {
-            qsrp_cand_fill_kernel<<<(unsigned) ((n_cand + 255) / 256), 256, 0, st>>>(cand_user, cand_query, n_cand, qip, U,
+            qsrp_cand_fill_kernel<<<(unsigned) ((n_cand + 255) / 256), 256, 0, st>>>(cand_user, cand_query, n_cand, qv,
                                                                                     cand_qip);
         });
         RKR_CUDA(cudaGetLastError());
@@ -978,7 +1076,7 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     RKR_TRY(refine_and_assemble_qsrp(ix, d_query, nq, topk, counts, res_user, res_rank, res_qip, n_cand, cand_user,
                                      cand_query, cand_lb, cand_ub, cand_qip, d_off, d_out, d_stats, st));
     timed(ix, st, "qsrp_state", [&] {
-        qsrp_state_kernel<<<(unsigned) ((U + 255) / 256), 256, 0, st>>>(code, qip, U, nq, ix->qip_state.as<float>());
+        qsrp_state_kernel<<<(unsigned) ((U + 255) / 256), 256, 0, st>>>(code, qv, U, nq, ix->qip_state.as<float>());
     });
     RKR_CUDA(cudaGetLastError());
     RKR_CUDA(cudaStreamSynchronize(st));

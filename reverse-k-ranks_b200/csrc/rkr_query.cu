@@ -152,7 +152,8 @@ struct QsCompactPolicy {
     int32_t *res_user, *cand_user, *cand_query;
     uint16_t *cand_bucket;
     __device__ bool query_active(int q) const { return true; }
-    __device__ int classify(int q, int64_t u, Aux &aux) const {
+    __device__ uint32_t need_mask(int, int64_t, int n) const { return (1u << n) - 1; }
+    __device__ int classify(int q, int64_t u, Aux &aux, bool) const {
         const uint16_t b = bucket[(int64_t) q * n_user + u];
         aux.b = b;
         const uint8_t k = __ldg(cls + (int64_t) q * (S + 1) + b);

@@ -77,3 +77,22 @@ def test_qsrp_full_size_matches_reference(full):
     for f in ("n_prune", "n_result", "n_refine", "ip_cost"):
         assert np.array_equal(sa[f], sb[f]), (f, sa[f], sb[f])
     assert same(a, b)
+
+
+def test_qsrp_full_batch_matches_oracle_on_sample(full):
+    """A 1,000-query batch (the throughput benchmark's batch) at full size: every 40th query's
+    result ids, ranks and counters equal the oracle's.  Ids, ranks and counters do not depend on the
+    scores carried between queries, so the sampled queries can be checked on their own."""
+    orc = Oracle()
+    ix = full["ix"]
+    rng = np.random.default_rng(5)
+    batch = full["item"][rng.choice(N_ITEM, 1000, replace=False)].copy()
+    ix.reset_state()
+    a, sa = ix.retrieval("QSRPNormalLP", batch, 100, stats=True)
+    pick = np.arange(0, 1000, 40)
+    b, sb = orc.qsrp_retrieval(full["un"], full["su"], full["ti"], full["item"], full["cd"], full["rank"], full["thr"],
+                               full["rank"], full["reg"], batch[pick], 100)
+    for f in STAT_FIELDS:
+        assert np.array_equal(sa[f][pick], sb[f]), (f, sa[f][pick], sb[f])
+    assert np.array_equal(a["user_id"][pick], b["user_id"])
+    assert np.array_equal(a["rank"][pick], b["rank"])

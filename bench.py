@@ -168,20 +168,21 @@ class Clocks:
 
 
 def kernel_model(name, cfg, nq, stats):
-    """Algorithmic (ops, bytes) per launch of the query kernels, from the workload's sizes."""
+    """Algorithmic (ops, bytes) per launch of the query kernels, from the workload's sizes.
+
+    ops counts binary32 multiplies and adds as separate operations: the exact dot products round
+    every product and every partial sum (no FMA), so each coordinate costs one multiply and one add.
+    bytes is what the kernel must move through HBM at the least."""
     n_user, n_item, dim = CONFIGS[cfg][:3]
-    c = stats["check_dim"]
-    if name == "qsrp_round1":
-        return 2.0 * n_user * nq * c, 4.0 * n_user * c + 4.0 * n_user * nq + 36.0 * n_user + 4.0 * nq * dim
+    pairs = float(n_user) * nq
+    if name == "qsrp_scores":
+        # per pair: levels (4 B) + full score (4 B) + round-2 group (1 B) written; the users'
+        # SVD vectors, regression records (32 B) and threshold summaries (128 B) read once
+        return 2.0 * pairs * dim, 9.0 * pairs + n_user * (4.0 * dim + 32 + 128) + 4.0 * nq * dim
     if name == "qsrp_round2":
-        el = stats["eligible2"]
-        return 2.0 * el * dim, 4.0 * n_user * nq + 2.0 * n_user * nq + 4.0 * el * 9
-    if name in ("qsrp_select1", "qsrp_count1"):
-        return 0.0, 4.0 * n_user * nq
-    if name == "qsrp_select2":
-        return 0.0, 2.0 * n_user * nq
-    if name == "qsrp_compact":
-        return 0.0, 6.0 * n_user * nq
+        return 0.0, 4.0 * pairs + 1.0 * pairs
+    if name == "level_hist":
+        return 0.0, 4.0 * pairs
     if name == "refine_tile":
         return 2.0 * stats["n_compute_item"] * dim, 4.0 * stats["n_compute_item"] * dim
     return 0.0, 0.0
@@ -343,9 +344,10 @@ def main():
     torch.cuda.synchronize()
     prof = ix.profile_read()
     ix.profile(False)
+    counters = {k: int(v[1]) for k, v in prof.items() if k.endswith("_pairs")}
+    prof = {k: v for k, v in prof.items() if not k.endswith("_pairs")}
     st = np.frombuffer(d_stats.cpu().numpy().tobytes(), dtype=R.QUERY_STATS)
-    model_stats = {"check_dim": parts["cd"], "n_compute_item": float(st["n_compute_item"].sum()),
-                   "eligible2": float(n_user * batch)}
+    model_stats = {"check_dim": parts["cd"], "n_compute_item": float(st["n_compute_item"].sum())}
     launches_per_step = sum(c for _, c in prof.values())
     stats_mean = {f: float(st[f].mean()) for f in R.QUERY_STATS.names}
     dom = max(prof.items(), key=lambda kv: kv[1][0])
@@ -364,7 +366,8 @@ def main():
                 "share_of_step": dom_ms / max(sum(v[0] for v in prof.values()), 1e-9),
                 "simt_fp32": {"achieved_tops": ops / avg_s / 1e12, "peak_tops_nominal": simt_peak_tops,
                               "frac": (ops / avg_s / 1e12) / simt_peak_tops},
-                "kernels_ms_per_step": {k: round(v[0], 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])}}
+                "kernels_ms_per_step": {k: round(v[0], 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
+                "counters_per_step": counters}
 
     # ---- latency ------------------------------------------------------------------------------------------
     single = []

@@ -155,6 +155,12 @@ __device__ __forceinline__ void exact_tile(TileSmem &sm, const float *__restrict
 // consecutive A rows, so outputs indexed [b][a] are written coalesced.
 
 constexpr int kBig = 128, kBigK = 16, kBigPad = 4, kBigThreads = 256;
+// k steps unrolled per iteration of the inner loop (the body is 128 FP32 instructions per step;
+// full unrolling of a stage overflows the instruction cache).
+#ifndef RKR_BIG_KK_UNROLL
+#define RKR_BIG_KK_UNROLL 4
+#endif
+constexpr int kBigKUnroll = RKR_BIG_KK_UNROLL;
 
 struct BigOperands {
     float a[2][kBigK][kBig + kBigPad];
@@ -173,7 +179,7 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
 __device__ __forceinline__ void big_load_stage(BigOperands &op, int buf, const float *__restrict__ A,
-                                               const int32_t *__restrict__ a_idx, int64_t n_a, int lda, int64_t a0,
+                                               const int32_t *__restrict__ a_rows, int64_t n_a, int lda, int64_t a0,
                                                const float *__restrict__ B, int64_t n_b, int ldb, int64_t b0, int k0,
                                                int k_end) {
 #pragma unroll 1
@@ -183,17 +189,18 @@ __device__ __forceinline__ void big_load_stage(BigOperands &op, int buf, const f
         const int k = k0 + kk;
         const int64_t ra = a0 + r, rb = b0 + r;
         const bool va = ra < n_a && k < k_end, vb = rb < n_b && k < k_end;
-        const int64_t row = va ? (a_idx ? (int64_t) a_idx[ra] : ra) : 0;
+        const int64_t row = va ? (a_rows ? (int64_t) a_rows[r] : ra) : 0;
         cp_async4(&op.a[buf][kk][r], va ? A + row * lda + k : A, va);
         cp_async4(&op.b[buf][kk][r], vb ? B + rb * ldb + k : B, vb);
     }
 }
 
 // Accumulates into acc (zeroed here) the thread's 8 x 8 block of dot products over [k_begin, k_end):
-// A rows a0 + 4 tx + {0..3, 64..67}, B rows b0 + 4 ty + {0..3, 64..67}.  Returns after a barrier,
-// with the operand buffers free.  Returns false (no barrier, acc zero) for an empty range.
+// A rows a0 + 4 tx + {0..3, 64..67} (or, with a_rows, the rows a_rows[4 tx + ...] of the tile's
+// gather list), B rows b0 + 4 ty + {0..3, 64..67}.  Returns after a barrier, with the operand
+// buffers free.  Returns false (no barrier, acc zero) for an empty range.
 __device__ __forceinline__ bool big_accumulate(BigOperands &op, float acc[8][8], const float *__restrict__ A,
-                                              const int32_t *__restrict__ a_idx, int64_t n_a, int lda, int64_t a0,
+                                              const int32_t *__restrict__ a_rows, int64_t n_a, int lda, int64_t a0,
                                               const float *__restrict__ B, int64_t n_b, int ldb, int64_t b0, int k_begin,
                                               int k_end) {
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -203,11 +210,11 @@ __device__ __forceinline__ bool big_accumulate(BigOperands &op, float acc[8][8],
         for (int j = 0; j < 8; j++) acc[i][j] = 0.0f;
     const int ns = (k_end - k_begin + kBigK - 1) / kBigK;
     if (ns <= 0) return false;
-    big_load_stage(op, 0, A, a_idx, n_a, lda, a0, B, n_b, ldb, b0, k_begin, k_end);
+    big_load_stage(op, 0, A, a_rows, n_a, lda, a0, B, n_b, ldb, b0, k_begin, k_end);
     cp_async_commit();
     for (int s = 0; s < ns; s++) {
         if (s + 1 < ns) {
-            big_load_stage(op, (s + 1) & 1, A, a_idx, n_a, lda, a0, B, n_b, ldb, b0, k_begin + (s + 1) * kBigK, k_end);
+            big_load_stage(op, (s + 1) & 1, A, a_rows, n_a, lda, a0, B, n_b, ldb, b0, k_begin + (s + 1) * kBigK, k_end);
             cp_async_commit();
             cp_async_wait<1>();
         } else {
@@ -215,7 +222,7 @@ __device__ __forceinline__ bool big_accumulate(BigOperands &op, float acc[8][8],
         }
         __syncthreads();
         const int buf = s & 1;
-#pragma unroll
+#pragma unroll kBigKUnroll
         for (int kk = 0; kk < kBigK; kk++) {
             const float4 a_lo = *reinterpret_cast<const float4 *>(&op.a[buf][kk][4 * tx]);
             const float4 a_hi = *reinterpret_cast<const float4 *>(&op.a[buf][kk][64 + 4 * tx]);
@@ -253,7 +260,8 @@ __device__ __forceinline__ void big_store(BigResult &res, const float acc[8][8],
     }
 }
 
-// Fills res with the 128 x 128 block of dot products (A rows a0.., B rows b0..) over [k_begin, k_end).
+// Fills res with the 128 x 128 block of dot products (A rows a0.., or a_idx[0..127] as a tile-local
+// gather list, B rows b0..) over [k_begin, k_end).
 __device__ __forceinline__ void exact_big_tile(char *smem, const float *__restrict__ A, const int32_t *__restrict__ a_idx,
                                               int64_t n_a, int lda, int64_t a0, const float *__restrict__ B,
                                               int64_t n_b, int ldb, int64_t b0, int k_begin, int k_end) {
@@ -279,7 +287,7 @@ __device__ __forceinline__ void exact_big_tile(char *smem, const float *__restri
         }
         __syncthreads();
         const int buf = s & 1;
-#pragma unroll
+#pragma unroll kBigKUnroll
         for (int kk = 0; kk < kBigK; kk++) {
             const float4 a_lo = *reinterpret_cast<const float4 *>(&op.a[buf][kk][4 * tx]);
             const float4 a_hi = *reinterpret_cast<const float4 *>(&op.a[buf][kk][64 + 4 * tx]);
@@ -318,10 +326,12 @@ __global__ void __launch_bounds__(kBigThreads, 2) exact_big_kernel(const float *
     char *extra = big_smem + kBigSmem;
     const int64_t b0 = (int64_t) blockIdx.x * kBig;
     const int64_t a0 = (int64_t) blockIdx.y * kBig;
+    __shared__ int32_t rows_s[kBig];  // the tile's gathered A rows
+    if (a_idx && threadIdx.x < kBig) rows_s[threadIdx.x] = a0 + threadIdx.x < n_a ? a_idx[a0 + threadIdx.x] : 0;
     epi.prologue(extra, a0, b0);
     __syncthreads();
     const bool live = epi.active(extra, a0, b0);
-    if (live) exact_big_tile(big_smem, A, a_idx, n_a, lda, a0, B, n_b, ldb, b0, k_begin, k_end);
+    if (live) exact_big_tile(big_smem, A, a_idx ? rows_s : nullptr, n_a, lda, a0, B, n_b, ldb, b0, k_begin, k_end);
     epi.finish(extra, *reinterpret_cast<const BigResult *>(big_smem), a0, b0, live);
 }
 
@@ -334,9 +344,12 @@ inline size_t big_kernel_smem() { return kBigSmem + Epi::kExtra; }
 // epi.finish_hi(extra, res, a0, b0, spare) sees the totals; spare is the operand buffers'
 // sizeof(BigOperands) bytes, free by then.  Operands and result have separate shared memory, so the
 // second range's loads do not wait for finish_lo.  Epi also provides kExtra and
-// prologue(extra, a0, b0).  Every thread calls each hook (they may synchronise the block).
+// prologue(extra, a0, b0), which returns whether the tile has work (the same answer in every
+// thread; false ends the CTA).  Rows of A may be gathered through a_idx.  Every thread calls each
+// hook (they may synchronise the block).
 template <class Epi>
-__global__ void __launch_bounds__(kBigThreads, 2) exact_big_split_kernel(const float *__restrict__ A, int64_t n_a,
+__global__ void __launch_bounds__(kBigThreads, 2) exact_big_split_kernel(const float *__restrict__ A,
+                                                                         const int32_t *__restrict__ a_idx, int64_t n_a,
                                                                          int lda, const float *__restrict__ B,
                                                                          int64_t n_b, int ldb, int k_split, int k_end,
                                                                          Epi epi) {
@@ -346,28 +359,34 @@ __global__ void __launch_bounds__(kBigThreads, 2) exact_big_split_kernel(const f
     char *extra = big_smem + sizeof(BigOperands) + sizeof(BigResult);
     const int64_t b0 = (int64_t) blockIdx.x * kBig;
     const int64_t a0 = (int64_t) blockIdx.y * kBig;
-    epi.prologue(extra, a0, b0);
+    if (!epi.prologue(extra, a0, b0)) return;
+    __shared__ int32_t rows_s[kBig];  // the tile's gathered A rows
+    if (a_idx) {
+        if (threadIdx.x < kBig) rows_s[threadIdx.x] = a0 + threadIdx.x < n_a ? a_idx[a0 + threadIdx.x] : 0;
+        __syncthreads();
+    }
+    const int32_t *a_rows = a_idx ? rows_s : nullptr;
     float acc[8][8];
-    big_accumulate(op, acc, A, nullptr, n_a, lda, a0, B, n_b, ldb, b0, 0, k_split);
+    big_accumulate(op, acc, A, a_rows, n_a, lda, a0, B, n_b, ldb, b0, 0, k_split);
     big_store(res, acc, false);
     __syncthreads();
     epi.finish_lo(extra, res, a0, b0);
     // big_accumulate's first barrier orders finish_lo's reads of res before the adds below
-    if (!big_accumulate(op, acc, A, nullptr, n_a, lda, a0, B, n_b, ldb, b0, k_split, k_end)) __syncthreads();
+    if (!big_accumulate(op, acc, A, a_rows, n_a, lda, a0, B, n_b, ldb, b0, k_split, k_end)) __syncthreads();
     big_store(res, acc, true);
     __syncthreads();
     epi.finish_hi(extra, res, a0, b0, big_smem);
 }
 
 template <class Epi>
-inline cudaError_t launch_big_split(const float *A, int64_t n_a, int lda, const float *B, int64_t n_b, int ldb,
-                                    int k_split, int k_end, const Epi &epi, cudaStream_t st) {
+inline cudaError_t launch_big_split(const float *A, const int32_t *a_idx, int64_t n_a, int lda, const float *B,
+                                    int64_t n_b, int ldb, int k_split, int k_end, const Epi &epi, cudaStream_t st) {
     const size_t smem = sizeof(BigOperands) + sizeof(BigResult) + Epi::kExtra;
     cudaError_t e =
         cudaFuncSetAttribute(exact_big_split_kernel<Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
     if (e != cudaSuccess) return e;
     dim3 grid((unsigned) ((n_b + kBig - 1) / kBig), (unsigned) ((n_a + kBig - 1) / kBig));
-    exact_big_split_kernel<Epi><<<grid, kBigThreads, smem, st>>>(A, n_a, lda, B, n_b, ldb, k_split, k_end, epi);
+    exact_big_split_kernel<Epi><<<grid, kBigThreads, smem, st>>>(A, a_idx, n_a, lda, B, n_b, ldb, k_split, k_end, epi);
     return cudaGetLastError();
 }
 

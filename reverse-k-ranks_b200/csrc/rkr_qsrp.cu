@@ -122,10 +122,11 @@ __device__ __noinline__ void regression_levels_exact(const RegModel &m, int64_t 
     }
 }
 
-// One user's model prepared for the screen.
+// One user's model prepared for the screen.  A user whose fit error reaches the cap (the
+// reference then gives up on the model: ComputeRankBound's error test) gets an infinite margin,
+// so every one of its pairs goes to the reference's own arithmetic.
 struct RegUser {
     float a, b, mu, inv_sigma, err, smax, smin, margin;
-    bool err_big;
 };
 
 __device__ __forceinline__ RegUser reg_user(const RegModel &m, int64_t u) {
@@ -134,10 +135,11 @@ __device__ __forceinline__ RegUser reg_user(const RegModel &m, int64_t u) {
     RegUser r;
     r.a = r0.x; r.b = r0.y; r.mu = r0.z; r.inv_sigma = __frcp_rn(r0.w);
     r.err = r1.x; r.smax = r1.y; r.smin = r1.z;
-    r.err_big = (double) r1.x >= m.err_cap;
     // |pred -+ err| moves by at most |a| * kCdfFastErr through the CDF, plus a few roundings of
     // values no larger than |a| + |b| + |err| in either evaluation.
-    r.margin = fabsf(r.a) * kCdfFastErr + (fabsf(r.a) + fabsf(r.b) + fabsf(r.err)) * 4.8e-7f + 1e-6f;
+    r.margin = (double) r1.x >= m.err_cap
+                   ? INFINITY
+                   : fabsf(r.a) * kCdfFastErr + (fabsf(r.a) + fabsf(r.b) + fabsf(r.err)) * 4.8e-7f + 1e-6f;
     return r;
 }
 
@@ -155,13 +157,15 @@ __device__ __forceinline__ bool regression_levels_fast(const RegUser &r, int S, 
                                                        int &lvl_ub) {
     const float vl = fmaf(cdf_phi_fast(__fsub_rn(qlb, r.mu) * r.inv_sigma), r.a, r.b) + r.err;
     const float vu = fmaf(cdf_phi_fast(__fsub_rn(qub, r.mu) * r.inv_sigma), r.a, r.b) - r.err;
-    const bool in_l = !(qlb > r.smax) && !(qlb < r.smin) && !r.err_big;
-    const bool in_u = !(qub > r.smax) && !(qub < r.smin) && !r.err_big;
+    const bool in_l = !(qlb > r.smax) && !(qlb < r.smin);
+    const bool in_u = !(qub > r.smax) && !(qub < r.smin);
+    // |v| < 1e18 (the reference's int64 conversion is exact there) folds into the margin test
     const bool ok_l = fabsf(vl - rintf(vl)) > r.margin && fabsf(vl) < 1e18f;
     const bool ok_u = fabsf(vu - rintf(vu)) > r.margin && fabsf(vu) < 1e18f;
     lvl_lb = qlb > r.smax ? 1 : (in_l ? level_of(ceilf(vl), S, 1) : S + 1);
-    lvl_ub = qub > r.smax ? 0 : (qub < r.smin ? S : (r.err_big ? 0 : level_of(floorf(vu), S, 0)));
-    return (!in_l || ok_l) && (!in_u || ok_u);
+    lvl_ub = qub > r.smax ? 0 : (in_u ? level_of(floorf(vu), S, 0) : S);
+    // a capped-error user's margin is infinite: its in-range sides are always left undecided
+    return (!in_l || ok_l) && (!in_u || ok_u) && r.margin < INFINITY;
 }
 
 __device__ __forceinline__ int level_rank(int lvl, const int32_t *rank, int S, int n_item) {
@@ -255,9 +259,10 @@ struct Round1Epi {
     int nb;
     int64_t n_user, n_query;
     FixList fix;
-    __device__ void prologue(char *x, int64_t, int64_t b0) const {
+    __device__ bool prologue(char *x, int64_t, int64_t b0) const {
         float *qn = reinterpret_cast<float *>(x);
         if (threadIdx.x < kBig) qn[threadIdx.x] = b0 + threadIdx.x < n_query ? __ldg(qnorm + b0 + threadIdx.x) : 0.0f;
+        return true;
     }
     __device__ void finish_lo(char *x, const BigResult &res, int64_t a0, int64_t b0) const {
         const float *qn = reinterpret_cast<const float *>(x);
@@ -271,26 +276,39 @@ struct Round1Epi {
         const int64_t step = 2 * n_user;
         const int64_t left_rows = (n_query - b0 - half + 1) / 2;
         const int nrow = left_rows < kBig / 2 ? (int) left_rows : kBig / 2;
-        for (int i = 0; i < nrow; i++, out += step) {
-            const int rb = half + 2 * i;
-            const float left = res.v[rb][ra];
-            const float right = __fmul_rn(un, qn[rb]);
-            int l, h;
-            const bool ok = regression_levels_fast(r, m.S, __fsub_rn(left, right), __fadd_rn(left, right), l, h);
-            uint32_t packed = (uint32_t) l | ((uint32_t) h << 16);
-            const unsigned need = __ballot_sync(alive, !ok);
-            if (need) {
-                const int leader = __ffs(need) - 1;
-                int base = 0;
-                if (lane == leader) base = atomicAdd(fix.count, __popc(need));
-                base = __shfl_sync(alive, base, leader);
-                if (!ok) {
-                    const int idx = base + __popc(need & ((1u << lane) - 1));
-                    if (idx < fix.cap) fix.e[idx] = make_int4((int) (b0 + rb), (int) u, __float_as_int(left), 0);
-                    else packed = kLvUndecided;
+        // two queries per iteration: their screens are independent chains
+        for (int i = 0; i < nrow; i += 2, out += 2 * step) {
+            float left[2];
+            uint32_t packed[2];
+            bool ok[2];
+#pragma unroll
+            for (int g = 0; g < 2; g++) {
+                const int rb = half + 2 * min(i + g, nrow - 1);
+                left[g] = res.v[rb][ra];
+                const float right = __fmul_rn(un, qn[rb]);
+                int l, h;
+                ok[g] = regression_levels_fast(r, m.S, __fsub_rn(left[g], right), __fadd_rn(left[g], right), l, h);
+                packed[g] = (uint32_t) l | ((uint32_t) h << 16);
+            }
+            ok[1] = ok[1] || i + 1 >= nrow;
+#pragma unroll
+            for (int g = 0; g < 2; g++) {
+                const unsigned need = __ballot_sync(alive, !ok[g]);
+                if (need) {
+                    const int leader = __ffs(need) - 1;
+                    int base = 0;
+                    if (lane == leader) base = atomicAdd(fix.count, __popc(need));
+                    base = __shfl_sync(alive, base, leader);
+                    if (!ok[g]) {
+                        const int idx = base + __popc(need & ((1u << lane) - 1));
+                        if (idx < fix.cap)
+                            fix.e[idx] = make_int4((int) (b0 + half + 2 * (i + g)), (int) u, __float_as_int(left[g]), 0);
+                        else packed[g] = kLvUndecided;
+                    }
                 }
             }
-            *out = packed;
+            out[0] = packed[0];
+            if (i + 1 < nrow) out[step] = packed[1];
         }
     }
     __device__ void finish_hi(char *, const BigResult &res, int64_t a0, int64_t b0, char *spare) const {
@@ -387,12 +405,19 @@ __global__ void __launch_bounds__(kHistThreads) level_hist_kernel(const uint32_t
     const uint32_t *row = lv + (int64_t) q * n_user;
     const int64_t u0 = (int64_t) blockIdx.x * chunk, u1 = min(u0 + chunk, n_user);
     int my_anom = 0;
-    for (int64_t u = u0 + threadIdx.x; u < u1; u += kHistThreads) {
-        const uint32_t v = row[u];
-        const int l = v & 0xffff, hh = v >> 16;
-        atomicAdd(mine + l, 1);
-        atomicAdd(mine + nl + hh, 1);
-        my_anom += hh > l && level_rank(hh, rank, S, n_item) > level_rank(l, rank, S, n_item);
+    constexpr int G = 8;  // loads in flight per thread
+    for (int64_t ub = u0 + threadIdx.x; ub < u1; ub += G * kHistThreads) {
+        uint32_t v[G];
+#pragma unroll
+        for (int g = 0; g < G; g++) v[g] = ub + g * kHistThreads < u1 ? __ldg(row + ub + g * kHistThreads) : 0xffffffffu;
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+            if (v[g] == 0xffffffffu) continue;
+            const int l = v[g] & 0xffff, hh = v[g] >> 16;
+            atomicAdd(mine + l, 1);
+            atomicAdd(mine + nl + hh, 1);
+            my_anom += hh > l && level_rank(hh, rank, S, n_item) > level_rank(l, rank, S, n_item);
+        }
     }
     if (my_anom) atomicAdd(&anom, my_anom);
     __syncthreads();
@@ -537,12 +562,12 @@ __global__ void __launch_bounds__(kHistThreads) qsrp_round2_kernel(const uint32_
     const uint32_t *lrow = lv + (int64_t) q * n_user;
     uint8_t *crow = code + (int64_t) q * n_user;
     const int64_t u0 = (int64_t) blockIdx.x * chunk, u1 = min(u0 + chunk, n_user);
-    constexpr int G = 4;
+    constexpr int G = 4;  // loads in flight per thread
     for (int64_t ub = u0 + threadIdx.x; ub < u1; ub += G * kHistThreads) {
         uint32_t v[G];
         bool el[G];
 #pragma unroll
-        for (int g = 0; g < G; g++) v[g] = ub + g * kHistThreads < u1 ? lrow[ub + g * kHistThreads] : 0u;
+        for (int g = 0; g < G; g++) v[g] = ub + g * kHistThreads < u1 ? __ldg(lrow + ub + g * kHistThreads) : 0u;
 #pragma unroll
         for (int g = 0; g < G; g++) {
             const int64_t u = ub + g * kHistThreads;
@@ -955,7 +980,7 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     e1.n_query = nq;
     e1.fix = fix;
     cudaError_t ce = cudaSuccess;
-    timed(ix, st, "qsrp_scores", [&] { ce = launch_big_split(ix->svd_user.as<float>(), U, dim, qtr, nq, dim, c, dim, e1, st); });
+    timed(ix, st, "qsrp_scores", [&] { ce = launch_big_split(ix->svd_user.as<float>(), nullptr, U, dim, qtr, nq, dim, c, dim, e1, st); });
     RKR_CUDA(ce);
     timed(ix, st, "qsrp_fix1", [&] { qsrp_fix1_kernel<<<148 * 4, 256, 0, st>>>(fix, m, e1.unorm, qnorm, U, lv); });
     RKR_CUDA(cudaGetLastError());

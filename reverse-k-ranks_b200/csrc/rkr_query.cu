@@ -234,79 +234,92 @@ __global__ void refine_prep_kernel(RefineArgs a) {
     a.ref_user[slot] = u;
 }
 
-// Candidates x items: the reference's per-item test, summed per candidate
+// Candidates x items on 128 x 128 tiles: the reference's per-item test, summed per candidate
 // (RefineCPUIPBound::RefineRank, RefineCPUIPBound.hpp:93-150, with the split sums of
-// RefineCPUPartDimPartNorm.hpp:83-152; RefineCPU::RefineRank, RefineCPU.hpp:33-55).
-__global__ void __launch_bounds__(kTileThreads) refine_tile_kernel(RefineArgs a, const float *__restrict__ items,
-                                                                  const float *__restrict__ item_rnorm,
-                                                                  const float *__restrict__ user_rnorm,
-                                                                  int check_dim) {
-    __shared__ TileSmem sm;
-    __shared__ int nproc_s[kTile];
-    __shared__ float qip_s[kTile], urn_s[kTile];
-    __shared__ int cnt_s[kTile], und_s[kTile];
-    __shared__ int max_np;
-    const int n_ref = *a.n_ref;
-    const int64_t b0 = (int64_t) blockIdx.x * kTile;  // items
-    const int ks = a.ipbound ? check_dim : a.dim;
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    for (int64_t a0 = (int64_t) blockIdx.y * kTile; a0 < n_ref; a0 += (int64_t) gridDim.y * kTile) {
-        __syncthreads();
-        if (threadIdx.x == 0) max_np = 0;
-        __syncthreads();
-        if (threadIdx.x < kTile) {
-            const int64_t r = a0 + threadIdx.x;
-            int np = 0;
+// RefineCPUPartDimPartNorm.hpp:83-152; RefineCPU::RefineRank, RefineCPU.hpp:33-55).  The partial
+// score over the first check_dim coordinates +- the product of the remaining norms settles most
+// items; the undecided ones are tested on partial + remainder.  Rows are the refined candidates
+// (users gathered through ref_user, whose entries past n_ref are 0), columns the items in the
+// order the bound assumes; a candidate's items past its cut-off nproc are not counted.
+struct RefineEpi {
+    static constexpr size_t kExtra = sizeof(int) * kBig * 2 + sizeof(float) * kBig * 3 + sizeof(uint32_t) * kBigThreads * 2;
+    RefineArgs a;
+    const float *item_rnorm, *user_rnorm;
+    int64_t row0;  // candidate offset of this launch
+    __device__ int *rows_e(char *x) const { return reinterpret_cast<int *>(x); }
+    __device__ int *rows_np(char *x) const { return reinterpret_cast<int *>(x) + kBig; }
+    __device__ float *rows_qv(char *x) const { return reinterpret_cast<float *>(x) + 2 * kBig; }
+    __device__ float *rows_un(char *x) const { return reinterpret_cast<float *>(x) + 3 * kBig; }
+    __device__ float *cols_rn(char *x) const { return reinterpret_cast<float *>(x) + 4 * kBig; }
+    __device__ uint32_t *und_bits(char *x) const { return reinterpret_cast<uint32_t *>(x) + 5 * kBig; }
+    __device__ bool prologue(char *x, int64_t a0, int64_t b0) const {
+        const int n_ref = *a.n_ref;
+        bool live = false;
+        if (threadIdx.x < kBig) {
+            const int64_t r = row0 + a0 + threadIdx.x;
+            int e = -1, np = 0;
             float qv = 0.0f, un = 0.0f;
             if (r < n_ref) {
-                const int e = a.ref_idx[r];
+                e = a.ref_idx[r];
                 np = a.nproc[e];
                 qv = a.qip[e];
                 if (a.ipbound) un = user_rnorm[a.ref_user[r]];
             }
-            nproc_s[threadIdx.x] = np;
-            qip_s[threadIdx.x] = qv;
-            urn_s[threadIdx.x] = un;
-            cnt_s[threadIdx.x] = 0;
-            und_s[threadIdx.x] = 0;
-            atomicMax(&max_np, np);
+            rows_e(x)[threadIdx.x] = e;
+            rows_np(x)[threadIdx.x] = np;
+            rows_qv(x)[threadIdx.x] = qv;
+            rows_un(x)[threadIdx.x] = un;
+            const int64_t it = b0 + threadIdx.x;
+            cols_rn(x)[threadIdx.x] = a.ipbound && it < a.n_item ? __ldg(item_rnorm + it) : 0.0f;
+            live = b0 < np;
         }
-        __syncthreads();
-        if (b0 >= max_np) continue;
-        float lo[4][4], hi[4][4];
-        exact_tile(sm, a.user, a.ref_user, n_ref, a.dim, a0, items, a.n_item, a.dim, b0, 0, ks, a.dim, lo, hi);
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            const int r = 4 * tx + i;
-            const float qv = qip_s[r];
-            const int np = nproc_s[r];
+        return __syncthreads_or(live);
+    }
+    __device__ void finish_lo(char *x, const BigResult &res, int64_t, int64_t b0) const {
+        const int ra = threadIdx.x & (kBig - 1), half = threadIdx.x >> 7;
+        const int e = rows_e(x)[ra];
+        uint32_t bits[2] = {0u, 0u};
+        if (e >= 0) {
+            const int np = rows_np(x)[ra];
+            const float qv = rows_qv(x)[ra], un = rows_un(x)[ra];
+            const float lowq = __fsub_rn(qv, 8e-3f), highq = __fadd_rn(qv, 8e-3f);
+            const float *rn = cols_rn(x);
             int c = 0, und = 0;
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const int64_t it = b0 + 4 * ty + j;
-                if (it >= np) continue;
+            for (int i = 0; i < kBig / 2; i++) {
+                const int rb = half + 2 * i;
+                if (b0 + rb >= np) break;
+                const float lo = res.v[rb][ra];
                 if (a.ipbound) {
-                    const float lowq = __fsub_rn(qv, 8e-3f), highq = __fadd_rn(qv, 8e-3f);
-                    const float right = __fmul_rn(__ldg(item_rnorm + it), urn_s[r]);
-                    const float lbv = __fsub_rn(lo[i][j], right), ubv = __fadd_rn(lo[i][j], right);
+                    const float right = __fmul_rn(rn[rb], un);
+                    const float lbv = __fsub_rn(lo, right), ubv = __fadd_rn(lo, right);
                     if (lowq > ubv) continue;
                     if (highq < lbv) { c++; continue; }
                     und++;
-                    c += __fadd_rn(lo[i][j], hi[i][j]) >= qv;
+                    bits[i >> 5] |= 1u << (i & 31);
                 } else {
-                    c += lo[i][j] > qv;
+                    c += lo > qv;
                 }
             }
-            if (c) atomicAdd(&cnt_s[r], c);
-            if (und) atomicAdd(&und_s[r], und);
+            if (c) atomicAdd(a.rank + e, c);
+            if (und) atomicAdd(a.undecided + e, und);
         }
-        __syncthreads();
-        if (threadIdx.x < kTile && a0 + threadIdx.x < n_ref) {
-            if (cnt_s[threadIdx.x]) atomicAdd(a.rank + a.ref_idx[a0 + threadIdx.x], cnt_s[threadIdx.x]);
-            if (und_s[threadIdx.x]) atomicAdd(a.undecided + a.ref_idx[a0 + threadIdx.x], und_s[threadIdx.x]);
-        }
+        und_bits(x)[2 * threadIdx.x] = bits[0];
+        und_bits(x)[2 * threadIdx.x + 1] = bits[1];
     }
-}
+    __device__ void finish_hi(char *x, const BigResult &res, int64_t, int64_t, char *) const {
+        const int ra = threadIdx.x & (kBig - 1), half = threadIdx.x >> 7;
+        const int e = rows_e(x)[ra];
+        if (e < 0) return;
+        const float qv = rows_qv(x)[ra];
+        int c = 0;
+        for (int w = 0; w < 2; w++)
+            for (uint32_t m = und_bits(x)[2 * threadIdx.x + w]; m; m &= m - 1) {
+                const int i = 32 * w + __ffs(m) - 1;
+                c += res.v[half + 2 * i][ra] >= qv;
+            }
+        if (c) atomicAdd(a.rank + e, c);
+    }
+};
 
 // ============================================================================================
 // assembly
@@ -549,6 +562,7 @@ static int refine_and_assemble(rkr_index *ix, int method, const float *d_query, 
     int32_t *undecided = carve<int32_t>(p, n_cand);
     int32_t *n_ref = carve<int32_t>(p, 1);
     RKR_CUDA(cudaMemsetAsync(n_ref, 0, sizeof(int32_t), st));
+    RKR_CUDA(cudaMemsetAsync(ref_user, 0, sizeof(int32_t) * n_cand, st));
     if (n_cand > 0) {
         RefineArgs ra;
         ra.user = ix->user.as<float>();
@@ -573,11 +587,21 @@ static int refine_and_assemble(rkr_index *ix, int method, const float *d_query, 
         timed(ix, st, "refine_prep", [&] { refine_prep_kernel<<<(unsigned) ((n_cand + 255) / 256), 256, 0, st>>>(ra); });
         RKR_CUDA(cudaGetLastError());
         const float *items = ipbound ? ix->item_sorted.as<float>() : ix->item.as<float>();
-        dim3 grid((unsigned) ((ix->n_item + kTile - 1) / kTile),
-                  (unsigned) std::min<int64_t>((n_cand + kTile - 1) / kTile, 65535));
-        timed(ix, st, "refine_tile", [&] { refine_tile_kernel<<<grid, kTileThreads, 0, st>>>(ra, items, ix->item_rnorm.as<float>(),
-                                                         ix->user_rnorm.as<float>(), ipbound ? ix->check_dim : ix->dim); });
-        RKR_CUDA(cudaGetLastError());
+        RefineEpi re;
+        re.a = ra;
+        re.item_rnorm = ix->item_rnorm.as<float>();
+        re.user_rnorm = ix->user_rnorm.as<float>();
+        const int k_split = ipbound ? ix->check_dim : ix->dim;
+        const int64_t per = (int64_t) 65535 * kBig;
+        for (int64_t r0 = 0; r0 < n_cand; r0 += per) {
+            re.row0 = r0;
+            cudaError_t ce = cudaSuccess;
+            timed(ix, st, "refine_tile", [&] {
+                ce = launch_big_split(ix->user.as<float>(), ref_user + r0, std::min(per, n_cand - r0), ix->dim, items,
+                                      ix->n_item, ix->dim, k_split, ix->dim, re, st);
+            });
+            RKR_CUDA(ce);
+        }
     }
     AssembleArgs aa;
     aa.counts = d_counts;

@@ -51,6 +51,33 @@ __global__ void gather_rows_kernel(const float *__restrict__ src, const int32_t 
     for (int j = threadIdx.x; j < dim; j += blockDim.x) dst[r * dim + j] = s[j];
 }
 
+__global__ void to_kmajor_kernel(const float *__restrict__ src, const int32_t *__restrict__ idx, int64_t n, int dim,
+                                 int64_t ld, float *__restrict__ dst) {
+    __shared__ float t[32][33];
+    const int64_t r0 = (int64_t) blockIdx.x * 32;
+    const int d0 = blockIdx.y * 32;
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int64_t r = r0 + i;
+        const int d = d0 + threadIdx.x;
+        t[i][threadIdx.x] = r < n && d < dim ? src[(idx ? (int64_t) idx[r] : r) * dim + d] : 0.0f;
+    }
+    __syncthreads();
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int d = d0 + i;
+        const int64_t r = r0 + threadIdx.x;
+        if (d < dim && r < ld) dst[(int64_t) d * ld + r] = t[threadIdx.x][i];
+    }
+}
+
+int to_kmajor(const float *src, const int32_t *idx, int64_t n, int dim, float *dst, cudaStream_t st) {
+    const int64_t ld = kmajor_ld(n);
+    if (ld == 0) return RKR_OK;
+    dim3 grid((unsigned) (ld / 32), (unsigned) ((dim + 31) / 32));
+    to_kmajor_kernel<<<grid, dim3(32, 8), 0, st>>>(src, idx, n, dim, ld, dst);
+    RKR_CUDA(cudaGetLastError());
+    return RKR_OK;
+}
+
 // Norms the refinement bound needs for the current check_dim (recomputed when it changes).
 int refine_prepare_norms(rkr_index *ix) {
     const int c = ix->check_dim;
@@ -158,7 +185,17 @@ int rkr_index_create(int32_t device, const float *user, int64_t n_user, const fl
     gather_rows_kernel<<<(unsigned) n_item, 64, 0, ix->stream>>>(ix->item.as<float>(), ix->ws_misc.as<int32_t>(), n_item,
                                                                 dim, ix->item_sorted.as<float>());
     e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ix->stream);
+    if (e != cudaSuccess) {
+        set_error("rkr_index_create: %s", cudaGetErrorString(e));
+        return fail(RKR_ERR_CUDA);
+    }
+    // k-major copies for the refinement tiles
+    const size_t km = sizeof(float) * (size_t) dim * (size_t) kmajor_ld(n_item);
+    if ((s = ix->item_km.ensure(km)) || (s = ix->item_sorted_km.ensure(km)) ||
+        (s = to_kmajor(ix->item.as<float>(), nullptr, n_item, dim, ix->item_km.as<float>(), ix->stream)) ||
+        (s = to_kmajor(ix->item_sorted.as<float>(), nullptr, n_item, dim, ix->item_sorted_km.as<float>(), ix->stream)))
+        return fail(s);
+    e = cudaStreamSynchronize(ix->stream);
     if (e != cudaSuccess) {
         set_error("rkr_index_create: %s", cudaGetErrorString(e));
         return fail(RKR_ERR_CUDA);
@@ -173,6 +210,7 @@ int rkr_index_destroy(rkr_index *ix) {
     if (ix->stream) cudaStreamSynchronize(ix->stream);
     for (DevBuf *b : {&ix->user, &ix->item, &ix->item_sorted, &ix->item_norm, &ix->item_rnorm, &ix->user_rnorm,
                       &ix->sample_rank, &ix->thr, &ix->thr_summ, &ix->reg_rank, &ix->reg, &ix->transfer_item, &ix->svd_user,
+                      &ix->svd_user_km, &ix->item_km, &ix->item_sorted_km, &ix->ws_km,
                       &ix->svd_unorm, &ix->qip_state, &ix->ws_query, &ix->ws_qtr, &ix->ws_qnorm, &ix->ws_bucket,
                       &ix->ws_bucket2, &ix->ws_levels, &ix->ws_cls, &ix->ws_counts, &ix->ws_hist, &ix->ws_res,
                       &ix->ws_cand, &ix->ws_cand_off, &ix->ws_refine, &ix->ws_rank, &ix->ws_out, &ix->ws_stats,
@@ -260,6 +298,8 @@ int rkr_index_load_svd(rkr_index *ix, int32_t check_dim, const float *transfer_i
     RKR_CUDA(cudaMemcpyAsync(ix->transfer_item.p, transfer_item, sizeof(float) * d * d, cudaMemcpyHostToDevice, ix->stream));
     RKR_CUDA(cudaMemcpyAsync(ix->svd_user.p, svd_user, sizeof(float) * (size_t) ix->n_user * d, cudaMemcpyHostToDevice,
                              ix->stream));
+    RKR_TRY(ix->svd_user_km.ensure(sizeof(float) * d * (size_t) kmajor_ld(ix->n_user)));
+    RKR_TRY(to_kmajor(ix->svd_user.as<float>(), nullptr, ix->n_user, (int) d, ix->svd_user_km.as<float>(), ix->stream));
     ix->has_svd = true;
     ix->check_dim = check_dim;
     return refine_prepare_norms(ix);
@@ -278,7 +318,7 @@ int rkr_index_size_bytes(const rkr_index *ix, uint64_t *bytes) {
     uint64_t s = 0;
     for (const DevBuf *b : {&ix->user, &ix->item, &ix->item_sorted, &ix->item_norm, &ix->item_rnorm, &ix->user_rnorm,
                             &ix->sample_rank, &ix->thr, &ix->thr_summ, &ix->reg_rank, &ix->reg, &ix->transfer_item, &ix->svd_user,
-                            &ix->svd_unorm, &ix->qip_state})
+                            &ix->svd_user_km, &ix->item_km, &ix->item_sorted_km, &ix->svd_unorm, &ix->qip_state})
         s += b->bytes;
     *bytes = s;
     return RKR_OK;

@@ -338,20 +338,91 @@ __global__ void __launch_bounds__(kBigThreads, 2) exact_big_kernel(const float *
 template <class Epi>
 inline size_t big_kernel_smem() { return kBigSmem + Epi::kExtra; }
 
+// ---- k-major operands -----------------------------------------------------------------------------
+//
+// A k-major matrix keeps coordinate k of row r at p[k * ld + r], with ld a multiple of 32 and the
+// columns [n, ld) zero.  A 16 x 128 stage of the tile pipeline is then 16 contiguous runs of 512
+// bytes: two 16-byte cp.async per thread and operand, no transposition and no per-element address
+// arithmetic, and a stage can end at any k (the k loop is bounded by the stage's real extent).
+
+struct KMajor {
+    const float *p;
+    int64_t n;     // rows
+    int64_t ld;    // row pitch of a k step, a multiple of 32
+    int64_t cols;  // columns readable from p on each k step (ld for a whole matrix; less for a slice)
+};
+
+__host__ __device__ inline int64_t kmajor_ld(int64_t n) { return (n + 31) & ~int64_t(31); }
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, bool valid) {
+    const unsigned s = (unsigned) __cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 16 : 0));
+}
+
+__device__ __forceinline__ void big_load_stage_km(BigOperands &op, int buf, const KMajor &A, int64_t a0,
+                                                  const KMajor &B, int64_t b0, int k0, int k_end) {
+#pragma unroll
+    for (int t = 0; t < (kBig * kBigK / 4) / kBigThreads; t++) {
+        const int c = threadIdx.x + t * kBigThreads;
+        const int kk = c >> 5, col = (c & 31) * 4;
+        const int k = k0 + kk;
+        const bool va = k < k_end && a0 + col < A.cols, vb = k < k_end && b0 + col < B.cols;
+        cp_async16(&op.a[buf][kk][col], va ? A.p + (int64_t) k * A.ld + a0 + col : A.p, va);
+        cp_async16(&op.b[buf][kk][col], vb ? B.p + (int64_t) k * B.ld + b0 + col : B.p, vb);
+    }
+}
+
+// big_accumulate over k-major operands: the same products and sums in the same k order.
+__device__ __forceinline__ bool big_accumulate_km(BigOperands &op, float acc[8][8], const KMajor &A, int64_t a0,
+                                                 const KMajor &B, int64_t b0, int k_begin, int k_end) {
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] = 0.0f;
+    const int ns = (k_end - k_begin + kBigK - 1) / kBigK;
+    if (ns <= 0) return false;
+    big_load_stage_km(op, 0, A, a0, B, b0, k_begin, k_end);
+    cp_async_commit();
+    for (int s = 0; s < ns; s++) {
+        if (s + 1 < ns) {
+            big_load_stage_km(op, (s + 1) & 1, A, a0, B, b0, k_begin + (s + 1) * kBigK, k_end);
+            cp_async_commit();
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        const int buf = s & 1;
+        const int kc = min(kBigK, k_end - k_begin - s * kBigK);
+#pragma unroll kBigKUnroll
+        for (int kk = 0; kk < kc; kk++) {
+            const float4 a_lo = *reinterpret_cast<const float4 *>(&op.a[buf][kk][4 * tx]);
+            const float4 a_hi = *reinterpret_cast<const float4 *>(&op.a[buf][kk][64 + 4 * tx]);
+            const float4 b_lo = *reinterpret_cast<const float4 *>(&op.b[buf][kk][4 * ty]);
+            const float4 b_hi = *reinterpret_cast<const float4 *>(&op.b[buf][kk][64 + 4 * ty]);
+            const float av[8] = {a_lo.x, a_lo.y, a_lo.z, a_lo.w, a_hi.x, a_hi.y, a_hi.z, a_hi.w};
+            const float bv[8] = {b_lo.x, b_lo.y, b_lo.z, b_lo.w, b_hi.x, b_hi.y, b_hi.z, b_hi.w};
+#pragma unroll
+            for (int i = 0; i < 8; i++)
+#pragma unroll
+                for (int j = 0; j < 8; j++) acc[i][j] = __fadd_rn(acc[i][j], __fmul_rn(av[i], bv[j]));
+        }
+        __syncthreads();
+    }
+    return true;
+}
+
 // Split form: the block of partial sums over [0, k_split) goes to epi.finish_lo(extra, res, a0, b0),
 // then the sums over [k_split, k_end) -- each accumulated from 0, as the reference keeps a partial
 // score and its remainder apart -- are added to them with one rounding and
 // epi.finish_hi(extra, res, a0, b0, spare) sees the totals; spare is the operand buffers'
-// sizeof(BigOperands) bytes, free by then.  Operands and result have separate shared memory, so the
-// second range's loads do not wait for finish_lo.  Epi also provides kExtra and
+// sizeof(BigOperands) bytes, free by then.  Operands (k-major) and result have separate shared
+// memory, so the second range's loads do not wait for finish_lo.  Epi also provides kExtra and
 // prologue(extra, a0, b0), which returns whether the tile has work (the same answer in every
-// thread; false ends the CTA).  Rows of A may be gathered through a_idx.  Every thread calls each
-// hook (they may synchronise the block).
+// thread; false ends the CTA).  Every thread calls each hook (they may synchronise the block).
 template <class Epi>
-__global__ void __launch_bounds__(kBigThreads, 2) exact_big_split_kernel(const float *__restrict__ A,
-                                                                         const int32_t *__restrict__ a_idx, int64_t n_a,
-                                                                         int lda, const float *__restrict__ B,
-                                                                         int64_t n_b, int ldb, int k_split, int k_end,
+__global__ void __launch_bounds__(kBigThreads, 2) exact_big_split_kernel(KMajor A, KMajor B, int k_split, int k_end,
                                                                          Epi epi) {
     extern __shared__ __align__(16) char big_smem[];
     BigOperands &op = *reinterpret_cast<BigOperands *>(big_smem);
@@ -360,35 +431,35 @@ __global__ void __launch_bounds__(kBigThreads, 2) exact_big_split_kernel(const f
     const int64_t b0 = (int64_t) blockIdx.x * kBig;
     const int64_t a0 = (int64_t) blockIdx.y * kBig;
     if (!epi.prologue(extra, a0, b0)) return;
-    __shared__ int32_t rows_s[kBig];  // the tile's gathered A rows
-    if (a_idx) {
-        if (threadIdx.x < kBig) rows_s[threadIdx.x] = a0 + threadIdx.x < n_a ? a_idx[a0 + threadIdx.x] : 0;
-        __syncthreads();
-    }
-    const int32_t *a_rows = a_idx ? rows_s : nullptr;
     float acc[8][8];
-    big_accumulate(op, acc, A, a_rows, n_a, lda, a0, B, n_b, ldb, b0, 0, k_split);
+    big_accumulate_km(op, acc, A, a0, B, b0, 0, k_split);
     big_store(res, acc, false);
     __syncthreads();
     epi.finish_lo(extra, res, a0, b0);
-    // big_accumulate's first barrier orders finish_lo's reads of res before the adds below
-    if (!big_accumulate(op, acc, A, a_rows, n_a, lda, a0, B, n_b, ldb, b0, k_split, k_end)) __syncthreads();
+    // big_accumulate_km's first barrier orders finish_lo's reads of res before the adds below
+    if (!big_accumulate_km(op, acc, A, a0, B, b0, k_split, k_end)) __syncthreads();
     big_store(res, acc, true);
     __syncthreads();
     epi.finish_hi(extra, res, a0, b0, big_smem);
 }
 
 template <class Epi>
-inline cudaError_t launch_big_split(const float *A, const int32_t *a_idx, int64_t n_a, int lda, const float *B,
-                                    int64_t n_b, int ldb, int k_split, int k_end, const Epi &epi, cudaStream_t st) {
+inline cudaError_t launch_big_split(const KMajor &A, const KMajor &B, int k_split, int k_end, const Epi &epi,
+                                    cudaStream_t st) {
     const size_t smem = sizeof(BigOperands) + sizeof(BigResult) + Epi::kExtra;
     cudaError_t e =
         cudaFuncSetAttribute(exact_big_split_kernel<Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
     if (e != cudaSuccess) return e;
-    dim3 grid((unsigned) ((n_b + kBig - 1) / kBig), (unsigned) ((n_a + kBig - 1) / kBig));
-    exact_big_split_kernel<Epi><<<grid, kBigThreads, smem, st>>>(A, a_idx, n_a, lda, B, n_b, ldb, k_split, k_end, epi);
+    dim3 grid((unsigned) ((B.n + kBig - 1) / kBig), (unsigned) ((A.n + kBig - 1) / kBig));
+    exact_big_split_kernel<Epi><<<grid, kBigThreads, smem, st>>>(A, B, k_split, k_end, epi);
     return cudaGetLastError();
 }
+
+// Row-major [n][dim] rows (gathered through idx when given) to k-major [dim][ld], zeroing the
+// columns [n, ld).  Grid (ld / 32, ceil(dim / 32)), block (32, 8).
+__global__ void to_kmajor_kernel(const float *__restrict__ src, const int32_t *__restrict__ idx, int64_t n, int dim,
+                                 int64_t ld, float *__restrict__ dst);
+int to_kmajor(const float *src, const int32_t *idx, int64_t n, int dim, float *dst, cudaStream_t st);
 
 // Launches exact_big_kernel<Epi> over n_a x n_b pairs on stream st.
 template <class Epi>
@@ -766,6 +837,8 @@ struct rkr_index {
     rkr::DevBuf user;          // [n_user][dim], normalised
     rkr::DevBuf item;          // [n_item][dim], original order
     rkr::DevBuf item_sorted;   // [n_item][dim], by norm, descending
+    rkr::DevBuf item_km;       // k-major copies: [dim][kmajor_ld(n_item)] of item ...
+    rkr::DevBuf item_sorted_km;  // ... and of item_sorted
     rkr::DevBuf item_norm;     // [n_item], descending
     rkr::DevBuf item_rnorm;    // [n_item], norm of dims [check_dim, dim) of item_sorted
     rkr::DevBuf user_rnorm;    // [n_user], norm of dims [check_dim, dim) of user
@@ -785,11 +858,12 @@ struct rkr_index {
     bool has_svd = false;
     rkr::DevBuf transfer_item; // [dim][dim]
     rkr::DevBuf svd_user;      // [n_user][dim]
+    rkr::DevBuf svd_user_km;   // k-major copy: [dim][kmajor_ld(n_user)]
     rkr::DevBuf svd_unorm;     // [n_user], norm of dims [check_dim, dim) of svd_user
     rkr::DevBuf qip_state;     // [n_user], QSRPNormalLP's carried query scores
     // per-call workspace
     rkr::DevBuf ws_query, ws_qtr, ws_qnorm, ws_bucket, ws_bucket2, ws_levels, ws_cls, ws_counts, ws_hist;
-    rkr::DevBuf ws_res, ws_cand, ws_cand_off, ws_refine, ws_rank, ws_out, ws_stats, ws_misc, ws_fix;
+    rkr::DevBuf ws_res, ws_cand, ws_cand_off, ws_refine, ws_rank, ws_out, ws_stats, ws_misc, ws_fix, ws_km;
     std::vector<uint8_t> h_scratch;
     rkr::Profiler prof;
 };

@@ -953,6 +953,8 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
         transfer_query_kernel<<<nq, 128, 0, st>>>(d_query, ix->transfer_item.as<float>(), dim, c, qtr, qnorm);
     });
     RKR_CUDA(cudaGetLastError());
+    RKR_TRY(ix->ws_km.ensure(sizeof(float) * (size_t) dim * (size_t) kmajor_ld(nq)));
+    RKR_TRY(to_kmajor(qtr, nullptr, nq, dim, ix->ws_km.as<float>(), st));
     ScoreSrc sc;
     sc.svd_user = ix->svd_user.as<float>();
     sc.qtr = qtr;
@@ -980,7 +982,9 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     e1.n_query = nq;
     e1.fix = fix;
     cudaError_t ce = cudaSuccess;
-    timed(ix, st, "qsrp_scores", [&] { ce = launch_big_split(ix->svd_user.as<float>(), nullptr, U, dim, qtr, nq, dim, c, dim, e1, st); });
+    const KMajor ka = {ix->svd_user_km.as<float>(), U, kmajor_ld(U), kmajor_ld(U)};
+    const KMajor kb = {ix->ws_km.as<float>(), nq, kmajor_ld(nq), kmajor_ld(nq)};
+    timed(ix, st, "qsrp_scores", [&] { ce = launch_big_split(ka, kb, c, dim, e1, st); });
     RKR_CUDA(ce);
     timed(ix, st, "qsrp_fix1", [&] { qsrp_fix1_kernel<<<148 * 4, 256, 0, st>>>(fix, m, e1.unorm, qnorm, U, lv); });
     RKR_CUDA(cudaGetLastError());

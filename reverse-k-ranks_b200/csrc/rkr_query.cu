@@ -551,7 +551,7 @@ static int refine_and_assemble(rkr_index *ix, int method, const float *d_query, 
                                int32_t *d_cand_ub, const float *d_cand_qip_given, const int64_t *d_cand_off,
                                rkr_user_rank *d_out, rkr_query_stats *d_stats, cudaStream_t st) {
     const bool ipbound = method != RKR_METHOD_US;
-    size_t need = carve_size(n_cand, 4) * 7 + carve_size(1, 4);
+    size_t need = carve_size(n_cand, 4) * 7 + carve_size(1, 4) + carve_size((size_t) ix->dim * kmajor_ld(n_cand), 4);
     RKR_TRY(ix->ws_refine.ensure(need));
     uint8_t *p = ix->ws_refine.as<uint8_t>();
     float *qip = carve<float>(p, n_cand);
@@ -561,6 +561,7 @@ static int refine_and_assemble(rkr_index *ix, int method, const float *d_query, 
     int32_t *ref_user = carve<int32_t>(p, n_cand);
     int32_t *undecided = carve<int32_t>(p, n_cand);
     int32_t *n_ref = carve<int32_t>(p, 1);
+    float *cand_km = carve<float>(p, (size_t) ix->dim * kmajor_ld(n_cand));
     RKR_CUDA(cudaMemsetAsync(n_ref, 0, sizeof(int32_t), st));
     RKR_CUDA(cudaMemsetAsync(ref_user, 0, sizeof(int32_t) * n_cand, st));
     if (n_cand > 0) {
@@ -586,20 +587,23 @@ static int refine_and_assemble(rkr_index *ix, int method, const float *d_query, 
         ra.undecided = undecided;
         timed(ix, st, "refine_prep", [&] { refine_prep_kernel<<<(unsigned) ((n_cand + 255) / 256), 256, 0, st>>>(ra); });
         RKR_CUDA(cudaGetLastError());
-        const float *items = ipbound ? ix->item_sorted.as<float>() : ix->item.as<float>();
+        // the refined candidates' user vectors, gathered k-major (rows past n_ref gather user 0)
+        timed(ix, st, "refine_gather", [&] { to_kmajor(ix->user.as<float>(), ref_user, n_cand, ix->dim, cand_km, st); });
+        RKR_CUDA(cudaGetLastError());
+        const KMajor items = {ipbound ? ix->item_sorted_km.as<float>() : ix->item_km.as<float>(), ix->n_item,
+                              kmajor_ld(ix->n_item), kmajor_ld(ix->n_item)};
         RefineEpi re;
         re.a = ra;
         re.item_rnorm = ix->item_rnorm.as<float>();
         re.user_rnorm = ix->user_rnorm.as<float>();
         const int k_split = ipbound ? ix->check_dim : ix->dim;
         const int64_t per = (int64_t) 65535 * kBig;
+        const int64_t ldc = kmajor_ld(n_cand);
         for (int64_t r0 = 0; r0 < n_cand; r0 += per) {
             re.row0 = r0;
+            const KMajor cands = {cand_km + r0, std::min(per, n_cand - r0), ldc, ldc - r0};
             cudaError_t ce = cudaSuccess;
-            timed(ix, st, "refine_tile", [&] {
-                ce = launch_big_split(ix->user.as<float>(), ref_user + r0, std::min(per, n_cand - r0), ix->dim, items,
-                                      ix->n_item, ix->dim, k_split, ix->dim, re, st);
-            });
+            timed(ix, st, "refine_tile", [&] { ce = launch_big_split(cands, items, k_split, ix->dim, re, st); });
             RKR_CUDA(ce);
         }
     }

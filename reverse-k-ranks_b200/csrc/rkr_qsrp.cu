@@ -430,48 +430,73 @@ __global__ void __launch_bounds__(kHistThreads) level_hist_kernel(const uint32_t
     if (threadIdx.x == 0 && anom) atomicAdd(anomaly + q, anom);
 }
 
+// ---- one warp per query -------------------------------------------------------------------------
+
+__device__ __forceinline__ int64_t warp_sum64(int64_t v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// First index b in [0, n) at which the running sum of h reaches need (n - 1 if it never does).
+__device__ __forceinline__ int warp_first_reaching(const int *__restrict__ h, int n, int64_t need) {
+    const int lane = threadIdx.x & 31;
+    int64_t base = 0;
+    for (int c0 = 0; c0 < n; c0 += 32) {
+        const int b = c0 + lane;
+        const int v = b < n ? h[b] : 0;
+        const int incl = warp_incl_scan(v);
+        const unsigned hit = __ballot_sync(0xffffffffu, b < n && base + incl >= need);
+        if (hit) return c0 + __ffs(hit) - 1;
+        base += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    return n - 1;
+}
+
 // Round-1 k-th smallest bounds per query (PruneCandidateByBound.hpp:36-77 with nothing excluded)
-// and the class counts.  While every pair has ub <= lb, a result (lb <= U*) and a prune
-// (ub >= L*) cannot coincide unless L* == U*, so the counts follow from the two histograms;
-// otherwise qsrp_count1 counts pair by pair.
+// and the class counts, one warp per query.  While every pair has ub <= lb, a result (lb <= U*)
+// and a prune (ub >= L*) cannot coincide unless L* == U*, so the counts follow from the two
+// histograms; otherwise qsrp_count1 counts pair by pair.  rank(level) is non-decreasing, so the
+// levels with rank <= X form a prefix and the thresholds are counts.
 __global__ void qsrp_select1_kernel(const int *__restrict__ hist_all, const int *__restrict__ anomaly, int64_t n_user,
                                     const int32_t *__restrict__ rank, int S, int n_item, int topk, int nq,
                                     QsrpParams *__restrict__ par) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (q >= nq) return;
     const int nl = S + 2;
     const int *h = hist_all + (int64_t) q * 2 * nl;
-    int kl = nl - 1, kh = nl - 1;
-    int64_t c = 0;
-    for (int b = 0; b < nl; b++) { c += h[b]; if (c >= topk) { kl = b; break; } }
-    c = 0;
-    for (int b = 0; b < nl; b++) { c += h[nl + b]; if (c >= topk) { kh = b; break; } }
+    const int kl = warp_first_reaching(h, nl, topk), kh = warp_first_reaching(h + nl, nl, topk);
     QsrpParams p = {};
     p.L1 = level_rank(kl, rank, S, n_item);
     p.U1 = level_rank(kh, rank, S, n_item);
     p.mode1 = p.L1 == p.U1;
-    p.lv_res = -1; p.lv_pr = nl; p.lv_m1 = -1;
-    for (int l = 0; l < nl; l++) {
+    int64_t c_res = 0, c_m1 = 0, c_lt = 0;
+    for (int l = lane; l < nl; l += 32) {
         const int rl = level_rank(l, rank, S, n_item);
-        if (rl <= p.U1) p.lv_res = l;
-        if (rl <= p.L1) p.lv_m1 = l;
-        if (rl >= p.L1 && p.lv_pr == nl) p.lv_pr = l;
+        c_res += rl <= p.U1;
+        c_m1 += rl <= p.L1;
+        c_lt += rl < p.L1;
     }
+    p.lv_res = (int) warp_sum64(c_res) - 1;
+    p.lv_m1 = (int) warp_sum64(c_m1) - 1;
+    p.lv_pr = (int) warp_sum64(c_lt);
     if (!p.mode1) {
         if (anomaly[q]) {
             p.exact1 = 1;
         } else {
             int64_t nres = 0, npr = 0;
-            for (int b = 0; b < nl; b++) {
+            for (int b = lane; b < nl; b += 32) {
                 if (b <= p.lv_res) nres += h[b];
                 if (b >= p.lv_pr) npr += h[nl + b];
             }
+            nres = warp_sum64(nres);
+            npr = warp_sum64(npr);
             p.n_res1 = (int) nres;
             p.n_pr1 = (int) npr;
             p.n_ref1 = (int) (n_user - nres - npr);
         }
     }
-    par[q] = p;
+    if (lane == 0) par[q] = p;
 }
 
 // Round-1 class counts pair by pair (the reduction at PruneCandidateByBound.hpp:115-136), for
@@ -562,25 +587,23 @@ __global__ void __launch_bounds__(kHistThreads) qsrp_round2_kernel(const uint32_
     const uint32_t *lrow = lv + (int64_t) q * n_user;
     uint8_t *crow = code + (int64_t) q * n_user;
     const int64_t u0 = (int64_t) blockIdx.x * chunk, u1 = min(u0 + chunk, n_user);
-    constexpr int G = 4;  // loads in flight per thread
+    constexpr int G = 4;  // pairs in flight per thread; the group code is loaded with the levels
     for (int64_t ub = u0 + threadIdx.x; ub < u1; ub += G * kHistThreads) {
         uint32_t v[G];
-        bool el[G];
-#pragma unroll
-        for (int g = 0; g < G; g++) v[g] = ub + g * kHistThreads < u1 ? __ldg(lrow + ub + g * kHistThreads) : 0u;
+        unsigned cc[G];
 #pragma unroll
         for (int g = 0; g < G; g++) {
-            const int64_t u = ub + g * kHistThreads;
-            if (u >= u1) break;
-            const int k = class1_lv(p, v[g] & 0xffff, v[g] >> 16);
-            el[g] = k == kClsRefine || k == kClsIdle;
-            if (!el[g]) crow[u] = k == kClsResult ? kCodeResult1 : kCodePruned1;
+            const bool in = ub + g * kHistThreads < u1;
+            v[g] = in ? __ldg(lrow + ub + g * kHistThreads) : 0u;
+            cc[g] = in ? crow[ub + g * kHistThreads] : 0u;
         }
 #pragma unroll
         for (int g = 0; g < G; g++) {
             const int64_t u = ub + g * kHistThreads;
             if (u >= u1) break;
-            if (el[g]) atomicAdd(mine + crow[u], 1);
+            const int k = class1_lv(p, v[g] & 0xffff, v[g] >> 16);
+            if (k == kClsRefine || k == kClsIdle) atomicAdd(mine + cc[g], 1);
+            else crow[u] = k == kClsResult ? kCodeResult1 : kCodePruned1;
         }
     }
     __syncthreads();
@@ -630,28 +653,108 @@ __global__ void qsrp_select2c_kernel(const int *__restrict__ hist_c, int nb, int
     par[q] = p;
 }
 
-// Exact bucket histogram of the pairs whose coarse group is flagged for their query (mask1 or
-// mask2); grid (users / (256 x 16), queries), each thread 16 consecutive users.
+// Pairs whose exact bucket a fine pass needs: (query << 40 | user << 8 | group), resolved by
+// qsrp_fine2_list_kernel; past the capacity the scan resolves them itself.
+struct HitList {
+    uint64_t *e;
+    int *count;
+    int cap;
+};
+
+__device__ __forceinline__ void fine2_hit(const HitList &hl, bool hit, int64_t q, int64_t u, unsigned c, QipView sc,
+                                          const float *__restrict__ thr, int S, int gs, int *__restrict__ hist_f) {
+    const unsigned want = __ballot_sync(0xffffffffu, hit);  // called by whole warps
+    if (!want) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(want) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(hl.count, __popc(want));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (!hit) return;
+    const int idx = base + __popc(want & ((1u << lane) - 1));
+    if (idx < hl.cap) hl.e[idx] = ((uint64_t) q << 40) | ((uint64_t) u << 8) | c;
+    else atomicAdd(hist_f + q * (S + 1) + fine_bucket(thr + u * S, S, gs, (int) c, sc(u, q)), 1);
+}
+
+// Scan for the pairs whose coarse group is flagged for their query (mask1, or mask2 when any
+// query has one): a grid-stride pass over the batch's codes as one flat [query][user] array, 16
+// codes per thread and step.
 __global__ void __launch_bounds__(256) qsrp_fine2_kernel(const uint8_t *__restrict__ code, QipView sc, int64_t n_user,
-                                                        const float *__restrict__ thr, int S, int gs,
-                                                        const QsrpParams *__restrict__ par, int second,
+                                                        int nq, double inv_user, const float *__restrict__ thr, int S,
+                                                        int gs, const QsrpParams *__restrict__ par, int second,
+                                                        const int *__restrict__ any2, HitList hl,
                                                         int *__restrict__ hist_f) {
-    const int q = blockIdx.y;
-    const uint32_t mask = (uint32_t) (second ? par[q].mask2 : par[q].mask1);
-    if (!mask) return;
-    const int64_t u0 = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) * 16;
-    if (u0 >= n_user) return;
-    const int n = (int) (n_user - u0 < 16 ? n_user - u0 : 16);
-    uint32_t w[4];
-    load16_bytes(code + (int64_t) q * n_user + u0, w);
-    int *hq = hist_f + (int64_t) q * (S + 1);
+    if (second && !*any2) return;
+    const int64_t total = n_user * nq;
+    // whole warps step together over 512-code segments (the hit appends are warp-wide)
+    const int64_t warp = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t stride = (int64_t) gridDim.x * blockDim.x * 16;
+    for (int64_t seg = warp * 512; seg < total; seg += stride) {
+        const int64_t base = seg + (threadIdx.x & 31) * 16;
+        uint32_t w[4];
+        if (base >= total) {
+            w[0] = w[1] = w[2] = w[3] = 0xffffffffu;
+        } else if (base + 16 <= total) {
+            const uint4 x = *reinterpret_cast<const uint4 *>(code + base);
+            w[0] = x.x; w[1] = x.y; w[2] = x.z; w[3] = x.w;
+        } else {
 #pragma unroll
-    for (int e = 0; e < 16; e++) {
-        const unsigned c = (w[e >> 2] >> (8 * (e & 3))) & 0xff;
-        if (e < n && c < 32 && (mask >> c & 1u)) {
-            const int64_t u = u0 + e;
-            atomicAdd(hq + fine_bucket(thr + u * S, S, gs, (int) c, sc(u, q)), 1);
+            for (int i = 0; i < 4; i++) {
+                w[i] = 0xffffffffu;
+                for (int j = 0; j < 4; j++)
+                    if (base + 4 * i + j < total) w[i] = (w[i] & ~(0xffu << (8 * j))) | ((uint32_t) code[base + 4 * i + j] << (8 * j));
+            }
         }
+        if (n_user < 16) {  // a step may span several queries
+            for (int e = 0; e < 16; e++) {
+                const unsigned c = (w[e >> 2] >> (8 * (e & 3))) & 0xff;
+                const int64_t pos = base + e;
+                if (pos >= total || c >= 32) continue;
+                const int64_t q = pos / n_user, u = pos % n_user;
+                if ((uint32_t) (second ? par[q].mask2 : par[q].mask1) >> c & 1u)
+                    atomicAdd(hist_f + q * (S + 1) + fine_bucket(thr + u * S, S, gs, (int) c, sc(u, q)), 1);
+            }
+            continue;
+        }
+        // with at least 16 users a step of 16 codes meets at most one query boundary
+        int64_t q0 = 0, edge = 0;
+        uint32_t m0 = 0, m1 = 0;
+        if (base < total) {
+            q0 = (int64_t) ((double) base * inv_user);
+            if (q0 * n_user > base) q0--;
+            else if ((q0 + 1) * n_user <= base) q0++;
+            edge = (q0 + 1) * n_user;
+            m0 = (uint32_t) (second ? par[q0].mask2 : par[q0].mask1);
+            m1 = edge < base + 16 && q0 + 1 < nq ? (uint32_t) (second ? par[q0 + 1].mask2 : par[q0 + 1].mask1) : 0u;
+        }
+        uint32_t hits = 0;
+        if (m0 | m1) {
+#pragma unroll
+            for (int e = 0; e < 16; e++) {
+                const unsigned c = (w[e >> 2] >> (8 * (e & 3))) & 0xff;
+                const uint32_t m = base + e >= edge ? m1 : m0;
+                hits |= (uint32_t) (base + e < total && c < 32 && (m >> c & 1u)) << e;
+            }
+        }
+        // one hit per lane and round, so that the list append stays warp-aggregated
+        while (__any_sync(0xffffffffu, hits != 0)) {
+            const int e = hits ? __ffs(hits) - 1 : 0;
+            const int64_t pos = base + e;
+            const int64_t q = pos >= edge ? q0 + 1 : q0;
+            fine2_hit(hl, hits != 0, q, pos - q * n_user, (w[e >> 2] >> (8 * (e & 3))) & 0xff, sc, thr, S, gs, hist_f);
+            hits &= hits - 1;
+        }
+    }
+}
+
+// Exact buckets of the listed pairs.
+__global__ void qsrp_fine2_list_kernel(HitList hl, QipView sc, int64_t n_user, const float *__restrict__ thr, int S,
+                                       int gs, int *__restrict__ hist_f) {
+    const int n = min(*hl.count, hl.cap);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint64_t x = hl.e[i];
+        const int64_t q = (int64_t) (x >> 40), u = (int64_t) ((x >> 8) & 0xffffffffu);
+        const int c = (int) (x & 0xff);
+        atomicAdd(hist_f + q * (S + 1) + fine_bucket(thr + u * S, S, gs, c, sc(u, q)), 1);
     }
 }
 
@@ -665,14 +768,14 @@ __device__ __forceinline__ uint8_t class2_of(int b, int S, const int32_t *rank, 
     return kClsRefine;
 }
 
-// Round-2 selection, exact step: the k-th bucket from the critical group's exact histogram, the
-// bounds (L2, U2), each bucket's and each group's class, and the mixed groups still without an
-// exact histogram (mask2).
+// Round-2 selection, exact step, one warp per query: the k-th bucket from the critical group's
+// exact histogram, the bounds (L2, U2), each bucket's and each group's class, and the mixed groups
+// still without an exact histogram (mask2).
 __global__ void qsrp_select2f_kernel(const int *__restrict__ hist_f, int nb, int gs, int S,
                                      const int32_t *__restrict__ rank, int n_item, int topk, int nq,
                                      QsrpParams *__restrict__ par, uint8_t *__restrict__ cls2,
-                                     uint8_t *__restrict__ clsg) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+                                     uint8_t *__restrict__ clsg, int *__restrict__ any2) {
+    const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (q >= nq) return;
     QsrpParams p = par[q];
     if (p.skip2) return;
@@ -702,26 +805,31 @@ __global__ void qsrp_select2f_kernel(const int *__restrict__ hist_f, int nb, int
     p.L2 = L; p.U2 = U; p.mode2 = L == U;
     uint8_t *cq = cls2 + (int64_t) q * (S + 1);
     uint8_t *cg = clsg + (int64_t) q * (nb + 1);
-    for (int b = 0; b <= S; b++) cq[b] = class2_of(b, S, rank, n_item, L, U, p.mode2);
+    for (int b = lane; b <= S; b += 32) cq[b] = class2_of(b, S, rank, n_item, L, U, p.mode2);
     uint32_t mask2 = 0;
-    for (int g = 0; g < nb; g++) {
+    for (int g = lane; g < nb; g += 32) {
         const int b0 = g * gs, b1 = min(b0 + gs, S);
-        uint8_t k = cq[b0];
-        for (int b = b0 + 1; b < b1; b++) if (cq[b] != k) { k = kClsMixed; break; }
+        uint8_t k = class2_of(b0, S, rank, n_item, L, U, p.mode2);
+        for (int b = b0 + 1; b < b1; b++) if (class2_of(b, S, rank, n_item, L, U, p.mode2) != k) { k = kClsMixed; break; }
         cg[g] = k;
         if (k == kClsMixed && !p.mode2 && !(p.mask1 >> g & 1)) mask2 |= 1u << g;
     }
-    cg[nb] = cq[S];
-    p.mask2 = (int32_t) mask2;
-    par[q] = p;
+    mask2 = __reduce_or_sync(0xffffffffu, mask2);
+    if (lane == 0) {
+        cg[nb] = class2_of(S, S, rank, n_item, L, U, p.mode2);
+        p.mask2 = (int32_t) mask2;
+        par[q] = p;
+        if (mask2) *any2 = 1;
+    }
 }
 
-// Round-2 class counts (PruneCandidateByBound.hpp:83-150): pure groups count whole from the
-// coarse histogram, mixed groups bucket by bucket; then the "all survivors are results" rule.
+// Round-2 class counts (PruneCandidateByBound.hpp:83-150), one warp per query: pure groups count
+// whole from the coarse histogram, mixed groups bucket by bucket; then the "all survivors are
+// results" rule and the groups the compaction must classify.
 __global__ void qsrp_final2_kernel(const int *__restrict__ hist_c, const int *__restrict__ hist_f, int nb, int gs, int S,
                                    int topk, int nq, QsrpParams *__restrict__ par, uint8_t *__restrict__ cls2,
                                    uint8_t *__restrict__ clsg, QueryCounts *__restrict__ counts) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (q >= nq) return;
     QsrpParams p = par[q];
     if (p.skip2) return;
@@ -729,6 +837,9 @@ __global__ void qsrp_final2_kernel(const int *__restrict__ hist_c, const int *__
     c.lstar = p.L2;
     c.ustar = p.U2;
     c.ip_base = p.n_ref1;  // QSRPNormalLP.hpp:177: refine_user_size after the first prune
+    uint8_t *cq = cls2 + (int64_t) q * (S + 1);
+    uint8_t *cg = clsg + (int64_t) q * (nb + 1);
+    bool all2 = false;
     if (p.mode2) {
         c.mode = 1;
         c.n_result = topk;
@@ -737,20 +848,20 @@ __global__ void qsrp_final2_kernel(const int *__restrict__ hist_c, const int *__
     } else {
         const int *hc = hist_c + (int64_t) q * (nb + 1);
         const int *hf = hist_f + (int64_t) q * (S + 1);
-        uint8_t *cq = cls2 + (int64_t) q * (S + 1);
-        uint8_t *cg = clsg + (int64_t) q * (nb + 1);
         int64_t n[4] = {0, 0, 0, 0};
-        for (int g = 0; g <= nb; g++) {
-            if (cg[g] != kClsMixed) {
-                n[cg[g]] += hc[g];
+        for (int g = lane; g <= nb; g += 32) {
+            const uint8_t k = cg[g];
+            if (k != kClsMixed) {
+                n[k] += hc[g];
             } else {
                 for (int b = g * gs; b < min(g * gs + gs, S); b++) n[cq[b]] += hf[b];
             }
         }
-        int64_t nres = p.n_res1 + n[kClsResult], npr = p.n_pr1 + n[kClsPrune], nref = n[kClsRefine];
+        int64_t nres = p.n_res1 + warp_sum64(n[kClsResult]), npr = p.n_pr1 + warp_sum64(n[kClsPrune]);
+        int64_t nref = warp_sum64(n[kClsRefine]);
         if (nres + nref == topk) {
-            for (int b = 0; b <= S; b++) if (cq[b] == kClsRefine) cq[b] = kClsResult;
-            for (int g = 0; g <= nb; g++) if (cg[g] == kClsRefine) cg[g] = kClsResult;
+            all2 = true;
+            for (int b = lane; b <= S; b += 32) if (cq[b] == kClsRefine) cq[b] = kClsResult;
             nres = topk;
             nref = 0;
         }
@@ -759,16 +870,21 @@ __global__ void qsrp_final2_kernel(const int *__restrict__ hist_c, const int *__
         c.n_prune = (int) npr;
         c.n_cand = nres >= topk ? 0 : (int) nref;
     }
-    const uint8_t *cg = clsg + (int64_t) q * (nb + 1);
-    uint64_t need = 0;
-    for (int g = 0; g <= nb; g++) {
-        const uint8_t k = cg[g];
-        if (k == kClsResult || k == kClsMixed || (k == kClsRefine && c.n_cand > 0)) need |= uint64_t(1) << g;
+    uint32_t need_lo = 0, need_hi = 0;
+    for (int g = lane; g <= nb; g += 32) {
+        uint8_t k = cg[g];
+        if (all2 && k == kClsRefine) cg[g] = k = kClsResult;
+        const bool need = k == kClsResult || k == kClsMixed || (k == kClsRefine && c.n_cand > 0);
+        if (need) { if (g < 32) need_lo |= 1u << g; else need_hi |= 1u << (g - 32); }
     }
-    p.gneed_lo = (int32_t) (uint32_t) need;
-    p.gneed_hi = (int32_t) (uint32_t) (need >> 32);
-    par[q] = p;
-    counts[q] = c;
+    need_lo = __reduce_or_sync(0xffffffffu, need_lo);
+    need_hi = __reduce_or_sync(0xffffffffu, need_hi);
+    if (lane == 0) {
+        p.gneed_lo = (int32_t) need_lo;
+        p.gneed_hi = (int32_t) need_hi;
+        par[q] = p;
+        counts[q] = c;
+    }
 }
 
 // Classification of a pair after both rounds for the ordered compaction: result users carry their
@@ -914,13 +1030,15 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     const int nl = Sr + 2;
     const int gs = thr_group(S), nb = (S + gs - 1) / gs;
     RKR_TRY(ix->ws_qtr.ensure(carve_size((size_t) nq * dim, 4) + carve_size(nq, 4) + carve_size(nq, sizeof(QsrpParams)) +
-                              carve_size(nq, 4) + carve_size(1, 4)));
+                              carve_size(nq, 4) + carve_size(1, 4) * 2 + carve_size(2, 4)));
     uint8_t *p0 = ix->ws_qtr.as<uint8_t>();
     float *qtr = carve<float>(p0, (size_t) nq * dim);
     float *qnorm = carve<float>(p0, nq);
     QsrpParams *par = carve<QsrpParams>(p0, nq);
     int *anomaly = carve<int>(p0, nq);
     int *fix_count = carve<int>(p0, 1);
+    int *any2 = carve<int>(p0, 1);
+    int *hit_count = carve<int>(p0, 2);
     RKR_TRY(ix->ws_levels.ensure((size_t) nq * U * 8));
     RKR_TRY(ix->ws_bucket2.ensure((size_t) nq * U));
     RKR_TRY(ix->ws_cls.ensure(carve_size((size_t) nq * (S + 1), 1) + carve_size((size_t) nq * (nb + 1), 1)));
@@ -928,7 +1046,8 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     const size_t n_hist_l = (size_t) nq * 2 * nl, n_hist_c = (size_t) nq * (nb + 1), n_hist_f = (size_t) nq * (S + 1);
     RKR_TRY(ix->ws_hist.ensure(carve_size(n_hist_l, 4) + carve_size(n_hist_c, 4) + carve_size(n_hist_f, 4)));
     const int fix_cap = (int) std::min<int64_t>(int64_t(1) << 26, std::max<int64_t>(int64_t(1) << 20, U * nq / 64));
-    RKR_TRY(ix->ws_fix.ensure(carve_size(fix_cap, sizeof(int4))));
+    const int hit_cap = 1 << 22;
+    RKR_TRY(ix->ws_fix.ensure(carve_size(fix_cap, sizeof(int4)) + carve_size(hit_cap, 8)));
     uint32_t *lv = ix->ws_levels.as<uint32_t>();
     float *qip = reinterpret_cast<float *>(lv + (size_t) nq * U);
     uint8_t *code = ix->ws_bucket2.as<uint8_t>();
@@ -945,8 +1064,13 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     fix.e = carve<int4>(pm, fix_cap);
     fix.count = fix_count;
     fix.cap = fix_cap;
+    HitList hl;
+    hl.e = carve<uint64_t>(pm, hit_cap);
+    hl.cap = hit_cap;
     RKR_CUDA(cudaMemsetAsync(anomaly, 0, sizeof(int) * nq, st));
     RKR_CUDA(cudaMemsetAsync(fix_count, 0, sizeof(int), st));
+    RKR_CUDA(cudaMemsetAsync(any2, 0, sizeof(int), st));
+    RKR_CUDA(cudaMemsetAsync(hit_count, 0, 2 * sizeof(int), st));
     RKR_CUDA(cudaMemsetAsync(ix->ws_hist.p, 0, (size_t) (ph - ix->ws_hist.as<uint8_t>()), st));
 
     timed(ix, st, "transfer_query", [&] {
@@ -1000,7 +1124,7 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     });
     RKR_CUDA(cudaGetLastError());
     timed(ix, st, "qsrp_select1", [&] {
-        qsrp_select1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(hist_l, anomaly, U, m.rank, Sr, n_item, topk, nq, par);
+        qsrp_select1_kernel<<<(nq + 3) / 4, 128, 0, st>>>(hist_l, anomaly, U, m.rank, Sr, n_item, topk, nq, par);
     });
     RKR_CUDA(cudaGetLastError());
     {
@@ -1021,21 +1145,28 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     RKR_CUDA(cudaGetLastError());
     const float *thr = ix->thr.as<float>();
     const int32_t *srank = ix->sample_rank.as<int32_t>();
-    const dim3 fg((unsigned) ((U + 256 * 16 - 1) / (256 * 16)), (unsigned) nq);
+    const unsigned fg = 148 * 8;
+    const double inv_user = 1.0 / (double) U;
+    hl.count = hit_count;
     timed(ix, st, "qsrp_fine2", [&] {
-        qsrp_fine2_kernel<<<fg, 256, 0, st>>>(code, qv, U, thr, S, gs, par, 0, hist_f);
+        qsrp_fine2_kernel<<<fg, 256, 0, st>>>(code, qv, U, nq, inv_user, thr, S, gs, par, 0, any2, hl, hist_f);
     });
+    RKR_CUDA(cudaGetLastError());
+    timed(ix, st, "qsrp_fine2_list", [&] { qsrp_fine2_list_kernel<<<148 * 8, 256, 0, st>>>(hl, qv, U, thr, S, gs, hist_f); });
     RKR_CUDA(cudaGetLastError());
     timed(ix, st, "qsrp_select2f", [&] {
-        qsrp_select2f_kernel<<<(nq + 127) / 128, 128, 0, st>>>(hist_f, nb, gs, S, srank, n_item, topk, nq, par, cls2, clsg);
+        qsrp_select2f_kernel<<<(nq + 3) / 4, 128, 0, st>>>(hist_f, nb, gs, S, srank, n_item, topk, nq, par, cls2, clsg, any2);
     });
     RKR_CUDA(cudaGetLastError());
+    hl.count = hit_count + 1;
     timed(ix, st, "qsrp_fine2", [&] {
-        qsrp_fine2_kernel<<<fg, 256, 0, st>>>(code, qv, U, thr, S, gs, par, 1, hist_f);
+        qsrp_fine2_kernel<<<fg, 256, 0, st>>>(code, qv, U, nq, inv_user, thr, S, gs, par, 1, any2, hl, hist_f);
     });
+    RKR_CUDA(cudaGetLastError());
+    timed(ix, st, "qsrp_fine2_list", [&] { qsrp_fine2_list_kernel<<<148 * 8, 256, 0, st>>>(hl, qv, U, thr, S, gs, hist_f); });
     RKR_CUDA(cudaGetLastError());
     timed(ix, st, "qsrp_final2", [&] {
-        qsrp_final2_kernel<<<(nq + 127) / 128, 128, 0, st>>>(hist_c, hist_f, nb, gs, S, topk, nq, par, cls2, clsg, counts);
+        qsrp_final2_kernel<<<(nq + 3) / 4, 128, 0, st>>>(hist_c, hist_f, nb, gs, S, topk, nq, par, cls2, clsg, counts);
     });
     RKR_CUDA(cudaGetLastError());
 

@@ -677,7 +677,7 @@ __device__ __forceinline__ void fine2_hit(const HitList &hl, bool hit, int64_t q
 
 // Scan for the pairs whose coarse group is flagged for their query (mask1, or mask2 when any
 // query has one): a grid-stride pass over the batch's codes as one flat [query][user] array, 16
-// codes per thread and step.
+// codes per thread and 512 per warp and step.
 __global__ void __launch_bounds__(256) qsrp_fine2_kernel(const uint8_t *__restrict__ code, QipView sc, int64_t n_user,
                                                         int nq, double inv_user, const float *__restrict__ thr, int S,
                                                         int gs, const QsrpParams *__restrict__ par, int second,
@@ -704,7 +704,7 @@ __global__ void __launch_bounds__(256) qsrp_fine2_kernel(const uint8_t *__restri
                     if (base + 4 * i + j < total) w[i] = (w[i] & ~(0xffu << (8 * j))) | ((uint32_t) code[base + 4 * i + j] << (8 * j));
             }
         }
-        if (n_user < 16) {  // a step may span several queries
+        if (n_user < 512) {  // a segment may span several queries
             for (int e = 0; e < 16; e++) {
                 const unsigned c = (w[e >> 2] >> (8 * (e & 3))) & 0xff;
                 const int64_t pos = base + e;
@@ -715,19 +715,36 @@ __global__ void __launch_bounds__(256) qsrp_fine2_kernel(const uint8_t *__restri
             }
             continue;
         }
-        // with at least 16 users a step of 16 codes meets at most one query boundary
+        // with at least 512 users a 512-code segment meets at most one query boundary: the
+        // segment's first query, found once per warp, and the next
+        int64_t qs = 0;
+        if ((threadIdx.x & 31) == 0) {
+            qs = (int64_t) ((double) seg * inv_user);
+            if (qs * n_user > seg) qs--;
+            else if ((qs + 1) * n_user <= seg) qs++;
+        }
+        qs = __shfl_sync(0xffffffffu, qs, 0);
         int64_t q0 = 0, edge = 0;
         uint32_t m0 = 0, m1 = 0;
         if (base < total) {
-            q0 = (int64_t) ((double) base * inv_user);
-            if (q0 * n_user > base) q0--;
-            else if ((q0 + 1) * n_user <= base) q0++;
+            q0 = base >= (qs + 1) * n_user ? qs + 1 : qs;
             edge = (q0 + 1) * n_user;
             m0 = (uint32_t) (second ? par[q0].mask2 : par[q0].mask1);
             m1 = edge < base + 16 && q0 + 1 < nq ? (uint32_t) (second ? par[q0 + 1].mask2 : par[q0 + 1].mask1) : 0u;
         }
         uint32_t hits = 0;
-        if (m0 | m1) {
+        const bool one_query = edge >= base + 16 && base + 16 <= total;
+        if (one_query && !m0) {
+            // nothing flagged for this query
+        } else if (one_query && (m0 & (m0 - 1)) == 0) {
+            // one flagged group and one query: a bytewise compare per word
+            const uint32_t pat = (uint32_t) (__ffs(m0) - 1) * 0x01010101u;
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const uint32_t eq = __vcmpeq4(w[i], pat) & 0x01010101u;
+                hits |= ((eq * 0x01020408u) >> 24) << (4 * i);
+            }
+        } else if (m0 | m1) {
 #pragma unroll
             for (int e = 0; e < 16; e++) {
                 const unsigned c = (w[e >> 2] >> (8 * (e & 3))) & 0xff;
@@ -1145,7 +1162,7 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     RKR_CUDA(cudaGetLastError());
     const float *thr = ix->thr.as<float>();
     const int32_t *srank = ix->sample_rank.as<int32_t>();
-    const unsigned fg = 148 * 8;
+    const unsigned fg = 148 * 16;
     const double inv_user = 1.0 / (double) U;
     hl.count = hit_count;
     timed(ix, st, "qsrp_fine2", [&] {

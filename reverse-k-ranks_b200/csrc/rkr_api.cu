@@ -1,6 +1,7 @@
 // rkr_api.cu -- the C ABI of librkr_b200.so (declared in include/rkr.h).
 #include <algorithm>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <vector>
@@ -131,6 +132,8 @@ int rkr_index_create(int32_t device, const float *user, int64_t n_user, const fl
     RKR_REQUIRE(device >= 0 && device < n_dev, "rkr_index_create: device %d of %d", device, n_dev);
     rkr_index *ix = new rkr_index();
     ix->device = device;
+    // RKR_REFINE_TC=0 keeps refinement on the exact tiles (both paths give the same results)
+    if (const char *v = getenv("RKR_REFINE_TC")) ix->refine_tc_on = strcmp(v, "0") != 0;
     ix->n_user = n_user;
     ix->n_item = n_item;
     ix->dim = dim;
@@ -210,7 +213,8 @@ int rkr_index_destroy(rkr_index *ix) {
     if (ix->stream) cudaStreamSynchronize(ix->stream);
     for (DevBuf *b : {&ix->user, &ix->item, &ix->item_sorted, &ix->item_norm, &ix->item_rnorm, &ix->user_rnorm,
                       &ix->sample_rank, &ix->thr, &ix->thr_summ, &ix->reg_rank, &ix->reg, &ix->transfer_item, &ix->svd_user,
-                      &ix->svd_user_km, &ix->item_km, &ix->item_sorted_km, &ix->ws_km,
+                      &ix->svd_user_km, &ix->item_km, &ix->item_sorted_km, &ix->ws_km, &ix->item_tc,
+                      &ix->item_tc_norm, &ix->item_tc_us, &ix->item_tc_us_norm, &ix->ws_tc,
                       &ix->svd_unorm, &ix->qip_state, &ix->ws_query, &ix->ws_qtr, &ix->ws_qnorm, &ix->ws_bucket,
                       &ix->ws_bucket2, &ix->ws_levels, &ix->ws_cls, &ix->ws_counts, &ix->ws_hist, &ix->ws_res,
                       &ix->ws_cand, &ix->ws_cand_off, &ix->ws_refine, &ix->ws_rank, &ix->ws_out, &ix->ws_stats,

@@ -842,6 +842,11 @@ struct rkr_index {
     rkr::DevBuf item_norm;     // [n_item], descending
     rkr::DevBuf item_rnorm;    // [n_item], norm of dims [check_dim, dim) of item_sorted
     rkr::DevBuf user_rnorm;    // [n_user], norm of dims [check_dim, dim) of user
+    // tensor-core refinement operands (built on first use for the current check_dim)
+    int tc_check_dim = -2;
+    bool refine_tc_on = true;                 // refinement counts on the tensor cores where the shape fits
+    rkr::DevBuf item_tc, item_tc_norm;        // item_sorted, split at check_dim, TF32-rounded; norms of both parts
+    rkr::DevBuf item_tc_us, item_tc_us_norm;  // item (original order), unsplit
     std::vector<float> h_item_norm_sorted;
     std::vector<int32_t> h_item_order;
     // SampleSearch
@@ -863,7 +868,7 @@ struct rkr_index {
     rkr::DevBuf qip_state;     // [n_user], QSRPNormalLP's carried query scores
     // per-call workspace
     rkr::DevBuf ws_query, ws_qtr, ws_qnorm, ws_bucket, ws_bucket2, ws_levels, ws_cls, ws_counts, ws_hist;
-    rkr::DevBuf ws_res, ws_cand, ws_cand_off, ws_refine, ws_rank, ws_out, ws_stats, ws_misc, ws_fix, ws_km;
+    rkr::DevBuf ws_res, ws_cand, ws_cand_off, ws_refine, ws_rank, ws_out, ws_stats, ws_misc, ws_fix, ws_km, ws_tc;
     std::vector<uint8_t> h_scratch;
     rkr::Profiler prof;
 };
@@ -908,7 +913,33 @@ inline int run_compaction(rkr_index *ix, P p, int nq, int topk, QueryCounts *cou
     return RKR_OK;
 }
 
+// Candidate refinement (refine_prep_kernel, then the per-item counting on tiles).
+struct RefineArgs {
+    const float *user;        // rows refined against the items (raw users)
+    const float *query;       // [n_query][dim] (QS/US: the score is recomputed from it)
+    const float *cand_qip;    // QSRP: score per candidate given; else nullptr
+    const int32_t *cand_user;
+    const int32_t *cand_query;
+    const int32_t *cand_lb, *cand_ub;
+    int64_t n_cand;
+    int dim;
+    int ipbound;              // 1: RefineCPUIPBound (QS, QSRP); 0: RefineCPU (US)
+    const float *item_norm;   // descending (ipbound)
+    int64_t n_item;
+    // outputs
+    float *qip;               // [n_cand]
+    int32_t *rank;            // [n_cand]
+    int32_t *nproc;           // [n_cand]
+    int32_t *ref_idx;         // refined candidates (compacted)
+    int32_t *ref_user;        // their users
+    int32_t *n_ref;           // device counter
+    int32_t *undecided;       // [n_cand] items whose score had to be computed in full
+};
+
 int ensure_device(const rkr_index *ix);
+// Counting step of the refinement on the tensor cores; sets *done = false (and does nothing) where
+// the shape does not fit it, leaving the exact tiles to run.
+int refine_tc(rkr_index *ix, const RefineArgs &ra, cudaStream_t st, bool *done);
 int thr_summary_build(rkr_index *ix);
 int refine_prepare_norms(rkr_index *ix);
 int query_batch(rkr_index *ix, int method, const float *d_query, int n_query, int topk, rkr_user_rank *d_out,

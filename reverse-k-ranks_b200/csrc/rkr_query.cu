@@ -176,27 +176,6 @@ struct QsCompactPolicy {
 // refinement
 // ============================================================================================
 
-struct RefineArgs {
-    const float *user;        // rows refined against the items (raw users)
-    const float *query;       // [n_query][dim] (QS/US: the score is recomputed from it)
-    const float *cand_qip;    // QSRP: score per candidate given; else nullptr
-    const int32_t *cand_user;
-    const int32_t *cand_query;
-    const int32_t *cand_lb, *cand_ub;
-    int64_t n_cand;
-    int dim;
-    int ipbound;              // 1: RefineCPUIPBound (QS, QSRP); 0: RefineCPU (US)
-    const float *item_norm;   // descending (ipbound)
-    int64_t n_item;
-    // outputs
-    float *qip;               // [n_cand]
-    int32_t *rank;            // [n_cand]
-    int32_t *nproc;           // [n_cand]
-    int32_t *ref_idx;         // refined candidates (compacted)
-    int32_t *ref_user;        // their users
-    int32_t *n_ref;           // device counter
-    int32_t *undecided;       // [n_cand] items whose score had to be computed in full
-};
 
 // Score of each candidate and its rank when the bounds agree (ComputeAllIPBound.hpp:319-341;
 // ComputeAll.hpp:84-100); the rest are queued for refine_tile with their item cut-off
@@ -587,6 +566,9 @@ static int refine_and_assemble(rkr_index *ix, int method, const float *d_query, 
         ra.undecided = undecided;
         timed(ix, st, "refine_prep", [&] { refine_prep_kernel<<<(unsigned) ((n_cand + 255) / 256), 256, 0, st>>>(ra); });
         RKR_CUDA(cudaGetLastError());
+        bool tc_done = false;
+        if (ix->refine_tc_on) RKR_TRY(refine_tc(ix, ra, st, &tc_done));
+        if (!tc_done) {
         // the refined candidates' user vectors, gathered k-major (rows past n_ref gather user 0)
         timed(ix, st, "refine_gather", [&] { to_kmajor(ix->user.as<float>(), ref_user, n_cand, ix->dim, cand_km, st); });
         RKR_CUDA(cudaGetLastError());
@@ -605,6 +587,7 @@ static int refine_and_assemble(rkr_index *ix, int method, const float *d_query, 
             cudaError_t ce = cudaSuccess;
             timed(ix, st, "refine_tile", [&] { ce = launch_big_split(cands, items, k_split, ix->dim, re, st); });
             RKR_CUDA(ce);
+        }
         }
     }
     AssembleArgs aa;

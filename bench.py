@@ -247,6 +247,8 @@ def main():
     n_user, n_item, dim, n_sample, n_si, stopk, batch, topk = CONFIGS[args.config]
     if args.batch:
         batch = args.batch
+    elif args.method == "US":
+        batch = 100  # US answers exactly 100 queries per call when S <= 1000 (US.hpp:117-131)
     n_thread = os.cpu_count() or 1
 
     if args.impl == "reference" and rank_id != 0:
@@ -372,7 +374,9 @@ def main():
     # ---- latency ------------------------------------------------------------------------------------------
     single = []
     q1 = batches[0]
-    for i in range(args.single_queries):
+    # US answers exactly 100 queries per call when S <= 1000 (US.hpp:117-131): no single-query latency
+    n_single = 0 if args.method == "US" else args.single_queries
+    for i in range(n_single):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -401,7 +405,7 @@ def main():
            "h2d_bytes_per_step": batch * dim * 4, "d2h_bytes_per_step": batch * topk * rec_bytes}
 
     cpu = None
-    if rank_id == 0 and world == 1 and reference_available():
+    if rank_id == 0 and world == 1 and args.method == "QSRPNormalLP" and reference_available():
         timer = ReferenceTimer(parts, item, n_thread)
         n, secs = timer.run(batches[0].cpu().numpy(), topk, args.cpu_seconds)
         timer.close()
@@ -423,8 +427,8 @@ def main():
                        "l2": "inputs larger than L2 (resident index ~1.6 GB)",
                        "parallelism": f"replica x{world} (queries split across GPUs)"},
             "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
-            "single_query_p50_ms": float(np.percentile(single, 50)),
-            "single_query_p99_ms": float(np.percentile(single, 99)),
+            "single_query_p50_ms": float(np.percentile(single, 50)) if single else None,
+            "single_query_p99_ms": float(np.percentile(single, 99)) if single else None,
             "build_sec": build_sec, "build_stages_sec": {k: round(v, 3) for k, v in stages.items()},
             "e2e": e2e, "gpu_launches": int(launches_per_step * args.steps), "roofline": roofline,
             "cpu_baseline": cpu, "clocks": clk.summary(), "query_stats_mean": stats_mean,

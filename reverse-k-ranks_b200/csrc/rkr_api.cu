@@ -194,6 +194,10 @@ int rkr_index_create(int32_t device, const float *user, int64_t n_user, const fl
     }
     // k-major copies for the refinement tiles
     const size_t km = sizeof(float) * (size_t) dim * (size_t) kmajor_ld(n_item);
+    const size_t kmu = sizeof(float) * (size_t) dim * (size_t) kmajor_ld(n_user);
+    if ((s = ix->user_km.ensure(kmu)) ||
+        (s = to_kmajor(ix->user.as<float>(), nullptr, n_user, dim, ix->user_km.as<float>(), ix->stream)))
+        return fail(s);
     if ((s = ix->item_km.ensure(km)) || (s = ix->item_sorted_km.ensure(km)) ||
         (s = to_kmajor(ix->item.as<float>(), nullptr, n_item, dim, ix->item_km.as<float>(), ix->stream)) ||
         (s = to_kmajor(ix->item_sorted.as<float>(), nullptr, n_item, dim, ix->item_sorted_km.as<float>(), ix->stream)))
@@ -213,7 +217,7 @@ int rkr_index_destroy(rkr_index *ix) {
     if (ix->stream) cudaStreamSynchronize(ix->stream);
     for (DevBuf *b : {&ix->user, &ix->item, &ix->item_sorted, &ix->item_norm, &ix->item_rnorm, &ix->user_rnorm,
                       &ix->sample_rank, &ix->thr, &ix->thr_summ, &ix->reg_rank, &ix->reg, &ix->transfer_item, &ix->svd_user,
-                      &ix->svd_user_km, &ix->item_km, &ix->item_sorted_km, &ix->ws_km, &ix->item_tc,
+                      &ix->svd_user_km, &ix->user_km, &ix->item_km, &ix->item_sorted_km, &ix->ws_km, &ix->item_tc,
                       &ix->item_tc_norm, &ix->item_tc_us, &ix->item_tc_us_norm, &ix->ws_tc,
                       &ix->svd_unorm, &ix->qip_state, &ix->ws_query, &ix->ws_qtr, &ix->ws_qnorm, &ix->ws_bucket,
                       &ix->ws_bucket2, &ix->ws_levels, &ix->ws_cls, &ix->ws_counts, &ix->ws_hist, &ix->ws_res,
@@ -322,7 +326,8 @@ int rkr_index_size_bytes(const rkr_index *ix, uint64_t *bytes) {
     uint64_t s = 0;
     for (const DevBuf *b : {&ix->user, &ix->item, &ix->item_sorted, &ix->item_norm, &ix->item_rnorm, &ix->user_rnorm,
                             &ix->sample_rank, &ix->thr, &ix->thr_summ, &ix->reg_rank, &ix->reg, &ix->transfer_item, &ix->svd_user,
-                            &ix->svd_user_km, &ix->item_km, &ix->item_sorted_km, &ix->svd_unorm, &ix->qip_state})
+                            &ix->svd_user_km, &ix->user_km, &ix->item_km, &ix->item_sorted_km, &ix->svd_unorm,
+                            &ix->qip_state})
         s += b->bytes;
     *bytes = s;
     return RKR_OK;

@@ -864,6 +864,7 @@ struct rkr_index {
     rkr::DevBuf transfer_item; // [dim][dim]
     rkr::DevBuf svd_user;      // [n_user][dim]
     rkr::DevBuf svd_user_km;   // k-major copy: [dim][kmajor_ld(n_user)]
+    rkr::DevBuf user_km;       // k-major copy of user: [dim][kmajor_ld(n_user)]
     rkr::DevBuf svd_unorm;     // [n_user], norm of dims [check_dim, dim) of svd_user
     rkr::DevBuf qip_state;     // [n_user], QSRPNormalLP's carried query scores
     // per-call workspace

@@ -28,12 +28,13 @@
 
 namespace rkr {
 
-// launched from rkr_query.cu
-int refine_and_assemble_qsrp(rkr_index *ix, const float *d_query, int nq, int topk, const QueryCounts *d_counts,
-                             const int32_t *d_res_user, const int32_t *d_res_rank, const float *d_res_qip, int64_t n_cand,
-                             int32_t *d_cand_user, int32_t *d_cand_query, int32_t *d_cand_lb, int32_t *d_cand_ub,
-                             const float *d_cand_qip, const int64_t *d_cand_off, rkr_user_rank *d_out,
-                             rkr_query_stats *d_stats, cudaStream_t st);
+// in rkr_query.cu
+int refine_and_assemble_pairs(rkr_index *ix, int method, const float *d_query, int nq, int topk,
+                              const QueryCounts *d_counts, const int32_t *d_res_user, const int32_t *d_res_rank,
+                              const float *d_res_qip, int64_t n_cand, int32_t *d_cand_user, int32_t *d_cand_query,
+                              int32_t *d_cand_lb, int32_t *d_cand_ub, const float *d_cand_qip,
+                              const int64_t *d_cand_off, rkr_user_rank *d_out, rkr_query_stats *d_stats,
+                              cudaStream_t st);
 
 // ---- the regression model's arithmetic (NormalLinearRegressionLP.hpp) ------------------------------
 
@@ -265,6 +266,7 @@ struct Round1Epi {
         return true;
     }
     __device__ void finish_lo(char *x, const BigResult &res, int64_t a0, int64_t b0) const {
+        if (!lv) return;  // no round 1 (QS, US)
         const float *qn = reinterpret_cast<const float *>(x);
         const int ra = threadIdx.x & (kBig - 1), half = threadIdx.x >> 7, lane = threadIdx.x & 31;
         const int64_t u = a0 + ra;
@@ -547,6 +549,19 @@ __global__ void qsrp_final1_kernel(QsrpParams *__restrict__ par, int nq, int top
     par[q] = p;
 }
 
+// QS and US have no round 1: every user reaches the sampled-threshold bounds, and the reference's
+// ip_cost starts at n_user (QS.hpp:143, US.hpp:131).
+__global__ void qs_params_kernel(QsrpParams *__restrict__ par, int nq, int64_t n_user) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    QsrpParams p = {};
+    p.lv_res = -1;
+    p.lv_pr = 1 << 30;
+    p.lv_m1 = -1;
+    p.n_ref1 = (int) n_user;
+    par[q] = p;
+}
+
 // ---- round 2 -------------------------------------------------------------------------------------
 
 // The bucket of s inside coarse group g (< nb): g * gs + the group's thresholds >= s.
@@ -581,10 +596,11 @@ __global__ void __launch_bounds__(kHistThreads) qsrp_round2_kernel(const uint32_
         const QsrpParams &g = par[q];
         p.mode1 = g.mode1; p.all1 = g.all1; p.lv_res = g.lv_res; p.lv_pr = g.lv_pr; p.lv_m1 = g.lv_m1;
     }
+    const bool all_survive = lv == nullptr;  // QS and US: no round 1
     for (int b = threadIdx.x; b < copies * nbin; b += blockDim.x) h[b] = 0;
     __syncthreads();
     int *mine = h + ((threadIdx.x >> 5) % copies) * nbin;
-    const uint32_t *lrow = lv + (int64_t) q * n_user;
+    const uint32_t *lrow = lv ? lv + (int64_t) q * n_user : nullptr;
     uint8_t *crow = code + (int64_t) q * n_user;
     const int64_t u0 = (int64_t) blockIdx.x * chunk, u1 = min(u0 + chunk, n_user);
     constexpr int G = 4;  // pairs in flight per thread; the group code is loaded with the levels
@@ -594,14 +610,14 @@ __global__ void __launch_bounds__(kHistThreads) qsrp_round2_kernel(const uint32_
 #pragma unroll
         for (int g = 0; g < G; g++) {
             const bool in = ub + g * kHistThreads < u1;
-            v[g] = in ? __ldg(lrow + ub + g * kHistThreads) : 0u;
+            v[g] = in && !all_survive ? __ldg(lrow + ub + g * kHistThreads) : 0u;
             cc[g] = in ? crow[ub + g * kHistThreads] : 0u;
         }
 #pragma unroll
         for (int g = 0; g < G; g++) {
             const int64_t u = ub + g * kHistThreads;
             if (u >= u1) break;
-            const int k = class1_lv(p, v[g] & 0xffff, v[g] >> 16);
+            const int k = all_survive ? kClsRefine : class1_lv(p, v[g] & 0xffff, v[g] >> 16);
             if (k == kClsRefine || k == kClsIdle) atomicAdd(mine + cc[g], 1);
             else crow[u] = k == kClsResult ? kCodeResult1 : kCodePruned1;
         }
@@ -1039,8 +1055,11 @@ template <typename T> T *carve(uint8_t *&p, size_t n) {
 inline size_t carve_size(size_t n, size_t elem) { return ((n * elem + 255) & ~size_t(255)) + 256; }
 }  // namespace
 
-int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_rank *d_out, rkr_query_stats *d_stats,
-               cudaStream_t st) {
+// One chunk of queries.  QSRPNormalLP runs both rounds; QS and US (no regression round, scores
+// in the original space) run the scores tile without levels and start at round 2.
+int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, int topk, rkr_user_rank *d_out,
+               rkr_query_stats *d_stats, cudaStream_t st) {
+    const bool qsrp = method == RKR_METHOD_QSRP_NORMAL_LP;
     const int64_t U = ix->n_user;
     const int dim = ix->dim, c = ix->check_dim, S = ix->n_sample, Sr = ix->n_sample_reg;
     const int n_item = (int) ix->n_item;
@@ -1090,12 +1109,16 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     RKR_CUDA(cudaMemsetAsync(hit_count, 0, 2 * sizeof(int), st));
     RKR_CUDA(cudaMemsetAsync(ix->ws_hist.p, 0, (size_t) (ph - ix->ws_hist.as<uint8_t>()), st));
 
-    timed(ix, st, "transfer_query", [&] {
-        transfer_query_kernel<<<nq, 128, 0, st>>>(d_query, ix->transfer_item.as<float>(), dim, c, qtr, qnorm);
-    });
-    RKR_CUDA(cudaGetLastError());
+    if (qsrp) {
+        timed(ix, st, "transfer_query", [&] {
+            transfer_query_kernel<<<nq, 128, 0, st>>>(d_query, ix->transfer_item.as<float>(), dim, c, qtr, qnorm);
+        });
+        RKR_CUDA(cudaGetLastError());
+    } else {
+        RKR_CUDA(cudaMemsetAsync(qnorm, 0, sizeof(float) * nq, st));
+    }
     RKR_TRY(ix->ws_km.ensure(sizeof(float) * (size_t) dim * (size_t) kmajor_ld(nq)));
-    RKR_TRY(to_kmajor(qtr, nullptr, nq, dim, ix->ws_km.as<float>(), st));
+    RKR_TRY(to_kmajor(qsrp ? qtr : d_query, nullptr, nq, dim, ix->ws_km.as<float>(), st));
     ScoreSrc sc;
     sc.svd_user = ix->svd_user.as<float>();
     sc.qtr = qtr;
@@ -1115,7 +1138,7 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     e1.qnorm = qnorm;
     e1.thr_summ = ix->thr_summ.as<float>();
     e1.m = m;
-    e1.lv = lv;
+    e1.lv = qsrp ? lv : nullptr;
     e1.code = code;
     e1.qip = qip;
     e1.nb = nb;
@@ -1123,18 +1146,20 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     e1.n_query = nq;
     e1.fix = fix;
     cudaError_t ce = cudaSuccess;
-    const KMajor ka = {ix->svd_user_km.as<float>(), U, kmajor_ld(U), kmajor_ld(U)};
+    const KMajor ka = {(qsrp ? ix->svd_user_km : ix->user_km).as<float>(), U, kmajor_ld(U), kmajor_ld(U)};
     const KMajor kb = {ix->ws_km.as<float>(), nq, kmajor_ld(nq), kmajor_ld(nq)};
-    timed(ix, st, "qsrp_scores", [&] { ce = launch_big_split(ka, kb, c, dim, e1, st); });
+    // QS / US: one sequential sum over all coordinates (QS.hpp:137-143), seen by finish_hi
+    timed(ix, st, "qsrp_scores", [&] { ce = launch_big_split(ka, kb, qsrp ? c : dim, dim, e1, st); });
     RKR_CUDA(ce);
+    const int64_t chunk = 16384;
+    dim3 hg((unsigned) ((U + chunk - 1) / chunk), (unsigned) nq);
+    if (qsrp) {
     timed(ix, st, "qsrp_fix1", [&] { qsrp_fix1_kernel<<<148 * 4, 256, 0, st>>>(fix, m, e1.unorm, qnorm, U, lv); });
     RKR_CUDA(cudaGetLastError());
     timed(ix, st, "qsrp_fix1_scan", [&] {
         qsrp_fix1_scan_kernel<<<148 * 8, 256, 0, st>>>(fix_count, fix_cap, m, sc, e1.unorm, qnorm, U, nq, lv);
     });
     RKR_CUDA(cudaGetLastError());
-    const int64_t chunk = 16384;
-    dim3 hg((unsigned) ((U + chunk - 1) / chunk), (unsigned) nq);
     timed(ix, st, "level_hist", [&] {
         level_hist_kernel<<<hg, kHistThreads, hist_copies(2 * nl) * 2 * nl * sizeof(int), st>>>(lv, U, m.rank, Sr, n_item,
                                                                                                chunk, hist_l, anomaly);
@@ -1151,9 +1176,13 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
     }
     timed(ix, st, "qsrp_final1", [&] { qsrp_final1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, topk); });
     RKR_CUDA(cudaGetLastError());
+    } else {
+        qs_params_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, U);
+        RKR_CUDA(cudaGetLastError());
+    }
     timed(ix, st, "qsrp_round2", [&] {
-        qsrp_round2_kernel<<<hg, kHistThreads, hist_copies(nb + 1) * (nb + 1) * sizeof(int), st>>>(lv, code, U, par, nb,
-                                                                                                  chunk, hist_c);
+        qsrp_round2_kernel<<<hg, kHistThreads, hist_copies(nb + 1) * (nb + 1) * sizeof(int), st>>>(
+            qsrp ? lv : nullptr, code, U, par, nb, chunk, hist_c);
     });
     RKR_CUDA(cudaGetLastError());
     timed(ix, st, "qsrp_select2c", [&] {
@@ -1250,9 +1279,9 @@ int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_r
         });
         RKR_CUDA(cudaGetLastError());
     }
-    RKR_TRY(refine_and_assemble_qsrp(ix, d_query, nq, topk, counts, res_user, res_rank, res_qip, n_cand, cand_user,
-                                     cand_query, cand_lb, cand_ub, cand_qip, d_off, d_out, d_stats, st));
-    timed(ix, st, "qsrp_state", [&] {
+    RKR_TRY(refine_and_assemble_pairs(ix, method, d_query, nq, topk, counts, res_user, res_rank, res_qip, n_cand,
+                                      cand_user, cand_query, cand_lb, cand_ub, cand_qip, d_off, d_out, d_stats, st));
+    if (qsrp) timed(ix, st, "qsrp_state", [&] {
         qsrp_state_kernel<<<(unsigned) ((U + 255) / 256), 256, 0, st>>>(code, qv, U, nq, ix->qip_state.as<float>());
     });
     RKR_CUDA(cudaGetLastError());

@@ -1,20 +1,16 @@
-// rkr_query.cu -- batched reverse k-ranks retrieval on the device (QS, QSRPNormalLP, US).
+// rkr_query.cu -- batched reverse k-ranks retrieval on the device (QS, QSRPNormalLP, US): the
+// refinement of candidates and the assembly of results, and the batch driver.
 //
 // A batch of queries runs as a short pipeline of kernels; every (query, user) decision the
 // reference makes one query at a time (src/impl/QS.hpp:127-224, src/impl/QSRPNormalLP.hpp:137-253,
-// src/impl/US.hpp:117-201) is made for the whole batch at once:
+// src/impl/US.hpp:117-201) is made for the whole batch at once.  The bound and prune stages are in
+// rkr_qsrp.cu (QS and US are its second round on its own); here:
 //
-//   score_bucket      exact query score of every (user, query) pair + binary search over the
-//                     user's sampled thresholds -> one 16-bit bucket per pair      [SIMT, FP32 exact]
-//   select_bucket     per query: histogram of buckets -> k-th smallest lower/upper rank bound ->
-//                     class (result / prune / refine) of every bucket value
-//   compact           per query, in user-id order: first top-k result users, all candidates
-//   refine_prep       candidates: exact score, norm cut-off, rank when the bounds already agree
-//   refine_tile       candidates x norm-ordered items: exact split-sum scores, bound tests,
-//                     count of items scoring >= the query (or > for US)      [SIMT, FP32 exact]
+//   refine_prep       candidates: score, norm cut-off, rank when the bounds already agree
+//   refine_tc         candidates x items: the reference's per-item test on tensor-core scores with
+//                     exact resolution of undecided pairs (rkr_refine_tc.cu); refine_tile, the
+//                     exact SIMT tiles, where that path does not apply
 //   assemble          per query: results in user-id order, then candidates by (rank, user id)
-//
-// QSRPNormalLP adds the regression stage before it (qsrp_* kernels below).
 #include <algorithm>
 #include <cstring>
 #include <numeric>
@@ -24,158 +20,8 @@
 namespace rkr {
 
 // ============================================================================================
-// shared pieces
-// ============================================================================================
-
-// ============================================================================================
-// QS / US: bucket per pair
-// ============================================================================================
-
-// queryIP = InnerProduct(query, user) over all dims (QS.hpp:137-143, US.hpp:125-131), then
-// SampleSearch::CoarseBinarySearch's bucket (SampleSearch.hpp:91-107).
-__global__ void __launch_bounds__(kTileThreads) score_bucket_kernel(const float *__restrict__ user, int64_t n_user,
-                                                                   int dim, const float *__restrict__ query,
-                                                                   int n_query, const float *__restrict__ thr, int S,
-                                                                   uint16_t *__restrict__ bucket) {
-    __shared__ TileSmem sm;
-    __shared__ ThrSummary ts;
-    const int64_t b0 = (int64_t) blockIdx.x * kTile;  // queries
-    const int64_t a0 = (int64_t) blockIdx.y * kTile;  // users
-    load_thr_summary(ts, thr, n_user, a0, S);
-    float lo[4][4], hi[4][4];
-    exact_tile(sm, user, nullptr, n_user, dim, a0, query, n_query, dim, b0, 0, dim, dim, lo, hi);
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const int64_t u = a0 + 4 * tx + i;
-        if (u >= n_user) continue;
-        const float *row = thr + u * S;
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int64_t q = b0 + 4 * ty + j;
-            if (q >= n_query) continue;
-            bucket[q * n_user + u] = (uint16_t) bucket_of_2level(ts.v[4 * tx + i], row, S, lo[i][j]);
-        }
-    }
-}
-
-// score_bucket on 128 x 128 tiles: the exact score of each (user, query) pair and its bucket.
-struct QsBucketEpi {
-    static constexpr size_t kExtra = sizeof(float) * kBig * ThrSummary::kMaxGroups;
-    const float *thr;
-    int64_t n_user, n_query;
-    int S;
-    uint16_t *bucket;
-    __device__ void prologue(char *extra, int64_t a0, int64_t) const {
-        load_thr_summary_rows(reinterpret_cast<float *>(extra), kBig, thr, n_user, a0, S);
-    }
-    __device__ bool active(char *, int64_t, int64_t) const { return true; }
-    __device__ void finish(char *extra, const BigResult &res, int64_t a0, int64_t b0, bool) const {
-        const int ra = threadIdx.x & (kBig - 1), half = threadIdx.x >> 7;
-        const int64_t u = a0 + ra;
-        if (u >= n_user) return;
-        const float *summ = reinterpret_cast<const float *>(extra) + ra * ThrSummary::kMaxGroups;
-        const float *row = thr + u * S;
-#pragma unroll 4
-        for (int i = 0; i < kBig / 2; i++) {
-            const int rb = half + 2 * i;
-            const int64_t q = b0 + rb;
-            if (q >= n_query) break;
-            bucket[q * n_user + u] = (uint16_t) bucket_of_2level(summ, row, S, res.v[rb][ra]);
-        }
-    }
-};
-
-__global__ void select_bucket_kernel(const int *__restrict__ hist_all, int S, const int32_t *__restrict__ rank,
-                                     int n_item, int topk, int n_user, uint8_t *__restrict__ cls,
-                                     QueryCounts *__restrict__ counts) {
-    const int q = blockIdx.x;
-    const int *hist = hist_all + (int64_t) q * (S + 1);
-    if (threadIdx.x == 0) {
-        int bk = S;
-        int64_t cum = 0;
-        for (int b = 0; b <= S; b++) {
-            cum += hist[b];
-            if (cum >= topk) { bk = b; break; }
-        }
-        int L, U;
-        bucket_bounds(bk, S, rank, n_item, L, U);
-        QueryCounts c = {};
-        c.bk = bk; c.lstar = L; c.ustar = U;
-        c.ip_base = n_user;
-        uint8_t *cq = cls + (int64_t) q * (S + 1);
-        if (L == U) {
-            int64_t nres = 0;
-            for (int b = 0; b <= S; b++) {
-                int lb, ub;
-                bucket_bounds(b, S, rank, n_item, lb, ub);
-                const bool r = ub <= L && lb <= L;
-                cq[b] = r ? kClsResult : kClsIdle;
-                if (r) nres += hist[b];
-            }
-            c.mode = 1; c.n_result = topk; c.n_prune = 0; c.n_cand = 0;
-            c.n_res_emit = (int) (nres < topk ? nres : (int64_t) topk);
-        } else {
-            int64_t nres = 0, npr = 0, nref = 0;
-            for (int b = 0; b <= S; b++) {
-                int lb, ub;
-                bucket_bounds(b, S, rank, n_item, lb, ub);
-                uint8_t k;
-                if (lb <= U) { k = kClsResult; nres += hist[b]; }
-                else if (L <= ub) { k = kClsPrune; npr += hist[b]; }
-                else { k = kClsRefine; nref += hist[b]; }
-                cq[b] = k;
-            }
-            c.mode = 0;
-            if (nres + nref == topk) {  // PruneCandidateByBound.hpp:139-150
-                for (int b = 0; b <= S; b++) if (cq[b] == kClsRefine) cq[b] = kClsResult;
-                nres = topk; nref = 0;
-            }
-            c.n_result = (int) nres; c.n_prune = (int) npr;
-            c.n_cand = nres >= topk ? 0 : (int) nref;
-            c.n_res_emit = (int) (nres < topk ? nres : (int64_t) topk);
-        }
-        counts[q] = c;
-    }
-}
-
-// QS / US classification of a pair for the ordered compaction: the class of its bucket.
-struct QsCompactPolicy {
-    struct Aux { uint16_t b; };
-    const uint16_t *bucket;
-    int64_t n_user;
-    const uint8_t *cls;
-    int S;
-    const QueryCounts *counts;
-    const int64_t *cand_off;
-    int topk;
-    int32_t *res_user, *cand_user, *cand_query;
-    uint16_t *cand_bucket;
-    __device__ bool query_active(int q) const { return true; }
-    __device__ uint32_t need_mask(int, int64_t, int n) const { return (1u << n) - 1; }
-    __device__ int classify(int q, int64_t u, Aux &aux, bool) const {
-        const uint16_t b = bucket[(int64_t) q * n_user + u];
-        aux.b = b;
-        const uint8_t k = __ldg(cls + (int64_t) q * (S + 1) + b);
-        if (k == kClsResult) return 1;
-        return (k == kClsRefine && counts[q].n_cand > 0) ? 2 : 0;
-    }
-    __device__ void emit_result(int q, int pos, int64_t u, const Aux &) const {
-        res_user[(int64_t) q * topk + pos] = (int32_t) u;
-    }
-    __device__ void emit_cand(int q, int pos, int64_t u, const Aux &aux) const {
-        if (pos >= counts[q].n_cand) return;  // the count pass disagrees; reported by compact_scan
-        const int64_t e = cand_off[q] + pos;
-        cand_user[e] = (int32_t) u;
-        cand_query[e] = q;
-        cand_bucket[e] = aux.b;
-    }
-};
-
-// ============================================================================================
 // refinement
 // ============================================================================================
-
 
 // Score of each candidate and its rank when the bounds agree (ComputeAllIPBound.hpp:319-341;
 // ComputeAll.hpp:84-100); the rest are queued for refine_tile with their item cut-off
@@ -474,36 +320,6 @@ __global__ void assemble_kernel(AssembleArgs a) {
     }
 }
 
-// Ranks and exact scores of the emitted result users (QS/US): rank = lower bound of the bucket,
-// score = InnerProduct(query, user).
-__global__ void result_fill_kernel(const QueryCounts *__restrict__ counts, const int32_t *__restrict__ res_user,
-                                   const uint16_t *__restrict__ bucket, int64_t n_user, const float *__restrict__ user,
-                                   const float *__restrict__ query, int dim, int S, const int32_t *__restrict__ rank,
-                                   int n_item, int topk, int32_t *__restrict__ res_rank, float *__restrict__ res_qip) {
-    const int q = blockIdx.x;
-    const int n = counts[q].n_res_emit;
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        const int64_t i = (int64_t) q * topk + k;
-        const int u = res_user[i];
-        int lb, ub;
-        bucket_bounds(bucket[(int64_t) q * n_user + u], S, rank, n_item, lb, ub);
-        res_rank[i] = lb;
-        res_qip[i] = exact_dot(query + (int64_t) q * dim, user + (int64_t) u * dim, dim);
-    }
-}
-
-// Bounds of each candidate from its bucket.
-__global__ void cand_bounds_kernel(const uint16_t *__restrict__ cand_bucket, int64_t n, int S,
-                                   const int32_t *__restrict__ rank, int n_item, int32_t *__restrict__ lb_out,
-                                   int32_t *__restrict__ ub_out) {
-    const int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= n) return;
-    int lb, ub;
-    bucket_bounds(cand_bucket[e], S, rank, n_item, lb, ub);
-    lb_out[e] = lb;
-    ub_out[e] = ub;
-}
-
 // ============================================================================================
 // host orchestration
 // ============================================================================================
@@ -616,115 +432,28 @@ static int refine_and_assemble(rkr_index *ix, int method, const float *d_query, 
     return RKR_OK;
 }
 
-// QS and US: one chunk of queries.
-static int qs_chunk(rkr_index *ix, int method, const float *d_query, int nq, int topk, rkr_user_rank *d_out,
-                    rkr_query_stats *d_stats, cudaStream_t st) {
-    const int64_t U = ix->n_user;
-    const int S = ix->n_sample;
-    const int dim = ix->dim;
-    RKR_TRY(ix->ws_bucket.ensure((size_t) nq * (size_t) U * sizeof(uint16_t)));
-    uint16_t *bucket = ix->ws_bucket.as<uint16_t>();
-    RKR_TRY(ix->ws_cls.ensure((size_t) nq * (S + 1)));
-    RKR_TRY(ix->ws_counts.ensure(sizeof(QueryCounts) * (size_t) nq));
-    RKR_TRY(ix->ws_hist.ensure(sizeof(int) * (size_t) nq * (S + 1)));
-    QueryCounts *counts = ix->ws_counts.as<QueryCounts>();
-    int *hist = ix->ws_hist.as<int>();
-    {
-        QsBucketEpi epi;
-        epi.thr = ix->thr.as<float>();
-        epi.n_user = U;
-        epi.n_query = nq;
-        epi.S = S;
-        epi.bucket = bucket;
-        cudaError_t e = cudaSuccess;
-        timed(ix, st, "score_bucket", [&] {
-            e = launch_big(ix->user.as<float>(), nullptr, U, dim, d_query, nq, dim, 0, dim, epi, st);
-        });
-        RKR_CUDA(e);
-        RKR_CUDA(cudaMemsetAsync(hist, 0, sizeof(int) * (size_t) nq * (S + 1), st));
-        const int64_t chunk = 16384;
-        dim3 hg((unsigned) ((U + chunk - 1) / chunk), (unsigned) nq);
-        timed(ix, st, "bucket_hist", [&] {
-            bucket_hist_kernel<<<hg, kHistThreads, hist_copies(S + 1) * (S + 1) * sizeof(int), st>>>(bucket, U, S + 1,
-                                                                                                  chunk, hist);
-        });
-        RKR_CUDA(cudaGetLastError());
-        timed(ix, st, "select_bucket", [&] {
-            select_bucket_kernel<<<nq, 32, 0, st>>>(hist, S, ix->sample_rank.as<int32_t>(), (int) ix->n_item, topk,
-                                                   (int) U, ix->ws_cls.as<uint8_t>(), counts);
-        });
-        RKR_CUDA(cudaGetLastError());
-    }
-    std::vector<QueryCounts> hc(nq);
-    RKR_CUDA(cudaMemcpyAsync(hc.data(), counts, sizeof(QueryCounts) * nq, cudaMemcpyDeviceToHost, st));
-    RKR_CUDA(cudaStreamSynchronize(st));
-    std::vector<int64_t> off(nq + 1, 0);
-    for (int q = 0; q < nq; q++) off[q + 1] = off[q] + hc[q].n_cand;
-    const int64_t n_cand = off[nq];
-    size_t need = carve_size(nq + 1, 8) + carve_size((size_t) nq * topk, 4) * 3 + carve_size(n_cand, 4) * 4 +
-                  carve_size(n_cand, 2);
-    RKR_TRY(ix->ws_cand.ensure(need));
-    uint8_t *p = ix->ws_cand.as<uint8_t>();
-    int64_t *d_off = carve<int64_t>(p, nq + 1);
-    int32_t *res_user = carve<int32_t>(p, (size_t) nq * topk);
-    int32_t *res_rank = carve<int32_t>(p, (size_t) nq * topk);
-    float *res_qip = carve<float>(p, (size_t) nq * topk);
-    int32_t *cand_user = carve<int32_t>(p, n_cand);
-    int32_t *cand_query = carve<int32_t>(p, n_cand);
-    int32_t *cand_lb = carve<int32_t>(p, n_cand);
-    int32_t *cand_ub = carve<int32_t>(p, n_cand);
-    uint16_t *cand_bucket = carve<uint16_t>(p, n_cand);
-    RKR_CUDA(cudaMemcpyAsync(d_off, off.data(), sizeof(int64_t) * (nq + 1), cudaMemcpyHostToDevice, st));
-    QsCompactPolicy pol;
-    pol.bucket = bucket;
-    pol.n_user = U;
-    pol.cls = ix->ws_cls.as<uint8_t>();
-    pol.S = S;
-    pol.counts = counts;
-    pol.cand_off = d_off;
-    pol.topk = topk;
-    pol.res_user = res_user;
-    pol.cand_user = cand_user;
-    pol.cand_query = cand_query;
-    pol.cand_bucket = cand_bucket;
-    RKR_TRY(run_compaction(ix, pol, nq, topk, counts, st));
-    timed(ix, st, "result_fill", [&] {
-        result_fill_kernel<<<nq, 128, 0, st>>>(counts, res_user, bucket, U, ix->user.as<float>(), d_query, dim, S,
-                                               ix->sample_rank.as<int32_t>(), (int) ix->n_item, topk, res_rank, res_qip);
-    });
-    RKR_CUDA(cudaGetLastError());
-    if (n_cand > 0) {
-        timed(ix, st, "cand_bounds", [&] {
-            cand_bounds_kernel<<<(unsigned) ((n_cand + 255) / 256), 256, 0, st>>>(
-                cand_bucket, n_cand, S, ix->sample_rank.as<int32_t>(), (int) ix->n_item, cand_lb, cand_ub);
-        });
-        RKR_CUDA(cudaGetLastError());
-    }
-    RKR_TRY(refine_and_assemble(ix, method, d_query, nq, topk, counts, hc, res_user, res_rank, res_qip, n_cand,
-                                cand_user, cand_query, cand_lb, cand_ub, nullptr, d_off, d_out, d_stats, st));
-    RKR_CUDA(cudaStreamSynchronize(st));
-    return RKR_OK;
-}
+// One chunk of queries, every method (rkr_qsrp.cu).
+int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, int topk, rkr_user_rank *d_out,
+               rkr_query_stats *d_stats, cudaStream_t st);
 
-int qsrp_chunk(rkr_index *ix, const float *d_query, int nq, int topk, rkr_user_rank *d_out, rkr_query_stats *d_stats,
-               cudaStream_t st);
-
-int refine_and_assemble_qsrp(rkr_index *ix, const float *d_query, int nq, int topk, const QueryCounts *d_counts,
-                             const int32_t *d_res_user, const int32_t *d_res_rank, const float *d_res_qip, int64_t n_cand,
-                             int32_t *d_cand_user, int32_t *d_cand_query, int32_t *d_cand_lb, int32_t *d_cand_ub,
-                             const float *d_cand_qip, const int64_t *d_cand_off, rkr_user_rank *d_out,
-                             rkr_query_stats *d_stats, cudaStream_t st) {
+int refine_and_assemble_pairs(rkr_index *ix, int method, const float *d_query, int nq, int topk,
+                              const QueryCounts *d_counts, const int32_t *d_res_user, const int32_t *d_res_rank,
+                              const float *d_res_qip, int64_t n_cand, int32_t *d_cand_user, int32_t *d_cand_query,
+                              int32_t *d_cand_lb, int32_t *d_cand_ub, const float *d_cand_qip,
+                              const int64_t *d_cand_off, rkr_user_rank *d_out, rkr_query_stats *d_stats,
+                              cudaStream_t st) {
     std::vector<QueryCounts> unused;
-    return refine_and_assemble(ix, RKR_METHOD_QSRP_NORMAL_LP, d_query, nq, topk, d_counts, unused, d_res_user, d_res_rank,
-                               d_res_qip, n_cand, d_cand_user, d_cand_query, d_cand_lb, d_cand_ub, d_cand_qip, d_cand_off,
-                               d_out, d_stats, st);
+    return refine_and_assemble(ix, method, d_query, nq, topk, d_counts, unused, d_res_user, d_res_rank, d_res_qip, n_cand,
+                               d_cand_user, d_cand_query, d_cand_lb, d_cand_ub, d_cand_qip, d_cand_off, d_out, d_stats,
+                               st);
 }
 
 int query_batch(rkr_index *ix, int method, const float *d_query, int n_query, int topk, rkr_user_rank *d_out,
                 rkr_query_stats *d_stats, cudaStream_t st) {
-    // Chunk so the per-pair bucket array stays within a bounded slice of device memory.
-    const int64_t budget = int64_t(6) << 30;
-    int64_t per_q = ix->n_user * 4 + 4096;
+    // Chunk so the per-pair arrays (levels, scores, codes: 9 bytes a pair) stay within a bounded
+    // slice of device memory.
+    const int64_t budget = int64_t(16) << 30;
+    const int64_t per_q = ix->n_user * 9 + 4096;
     int chunk = (int) std::max<int64_t>(1, std::min<int64_t>(n_query, budget / per_q));
     chunk = std::min(chunk, 4096);
     for (int q0 = 0; q0 < n_query; q0 += chunk) {
@@ -732,11 +461,7 @@ int query_batch(rkr_index *ix, int method, const float *d_query, int n_query, in
         const float *dq = d_query + (int64_t) q0 * ix->dim;
         rkr_user_rank *dout = d_out + (int64_t) q0 * topk;
         rkr_query_stats *dst = d_stats ? d_stats + q0 : nullptr;
-        if (method == RKR_METHOD_QSRP_NORMAL_LP) {
-            RKR_TRY(qsrp_chunk(ix, dq, nq, topk, dout, dst, st));
-        } else {
-            RKR_TRY(qs_chunk(ix, method, dq, nq, topk, dout, dst, st));
-        }
+        RKR_TRY(pair_chunk(ix, method, dq, nq, topk, dout, dst, st));
     }
     return RKR_OK;
 }

@@ -188,6 +188,12 @@ def kernel_model(name, cfg, nq, stats):
     return 0.0, 0.0
 
 
+# DRAM bytes (read + write) per (query, user) pair of the dominant kernels, from one ncu capture at a
+# 200-query batch of the same workload (profiles/qsrp_query_kernels_batch200_full.md); traffic grows
+# with the pairs a launch processes, so a launch's traffic is this figure times its pairs.
+NCU_BYTES_PER_PAIR = {"qsrp_scores": (367.812096e6 + 819.383040e6) / (200 * 480189.0)}
+
+
 class ReferenceTimer:
     """The reference's QSRPNormalLP::Retrieval (oracle/_ref) held open on the same index; each run
     times a bounded sample of queries with all host threads."""
@@ -364,7 +370,9 @@ def main():
     roofline = {"kernel": dom_name, "bound": "hbm", "achieved": nbytes / avg_s / 1e9, "peak": hbm_peak,
                 "unit": "GB/s", "frac": (nbytes / avg_s / 1e9) / hbm_peak,
                 "peak_source": "MEASURED_PEAKS.json" if peaks else "fallback",
-                "traffic": None, "avg_launch_ms": avg_s * 1e3,
+                "traffic": (NCU_BYTES_PER_PAIR[dom_name] * CONFIGS[args.config][0] * batch
+                            if dom_name in NCU_BYTES_PER_PAIR and args.config == "config2" else None),
+                "avg_launch_ms": avg_s * 1e3,
                 "share_of_step": dom_ms / max(sum(v[0] for v in prof.values()), 1e-9),
                 "simt_fp32": {"achieved_tops": ops / avg_s / 1e12, "peak_tops_nominal": simt_peak_tops,
                               "frac": (ops / avg_s / 1e12) / simt_peak_tops},

@@ -397,7 +397,7 @@ def main():
     # ---- end to end through the host API -----------------------------------------------------------------
     pinned = [torch.from_numpy(draw_batch()).pin_memory() for _ in range(args.steps)]
     for s in range(min(2, args.warmup)):
-        ix.retrieval(args.method, pinned[s].numpy(), topk)
+        ix.retrieval(args.method, pinned[s % len(pinned)].numpy(), topk)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()

@@ -126,8 +126,11 @@ int rkr_retrieval_device(rkr_index *index, int32_t method, const float *d_query,
  * the launch count since the previous complete read (a read with max_kernels >= *n_kernels clears
  * them; a smaller one only reports the count); names is [max_kernels][64] chars.  Entries whose
  * name ends in "_pairs" are counters rather than kernels (time 0, `launches` holds the count):
- * screen_undecided_pairs counts the QSRPNormalLP (query, user) pairs whose regression bound the
- * fast binary32 screen left to the reference's own float/double arithmetic.
+ * screen_undecided_pairs counts the (query, user) pairs whose regression levels or threshold group
+ * the screens (tensor-core scores with an error bound, the fast binary32 CDF) left to the
+ * reference's own arithmetic; rescored_pairs the pairs whose score a later pass recomputed (a fine
+ * threshold bucket within the bound, a reported or carried score); refine_exact_pairs the
+ * refinement's (candidate, item) tests the tensor-core bound left undecided.
  * (The reference's counterpart is its TimeRecord per stage, src/include/util/TimeMemory.hpp:7-24.) */
 int rkr_profile_enable(rkr_index *index, int32_t on);
 int rkr_profile_read(rkr_index *index, int32_t max_kernels, char *names, double *total_ms, int64_t *launches,

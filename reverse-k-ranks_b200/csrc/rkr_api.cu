@@ -134,6 +134,8 @@ int rkr_index_create(int32_t device, const float *user, int64_t n_user, const fl
     ix->device = device;
     // RKR_REFINE_TC=0 keeps refinement on the exact tiles (both paths give the same results)
     if (const char *v = getenv("RKR_REFINE_TC")) ix->refine_tc_on = strcmp(v, "0") != 0;
+    // RKR_SCORES_TC=0 keeps the bound rounds' pair scores on the exact tiles (same results)
+    if (const char *v = getenv("RKR_SCORES_TC")) ix->scores_tc_on = strcmp(v, "0") != 0;
     ix->n_user = n_user;
     ix->n_item = n_item;
     ix->dim = dim;
@@ -222,7 +224,8 @@ int rkr_index_destroy(rkr_index *ix) {
                       &ix->svd_unorm, &ix->qip_state, &ix->ws_query, &ix->ws_qtr, &ix->ws_qnorm, &ix->ws_bucket,
                       &ix->ws_bucket2, &ix->ws_levels, &ix->ws_cls, &ix->ws_counts, &ix->ws_hist, &ix->ws_res,
                       &ix->ws_cand, &ix->ws_cand_off, &ix->ws_refine, &ix->ws_rank, &ix->ws_out, &ix->ws_stats,
-                      &ix->ws_misc, &ix->ws_fix})
+                      &ix->ws_misc, &ix->ws_fix, &ix->ws_sc, &ix->sc_user_split, &ix->sc_umeta_split,
+                      &ix->sc_user_full, &ix->sc_umeta_full, &ix->sc_cdf_tab})
         b->release();
     ix->prof.release();
     if (ix->stream) cudaStreamDestroy(ix->stream);
@@ -310,6 +313,7 @@ int rkr_index_load_svd(rkr_index *ix, int32_t check_dim, const float *transfer_i
     RKR_TRY(to_kmajor(ix->svd_user.as<float>(), nullptr, ix->n_user, (int) d, ix->svd_user_km.as<float>(), ix->stream));
     ix->has_svd = true;
     ix->check_dim = check_dim;
+    ix->sc_key_split = -2;  // the SVD users changed: rebuild their digit tiles on next use
     return refine_prepare_norms(ix);
 }
 
@@ -327,7 +331,8 @@ int rkr_index_size_bytes(const rkr_index *ix, uint64_t *bytes) {
     for (const DevBuf *b : {&ix->user, &ix->item, &ix->item_sorted, &ix->item_norm, &ix->item_rnorm, &ix->user_rnorm,
                             &ix->sample_rank, &ix->thr, &ix->thr_summ, &ix->reg_rank, &ix->reg, &ix->transfer_item, &ix->svd_user,
                             &ix->svd_user_km, &ix->user_km, &ix->item_km, &ix->item_sorted_km, &ix->svd_unorm,
-                            &ix->qip_state})
+                            &ix->qip_state, &ix->sc_user_split, &ix->sc_umeta_split, &ix->sc_user_full,
+                            &ix->sc_umeta_full})
         s += b->bytes;
     *bytes = s;
     return RKR_OK;

@@ -476,7 +476,18 @@ inline cudaError_t launch_big(const float *A, const int32_t *a_idx, int64_t n_a,
 // Sequential binary32 dot product of one pair (thread-serial), same arithmetic as exact_tile.
 __device__ __forceinline__ float exact_dot(const float *__restrict__ a, const float *__restrict__ b, int n) {
     float acc = 0.0f;
-    for (int j = 0; j < n; j++) acc = __fadd_rn(acc, __fmul_rn(__ldg(a + j), __ldg(b + j)));
+    int j = 0;
+    for (; j + 8 <= n; j += 8) {  // loads of eight coordinates ahead of their (ordered) sum
+        float x[8], y[8];
+#pragma unroll
+        for (int t = 0; t < 8; t++) {
+            x[t] = __ldg(a + j + t);
+            y[t] = __ldg(b + j + t);
+        }
+#pragma unroll
+        for (int t = 0; t < 8; t++) acc = __fadd_rn(acc, __fmul_rn(x[t], y[t]));
+    }
+    for (; j < n; j++) acc = __fadd_rn(acc, __fmul_rn(__ldg(a + j), __ldg(b + j)));
     return acc;
 }
 
@@ -847,6 +858,10 @@ struct rkr_index {
     bool refine_tc_on = true;                 // refinement counts on the tensor cores where the shape fits
     rkr::DevBuf item_tc, item_tc_norm;        // item_sorted, split at check_dim, TF32-rounded; norms of both parts
     rkr::DevBuf item_tc_us, item_tc_us_norm;  // item (original order), unsplit
+    // tensor-core pair scores: user digit tiles for the SVD split at check_dim (QSRP) and unsplit (QS, US)
+    bool scores_tc_on = true;
+    int sc_key_split = -2, sc_key_full = -2;  // the split the tiles were built for (-2: none)
+    rkr::DevBuf sc_user_split, sc_umeta_split, sc_user_full, sc_umeta_full, sc_cdf_tab;
     std::vector<float> h_item_norm_sorted;
     std::vector<int32_t> h_item_order;
     // SampleSearch
@@ -869,7 +884,7 @@ struct rkr_index {
     rkr::DevBuf qip_state;     // [n_user], QSRPNormalLP's carried query scores
     // per-call workspace
     rkr::DevBuf ws_query, ws_qtr, ws_qnorm, ws_bucket, ws_bucket2, ws_levels, ws_cls, ws_counts, ws_hist;
-    rkr::DevBuf ws_res, ws_cand, ws_cand_off, ws_refine, ws_rank, ws_out, ws_stats, ws_misc, ws_fix, ws_km, ws_tc;
+    rkr::DevBuf ws_res, ws_cand, ws_cand_off, ws_refine, ws_rank, ws_out, ws_stats, ws_misc, ws_fix, ws_km, ws_tc, ws_sc;
     std::vector<uint8_t> h_scratch;
     rkr::Profiler prof;
 };

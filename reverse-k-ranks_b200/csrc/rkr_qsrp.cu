@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "rkr_internal.cuh"
+#include "rkr_regression.cuh"
 
 namespace rkr {
 
@@ -35,143 +36,6 @@ int refine_and_assemble_pairs(rkr_index *ix, int method, const float *d_query, i
                               int32_t *d_cand_lb, int32_t *d_cand_ub, const float *d_cand_qip,
                               const int64_t *d_cand_off, rkr_user_rank *d_out, rkr_query_stats *d_stats,
                               cudaStream_t st);
-
-// ---- the regression model's arithmetic (NormalLinearRegressionLP.hpp) ------------------------------
-
-// float -> int64 as x86-64 converts it (cvttss2si): NaN and out-of-range values give INT64_MIN.
-__device__ __forceinline__ int64_t f2i64_x86(float v) {
-    if (!(v >= -9.2233720368547758e18f && v < 9.2233720368547758e18f)) return INT64_MIN;
-    return (int64_t) v;
-}
-
-// NormalLinearRegressionLP::CDFPhi (:123-143).  Float constants; t and the closing expression pass
-// through double; exp is the double ::exp (the query and regression apps never bring the float
-// overload into scope).  sqrt_2_ is ReverseMIPS::sqrt(2.0) (MathUtil.hpp:10-27), which equals
-// the binary32 nearest to sqrt(2).
-__device__ __forceinline__ float cdf_phi(float x) {
-    const float a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f;
-    const float a4 = -1.453152027f, a5 = 1.061405429f, p = 0.3275911f;
-    const float sqrt_2 = __int_as_float(0x3fb504f3);
-    const int sign = x < 0 ? -1 : 1;
-    x = __fdiv_rn(fabsf(x), sqrt_2);
-    const float t = __double2float_rn(__ddiv_rn(1.0, __dadd_rn(1.0, (double) __fmul_rn(p, x))));
-    float poly = __fadd_rn(__fmul_rn(a5, t), a4);
-    poly = __fmul_rn(poly, t);
-    poly = __fadd_rn(poly, a3);
-    poly = __fadd_rn(__fmul_rn(poly, t), a2);
-    poly = __fadd_rn(__fmul_rn(poly, t), a1);
-    const float pt = __fmul_rn(poly, t);
-    const double e = exp((double) __fmul_rn(-x, x));
-    const float y = __double2float_rn(__dsub_rn(1.0, __dmul_rn((double) pt, e)));
-    return __double2float_rn(__dmul_rn(0.5, __dadd_rn(1.0, (double) __fmul_rn((float) sign, y))));
-}
-
-// The same formula in binary32 with the hardware reciprocal and exponential, for screening.
-// Against cdf_phi, with z given as (q - mu) * (1 / sigma) instead of (q - mu) / sigma, it differs
-// by less than kCdfFastErr: the argument and x differ by a few ulps (< 1e-7 after the slope of
-// the CDF), t by a few ulps (< 4e-7 on pt * e), the fused polynomial and the approximate exp by a
-// few ulps more (< 3e-7), and the closing steps by one rounding each.
-constexpr float kCdfFastErr = 2.0e-6f;
-
-__device__ __forceinline__ float cdf_phi_fast(float z) {
-    const float a1 = 0.254829592f, a2 = -0.284496736f, a3 = 1.421413741f;
-    const float a4 = -1.453152027f, a5 = 1.061405429f, p = 0.3275911f;
-    const float x = fabsf(z) * 0.70710677f;
-    const float t = __fdividef(1.0f, fmaf(p, x, 1.0f));
-    const float pt = fmaf(fmaf(fmaf(fmaf(a5, t, a4), t, a3), t, a2), t, a1) * t;
-    const float y = fmaf(-pt, __expf(-x * x), 1.0f);
-    return fmaf(z < 0.0f ? -0.5f : 0.5f, y, 0.5f);
-}
-
-struct RegModel {           // device view of the regression index
-    const float *rec;       // [n_user][8]
-    const int32_t *rank;    // [S]
-    int S;
-    double err_cap;         // S - 1e-3
-    int n_item;
-};
-
-// The reference's float/double evaluation of one side of ComputeRankBound's index arithmetic:
-// pr = ceil(pred + err) (upper = 0) or floor(pred - err) (upper = 1), pred = cdf(nx) * a + b.
-__device__ __forceinline__ int64_t regression_index_exact(float nx, float a, float b, float err, bool upper) {
-    const float ix = cdf_phi(nx);
-    const float pred = __fadd_rn(__fmul_rn(ix, a), b);
-    return upper ? f2i64_x86(floorf(__fsub_rn(pred, err))) : f2i64_x86(ceilf(__fadd_rn(pred, err)));
-}
-
-// ComputeRankBound (:326-380) with the reference's arithmetic, returning levels: 0 -> rank 0,
-// j + 1 -> rank[j], S + 1 -> n_item.
-__device__ __noinline__ void regression_levels_exact(const RegModel &m, int64_t u, float qlb, float qub, int &lvl_lb,
-                                                     int &lvl_ub) {
-    const float4 r0 = __ldg(reinterpret_cast<const float4 *>(m.rec + u * 8));
-    const float4 r1 = __ldg(reinterpret_cast<const float4 *>(m.rec + u * 8 + 4));
-    const float a = r0.x, b = r0.y, mu = r0.z, sigma = r0.w, err = r1.x, smax = r1.y, smin = r1.z;
-    const int S = m.S;
-    if (qlb > smax) lvl_lb = 1;
-    else if (qlb < smin) lvl_lb = S + 1;
-    else if ((double) err >= m.err_cap) lvl_lb = S + 1;
-    else {
-        const int64_t pr = regression_index_exact(__fdiv_rn(__fsub_rn(qlb, mu), sigma), a, b, err, false);
-        lvl_lb = pr >= S ? S + 1 : (pr < 0 ? 1 : (int) pr + 1);
-    }
-    if (qub > smax) lvl_ub = 0;
-    else if (qub < smin) lvl_ub = S;
-    else if ((double) err >= m.err_cap) lvl_ub = 0;
-    else {
-        const int64_t pr = regression_index_exact(__fdiv_rn(__fsub_rn(qub, mu), sigma), a, b, err, true);
-        lvl_ub = pr >= S ? S + 1 : (pr < 0 ? 0 : (int) pr + 1);
-    }
-}
-
-// One user's model prepared for the screen.  A user whose fit error reaches the cap (the
-// reference then gives up on the model: ComputeRankBound's error test) gets an infinite margin,
-// so every one of its pairs goes to the reference's own arithmetic.
-struct RegUser {
-    float a, b, mu, inv_sigma, err, smax, smin, margin;
-};
-
-__device__ __forceinline__ RegUser reg_user(const RegModel &m, int64_t u) {
-    const float4 r0 = __ldg(reinterpret_cast<const float4 *>(m.rec + u * 8));
-    const float4 r1 = __ldg(reinterpret_cast<const float4 *>(m.rec + u * 8 + 4));
-    RegUser r;
-    r.a = r0.x; r.b = r0.y; r.mu = r0.z; r.inv_sigma = __frcp_rn(r0.w);
-    r.err = r1.x; r.smax = r1.y; r.smin = r1.z;
-    // |pred -+ err| moves by at most |a| * kCdfFastErr through the CDF, plus a few roundings of
-    // values no larger than |a| + |b| + |err| in either evaluation.
-    r.margin = (double) r1.x >= m.err_cap
-                   ? INFINITY
-                   : fabsf(r.a) * kCdfFastErr + (fabsf(r.a) + fabsf(r.b) + fabsf(r.err)) * 4.8e-7f + 1e-6f;
-    return r;
-}
-
-// Level of one side from the integral-valued c = ceil (lower bound) or floor (upper bound) of
-// pred -+ err: c >= S -> S + 1, c < 0 -> low, else c + 1.
-__device__ __forceinline__ int level_of(float c, int S, int low) {
-    return c >= (float) S ? S + 1 : (c < 0.0f ? low : (int) c + 1);
-}
-
-// Screened ComputeRankBound: the fast CDF decides a side whenever pred -+ err lies farther than
-// the margin from an integer, so that the reference's ceil / floor cannot differ (values beyond
-// 1e18, where the reference's int64 conversion saturates, are left undecided too).  Returns false
-// when a side is undecided (its level is then not meaningful).
-__device__ __forceinline__ bool regression_levels_fast(const RegUser &r, int S, float qlb, float qub, int &lvl_lb,
-                                                       int &lvl_ub) {
-    const float vl = fmaf(cdf_phi_fast(__fsub_rn(qlb, r.mu) * r.inv_sigma), r.a, r.b) + r.err;
-    const float vu = fmaf(cdf_phi_fast(__fsub_rn(qub, r.mu) * r.inv_sigma), r.a, r.b) - r.err;
-    const bool in_l = !(qlb > r.smax) && !(qlb < r.smin);
-    const bool in_u = !(qub > r.smax) && !(qub < r.smin);
-    // |v| < 1e18 (the reference's int64 conversion is exact there) folds into the margin test
-    const bool ok_l = fabsf(vl - rintf(vl)) > r.margin && fabsf(vl) < 1e18f;
-    const bool ok_u = fabsf(vu - rintf(vu)) > r.margin && fabsf(vu) < 1e18f;
-    lvl_lb = qlb > r.smax ? 1 : (in_l ? level_of(ceilf(vl), S, 1) : S + 1);
-    lvl_ub = qub > r.smax ? 0 : (in_u ? level_of(floorf(vu), S, 0) : S);
-    // a capped-error user's margin is infinite: its in-range sides are always left undecided
-    return (!in_l || ok_l) && (!in_u || ok_u) && r.margin < INFINITY;
-}
-
-__device__ __forceinline__ int level_rank(int lvl, const int32_t *rank, int S, int n_item) {
-    return lvl == 0 ? 0 : (lvl > S ? n_item : rank[lvl - 1]);
-}
 
 // ---- per-query state ---------------------------------------------------------------------------------
 
@@ -231,10 +95,97 @@ struct ScoreSrc {
 
 // The batch's full scores as the tile kernel stored them ([query][user]).
 struct QipView {
-    const float *qip;
+    float *qip;
     int64_t n_user;
-    __device__ float operator()(int64_t u, int64_t q) const { return __ldg(qip + q * n_user + u); }
+    // the reference's score of a pair: a sum over [0, c) and one over [c, dim), added once (c == dim:
+    // one sum); the user rows are SVD-space for QSRP
+    const float *urow, *qrow;
+    int dim, c;
+    PairScreen scr;  // scr.umeta null: the stored scores are the reference's
+    // stored values are read through L2: passes write recomputed scores back
+    __device__ float stored(int64_t u, int64_t q) const { return __ldcg(qip + q * n_user + u); }
+    __device__ bool is_exact(int64_t u, int64_t q) const {
+        if (!scr.umeta) return true;
+        const int64_t words = (n_user + 31) >> 5;
+        return (__ldcg(scr.xbits + q * words + (u >> 5)) >> (u & 31)) & 1u;
+    }
+    // The reference's score; a recomputed one is stored back and marked, so that later passes
+    // over the same pair read it.
+    __device__ float exact(int64_t u, int64_t q) const {
+        const int64_t o = q * n_user + u;
+        if (is_exact(u, q)) return __ldcg(qip + o);
+        const float *ur = urow + u * dim, *qr = qrow + q * dim;
+        const float left = exact_dot(ur, qr, c);
+        const float v = c < dim ? __fadd_rn(left, exact_dot(ur + c, qr + c, dim - c)) : left;
+        qip[o] = v;
+        __threadfence();
+        atomicOr(scr.xbits + q * ((n_user + 31) >> 5) + (u >> 5), 1u << (u & 31));
+        if (scr.n_exact) atomicAdd(scr.n_exact, 1);
+        return v;
+    }
+    // distance bound between a stored score s and the reference's
+    __device__ float delta(int64_t u, int64_t q, float s) const {
+        const float4 um = __ldg(scr.umeta + u), qm = __ldg(scr.qmeta + q);
+        const float ee = um.x * qm.x;
+        const float d = fmaf(scr.cl * um.y, qm.y, ee * scr.kl) + fmaf(scr.cr * um.z, qm.z, ee * scr.kr);
+        return fmaf(fabsf(s), 2.4e-7f, d * 1.0001f);
+    }
 };
+
+// The bucket of s inside coarse group g (< nb): g * gs + the group's thresholds >= s.
+__device__ __forceinline__ int fine_bucket(const float *__restrict__ row, int S, int gs, int g, float s) {
+    const int base = g * gs, end = min(base + gs, S);
+    int c = 0;
+    if ((gs & 15) == 0 && end - base == gs && (S & 3) == 0) {
+        const float4 *p = reinterpret_cast<const float4 *>(row + base);
+        for (int t = 0; t < gs / 16; t++, p += 4) {
+            const float4 x0 = __ldg(p), x1 = __ldg(p + 1), x2 = __ldg(p + 2), x3 = __ldg(p + 3);
+            c += (x0.x >= s) + (x0.y >= s) + (x0.z >= s) + (x0.w >= s) + (x1.x >= s) + (x1.y >= s) + (x1.z >= s) +
+                 (x1.w >= s) + (x2.x >= s) + (x2.y >= s) + (x2.z >= s) + (x2.w >= s) + (x3.x >= s) + (x3.y >= s) +
+                 (x3.z >= s) + (x3.w >= s);
+        }
+    } else {
+        for (int i = base; i < end; i++) c += __ldg(row + i) >= s;
+    }
+    return base + c;
+}
+
+// Thresholds of group g (< nb) >= hi and >= lo, in one pass.
+__device__ __forceinline__ void fine_bucket2(const float *__restrict__ row, int S, int gs, int g, float hi, float lo,
+                                             int &b_hi, int &b_lo) {
+    const int base = g * gs, end = min(base + gs, S);
+    int ch = 0, cl = 0;
+    if ((gs & 3) == 0 && end - base == gs && (S & 3) == 0) {
+        const float4 *p = reinterpret_cast<const float4 *>(row + base);
+        for (int t = 0; t < gs / 4; t++) {
+            const float4 x = __ldg(p + t);
+            ch += (x.x >= hi) + (x.y >= hi) + (x.z >= hi) + (x.w >= hi);
+            cl += (x.x >= lo) + (x.y >= lo) + (x.z >= lo) + (x.w >= lo);
+        }
+    } else {
+        for (int i = base; i < end; i++) {
+            const float x = __ldg(row + i);
+            ch += x >= hi;
+            cl += x >= lo;
+        }
+    }
+    b_hi = base + ch;
+    b_lo = base + cl;
+}
+
+// The bucket (inside its coarse group g) of a pair's reference score: from the stored score when it
+// is exact or no threshold lies within its bound, else from the recomputed score.
+__device__ __forceinline__ int pair_bucket(const QipView &sc, const float *__restrict__ thr, int S, int gs, int g,
+                                           int64_t u, int64_t q) {
+    const float *row = thr + u * S;
+    if (sc.is_exact(u, q)) return fine_bucket(row, S, gs, g, sc.stored(u, q));  // the bit first, then the value
+    const float s = sc.stored(u, q);
+    const float d = sc.delta(u, q, s);
+    int b_hi, b_lo;
+    fine_bucket2(row, S, gs, g, s + d, s - d, b_hi, b_lo);
+    if (b_hi == b_lo) return b_hi;
+    return fine_bucket(row, S, gs, g, sc.exact(u, q));
+}
 
 // Pairs the screen left undecided, resolved by qsrp_fix1_kernel: (query, user, partial score).
 // Past the list's capacity the pair's levels are written as kLvUndecided and count keeps growing,
@@ -363,9 +314,8 @@ __global__ void qsrp_fix1_kernel(FixList fix, RegModel m, const float *__restric
         const int4 e = fix.e[i];
         const float left = __int_as_float(e.z);
         const float right = __fmul_rn(__ldg(unorm + e.y), __ldg(qnorm + e.x));
-        int l, h;
-        regression_levels_exact(m, e.y, __fsub_rn(left, right), __fadd_rn(left, right), l, h);
-        lv[(int64_t) e.x * n_user + e.y] = (uint32_t) l | ((uint32_t) h << 16);
+        lv[(int64_t) e.x * n_user + e.y] =
+            regression_levels_exact(m.rec, m.S, m.err_cap, e.y, __fsub_rn(left, right), __fadd_rn(left, right));
     }
 }
 
@@ -381,9 +331,7 @@ __global__ void qsrp_fix1_scan_kernel(const int *__restrict__ count, int cap, Re
         const int64_t q = i / n_user, u = i % n_user;
         const float left = sc.left(u, q);
         const float right = __fmul_rn(__ldg(unorm + u), __ldg(qnorm + q));
-        int l, h;
-        regression_levels_exact(m, u, __fsub_rn(left, right), __fadd_rn(left, right), l, h);
-        lv[i] = (uint32_t) l | ((uint32_t) h << 16);
+        lv[i] = regression_levels_exact(m.rec, m.S, m.err_cap, u, __fsub_rn(left, right), __fadd_rn(left, right));
     }
 }
 
@@ -564,24 +512,6 @@ __global__ void qs_params_kernel(QsrpParams *__restrict__ par, int nq, int64_t n
 
 // ---- round 2 -------------------------------------------------------------------------------------
 
-// The bucket of s inside coarse group g (< nb): g * gs + the group's thresholds >= s.
-__device__ __forceinline__ int fine_bucket(const float *__restrict__ row, int S, int gs, int g, float s) {
-    const int base = g * gs, end = min(base + gs, S);
-    int c = 0;
-    if ((gs & 15) == 0 && end - base == gs && (S & 3) == 0) {
-        const float4 *p = reinterpret_cast<const float4 *>(row + base);
-        for (int t = 0; t < gs / 16; t++, p += 4) {
-            const float4 x0 = __ldg(p), x1 = __ldg(p + 1), x2 = __ldg(p + 2), x3 = __ldg(p + 3);
-            c += (x0.x >= s) + (x0.y >= s) + (x0.z >= s) + (x0.w >= s) + (x1.x >= s) + (x1.y >= s) + (x1.z >= s) +
-                 (x1.w >= s) + (x2.x >= s) + (x2.y >= s) + (x2.z >= s) + (x2.w >= s) + (x3.x >= s) + (x3.y >= s) +
-                 (x3.z >= s) + (x3.w >= s);
-        }
-    } else {
-        for (int i = base; i < end; i++) c += __ldg(row + i) >= s;
-    }
-    return base + c;
-}
-
 // Round 2 per (user chunk, query): pairs that did not reach round 2 get their round-1 state code in
 // place of the group code; the others are counted by group (per-warp shared-memory copies).
 __global__ void __launch_bounds__(kHistThreads) qsrp_round2_kernel(const uint32_t *__restrict__ lv,
@@ -688,7 +618,7 @@ __device__ __forceinline__ void fine2_hit(const HitList &hl, bool hit, int64_t q
     if (!hit) return;
     const int idx = base + __popc(want & ((1u << lane) - 1));
     if (idx < hl.cap) hl.e[idx] = ((uint64_t) q << 40) | ((uint64_t) u << 8) | c;
-    else atomicAdd(hist_f + q * (S + 1) + fine_bucket(thr + u * S, S, gs, (int) c, sc(u, q)), 1);
+    else atomicAdd(hist_f + q * (S + 1) + pair_bucket(sc, thr, S, gs, (int) c, u, q), 1);
 }
 
 // Scan for the pairs whose coarse group is flagged for their query (mask1, or mask2 when any
@@ -727,7 +657,7 @@ __global__ void __launch_bounds__(256) qsrp_fine2_kernel(const uint8_t *__restri
                 if (pos >= total || c >= 32) continue;
                 const int64_t q = pos / n_user, u = pos % n_user;
                 if ((uint32_t) (second ? par[q].mask2 : par[q].mask1) >> c & 1u)
-                    atomicAdd(hist_f + q * (S + 1) + fine_bucket(thr + u * S, S, gs, (int) c, sc(u, q)), 1);
+                    atomicAdd(hist_f + q * (S + 1) + pair_bucket(sc, thr, S, gs, (int) c, u, q), 1);
             }
             continue;
         }
@@ -787,7 +717,7 @@ __global__ void qsrp_fine2_list_kernel(HitList hl, QipView sc, int64_t n_user, c
         const uint64_t x = hl.e[i];
         const int64_t q = (int64_t) (x >> 40), u = (int64_t) ((x >> 8) & 0xffffffffu);
         const int c = (int) (x & 0xff);
-        atomicAdd(hist_f + q * (S + 1) + fine_bucket(thr + u * S, S, gs, c, sc(u, q)), 1);
+        atomicAdd(hist_f + q * (S + 1) + pair_bucket(sc, thr, S, gs, c, u, q), 1);
     }
 }
 
@@ -969,7 +899,7 @@ struct QsrpCompactPolicy {
             const bool cand_ok = counts[q].n_cand > 0;
             if (kg == kClsRefine && !cand_ok) return 0;
             if (!with_aux && kg != kClsMixed) return kg == kClsResult ? 1 : 2;
-            const int b = c == (unsigned) nb ? S : fine_bucket(thr + u * S, S, gs, (int) c, sc(u, q));
+            const int b = c == (unsigned) nb ? S : pair_bucket(sc, thr, S, gs, (int) c, u, q);
             const uint8_t k2 = cls2[(int64_t) q * (S + 1) + b];
             int lb, ub;
             bucket_bounds(b, S, rank, n_item, lb, ub);
@@ -1019,7 +949,7 @@ __global__ void qsrp_result_fill_kernel(const QueryCounts *__restrict__ counts, 
         int src = res_fresh[i] ? q : -1;
         for (int qq = q - 1; src < 0 && qq >= 0; qq--)
             if (code[(int64_t) qq * n_user + u] < kCodeResult1) src = qq;
-        res_qip[i] = src >= 0 ? sc(u, src) : state[u];
+        res_qip[i] = src >= 0 ? sc.exact(u, src) : state[u];
     }
 }
 
@@ -1027,7 +957,7 @@ __global__ void qsrp_cand_fill_kernel(const int32_t *__restrict__ cand_user, con
                                       int64_t n, QipView sc, float *__restrict__ cand_qip) {
     const int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n) return;
-    cand_qip[e] = sc(cand_user[e], cand_query[e]);
+    cand_qip[e] = sc.exact(cand_user[e], cand_query[e]);
 }
 
 // Carried state after the batch: each user's score at its last round-2 query of the batch.
@@ -1037,7 +967,7 @@ __global__ void qsrp_state_kernel(const uint8_t *__restrict__ code, QipView sc, 
     if (u >= n_user) return;
     for (int q = nq - 1; q >= 0; q--)
         if (code[(int64_t) q * n_user + u] < kCodeResult1) {
-            state[u] = sc(u, q);
+            state[u] = sc.exact(u, q);
             return;
         }
 }
@@ -1117,8 +1047,6 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, int topk
     } else {
         RKR_CUDA(cudaMemsetAsync(qnorm, 0, sizeof(float) * nq, st));
     }
-    RKR_TRY(ix->ws_km.ensure(sizeof(float) * (size_t) dim * (size_t) kmajor_ld(nq)));
-    RKR_TRY(to_kmajor(qsrp ? qtr : d_query, nullptr, nq, dim, ix->ws_km.as<float>(), st));
     ScoreSrc sc;
     sc.svd_user = ix->svd_user.as<float>();
     sc.qtr = qtr;
@@ -1133,6 +1061,10 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, int topk
     QipView qv;
     qv.qip = qip;
     qv.n_user = U;
+    qv.urow = (qsrp ? ix->svd_user : ix->user).as<float>();
+    qv.qrow = qsrp ? qtr : d_query;
+    qv.dim = dim;
+    qv.c = qsrp ? c : dim;
     Round1Epi e1;
     e1.unorm = ix->svd_unorm.as<float>();
     e1.qnorm = qnorm;
@@ -1145,21 +1077,45 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, int topk
     e1.n_user = U;
     e1.n_query = nq;
     e1.fix = fix;
-    cudaError_t ce = cudaSuccess;
-    const KMajor ka = {(qsrp ? ix->svd_user_km : ix->user_km).as<float>(), U, kmajor_ld(U), kmajor_ld(U)};
-    const KMajor kb = {ix->ws_km.as<float>(), nq, kmajor_ld(nq), kmajor_ld(nq)};
-    // QS / US: one sequential sum over all coordinates (QS.hpp:137-143), seen by finish_hi
-    timed(ix, st, "qsrp_scores", [&] { ce = launch_big_split(ka, kb, qsrp ? c : dim, dim, e1, st); });
-    RKR_CUDA(ce);
+    // pair scores, levels and coarse groups: on the tensor cores with exact resolution of undecided
+    // pairs where the shape allows, else on the exact tiles
+    bool tc_done = false;
+    {
+        ScoresTcCall call;
+        call.qsrp = qsrp;
+        call.qrows = qv.qrow;
+        call.qnorm = qnorm;
+        call.unorm = e1.unorm;
+        call.nq = nq;
+        call.m = m;
+        call.nb = nb;
+        call.lv = e1.lv;
+        call.code = code;
+        call.qip = qip;
+        RKR_TRY(scores_tc(ix, call, st, &qv.scr, &tc_done));
+    }
+    if (!tc_done) {
+        qv.scr = PairScreen();
+        RKR_TRY(ix->ws_km.ensure(sizeof(float) * (size_t) dim * (size_t) kmajor_ld(nq)));
+        RKR_TRY(to_kmajor(qsrp ? qtr : d_query, nullptr, nq, dim, ix->ws_km.as<float>(), st));
+        cudaError_t ce = cudaSuccess;
+        const KMajor ka = {(qsrp ? ix->svd_user_km : ix->user_km).as<float>(), U, kmajor_ld(U), kmajor_ld(U)};
+        const KMajor kb = {ix->ws_km.as<float>(), nq, kmajor_ld(nq), kmajor_ld(nq)};
+        // QS / US: one sequential sum over all coordinates (QS.hpp:137-143), seen by finish_hi
+        timed(ix, st, "qsrp_scores", [&] { ce = launch_big_split(ka, kb, qsrp ? c : dim, dim, e1, st); });
+        RKR_CUDA(ce);
+    }
     const int64_t chunk = 16384;
     dim3 hg((unsigned) ((U + chunk - 1) / chunk), (unsigned) nq);
     if (qsrp) {
-    timed(ix, st, "qsrp_fix1", [&] { qsrp_fix1_kernel<<<148 * 4, 256, 0, st>>>(fix, m, e1.unorm, qnorm, U, lv); });
-    RKR_CUDA(cudaGetLastError());
-    timed(ix, st, "qsrp_fix1_scan", [&] {
-        qsrp_fix1_scan_kernel<<<148 * 8, 256, 0, st>>>(fix_count, fix_cap, m, sc, e1.unorm, qnorm, U, nq, lv);
-    });
-    RKR_CUDA(cudaGetLastError());
+    if (!tc_done) {
+        timed(ix, st, "qsrp_fix1", [&] { qsrp_fix1_kernel<<<148 * 4, 256, 0, st>>>(fix, m, e1.unorm, qnorm, U, lv); });
+        RKR_CUDA(cudaGetLastError());
+        timed(ix, st, "qsrp_fix1_scan", [&] {
+            qsrp_fix1_scan_kernel<<<148 * 8, 256, 0, st>>>(fix_count, fix_cap, m, sc, e1.unorm, qnorm, U, nq, lv);
+        });
+        RKR_CUDA(cudaGetLastError());
+    }
     timed(ix, st, "level_hist", [&] {
         level_hist_kernel<<<hg, kHistThreads, hist_copies(2 * nl) * 2 * nl * sizeof(int), st>>>(lv, U, m.rank, Sr, n_item,
                                                                                                chunk, hist_l, anomaly);
@@ -1286,6 +1242,11 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, int topk
     });
     RKR_CUDA(cudaGetLastError());
     RKR_CUDA(cudaStreamSynchronize(st));
+    if (ix->prof.on && qv.scr.n_exact) {
+        int h = 0;
+        RKR_CUDA(cudaMemcpy(&h, qv.scr.n_exact, sizeof(int), cudaMemcpyDeviceToHost));
+        ix->prof.add_count("rescored_pairs", h);
+    }
     return RKR_OK;
 }
 

@@ -1,0 +1,805 @@
+// rkr_scores_tc.cu -- the (query, user) scores of the bound rounds on the tensor cores (tcgen05, int8).
+//
+// The bound rounds only ask, per (query, user) pair, which regression level its partial score falls
+// on (QSRPNormalLP round 1: NormalLinearRegressionLP::ComputeRankBound on the bounds of
+// PartDimPartNorm::IPBound, PartDimPartNorm.hpp:52-74) and which coarse group of sampled thresholds
+// its full score falls in (SampleSearch::RankBound, SampleSearch.hpp:91-156; QS.hpp:137-143 for QS
+// and US).  Both are decided from a tensor-core score with a rigorous bound on its distance to the
+// reference's binary32 score; pairs whose bound interval reaches a decision boundary are recomputed
+// with the reference's own arithmetic inside the same kernel.
+//
+// Scores.  Each row (user or query) is scaled by a power of two 2^e with every |coordinate| < 2^(e-1)
+// and split into four signed 7-bit digits per coordinate, a = 2^e (d1 2^-7 + d2 2^-14 + d3 2^-21 +
+// d4 2^-28 + r), |d| <= 64, |r| <= 2^-29 (each digit is the nearest integer of the remainder times
+// 128, all steps exact in binary32).  The ten digit products with i + j <= 5 run as int8 MMAs
+// (tcgen05.mma kind::i8) into four int32 TMEM accumulators per part (grouped by i + j); integer
+// accumulation is exact.  Per part P of n coordinates the computed value differs from the exact
+// dot product by at most 2^(ea+eb) n (3.02 2^-30 + 2^-29 + 3 2^-24 0.008) (dropped digit products,
+// the remainders, and the three roundings that combine the accumulators), and the reference's
+// sequential binary32 sum differs from the exact one by at most n 2^-24 / (1 - n 2^-24) |a_P| |b_P|.
+//
+// Tiles.  One CTA per 128 users (the MMA's M and the TMEM lanes) holds the users' digits for the
+// whole K extent in shared memory and walks the batch's queries in chunks of 32 (the MMA's N), the
+// query digits double-buffered by bulk copies and the accumulators double-buffered in TMEM (2 x 8
+// accumulators x 32 columns = 512 columns), so that the MMAs of one chunk overlap the epilogue of
+// the previous one.  Warp 16 issues the copies and the MMAs; warps 0-15 read TMEM (warp w: lane
+// quadrant w % 4, columns 8 (w / 4) .. + 8 of each accumulator) and run the epilogue.
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "rkr_internal.cuh"
+#include "rkr_regression.cuh"
+
+namespace rkr {
+
+namespace {
+
+constexpr int kScM = 128;                          // users per CTA
+constexpr int kScN = 32;                           // queries per chunk
+constexpr int kScSlices = 4;                       // digits per coordinate
+constexpr int kScEpiWarps = 16;
+constexpr int kScThreads = 32 * (kScEpiWarps + 1);
+constexpr int kScListCap = 4096;                   // undecided pairs per CTA resolved in the kernel
+constexpr int kScMaxQ = 1024;                      // queries per launch (their data sits in shared memory)
+constexpr int kScMaxKp = 224;                      // padded coordinates (both parts): shared memory
+constexpr int kScMaxPart = 240;                    // coordinates per part: digit sums stay below 2^22
+constexpr int kScSummStride = ThrSummary::kMaxGroups + 1;
+constexpr int kScMaxExp = 40;                      // rows scaled beyond 2^+-40 go to the exact path
+
+__host__ __device__ inline int round32(int x) { return (x + 31) & ~31; }
+
+// ---- operands ----------------------------------------------------------------------------------------
+
+// Rows [n][dim] to the digit layout of the tiles: per tile of tr rows, 4 slices of [kp / 16][tr / 8]
+// [8 rows][16 bytes] (K-major core matrices); coordinates [0, c) at k in [0, c), [c, dim) at
+// [cp, cp + dim - c), zeros elsewhere and in rows [n, n_pad).  meta[r] = {2^e, upper bounds of the
+// norms of the two parts, e (as int bits)}; a row with a non-finite coordinate or a scale beyond
+// 2^+-kScMaxExp gets 2^e = inf, which sends all of its pairs to the exact path.  One warp per row.
+__global__ void slice_rows_kernel(const float *__restrict__ src, int64_t n, int64_t n_pad, int dim, int c, int cp,
+                                  int kp, int tr, int8_t *__restrict__ dst, float4 *__restrict__ meta) {
+    const int64_t r = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= n_pad) return;
+    const float *row = r < n ? src + r * dim : nullptr;
+    float mx = 0.0f;
+    int bad = 0;
+    if (row)
+        for (int k = lane; k < dim; k += 32) {
+            const float v = row[k];
+            bad |= !isfinite(v);
+            mx = fmaxf(mx, fabsf(v));
+        }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+    }
+    int e = 0;
+    if (mx > 0.0f) {
+        int x;
+        frexpf(mx, &x);  // mx = m 2^x, m in [0.5, 1): mx 2^-(x + 1) < 0.5
+        e = x + 1;
+    }
+    if (e > kScMaxExp || e < -kScMaxExp) bad = 1;
+    const float scale = bad ? 0.0f : ldexpf(1.0f, -e);
+    double sl = 0.0, sr = 0.0;
+    const size_t slice_bytes = (size_t) tr * kp;
+    int8_t *tb = dst + (size_t) (r / tr) * kScSlices * slice_bytes;
+    const int rr = (int) (r % tr);
+    for (int p = lane; p < kp; p += 32) {
+        const int k = p < cp ? (p < c ? p : -1) : (p - cp + c < dim ? p - cp + c : -1);
+        float v = 0.0f;
+        if (row && k >= 0) {
+            v = row[k];
+            if (k < c) sl += (double) v * v;
+            else sr += (double) v * v;
+        }
+        float a = v * scale;  // exact: a power of two
+        const size_t off = (size_t) (p >> 4) * (tr * 16) + (rr >> 3) * 128 + (rr & 7) * 16 + (p & 15);
+#pragma unroll
+        for (int s = 0; s < kScSlices; s++) {
+            const float t = a * 128.0f;  // exact
+            const float d = rintf(t);    // |t| < 64
+            a = t - d;                   // exact, |a| <= 0.5
+            tb[s * slice_bytes + off] = (int8_t) (int) d;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        sl += __shfl_xor_sync(0xffffffffu, sl, o);
+        sr += __shfl_xor_sync(0xffffffffu, sr, o);
+    }
+    if (lane == 0) {
+        float4 m;
+        m.x = bad ? INFINITY : ldexpf(1.0f, e);
+        m.y = __double2float_ru(sqrt(sl * (1.0 + 1e-12)));
+        m.z = __double2float_ru(sqrt(sr * (1.0 + 1e-12)));
+        m.w = __int_as_float(bad ? 0 : e);
+        meta[r] = m;
+    }
+}
+
+// ---- tcgen05 / mbarrier helpers ----------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t) __cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *b, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *b, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint64_t *b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok) : "r"(smem_u32(b)), "r"(parity) : "memory");
+    return ok != 0;
+}
+// Bounded wait; gives up early when another thread of the CTA has given up.
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity, volatile int *abort) {
+    for (int it = 0; it < (1 << 22); it++) {
+        if (mbar_try(b, parity)) return true;
+        if (*abort) return false;
+    }
+    return false;
+}
+// Plain (non-multicast) bulk copy global -> this CTA's shared memory, completing on an mbarrier.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// Shared-memory matrix descriptor, K-major without swizzle: 8-row x 16-byte core matrices, lbo the
+// byte distance between the two core matrices of one K step, sbo between groups of 8 rows.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = (uint64_t) ((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t) ((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t) ((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t) 1 << 46;  // descriptor version of sm_100
+    return d;
+}
+
+// Instruction descriptor: kind::i8, A and B signed 8-bit K-major, int32 accumulator, M = 128, N = 32.
+constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) (kScN >> 3) << 17) |
+                              ((uint32_t) (kScM >> 4) << 24);
+
+__device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t"
+        "}\n" ::"r"(d_tmem), "l"(a), "l"(b), "r"(kIdescI8), "r"(accumulate) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t addr, uint32_t (&v)[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "r"(addr));
+}
+
+// int32 of magnitude below 2^22 to binary32, exactly (the value sits in the significand of 1.5 2^23).
+__device__ __forceinline__ float i2f_small(uint32_t x) {
+    return __fsub_rn(__int_as_float((int) x + 0x4B400000), 12582912.0f);
+}
+// 2^35 times the digit-product value of one part: a0 2^21 + a1 2^14 + a2 2^7 + a3.
+__device__ __forceinline__ float combine4(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3) {
+    return fmaf(fmaf(fmaf(i2f_small(a0), 128.0f, i2f_small(a1)), 128.0f, i2f_small(a2)), 128.0f, i2f_small(a3));
+}
+
+// ---- screened regression levels ------------------------------------------------------------------------
+
+// The regression CDF from a table: the reference's formula (Abramowitz & Stegun 7.1.26, as
+// NormalLinearRegressionLP::CDFPhi evaluates it, NormalLinearRegressionLP.hpp:123-143) tabulated in
+// double at z = -8 + i / 128 (2048 cells, values and differences rounded to binary32) and
+// interpolated linearly.  Against the reference's evaluation at the same argument the result is
+// within kCdfTabErr: interpolation h^2 / 8 max|f''| <= 1.9e-6, the table's roundings and the
+// interpolation's own < 3e-7, the reference's roundings < 6e-7, and the argument's few ulps.
+constexpr int kCdfTabCells = 2048;
+constexpr float kCdfTabErr = 4.0e-6f;
+
+// One side of the screen for a bound score q known to within dq of the reference's.  Within a cell
+// the formula's slope stays within a factor 1.1 of the cell's mean slope D * 128 on the cell widened
+// by dq / sigma <= 2^-10 (|z| <= 8; beyond, the slope is below 1e-14), so the CDF moves by at most
+// (D * 141 + 1e-6) dq / sigma, the 1e-6 covering the formula's deviation from the normal density.
+// A user whose fit error reaches the cap takes the reference's capped levels in range
+// (ComputeRankBound's error test).  Returns false when undecided.
+__device__ __forceinline__ bool level_side(const RegUser &r, float margin0, float cu, int S, float q, float dq,
+                                           bool upper, const float2 *__restrict__ tab, int &lvl) {
+    const float z = __fsub_rn(q, r.mu) * r.inv_sigma;
+    const float t = fminf(fmaxf(fmaf(z, 128.0f, 1024.0f), 0.0f), 2047.0f);
+    const float tu = (t - 0.5f) + 12582912.0f;          // nearest integer of t - 0.5, in the significand
+    const int i = __float_as_int(tu) - 0x4B400000;      // in [0, 2047]: floor(t), or floor(t) - 1 near integral t
+    const float f = t - (tu - 12582912.0f);             // in [0, 1] up to 2^-14
+    const float2 e = tab[i];
+    const float base = fmaf(fmaf(f, e.y, e.x), r.a, r.b);
+    const float v = upper ? base - r.err : base + r.err;
+    const float margin = fmaf(cu * dq, fmaf(e.y, 141.0f, 1e-6f), margin0);
+    const bool capped = !(margin0 < INFINITY);
+    const bool above = q - dq > r.smax, below = q + dq < r.smin;
+    const bool inside = q + dq <= r.smax && q - dq >= r.smin;
+    // one rounding instruction: floor; ceil and the distance to the nearest integer follow from it
+    const float fl = floorf(v);
+    const float frac = v - fl;  // exact for |v| < 2^24; larger values stay undecided
+    const float cv = upper ? fl : (frac > 0.0f ? fl + 1.0f : fl);
+    // level of cv (integral): >= S -> S + 1, < 0 -> low, else cv + 1 (cv < 2^22: read off the significand)
+    const int low = upper ? 0 : 1;
+    const int in_range = __float_as_int(cv + 12582912.0f) - 0x4B400000 + 1;
+    const int lv_model = cv >= (float) S ? S + 1 : (cv < 0.0f ? low : in_range);
+    const int in_lvl = capped ? (upper ? 0 : S + 1) : lv_model;
+    if (upper) lvl = above ? 0 : (below ? S : in_lvl);
+    else lvl = above ? 1 : (below ? S + 1 : in_lvl);
+    const bool decided_in = capped || (fminf(frac, 1.0f - frac) > margin && fabsf(v) < 1.6e7f);
+    return (above || below || (inside && decided_in)) && dq * r.inv_sigma <= 9.765625e-4f;
+}
+
+// ---- the tile kernel -----------------------------------------------------------------------------------
+
+struct ScArgs {
+    const int8_t *a_sl, *b_sl;     // user tiles (kScM rows), query chunks (kScN rows)
+    const float4 *umeta, *qmeta;
+    const float *unorm, *qnorm;    // the reference's remaining-coordinate norms (QSRP)
+    const float *urow, *qrow;      // exact rows: [n_user][dim], [nq][dim]
+    const float *thr_summ;
+    RegModel m;
+    uint32_t *lv;                  // nullptr: no regression round (QS, US)
+    const float2 *cdf_tab;         // [kCdfTabCells] (value, difference to the next node)
+    uint8_t *code;
+    float *qip;
+    uint32_t *xbits;               // [query][(n_user + 31) / 32]: pairs whose stored score is the reference's
+    int2 *ovf;                     // undecided pairs past a CTA's list: (query, user)
+    int *ovf_count, *status, *undecided;
+    int ovf_cap;
+    int q_base;                    // the launch's first query in the batch (overflow entries hold batch queries)
+    int64_t n_user;
+    int nq, dim, c, kp, ksplit, ksteps, two_parts, nb;
+    float cl, kl, cr, kr;          // bound coefficients of the two parts
+};
+
+// The reference's scores and decisions for one pair: levels, group code and score stored.
+// exact_dot with the first operand in shared or global memory (generic loads; __ldg would not
+// accept a shared-memory address).
+__device__ __forceinline__ float exact_dot_any(const float *a, const float *__restrict__ b, int n) {
+    float acc = 0.0f;
+    int j = 0;
+    for (; j + 32 <= n; j += 32) {  // 32 loads of the global operand ahead of their (ordered) sum
+        float y[32];
+#pragma unroll
+        for (int t = 0; t < 32; t++) y[t] = __ldg(b + j + t);
+#pragma unroll
+        for (int t = 0; t < 32; t++) acc = __fadd_rn(acc, __fmul_rn(a[j + t], y[t]));
+    }
+    for (; j + 8 <= n; j += 8) {
+        float y[8];
+#pragma unroll
+        for (int t = 0; t < 8; t++) y[t] = __ldg(b + j + t);
+#pragma unroll
+        for (int t = 0; t < 8; t++) acc = __fadd_rn(acc, __fmul_rn(a[j + t], y[t]));
+    }
+    for (; j < n; j++) acc = __fadd_rn(acc, __fmul_rn(a[j], __ldg(b + j)));
+    return acc;
+}
+
+// ur: the user's row (shared or global memory); the query's row is read from global memory.
+__device__ __forceinline__ void exact_pair(const ScArgs &a, int64_t u, int q, const float *summ, const float *ur) {
+    const float *qr = a.qrow + (int64_t) q * a.dim;
+    const float left = exact_dot_any(ur, qr, a.c);
+    float full = left;
+    const int64_t o = (int64_t) q * a.n_user + u;
+    if (a.lv) {
+        const float right = __fmul_rn(a.unorm[u], a.qnorm[q]);
+        a.lv[o] = regression_levels_exact(a.m.rec, a.m.S, a.m.err_cap, u, __fsub_rn(left, right),
+                                          __fadd_rn(left, right));
+    }
+    if (a.c < a.dim) full = __fadd_rn(left, exact_dot_any(ur + a.c, qr + a.c, a.dim - a.c));
+    int g = 0;
+    for (int j = 0; j < ThrSummary::kMaxGroups; j++) g += summ[j] >= full;
+    a.code[o] = (uint8_t) min(g, a.nb);
+    a.qip[o] = full;
+    atomicOr(a.xbits + (int64_t) q * ((a.n_user + 31) >> 5) + (u >> 5), 1u << (u & 31));
+}
+
+__global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
+    extern __shared__ __align__(1024) uint8_t sm_raw[];
+    __shared__ uint64_t bar_a, bar_b[2], bar_mma[2], bar_free[2];
+    __shared__ uint32_t tslot;
+    __shared__ int list_n, abort_flag;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t u0 = (int64_t) blockIdx.x * kScM;
+    const int kp = a.kp, nq = a.nq;
+    const int nchunks = (nq + kScN - 1) / kScN;
+    const uint32_t a_bytes = (uint32_t) (kScSlices * kScM * kp), b_bytes = (uint32_t) (kScSlices * kScN * kp);
+    uint8_t *sA = sm_raw;
+    uint8_t *sB = sA + a_bytes;
+    float *summ = reinterpret_cast<float *>(sB + 2 * b_bytes);
+    uint32_t *list = reinterpret_cast<uint32_t *>(summ + kScM * kScSummStride);
+    float2 *tab = reinterpret_cast<float2 *>(list + kScListCap);
+    float4 *sq = reinterpret_cast<float4 *>(tab + kCdfTabCells);  // the batch's query data
+    float *sqn = reinterpret_cast<float *>(sq + kScMaxQ);
+    volatile int *abort = &abort_flag;
+
+    if (tid == 0) {
+        mbar_init(&bar_a, 1);
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&bar_b[b], 1);
+            mbar_init(&bar_mma[b], 1);
+            mbar_init(&bar_free[b], kScEpiWarps);
+        }
+        list_n = 0;
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&tslot))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    for (int idx = tid; idx < kScM * ThrSummary::kMaxGroups; idx += kScThreads) {
+        const int rr = idx / ThrSummary::kMaxGroups, j = idx % ThrSummary::kMaxGroups;
+        summ[rr * kScSummStride + j] =
+            u0 + rr < a.n_user ? __ldg(a.thr_summ + (u0 + rr) * ThrSummary::kMaxGroups + j) : -INFINITY;
+    }
+    if (a.lv)
+        for (int i = tid; i < kCdfTabCells; i += kScThreads) tab[i] = __ldg(a.cdf_tab + i);
+    for (int i = tid; i < nq; i += kScThreads) {
+        sq[i] = __ldg(a.qmeta + i);
+        sqn[i] = a.lv ? __ldg(a.qnorm + i) : 0.0f;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t taddr = tslot;
+    const int nacc = a.two_parts ? 8 : 4;
+    const uint32_t buf_cols = (uint32_t) (nacc * kScN);
+
+    if (warp == kScEpiWarps) {
+        // ---- copies and MMAs (one thread) ----
+        if (lane == 0) {
+            bool ok = true;
+            int last = -1;  // last chunk whose MMAs were committed
+            mbar_expect_tx(&bar_a, a_bytes);
+            bulk_g2s(sA, a.a_sl + (size_t) blockIdx.x * a_bytes, a_bytes, &bar_a);
+            for (int j = 0; j < 2 && j < nchunks; j++) {
+                mbar_expect_tx(&bar_b[j], b_bytes);
+                bulk_g2s(sB + (size_t) j * b_bytes, a.b_sl + (size_t) j * b_bytes, b_bytes, &bar_b[j]);
+            }
+            ok = mbar_wait(&bar_a, 0, abort);
+            constexpr uint32_t kAChunk = kScM * 16, kBChunk = kScN * 16;  // bytes per 16-coordinate block
+            // descriptors: a base per operand buffer, slices and K steps as offsets of the start address
+            // (16-byte units, within the descriptor's 14-bit field: shared memory stays below 256 KB)
+            const uint64_t da0 = umma_desc(smem_u32(sA), kAChunk, 128);
+            const uint64_t db_0 = umma_desc(smem_u32(sB), kBChunk, 128);
+            const uint64_t db_1 = umma_desc(smem_u32(sB + b_bytes), kBChunk, 128);
+            const uint32_t a_slice = (uint32_t) (kScM * kp) >> 4, b_slice = (uint32_t) (kScN * kp) >> 4;
+            for (int j = 0; ok && j < nchunks; j++) {
+                const int b = j & 1;
+                const uint32_t ph = (uint32_t) (j >> 1) & 1u;
+                ok = mbar_wait(&bar_b[b], ph, abort);
+                if (ok && j >= 2) ok = mbar_wait(&bar_free[b], (uint32_t) ((j - 2) >> 1) & 1u, abort);
+                if (!ok) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t d0 = taddr + (uint32_t) b * buf_cols;
+                for (int s = 0; s < a.ksteps; s++) {
+                    const int part = s < a.ksplit ? 0 : 1;
+                    const bool first_s = s == 0 || s == a.ksplit;
+                    const uint64_t das = da0 + ((uint32_t) s * 2 * kAChunk >> 4);
+                    const uint64_t dbs = (b ? db_1 : db_0) + ((uint32_t) s * 2 * kBChunk >> 4);
+                    const uint32_t dp = d0 + (uint32_t) part * 4 * kScN;
+                    // digit products (A slice i, B slice j) into accumulator i + j, i + j <= 3
+                    constexpr int kI[10] = {0, 0, 1, 0, 1, 2, 0, 1, 2, 3}, kJ[10] = {0, 1, 0, 2, 1, 0, 3, 2, 1, 0};
+#pragma unroll
+                    for (int pi = 0; pi < 10; pi++) {
+                        const bool first_g = pi == 0 || pi == 1 || pi == 3 || pi == 6;
+                        umma_i8(dp + (uint32_t) (kI[pi] + kJ[pi]) * kScN, das + kI[pi] * a_slice, dbs + kJ[pi] * b_slice,
+                                !(first_s && first_g));
+                    }
+                }
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&bar_mma[b]))
+                             : "memory");
+                last = j;
+                if (j >= 1 && j + 1 < nchunks) {
+                    // the previous chunk's MMAs have read its query digits: refill that buffer with the next
+                    // chunk while this chunk's MMAs run
+                    const int pb = (j - 1) & 1;
+                    ok = mbar_wait(&bar_mma[pb], (uint32_t) ((j - 1) >> 1) & 1u, abort);
+                    if (!ok) break;
+                    mbar_expect_tx(&bar_b[pb], b_bytes);
+                    bulk_g2s(sB + (size_t) pb * b_bytes, a.b_sl + (size_t) (j + 1) * b_bytes, b_bytes, &bar_b[pb]);
+                }
+            }
+            if (!ok) {
+                *abort = 1;
+                atomicExch(a.status, 1);
+            }
+            // the MMAs of the last committed chunk finish on their own: wait for them (bounded) before
+            // the columns are released
+            if (last >= 0)
+                for (int it = 0; it < (1 << 22) && !mbar_try(&bar_mma[last & 1], (uint32_t) (last >> 1) & 1u); it++) {
+                }
+        }
+    } else {
+        // ---- epilogue ----
+        const int quad = warp & 3, cg = warp >> 2;
+        const int row = 32 * quad + lane;
+        const int64_t u = u0 + row;
+        const bool uval = u < a.n_user;
+        const float *srow = summ + row * kScSummStride;
+        RegUser r = {};
+        float un = 0.0f, cu = 0.0f, margin0 = 0.0f;
+        float4 um = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (uval) {
+            um = __ldg(a.umeta + u);
+            if (a.lv) {
+                r = reg_user(a.m, u);
+                un = __ldg(a.unorm + u);
+                cu = fabsf(r.a) * r.inv_sigma * 1.0001f;
+                // the screen's margin for a known score, with the table's error in place of the fast CDF's
+                margin0 = r.margin < INFINITY
+                              ? fabsf(r.a) * kCdfTabErr + (fabsf(r.a) + fabsf(r.b) + fabsf(r.err)) * 4.8e-7f + 1e-6f
+                              : INFINITY;
+            }
+        }
+        // the first two steps of the group search from registers
+        const float s7 = srow[7], s15 = srow[15], s23 = srow[23];
+        const int ue = __float_as_int(um.w);
+        const float cl_u = a.cl * um.y, cr_u = a.cr * um.z;
+        const uint32_t lane_base = taddr + ((uint32_t) (32 * quad) << 16) + (uint32_t) (8 * cg);
+        const int S = a.m.S;
+        int n_und = 0;
+        for (int j = 0; j < nchunks; j++) {
+            const int b = j & 1;
+            const uint32_t ph = (uint32_t) (j >> 1) & 1u;
+            if (!mbar_wait(&bar_mma[b], ph, abort)) {
+                *abort = 1;
+                atomicExch(a.status, 1);
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            float sl[8], sr[8];
+            {
+                uint32_t v0[8], v1[8], v2[8], v3[8];
+                const uint32_t base = lane_base + (uint32_t) b * buf_cols;
+                tmem_ld8(base, v0);
+                tmem_ld8(base + kScN, v1);
+                tmem_ld8(base + 2 * kScN, v2);
+                tmem_ld8(base + 3 * kScN, v3);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int i = 0; i < 8; i++) sl[i] = combine4(v0[i], v1[i], v2[i], v3[i]);
+                if (a.two_parts) {
+                    tmem_ld8(base + 4 * kScN, v0);
+                    tmem_ld8(base + 5 * kScN, v1);
+                    tmem_ld8(base + 6 * kScN, v2);
+                    tmem_ld8(base + 7 * kScN, v3);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                    for (int i = 0; i < 8; i++) sr[i] = combine4(v0[i], v1[i], v2[i], v3[i]);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 8; i++) sr[i] = 0.0f;
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&bar_free[b]);
+            uint32_t und_bits = 0;
+            // four pairs at a time, in side-effect-free phases so that their chains interleave
+#pragma unroll
+            for (int i0 = 0; i0 < 8; i0 += 4) {
+                constexpr int G = 4;
+                float vl[G], full[G], dl[G], df[G];
+                uint32_t packed[G];
+                bool ok[G];
+#pragma unroll
+                for (int g = 0; g < G; g++) {
+                    const int i = i0 + g;
+                    const float4 qm = sq[min(j * kScN + 8 * cg + i, nq - 1)];
+                    const float scale = __int_as_float((ue + __float_as_int(qm.w) - 35 + 127) << 23);
+                    vl[g] = sl[i] * scale;
+                    const float ee = um.x * qm.x;
+                    dl[g] = fmaf(cl_u, qm.y, ee * a.kl);
+                    const float dr = fmaf(cr_u, qm.z, ee * a.kr);
+                    full[g] = a.two_parts ? __fadd_rn(vl[g], sr[i] * scale) : vl[g];
+                    df[g] = fmaf(fabsf(full[g]), 2.4e-7f, (dl[g] + dr) * 1.0001f);
+                    ok[g] = true;
+                    packed[g] = 0;
+                }
+                if (a.lv) {
+#pragma unroll
+                    for (int g = 0; g < G; g++) {
+                        const float right = __fmul_rn(un, sqn[min(j * kScN + 8 * cg + i0 + g, nq - 1)]);
+                        const float qlb = __fsub_rn(vl[g], right), qub = __fadd_rn(vl[g], right);
+                        const float dq = dl[g] * 1.0001f;
+                        int l, h;
+                        const bool okl = level_side(r, margin0, cu, S, qlb, fmaf(fabsf(qlb), 2.4e-7f, dq), false, tab, l);
+                        const bool oku = level_side(r, margin0, cu, S, qub, fmaf(fabsf(qub), 2.4e-7f, dq), true, tab, h);
+                        ok[g] = okl && oku;
+                        packed[g] = (uint32_t) l | ((uint32_t) h << 16);
+                    }
+                }
+                // coarse group: the summary entries >= full (a five-step search and one compare)
+                int lo[G];
+#pragma unroll
+                for (int g = 0; g < G; g++) {
+                    lo[g] = s15 >= full[g] ? 16 : 0;
+                    lo[g] += (lo[g] ? s23 : s7) >= full[g] ? 8 : 0;
+                }
+#pragma unroll
+                for (int st = 4; st >= 1; st >>= 1)
+#pragma unroll
+                    for (int g = 0; g < G; g++) lo[g] += srow[lo[g] + st - 1] >= full[g] ? st : 0;
+#pragma unroll
+                for (int g = 0; g < G; g++) {
+                    lo[g] += srow[lo[g]] >= full[g];
+                    const bool gok = (lo[g] == 0 || srow[lo[g] - 1] >= full[g] + df[g]) &&
+                                     (lo[g] >= ThrSummary::kMaxGroups || srow[lo[g]] < full[g] - df[g]) &&
+                                     df[g] < 1e30f && full[g] == full[g];
+                    ok[g] = ok[g] && gok;
+                }
+                // every pair is stored; the exact pass rewrites the undecided ones
+#pragma unroll
+                for (int g = 0; g < G; g++) {
+                    const int q = j * kScN + 8 * cg + i0 + g;
+                    if (!uval || q >= nq) continue;
+                    const int64_t o = (int64_t) q * a.n_user + u;
+                    if (a.lv) a.lv[o] = ok[g] ? packed[g] : 0u;  // a placeholder in range until rewritten
+                    a.code[o] = (uint8_t) min(lo[g], a.nb);
+                    a.qip[o] = full[g];
+                    und_bits |= (uint32_t) !ok[g] << (i0 + g);
+                }
+            }
+            // the chunk's undecided pairs into the list: one shared-memory atomic per warp
+            const int cnt = __popc(und_bits);
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int tot = __shfl_sync(0xffffffffu, incl, 31);
+            if (tot) {
+                int base = 0;
+                if (lane == 31) base = atomicAdd(&list_n, tot);
+                base = __shfl_sync(0xffffffffu, base, 31);
+                int slot = base + incl - cnt;
+                n_und += cnt;
+                for (uint32_t m = und_bits; m; m &= m - 1, slot++) {
+                    const int q = j * kScN + 8 * cg + __ffs(m) - 1;
+                    if (slot < kScListCap) {
+                        list[slot] = (uint32_t) q | ((uint32_t) row << 16);
+                    } else {
+                        const int go = atomicAdd(a.ovf_count, 1);
+                        if (go < a.ovf_cap) a.ovf[go] = make_int2(a.q_base + q, (int) u);
+                        else atomicExch(a.status, 2);
+                    }
+                }
+            }
+        }
+        if (n_und) atomicAdd(a.undecided, n_und);
+    }
+    // all MMAs have completed once every epilogue warp has passed its last wait (or given up)
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    const int n_list = min(list_n, kScListCap);
+    if (!*abort && n_list > 0) {
+        // the tile's user rows (contiguous in global memory, 16-byte aligned: kScM rows of dim floats,
+        // kScM * 4 a multiple of 16) into the freed operand buffers, then the listed pairs
+        float *rows = reinterpret_cast<float *>(sm_raw);
+        const int ld = a.dim;
+        const int64_t n_rows = a.n_user - u0 < kScM ? a.n_user - u0 : kScM;
+        const float *src = a.urow + u0 * a.dim;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // after the tensor cores' reads
+        const int n_f = (int) n_rows * a.dim, n_v = n_f >> 2;
+        const float4 *src4 = reinterpret_cast<const float4 *>(src);
+        float4 *dst4 = reinterpret_cast<float4 *>(rows);
+        int v = tid;
+        for (; v + 3 * kScThreads < n_v; v += 4 * kScThreads) {  // four 16-byte loads in flight
+            const float4 x0 = __ldg(src4 + v), x1 = __ldg(src4 + v + kScThreads), x2 = __ldg(src4 + v + 2 * kScThreads),
+                         x3 = __ldg(src4 + v + 3 * kScThreads);
+            dst4[v] = x0;
+            dst4[v + kScThreads] = x1;
+            dst4[v + 2 * kScThreads] = x2;
+            dst4[v + 3 * kScThreads] = x3;
+        }
+        for (; v < n_v; v += kScThreads) dst4[v] = __ldg(src4 + v);
+        for (int f = 4 * n_v + tid; f < n_f; f += kScThreads) rows[f] = __ldg(src + f);
+        __syncthreads();
+        for (int i = tid; i < n_list; i += kScThreads) {
+            const uint32_t e = list[i];
+            const int row = (int) (e >> 16), q = (int) (e & 0xffffu);
+            exact_pair(a, u0 + row, q, summ + row * kScSummStride, rows + row * ld);
+        }
+    }
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(taddr) : "memory");
+    }
+}
+
+// Undecided pairs past the CTAs' lists.
+__global__ void scores_tc_ovf_kernel(ScArgs a) {
+    const int n = min(*a.ovf_count, a.ovf_cap);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int2 x = a.ovf[i];
+        float summ[ThrSummary::kMaxGroups];
+        for (int j = 0; j < ThrSummary::kMaxGroups; j++) summ[j] = __ldg(a.thr_summ + (int64_t) x.y * ThrSummary::kMaxGroups + j);
+        exact_pair(a, x.y, x.x, summ, a.urow + (int64_t) x.y * a.dim);
+    }
+}
+
+// The regression CDF table (see level_side): per cell (value at the node, difference to the next).
+void cdf_table_host(float2 *out) {
+    auto phi = [](double z) {
+        const double a1 = 0.254829592, a2 = -0.284496736, a3 = 1.421413741;
+        const double a4 = -1.453152027, a5 = 1.061405429, p = 0.3275911;
+        const double sign = z < 0 ? -1.0 : 1.0;
+        const double x = std::fabs(z) / std::sqrt(2.0);
+        const double t = 1.0 / (1.0 + p * x);
+        const double y = 1.0 - (((((a5 * t + a4) * t) + a3) * t + a2) * t + a1) * t * std::exp(-x * x);
+        return 0.5 * (1.0 + sign * y);
+    };
+    for (int i = 0; i < kCdfTabCells; i++) {
+        const double z0 = -8.0 + i / 128.0, v0 = phi(z0), v1 = phi(z0 + 1.0 / 128.0);
+        out[i] = make_float2((float) v0, (float) (v1 - v0));
+    }
+}
+
+// Bound coefficients of a part of n coordinates: (on the norm product, on 2^(ea + eb)).
+inline void part_coef(int n, float &cn, float &ke) {
+    if (n <= 0) {
+        cn = ke = 0.0f;
+        return;
+    }
+    const double u = 5.9604644775390625e-8;  // 2^-24
+    const double gamma = n * u / (1.0 - n * u);
+    cn = (float) ((gamma * 1.01 + 3.0 * u) * 1.0001);
+    ke = (float) (n * (3.02 * 9.313225746154785e-10 + 1.862645149230957e-9 + 3.0 * u * 0.008) * 1.01);
+}
+
+}  // namespace
+
+int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, PairScreen *screen, bool *done) {
+    *done = false;
+    if (!ix->scores_tc_on) return RKR_OK;
+    const int dim = ix->dim, nq = call.nq;
+    const int c = call.qsrp ? ix->check_dim : dim;
+    const int n1 = c, n2 = dim - c;
+    if (n1 <= 0 || n1 > kScMaxPart || n2 > kScMaxPart || nq <= 0) return RKR_OK;
+    const int cp = round32(n1), kp = cp + round32(n2);
+    if (kp > kScMaxKp) return RKR_OK;
+    const int64_t U = ix->n_user;
+    const int64_t n_tiles = (U + kScM - 1) / kScM;
+    if (n_tiles > 0x7fffffff) return RKR_OK;
+    // user digits for this split (built once per split and kept)
+    DevBuf &ub = call.qsrp ? ix->sc_user_split : ix->sc_user_full;
+    DevBuf &um = call.qsrp ? ix->sc_umeta_split : ix->sc_umeta_full;
+    int &key = call.qsrp ? ix->sc_key_split : ix->sc_key_full;
+    if (key != c) {
+        const int64_t n_pad = n_tiles * kScM;
+        RKR_TRY(ub.ensure((size_t) n_pad * kScSlices * kp));
+        RKR_TRY(um.ensure(sizeof(float4) * (size_t) n_pad));
+        const float *src = (call.qsrp ? ix->svd_user : ix->user).as<float>();
+        const unsigned g = (unsigned) ((n_pad * 32 + 255) / 256);
+        slice_rows_kernel<<<g, 256, 0, st>>>(src, U, n_pad, dim, c, cp, kp, kScM, ub.as<int8_t>(), um.as<float4>());
+        RKR_CUDA(cudaGetLastError());
+        key = c;
+    }
+    // query digits, chunks of kScN
+    const int nchunks = (nq + kScN - 1) / kScN;
+    const int64_t nq_pad = (int64_t) nchunks * kScN;
+    const int ovf_cap = (int) std::min<int64_t>(int64_t(1) << 24, std::max<int64_t>(int64_t(1) << 16, U * nq / 32));
+    const size_t b_total = (size_t) nq_pad * kScSlices * kp;
+    const int64_t words = (U + 31) / 32;
+    const size_t xbytes = sizeof(uint32_t) * (size_t) words * nq;
+    const size_t need = b_total + 256 + sizeof(float4) * (size_t) nq_pad + 256 + sizeof(int2) * (size_t) ovf_cap + 256 +
+                        xbytes + 256 + 64;
+    RKR_TRY(ix->ws_sc.ensure(need));
+    uint8_t *p = ix->ws_sc.as<uint8_t>();
+    auto take = [&](size_t bytes) {
+        uint8_t *r = p;
+        p += (bytes + 255) & ~size_t(255);
+        return r;
+    };
+    int8_t *b_sl = reinterpret_cast<int8_t *>(take(b_total));
+    float4 *qmeta = reinterpret_cast<float4 *>(take(sizeof(float4) * (size_t) nq_pad));
+    int2 *ovf = reinterpret_cast<int2 *>(take(sizeof(int2) * (size_t) ovf_cap));
+    uint32_t *xbits = reinterpret_cast<uint32_t *>(take(xbytes));
+    int *counters = reinterpret_cast<int *>(take(64));  // ovf_count, status, undecided, recomputed scores
+    RKR_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(int), st));
+    RKR_CUDA(cudaMemsetAsync(xbits, 0, xbytes, st));
+    {
+        const unsigned g = (unsigned) ((nq_pad * 32 + 255) / 256);
+        timed(ix, st, "scores_tc_prep", [&] {
+            slice_rows_kernel<<<g, 256, 0, st>>>(call.qrows, nq, nq_pad, dim, c, cp, kp, kScN, b_sl, qmeta);
+        });
+        RKR_CUDA(cudaGetLastError());
+    }
+    ScArgs a = {};
+    a.a_sl = ub.as<int8_t>();
+    a.b_sl = b_sl;
+    a.umeta = um.as<float4>();
+    a.qmeta = qmeta;
+    a.unorm = call.unorm;
+    a.qnorm = call.qnorm;
+    a.urow = (call.qsrp ? ix->svd_user : ix->user).as<float>();
+    a.qrow = call.qrows;
+    a.thr_summ = ix->thr_summ.as<float>();
+    a.m = call.m;
+    a.lv = call.lv;
+    a.code = call.code;
+    a.qip = call.qip;
+    a.xbits = xbits;
+    a.ovf = ovf;
+    a.ovf_count = counters;
+    a.status = counters + 1;
+    a.undecided = counters + 2;
+    a.ovf_cap = ovf_cap;
+    a.n_user = U;
+    a.nq = nq;
+    a.dim = dim;
+    a.c = c;
+    a.kp = kp;
+    a.ksplit = cp / 32;
+    a.ksteps = kp / 32;
+    a.two_parts = n2 > 0;
+    a.nb = call.nb;
+    part_coef(n1, a.cl, a.kl);
+    part_coef(n2, a.cr, a.kr);
+    if (call.qsrp && !ix->sc_cdf_tab.p) {
+        std::vector<float2> h(kCdfTabCells);
+        cdf_table_host(h.data());
+        RKR_TRY(ix->sc_cdf_tab.ensure(sizeof(float2) * kCdfTabCells));
+        RKR_CUDA(cudaMemcpy(ix->sc_cdf_tab.p, h.data(), sizeof(float2) * kCdfTabCells, cudaMemcpyHostToDevice));
+    }
+    a.cdf_tab = ix->sc_cdf_tab.as<float2>();
+    const size_t smem = (size_t) kScSlices * kp * (kScM + 2 * kScN) + sizeof(float) * kScM * kScSummStride +
+                        sizeof(uint32_t) * kScListCap + sizeof(float2) * kCdfTabCells +
+                        (sizeof(float4) + sizeof(float)) * kScMaxQ;
+    if (smem + 1024 > 227 * 1024) return RKR_OK;
+    RKR_CUDA(cudaFuncSetAttribute(scores_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    // launches of at most kScMaxQ queries (whole chunks): their data sits in shared memory
+    for (int q0 = 0; q0 < nq; q0 += kScMaxQ) {
+        ScArgs s = a;
+        s.q_base = q0;
+        s.nq = std::min(kScMaxQ, nq - q0);
+        s.b_sl = b_sl + (size_t) (q0 / kScN) * kScSlices * kScN * kp;
+        s.qmeta = qmeta + q0;
+        s.qnorm = a.qnorm ? a.qnorm + q0 : nullptr;
+        s.qrow = a.qrow + (size_t) q0 * dim;
+        s.lv = a.lv ? a.lv + (size_t) q0 * U : nullptr;
+        s.code = a.code + (size_t) q0 * U;
+        s.qip = a.qip + (size_t) q0 * U;
+        s.xbits = a.xbits + (size_t) q0 * words;
+        timed(ix, st, "qsrp_scores_tc", [&] { scores_tc_kernel<<<(unsigned) n_tiles, kScThreads, smem, st>>>(s); });
+        RKR_CUDA(cudaGetLastError());
+    }
+    timed(ix, st, "qsrp_scores_tc_ovf", [&] { scores_tc_ovf_kernel<<<148 * 4, 256, 0, st>>>(a); });
+    RKR_CUDA(cudaGetLastError());
+    int h[3] = {0, 0, 0};
+    RKR_CUDA(cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, st));
+    RKR_CUDA(cudaStreamSynchronize(st));
+    if (ix->prof.on) ix->prof.add_count("screen_undecided_pairs", h[2]);
+    if (h[1]) return RKR_OK;  // a wait gave up or the overflow list filled: the exact tiles redo the chunk
+    screen->umeta = a.umeta;
+    screen->qmeta = qmeta;
+    screen->cl = a.cl;
+    screen->kl = a.kl;
+    screen->cr = a.cr;
+    screen->kr = a.kr;
+    screen->xbits = xbits;
+    screen->n_exact = counters + 3;
+    *done = true;
+    return RKR_OK;
+}
+
+}  // namespace rkr

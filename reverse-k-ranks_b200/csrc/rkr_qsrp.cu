@@ -127,7 +127,10 @@ struct QipView {
     __device__ float delta(int64_t u, int64_t q, float s) const {
         const float4 um = __ldg(scr.umeta + u), qm = __ldg(scr.qmeta + q);
         const float ee = um.x * qm.x;
-        const float d = fmaf(scr.cl * um.y, qm.y, ee * scr.kl) + fmaf(scr.cr * um.z, qm.z, ee * scr.kr);
+        // per part: the weighted-norm term, the digits' term and the combination's leading term
+        // 3.002 u |part| <= 2.2 u Wa Wb (|part| <= Wa Wb / sqrt 2: every weight is at least 2)
+        const float nl = um.y * qm.y, nr = um.z * qm.z;
+        const float d = fmaf(scr.cl + 1.32e-7f, nl, ee * scr.kl) + fmaf(scr.cr + 1.32e-7f, nr, ee * scr.kr);
         return fmaf(fabsf(s), 2.4e-7f, d * 1.0001f);
     }
 };

@@ -14,9 +14,10 @@
 // 128, all steps exact in binary32).  The ten digit products with i + j <= 5 run as int8 MMAs
 // (tcgen05.mma kind::i8) into four int32 TMEM accumulators per part (grouped by i + j); integer
 // accumulation is exact.  Per part P of n coordinates the computed value differs from the exact
-// dot product by at most 2^(ea+eb) n (3.02 2^-30 + 2^-29 + 3 2^-24 0.008) (dropped digit products,
-// the remainders, and the three roundings that combine the accumulators), and the reference's
-// sequential binary32 sum differs from the exact one by at most n 2^-24 / (1 - n 2^-24) |a_P| |b_P|.
+// dot product by at most 2^(ea+eb) n (3.02 2^-30 + 2^-29 + 1.1e-4 2^-24) + 3.002 2^-24 |value|
+// (dropped digit products, the remainders, and the three roundings that combine the accumulators),
+// and the reference's sequential binary32 sum differs from the exact one by at most about 2^-24
+// Wa Wb, W the rows' position-weighted norms (part_coef).
 //
 // Tiles.  One CTA per 128 users (the MMA's M and the TMEM lanes) holds the users' digits for the
 // whole K extent in shared memory and walks the batch's queries in chunks of 32 (the MMA's N), the
@@ -54,8 +55,9 @@ __host__ __device__ inline int round32(int x) { return (x + 31) & ~31; }
 // Rows [n][dim] to the digit layout of the tiles: per tile of tr rows, 4 slices of [kp / 16][tr / 8]
 // [8 rows][16 bytes] (K-major core matrices); coordinates [0, c) at k in [0, c), [c, dim) at
 // [cp, cp + dim - c), zeros elsewhere and in rows [n, n_pad).  meta[r] = {2^e, upper bounds of the
-// norms of the two parts, e (as int bits)}; a row with a non-finite coordinate or a scale beyond
-// 2^+-kScMaxExp gets 2^e = inf, which sends all of its pairs to the exact path.  One warp per row.
+// weighted norms (sum_t w(t) x_t^2)^(1/2) of the two parts, e (as int bits)}; a row with a non-finite
+// coordinate or a scale beyond 2^+-kScMaxExp gets 2^e = inf, which sends all of its pairs to the
+// exact path.  One warp per row.
 __global__ void slice_rows_kernel(const float *__restrict__ src, int64_t n, int64_t n_pad, int dim, int c, int cp,
                                   int kp, int tr, int8_t *__restrict__ dst, float4 *__restrict__ meta) {
     const int64_t r = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -92,8 +94,11 @@ __global__ void slice_rows_kernel(const float *__restrict__ src, int64_t n, int6
         float v = 0.0f;
         if (row && k >= 0) {
             v = row[k];
-            if (k < c) sl += (double) v * v;
-            else sr += (double) v * v;
+            // position t of the coordinate in its part's sequential sum, weight w(t) (see part_coef)
+            const int t = k < c ? k : k - c, n = k < c ? c : dim - c;
+            const double w = t == 0 ? n : n - t + 1;
+            if (k < c) sl += w * v * v;
+            else sr += w * v * v;
         }
         float a = v * scale;  // exact: a power of two
         const size_t off = (size_t) (p >> 4) * (tr * 16) + (rr >> 3) * 128 + (rr & 7) * 16 + (p & 15);
@@ -199,12 +204,13 @@ __device__ __forceinline__ float combine4(uint32_t a0, uint32_t a1, uint32_t a2,
 
 // The regression CDF from a table: the reference's formula (Abramowitz & Stegun 7.1.26, as
 // NormalLinearRegressionLP::CDFPhi evaluates it, NormalLinearRegressionLP.hpp:123-143) tabulated in
-// double at z = -8 + i / 128 (2048 cells, values and differences rounded to binary32) and
-// interpolated linearly.  Against the reference's evaluation at the same argument the result is
-// within kCdfTabErr: interpolation h^2 / 8 max|f''| <= 1.9e-6, the table's roundings and the
-// interpolation's own < 3e-7, the reference's roundings < 6e-7, and the argument's few ulps.
+// double at z_i = -8 + i / 128 and interpolated by the quadratic through z_i, z_i+1, z_i+2 (Newton
+// form: value, first difference, half the second difference, each rounded to binary32).  Against the
+// reference's own evaluation at the same argument the result is within kCdfTabErr: interpolation
+// f (f-1) (f-2) / 6 h^3 max|f^(3)| < 2e-8, the table's and the evaluation's roundings < 3e-7, the
+// reference's roundings < 4e-7, and the argument's few ulps.
 constexpr int kCdfTabCells = 2048;
-constexpr float kCdfTabErr = 4.0e-6f;
+constexpr float kCdfTabErr = 1.0e-6f;
 
 // One side of the screen for a bound score q known to within dq of the reference's.  Within a cell
 // the formula's slope stays within a factor 1.1 of the cell's mean slope D * 128 on the cell widened
@@ -213,14 +219,16 @@ constexpr float kCdfTabErr = 4.0e-6f;
 // A user whose fit error reaches the cap takes the reference's capped levels in range
 // (ComputeRankBound's error test).  Returns false when undecided.
 __device__ __forceinline__ bool level_side(const RegUser &r, float margin0, float cu, int S, float q, float dq,
-                                           bool upper, const float2 *__restrict__ tab, int &lvl) {
+                                           bool upper, const float2 *__restrict__ tab, const float *__restrict__ tab2,
+                                           int &lvl) {
     const float z = __fsub_rn(q, r.mu) * r.inv_sigma;
     const float t = fminf(fmaxf(fmaf(z, 128.0f, 1024.0f), 0.0f), 2047.0f);
     const float tu = (t - 0.5f) + 12582912.0f;          // nearest integer of t - 0.5, in the significand
     const int i = __float_as_int(tu) - 0x4B400000;      // in [0, 2047]: floor(t), or floor(t) - 1 near integral t
     const float f = t - (tu - 12582912.0f);             // in [0, 1] up to 2^-14
     const float2 e = tab[i];
-    const float base = fmaf(fmaf(f, e.y, e.x), r.a, r.b);
+    const float cdf = fmaf(f, fmaf(f - 1.0f, tab2[i], e.y), e.x);
+    const float base = fmaf(cdf, r.a, r.b);
     const float v = upper ? base - r.err : base + r.err;
     const float margin = fmaf(cu * dq, fmaf(e.y, 141.0f, 1e-6f), margin0);
     const bool capped = !(margin0 < INFINITY);
@@ -251,7 +259,8 @@ struct ScArgs {
     const float *thr_summ;
     RegModel m;
     uint32_t *lv;                  // nullptr: no regression round (QS, US)
-    const float2 *cdf_tab;         // [kCdfTabCells] (value, difference to the next node)
+    const float2 *cdf_tab;         // [kCdfTabCells] (value, first difference)
+    const float *cdf_tab2;         // [kCdfTabCells] half the second difference
     uint8_t *code;
     float *qip;
     uint32_t *xbits;               // [query][(n_user + 31) / 32]: pairs whose stored score is the reference's
@@ -288,7 +297,7 @@ __device__ __forceinline__ float exact_dot_any(const float *a, const float *__re
     return acc;
 }
 
-// ur: the user's row (shared or global memory); the query's row is read from global memory.
+// The user's and the query's rows and the user's threshold summary in global memory.
 __device__ __forceinline__ void exact_pair(const ScArgs &a, int64_t u, int q, const float *summ, const float *ur) {
     const float *qr = a.qrow + (int64_t) q * a.dim;
     const float left = exact_dot_any(ur, qr, a.c);
@@ -300,8 +309,10 @@ __device__ __forceinline__ void exact_pair(const ScArgs &a, int64_t u, int q, co
                                           __fadd_rn(left, right));
     }
     if (a.c < a.dim) full = __fadd_rn(left, exact_dot_any(ur + a.c, qr + a.c, a.dim - a.c));
-    int g = 0;
-    for (int j = 0; j < ThrSummary::kMaxGroups; j++) g += summ[j] >= full;
+    int g = 0;  // the summary entries >= full (descending, -inf padded)
+#pragma unroll
+    for (int st = 16; st >= 1; st >>= 1) g += __ldg(summ + g + st - 1) >= full ? st : 0;
+    g += __ldg(summ + g) >= full;
     a.code[o] = (uint8_t) min(g, a.nb);
     a.qip[o] = full;
     atomicOr(a.xbits + (int64_t) q * ((a.n_user + 31) >> 5) + (u >> 5), 1u << (u & 31));
@@ -322,7 +333,8 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
     float *summ = reinterpret_cast<float *>(sB + 2 * b_bytes);
     uint32_t *list = reinterpret_cast<uint32_t *>(summ + kScM * kScSummStride);
     float2 *tab = reinterpret_cast<float2 *>(list + kScListCap);
-    float4 *sq = reinterpret_cast<float4 *>(tab + kCdfTabCells);  // the batch's query data
+    float *tab2 = reinterpret_cast<float *>(tab + kCdfTabCells);
+    float4 *sq = reinterpret_cast<float4 *>(tab2 + kCdfTabCells);  // the batch's query data
     float *sqn = reinterpret_cast<float *>(sq + kScMaxQ);
     volatile int *abort = &abort_flag;
 
@@ -348,7 +360,10 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
             u0 + rr < a.n_user ? __ldg(a.thr_summ + (u0 + rr) * ThrSummary::kMaxGroups + j) : -INFINITY;
     }
     if (a.lv)
-        for (int i = tid; i < kCdfTabCells; i += kScThreads) tab[i] = __ldg(a.cdf_tab + i);
+        for (int i = tid; i < kCdfTabCells; i += kScThreads) {
+            tab[i] = __ldg(a.cdf_tab + i);
+            tab2[i] = __ldg(a.cdf_tab2 + i);
+        }
     for (int i = tid; i < nq; i += kScThreads) {
         sq[i] = __ldg(a.qmeta + i);
         sqn[i] = a.lv ? __ldg(a.qnorm + i) : 0.0f;
@@ -506,9 +521,10 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                     const float scale = __int_as_float((ue + __float_as_int(qm.w) - 35 + 127) << 23);
                     vl[g] = sl[i] * scale;
                     const float ee = um.x * qm.x;
-                    dl[g] = fmaf(cl_u, qm.y, ee * a.kl);
-                    const float dr = fmaf(cr_u, qm.z, ee * a.kr);
-                    full[g] = a.two_parts ? __fadd_rn(vl[g], sr[i] * scale) : vl[g];
+                    dl[g] = fmaf(cl_u, qm.y, fmaf(fabsf(vl[g]), 1.8e-7f, ee * a.kl));
+                    const float vr = sr[i] * scale;
+                    const float dr = fmaf(cr_u, qm.z, fmaf(fabsf(vr), 1.8e-7f, ee * a.kr));
+                    full[g] = a.two_parts ? __fadd_rn(vl[g], vr) : vl[g];
                     df[g] = fmaf(fabsf(full[g]), 2.4e-7f, (dl[g] + dr) * 1.0001f);
                     ok[g] = true;
                     packed[g] = 0;
@@ -520,8 +536,8 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                         const float qlb = __fsub_rn(vl[g], right), qub = __fadd_rn(vl[g], right);
                         const float dq = dl[g] * 1.0001f;
                         int l, h;
-                        const bool okl = level_side(r, margin0, cu, S, qlb, fmaf(fabsf(qlb), 2.4e-7f, dq), false, tab, l);
-                        const bool oku = level_side(r, margin0, cu, S, qub, fmaf(fabsf(qub), 2.4e-7f, dq), true, tab, h);
+                        const bool okl = level_side(r, margin0, cu, S, qlb, fmaf(fabsf(qlb), 2.4e-7f, dq), false, tab, tab2, l);
+                        const bool oku = level_side(r, margin0, cu, S, qub, fmaf(fabsf(qub), 2.4e-7f, dq), true, tab, tab2, h);
                         ok[g] = okl && oku;
                         packed[g] = (uint32_t) l | ((uint32_t) h << 16);
                     }
@@ -589,35 +605,17 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
     // all MMAs have completed once every epilogue warp has passed its last wait (or given up)
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
+    // the tile's undecided pairs join the batch's list (one global atomic per CTA); a separate kernel
+    // with many threads in flight resolves them, hiding the latency of the rows' loads
+    __shared__ int list_base;
     const int n_list = min(list_n, kScListCap);
-    if (!*abort && n_list > 0) {
-        // the tile's user rows (contiguous in global memory, 16-byte aligned: kScM rows of dim floats,
-        // kScM * 4 a multiple of 16) into the freed operand buffers, then the listed pairs
-        float *rows = reinterpret_cast<float *>(sm_raw);
-        const int ld = a.dim;
-        const int64_t n_rows = a.n_user - u0 < kScM ? a.n_user - u0 : kScM;
-        const float *src = a.urow + u0 * a.dim;
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // after the tensor cores' reads
-        const int n_f = (int) n_rows * a.dim, n_v = n_f >> 2;
-        const float4 *src4 = reinterpret_cast<const float4 *>(src);
-        float4 *dst4 = reinterpret_cast<float4 *>(rows);
-        int v = tid;
-        for (; v + 3 * kScThreads < n_v; v += 4 * kScThreads) {  // four 16-byte loads in flight
-            const float4 x0 = __ldg(src4 + v), x1 = __ldg(src4 + v + kScThreads), x2 = __ldg(src4 + v + 2 * kScThreads),
-                         x3 = __ldg(src4 + v + 3 * kScThreads);
-            dst4[v] = x0;
-            dst4[v + kScThreads] = x1;
-            dst4[v + 2 * kScThreads] = x2;
-            dst4[v + 3 * kScThreads] = x3;
-        }
-        for (; v < n_v; v += kScThreads) dst4[v] = __ldg(src4 + v);
-        for (int f = 4 * n_v + tid; f < n_f; f += kScThreads) rows[f] = __ldg(src + f);
-        __syncthreads();
-        for (int i = tid; i < n_list; i += kScThreads) {
-            const uint32_t e = list[i];
-            const int row = (int) (e >> 16), q = (int) (e & 0xffffu);
-            exact_pair(a, u0 + row, q, summ + row * kScSummStride, rows + row * ld);
-        }
+    if (tid == 0) list_base = n_list ? atomicAdd(a.ovf_count, n_list) : 0;
+    __syncthreads();
+    for (int i = tid; i < n_list; i += kScThreads) {
+        const uint32_t e = list[i];
+        const int g = list_base + i;
+        if (g < a.ovf_cap) a.ovf[g] = make_int2(a.q_base + (int) (e & 0xffffu), (int) (u0 + (e >> 16)));
+        else atomicExch(a.status, 2);
     }
     __syncthreads();
     if (warp == 0) {
@@ -626,19 +624,19 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
     }
 }
 
-// Undecided pairs past the CTAs' lists.
-__global__ void scores_tc_ovf_kernel(ScArgs a) {
+// The listed (undecided) pairs, by the reference's arithmetic; consecutive entries come from one tile
+// of users, whose rows stay in L1.
+__global__ void __launch_bounds__(256) scores_tc_exact_kernel(ScArgs a) {
     const int n = min(*a.ovf_count, a.ovf_cap);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int2 x = a.ovf[i];
-        float summ[ThrSummary::kMaxGroups];
-        for (int j = 0; j < ThrSummary::kMaxGroups; j++) summ[j] = __ldg(a.thr_summ + (int64_t) x.y * ThrSummary::kMaxGroups + j);
-        exact_pair(a, x.y, x.x, summ, a.urow + (int64_t) x.y * a.dim);
+        exact_pair(a, x.y, x.x, a.thr_summ + (int64_t) x.y * ThrSummary::kMaxGroups, a.urow + (int64_t) x.y * a.dim);
     }
 }
 
-// The regression CDF table (see level_side): per cell (value at the node, difference to the next).
-void cdf_table_host(float2 *out) {
+// The regression CDF table (see level_side): per cell the value at the node, the first difference,
+// and half the second difference.
+void cdf_table_host(float2 *out, float *out2) {
     auto phi = [](double z) {
         const double a1 = 0.254829592, a2 = -0.284496736, a3 = 1.421413741;
         const double a4 = -1.453152027, a5 = 1.061405429, p = 0.3275911;
@@ -649,12 +647,21 @@ void cdf_table_host(float2 *out) {
         return 0.5 * (1.0 + sign * y);
     };
     for (int i = 0; i < kCdfTabCells; i++) {
-        const double z0 = -8.0 + i / 128.0, v0 = phi(z0), v1 = phi(z0 + 1.0 / 128.0);
+        const double z0 = -8.0 + i / 128.0;
+        const double v0 = phi(z0), v1 = phi(z0 + 1.0 / 128.0), v2 = phi(z0 + 2.0 / 128.0);
         out[i] = make_float2((float) v0, (float) (v1 - v0));
+        out2[i] = (float) (0.5 * (v2 - 2.0 * v1 + v0));
     }
 }
 
-// Bound coefficients of a part of n coordinates: (on the norm product, on 2^(ea + eb)).
+// Bound coefficients of a part of n coordinates: (on the product of the rows' weighted norms, on
+// 2^(ea + eb)).  The reference's sequential binary32 sum of p_t = a_t b_t (t = 1..n, one rounding
+// per product and per addition) differs from the exact sum by at most u (1 + gamma_n) / (1 - u)
+// sum_t w_t |p_t|, w_1 = n, w_t = n - t + 2 (each product's rounding, plus the rounding of every
+// partial sum that contains it), and sum_t w_t |a_t b_t| <= Wa Wb with W = (sum_t w_t x_t^2)^(1/2)
+// (Cauchy-Schwarz).  The digits: dropped products 3.02 n 2^-30, remainders n 2^-29, and the tails
+// of the three roundings that combine the accumulators n 1.1e-4 u (their leading part, 3.002 u
+// times the computed value, is added per pair).
 inline void part_coef(int n, float &cn, float &ke) {
     if (n <= 0) {
         cn = ke = 0.0f;
@@ -662,8 +669,8 @@ inline void part_coef(int n, float &cn, float &ke) {
     }
     const double u = 5.9604644775390625e-8;  // 2^-24
     const double gamma = n * u / (1.0 - n * u);
-    cn = (float) ((gamma * 1.01 + 3.0 * u) * 1.0001);
-    ke = (float) (n * (3.02 * 9.313225746154785e-10 + 1.862645149230957e-9 + 3.0 * u * 0.008) * 1.01);
+    cn = (float) (u * (1.0 + gamma) / (1.0 - u) * 1.0001);
+    ke = (float) (n * (3.02 * 9.313225746154785e-10 + 1.862645149230957e-9 + 1.1e-4 * u) * 1.01);
 }
 
 }  // namespace
@@ -757,13 +764,17 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, PairScre
     part_coef(n2, a.cr, a.kr);
     if (call.qsrp && !ix->sc_cdf_tab.p) {
         std::vector<float2> h(kCdfTabCells);
-        cdf_table_host(h.data());
-        RKR_TRY(ix->sc_cdf_tab.ensure(sizeof(float2) * kCdfTabCells));
+        std::vector<float> h2(kCdfTabCells);
+        cdf_table_host(h.data(), h2.data());
+        RKR_TRY(ix->sc_cdf_tab.ensure((sizeof(float2) + sizeof(float)) * kCdfTabCells));
         RKR_CUDA(cudaMemcpy(ix->sc_cdf_tab.p, h.data(), sizeof(float2) * kCdfTabCells, cudaMemcpyHostToDevice));
+        RKR_CUDA(cudaMemcpy(ix->sc_cdf_tab.as<uint8_t>() + sizeof(float2) * kCdfTabCells, h2.data(),
+                            sizeof(float) * kCdfTabCells, cudaMemcpyHostToDevice));
     }
     a.cdf_tab = ix->sc_cdf_tab.as<float2>();
+    a.cdf_tab2 = reinterpret_cast<const float *>(ix->sc_cdf_tab.as<uint8_t>() + sizeof(float2) * kCdfTabCells);
     const size_t smem = (size_t) kScSlices * kp * (kScM + 2 * kScN) + sizeof(float) * kScM * kScSummStride +
-                        sizeof(uint32_t) * kScListCap + sizeof(float2) * kCdfTabCells +
+                        sizeof(uint32_t) * kScListCap + (sizeof(float2) + sizeof(float)) * kCdfTabCells +
                         (sizeof(float4) + sizeof(float)) * kScMaxQ;
     if (smem + 1024 > 227 * 1024) return RKR_OK;
     RKR_CUDA(cudaFuncSetAttribute(scores_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
@@ -783,7 +794,7 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, PairScre
         timed(ix, st, "qsrp_scores_tc", [&] { scores_tc_kernel<<<(unsigned) n_tiles, kScThreads, smem, st>>>(s); });
         RKR_CUDA(cudaGetLastError());
     }
-    timed(ix, st, "qsrp_scores_tc_ovf", [&] { scores_tc_ovf_kernel<<<148 * 4, 256, 0, st>>>(a); });
+    timed(ix, st, "qsrp_scores_tc_exact", [&] { scores_tc_exact_kernel<<<148 * 8, 256, 0, st>>>(a); });
     RKR_CUDA(cudaGetLastError());
     int h[3] = {0, 0, 0};
     RKR_CUDA(cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, st));

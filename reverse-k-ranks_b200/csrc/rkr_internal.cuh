@@ -477,6 +477,23 @@ inline cudaError_t launch_big(const float *A, const int32_t *a_idx, int64_t n_a,
 __device__ __forceinline__ float exact_dot(const float *__restrict__ a, const float *__restrict__ b, int n) {
     float acc = 0.0f;
     int j = 0;
+    if (((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b)) & 7) == 0) {
+        // 8-byte loads, sixteen coordinates ahead of their (ordered) sum: per-thread rows are read
+        // with half the memory transactions
+        for (; j + 16 <= n; j += 16) {
+            float2 x[8], y[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                x[t] = __ldg(reinterpret_cast<const float2 *>(a + j) + t);
+                y[t] = __ldg(reinterpret_cast<const float2 *>(b + j) + t);
+            }
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                acc = __fadd_rn(acc, __fmul_rn(x[t].x, y[t].x));
+                acc = __fadd_rn(acc, __fmul_rn(x[t].y, y[t].y));
+            }
+        }
+    }
     for (; j + 8 <= n; j += 8) {  // loads of eight coordinates ahead of their (ordered) sum
         float x[8], y[8];
 #pragma unroll

@@ -713,7 +713,7 @@ __global__ void __launch_bounds__(256) qsrp_fine2_kernel(const uint8_t *__restri
 }
 
 // Exact buckets of the listed pairs.
-__global__ void qsrp_fine2_list_kernel(HitList hl, QipView sc, int64_t n_user, const float *__restrict__ thr, int S,
+__global__ void __launch_bounds__(256, 4) qsrp_fine2_list_kernel(HitList hl, QipView sc, int64_t n_user, const float *__restrict__ thr, int S,
                                        int gs, int *__restrict__ hist_f) {
     const int n = min(*hl.count, hl.cap);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -940,7 +940,7 @@ struct QsrpCompactPolicy {
 
 // Scores of the emitted result users: this query's score when the user reached round 2, else the
 // score from its latest earlier round-2 query in the batch, else the carried state.
-__global__ void qsrp_result_fill_kernel(const QueryCounts *__restrict__ counts, const int32_t *__restrict__ res_user,
+__global__ void __launch_bounds__(128, 8) qsrp_result_fill_kernel(const QueryCounts *__restrict__ counts, const int32_t *__restrict__ res_user,
                                         const uint8_t *__restrict__ res_fresh, const uint8_t *__restrict__ code,
                                         QipView sc, int64_t n_user, const float *__restrict__ state, int topk,
                                         float *__restrict__ res_qip) {
@@ -956,7 +956,7 @@ __global__ void qsrp_result_fill_kernel(const QueryCounts *__restrict__ counts, 
     }
 }
 
-__global__ void qsrp_cand_fill_kernel(const int32_t *__restrict__ cand_user, const int32_t *__restrict__ cand_query,
+__global__ void __launch_bounds__(256, 4) qsrp_cand_fill_kernel(const int32_t *__restrict__ cand_user, const int32_t *__restrict__ cand_query,
                                       int64_t n, QipView sc, float *__restrict__ cand_qip) {
     const int64_t e = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n) return;
@@ -964,7 +964,7 @@ __global__ void qsrp_cand_fill_kernel(const int32_t *__restrict__ cand_user, con
 }
 
 // Carried state after the batch: each user's score at its last round-2 query of the batch.
-__global__ void qsrp_state_kernel(const uint8_t *__restrict__ code, QipView sc, int64_t n_user, int nq,
+__global__ void __launch_bounds__(256, 4) qsrp_state_kernel(const uint8_t *__restrict__ code, QipView sc, int64_t n_user, int nq,
                                   float *__restrict__ state) {
     const int64_t u = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= n_user) return;

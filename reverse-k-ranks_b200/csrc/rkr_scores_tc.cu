@@ -264,9 +264,13 @@ struct ScArgs {
     uint8_t *code;
     float *qip;
     uint32_t *xbits;               // [query][(n_user + 31) / 32]: pairs whose stored score is the reference's
-    int2 *ovf;                     // undecided pairs past a CTA's list: (query, user)
+    int2 *ovf;                     // undecided pairs, (query, user): each tile's list in one piece
     int *ovf_count, *status, *undecided;
     int ovf_cap;
+    int2 *tile_rng;                // per tile of the launch: (first entry, entries) in ovf
+    int2 *spill;                   // undecided pairs past a tile's shared-memory list
+    int *spill_count;
+    int spill_cap;
     int q_base;                    // the launch's first query in the batch (overflow entries hold batch queries)
     int64_t n_user;
     int nq, dim, c, kp, ksplit, ksteps, two_parts, nb;
@@ -279,12 +283,20 @@ struct ScArgs {
 __device__ __forceinline__ float exact_dot_any(const float *a, const float *__restrict__ b, int n) {
     float acc = 0.0f;
     int j = 0;
-    for (; j + 32 <= n; j += 32) {  // 32 loads of the global operand ahead of their (ordered) sum
-        float y[32];
+    if (((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b)) & 7) == 0) {
+        for (; j + 32 <= n; j += 32) {  // 8-byte loads, 32 coordinates ahead of their (ordered) sum
+            float2 x[16], y[16];
 #pragma unroll
-        for (int t = 0; t < 32; t++) y[t] = __ldg(b + j + t);
+            for (int t = 0; t < 16; t++) {
+                x[t] = reinterpret_cast<const float2 *>(a + j)[t];
+                y[t] = __ldg(reinterpret_cast<const float2 *>(b + j) + t);
+            }
 #pragma unroll
-        for (int t = 0; t < 32; t++) acc = __fadd_rn(acc, __fmul_rn(a[j + t], y[t]));
+            for (int t = 0; t < 16; t++) {
+                acc = __fadd_rn(acc, __fmul_rn(x[t].x, y[t].x));
+                acc = __fadd_rn(acc, __fmul_rn(x[t].y, y[t].y));
+            }
+        }
     }
     for (; j + 8 <= n; j += 8) {
         float y[8];
@@ -593,8 +605,8 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                     if (slot < kScListCap) {
                         list[slot] = (uint32_t) q | ((uint32_t) row << 16);
                     } else {
-                        const int go = atomicAdd(a.ovf_count, 1);
-                        if (go < a.ovf_cap) a.ovf[go] = make_int2(a.q_base + q, (int) u);
+                        const int go = atomicAdd(a.spill_count, 1);
+                        if (go < a.spill_cap) a.spill[go] = make_int2(a.q_base + q, (int) u);
                         else atomicExch(a.status, 2);
                     }
                 }
@@ -609,7 +621,10 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
     // with many threads in flight resolves them, hiding the latency of the rows' loads
     __shared__ int list_base;
     const int n_list = min(list_n, kScListCap);
-    if (tid == 0) list_base = n_list ? atomicAdd(a.ovf_count, n_list) : 0;
+    if (tid == 0) {
+        list_base = n_list ? atomicAdd(a.ovf_count, n_list) : 0;
+        a.tile_rng[blockIdx.x] = make_int2(list_base, list_base + n_list <= a.ovf_cap ? n_list : 0);
+    }
     __syncthreads();
     for (int i = tid; i < n_list; i += kScThreads) {
         const uint32_t e = list[i];
@@ -624,12 +639,33 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
     }
 }
 
-// The listed (undecided) pairs, by the reference's arithmetic; consecutive entries come from one tile
-// of users, whose rows stay in L1.
-__global__ void __launch_bounds__(256) scores_tc_exact_kernel(ScArgs a) {
-    const int n = min(*a.ovf_count, a.ovf_cap);
+// The listed (undecided) pairs of one tile of users, by the reference's arithmetic: the tile's user
+// rows are staged in shared memory once (they are contiguous in global memory), the queries' rows
+// come from L2.
+__global__ void __launch_bounds__(256, 2) scores_tc_exact_tile_kernel(ScArgs a, int n_tiles) {
+    extern __shared__ __align__(16) float rows[];
+    const int2 rng = a.tile_rng[(int64_t) blockIdx.y * n_tiles + blockIdx.x];
+    if (rng.y == 0) return;
+    const int64_t u0 = (int64_t) blockIdx.x * kScM;
+    const int64_t n_rows = a.n_user - u0 < kScM ? a.n_user - u0 : kScM;
+    const float *src = a.urow + u0 * a.dim;
+    const int n_f = (int) n_rows * a.dim, n_v = n_f >> 2;  // the tile starts 16-byte aligned (kScM * 4 | 16)
+    const float4 *src4 = reinterpret_cast<const float4 *>(src);
+    float4 *dst4 = reinterpret_cast<float4 *>(rows);
+    for (int v = threadIdx.x; v < n_v; v += blockDim.x) dst4[v] = __ldg(src4 + v);
+    for (int f = 4 * n_v + threadIdx.x; f < n_f; f += blockDim.x) rows[f] = __ldg(src + f);
+    __syncthreads();
+    for (int i = threadIdx.x; i < rng.y; i += blockDim.x) {
+        const int2 x = a.ovf[rng.x + i];
+        exact_pair(a, x.y, x.x, a.thr_summ + (int64_t) x.y * ThrSummary::kMaxGroups, rows + (x.y - u0) * a.dim);
+    }
+}
+
+// Undecided pairs past the tiles' shared-memory lists (a tile with more than kScListCap of them).
+__global__ void __launch_bounds__(256, 2) scores_tc_spill_kernel(ScArgs a) {
+    const int n = min(*a.spill_count, a.spill_cap);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int2 x = a.ovf[i];
+        const int2 x = a.spill[i];
         exact_pair(a, x.y, x.x, a.thr_summ + (int64_t) x.y * ThrSummary::kMaxGroups, a.urow + (int64_t) x.y * a.dim);
     }
 }
@@ -708,7 +744,10 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, PairScre
     const size_t b_total = (size_t) nq_pad * kScSlices * kp;
     const int64_t words = (U + 31) / 32;
     const size_t xbytes = sizeof(uint32_t) * (size_t) words * nq;
+    const int n_launch = (nq + kScMaxQ - 1) / kScMaxQ;
+    const int spill_cap = 1 << 20;
     const size_t need = b_total + 256 + sizeof(float4) * (size_t) nq_pad + 256 + sizeof(int2) * (size_t) ovf_cap + 256 +
+                        sizeof(int2) * ((size_t) n_launch * n_tiles + spill_cap) + 512 +
                         xbytes + 256 + 64;
     RKR_TRY(ix->ws_sc.ensure(need));
     uint8_t *p = ix->ws_sc.as<uint8_t>();
@@ -720,9 +759,11 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, PairScre
     int8_t *b_sl = reinterpret_cast<int8_t *>(take(b_total));
     float4 *qmeta = reinterpret_cast<float4 *>(take(sizeof(float4) * (size_t) nq_pad));
     int2 *ovf = reinterpret_cast<int2 *>(take(sizeof(int2) * (size_t) ovf_cap));
+    int2 *tile_rng = reinterpret_cast<int2 *>(take(sizeof(int2) * (size_t) n_launch * n_tiles));
+    int2 *spill = reinterpret_cast<int2 *>(take(sizeof(int2) * (size_t) spill_cap));
     uint32_t *xbits = reinterpret_cast<uint32_t *>(take(xbytes));
-    int *counters = reinterpret_cast<int *>(take(64));  // ovf_count, status, undecided, recomputed scores
-    RKR_CUDA(cudaMemsetAsync(counters, 0, 4 * sizeof(int), st));
+    int *counters = reinterpret_cast<int *>(take(64));  // ovf_count, status, undecided, recomputed scores, spill
+    RKR_CUDA(cudaMemsetAsync(counters, 0, 5 * sizeof(int), st));
     RKR_CUDA(cudaMemsetAsync(xbits, 0, xbytes, st));
     {
         const unsigned g = (unsigned) ((nq_pad * 32 + 255) / 256);
@@ -751,6 +792,9 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, PairScre
     a.status = counters + 1;
     a.undecided = counters + 2;
     a.ovf_cap = ovf_cap;
+    a.spill = spill;
+    a.spill_count = counters + 4;
+    a.spill_cap = spill_cap;
     a.n_user = U;
     a.nq = nq;
     a.dim = dim;
@@ -791,10 +835,19 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, PairScre
         s.code = a.code + (size_t) q0 * U;
         s.qip = a.qip + (size_t) q0 * U;
         s.xbits = a.xbits + (size_t) q0 * words;
+        s.tile_rng = tile_rng + (size_t) (q0 / kScMaxQ) * n_tiles;
         timed(ix, st, "qsrp_scores_tc", [&] { scores_tc_kernel<<<(unsigned) n_tiles, kScThreads, smem, st>>>(s); });
         RKR_CUDA(cudaGetLastError());
     }
-    timed(ix, st, "qsrp_scores_tc_exact", [&] { scores_tc_exact_kernel<<<148 * 8, 256, 0, st>>>(a); });
+    a.tile_rng = tile_rng;
+    const size_t rows_smem = sizeof(float) * kScM * (size_t) dim;
+    RKR_CUDA(cudaFuncSetAttribute(scores_tc_exact_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int) rows_smem));
+    timed(ix, st, "qsrp_scores_tc_exact", [&] {
+        scores_tc_exact_tile_kernel<<<dim3((unsigned) n_tiles, (unsigned) n_launch), 256, rows_smem, st>>>(a, (int) n_tiles);
+    });
+    RKR_CUDA(cudaGetLastError());
+    timed(ix, st, "qsrp_scores_tc_spill", [&] { scores_tc_spill_kernel<<<148 * 4, 256, 0, st>>>(a); });
     RKR_CUDA(cudaGetLastError());
     int h[3] = {0, 0, 0};
     RKR_CUDA(cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, st));

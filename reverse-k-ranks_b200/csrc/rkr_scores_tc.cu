@@ -45,7 +45,7 @@ constexpr int kScListCap = 4096;                   // undecided pairs per CTA re
 constexpr int kScMaxQ = 1024;                      // queries per launch (their data sits in shared memory)
 constexpr int kScMaxKp = 224;                      // padded coordinates (both parts): shared memory
 constexpr int kScMaxPart = 240;                    // coordinates per part: digit sums stay below 2^22
-constexpr int kScSummStride = ThrSummary::kMaxGroups + 1;
+constexpr int kScSummStride = kScM;  // summary transposed: entry j of row r at j * kScM + r (lanes hit distinct banks)
 constexpr int kScMaxExp = 40;                      // rows scaled beyond 2^+-40 go to the exact path
 
 __host__ __device__ inline int round32(int x) { return (x + 31) & ~31; }
@@ -343,7 +343,7 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
     uint8_t *sA = sm_raw;
     uint8_t *sB = sA + a_bytes;
     float *summ = reinterpret_cast<float *>(sB + 2 * b_bytes);
-    uint32_t *list = reinterpret_cast<uint32_t *>(summ + kScM * kScSummStride);
+    uint32_t *list = reinterpret_cast<uint32_t *>(summ + ThrSummary::kMaxGroups * kScSummStride);
     float2 *tab = reinterpret_cast<float2 *>(list + kScListCap);
     float *tab2 = reinterpret_cast<float *>(tab + kCdfTabCells);
     float4 *sq = reinterpret_cast<float4 *>(tab2 + kCdfTabCells);  // the batch's query data
@@ -368,7 +368,7 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
     }
     for (int idx = tid; idx < kScM * ThrSummary::kMaxGroups; idx += kScThreads) {
         const int rr = idx / ThrSummary::kMaxGroups, j = idx % ThrSummary::kMaxGroups;
-        summ[rr * kScSummStride + j] =
+        summ[j * kScSummStride + rr] =
             u0 + rr < a.n_user ? __ldg(a.thr_summ + (u0 + rr) * ThrSummary::kMaxGroups + j) : -INFINITY;
     }
     if (a.lv)
@@ -459,7 +459,7 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
         const int row = 32 * quad + lane;
         const int64_t u = u0 + row;
         const bool uval = u < a.n_user;
-        const float *srow = summ + row * kScSummStride;
+        const float *srow = summ + row;  // entry j at srow[j * kScSummStride]
         RegUser r = {};
         float un = 0.0f, cu = 0.0f, margin0 = 0.0f;
         float4 um = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -476,7 +476,7 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
             }
         }
         // the first two steps of the group search from registers
-        const float s7 = srow[7], s15 = srow[15], s23 = srow[23];
+        const float s7 = srow[7 * kScSummStride], s15 = srow[15 * kScSummStride], s23 = srow[23 * kScSummStride];
         const int ue = __float_as_int(um.w);
         const float cl_u = a.cl * um.y, cr_u = a.cr * um.z;
         const uint32_t lane_base = taddr + ((uint32_t) (32 * quad) << 16) + (uint32_t) (8 * cg);
@@ -564,12 +564,12 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
 #pragma unroll
                 for (int st = 4; st >= 1; st >>= 1)
 #pragma unroll
-                    for (int g = 0; g < G; g++) lo[g] += srow[lo[g] + st - 1] >= full[g] ? st : 0;
+                    for (int g = 0; g < G; g++) lo[g] += srow[(lo[g] + st - 1) * kScSummStride] >= full[g] ? st : 0;
 #pragma unroll
                 for (int g = 0; g < G; g++) {
-                    lo[g] += srow[lo[g]] >= full[g];
-                    const bool gok = (lo[g] == 0 || srow[lo[g] - 1] >= full[g] + df[g]) &&
-                                     (lo[g] >= ThrSummary::kMaxGroups || srow[lo[g]] < full[g] - df[g]) &&
+                    lo[g] += srow[lo[g] * kScSummStride] >= full[g];
+                    const bool gok = (lo[g] == 0 || srow[(lo[g] - 1) * kScSummStride] >= full[g] + df[g]) &&
+                                     (lo[g] >= ThrSummary::kMaxGroups || srow[lo[g] * kScSummStride] < full[g] - df[g]) &&
                                      df[g] < 1e30f && full[g] == full[g];
                     ok[g] = ok[g] && gok;
                 }
@@ -817,7 +817,7 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, PairScre
     }
     a.cdf_tab = ix->sc_cdf_tab.as<float2>();
     a.cdf_tab2 = reinterpret_cast<const float *>(ix->sc_cdf_tab.as<uint8_t>() + sizeof(float2) * kCdfTabCells);
-    const size_t smem = (size_t) kScSlices * kp * (kScM + 2 * kScN) + sizeof(float) * kScM * kScSummStride +
+    const size_t smem = (size_t) kScSlices * kp * (kScM + 2 * kScN) + sizeof(float) * ThrSummary::kMaxGroups * kScM +
                         sizeof(uint32_t) * kScListCap + (sizeof(float2) + sizeof(float)) * kCdfTabCells +
                         (sizeof(float4) + sizeof(float)) * kScMaxQ;
     if (smem + 1024 > 227 * 1024) return RKR_OK;

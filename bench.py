@@ -167,31 +167,43 @@ class Clocks:
                 "reasons": reasons, "samples": len(samples)}
 
 
-def kernel_model(name, cfg, nq, stats):
-    """Algorithmic (ops, bytes) per launch of the query kernels, from the workload's sizes.
+def kernel_model(name, cfg, nq, stats, method):
+    """Algorithmic (dot_flops, bytes, tensor_ops) per launch of the query kernels, from the workload's
+    sizes.
 
-    ops counts binary32 multiplies and adds as separate operations: the exact dot products round
-    every product and every partial sum (no FMA), so each coordinate costs one multiply and one add.
-    bytes is what the kernel must move through HBM at the least."""
+    dot_flops counts the exact dot products' binary32 multiplies and adds as separate operations (2 per
+    coordinate and pair).  bytes is what the kernel must move through HBM at the least.  tensor_ops
+    counts the tensor-core operations the kernel issues for them: the pair scores run ten int8 digit
+    products per coordinate (K padded to 32 per part), the refinement one TF32 product."""
     n_user, n_item, dim = CONFIGS[cfg][:3]
     pairs = float(n_user) * nq
-    if name == "qsrp_scores":
-        # per pair: levels (4 B) + full score (4 B) + round-2 group (1 B) written; the users'
-        # SVD vectors, regression records (32 B) and threshold summaries (128 B) read once
-        return 2.0 * pairs * dim, 9.0 * pairs + n_user * (4.0 * dim + 32 + 128) + 4.0 * nq * dim
+    r32 = lambda x: (x + 31) // 32 * 32
+    if name == "qsrp_scores_tc":
+        qsrp = method == "QSRPNormalLP"
+        cd = stats["check_dim"] if qsrp else dim
+        kp = r32(cd) + (r32(dim - cd) if dim > cd else 0)
+        # per pair: levels (4 B, QSRP) + coarse group (1 B) + score (4 B) written; per user its digits
+        # (4 kp B), scale and norms (16 B), threshold summary (128 B) and regression record (32 B) read
+        out = (9.0 if qsrp else 5.0) * pairs
+        per_user = 4.0 * kp + 16 + 128 + (32 if qsrp else 0)
+        return 2.0 * pairs * dim, out + n_user * per_user + nq * (4.0 * kp + 20), 10 * 2.0 * pairs * kp
     if name == "qsrp_round2":
-        return 0.0, 4.0 * pairs + 1.0 * pairs
+        return 0.0, 4.0 * pairs + 1.0 * pairs, 0.0
     if name == "level_hist":
-        return 0.0, 4.0 * pairs
-    if name == "refine_tile":
-        return 2.0 * stats["n_compute_item"] * dim, 4.0 * stats["n_compute_item"] * dim
-    return 0.0, 0.0
+        return 0.0, 4.0 * pairs, 0.0
+    if name == "refine_tc":
+        n = stats["n_compute_item"]
+        return 2.0 * n * dim, 4.0 * n_item * dim, 2.0 * n * (dim + 8)
+    return 0.0, 0.0, 0.0
 
 
-# DRAM bytes (read + write) per (query, user) pair of the dominant kernels, from one ncu capture at a
-# 200-query batch of the same workload (profiles/qsrp_query_kernels_batch200_full.md); traffic grows
+# DRAM bytes (read + write) per (query, user) pair of the dominant kernel, from one ncu capture at a
+# 200-query batch of the same workload (profiles/qsrp_tc_kernels_batch200_full.md); traffic grows
 # with the pairs a launch processes, so a launch's traffic is this figure times its pairs.
-NCU_BYTES_PER_PAIR = {"qsrp_scores": (367.812096e6 + 819.383040e6) / (200 * 480189.0)}
+NCU_BYTES_PER_PAIR = {("qsrp_scores_tc", "QSRPNormalLP"): (456.599e6 + 814.504e6) / (200 * 480189.0)}
+
+# Nominal dense tensor-core peaks of one B200 (T ops/s), for the tensor_ops figures.
+TENSOR_PEAK_NOMINAL = {"qsrp_scores_tc": ("int8", 4500.0), "refine_tc": ("tf32", 1125.0)}
 
 
 class ReferenceTimer:
@@ -360,24 +372,27 @@ def main():
     stats_mean = {f: float(st[f].mean()) for f in R.QUERY_STATS.names}
     dom = max(prof.items(), key=lambda kv: kv[1][0])
     dom_name, (dom_ms, dom_n) = dom
-    ops, nbytes = kernel_model(dom_name, args.config, batch, model_stats)
+    ops, nbytes, tops = kernel_model(dom_name, args.config, batch, model_stats, args.method)
     avg_s = dom_ms / 1e3 / max(dom_n, 1)
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    sm_clock_ghz = (peaks.get("sm_max_mhz", 1965.0)) / 1e3
-    simt_peak_tops = 148 * 128 * sm_clock_ghz / 1e3  # one FP32 add or mul per lane per clock, T ops/s
+    ncu_bpp = NCU_BYTES_PER_PAIR.get((dom_name, args.method))
     roofline = {"kernel": dom_name, "bound": "hbm", "achieved": nbytes / avg_s / 1e9, "peak": hbm_peak,
                 "unit": "GB/s", "frac": (nbytes / avg_s / 1e9) / hbm_peak,
                 "peak_source": "MEASURED_PEAKS.json" if peaks else "fallback",
-                "traffic": (NCU_BYTES_PER_PAIR[dom_name] * CONFIGS[args.config][0] * batch
-                            if dom_name in NCU_BYTES_PER_PAIR and args.config == "config2" else None),
+                "traffic": (ncu_bpp * CONFIGS[args.config][0] * batch
+                            if ncu_bpp is not None and args.config == "config2" else None),
                 "avg_launch_ms": avg_s * 1e3,
                 "share_of_step": dom_ms / max(sum(v[0] for v in prof.values()), 1e-9),
-                "simt_fp32": {"achieved_tops": ops / avg_s / 1e12, "peak_tops_nominal": simt_peak_tops,
-                              "frac": (ops / avg_s / 1e12) / simt_peak_tops},
+                "dot_tflops_fp32_equivalent": ops / avg_s / 1e12}
+    if dom_name in TENSOR_PEAK_NOMINAL:
+        kind, peak = TENSOR_PEAK_NOMINAL[dom_name]
+        roofline["tensor"] = {"kind": kind, "achieved_tops": tops / avg_s / 1e12, "peak_tops_nominal": peak,
+                              "frac": tops / avg_s / 1e12 / peak}
+    roofline.update({
                 "kernels_ms_per_step": {k: round(v[0], 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
-                "counters_per_step": counters}
+                "counters_per_step": counters})
 
     # ---- latency ------------------------------------------------------------------------------------------
     single = []

@@ -7,11 +7,12 @@
 //   2. full SVD-space score for the survivors (ComputeRemainDim, :76-95) -> sampled-threshold
 //      bounds (SampleSearch::RankBound) -> prune again.
 // Here a batch of queries runs as passes over all (query, user) pairs:
-//   * one tile kernel computes, for every pair, the partial score and its round-1 levels (a fast
-//     binary32 screen of the regression arithmetic; undecided pairs go to the reference's own
-//     arithmetic in a fix-up kernel), then the full score (partial + remainder, two separately
-//     accumulated sums added once, as the reference adds them) and the coarse group of its
-//     sampled-threshold bucket from a per-user summary of every 16th threshold;
+//   * one kernel scores every pair and decides its round-1 levels and the coarse group of its
+//     sampled-threshold bucket (a per-user summary of every 16th threshold): on the tensor cores
+//     (rkr_scores_tc.cu: int8 digit products, a rigorous bound against the reference's sums, exact
+//     resolution of the pairs the bound leaves undecided), or, where that path does not fit, as
+//     exact SIMT tiles (Round1Epi below: exact scores, a fast binary32 screen of the regression
+//     arithmetic, undecided pairs fixed by the reference's own arithmetic);
 //   * round 2 is a streaming pass that marks the pairs that did not survive round 1 and counts the
 //     survivors by group;
 //   * the exact bucket is resolved only where the k-th bound and the class counts need it: for the

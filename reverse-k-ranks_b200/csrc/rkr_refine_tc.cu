@@ -349,9 +349,23 @@ __global__ void __launch_bounds__(kTcThreads, 1) refine_tc_kernel(TcArgs a) {
         constexpr float kSlack = 4e-7f;  // a few roundings here and in the reference's one add
         int cnt = 0, und = 0;
         const uint32_t lane_base = taddr + ((uint32_t) (32 * quad) << 16) + (uint32_t) (16 * cg);
+        // the items' norms of this warp's 16 columns, one column per lane (lanes 0-15), loaded a tile
+        // ahead and broadcast by shuffles
+        auto col_norms = [&](int i, float &nx, float &ny, float &rn) {
+            const int64_t it = (int64_t) (blockIdx.x + i * gridDim.x) * kTcN + 16 * cg + (lane & 15);
+            const bool in = i < my_tiles && it < a.n_item;
+            const float2 v = in ? __ldg(a.item_norm + it) : make_float2(0.0f, 0.0f);
+            nx = v.x;
+            ny = v.y;
+            rn = in && a.ipbound ? __ldg(a.item_rnorm + it) : 0.0f;
+        };
+        float nx_next, ny_next, rn_next;
+        col_norms(0, nx_next, ny_next, rn_next);
         for (int i = 0; i < my_tiles; i++) {
             const int b = i & 1;
             const int64_t c0 = (int64_t) (blockIdx.x + i * gridDim.x) * kTcN + 16 * cg;
+            const float nx_cur = nx_next, ny_cur = ny_next, rn_cur = rn_next;
+            col_norms(i + 1, nx_next, ny_next, rn_next);
             if (!mbar_wait(&bar_mma[b], (uint32_t) (i >> 1) & 1u, abort)) {
                 *abort = 1;
                 atomicExch(a.status, 1);
@@ -372,12 +386,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) refine_tc_kernel(TcArgs a) {
                     const int64_t it = c0 + j0 + jj;
                     const bool valid = e >= 0 && it < np;
                     const float left = __uint_as_float(L[jj]);
-                    const float2 bn = it < a.n_item ? __ldg(a.item_norm + it) : make_float2(0.0f, 0.0f);
+                    const float2 bn = make_float2(__shfl_sync(0xffffffffu, nx_cur, j0 + jj),
+                                                  __shfl_sync(0xffffffffu, ny_cur, j0 + jj));
+                    const float irn = __shfl_sync(0xffffffffu, rn_cur, j0 + jj);
                     const float dl = a.err_l * an.x * bn.x;
                     int mode = -1;  // -1: settled here; else the mode of the exact resolution
                     if (a.ipbound) {
                         const float rest = __uint_as_float(R[jj]);
-                        const float irn = it < a.n_item ? __ldg(a.item_rnorm + it) : 0.0f;
                         const float right = __fmul_rn(irn, un);
                         const float ub_hi = (left + dl) + right, ub_lo = (left - dl) + right;
                         const float lb_hi = (left + dl) - right, lb_lo = (left - dl) - right;

@@ -643,18 +643,42 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
 // rows are staged in shared memory once (they are contiguous in global memory), the queries' rows
 // come from L2.
 __global__ void __launch_bounds__(256, 2) scores_tc_exact_tile_kernel(ScArgs a, int n_tiles) {
-    extern __shared__ __align__(16) float rows[];
+    extern __shared__ __align__(128) float rows[];
+    __shared__ uint64_t bar;
+    __shared__ int failed;
     const int2 rng = a.tile_rng[(int64_t) blockIdx.y * n_tiles + blockIdx.x];
     if (rng.y == 0) return;
     const int64_t u0 = (int64_t) blockIdx.x * kScM;
     const int64_t n_rows = a.n_user - u0 < kScM ? a.n_user - u0 : kScM;
     const float *src = a.urow + u0 * a.dim;
-    const int n_f = (int) n_rows * a.dim, n_v = n_f >> 2;  // the tile starts 16-byte aligned (kScM * 4 | 16)
-    const float4 *src4 = reinterpret_cast<const float4 *>(src);
-    float4 *dst4 = reinterpret_cast<float4 *>(rows);
-    for (int v = threadIdx.x; v < n_v; v += blockDim.x) dst4[v] = __ldg(src4 + v);
+    // the tile's rows (contiguous, 16-byte aligned: kScM * 4 | 16) in one bulk copy; a tail that is not
+    // a whole 16 bytes by plain loads
+    const int n_f = (int) n_rows * a.dim, n_v = n_f >> 2;
+    const uint32_t bytes = (uint32_t) n_v * 16;
+    if (threadIdx.x == 0) {
+        failed = 0;
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        if (bytes) {
+            mbar_expect_tx(&bar, bytes);
+            bulk_g2s(rows, src, bytes, &bar);
+        } else {
+            mbar_arrive(&bar);
+        }
+    }
     for (int f = 4 * n_v + threadIdx.x; f < n_f; f += blockDim.x) rows[f] = __ldg(src + f);
     __syncthreads();
+    {
+        // every thread observes the copy's completion (bounded wait)
+        bool ok = false;
+        for (int it = 0; it < (1 << 22) && !ok; it++) ok = mbar_try(&bar, 0);
+        if (!ok) {
+            failed = 1;
+            atomicExch(a.status, 1);
+        }
+    }
+    __syncthreads();
+    if (failed) return;
     for (int i = threadIdx.x; i < rng.y; i += blockDim.x) {
         const int2 x = a.ovf[rng.x + i];
         exact_pair(a, x.y, x.x, a.thr_summ + (int64_t) x.y * ThrSummary::kMaxGroups, rows + (x.y - u0) * a.dim);

@@ -505,7 +505,9 @@ int refine_tc(rkr_index *ix, const RefineArgs &ra, cudaStream_t st, bool *done) 
         ix->tc_check_dim = ix->check_dim;
     }
     const int64_t cand_pad = (ra.n_cand + kTcTile - 1) / kTcTile * kTcTile;
-    const int list_cap = 1 << 22;
+    // undecided tests (about 0.4% of the candidates' items); past the list they are resolved in line
+    const int list_cap = (int) std::min<int64_t>(int64_t(1) << 26,
+                                                 std::max<int64_t>(int64_t(1) << 22, cand_pad * n_item / 128));
     RKR_TRY(ix->ws_tc.ensure(carve_bytes(sizeof(float) * (size_t) cand_pad * kp) + carve_bytes(sizeof(float2) * cand_pad) +
                              carve_bytes(sizeof(int4) * (size_t) list_cap) + carve_bytes(sizeof(int) * 2)));
     uint8_t *p = ix->ws_tc.as<uint8_t>();

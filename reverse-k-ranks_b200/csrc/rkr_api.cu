@@ -219,8 +219,8 @@ int rkr_index_destroy(rkr_index *ix) {
     if (ix->stream) cudaStreamSynchronize(ix->stream);
     for (DevBuf *b : {&ix->user, &ix->item, &ix->item_sorted, &ix->item_norm, &ix->item_rnorm, &ix->user_rnorm,
                       &ix->sample_rank, &ix->thr, &ix->thr_summ, &ix->reg_rank, &ix->reg, &ix->transfer_item, &ix->svd_user,
-                      &ix->svd_user_km, &ix->user_km, &ix->item_km, &ix->item_sorted_km, &ix->ws_km, &ix->item_tc,
-                      &ix->item_tc_norm, &ix->item_tc_us, &ix->item_tc_us_norm, &ix->ws_tc,
+                      &ix->svd_user_km, &ix->user_km, &ix->item_km, &ix->item_sorted_km, &ix->ws_km, &ix->ri_item_split,
+                      &ix->ri_imeta_split, &ix->ri_item_full, &ix->ri_imeta_full, &ix->ws_tc,
                       &ix->svd_unorm, &ix->qip_state, &ix->ws_query, &ix->ws_qtr, &ix->ws_qnorm, &ix->ws_bucket,
                       &ix->ws_bucket2, &ix->ws_levels, &ix->ws_cls, &ix->ws_counts, &ix->ws_hist, &ix->ws_res,
                       &ix->ws_cand, &ix->ws_cand_off, &ix->ws_refine, &ix->ws_rank, &ix->ws_out, &ix->ws_stats,
@@ -332,7 +332,8 @@ int rkr_index_size_bytes(const rkr_index *ix, uint64_t *bytes) {
                             &ix->sample_rank, &ix->thr, &ix->thr_summ, &ix->reg_rank, &ix->reg, &ix->transfer_item, &ix->svd_user,
                             &ix->svd_user_km, &ix->user_km, &ix->item_km, &ix->item_sorted_km, &ix->svd_unorm,
                             &ix->qip_state, &ix->sc_user_split, &ix->sc_umeta_split, &ix->sc_user_full,
-                            &ix->sc_umeta_full})
+                            &ix->sc_umeta_full, &ix->ri_item_split, &ix->ri_imeta_split, &ix->ri_item_full,
+                            &ix->ri_imeta_full})
         s += b->bytes;
     *bytes = s;
     return RKR_OK;

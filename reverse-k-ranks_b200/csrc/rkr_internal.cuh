@@ -870,11 +870,11 @@ struct rkr_index {
     rkr::DevBuf item_norm;     // [n_item], descending
     rkr::DevBuf item_rnorm;    // [n_item], norm of dims [check_dim, dim) of item_sorted
     rkr::DevBuf user_rnorm;    // [n_user], norm of dims [check_dim, dim) of user
-    // tensor-core refinement operands (built on first use for the current check_dim)
-    int tc_check_dim = -2;
+    // tensor-core refinement: item digit tiles, built on first use, of item_sorted split at check_dim
+    // (QS, QSRP) and of item unsplit (US)
     bool refine_tc_on = true;                 // refinement counts on the tensor cores where the shape fits
-    rkr::DevBuf item_tc, item_tc_norm;        // item_sorted, split at check_dim, TF32-rounded; norms of both parts
-    rkr::DevBuf item_tc_us, item_tc_us_norm;  // item (original order), unsplit
+    int ri_key_split = -2, ri_key_full = -2;  // the split the tiles were built for (-2: none)
+    rkr::DevBuf ri_item_split, ri_imeta_split, ri_item_full, ri_imeta_full;
     // tensor-core pair scores: user digit tiles for the SVD split at check_dim (QSRP) and unsplit (QS, US)
     bool scores_tc_on = true;
     int sc_key_split = -2, sc_key_full = -2;  // the split the tiles were built for (-2: none)

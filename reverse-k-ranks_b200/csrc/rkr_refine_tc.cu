@@ -1,185 +1,168 @@
-// rkr_refine_tc.cu -- the counting step of candidate refinement on the tensor cores (tcgen05, TF32).
+// rkr_refine_tc.cu -- the counting step of candidate refinement on the tensor cores (tcgen05, int8).
 //
 // Refinement counts, per candidate (user u, score qv) and item in the norm cut-off, the reference's
 // per-item test (RefineCPUIPBound::RefineRank, RefineCPUIPBound.hpp:93-150 with the split sums of
 // RefineCPUPartDimPartNorm.hpp:83-152; RefineCPU::RefineRank, RefineCPU.hpp:33-55 without the bound).
 // The test only asks on which side of a few thresholds a pair's scores fall: its partial score over
 // the first check_dim coordinates against lowq - right and highq + right, and its full score against
-// qv.  So the scores come from TF32 tensor-core passes (the partial and the remaining coordinates in
-// two TMEM accumulators), each with a bound on its distance to the reference's binary32 value; a
-// pair whose bound interval straddles a threshold is listed and decided by the reference's own
-// arithmetic (refine_tc_exact_kernel).
+// qv.  So the scores come from the int8 digit products of rkr_tc_common.cuh (exact integer
+// accumulation, the partial and the remaining coordinates in separate TMEM accumulators), each
+// with a rigorous bound on its distance to the reference's binary32 value; a pair whose bound
+// interval straddles a threshold is listed and decided by the reference's own arithmetic
+// (refine_tc_exact_kernel).
 //
-// Tiles.  A CTA holds 128 candidates (the MMA's M, TMEM lanes) in shared memory and walks a strided
-// share of the item tiles (64 items, the MMA's N) inside its candidates' norm cut-off, the item
-// operands double-buffered by bulk copies (items are stored in that tile layout) and the
-// accumulators double-buffered in TMEM, so that one tile's MMAs overlap the previous tile's
-// epilogue.  Warp 16 issues the copies and the MMAs; warps 0-15 run the epilogue (warp w: lane
-// quadrant w % 4, columns 16 (w / 4) .. + 16).
+// Items in groups.  Items are taken in the norm order (item_sorted; US counts over all items, in any
+// order) and cut into groups of 8 that share one power-of-two scale and one set of bound data (the
+// largest weighted and plain norms of the group).  A warp's 8 columns of a chunk are one group, so
+// each thread turns its candidate's bound and the six thresholds of the test into the digit units of
+// its (candidate, group) once per chunk, and a pair costs the combination of its accumulators, one
+// product (the reference's right = |item rest| |user rest|), three sums and six comparisons.
 //
-// Error bound.  Operands are rounded to TF32 (11 significant bits, round to nearest), so each
-// product is within 2^-10 (1 + 2^-12) |a b| of the exact one; the FP32 accumulation of a K step of
-// eight products into the accumulator is taken to cost at most 9 ulps of sum |a b| per step (each
-// product aligned with less than an ulp lost, one final rounding) plus 8; and the reference's
-// sequential sum of n terms at most n * 2^-24 / (1 - n 2^-24) sum |a b|.  Sum |a b| <= |a| |b|
-// (Cauchy-Schwarz) over each part.  The TF32 term dominates: the accumulation term is under 3% of it.
+// Tiles.  A CTA holds the digits of 128 candidates (the MMA's M, TMEM lanes) and walks a strided
+// share of the 32-item chunks inside its candidates' norm cut-off; the items' digit chunks are
+// bulk-copied and double-buffered, the accumulators double-buffered in TMEM, so that one chunk's
+// MMAs overlap the previous chunk's epilogue.  Warp 16 issues the copies and the MMAs; warps 0-15
+// run the epilogue (warp w: lane quadrant w % 4, columns 8 (w / 4) .. + 8 of each accumulator).
 #include <algorithm>
 #include <cstdio>
 
 #include "rkr_internal.cuh"
+#include "rkr_tc_common.cuh"
 
 namespace rkr {
 
 namespace {
 
-constexpr int kTcTile = 128;     // candidates per CTA (TMEM lanes)
-constexpr int kTcN = 64;         // items per tile (MMA N)
-constexpr int kTcEpiWarps = 16;  // warp w reads TMEM lane quadrant w % 4, columns 16 (w / 4) + [0, 16)
-constexpr int kTcThreads = 32 * (kTcEpiWarps + 1);
-constexpr int kTcMaxK = 208;     // the candidate tile and two item tiles fit in shared memory up to this K
+constexpr int kRfEpiWarps = 16;
+constexpr int kRfThreads = 32 * (kRfEpiWarps + 1);
+constexpr int kRfMaxKp = 224;  // the candidate tile and two item chunks fit in shared memory up to this K
+constexpr int kRfGroup = 8;    // items per group (a warp's columns of a chunk)
 
-__host__ __device__ inline int round8(int x) { return (x + 7) & ~7; }
+// Per candidate row, 2 float4: {2^e, weighted norms WL, WR, plain norm NL}, {NR, e (int bits), 0, 0}.
+// Per item group, 4 float4: {the reference's rest norms (item_rnorm) of the 8 items}, {2^e, WL max,
+// WR max, NL max}, {NR max, rest norm max, e (int bits), 0}.  Weighted norms as in part_coef, plain
+// norms the Euclidean norms of the two parts; all rounded up.
 
-// Nearest TF32 value (ties to even); infinities and NaN pass through.
-__device__ __forceinline__ float tf32_rne(float x) {
-    uint32_t u = __float_as_uint(x);
-    if ((u & 0x7f800000u) == 0x7f800000u) return x;
-    u = (u + 0xfffu + ((u >> 13) & 1u)) & ~0x1fffu;
-    return __uint_as_float(u);
-}
-
-// Rows [n][dim] (gathered through idx when given) to TF32 rows of kp values: coordinates [0, c) at
-// [0, c), coordinates [c, dim) at [c8, c8 + dim - c), zeros elsewhere; rows [n, n_pad) zero.  norms
-// gets (|first c coordinates|, |remaining coordinates|) of the unrounded row.  tiled: rows stored
-// as tiles of kTcN in the shared-memory layout of an MMA operand (element (r, k) of a tile at
-// ((k / 4) * (kTcN / 8) + r / 8) * 32 + (r % 8) * 4 + k % 4), else [n_pad][kp].  One warp per row.
-__global__ void tc_operand_kernel(const float *__restrict__ src, const int32_t *__restrict__ idx, int64_t n,
-                                  int64_t n_pad, int dim, int c, int c8, int kp, float *__restrict__ dst,
-                                  float2 *__restrict__ norms, int tiled) {
-    const int64_t r = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (r >= n_pad) return;
+// Rows to 4-digit tiles of tr rows (the layout of slice_rows_kernel), one block of 8 warps per 8 rows.
+// grouped: the 8 rows share the scale of their largest coordinate and write group data; else each
+// row has its own scale and writes row data.  A group or row with a non-finite coordinate or a scale
+// beyond 2^+-kScMaxExp gets 2^e = inf (its pairs all go to the exact path) and zero digits.
+__global__ void __launch_bounds__(256) rf_slice_kernel(const float *__restrict__ src, const int32_t *__restrict__ idx,
+                                                       int64_t n, int dim, int c, int cp, int kp, int tr, int grouped,
+                                                       const float *__restrict__ rnorm, int8_t *__restrict__ dst,
+                                                       float4 *__restrict__ row_meta, float4 *__restrict__ grp_meta) {
+    __shared__ float s_mx[kRfGroup], s_v[kRfGroup][5];
+    __shared__ int s_bad[kRfGroup];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t r = (int64_t) blockIdx.x * kRfGroup + warp;  // grid covers the padded rows exactly
     const float *row = r < n ? src + (idx ? (int64_t) idx[r] : r) * dim : nullptr;
-    float sl = 0.0f, sr = 0.0f;
+    float mx = 0.0f;
+    int bad = 0;
+    if (row)
+        for (int k = lane; k < dim; k += 32) {
+            const float v = row[k];
+            bad |= !isfinite(v);
+            mx = fmaxf(mx, fabsf(v));
+        }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        bad |= __shfl_xor_sync(0xffffffffu, bad, o);
+    }
+    if (grouped) {
+        if (lane == 0) {
+            s_mx[warp] = mx;
+            s_bad[warp] = bad;
+        }
+        __syncthreads();
+        mx = 0.0f;
+        bad = 0;
+#pragma unroll
+        for (int w = 0; w < kRfGroup; w++) {
+            mx = fmaxf(mx, s_mx[w]);
+            bad |= s_bad[w];
+        }
+    }
+    int e = 0;
+    if (mx > 0.0f) {
+        int x;
+        frexpf(mx, &x);  // mx = m 2^x, m in [0.5, 1): mx 2^-(x + 1) < 0.5
+        e = x + 1;
+    }
+    if (e > kScMaxExp || e < -kScMaxExp) bad = 1;
+    const float scale = bad ? 0.0f : ldexpf(1.0f, -e);
+    double wl = 0.0, wr = 0.0, nl = 0.0, nr = 0.0;
+    const size_t slice_bytes = (size_t) tr * kp;
+    int8_t *tb = dst + (size_t) (r / tr) * kScSlices * slice_bytes;
+    const int rr = (int) (r % tr);
     for (int p = lane; p < kp; p += 32) {
-        const int k = p < c8 ? (p < c ? p : -1) : (p - c8 + c < dim ? p - c8 + c : -1);
+        const int k = p < cp ? (p < c ? p : -1) : (p - cp + c < dim ? p - cp + c : -1);
         float v = 0.0f;
         if (row && k >= 0) {
             v = row[k];
-            if (k < c) sl = fmaf(v, v, sl);
-            else sr = fmaf(v, v, sr);
+            const int t = k < c ? k : k - c, m = k < c ? c : dim - c;
+            const double w = t == 0 ? m : m - t + 1, v2 = (double) v * v;
+            if (k < c) { wl += w * v2; nl += v2; }
+            else { wr += w * v2; nr += v2; }
         }
-        const int64_t at = tiled ? (r / kTcN) * kTcN * kp + ((p >> 2) * (kTcN / 8) + (r % kTcN) / 8) * 32 +
-                                       (r & 7) * 4 + (p & 3)
-                                 : r * kp + p;
-        dst[at] = tf32_rne(v);
+        float a = v * scale;  // exact: a power of two
+        const size_t off = (size_t) (p >> 4) * (tr * 16) + (rr >> 3) * 128 + (rr & 7) * 16 + (p & 15);
+#pragma unroll
+        for (int s = 0; s < kScSlices; s++) {
+            const float t = a * 128.0f;  // exact
+            const float d = rintf(t);    // |t| < 64
+            a = t - d;                   // exact, |a| <= 0.5
+            tb[s * slice_bytes + off] = (int8_t) (int) d;
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        sl += __shfl_xor_sync(0xffffffffu, sl, o);
-        sr += __shfl_xor_sync(0xffffffffu, sr, o);
+        wl += __shfl_xor_sync(0xffffffffu, wl, o);
+        wr += __shfl_xor_sync(0xffffffffu, wr, o);
+        nl += __shfl_xor_sync(0xffffffffu, nl, o);
+        nr += __shfl_xor_sync(0xffffffffu, nr, o);
     }
-    if (lane == 0) norms[r] = make_float2(sqrtf(sl), sqrtf(sr));
-}
-
-// ---- tcgen05 helpers ----------------------------------------------------------------------------
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t) __cvta_generic_to_shared(p); }
-
-// Shared-memory matrix descriptor, K-major without swizzle: 8-row x 16-byte core matrices, lbo the
-// byte distance between the two core matrices of a K step, sbo between groups of 8 rows.
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-    uint64_t d = (uint64_t) ((saddr >> 4) & 0x3FFF);
-    d |= (uint64_t) ((lbo >> 4) & 0x3FFF) << 16;
-    d |= (uint64_t) ((sbo >> 4) & 0x3FFF) << 32;
-    d |= (uint64_t) 1 << 46;  // descriptor version of sm_100
-    return d;
-}
-
-// Instruction descriptor: kind::tf32, A and B K-major TF32, FP32 accumulator, M = 128, N = 64.
-constexpr uint32_t kIdescTf32 = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t) (kTcN >> 3) << 17) |
-                                ((uint32_t) (kTcTile >> 4) << 24);
-
-__device__ __forceinline__ void umma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t"
-        "}\n" ::"r"(d_tmem), "l"(a), "l"(b), "r"(kIdescTf32), "r"(accumulate) : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld4(uint32_t addr, uint32_t (&v)[4]) {
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
-                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
-                 : "r"(addr));
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t (&v)[16]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
-          "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-        : "r"(addr));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *b, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *b, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t *b) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint64_t *b, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok) : "r"(smem_u32(b)), "r"(parity) : "memory");
-    return ok != 0;
-}
-// Bounded wait; gives up early when another thread of the CTA has given up.
-__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity, volatile int *abort) {
-    for (int it = 0; it < (1 << 22); it++) {
-        if (mbar_try(b, parity)) return true;
-        if (*abort) return false;
+    const float E = bad ? INFINITY : ldexpf(1.0f, e);
+    const float WL = __double2float_ru(sqrt(wl * (1.0 + 1e-12))), WR = __double2float_ru(sqrt(wr * (1.0 + 1e-12)));
+    const float NL = __double2float_ru(sqrt(nl * (1.0 + 1e-12))), NR = __double2float_ru(sqrt(nr * (1.0 + 1e-12)));
+    if (!grouped) {
+        if (lane == 0) {
+            row_meta[2 * r] = make_float4(E, WL, WR, NL);
+            row_meta[2 * r + 1] = make_float4(NR, __int_as_float(bad ? 0 : e), 0.0f, 0.0f);
+        }
+        return;
     }
-    return false;
+    if (lane == 0) {
+        s_v[warp][0] = WL;
+        s_v[warp][1] = WR;
+        s_v[warp][2] = NL;
+        s_v[warp][3] = NR;
+        s_v[warp][4] = r < n && rnorm ? rnorm[r] : 0.0f;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float m[5] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+        for (int w = 0; w < kRfGroup; w++)
+            for (int j = 0; j < 5; j++) m[j] = fmaxf(m[j], s_v[w][j]);
+        float4 *g = grp_meta + 4 * blockIdx.x;
+        g[0] = make_float4(s_v[0][4], s_v[1][4], s_v[2][4], s_v[3][4]);
+        g[1] = make_float4(s_v[4][4], s_v[5][4], s_v[6][4], s_v[7][4]);
+        g[2] = make_float4(E, m[0], m[1], m[2]);
+        g[3] = make_float4(m[3], m[4], __int_as_float(bad ? 0 : e), 0.0f);
+    }
 }
-// Plain (non-multicast) bulk copy global -> this CTA's shared memory, completing on an mbarrier.
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld32(uint32_t addr, uint32_t (&v)[32]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]),
-          "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]), "=r"(v[16]),
-          "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]),
-          "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-        : "r"(addr));
-}
-
-// ---- the tile kernel -------------------------------------------------------------------------------
 
 struct TcArgs {
-    const float *cand, *item;                  // TF32 operands, [rows][kp]
-    const float2 *cand_norm, *item_norm;       // norms of the two parts
+    const int8_t *cand_sl, *item_sl;           // digit tiles: candidates (kScM rows), items (kScN rows)
+    const float4 *cand_meta, *grp_meta;        // row data (2 float4 per candidate), group data (4 per group)
     const float *item_rnorm, *user_rnorm;      // the reference's remaining-coordinate norms (bound test)
-    const float *user_rows, *item_rows;        // exact rows for undecided pairs (item_rows in the item order)
+    const float *user_rows, *item_rows;        // exact rows for undecided pairs (item_rows: item_sorted)
     const int32_t *ref_idx, *ref_user, *n_ref, *nproc;
     const float *qip;
     int32_t *rank, *undecided;
     int64_t n_item;
-    int dim, c, c8, kp, ipbound;
-    float err_l, err_r;                        // bound coefficients of the two parts
+    int dim, c, kp, ksplit, ksteps, ipbound;
+    float cl, kl, cr, kr;                      // bound coefficients of the two parts (part_coef)
     int4 *list;                                // undecided pairs: (candidate, user, item, mode)
     int *list_count, *status;
     int list_cap;
@@ -217,117 +200,121 @@ __device__ __noinline__ void exact_pair_now(TcArgs a, int e, int u, int64_t it, 
     if (und) atomicAdd(a.undecided + e, und);
 }
 
-__global__ void __launch_bounds__(kTcThreads, 1) refine_tc_kernel(TcArgs a) {
+// 2^k as a float, k in [-126, 127].
+__device__ __forceinline__ float pow2f(int k) { return __int_as_float((k + 127) << 23); }
+
+__global__ void __launch_bounds__(kRfThreads, 1) refine_tc_kernel(TcArgs a) {
     extern __shared__ __align__(1024) uint8_t tc_smem[];
-    __shared__ uint64_t bar_b[2], bar_mma[2], bar_free[2];
+    __shared__ uint64_t bar_a, bar_b[2], bar_mma[2], bar_free[2];
     __shared__ uint32_t tslot;
-    __shared__ int e_s[kTcTile], np_s[kTcTile], u_s[kTcTile], max_np, abort_flag;
-    __shared__ float qv_s[kTcTile], un_s[kTcTile];
-    __shared__ float2 an_s[kTcTile];
+    __shared__ int e_s[kScM], np_s[kScM], u_s[kScM], max_np, abort_flag;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int64_t r0 = (int64_t) blockIdx.y * kTcTile;
+    const int64_t r0 = (int64_t) blockIdx.y * kScM;
     const int n_ref = *a.n_ref;
     if (r0 >= n_ref) return;
     volatile int *abort = &abort_flag;
-    if (tid < kTcTile) {
+    if (tid < kScM) {
         const int64_t r = r0 + tid;
         int e = -1, np = 0, u = 0;
-        float qv = 0.0f, un = 0.0f;
-        float2 an = make_float2(0.0f, 0.0f);
         if (r < n_ref) {
             e = a.ref_idx[r];
             np = a.nproc[e];
-            qv = a.qip[e];
             u = a.ref_user[r];
-            un = a.ipbound ? a.user_rnorm[u] : 0.0f;
-            an = a.cand_norm[r];
         }
-        e_s[tid] = e; np_s[tid] = np; u_s[tid] = u; qv_s[tid] = qv; un_s[tid] = un; an_s[tid] = an;
+        e_s[tid] = e; np_s[tid] = np; u_s[tid] = u;
     }
     if (tid == 0) {
         max_np = 0;
         abort_flag = 0;
     }
     __syncthreads();
-    if (tid < kTcTile) atomicMax(&max_np, np_s[tid]);
+    if (tid < kScM) atomicMax(&max_np, np_s[tid]);
     __syncthreads();
-    // this CTA's item tiles: s, s + gridDim.x, ... below the candidates' largest cut-off
-    const int n_tiles = (max_np + kTcN - 1) / kTcN;
-    const int my_tiles = n_tiles > (int) blockIdx.x ? (n_tiles - (int) blockIdx.x + (int) gridDim.x - 1) / (int) gridDim.x : 0;
-    if (my_tiles == 0) return;
+    // this CTA's item chunks: s, s + gridDim.x, ... below the candidates' largest cut-off
+    const int n_chunks = (max_np + kScN - 1) / kScN;
+    const int mine = n_chunks > (int) blockIdx.x ? (n_chunks - (int) blockIdx.x + (int) gridDim.x - 1) / (int) gridDim.x : 0;
+    if (mine == 0) return;
 
-    // candidates into shared memory as K-major core matrices: element (row r, k) at
-    // ((k / 4) * 16 + r / 8) * 128 + (r % 8) * 16 + (k % 4) * 4 bytes; then two item tile buffers
-    const int kp = a.kp, ch = kp / 4;
-    float *sa = reinterpret_cast<float *>(tc_smem);
-    uint8_t *sb = reinterpret_cast<uint8_t *>(sa + kTcTile * kp);
-    const uint32_t b_bytes = (uint32_t) (sizeof(float) * kTcN * kp);
-    for (int idx = tid; idx < kTcTile * ch; idx += kTcThreads) {
-        const int r = idx / ch, j = idx % ch;
-        const int off = (j * (kTcTile / 8) + (r >> 3)) * 32 + (r & 7) * 4;
-        cp_async16(sa + off, a.cand + (r0 + r) * kp + 4 * j, true);
-    }
-    cp_async_commit();
-    cp_async_wait<0>();
+    const int kp = a.kp;
+    const uint32_t a_bytes = (uint32_t) (kScSlices * kScM * kp), b_bytes = (uint32_t) (kScSlices * kScN * kp);
+    uint8_t *sA = tc_smem;
+    uint8_t *sB = sA + a_bytes;
     if (tid == 0) {
+        mbar_init(&bar_a, 1);
         for (int b = 0; b < 2; b++) {
             mbar_init(&bar_b[b], 1);
             mbar_init(&bar_mma[b], 1);
-            mbar_init(&bar_free[b], kTcEpiWarps);
+            mbar_init(&bar_free[b], kRfEpiWarps);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;" ::"r"(smem_u32(&tslot))
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(&tslot))
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t taddr = tslot;
-    const int ksplit = a.c8 / 8, ksteps = kp / 8;
-    const uint8_t *item_tiles = reinterpret_cast<const uint8_t *>(a.item);
+    const bool has_rest = a.ksteps > a.ksplit;
+    const uint32_t buf_cols = (uint32_t) ((has_rest ? 8 : 4) * kScN);
 
-    if (warp == kTcEpiWarps) {
+    if (warp == kRfEpiWarps) {
         // ---- copies and MMAs (one thread) ----
         if (lane == 0) {
             bool ok = true;
             int last = -1;
-            for (int i = 0; i < 2 && i < my_tiles; i++) {
+            mbar_expect_tx(&bar_a, a_bytes);
+            bulk_g2s(sA, a.cand_sl + (size_t) blockIdx.y * a_bytes, a_bytes, &bar_a);
+            for (int i = 0; i < 2 && i < mine; i++) {
                 const int t = blockIdx.x + i * gridDim.x;
                 mbar_expect_tx(&bar_b[i], b_bytes);
-                bulk_g2s(sb + (size_t) i * b_bytes, item_tiles + (size_t) t * b_bytes, b_bytes, &bar_b[i]);
+                bulk_g2s(sB + (size_t) i * b_bytes, a.item_sl + (size_t) t * b_bytes, b_bytes, &bar_b[i]);
             }
-            constexpr uint32_t kAChunk = (kTcTile / 8) * 128, kBChunk = (kTcN / 8) * 128;  // bytes per 4-value k chunk
-            for (int i = 0; ok && i < my_tiles; i++) {
+            ok = mbar_wait(&bar_a, 0, abort);
+            constexpr uint32_t kAChunk = kScM * 16, kBChunk = kScN * 16;  // bytes per 16-coordinate block
+            // descriptors: a base per operand buffer, slices and K steps as offsets of the start address
+            // (16-byte units, within the descriptor's 14-bit field: shared memory stays below 256 KB)
+            const uint64_t da0 = umma_desc(smem_u32(sA), kAChunk, 128);
+            const uint64_t db_0 = umma_desc(smem_u32(sB), kBChunk, 128);
+            const uint64_t db_1 = umma_desc(smem_u32(sB + b_bytes), kBChunk, 128);
+            const uint32_t a_slice = (uint32_t) (kScM * kp) >> 4, b_slice = (uint32_t) (kScN * kp) >> 4;
+            for (int i = 0; ok && i < mine; i++) {
                 const int b = i & 1;
                 const uint32_t ph = (uint32_t) (i >> 1) & 1u;
                 ok = mbar_wait(&bar_b[b], ph, abort);
                 if (ok && i >= 2) ok = mbar_wait(&bar_free[b], (uint32_t) ((i - 2) >> 1) & 1u, abort);
                 if (!ok) break;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t d0 = taddr + (uint32_t) b * (2 * kTcN);
-                const uint32_t sb0 = smem_u32(sb + (size_t) b * b_bytes);
-                for (int s = 0; s < ksteps; s++) {
-                    const uint64_t da = umma_desc(smem_u32(sa) + (uint32_t) s * 2 * kAChunk, kAChunk, 128);
-                    const uint64_t db = umma_desc(sb0 + (uint32_t) s * 2 * kBChunk, kBChunk, 128);
-                    if (s < ksplit) umma_tf32(d0, da, db, s > 0);
-                    else umma_tf32(d0 + kTcN, da, db, s > ksplit);
+                const uint32_t d0 = taddr + (uint32_t) b * buf_cols;
+                for (int s = 0; s < a.ksteps; s++) {
+                    const int part = s < a.ksplit ? 0 : 1;
+                    const bool first_s = s == 0 || s == a.ksplit;
+                    const uint64_t das = da0 + ((uint32_t) s * 2 * kAChunk >> 4);
+                    const uint64_t dbs = (b ? db_1 : db_0) + ((uint32_t) s * 2 * kBChunk >> 4);
+                    const uint32_t dp = d0 + (uint32_t) part * 4 * kScN;
+                    // digit products (A slice i, B slice j) into accumulator i + j, i + j <= 3
+                    constexpr int kI[10] = {0, 0, 1, 0, 1, 2, 0, 1, 2, 3}, kJ[10] = {0, 1, 0, 2, 1, 0, 3, 2, 1, 0};
+#pragma unroll
+                    for (int pi = 0; pi < 10; pi++) {
+                        const bool first_g = pi == 0 || pi == 1 || pi == 3 || pi == 6;
+                        umma_i8(dp + (uint32_t) (kI[pi] + kJ[pi]) * kScN, das + kI[pi] * a_slice, dbs + kJ[pi] * b_slice,
+                                !(first_s && first_g));
+                    }
                 }
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                                  smem_u32(&bar_mma[b]))
                              : "memory");
                 last = i;
-                if (i >= 1 && i + 1 < my_tiles) {
-                    // the previous tile's MMAs have read their items: refill that buffer
+                if (i >= 1 && i + 1 < mine) {
+                    // the previous chunk's MMAs have read its items: refill that buffer
                     const int pb = (i - 1) & 1;
                     ok = mbar_wait(&bar_mma[pb], (uint32_t) ((i - 1) >> 1) & 1u, abort);
                     if (!ok) break;
                     const int t = blockIdx.x + (i + 1) * gridDim.x;
                     mbar_expect_tx(&bar_b[pb], b_bytes);
-                    bulk_g2s(sb + (size_t) pb * b_bytes, item_tiles + (size_t) t * b_bytes, b_bytes, &bar_b[pb]);
+                    bulk_g2s(sB + (size_t) pb * b_bytes, a.item_sl + (size_t) t * b_bytes, b_bytes, &bar_b[pb]);
                 }
             }
             if (!ok) {
@@ -342,101 +329,131 @@ __global__ void __launch_bounds__(kTcThreads, 1) refine_tc_kernel(TcArgs a) {
         // ---- epilogue ----
         const int quad = warp & 3, cg = warp >> 2, row = 32 * quad + lane;
         const int e = e_s[row], np = np_s[row], u = u_s[row];
-        const float qv = qv_s[row], un = un_s[row];
-        const float2 an = an_s[row];
+        const float qv = e >= 0 ? a.qip[e] : 0.0f;
+        const float un = e >= 0 && a.ipbound ? a.user_rnorm[u] : 0.0f;
+        const float4 m0 = a.cand_meta[2 * (r0 + row)], m1 = a.cand_meta[2 * (r0 + row) + 1];
+        const float Eu = m0.x, NLu = m0.w, NRu = m1.x;
+        const int eu = __float_as_int(m1.y);
+        const float cWL = a.cl * m0.y, cWR = a.cr * m0.z;
         const float lowq = __fsub_rn(qv, 8e-3f), highq = __fadd_rn(qv, 8e-3f);
-        const bool has_rest = ksteps > ksplit;
-        constexpr float kSlack = 4e-7f;  // a few roundings here and in the reference's one add
+        // The bound in real units, per (candidate, group): the digit products' distance to the
+        // reference's sums (part_coef; the combination's roundings as 1.8e-7 |part| with |part| <=
+        // plain norm x plain norm), plus kSigma (|left| + right) or (|left| + |rest|) for the
+        // rounding of our own sum of the two terms and of the reference's, all times kSafe for the
+        // roundings of this arithmetic.
+        constexpr float kComb = 1.8e-7f, kSigma = 1.3e-7f, kSafe = 1.0f + 1.0f / 65536.0f;
         int cnt = 0, und = 0;
-        const uint32_t lane_base = taddr + ((uint32_t) (32 * quad) << 16) + (uint32_t) (16 * cg);
-        // the items' norms of this warp's 16 columns, one column per lane (lanes 0-15), loaded a tile
-        // ahead and broadcast by shuffles
-        auto col_norms = [&](int i, float &nx, float &ny, float &rn) {
-            const int64_t it = (int64_t) (blockIdx.x + i * gridDim.x) * kTcN + 16 * cg + (lane & 15);
-            const bool in = i < my_tiles && it < a.n_item;
-            const float2 v = in ? __ldg(a.item_norm + it) : make_float2(0.0f, 0.0f);
-            nx = v.x;
-            ny = v.y;
-            rn = in && a.ipbound ? __ldg(a.item_rnorm + it) : 0.0f;
+        const uint32_t lane_base = taddr + ((uint32_t) (32 * quad) << 16) + (uint32_t) (8 * cg);
+        // the warp's group data of chunk i, a chunk ahead: float q of the group's 16 in lane q (one
+        // coalesced load), handed out by shuffles
+        const float *gmeta = reinterpret_cast<const float *>(a.grp_meta);
+        auto grp = [&](int i) {
+            const int64_t gi = ((int64_t) (blockIdx.x + i * gridDim.x) * kScN + 8 * cg) / kRfGroup;
+            return i < mine && lane < 16 ? __ldg(gmeta + 16 * gi + lane) : 0.0f;
         };
-        float nx_next, ny_next, rn_next;
-        col_norms(0, nx_next, ny_next, rn_next);
-        for (int i = 0; i < my_tiles; i++) {
+        float gn = grp(0);
+        for (int i = 0; i < mine; i++) {
             const int b = i & 1;
-            const int64_t c0 = (int64_t) (blockIdx.x + i * gridDim.x) * kTcN + 16 * cg;
-            const float nx_cur = nx_next, ny_cur = ny_next, rn_cur = rn_next;
-            col_norms(i + 1, nx_next, ny_next, rn_next);
+            const int64_t c0 = (int64_t) (blockIdx.x + i * gridDim.x) * kScN + 8 * cg;
+            const float gv = gn;
+            gn = grp(i + 1);
             if (!mbar_wait(&bar_mma[b], (uint32_t) (i >> 1) & 1u, abort)) {
                 *abort = 1;
                 atomicExch(a.status, 1);
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t tbase = lane_base + (uint32_t) b * (2 * kTcN);
-            // four columns at a time (a compact loop body keeps the instruction cache warm); the
-            // accumulators are released after the last of them
-#pragma unroll 1
-            for (int j0 = 0; j0 < 16; j0 += 4) {
-                uint32_t L[4], R[4] = {0u, 0u, 0u, 0u};
-                tmem_ld4(tbase + (uint32_t) j0, L);
-                if (has_rest) tmem_ld4(tbase + kTcN + (uint32_t) j0, R);
+            float l[8], r[8];
+            {
+                uint32_t v0[8], v1[8], v2[8], v3[8];
+                const uint32_t base = lane_base + (uint32_t) b * buf_cols;
+                tmem_ld8(base, v0);
+                tmem_ld8(base + kScN, v1);
+                tmem_ld8(base + 2 * kScN, v2);
+                tmem_ld8(base + 3 * kScN, v3);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-                for (int jj = 0; jj < 4; jj++) {
-                    const int64_t it = c0 + j0 + jj;
-                    const bool valid = e >= 0 && it < np;
-                    const float left = __uint_as_float(L[jj]);
-                    const float2 bn = make_float2(__shfl_sync(0xffffffffu, nx_cur, j0 + jj),
-                                                  __shfl_sync(0xffffffffu, ny_cur, j0 + jj));
-                    const float irn = __shfl_sync(0xffffffffu, rn_cur, j0 + jj);
-                    const float dl = a.err_l * an.x * bn.x;
-                    int mode = -1;  // -1: settled here; else the mode of the exact resolution
-                    if (a.ipbound) {
-                        const float rest = __uint_as_float(R[jj]);
-                        const float right = __fmul_rn(irn, un);
-                        const float ub_hi = (left + dl) + right, ub_lo = (left - dl) + right;
-                        const float lb_hi = (left + dl) - right, lb_lo = (left - dl) - right;
-                        const bool skip = lowq > ub_hi + fabsf(ub_hi) * kSlack;       // skipped by the reference
-                        const bool noskip = lowq <= ub_lo - fabsf(ub_lo) * kSlack;
-                        const bool counted = noskip && highq < lb_lo - fabsf(lb_lo) * kSlack;  // counted on its bound
-                        const bool full = noskip && highq >= lb_hi + fabsf(lb_hi) * kSlack;    // scored in full
-                        const float tot = left + rest;
-                        const float dt = dl + a.err_r * an.y * bn.y + fabsf(tot) * kSlack;
-                        const bool hit = tot - dt >= qv, miss = tot + dt < qv;
-                        if (valid && !skip) {
-                            if (counted) cnt++;
-                            else if (full) {
-                                und++;
-                                cnt += hit;
-                                if (!hit && !miss) mode = kModeCountOnly;
-                            } else {
-                                mode = kModeFull;
-                            }
-                        }
-                    } else {
-                        const float d = dl + fabsf(left) * kSlack;
-                        if (valid) {
-                            if (left - d > qv) cnt++;
-                            else if (left + d > qv) mode = kModeFull;
-                        }
-                    }
-                    const unsigned need = __ballot_sync(0xffffffffu, mode >= 0);
-                    if (need) {
-                        const int leader = __ffs(need) - 1;
-                        int base = 0;
-                        if (lane == leader) base = atomicAdd(a.list_count, __popc(need));
-                        base = __shfl_sync(0xffffffffu, base, leader);
-                        if (mode >= 0) {
-                            const int slot = base + __popc(need & ((1u << lane) - 1));
-                            if (slot < a.list_cap) a.list[slot] = make_int4(e, u, (int) it, mode);
-                            else exact_pair_now(a, e, u, it, mode);
-                        }
-                    }
+                for (int j = 0; j < 8; j++) l[j] = combine4(v0[j], v1[j], v2[j], v3[j]);
+                if (has_rest) {
+                    tmem_ld8(base + 4 * kScN, v0);
+                    tmem_ld8(base + 5 * kScN, v1);
+                    tmem_ld8(base + 6 * kScN, v2);
+                    tmem_ld8(base + 7 * kScN, v3);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                    for (int j = 0; j < 8; j++) r[j] = combine4(v0[j], v1[j], v2[j], v3[j]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 8; j++) r[j] = 0.0f;
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(&bar_free[b]);
+            // thresholds of this (candidate, group) in digit units: the scores are 2^(eu + eg - 35)
+            // times the combined accumulators, and scaling by a power of two is exact
+            const float Eg = __shfl_sync(0xffffffffu, gv, 8), WLg = __shfl_sync(0xffffffffu, gv, 9);
+            const float WRg = __shfl_sync(0xffffffffu, gv, 10), NLg = __shfl_sync(0xffffffffu, gv, 11);
+            const float NRg = __shfl_sync(0xffffffffu, gv, 12), IRg = __shfl_sync(0xffffffffu, gv, 13);
+            const int eg = __float_as_int(__shfl_sync(0xffffffffu, gv, 14));
+            const float EE = Eu * Eg;
+            const float nl = NLu * NLg;
+            const float DL = fmaf(cWL, WLg, fmaf(EE, a.kl, kComb * nl));
+            const float inv = pow2f(35 - eu - eg);
+            const int nvalid = e < 0 ? 0 : (int) max((int64_t) 0, min((int64_t) 8, (int64_t) np - c0));
+            unsigned lmask = 0;  // 2 bits per column: 1 listed in full, 2 listed for its count
+            if (a.ipbound) {
+                const float DR = fmaf(cWR, WRg, fmaf(EE, a.kr, kComb * NRu * NRg));
+                const float Ms = fmaf(kSigma, fmaf(un, IRg, nl), DL) * kSafe;
+                const float Mt = fmaf(kSigma, fmaf(NRu, NRg, nl), DL + DR) * kSafe;
+                const float t_sk = __fadd_rd(lowq, -Ms) * inv, t_ns = __fadd_ru(lowq, Ms) * inv;
+                const float t_ct = __fadd_ru(highq, Ms) * inv, t_fu = __fadd_rd(highq, -Ms) * inv;
+                const float t_hi = __fadd_ru(qv, Mt) * inv, t_mi = __fadd_rd(qv, -Mt) * inv;
+                const float un_s = un * inv;
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const float rt = __shfl_sync(0xffffffffu, gv, j) * un_s;  // the reference's right, scaled
+                    const float s = l[j] + rt, d = l[j] - rt, t = l[j] + r[j];
+                    const bool act = j < nvalid && !(s < t_sk);          // not surely skipped
+                    const bool ns = s >= t_ns;                             // surely not skipped
+                    const bool c1 = ns && d > t_ct;                        // surely counted on its bound
+                    const bool f1 = ns && !c1 && d <= t_fu;                // surely scored in full
+                    const bool hi = t >= t_hi, mi = t < t_mi;
+                    cnt += act && (c1 || (f1 && hi));
+                    und += act && f1;
+                    const unsigned lf = act && !c1 && !f1, lc = act && f1 && !hi && !mi;
+                    lmask |= (lf | (lc << 1)) << (2 * j);
+                }
+            } else {
+                const float M = fmaf(kSigma, nl, DL) * kSafe;
+                const float t_hi = __fadd_ru(qv, M) * inv, t_lo = __fadd_rd(qv, -M) * inv;
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const bool act = j < nvalid;
+                    cnt += act && l[j] > t_hi;
+                    const unsigned lf = act && !(l[j] > t_hi) && !(l[j] <= t_lo);
+                    lmask |= lf << (2 * j);
+                }
+            }
+            if (__any_sync(0xffffffffu, lmask != 0)) {
+                // the listed pairs, appended by one atomic per column of the warp
+#pragma unroll 1
+                for (int j = 0; j < 8; j++) {
+                    const unsigned m = (lmask >> (2 * j)) & 3u;
+                    const unsigned need = __ballot_sync(0xffffffffu, m != 0);
+                    if (!need) continue;
+                    const int leader = __ffs(need) - 1;
+                    int base = 0;
+                    if (lane == leader) base = atomicAdd(a.list_count, __popc(need));
+                    base = __shfl_sync(0xffffffffu, base, leader);
+                    if (m) {
+                        const int mode = m == 1 ? kModeFull : kModeCountOnly;
+                        const int slot = base + __popc(need & ((1u << lane) - 1));
+                        if (slot < a.list_cap) a.list[slot] = make_int4(e, u, (int) (c0 + j), mode);
+                        else exact_pair_now(a, e, u, c0 + j, mode);
+                    }
+                }
+            }
         }
         if (e >= 0) {
             if (cnt) atomicAdd(a.rank + e, cnt);
@@ -447,7 +464,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) refine_tc_kernel(TcArgs a) {
     __syncthreads();
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;" ::"r"(taddr) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(taddr) : "memory");
     }
 }
 
@@ -471,12 +488,22 @@ template <typename T> T *carve_at(uint8_t *&p, size_t n) {
     return r;
 }
 
-// Bound coefficient of a part of n coordinates taken in `steps` tensor-core K steps.
-inline float part_err(int n, int steps) {
-    const double tf32 = 9.765625e-4 * (1.0 + 1.0 / 4096.0);          // 2^-10 (1 + 2^-12)
-    const double acc = (9.0 * steps + 8) * 1.1920928955078125e-7;    // 9 ulps of FP32 per K step, plus 8
-    const double ref = n * 5.9604644775390625e-8 / (1.0 - n * 5.96e-8);  // the reference's sequential sum
-    return (float) ((tf32 + acc + ref) * 1.01);
+// Shares of the item chunks per candidate tile: about 6-12 waves of one CTA per SM, the count whose
+// last wave is fullest.
+int64_t pick_shares(int64_t tiles, int64_t chunks) {
+    const int64_t sms = 148;
+    int64_t best = 1;
+    double best_eff = -1.0;
+    for (int64_t w = 6; w <= 12; w++) {
+        const int64_t s = std::max<int64_t>(1, std::min<int64_t>((chunks + 7) / 8, sms * w / tiles));
+        const int64_t total = s * tiles, waves = (total + sms - 1) / sms;
+        const double eff = (double) total / (double) (waves * sms);
+        if (eff > best_eff + 1e-9) {
+            best_eff = eff;
+            best = s;
+        }
+    }
+    return best;
 }
 
 }  // namespace
@@ -485,52 +512,54 @@ int refine_tc(rkr_index *ix, const RefineArgs &ra, cudaStream_t st, bool *done) 
     *done = false;
     const int dim = ix->dim;
     const int c = ra.ipbound ? ix->check_dim : dim;
-    const int c8 = round8(c), kp = c8 + round8(dim - c);
-    if (kp > kTcMaxK || ra.n_cand <= 0) return RKR_OK;
-    const int64_t n_item = ix->n_item, item_pad = (n_item + kTcN - 1) / kTcN * kTcN;
-    // item operands for the current check_dim
-    if (ix->tc_check_dim != ix->check_dim) {
-        const int cs = ix->check_dim, cs8 = round8(cs), kps = cs8 + round8(dim - cs), kpu = round8(dim);
-        RKR_TRY(ix->item_tc.ensure(sizeof(float) * (size_t) item_pad * kps));
-        RKR_TRY(ix->item_tc_norm.ensure(sizeof(float2) * (size_t) item_pad));
-        RKR_TRY(ix->item_tc_us.ensure(sizeof(float) * (size_t) item_pad * kpu));
-        RKR_TRY(ix->item_tc_us_norm.ensure(sizeof(float2) * (size_t) item_pad));
-        const unsigned g = (unsigned) ((item_pad * 32 + 255) / 256);
-        tc_operand_kernel<<<g, 256, 0, st>>>(ix->item_sorted.as<float>(), nullptr, n_item, item_pad, dim, cs, cs8, kps,
-                                             ix->item_tc.as<float>(), ix->item_tc_norm.as<float2>(), 1);
+    const int n1 = c, n2 = dim - c;
+    if (n1 <= 0 || n1 > kScMaxPart || n2 > kScMaxPart || ra.n_cand <= 0) return RKR_OK;
+    const int cp = round32(n1), kp = cp + round32(n2);
+    if (kp > kRfMaxKp) return RKR_OK;
+    const int64_t n_item = ix->n_item, item_pad = (n_item + kScN - 1) / kScN * kScN;
+    const int64_t cand_pad = (ra.n_cand + kScM - 1) / kScM * kScM;
+    if (cand_pad / kScM > 65535) return RKR_OK;  // the exact tiles take batches this large
+    // the items' digit chunks and group data for this split, in the norm order (built once, kept)
+    DevBuf &isl = ra.ipbound ? ix->ri_item_split : ix->ri_item_full;
+    DevBuf &imeta = ra.ipbound ? ix->ri_imeta_split : ix->ri_imeta_full;
+    int &key = ra.ipbound ? ix->ri_key_split : ix->ri_key_full;
+    if (key != c) {
+        key = -2;
+        RKR_TRY(isl.ensure((size_t) item_pad * kScSlices * kp));
+        RKR_TRY(imeta.ensure(sizeof(float4) * 4 * (size_t) (item_pad / kRfGroup)));
+        rf_slice_kernel<<<(unsigned) (item_pad / kRfGroup), 256, 0, st>>>(
+            ix->item_sorted.as<float>(), nullptr, n_item, dim, c, cp, kp, kScN, 1,
+            ra.ipbound ? ix->item_rnorm.as<float>() : nullptr, isl.as<int8_t>(), nullptr, imeta.as<float4>());
         RKR_CUDA(cudaGetLastError());
-        tc_operand_kernel<<<g, 256, 0, st>>>(ix->item.as<float>(), nullptr, n_item, item_pad, dim, dim, kpu, kpu,
-                                             ix->item_tc_us.as<float>(), ix->item_tc_us_norm.as<float2>(), 1);
-        RKR_CUDA(cudaGetLastError());
-        ix->tc_check_dim = ix->check_dim;
+        key = c;
     }
-    const int64_t cand_pad = (ra.n_cand + kTcTile - 1) / kTcTile * kTcTile;
-    // undecided tests (about 0.4% of the candidates' items); past the list they are resolved in line
+    // undecided tests (a small fraction of the candidates' items); past the list they are resolved in line
     const int list_cap = (int) std::min<int64_t>(int64_t(1) << 26,
-                                                 std::max<int64_t>(int64_t(1) << 22, cand_pad * n_item / 128));
-    RKR_TRY(ix->ws_tc.ensure(carve_bytes(sizeof(float) * (size_t) cand_pad * kp) + carve_bytes(sizeof(float2) * cand_pad) +
+                                                 std::max<int64_t>(int64_t(1) << 20, cand_pad * n_item / 1024));
+    RKR_TRY(ix->ws_tc.ensure(carve_bytes((size_t) cand_pad * kScSlices * kp) + carve_bytes(sizeof(float4) * 2 * cand_pad) +
                              carve_bytes(sizeof(int4) * (size_t) list_cap) + carve_bytes(sizeof(int) * 2)));
     uint8_t *p = ix->ws_tc.as<uint8_t>();
-    float *cand = carve_at<float>(p, (size_t) cand_pad * kp);
-    float2 *cand_norm = carve_at<float2>(p, cand_pad);
+    int8_t *cand = carve_at<int8_t>(p, (size_t) cand_pad * kScSlices * kp);
+    float4 *cand_meta = carve_at<float4>(p, 2 * cand_pad);
     int4 *list = carve_at<int4>(p, list_cap);
     int *counters = carve_at<int>(p, 2);
     RKR_CUDA(cudaMemsetAsync(counters, 0, sizeof(int) * 2, st));
+    // the candidates' rows (users gathered through ref_user, whose entries past n_ref are 0)
     timed(ix, st, "refine_tc_prep", [&] {
-        tc_operand_kernel<<<(unsigned) ((cand_pad * 32 + 255) / 256), 256, 0, st>>>(ra.user, ra.ref_user, ra.n_cand,
-                                                                                    cand_pad, dim, c, c8, kp, cand,
-                                                                                    cand_norm, 0);
+        rf_slice_kernel<<<(unsigned) (cand_pad / kRfGroup), 256, 0, st>>>(ra.user, ra.ref_user, ra.n_cand, dim, c, cp,
+                                                                          kp, kScM, 0, nullptr, cand, cand_meta,
+                                                                          nullptr);
     });
     RKR_CUDA(cudaGetLastError());
     TcArgs a;
-    a.cand = cand;
-    a.cand_norm = cand_norm;
-    a.item = ra.ipbound ? ix->item_tc.as<float>() : ix->item_tc_us.as<float>();
-    a.item_norm = ra.ipbound ? ix->item_tc_norm.as<float2>() : ix->item_tc_us_norm.as<float2>();
+    a.cand_sl = cand;
+    a.item_sl = isl.as<int8_t>();
+    a.cand_meta = cand_meta;
+    a.grp_meta = imeta.as<float4>();
     a.item_rnorm = ix->item_rnorm.as<float>();
     a.user_rnorm = ix->user_rnorm.as<float>();
     a.user_rows = ra.user;
-    a.item_rows = ra.ipbound ? ix->item_sorted.as<float>() : ix->item.as<float>();
+    a.item_rows = ix->item_sorted.as<float>();
     a.ref_idx = ra.ref_idx;
     a.ref_user = ra.ref_user;
     a.n_ref = ra.n_ref;
@@ -541,24 +570,21 @@ int refine_tc(rkr_index *ix, const RefineArgs &ra, cudaStream_t st, bool *done) 
     a.n_item = n_item;
     a.dim = dim;
     a.c = c;
-    a.c8 = c8;
     a.kp = kp;
+    a.ksplit = cp / 32;
+    a.ksteps = kp / 32;
     a.ipbound = ra.ipbound;
-    a.err_l = part_err(c, c8 / 8);
-    a.err_r = part_err(dim - c, (kp - c8) / 8);
+    part_coef(n1, a.cl, a.kl);
+    part_coef(n2, a.cr, a.kr);
     a.list = list;
     a.list_count = counters;
     a.status = counters + 1;
     a.list_cap = list_cap;
-    const size_t smem = sizeof(float) * (kTcTile + 2 * kTcN) * (size_t) kp;
+    const size_t smem = (size_t) kScSlices * kp * (kScM + 2 * kScN);
     RKR_CUDA(cudaFuncSetAttribute(refine_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-    // candidate tiles x strided shares of the item tiles: about two waves of CTAs
-    const int64_t cand_tiles = cand_pad / kTcTile;
-    const int64_t item_tiles = item_pad / kTcN;
-    const int64_t shares = std::max<int64_t>(1, std::min<int64_t>(item_tiles, (2 * 148 + cand_tiles - 1) / cand_tiles));
-    const dim3 grid((unsigned) shares, (unsigned) cand_tiles);
-    if (grid.y > 65535) return RKR_OK;  // the exact tiles take batches this large
-    timed(ix, st, "refine_tc", [&] { refine_tc_kernel<<<grid, kTcThreads, smem, st>>>(a); });
+    const int64_t cand_tiles = cand_pad / kScM;
+    const dim3 grid((unsigned) pick_shares(cand_tiles, item_pad / kScN), (unsigned) cand_tiles);
+    timed(ix, st, "refine_tc", [&] { refine_tc_kernel<<<grid, kRfThreads, smem, st>>>(a); });
     RKR_CUDA(cudaGetLastError());
     timed(ix, st, "refine_tc_exact", [&] { refine_tc_exact_kernel<<<148 * 4, 256, 0, st>>>(a); });
     RKR_CUDA(cudaGetLastError());

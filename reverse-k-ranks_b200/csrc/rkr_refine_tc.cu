@@ -21,8 +21,12 @@
 // Tiles.  A CTA holds the digits of 128 candidates (the MMA's M, TMEM lanes) and walks a strided
 // share of the 32-item chunks inside its candidates' norm cut-off; the items' digit chunks are
 // bulk-copied and double-buffered, the accumulators double-buffered in TMEM, so that one chunk's
-// MMAs overlap the previous chunk's epilogue.  Warp 16 issues the copies and the MMAs; warps 0-15
-// run the epilogue (warp w: lane quadrant w % 4, columns 8 (w / 4) .. + 8 of each accumulator).
+// MMAs overlap the previous chunk's epilogue.  The chunk's four digit slices sit side by side behind
+// three blocks of zeros, so that one MMA of N = 128 per candidate slice i and K step fills the four
+// digit-group accumulators at once (4 MMAs per K step instead of the 10 digit pairs; the operand
+// traffic of shared memory, which bounds these small MMAs, falls by 1.6x).  Warp 16 runs the
+// copies and the MMAs (one elected lane issues); warps 0-15 run the epilogue (warp w: lane
+// quadrant w % 4, columns 8 (w / 4) .. + 8 of each accumulator).
 #include <algorithm>
 #include <cstdio>
 
@@ -35,7 +39,7 @@ namespace {
 
 constexpr int kRfEpiWarps = 16;
 constexpr int kRfThreads = 32 * (kRfEpiWarps + 1);
-constexpr int kRfMaxKp = 224;  // the candidate tile and two item chunks fit in shared memory up to this K
+constexpr int kRfMaxKp = 224;  // the candidate tile and two stacked item buffers fit in shared memory up to this K
 constexpr int kRfGroup = 8;    // items per group (a warp's columns of a chunk)
 
 // Per candidate row, 2 float4: {2^e, weighted norms WL, WR, plain norm NL}, {NR, e (int bits), 0, 0}.
@@ -43,9 +47,9 @@ constexpr int kRfGroup = 8;    // items per group (a warp's columns of a chunk)
 // WR max, NL max}, {NR max, rest norm max, e (int bits), 0}.  Weighted norms as in part_coef, plain
 // norms the Euclidean norms of the two parts; all rounded up.
 
-// Rows to 4-digit tiles of tr rows (the layout of slice_rows_kernel), one block of 8 warps per 8 rows.
-// grouped: the 8 rows share the scale of their largest coordinate and write group data; else each
-// row has its own scale and writes row data.  A group or row with a non-finite coordinate or a scale
+// Rows to 4-digit tiles of tr rows, one block of 8 warps per 8 rows.  grouped (items, the B operand):
+// the 8 rows share the scale of their largest coordinate, write group data and take the stacked
+// layout of digit_off; else (candidates, the A operand) each row has its own scale and writes row data.  A group or row with a non-finite coordinate or a scale
 // beyond 2^+-kScMaxExp gets 2^e = inf (its pairs all go to the exact path) and zero digits.
 __global__ void __launch_bounds__(256) rf_slice_kernel(const float *__restrict__ src, const int32_t *__restrict__ idx,
                                                        int64_t n, int dim, int c, int cp, int kp, int tr, int grouped,
@@ -106,7 +110,7 @@ __global__ void __launch_bounds__(256) rf_slice_kernel(const float *__restrict__
             else { wr += w * v2; nr += v2; }
         }
         float a = v * scale;  // exact: a power of two
-        const size_t off = (size_t) (p >> 4) * (tr * 16) + (rr >> 3) * 128 + (rr & 7) * 16 + (p & 15);
+        const size_t off = digit_off(rr, p, tr, kp, grouped);  // items: the stacked B layout
 #pragma unroll
         for (int s = 0; s < kScSlices; s++) {
             const float t = a * 128.0f;  // exact
@@ -236,9 +240,18 @@ __global__ void __launch_bounds__(kRfThreads, 1) refine_tc_kernel(TcArgs a) {
     if (mine == 0) return;
 
     const int kp = a.kp;
-    const uint32_t a_bytes = (uint32_t) (kScSlices * kScM * kp), b_bytes = (uint32_t) (kScSlices * kScN * kp);
+    // shared memory: the candidate tile (A), then two item buffers of 7 blocks of kScN rows: three blocks
+    // of zeros and the chunk's 4 digit slices, so that the N = 128 operand starting 3 - i blocks in
+    // holds in column block g the item slice g - i (zeros for g < i)
+    const uint32_t a_bytes = (uint32_t) (kScSlices * kScM * kp), blk = (uint32_t) (kScN * kp);
+    const uint32_t b_bytes = kScSlices * blk, buf_bytes = (kScSlices + 3) * blk;
     uint8_t *sA = tc_smem;
     uint8_t *sB = sA + a_bytes;
+    for (uint32_t o = tid * 16; o < 3 * blk; o += kRfThreads * 16) {
+        *reinterpret_cast<uint4 *>(sB + o) = make_uint4(0u, 0u, 0u, 0u);
+        *reinterpret_cast<uint4 *>(sB + buf_bytes + o) = make_uint4(0u, 0u, 0u, 0u);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the zeros, for the MMAs' reads
     if (tid == 0) {
         mbar_init(&bar_a, 1);
         for (int b = 0; b < 2; b++) {
@@ -261,70 +274,78 @@ __global__ void __launch_bounds__(kRfThreads, 1) refine_tc_kernel(TcArgs a) {
     const uint32_t buf_cols = (uint32_t) ((has_rest ? 8 : 4) * kScN);
 
     if (warp == kRfEpiWarps) {
-        // ---- copies and MMAs (one thread) ----
-        if (lane == 0) {
-            bool ok = true;
-            int last = -1;
+        // ---- copies and MMAs: the warp runs the loop, one elected lane issues ----
+        bool ok = true;
+        int last = -1;
+        if (elect_one()) {
             mbar_expect_tx(&bar_a, a_bytes);
             bulk_g2s(sA, a.cand_sl + (size_t) blockIdx.y * a_bytes, a_bytes, &bar_a);
             for (int i = 0; i < 2 && i < mine; i++) {
                 const int t = blockIdx.x + i * gridDim.x;
                 mbar_expect_tx(&bar_b[i], b_bytes);
-                bulk_g2s(sB + (size_t) i * b_bytes, a.item_sl + (size_t) t * b_bytes, b_bytes, &bar_b[i]);
+                bulk_g2s(sB + i * buf_bytes + 3 * blk, a.item_sl + (size_t) t * b_bytes, b_bytes, &bar_b[i]);
             }
-            ok = mbar_wait(&bar_a, 0, abort);
-            constexpr uint32_t kAChunk = kScM * 16, kBChunk = kScN * 16;  // bytes per 16-coordinate block
-            // descriptors: a base per operand buffer, slices and K steps as offsets of the start address
-            // (16-byte units, within the descriptor's 14-bit field: shared memory stays below 256 KB)
-            const uint64_t da0 = umma_desc(smem_u32(sA), kAChunk, 128);
-            const uint64_t db_0 = umma_desc(smem_u32(sB), kBChunk, 128);
-            const uint64_t db_1 = umma_desc(smem_u32(sB + b_bytes), kBChunk, 128);
-            const uint32_t a_slice = (uint32_t) (kScM * kp) >> 4, b_slice = (uint32_t) (kScN * kp) >> 4;
-            for (int i = 0; ok && i < mine; i++) {
-                const int b = i & 1;
-                const uint32_t ph = (uint32_t) (i >> 1) & 1u;
-                ok = mbar_wait(&bar_b[b], ph, abort);
-                if (ok && i >= 2) ok = mbar_wait(&bar_free[b], (uint32_t) ((i - 2) >> 1) & 1u, abort);
-                if (!ok) break;
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t d0 = taddr + (uint32_t) b * buf_cols;
-                for (int s = 0; s < a.ksteps; s++) {
-                    const int part = s < a.ksplit ? 0 : 1;
-                    const bool first_s = s == 0 || s == a.ksplit;
-                    const uint64_t das = da0 + ((uint32_t) s * 2 * kAChunk >> 4);
-                    const uint64_t dbs = (b ? db_1 : db_0) + ((uint32_t) s * 2 * kBChunk >> 4);
-                    const uint32_t dp = d0 + (uint32_t) part * 4 * kScN;
-                    // digit products (A slice i, B slice j) into accumulator i + j, i + j <= 3
-                    constexpr int kI[10] = {0, 0, 1, 0, 1, 2, 0, 1, 2, 3}, kJ[10] = {0, 1, 0, 2, 1, 0, 3, 2, 1, 0};
+        }
+        __syncwarp();
+        ok = __all_sync(0xffffffffu, mbar_wait(&bar_a, 0, abort));
+        // descriptors (addresses in 16-byte units, within the 14-bit field: shared memory < 256 KB):
+        // A K blocks of kScM rows (K step s at s * 2 * kScM * 16 bytes, slice i at i * kScM * kp); the
+        // stacked B in row groups of kp * 8 bytes, K step s at s * 256 bytes
+        constexpr uint32_t kAChunk = kScM * 16;
+        const uint64_t da0 = umma_desc(smem_u32(sA), kAChunk, 128);
+        const uint64_t db0 = umma_desc(smem_u32(sB), 128, (uint32_t) kp * 8);
+        const uint32_t a_slice = (uint32_t) (kScM * kp) >> 4, b_blk = blk >> 4, b_buf = buf_bytes >> 4;
+        for (int i = 0; ok && i < mine; i++) {
+            const int b = i & 1;
+            const uint32_t ph = (uint32_t) (i >> 1) & 1u;
+            ok = mbar_wait(&bar_b[b], ph, abort);
+            if (ok && i >= 2) ok = mbar_wait(&bar_free[b], (uint32_t) ((i - 2) >> 1) & 1u, abort);
+            ok = __all_sync(0xffffffffu, ok);
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t d0 = taddr + (uint32_t) b * buf_cols;
+            const uint64_t dbb = db0 + (uint32_t) b * b_buf;
+            for (int s = 0; s < a.ksteps; s++) {
+                const int part = s < a.ksplit ? 0 : 1;
+                const bool first_s = s == 0 || s == a.ksplit;
+                const uint64_t das = da0 + ((uint32_t) s * 2 * kAChunk >> 4);
+                const uint64_t dbs = dbb + (uint32_t) s * 16;
+                const uint32_t dp = d0 + (uint32_t) part * 4 * kScN;
+                // candidate slice i against the stacked items from block 3 - i: column block g gets
+                // the products of digit pair (i, g - i), g = 0..3
+                if (elect_one()) {
 #pragma unroll
-                    for (int pi = 0; pi < 10; pi++) {
-                        const bool first_g = pi == 0 || pi == 1 || pi == 3 || pi == 6;
-                        umma_i8(dp + (uint32_t) (kI[pi] + kJ[pi]) * kScN, das + kI[pi] * a_slice, dbs + kJ[pi] * b_slice,
-                                !(first_s && first_g));
-                    }
+                    for (int si = 0; si < kScSlices; si++)
+                        umma_i8(dp, das + si * a_slice, dbs + (3 - si) * b_blk, !(first_s && si == 0), kIdescI8Stacked);
                 }
+                __syncwarp();
+            }
+            if (elect_one())
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                                  smem_u32(&bar_mma[b]))
                              : "memory");
-                last = i;
-                if (i >= 1 && i + 1 < mine) {
-                    // the previous chunk's MMAs have read its items: refill that buffer
-                    const int pb = (i - 1) & 1;
-                    ok = mbar_wait(&bar_mma[pb], (uint32_t) ((i - 1) >> 1) & 1u, abort);
-                    if (!ok) break;
+            __syncwarp();
+            last = i;
+            if (i >= 1 && i + 1 < mine) {
+                // the previous chunk's MMAs have read its items: refill that buffer
+                const int pb = (i - 1) & 1;
+                ok = __all_sync(0xffffffffu, mbar_wait(&bar_mma[pb], (uint32_t) ((i - 1) >> 1) & 1u, abort));
+                if (!ok) break;
+                if (elect_one()) {
                     const int t = blockIdx.x + (i + 1) * gridDim.x;
                     mbar_expect_tx(&bar_b[pb], b_bytes);
-                    bulk_g2s(sB + (size_t) pb * b_bytes, a.item_sl + (size_t) t * b_bytes, b_bytes, &bar_b[pb]);
+                    bulk_g2s(sB + pb * buf_bytes + 3 * blk, a.item_sl + (size_t) t * b_bytes, b_bytes, &bar_b[pb]);
                 }
+                __syncwarp();
             }
-            if (!ok) {
-                *abort = 1;
-                atomicExch(a.status, 1);
-            }
-            if (last >= 0)  // the last committed MMAs finish on their own: wait for them (bounded)
-                for (int it = 0; it < (1 << 22) && !mbar_try(&bar_mma[last & 1], (uint32_t) (last >> 1) & 1u); it++) {
-                }
         }
+        if (!ok && lane == 0) {
+            *abort = 1;
+            atomicExch(a.status, 1);
+        }
+        if (last >= 0)  // the last committed MMAs finish on their own: wait for them (bounded)
+            for (int it = 0; it < (1 << 22) && !mbar_try(&bar_mma[last & 1], (uint32_t) (last >> 1) & 1u); it++) {
+            }
     } else {
         // ---- epilogue ----
         const int quad = warp & 3, cg = warp >> 2, row = 32 * quad + lane;
@@ -580,7 +601,7 @@ int refine_tc(rkr_index *ix, const RefineArgs &ra, cudaStream_t st, bool *done) 
     a.list_count = counters;
     a.status = counters + 1;
     a.list_cap = list_cap;
-    const size_t smem = (size_t) kScSlices * kp * (kScM + 2 * kScN);
+    const size_t smem = (size_t) kp * (kScSlices * kScM + 2 * (kScSlices + 3) * kScN);
     RKR_CUDA(cudaFuncSetAttribute(refine_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     const int64_t cand_tiles = cand_pad / kScM;
     const dim3 grid((unsigned) pick_shares(cand_tiles, item_pad / kScN), (unsigned) cand_tiles);

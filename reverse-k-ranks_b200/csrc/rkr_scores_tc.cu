@@ -582,7 +582,8 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, PairScre
         RKR_TRY(um.ensure(sizeof(float4) * (size_t) n_pad));
         const float *src = (call.qsrp ? ix->svd_user : ix->user).as<float>();
         const unsigned g = (unsigned) ((n_pad * 32 + 255) / 256);
-        slice_rows_kernel<<<g, 256, 0, st>>>(src, nullptr, U, n_pad, dim, c, cp, kp, kScM, ub.as<int8_t>(), um.as<float4>());
+        slice_rows_kernel<<<g, 256, 0, st>>>(src, nullptr, U, n_pad, dim, c, cp, kp, kScM, 0, ub.as<int8_t>(),
+                                             um.as<float4>());
         RKR_CUDA(cudaGetLastError());
         key = c;
     }
@@ -617,7 +618,7 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, PairScre
     {
         const unsigned g = (unsigned) ((nq_pad * 32 + 255) / 256);
         timed(ix, st, "scores_tc_prep", [&] {
-            slice_rows_kernel<<<g, 256, 0, st>>>(call.qrows, nullptr, nq, nq_pad, dim, c, cp, kp, kScN, b_sl, qmeta);
+            slice_rows_kernel<<<g, 256, 0, st>>>(call.qrows, nullptr, nq, nq_pad, dim, c, cp, kp, kScN, 0, b_sl, qmeta);
         });
         RKR_CUDA(cudaGetLastError());
     }

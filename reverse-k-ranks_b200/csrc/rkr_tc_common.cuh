@@ -25,15 +25,24 @@ __host__ __device__ inline int round32(int x) { return (x + 31) & ~31; }
 
 // ---- operands ----------------------------------------------------------------------------------------
 
-// Rows [n][dim] (gathered through idx when given) to the digit layout of the tiles: per tile of tr rows, 4 slices of [kp / 16][tr / 8]
-// [8 rows][16 bytes] (K-major core matrices); coordinates [0, c) at k in [0, c), [c, dim) at
+// Byte offset of (row rr, coordinate p) within one digit slice of a tile of tr rows, as 8-row x
+// 16-byte core matrices: K blocks outermost ([kp / 16][tr / 8][8][16], the resident A tiles), or row
+// groups outermost ([tr / 8][kp / 16][8][16], the stacked B tiles, whose slices then follow each other
+// as whole 8-row groups).
+__host__ __device__ inline size_t digit_off(int rr, int p, int tr, int kp, bool rows_outer) {
+    return rows_outer ? (size_t) (rr >> 3) * (kp * 8) + (p >> 4) * 128 + (rr & 7) * 16 + (p & 15)
+                      : (size_t) (p >> 4) * (tr * 16) + (rr >> 3) * 128 + (rr & 7) * 16 + (p & 15);
+}
+
+// Rows [n][dim] (gathered through idx when given) to the digit layout of the tiles: per tile of tr rows,
+// 4 slices in the layout of digit_off; coordinates [0, c) at k in [0, c), [c, dim) at
 // [cp, cp + dim - c), zeros elsewhere and in rows [n, n_pad).  meta[r] = {2^e, upper bounds of the
 // weighted norms (sum_t w(t) x_t^2)^(1/2) of the two parts, e (as int bits)}; a row with a non-finite
 // coordinate or a scale beyond 2^+-kScMaxExp gets 2^e = inf, which sends all of its pairs to the
 // exact path.  One warp per row.
 __global__ void slice_rows_kernel(const float *__restrict__ src, const int32_t *__restrict__ idx, int64_t n,
-                                  int64_t n_pad, int dim, int c, int cp, int kp, int tr, int8_t *__restrict__ dst,
-                                  float4 *__restrict__ meta) {
+                                  int64_t n_pad, int dim, int c, int cp, int kp, int tr, int rows_outer,
+                                  int8_t *__restrict__ dst, float4 *__restrict__ meta) {
     const int64_t r = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (r >= n_pad) return;
@@ -75,7 +84,7 @@ __global__ void slice_rows_kernel(const float *__restrict__ src, const int32_t *
             else sr += w * v * v;
         }
         float a = v * scale;  // exact: a power of two
-        const size_t off = (size_t) (p >> 4) * (tr * 16) + (rr >> 3) * 128 + (rr & 7) * 16 + (p & 15);
+        const size_t off = digit_off(rr, p, tr, kp, rows_outer);
 #pragma unroll
         for (int s = 0; s < kScSlices; s++) {
             const float t = a * 128.0f;  // exact
@@ -147,16 +156,28 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
     return d;
 }
 
-// Instruction descriptor: kind::i8, A and B signed 8-bit K-major, int32 accumulator, M = 128, N = 32.
+// Instruction descriptors: kind::i8, A and B signed 8-bit K-major, int32 accumulator, M = 128, N = 32
+// (one digit slice of a row tile) or N = 128 (a stacked tile: four slices side by side).
 constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) (kScN >> 3) << 17) |
                               ((uint32_t) (kScM >> 4) << 24);
+constexpr uint32_t kIdescI8Stacked = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) ((4 * kScN) >> 3) << 17) |
+                                     ((uint32_t) (kScM >> 4) << 24);
 
-__device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+__device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate,
+                                        uint32_t idesc = kIdescI8) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t"
-        "}\n" ::"r"(d_tmem), "l"(a), "l"(b), "r"(kIdescI8), "r"(accumulate) : "memory");
+        "}\n" ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate) : "memory");
+}
+
+// One lane of the (fully active) warp: the issuing lane of the copies, MMAs and commits, while the
+// whole warp runs the loop around them (its values stay warp-uniform).
+__device__ __forceinline__ bool elect_one() {
+    uint32_t pred = 0;
+    asm volatile("{\n\t.reg .pred p;\n\telect.sync _|p, 0xffffffff;\n\tselp.u32 %0, 1, 0, p;\n\t}\n" : "=r"(pred));
+    return pred != 0;
 }
 
 __device__ __forceinline__ void tmem_ld8(uint32_t addr, uint32_t (&v)[8]) {

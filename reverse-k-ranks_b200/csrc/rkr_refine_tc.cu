@@ -21,10 +21,10 @@
 // Tiles.  A CTA holds the digits of 128 candidates (the MMA's M, TMEM lanes) and walks a strided
 // share of the 32-item chunks inside its candidates' norm cut-off; the items' digit chunks are
 // bulk-copied and double-buffered, the accumulators double-buffered in TMEM, so that one chunk's
-// MMAs overlap the previous chunk's epilogue.  The chunk's four digit slices sit side by side behind
-// three blocks of zeros, so that one MMA of N = 128 per candidate slice i and K step fills the four
-// digit-group accumulators at once (4 MMAs per K step instead of the 10 digit pairs; the operand
-// traffic of shared memory, which bounds these small MMAs, falls by 1.6x).  Warp 16 runs the
+// MMAs overlap the previous chunk's epilogue.  The chunk's four digit slices follow each other as row
+// groups, so that per candidate slice i and K step one MMA of N = 32 (4 - i) fills the digit-group
+// accumulators i .. 3 (umma_i8_step: 4 MMAs per K step instead of one per digit pair; the operand
+// traffic of shared memory, which bounds these small MMAs, falls by 1.9x).  Warp 16 runs the
 // copies and the MMAs (one elected lane issues); warps 0-15 run the epilogue (warp w: lane
 // quadrant w % 4, columns 8 (w / 4) .. + 8 of each accumulator).
 #include <algorithm>
@@ -39,7 +39,7 @@ namespace {
 
 constexpr int kRfEpiWarps = 16;
 constexpr int kRfThreads = 32 * (kRfEpiWarps + 1);
-constexpr int kRfMaxKp = 224;  // the candidate tile and two stacked item buffers fit in shared memory up to this K
+constexpr int kRfMaxKp = 224;  // the candidate tile and two item chunks fit in shared memory up to this K
 constexpr int kRfGroup = 8;    // items per group (a warp's columns of a chunk)
 
 // Per candidate row, 2 float4: {2^e, weighted norms WL, WR, plain norm NL}, {NR, e (int bits), 0, 0}.
@@ -240,18 +240,11 @@ __global__ void __launch_bounds__(kRfThreads, 1) refine_tc_kernel(TcArgs a) {
     if (mine == 0) return;
 
     const int kp = a.kp;
-    // shared memory: the candidate tile (A), then two item buffers of 7 blocks of kScN rows: three blocks
-    // of zeros and the chunk's 4 digit slices, so that the N = 128 operand starting 3 - i blocks in
-    // holds in column block g the item slice g - i (zeros for g < i)
-    const uint32_t a_bytes = (uint32_t) (kScSlices * kScM * kp), blk = (uint32_t) (kScN * kp);
-    const uint32_t b_bytes = kScSlices * blk, buf_bytes = (kScSlices + 3) * blk;
+    // shared memory: the candidate tile (A), then two item chunk buffers (B, slices as consecutive row
+    // groups)
+    const uint32_t a_bytes = (uint32_t) (kScSlices * kScM * kp), b_bytes = (uint32_t) (kScSlices * kScN * kp);
     uint8_t *sA = tc_smem;
     uint8_t *sB = sA + a_bytes;
-    for (uint32_t o = tid * 16; o < 3 * blk; o += kRfThreads * 16) {
-        *reinterpret_cast<uint4 *>(sB + o) = make_uint4(0u, 0u, 0u, 0u);
-        *reinterpret_cast<uint4 *>(sB + buf_bytes + o) = make_uint4(0u, 0u, 0u, 0u);
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the zeros, for the MMAs' reads
     if (tid == 0) {
         mbar_init(&bar_a, 1);
         for (int b = 0; b < 2; b++) {
@@ -283,18 +276,18 @@ __global__ void __launch_bounds__(kRfThreads, 1) refine_tc_kernel(TcArgs a) {
             for (int i = 0; i < 2 && i < mine; i++) {
                 const int t = blockIdx.x + i * gridDim.x;
                 mbar_expect_tx(&bar_b[i], b_bytes);
-                bulk_g2s(sB + i * buf_bytes + 3 * blk, a.item_sl + (size_t) t * b_bytes, b_bytes, &bar_b[i]);
+                bulk_g2s(sB + (size_t) i * b_bytes, a.item_sl + (size_t) t * b_bytes, b_bytes, &bar_b[i]);
             }
         }
         __syncwarp();
         ok = __all_sync(0xffffffffu, mbar_wait(&bar_a, 0, abort));
-        // descriptors (addresses in 16-byte units, within the 14-bit field: shared memory < 256 KB):
-        // A K blocks of kScM rows (K step s at s * 2 * kScM * 16 bytes, slice i at i * kScM * kp); the
-        // stacked B in row groups of kp * 8 bytes, K step s at s * 256 bytes
+        // descriptors (addresses in 16-byte units, within the 14-bit field: shared memory < 256 KB): A in
+        // K blocks of kScM rows (K step s at s * 2 * kScM * 16 bytes, slice i at i * kScM * kp); the
+        // item chunk in row groups of kp * 8 bytes (K step s at s * 256 bytes)
         constexpr uint32_t kAChunk = kScM * 16;
         const uint64_t da0 = umma_desc(smem_u32(sA), kAChunk, 128);
         const uint64_t db0 = umma_desc(smem_u32(sB), 128, (uint32_t) kp * 8);
-        const uint32_t a_slice = (uint32_t) (kScM * kp) >> 4, b_blk = blk >> 4, b_buf = buf_bytes >> 4;
+        const uint32_t a_slice = (uint32_t) (kScM * kp) >> 4, b_buf = b_bytes >> 4;
         for (int i = 0; ok && i < mine; i++) {
             const int b = i & 1;
             const uint32_t ph = (uint32_t) (i >> 1) & 1u;
@@ -304,20 +297,11 @@ __global__ void __launch_bounds__(kRfThreads, 1) refine_tc_kernel(TcArgs a) {
             if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t d0 = taddr + (uint32_t) b * buf_cols;
-            const uint64_t dbb = db0 + (uint32_t) b * b_buf;
             for (int s = 0; s < a.ksteps; s++) {
                 const int part = s < a.ksplit ? 0 : 1;
-                const bool first_s = s == 0 || s == a.ksplit;
                 const uint64_t das = da0 + ((uint32_t) s * 2 * kAChunk >> 4);
-                const uint64_t dbs = dbb + (uint32_t) s * 16;
-                const uint32_t dp = d0 + (uint32_t) part * 4 * kScN;
-                // candidate slice i against the stacked items from block 3 - i: column block g gets
-                // the products of digit pair (i, g - i), g = 0..3
-                if (elect_one()) {
-#pragma unroll
-                    for (int si = 0; si < kScSlices; si++)
-                        umma_i8(dp, das + si * a_slice, dbs + (3 - si) * b_blk, !(first_s && si == 0), kIdescI8Stacked);
-                }
+                const uint64_t dbs = db0 + (uint32_t) b * b_buf + (uint32_t) s * 16;
+                if (elect_one()) umma_i8_step(d0 + (uint32_t) part * 4 * kScN, das, a_slice, dbs, s == 0 || s == a.ksplit);
                 __syncwarp();
             }
             if (elect_one())
@@ -334,7 +318,7 @@ __global__ void __launch_bounds__(kRfThreads, 1) refine_tc_kernel(TcArgs a) {
                 if (elect_one()) {
                     const int t = blockIdx.x + (i + 1) * gridDim.x;
                     mbar_expect_tx(&bar_b[pb], b_bytes);
-                    bulk_g2s(sB + pb * buf_bytes + 3 * blk, a.item_sl + (size_t) t * b_bytes, b_bytes, &bar_b[pb]);
+                    bulk_g2s(sB + (size_t) pb * b_bytes, a.item_sl + (size_t) t * b_bytes, b_bytes, &bar_b[pb]);
                 }
                 __syncwarp();
             }
@@ -601,7 +585,7 @@ int refine_tc(rkr_index *ix, const RefineArgs &ra, cudaStream_t st, bool *done) 
     a.list_count = counters;
     a.status = counters + 1;
     a.list_cap = list_cap;
-    const size_t smem = (size_t) kp * (kScSlices * kScM + 2 * (kScSlices + 3) * kScN);
+    const size_t smem = (size_t) kScSlices * kp * (kScM + 2 * kScN);
     RKR_CUDA(cudaFuncSetAttribute(refine_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     const int64_t cand_tiles = cand_pad / kScM;
     const dim3 grid((unsigned) pick_shares(cand_tiles, item_pad / kScN), (unsigned) cand_tiles);

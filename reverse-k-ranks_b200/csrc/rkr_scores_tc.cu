@@ -23,8 +23,13 @@
 // whole K extent in shared memory and walks the batch's queries in chunks of 32 (the MMA's N), the
 // query digits double-buffered by bulk copies and the accumulators double-buffered in TMEM (2 x 8
 // accumulators x 32 columns = 512 columns), so that the MMAs of one chunk overlap the epilogue of
-// the previous one.  Warp 16 issues the copies and the MMAs; warps 0-15 read TMEM (warp w: lane
-// quadrant w % 4, columns 8 (w / 4) .. + 8 of each accumulator) and run the epilogue.
+// the previous one.  A chunk's four query digit slices follow each other as row groups, so that per
+// user slice i and K step one MMA of N = 32 (4 - i) covers the query slices 0 .. 3 - i and fills the
+// digit-group accumulators i .. 3 (umma_i8_step: 4 MMAs per K step instead of one per digit pair;
+// these small MMAs are bound by their shared-memory operand traffic, which falls by 1.9x).  Warp 16
+// runs the copies and the MMAs (one
+// elected lane issues); warps 0-15 read TMEM (warp w: lane quadrant w % 4, columns 8 (w / 4) .. + 8
+// of each accumulator) and run the epilogue.
 #include <cmath>
 #include <cstdio>
 #include <vector>
@@ -183,6 +188,8 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
     const int64_t u0 = (int64_t) blockIdx.x * kScM;
     const int kp = a.kp, nq = a.nq;
     const int nchunks = (nq + kScN - 1) / kScN;
+    // shared memory: the user tile (A), two query chunk buffers (B, slices as consecutive row groups),
+    // the threshold summary, the undecided list, the CDF table and the batch's query data
     const uint32_t a_bytes = (uint32_t) (kScSlices * kScM * kp), b_bytes = (uint32_t) (kScSlices * kScN * kp);
     uint8_t *sA = sm_raw;
     uint8_t *sB = sA + a_bytes;
@@ -232,71 +239,72 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
     const uint32_t buf_cols = (uint32_t) (nacc * kScN);
 
     if (warp == kScEpiWarps) {
-        // ---- copies and MMAs (one thread) ----
-        if (lane == 0) {
-            bool ok = true;
-            int last = -1;  // last chunk whose MMAs were committed
+        // ---- copies and MMAs: the warp runs the loop (warp-uniform values), one elected lane issues ----
+        bool ok = true;
+        int last = -1;  // last chunk whose MMAs were committed
+        if (elect_one()) {
             mbar_expect_tx(&bar_a, a_bytes);
             bulk_g2s(sA, a.a_sl + (size_t) blockIdx.x * a_bytes, a_bytes, &bar_a);
             for (int j = 0; j < 2 && j < nchunks; j++) {
                 mbar_expect_tx(&bar_b[j], b_bytes);
                 bulk_g2s(sB + (size_t) j * b_bytes, a.b_sl + (size_t) j * b_bytes, b_bytes, &bar_b[j]);
             }
-            ok = mbar_wait(&bar_a, 0, abort);
-            constexpr uint32_t kAChunk = kScM * 16, kBChunk = kScN * 16;  // bytes per 16-coordinate block
-            // descriptors: a base per operand buffer, slices and K steps as offsets of the start address
-            // (16-byte units, within the descriptor's 14-bit field: shared memory stays below 256 KB)
-            const uint64_t da0 = umma_desc(smem_u32(sA), kAChunk, 128);
-            const uint64_t db_0 = umma_desc(smem_u32(sB), kBChunk, 128);
-            const uint64_t db_1 = umma_desc(smem_u32(sB + b_bytes), kBChunk, 128);
-            const uint32_t a_slice = (uint32_t) (kScM * kp) >> 4, b_slice = (uint32_t) (kScN * kp) >> 4;
-            for (int j = 0; ok && j < nchunks; j++) {
-                const int b = j & 1;
-                const uint32_t ph = (uint32_t) (j >> 1) & 1u;
-                ok = mbar_wait(&bar_b[b], ph, abort);
-                if (ok && j >= 2) ok = mbar_wait(&bar_free[b], (uint32_t) ((j - 2) >> 1) & 1u, abort);
-                if (!ok) break;
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t d0 = taddr + (uint32_t) b * buf_cols;
-                for (int s = 0; s < a.ksteps; s++) {
-                    const int part = s < a.ksplit ? 0 : 1;
-                    const bool first_s = s == 0 || s == a.ksplit;
-                    const uint64_t das = da0 + ((uint32_t) s * 2 * kAChunk >> 4);
-                    const uint64_t dbs = (b ? db_1 : db_0) + ((uint32_t) s * 2 * kBChunk >> 4);
-                    const uint32_t dp = d0 + (uint32_t) part * 4 * kScN;
-                    // digit products (A slice i, B slice j) into accumulator i + j, i + j <= 3
-                    constexpr int kI[10] = {0, 0, 1, 0, 1, 2, 0, 1, 2, 3}, kJ[10] = {0, 1, 0, 2, 1, 0, 3, 2, 1, 0};
-#pragma unroll
-                    for (int pi = 0; pi < 10; pi++) {
-                        const bool first_g = pi == 0 || pi == 1 || pi == 3 || pi == 6;
-                        umma_i8(dp + (uint32_t) (kI[pi] + kJ[pi]) * kScN, das + kI[pi] * a_slice, dbs + kJ[pi] * b_slice,
-                                !(first_s && first_g));
-                    }
-                }
+        }
+        __syncwarp();
+        ok = __all_sync(0xffffffffu, mbar_wait(&bar_a, 0, abort));
+        // descriptors (addresses in 16-byte units, within the 14-bit field: shared memory < 256 KB): A in
+        // K blocks of kScM rows (K step s at s * 2 * kScM * 16 bytes, slice i at i * kScM * kp); the
+        // query chunk in row groups of kp * 8 bytes (K step s at s * 256 bytes)
+        constexpr uint32_t kAChunk = kScM * 16;
+        const uint64_t da0 = umma_desc(smem_u32(sA), kAChunk, 128);
+        const uint64_t db0 = umma_desc(smem_u32(sB), 128, (uint32_t) kp * 8);
+        const uint32_t a_slice = (uint32_t) (kScM * kp) >> 4, b_buf = b_bytes >> 4;
+        for (int j = 0; ok && j < nchunks; j++) {
+            const int b = j & 1;
+            const uint32_t ph = (uint32_t) (j >> 1) & 1u;
+            ok = mbar_wait(&bar_b[b], ph, abort);
+            if (ok && j >= 2) ok = mbar_wait(&bar_free[b], (uint32_t) ((j - 2) >> 1) & 1u, abort);
+            ok = __all_sync(0xffffffffu, ok);
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t d0 = taddr + (uint32_t) b * buf_cols;
+            for (int s = 0; s < a.ksteps; s++) {
+                const int part = s < a.ksplit ? 0 : 1;
+                const bool first_s = s == 0 || s == a.ksplit;
+                const uint64_t das = da0 + ((uint32_t) s * 2 * kAChunk >> 4);
+                const uint64_t dbs = db0 + (uint32_t) b * b_buf + (uint32_t) s * 16;
+                const uint32_t dp = d0 + (uint32_t) part * 4 * kScN;
+                if (elect_one()) umma_i8_step(dp, das, a_slice, dbs, first_s);
+                __syncwarp();
+            }
+            if (elect_one())
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                                  smem_u32(&bar_mma[b]))
                              : "memory");
-                last = j;
-                if (j >= 1 && j + 1 < nchunks) {
-                    // the previous chunk's MMAs have read its query digits: refill that buffer with the next
-                    // chunk while this chunk's MMAs run
-                    const int pb = (j - 1) & 1;
-                    ok = mbar_wait(&bar_mma[pb], (uint32_t) ((j - 1) >> 1) & 1u, abort);
-                    if (!ok) break;
+            __syncwarp();
+            last = j;
+            if (j >= 1 && j + 1 < nchunks) {
+                // the previous chunk's MMAs have read its query digits: refill that buffer with the next
+                // chunk while this chunk's MMAs run
+                const int pb = (j - 1) & 1;
+                ok = __all_sync(0xffffffffu, mbar_wait(&bar_mma[pb], (uint32_t) ((j - 1) >> 1) & 1u, abort));
+                if (!ok) break;
+                if (elect_one()) {
                     mbar_expect_tx(&bar_b[pb], b_bytes);
                     bulk_g2s(sB + (size_t) pb * b_bytes, a.b_sl + (size_t) (j + 1) * b_bytes, b_bytes, &bar_b[pb]);
                 }
+                __syncwarp();
             }
-            if (!ok) {
-                *abort = 1;
-                atomicExch(a.status, 1);
-            }
-            // the MMAs of the last committed chunk finish on their own: wait for them (bounded) before
-            // the columns are released
-            if (last >= 0)
-                for (int it = 0; it < (1 << 22) && !mbar_try(&bar_mma[last & 1], (uint32_t) (last >> 1) & 1u); it++) {
-                }
         }
+        if (!ok && lane == 0) {
+            *abort = 1;
+            atomicExch(a.status, 1);
+        }
+        // the MMAs of the last committed chunk finish on their own: wait for them (bounded) before
+        // the columns are released
+        if (last >= 0)
+            for (int it = 0; it < (1 << 22) && !mbar_try(&bar_mma[last & 1], (uint32_t) (last >> 1) & 1u); it++) {
+            }
     } else {
         // ---- epilogue ----
         const int quad = warp & 3, cg = warp >> 2;
@@ -618,7 +626,7 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, PairScre
     {
         const unsigned g = (unsigned) ((nq_pad * 32 + 255) / 256);
         timed(ix, st, "scores_tc_prep", [&] {
-            slice_rows_kernel<<<g, 256, 0, st>>>(call.qrows, nullptr, nq, nq_pad, dim, c, cp, kp, kScN, 0, b_sl, qmeta);
+            slice_rows_kernel<<<g, 256, 0, st>>>(call.qrows, nullptr, nq, nq_pad, dim, c, cp, kp, kScN, 1, b_sl, qmeta);
         });
         RKR_CUDA(cudaGetLastError());
     }

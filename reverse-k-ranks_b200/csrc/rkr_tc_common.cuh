@@ -156,12 +156,11 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
     return d;
 }
 
-// Instruction descriptors: kind::i8, A and B signed 8-bit K-major, int32 accumulator, M = 128, N = 32
-// (one digit slice of a row tile) or N = 128 (a stacked tile: four slices side by side).
-constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) (kScN >> 3) << 17) |
-                              ((uint32_t) (kScM >> 4) << 24);
-constexpr uint32_t kIdescI8Stacked = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) ((4 * kScN) >> 3) << 17) |
-                                     ((uint32_t) (kScM >> 4) << 24);
+// Instruction descriptor: kind::i8, A and B signed 8-bit K-major, int32 accumulator, M = 128, N = n.
+__host__ __device__ constexpr uint32_t idesc_i8(int n) {
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) (n >> 3) << 17) | ((uint32_t) (kScM >> 4) << 24);
+}
+constexpr uint32_t kIdescI8 = idesc_i8(kScN);
 
 __device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate,
                                         uint32_t idesc = kIdescI8) {
@@ -170,6 +169,18 @@ __device__ __forceinline__ void umma_i8(uint32_t d_tmem, uint64_t a, uint64_t b,
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t"
         "}\n" ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate) : "memory");
+}
+
+// The ten digit products of one K step as four MMAs: A slice i (a + i * a_slice) against B slices
+// 0 .. 3 - i, which follow each other as row groups from b (the row-group-outer layout of digit_off),
+// with N = 32 (4 - i) into the accumulators from column block i on (d + 32 i): column block g gets
+// the products of digit pair (i, g - i).  Slice 0 writes all four blocks first (accumulate = 0 at a
+// part's first K step).
+__device__ __forceinline__ void umma_i8_step(uint32_t d, uint64_t a, uint32_t a_slice, uint64_t b, bool first) {
+    umma_i8(d, a, b, !first, idesc_i8(4 * kScN));
+    umma_i8(d + kScN, a + a_slice, b, 1u, idesc_i8(3 * kScN));
+    umma_i8(d + 2 * kScN, a + 2 * a_slice, b, 1u, idesc_i8(2 * kScN));
+    umma_i8(d + 3 * kScN, a + 3 * a_slice, b, 1u, idesc_i8(kScN));
 }
 
 // One lane of the (fully active) warp: the issuing lane of the copies, MMAs and commits, while the

@@ -174,8 +174,8 @@ def kernel_model(name, cfg, nq, stats, method):
 
     dot_flops counts the exact dot products' binary32 multiplies and adds as separate operations (2 per
     coordinate and pair).  bytes is what the kernel must move through HBM at the least.  tensor_ops
-    counts the tensor-core operations the kernel issues for them: the pair scores run ten int8 digit
-    products per coordinate (K padded to 32 per part), the refinement one TF32 product."""
+    counts the tensor-core operations the kernel issues for them: the pair scores and the refinement
+    both run ten int8 digit products per coordinate (K padded to 32 per part)."""
     n_user, n_item, dim = CONFIGS[cfg][:3]
     pairs = float(n_user) * nq
     r32 = lambda x: (x + 31) // 32 * 32
@@ -193,18 +193,21 @@ def kernel_model(name, cfg, nq, stats, method):
     if name == "level_hist":
         return 0.0, 4.0 * pairs, 0.0
     if name == "refine_tc":
+        # per (candidate, item) pair in the norm cut-off; the items' digit chunks read once at the least
         n = stats["n_compute_item"]
-        return 2.0 * n * dim, 4.0 * n_item * dim, 2.0 * n * (dim + 8)
+        cd = stats["check_dim"] if method != "US" else dim
+        kp = r32(cd) + (r32(dim - cd) if dim > cd else 0)
+        return 2.0 * n * dim, 4.0 * kp * n_item, 10 * 2.0 * n * kp
     return 0.0, 0.0, 0.0
 
 
 # DRAM bytes (read + write) per (query, user) pair of the dominant kernel, from one ncu capture at a
 # 200-query batch of the same workload (profiles/qsrp_tc_kernels_batch200_full.md); traffic grows
 # with the pairs a launch processes, so a launch's traffic is this figure times its pairs.
-NCU_BYTES_PER_PAIR = {("qsrp_scores_tc", "QSRPNormalLP"): (456.599e6 + 814.504e6) / (200 * 480189.0)}
+NCU_BYTES_PER_PAIR = {("qsrp_scores_tc", "QSRPNormalLP"): (456.031e6 + 814.108e6) / (200 * 480189.0)}
 
 # Nominal dense tensor-core peaks of one B200 (T ops/s), for the tensor_ops figures.
-TENSOR_PEAK_NOMINAL = {"qsrp_scores_tc": ("int8", 4500.0), "refine_tc": ("tf32", 1125.0)}
+TENSOR_PEAK_NOMINAL = {"qsrp_scores_tc": ("int8", 4500.0), "refine_tc": ("int8", 4500.0)}
 
 
 class ReferenceTimer:

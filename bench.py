@@ -42,6 +42,8 @@ CONFIGS = {
     "config2": (480189, 17770, 150, 512, 150, 100, 1000, 100),
     "config1": (1000, 5000, 30, 64, 150, 10, 100, 10),
     "config4": (1000990, 624961, 150, 512, 150, 100, 1000, 100),
+    # the config-4 index serving a seeded Poisson stream of requests (serve())
+    "config5": (1000990, 624961, 150, 512, 150, 100, 1000, 100),
 }
 
 
@@ -70,7 +72,7 @@ def make_data(cfg, seed, rank_id):
     rng = np.random.default_rng(seed)
     user = rng.standard_normal((n_user, dim), dtype=np.float32) * np.float32(1 / np.sqrt(dim))
     item = rng.standard_normal((n_item, dim), dtype=np.float32) * np.float32(1 / np.sqrt(dim))
-    if cfg in ("config2", "config4"):
+    if cfg in ("config2", "config4", "config5"):
         item *= np.exp(rng.normal(0.0, 0.3, (n_item, 1))).astype(np.float32)
     qrng = np.random.default_rng(seed + 1000 + rank_id)
     return user, item, qrng
@@ -243,6 +245,48 @@ def reference_available():
     return Reference.available()
 
 
+def serve(ix, item, dim, seed, method, n_req, rate, log_prefix="[serve]"):
+    """A serving loop over a seeded Poisson arrival trace: each request holds 1-256 queries (uniform),
+    drawn from the items or out-of-set N(0, 1/dim) vectors with equal odds, and k ~ U[10, 200].
+    Requests are answered in arrival order, one end-to-end call each (host buffers in and out, as a
+    client makes them): QSRPNormalLP carries per-user scores from earlier queries into later results,
+    so the order of the calls is part of the answer, and the reference answers one k per call.
+    Returns per-request arrival, start and end times (seconds from the trace's start) and sizes."""
+    rng = np.random.default_rng(seed + 5000)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+    sizes = rng.integers(1, 257, n_req)
+    ks = rng.integers(10, 201, n_req)
+    from_items = rng.random(n_req) < 0.5
+    reqs = []
+    for i in range(n_req):
+        if from_items[i]:
+            reqs.append(item[rng.choice(item.shape[0], size=int(sizes[i]), replace=False)].copy())
+        else:
+            reqs.append((rng.standard_normal((int(sizes[i]), dim)) / np.sqrt(dim)).astype(np.float32))
+    start = np.zeros(n_req)
+    end = np.zeros(n_req)
+    t0 = time.perf_counter()
+    for i in range(n_req):
+        now = time.perf_counter() - t0
+        if now < arrivals[i]:
+            time.sleep(arrivals[i] - now)
+        start[i] = time.perf_counter() - t0
+        ix.retrieval(method, reqs[i], int(ks[i]))
+        end[i] = time.perf_counter() - t0
+    return arrivals, start, end, sizes
+
+
+def serve_summary(arrivals, start, end, sizes, rate):
+    lat = (end - arrivals) * 1e3
+    svc = (end - start) * 1e3
+    span = end[-1] - arrivals[0]
+    return {"offered_req_per_s": rate, "requests": int(len(sizes)), "queries": int(sizes.sum()),
+            "throughput_req_per_s": len(sizes) / span, "throughput_queries_per_s": float(sizes.sum()) / span,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+            "service_ms": {"p50": float(np.percentile(svc, 50)), "p99": float(np.percentile(svc, 99)),
+                           "mean": float(svc.mean())}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -255,6 +299,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--single-queries", type=int, default=100)
     ap.add_argument("--batch", type=int, default=0, help="queries per step (default: the workload's)")
+    ap.add_argument("--serve-requests", type=int, default=200, help="config5: requests per trace")
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="config5: offered requests/s")
     args = ap.parse_args()
 
     import torch
@@ -291,6 +337,42 @@ def main():
 
     def draw_batch():
         return item[qrng.choice(n_item, size=batch, replace=False)].copy()
+
+    if args.config == "config5":
+        if args.impl == "reference" or rank_id != 0:
+            if args.impl == "reference":
+                print(json.dumps({"impl": "reference", "unavailable": "config5 is a serving loop of the engine; "
+                                  "the reference arm is timed on config2/config4 batches"}))
+            ix.close()
+            if dist:
+                dist.destroy_process_group()
+            return
+        # warm-up: the largest request shape grows every workspace once
+        ix.retrieval(args.method, draw_batch()[:256], 200)
+        ix.retrieval(args.method, draw_batch()[:1], 10)
+        with Clocks(local) as clk:
+            t_a = time.perf_counter()
+            arr, st_, en, sz = serve(ix, item, dim, args.seed, args.method, args.serve_requests, args.serve_rate)
+            offered = serve_summary(arr, st_, en, sz, args.serve_rate)
+            # the same kind of trace at 70% of the capacity the first trace measured (1 / mean service time)
+            cap = 1e3 / offered["service_ms"]["mean"]
+            arr, st_, en, sz = serve(ix, item, dim, args.seed + 1, args.method, args.serve_requests, 0.7 * cap)
+            sustained = serve_summary(arr, st_, en, sz, 0.7 * cap)
+            clk.mark(t_a, time.perf_counter())
+        line = {"metric": "serving: request latency p50/p99 (ms) and throughput under Poisson arrivals",
+                "value": offered["latency_ms"]["p99"], "unit": "ms (p99 request latency at the offered rate)",
+                "higher_is_better": False, "n_gpus": 1, "dtype": "f32",
+                "data": "synthetic: seeded numpy N(0,1/150) users, lognormal-scaled N(0,1/150) items; requests of "
+                        "1-256 queries, half drawn from the items, half out-of-set N(0,1/150); k ~ U[10,200]",
+                "config": {"workload": f"config5: the config4 index ({n_user} users x {n_item} items, d={dim}, "
+                                       f"{n_sample} sampled thresholds/user + NormalLinearRegressionLP + SVD), "
+                                       f"{args.method}, Poisson arrivals, one end-to-end call per request in "
+                                       f"arrival order", "seed": args.seed},
+                "offered": offered, "at_70pct_capacity": sustained, "capacity_req_per_s": cap,
+                "build_sec": build_sec, "hbm_index_bytes": ix.size_bytes(), "clocks": clk.summary()}
+        print(json.dumps(line))
+        ix.close()
+        return
 
     if args.impl == "reference":
         if not reference_available():
@@ -467,7 +549,7 @@ def main():
             "single_query_p50_ms": float(np.percentile(single, 50)) if single else None,
             "single_query_p99_ms": float(np.percentile(single, 99)) if single else None,
             "build_sec": build_sec, "build_stages_sec": {k: round(v, 3) for k, v in stages.items()},
-            "e2e": e2e, "gpu_launches": int(launches_per_step * args.steps), "roofline": roofline,
+            "hbm_index_bytes": ix.size_bytes(), "e2e": e2e, "gpu_launches": int(launches_per_step * args.steps), "roofline": roofline,
             "cpu_baseline": cpu, "clocks": clk.summary(), "query_stats_mean": stats_mean,
         }
         print(json.dumps(line))

@@ -452,8 +452,9 @@ def main():
     torch.cuda.synchronize()
     prof = ix.profile_read()
     ix.profile(False)
-    counters = {k: int(v[1]) for k, v in prof.items() if k.endswith("_pairs")}
-    prof = {k: v for k, v in prof.items() if not k.endswith("_pairs")}
+    is_counter = lambda k: k.endswith("_pairs") or k.endswith("_queries")
+    counters = {k: int(v[1]) for k, v in prof.items() if is_counter(k)}
+    prof = {k: v for k, v in prof.items() if not is_counter(k)}
     st = np.frombuffer(d_stats.cpu().numpy().tobytes(), dtype=R.QUERY_STATS)
     model_stats = {"check_dim": parts["cd"], "n_compute_item": float(st["n_compute_item"].sum())}
     launches_per_step = sum(c for _, c in prof.values())

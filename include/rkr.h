@@ -125,7 +125,9 @@ int rkr_retrieval_device(rkr_index *index, int32_t method, const float *d_query,
  * events on the stream it runs on.  rkr_profile_read returns, per kernel name, the summed time and
  * the launch count since the previous complete read (a read with max_kernels >= *n_kernels clears
  * them; a smaller one only reports the count); names is [max_kernels][64] chars.  Entries whose
- * name ends in "_pairs" are counters rather than kernels (time 0, `launches` holds the count):
+ * name ends in "_pairs" or "_queries" are counters rather than kernels (time 0, `launches` holds
+ * the count): two_pass_compaction_queries counts the queries whose flagged users outgrew the sparse
+ * compaction's list and took the two-pass form;
  * screen_undecided_pairs counts the (query, user) pairs whose regression levels or threshold group
  * the screens (tensor-core scores with an error bound, the fast binary32 CDF) left to the
  * reference's own arithmetic; rescored_pairs the pairs whose score a later pass recomputed (a fine

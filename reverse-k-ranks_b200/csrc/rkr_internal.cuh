@@ -723,9 +723,10 @@ __device__ __forceinline__ void load16_bytes(const uint8_t *p, uint32_t w[4]) {
 
 template <class P>
 __global__ void __launch_bounds__(kCompactThreads) compact_count_kernel(P p, int64_t n_user, int nchunks,
-                                                                      int2 *__restrict__ cnt) {
+                                                                      int2 *__restrict__ cnt,
+                                                                      const int32_t *__restrict__ qmap) {
     __shared__ int warp_tot[9];
-    const int q = blockIdx.y;
+    const int qi = blockIdx.y, q = qmap ? qmap[qi] : qi;
     const int64_t u0 = (int64_t) blockIdx.x * kCompactChunk + (int64_t) threadIdx.x * kCompactPer;
     int r = 0, c = 0;
     if (u0 < n_user) {
@@ -742,18 +743,21 @@ __global__ void __launch_bounds__(kCompactThreads) compact_count_kernel(P p, int
     }
     int tot;
     block_excl_scan(r | (c << 16), warp_tot, &tot);
-    if (threadIdx.x == 0) cnt[(int64_t) q * nchunks + blockIdx.x] = make_int2(tot & 0xffff, tot >> 16);
+    if (threadIdx.x == 0) cnt[(int64_t) qi * nchunks + blockIdx.x] = make_int2(tot & 0xffff, tot >> 16);
 }
 
-// Offsets per (query, chunk); n_res_emit = min(results, topk); flags a candidate-count mismatch.
+// Offsets per (query, chunk); n_res_emit = min(results, topk); flags a candidate-count mismatch.  With
+// qmap the kernels of this form run on the listed queries only (slot qi holds query qmap[qi]).
 static __global__ void compact_scan_kernel(const int2 *__restrict__ cnt, int nchunks, int nq, int topk, int2 *__restrict__ off,
-                                    QueryCounts *__restrict__ counts, int *__restrict__ err) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= nq) return;
+                                    QueryCounts *__restrict__ counts, int *__restrict__ err,
+                                    const int32_t *__restrict__ qmap) {
+    const int qi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (qi >= nq) return;
+    const int q = qmap ? qmap[qi] : qi;
     int r = 0, c = 0;
     for (int i = 0; i < nchunks; i++) {
-        const int2 v = cnt[(int64_t) q * nchunks + i];
-        off[(int64_t) q * nchunks + i] = make_int2(r, c);
+        const int2 v = cnt[(int64_t) qi * nchunks + i];
+        off[(int64_t) qi * nchunks + i] = make_int2(r, c);
         r += v.x;
         c += v.y;
     }
@@ -764,11 +768,12 @@ static __global__ void compact_scan_kernel(const int2 *__restrict__ cnt, int nch
 template <class P>
 __global__ void __launch_bounds__(kCompactThreads) compact_write_kernel(P p, int64_t n_user, int nchunks,
                                                                       const int2 *__restrict__ cnt,
-                                                                      const int2 *__restrict__ off, int topk) {
+                                                                      const int2 *__restrict__ off, int topk,
+                                                                      const int32_t *__restrict__ qmap) {
     __shared__ int warp_tot[9];
-    const int q = blockIdx.y;
-    const int2 cc = cnt[(int64_t) q * nchunks + blockIdx.x];
-    const int2 oo = off[(int64_t) q * nchunks + blockIdx.x];
+    const int qi = blockIdx.y, q = qmap ? qmap[qi] : qi;
+    const int2 cc = cnt[(int64_t) qi * nchunks + blockIdx.x];
+    const int2 oo = off[(int64_t) qi * nchunks + blockIdx.x];
     if ((cc.x == 0 || oo.x >= topk) && cc.y == 0) return;
     // thread t owns users u0 + t*kCompactPer .. + kCompactPer - 1, so prefix order is user-id order
     const int64_t u0 = (int64_t) blockIdx.x * kCompactChunk + (int64_t) threadIdx.x * kCompactPer;
@@ -801,6 +806,103 @@ __global__ void __launch_bounds__(kCompactThreads) compact_write_kernel(P p, int
             p.emit_cand(q, pc, u0 + e, aux);
             pc++;
         }
+    }
+}
+
+// ---- sparse form of the same compaction -------------------------------------------------------------
+//
+// The users a query must classify are few (a few hundred of the 480 K at config 2), so the sparse
+// form streams the codes once: compact_need_kernel appends each query's flagged users to its list
+// (one atomic per warp, in no particular order), and compact_emit_kernel, one block per query, sorts
+// the list by user id and runs the ordered classification and emission of compact_write_kernel on
+// it.  A query whose list outgrows kNeedCap is listed and takes the two-pass form above.
+
+constexpr int kNeedCap = 4096;     // flagged users per query on the sparse path
+constexpr int kNeedGroups = 4;     // groups of kCompactPer users per thread in the streaming pass
+constexpr int64_t kNeedSpan = (int64_t) kCompactThreads * kNeedGroups * kCompactPer;
+
+template <class P>
+__global__ void __launch_bounds__(kCompactThreads) compact_need_kernel(P p, int64_t n_user, int32_t *__restrict__ need_n,
+                                                                     int32_t *__restrict__ need_u) {
+    const int q = blockIdx.y;
+    const int64_t base = (int64_t) blockIdx.x * kNeedSpan + (int64_t) threadIdx.x * (kNeedGroups * kCompactPer);
+    uint32_t m[kNeedGroups];
+#pragma unroll
+    for (int g = 0; g < kNeedGroups; g++) {
+        const int64_t u = base + g * kCompactPer;
+        m[g] = u < n_user ? p.need_mask(q, u, (int) (n_user - u < kCompactPer ? n_user - u : kCompactPer)) : 0u;
+    }
+    int cnt = 0;
+#pragma unroll
+    for (int g = 0; g < kNeedGroups; g++) cnt += __popc(m[g]);
+    const int lane = threadIdx.x & 31;
+    const int incl = warp_incl_scan(cnt);
+    const int tot = __shfl_sync(0xffffffffu, incl, 31);
+    if (tot == 0) return;
+    int at = 0;
+    if (lane == 31) at = atomicAdd(need_n + q, tot);
+    at = __shfl_sync(0xffffffffu, at, 31) + incl - cnt;
+    int32_t *list = need_u + (int64_t) q * kNeedCap;
+#pragma unroll
+    for (int g = 0; g < kNeedGroups; g++)
+        for (uint32_t x = m[g]; x; x &= x - 1, at++)
+            if (at < kNeedCap) list[at] = (int32_t) (base + g * kCompactPer + __ffs(x) - 1);
+}
+
+template <class P>
+__global__ void __launch_bounds__(kCompactThreads) compact_emit_kernel(P p, int topk, const int32_t *__restrict__ need_n,
+                                                                     const int32_t *__restrict__ need_u,
+                                                                     QueryCounts *__restrict__ counts, int *__restrict__ err,
+                                                                     int32_t *__restrict__ ovf_q) {
+    __shared__ int32_t s[kNeedCap];
+    __shared__ int warp_tot[9];
+    const int q = blockIdx.x, tid = threadIdx.x;
+    const int n = need_n[q];
+    if (n > kNeedCap) {  // listed for the two-pass form
+        if (tid == 0) ovf_q[atomicAdd(err + 1, 1)] = q;
+        return;
+    }
+    int pn = 1;
+    while (pn < n) pn <<= 1;
+    for (int i = tid; i < pn; i += kCompactThreads) s[i] = i < n ? need_u[(int64_t) q * kNeedCap + i] : INT32_MAX;
+    __syncthreads();
+    // bitonic sort, ascending user id (the order the reference lists users in)
+    for (int k = 2; k <= pn; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = tid; i < pn; i += kCompactThreads) {
+                const int ij = i ^ j;
+                if (ij > i) {
+                    const int32_t a = s[i], b = s[ij];
+                    if ((a > b) == ((i & k) == 0)) {
+                        s[i] = b;
+                        s[ij] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    int pr = 0, pc = 0;  // results and candidates before this tile
+    for (int t0 = 0; t0 < n; t0 += kCompactThreads) {
+        const int i = t0 + tid;
+        const int64_t u = i < n ? s[i] : 0;
+        typename P::Aux aux;
+        const int k = i < n ? p.classify(q, u, aux, false) : 0;
+        int tot;
+        const int pre = block_excl_scan((k == 1) | ((k == 2) << 16), warp_tot, &tot);
+        const int rpos = pr + (pre & 0xffff), cpos = pc + (pre >> 16);
+        if (k == 1 && rpos < topk) {
+            p.classify(q, u, aux, true);
+            p.emit_result(q, rpos, u, aux);
+        } else if (k == 2) {
+            p.classify(q, u, aux, true);
+            p.emit_cand(q, cpos, u, aux);
+        }
+        pr += tot & 0xffff;
+        pc += tot >> 16;
+    }
+    if (tid == 0) {
+        counts[q].n_res_emit = pr < topk ? pr : topk;
+        if (pc != counts[q].n_cand) atomicAdd(err, 1);
     }
 }
 
@@ -919,28 +1021,52 @@ template <typename F> inline void timed(rkr_index *ix, cudaStream_t st, const ch
     cudaEventRecord(p.b, st);
     ix->prof.pending.push_back(p);
 }
-// Ordered compaction driver shared by QS and QSRP (pass 1, scan, pass 2).
+// Ordered compaction driver shared by QS and QSRP: the sparse form (streaming pass, per-query sorted
+// lists), and the two-pass form (count, scan, write) for the queries that flag more than kNeedCap users.
 template <class P>
 inline int run_compaction(rkr_index *ix, P p, int nq, int topk, QueryCounts *counts, cudaStream_t st) {
     const int64_t U = ix->n_user;
     const int nchunks = (int) ((U + kCompactChunk - 1) / kCompactChunk);
-    RKR_TRY(ix->ws_cand_off.ensure(sizeof(int2) * 2 * (size_t) nq * nchunks + 256));
-    int2 *cnt = ix->ws_cand_off.as<int2>();
+    const size_t sparse = sizeof(int32_t) * ((size_t) nq * kNeedCap + 2 * (size_t) nq) + 256;
+    const size_t two_pass = sizeof(int2) * 2 * (size_t) nq * nchunks + 256;
+    RKR_TRY(ix->ws_cand_off.ensure(sparse + two_pass));
+    int32_t *need_n = ix->ws_cand_off.as<int32_t>();
+    int32_t *ovf_q = need_n + nq;
+    int32_t *need_u = ovf_q + nq;
+    int2 *cnt = reinterpret_cast<int2 *>(ix->ws_cand_off.as<uint8_t>() + sparse);
     int2 *off = cnt + (size_t) nq * nchunks;
     int *err = reinterpret_cast<int *>(off + (size_t) nq * nchunks);
-    RKR_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
-    dim3 g((unsigned) nchunks, (unsigned) nq);
-    timed(ix, st, "compact_count", [&] { compact_count_kernel<P><<<g, kCompactThreads, 0, st>>>(p, U, nchunks, cnt); });
+    RKR_CUDA(cudaMemsetAsync(err, 0, 2 * sizeof(int), st));
+    RKR_CUDA(cudaMemsetAsync(need_n, 0, sizeof(int32_t) * nq, st));
+    const dim3 g((unsigned) ((U + kNeedSpan - 1) / kNeedSpan), (unsigned) nq);
+    timed(ix, st, "compact_need", [&] { compact_need_kernel<P><<<g, kCompactThreads, 0, st>>>(p, U, need_n, need_u); });
     RKR_CUDA(cudaGetLastError());
-    timed(ix, st, "compact_scan", [&] { compact_scan_kernel<<<(nq + 127) / 128, 128, 0, st>>>(cnt, nchunks, nq, topk, off, counts, err); });
+    timed(ix, st, "compact_emit", [&] {
+        compact_emit_kernel<P><<<(unsigned) nq, kCompactThreads, 0, st>>>(p, topk, need_n, need_u, counts, err, ovf_q);
+    });
     RKR_CUDA(cudaGetLastError());
-    timed(ix, st, "compact_write", [&] { compact_write_kernel<P><<<g, kCompactThreads, 0, st>>>(p, U, nchunks, cnt, off, topk); });
-    RKR_CUDA(cudaGetLastError());
-    int h_err = 0;
-    RKR_CUDA(cudaMemcpyAsync(&h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int h_err[2] = {0, 0};
+    RKR_CUDA(cudaMemcpyAsync(h_err, err, sizeof(h_err), cudaMemcpyDeviceToHost, st));
     RKR_CUDA(cudaStreamSynchronize(st));
-    if (h_err) {
-        set_error("internal: candidate count mismatch in %d queries", h_err);
+    if (h_err[1]) {
+        const int n_ovf = h_err[1];
+        const dim3 g2((unsigned) nchunks, (unsigned) n_ovf);
+        timed(ix, st, "compact_count", [&] { compact_count_kernel<P><<<g2, kCompactThreads, 0, st>>>(p, U, nchunks, cnt, ovf_q); });
+        RKR_CUDA(cudaGetLastError());
+        timed(ix, st, "compact_scan", [&] {
+            compact_scan_kernel<<<(n_ovf + 127) / 128, 128, 0, st>>>(cnt, nchunks, n_ovf, topk, off, counts, err, ovf_q);
+        });
+        RKR_CUDA(cudaGetLastError());
+        timed(ix, st, "compact_write", [&] {
+            compact_write_kernel<P><<<g2, kCompactThreads, 0, st>>>(p, U, nchunks, cnt, off, topk, ovf_q);
+        });
+        RKR_CUDA(cudaGetLastError());
+        RKR_CUDA(cudaMemcpyAsync(h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        RKR_CUDA(cudaStreamSynchronize(st));
+    }
+    if (ix->prof.on) ix->prof.add_count("two_pass_compaction_queries", h_err[1]);
+    if (h_err[0]) {
+        set_error("internal: candidate count mismatch in %d queries", h_err[0]);
         return RKR_ERR_STATE;
     }
     return RKR_OK;

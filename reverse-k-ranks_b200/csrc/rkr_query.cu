@@ -180,7 +180,7 @@ __device__ __forceinline__ uint64_t cand_key(int rank, int user) {
 // entries are filled (QS.hpp:185-198).
 __global__ void assemble_kernel(AssembleArgs a) {
     __shared__ uint64_t keys[kSortCap];
-    __shared__ int n_refined, warp_tot[9];
+    __shared__ int n_refined;
     __shared__ int64_t n_items, ip_refine;
     __shared__ uint64_t thresh;
     const int q = blockIdx.x;

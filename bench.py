@@ -216,12 +216,13 @@ class ReferenceTimer:
     """The reference's QSRPNormalLP::Retrieval (oracle/_ref) held open on the same index; each run
     times a bounded sample of queries with all host threads."""
 
-    def __init__(self, parts, item, n_thread):
-        from checkers import ReferenceQsrp
+    def __init__(self, parts, item, n_thread, fast=False):
+        from checkers import REF_FAST_SO, REF_SO, ReferenceQsrp
         self.n_thread = n_thread
         with quiet_stdout():
             self.ref = ReferenceQsrp(parts["user"], parts["su"], parts["ti"], item, parts["cd"], parts["rank"],
-                                     parts["thr"], parts["rank"], parts["reg"], n_thread)
+                                     parts["thr"], parts["rank"], parts["reg"], n_thread,
+                                     so=REF_FAST_SO if fast else REF_SO)
         self.per_q = None
 
     def run(self, queries, topk, budget_s):
@@ -532,6 +533,15 @@ def main():
                "sample": f"{n} of the step's {batch} queries through the reference's QSRPNormalLP::Retrieval "
                          f"(oracle/_ref, the reference's unmodified headers) on the same index, {n_thread} threads",
                "results_identical_to_engine": bool(same)}
+        from checkers import REF_FAST_SO
+        if os.path.exists(REF_FAST_SO):
+            # the same path under the reference's Release flags (-Ofast), timing only: its sums may
+            # reassociate, so its results are not compared
+            timer = ReferenceTimer(parts, item, n_thread, fast=True)
+            nf, secs_f, _ = timer.run(qs, topk, args.cpu_seconds / 2)
+            timer.close()
+            cpu["ofast"] = {"value": nf / secs_f, "unit": "queries/s", "cores": n_thread,
+                            "sample": f"{nf} of the same queries, oracle/_ref/librkr_ref_fast.so (-Ofast)"}
 
     if rank_id == 0:
         line = {

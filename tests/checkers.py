@@ -19,6 +19,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 ORACLE_SO = os.path.join(ORACLE_DIR, "librkr_oracle.so")
 REF_SO = os.path.join(ORACLE_DIR, "_ref", "librkr_ref.so")
+REF_FAST_SO = os.path.join(ORACLE_DIR, "_ref", "librkr_ref_fast.so")  # -Ofast, timing only
 
 USER_RANK = np.dtype([("user_id", np.int32), ("rank", np.int32), ("query_ip", np.float32)])
 STATS = np.dtype([("n_prune", np.int32), ("n_result", np.int32), ("n_refine", np.int32),
@@ -327,8 +328,9 @@ class Reference:
 class ReferenceQsrp:
     """The reference's QSRPNormalLP index held open for repeated Retrieval timing (oracle/_ref)."""
 
-    def __init__(self, user, svd_user, transfer_item, item, check_dim, sample_rank, thr, reg_rank, reg, n_thread):
-        self.lib = C.CDLL(REF_SO)
+    def __init__(self, user, svd_user, transfer_item, item, check_dim, sample_rank, thr, reg_rank, reg, n_thread,
+                 so=REF_SO):
+        self.lib = C.CDLL(so)
         self.lib.ref_qsrp_open.restype = C.c_void_p
         self.lib.ref_set_threads(C.c_int(n_thread))
         self._keep = [_f32(user), _f32(svd_user), _f32(transfer_item), _f32(item), _i32(sample_rank), _f32(thr),

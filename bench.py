@@ -533,6 +533,24 @@ def main():
                "sample": f"{n} of the step's {batch} queries through the reference's QSRPNormalLP::Retrieval "
                          f"(oracle/_ref, the reference's unmodified headers) on the same index, {n_thread} threads",
                "results_identical_to_engine": bool(same)}
+        # the reference's own CPU build stages (score rows, per-user sort, thresholds; the query-rank
+        # distribution) on a subset of the users, extrapolated linearly to all of them as bstb does
+        # (BuildScoreTableBatch.cpp:56-64, 143-144)
+        from checkers import Reference
+        refb = Reference(n_thread)
+        n_sub = int(min(n_user, max(256, 2000 * 150 * 17770 // max(1, dim * n_item))))
+        sub = parts["user"][:n_sub]
+        t = time.perf_counter()
+        with quiet_stdout():
+            refb.query_rank_distribution(sub, item, R.sample_item(n_item, n_si))
+        t_qd = time.perf_counter() - t
+        t = time.perf_counter()
+        with quiet_stdout():
+            refb.build_thresholds(sub, item, parts["rank"])
+        t_thr = time.perf_counter() - t
+        cpu["build_extrapolated_sec"] = {"query_rank_distribution": t_qd * n_user / n_sub,
+                                         "thresholds": t_thr * n_user / n_sub, "users_timed": n_sub,
+                                         "threads": n_thread}
         from checkers import REF_FAST_SO
         if os.path.exists(REF_FAST_SO):
             # the same path under the reference's Release flags (-Ofast), timing only: its sums may

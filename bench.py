@@ -78,6 +78,23 @@ def make_data(cfg, seed, rank_id):
     return user, item, qrng
 
 
+def max_over_ranks(x, dist, device):
+    """x on this rank -> its maximum over all ranks (every rank takes part; the job's time is its
+    slowest rank's)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world, units_per_rank, seconds):
+    """Whole-job throughput of a replica run: every rank processes units_per_rank (weak scaling),
+    timed by the slowest rank."""
+    return world * units_per_rank / seconds
+
+
 def build_index(R, user_raw, item, cfg, device):
     n_user, n_item, dim, n_sample, n_si, stopk = CONFIGS[cfg][:6]
     stages = {}
@@ -441,11 +458,8 @@ def main():
     total_ms = t_all0.elapsed_time(t_all1)
     step_ms = [a.elapsed_time(b) for a, b in step_ms]
     log("[bench] step ms: " + " ".join(f"{v:.2f}" for v in step_ms))
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * batch * args.steps / (total_ms / 1e3)
+    total_ms = max_over_ranks(total_ms, dist, "cuda")
+    value = job_rate(world, batch * args.steps, total_ms / 1e3)
 
     # ---- per-kernel profile of one more step (outside the timed region) ---------------------------------
     ix.profile(True)
@@ -510,11 +524,8 @@ def main():
     for s in range(args.steps):
         res = ix.retrieval(args.method, pinned[s].numpy(), topk)
     e2e_s = time.perf_counter() - t
-    if dist:
-        tt = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
-    e2e = {"value": world * batch * args.steps / e2e_s, "unit": "queries/s",
+    e2e_s = max_over_ranks(e2e_s, dist, "cuda")
+    e2e = {"value": job_rate(world, batch * args.steps, e2e_s), "unit": "queries/s",
            "h2d_bytes_per_step": batch * dim * 4, "d2h_bytes_per_step": batch * topk * rec_bytes}
 
     cpu = None

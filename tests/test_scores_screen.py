@@ -171,3 +171,18 @@ def test_cdf_table_density_bound():
         h = 1e-7
         slope = np.max(np.abs(phi(zz + h) - phi(zz - h)) / (2 * h))
         assert slope <= td[i] * 141.0 + 1e-6, (i, slope, td[i] * 141.0)
+
+
+def test_bound_detects_a_margin_too_small():
+    """The check has teeth: the same sums against the bound scaled by 1e-3 leave some estimate outside
+    it (the planted error lives in this CPU restatement only)."""
+    rng = np.random.default_rng(5)
+    n = 150
+    a = np.abs(rng.standard_normal((32, n))).astype(np.float32)
+    b = np.abs(rng.standard_normal((24, n))).astype(np.float32)
+    ea, da = digits(a)
+    eb, db = digits(b)
+    got = tc_score(da, ea, db, eb).astype(np.float64)
+    ref = ref_seq(a, b).astype(np.float64)
+    d = (bound(a, ea, b, eb, n) + 1.8e-7 * np.abs(got)) * 1e-3
+    assert np.any(np.abs(got - ref) > d)

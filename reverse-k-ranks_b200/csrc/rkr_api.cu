@@ -136,6 +136,8 @@ int rkr_index_create(int32_t device, const float *user, int64_t n_user, const fl
     if (const char *v = getenv("RKR_REFINE_TC")) ix->refine_tc_on = strcmp(v, "0") != 0;
     // RKR_SCORES_TC=0 keeps the bound rounds' pair scores on the exact tiles (same results)
     if (const char *v = getenv("RKR_SCORES_TC")) ix->scores_tc_on = strcmp(v, "0") != 0;
+    // RKR_COMPACT_SPARSE=0 gives every query the two-pass ordered compaction (same results)
+    if (const char *v = getenv("RKR_COMPACT_SPARSE")) ix->compact_sparse_on = strcmp(v, "0") != 0;
     ix->n_user = n_user;
     ix->n_item = n_item;
     ix->dim = dim;

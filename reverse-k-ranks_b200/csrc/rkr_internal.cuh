@@ -979,6 +979,7 @@ struct rkr_index {
     rkr::DevBuf ri_item_split, ri_imeta_split, ri_item_full, ri_imeta_full;
     // tensor-core pair scores: user digit tiles for the SVD split at check_dim (QSRP) and unsplit (QS, US)
     bool scores_tc_on = true;
+    bool compact_sparse_on = true;            // the sparse ordered compaction (else two-pass for every query)
     int sc_key_split = -2, sc_key_full = -2;  // the split the tiles were built for (-2: none)
     rkr::DevBuf sc_user_split, sc_umeta_split, sc_user_full, sc_umeta_full, sc_cdf_tab;
     std::vector<float> h_item_norm_sorted;
@@ -1037,34 +1038,39 @@ inline int run_compaction(rkr_index *ix, P p, int nq, int topk, QueryCounts *cou
     int2 *off = cnt + (size_t) nq * nchunks;
     int *err = reinterpret_cast<int *>(off + (size_t) nq * nchunks);
     RKR_CUDA(cudaMemsetAsync(err, 0, 2 * sizeof(int), st));
-    RKR_CUDA(cudaMemsetAsync(need_n, 0, sizeof(int32_t) * nq, st));
-    const dim3 g((unsigned) ((U + kNeedSpan - 1) / kNeedSpan), (unsigned) nq);
-    timed(ix, st, "compact_need", [&] { compact_need_kernel<P><<<g, kCompactThreads, 0, st>>>(p, U, need_n, need_u); });
-    RKR_CUDA(cudaGetLastError());
-    timed(ix, st, "compact_emit", [&] {
-        compact_emit_kernel<P><<<(unsigned) nq, kCompactThreads, 0, st>>>(p, topk, need_n, need_u, counts, err, ovf_q);
-    });
-    RKR_CUDA(cudaGetLastError());
     int h_err[2] = {0, 0};
-    RKR_CUDA(cudaMemcpyAsync(h_err, err, sizeof(h_err), cudaMemcpyDeviceToHost, st));
-    RKR_CUDA(cudaStreamSynchronize(st));
-    if (h_err[1]) {
-        const int n_ovf = h_err[1];
-        const dim3 g2((unsigned) nchunks, (unsigned) n_ovf);
-        timed(ix, st, "compact_count", [&] { compact_count_kernel<P><<<g2, kCompactThreads, 0, st>>>(p, U, nchunks, cnt, ovf_q); });
+    int n_two = nq;                  // queries on the two-pass form
+    const int32_t *qmap = nullptr;   // which ones (nullptr: all)
+    if (ix->compact_sparse_on) {
+        RKR_CUDA(cudaMemsetAsync(need_n, 0, sizeof(int32_t) * nq, st));
+        const dim3 g((unsigned) ((U + kNeedSpan - 1) / kNeedSpan), (unsigned) nq);
+        timed(ix, st, "compact_need", [&] { compact_need_kernel<P><<<g, kCompactThreads, 0, st>>>(p, U, need_n, need_u); });
+        RKR_CUDA(cudaGetLastError());
+        timed(ix, st, "compact_emit", [&] {
+            compact_emit_kernel<P><<<(unsigned) nq, kCompactThreads, 0, st>>>(p, topk, need_n, need_u, counts, err, ovf_q);
+        });
+        RKR_CUDA(cudaGetLastError());
+        RKR_CUDA(cudaMemcpyAsync(h_err, err, sizeof(h_err), cudaMemcpyDeviceToHost, st));
+        RKR_CUDA(cudaStreamSynchronize(st));
+        n_two = h_err[1];
+        qmap = ovf_q;
+    }
+    if (n_two) {
+        const dim3 g2((unsigned) nchunks, (unsigned) n_two);
+        timed(ix, st, "compact_count", [&] { compact_count_kernel<P><<<g2, kCompactThreads, 0, st>>>(p, U, nchunks, cnt, qmap); });
         RKR_CUDA(cudaGetLastError());
         timed(ix, st, "compact_scan", [&] {
-            compact_scan_kernel<<<(n_ovf + 127) / 128, 128, 0, st>>>(cnt, nchunks, n_ovf, topk, off, counts, err, ovf_q);
+            compact_scan_kernel<<<(n_two + 127) / 128, 128, 0, st>>>(cnt, nchunks, n_two, topk, off, counts, err, qmap);
         });
         RKR_CUDA(cudaGetLastError());
         timed(ix, st, "compact_write", [&] {
-            compact_write_kernel<P><<<g2, kCompactThreads, 0, st>>>(p, U, nchunks, cnt, off, topk, ovf_q);
+            compact_write_kernel<P><<<g2, kCompactThreads, 0, st>>>(p, U, nchunks, cnt, off, topk, qmap);
         });
         RKR_CUDA(cudaGetLastError());
         RKR_CUDA(cudaMemcpyAsync(h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
         RKR_CUDA(cudaStreamSynchronize(st));
     }
-    if (ix->prof.on) ix->prof.add_count("two_pass_compaction_queries", h_err[1]);
+    if (ix->prof.on) ix->prof.add_count("two_pass_compaction_queries", n_two);
     if (h_err[0]) {
         set_error("internal: candidate count mismatch in %d queries", h_err[0]);
         return RKR_ERR_STATE;

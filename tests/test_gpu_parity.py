@@ -105,15 +105,18 @@ def random_case(seed, n_user, n_item, d, n_query, std=1.0, in_set=0.5):
     return user, item, query
 
 
-@pytest.mark.parametrize("shape,refine,scores", [((1001, 777, 30, 70), "tc", "tc"), ((2500, 3000, 48, 130), "tc", "tc"),
-                                                 ((640, 5000, 150, 64), "tc", "tc"), ((1001, 777, 30, 70), "tiles", "tiles"),
-                                                 ((640, 5000, 150, 64), "tiles", "tiles"),
-                                                 ((2500, 3000, 48, 130), "tc", "tiles")])
-def test_random_qs_qsrp_us_match_oracle(shape, refine, scores, orc, monkeypatch):
+@pytest.mark.parametrize("shape,refine,scores,compact", [
+    ((1001, 777, 30, 70), "tc", "tc", "sparse"), ((2500, 3000, 48, 130), "tc", "tc", "sparse"),
+    ((640, 5000, 150, 64), "tc", "tc", "sparse"), ((1001, 777, 30, 70), "tiles", "tiles", "sparse"),
+    ((640, 5000, 150, 64), "tiles", "tiles", "sparse"), ((2500, 3000, 48, 130), "tc", "tiles", "sparse"),
+    ((1001, 777, 30, 70), "tc", "tc", "two_pass"), ((640, 5000, 150, 64), "tc", "tc", "two_pass")])
+def test_random_qs_qsrp_us_match_oracle(shape, refine, scores, compact, orc, monkeypatch):
     """Both paths of the pair scores and of the refinement: tensor-core scores with exact
-    resolution of undecided pairs ("tc") and the exact SIMT tiles ("tiles")."""
+    resolution of undecided pairs ("tc") and the exact SIMT tiles ("tiles"); and both forms of the
+    ordered compaction (sparse per-query lists, or the two-pass form for every query)."""
     monkeypatch.setenv("RKR_REFINE_TC", "1" if refine == "tc" else "0")
     monkeypatch.setenv("RKR_SCORES_TC", "1" if scores == "tc" else "0")
+    monkeypatch.setenv("RKR_COMPACT_SPARSE", "1" if compact == "sparse" else "0")
     n_user, n_item, d, nq = shape
     user, item, query = random_case(sum(shape), n_user, n_item, d, nq)
     un = orc.normalize(user)

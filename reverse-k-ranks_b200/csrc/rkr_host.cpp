@@ -46,36 +46,72 @@ float cdf_phi(float x) {
 }
 
 // Minimax straight line through (x_i, y_i): minimise e = max |a x_i + b - y_i|, the optimum of
-// the LP in NormalLinearRegressionLP::LinearProgram (:181-213).  Points arrive sorted by x
-// ascending.  The optimal strip's direction is that of a convex-hull edge; each hull-edge slope is
-// tried and the narrowest vertical strip kept.  Double precision.
+// the LP in NormalLinearRegressionLP::LinearProgram (:181-213).  Points arrive sorted by (x, y)
+// ascending.  The optimal strip's direction is that of a convex-hull edge; each hull-edge slope s is
+// tried and the narrowest vertical strip kept.  The strip's top, max (y - s x), lies on the upper
+// hull, whose edge slopes fall along it, at the vertex where they cross s; its bottom, min (y - s x),
+// on the lower hull (rising slopes) likewise: both are found by binary search, and the vertices
+// around the crossing are evaluated so that rounding in the slopes cannot miss the extreme.  Double
+// precision.
 void minimax_fit(const std::vector<double> &xs, const std::vector<double> &ys, double &a, double &b, double &e) {
     const size_t n = xs.size();
     std::vector<size_t> lo, up;
     auto cross = [&](size_t o, size_t p, size_t q) {
         return (xs[p] - xs[o]) * (ys[q] - ys[o]) - (ys[p] - ys[o]) * (xs[q] - xs[o]);
     };
+    lo.reserve(n);
+    up.reserve(n);
+    // the lower hull takes the lowest point at each x, the upper hull the highest: the others can only
+    // sit on a vertical end edge, whose slope is never a candidate and whose top (bottom) point the
+    // other one dominates
     for (size_t i = 0; i < n; i++) {
-        while (lo.size() >= 2 && cross(lo[lo.size() - 2], lo.back(), i) <= 0) lo.pop_back();
-        lo.push_back(i);
-        while (up.size() >= 2 && cross(up[up.size() - 2], up.back(), i) >= 0) up.pop_back();
-        up.push_back(i);
+        if (i == 0 || xs[i] != xs[i - 1]) {
+            while (lo.size() >= 2 && cross(lo[lo.size() - 2], lo.back(), i) <= 0) lo.pop_back();
+            lo.push_back(i);
+        }
+        if (i + 1 == n || xs[i + 1] != xs[i]) {
+            while (up.size() >= 2 && cross(up[up.size() - 2], up.back(), i) >= 0) up.pop_back();
+            up.push_back(i);
+        }
     }
-    double best = std::numeric_limits<double>::infinity(), ba = 0, bb = 0;
-    auto try_slope = [&](double s) {
-        double mx = -std::numeric_limits<double>::infinity(), mn = std::numeric_limits<double>::infinity();
-        for (size_t i : up) { const double r = ys[i] - s * xs[i]; mx = std::max(mx, r); mn = std::min(mn, r); }
-        for (size_t i : lo) { const double r = ys[i] - s * xs[i]; mx = std::max(mx, r); mn = std::min(mn, r); }
-        const double w = 0.5 * (mx - mn);
-        if (w < best) { best = w; ba = s; bb = 0.5 * (mx + mn); }
+    const double inf = std::numeric_limits<double>::infinity();
+    // edge slopes (a vertical edge: +inf; only at the upper hull's start or the lower hull's end)
+    auto slopes = [&](const std::vector<size_t> &h) {
+        std::vector<double> sl(h.size() > 1 ? h.size() - 1 : 0);
+        for (size_t k = 0; k + 1 < h.size(); k++) {
+            const double dx = xs[h[k + 1]] - xs[h[k]];
+            sl[k] = dx != 0 ? (ys[h[k + 1]] - ys[h[k]]) / dx : inf;
+        }
+        return sl;
     };
+    const std::vector<double> s_up = slopes(up), s_lo = slopes(lo);
+    constexpr size_t kWin = 3;
+    auto top = [&](double s) {  // max (y - s x) over the upper hull
+        const size_t k = std::partition_point(s_up.begin(), s_up.end(), [&](double v) { return v > s; }) - s_up.begin();
+        double m = -inf;
+        for (size_t j = k > kWin ? k - kWin : 0; j < std::min(up.size(), k + kWin + 1); j++)
+            m = std::max(m, ys[up[j]] - s * xs[up[j]]);
+        return m;
+    };
+    auto bottom = [&](double s) {  // min (y - s x) over the lower hull
+        const size_t k = std::partition_point(s_lo.begin(), s_lo.end(), [&](double v) { return v < s; }) - s_lo.begin();
+        double m = inf;
+        for (size_t j = k > kWin ? k - kWin : 0; j < std::min(lo.size(), k + kWin + 1); j++)
+            m = std::min(m, ys[lo[j]] - s * xs[lo[j]]);
+        return m;
+    };
+    double best = inf, ba = 0, bb = 0;
     for (const auto *h : {&lo, &up})
         for (size_t k = 0; k + 1 < h->size(); k++) {
             const double dx = xs[(*h)[k + 1]] - xs[(*h)[k]];
-            if (dx != 0) try_slope((ys[(*h)[k + 1]] - ys[(*h)[k]]) / dx);
+            if (dx == 0) continue;
+            const double s = (ys[(*h)[k + 1]] - ys[(*h)[k]]) / dx;
+            const double mx = top(s), mn = bottom(s);
+            const double w = 0.5 * (mx - mn);
+            if (w < best) { best = w; ba = s; bb = 0.5 * (mx + mn); }
         }
-    if (!(best < std::numeric_limits<double>::infinity())) {
-        double mx = -std::numeric_limits<double>::infinity(), mn = std::numeric_limits<double>::infinity();
+    if (!(best < inf)) {
+        double mx = -inf, mn = inf;
         for (size_t i = 0; i < n; i++) { mx = std::max(mx, ys[i]); mn = std::min(mn, ys[i]); }
         ba = 0;
         bb = n ? 0.5 * (mx + mn) : 0;
@@ -111,14 +147,20 @@ void fit_user(const float *thr, int S, float *rec) {
         xs.push_back(cdf[j + 1]); ys.push_back(j + 1);
         xs.push_back(cdf[j]); ys.push_back(j + 1);
     }
-    // restore exact ascending order on ties/NaN-free input
-    std::vector<size_t> ord(xs.size());
-    std::iota(ord.begin(), ord.end(), 0);
-    std::stable_sort(ord.begin(), ord.end(), [&](size_t p, size_t q) {
-        return xs[p] < xs[q] || (xs[p] == xs[q] && ys[p] < ys[q]);
-    });
-    std::vector<double> sx(xs.size()), sy(ys.size());
-    for (size_t i = 0; i < ord.size(); i++) { sx[i] = xs[ord[i]]; sy[i] = ys[ord[i]]; }
+    // ascending (x, y) order: a stable insertion sort, linear here since the walk above leaves only
+    // adjacent equal-x pairs out of order (the same order a stable sort of any input gives)
+    std::vector<double> &sx = xs, &sy = ys;
+    for (size_t i = 1; i < sx.size(); i++) {
+        const double x = sx[i], y = sy[i];
+        size_t k = i;
+        while (k > 0 && (x < sx[k - 1] || (x == sx[k - 1] && y < sy[k - 1]))) {
+            sx[k] = sx[k - 1];
+            sy[k] = sy[k - 1];
+            k--;
+        }
+        sx[k] = x;
+        sy[k] = y;
+    }
     double a = 0, b = 0, e = -1;
     if (!sx.empty()) minimax_fit(sx, sy, a, b, e);
     float err = (float) e;
@@ -330,15 +372,28 @@ int rkr_svd_build(const float *user, int64_t n_user, int32_t dim, float sigma_ra
     }
     const int d = dim;
     std::vector<double> G((size_t) d * d, 0.0);
+    // the Gram matrix's upper triangle, kGramBlock users per pass over a thread's partial sums (each
+    // entry still adds the users' products one after another)
+    constexpr int kGramBlock = 8;
 #pragma omp parallel
     {
         std::vector<double> g((size_t) d * d, 0.0);
+        std::vector<double> rb((size_t) kGramBlock * d);
 #pragma omp for schedule(static)
-        for (int64_t u = 0; u < n_user; u++) {
-            const float *r = user + u * d;
+        for (int64_t u0 = 0; u0 < n_user; u0 += kGramBlock) {
+            const int nb = (int) std::min<int64_t>(kGramBlock, n_user - u0);
+            for (int b = 0; b < kGramBlock; b++)
+                for (int i = 0; i < d; i++) rb[(size_t) b * d + i] = b < nb ? (double) user[(u0 + b) * d + i] : 0.0;
             for (int i = 0; i < d; i++) {
-                const double ri = r[i];
-                for (int j = i; j < d; j++) g[(size_t) i * d + j] += ri * r[j];
+                double ri[kGramBlock];
+                for (int b = 0; b < kGramBlock; b++) ri[b] = rb[(size_t) b * d + i];
+                double *gi = g.data() + (size_t) i * d;
+#pragma omp simd
+                for (int j = i; j < d; j++) {
+                    double acc = gi[j];
+                    for (int b = 0; b < kGramBlock; b++) acc += ri[b] * rb[(size_t) b * d + j];
+                    gi[j] = acc;
+                }
             }
         }
 #pragma omp critical
@@ -391,13 +446,27 @@ int rkr_svd_build(const float *user, int64_t n_user, int32_t dim, float sigma_ra
     }
     for (int r = 0; r < d; r++)
         for (int c = 0; c < d; c++) transfer_item[(size_t) r * d + c] = (float) (s[r] * (float) Es[(size_t) c * d + r]);
-#pragma omp parallel for schedule(static)
-    for (int64_t u = 0; u < n_user; u++) {
-        const float *row = user + u * d;
-        for (int k = 0; k < d; k++) {
-            double acc = 0;
-            for (int i = 0; i < d; i++) acc += (double) row[i] * Es[(size_t) i * d + k];
-            svd_user[u * d + k] = s[k] > 0 ? (float) (acc / s[k]) : 0.0f;
+    // svd_user = user Es diag(1/s), kProjBlock users at a time, each output summed over i in order
+    constexpr int kProjBlock = 4;
+#pragma omp parallel
+    {
+        std::vector<double> acc((size_t) kProjBlock * d);
+#pragma omp for schedule(static)
+        for (int64_t u0 = 0; u0 < n_user; u0 += kProjBlock) {
+            const int nb = (int) std::min<int64_t>(kProjBlock, n_user - u0);
+            std::fill(acc.begin(), acc.end(), 0.0);
+            for (int i = 0; i < d; i++) {
+                const double *ei = Es.data() + (size_t) i * d;
+                for (int b = 0; b < nb; b++) {
+                    const double ri = user[(u0 + b) * d + i];
+                    double *ab = acc.data() + (size_t) b * d;
+#pragma omp simd
+                    for (int k = 0; k < d; k++) ab[k] += ri * ei[k];
+                }
+            }
+            for (int b = 0; b < nb; b++)
+                for (int k = 0; k < d; k++)
+                    svd_user[(u0 + b) * d + k] = s[k] > 0 ? (float) (acc[(size_t) b * d + k] / s[k]) : 0.0f;
         }
     }
     std::vector<float> cum(d);

@@ -373,6 +373,65 @@ void orc_regression_rank_bound(float qlb, float qub, const float *ab, const floa
     }
 }
 
+/* Level of a rank bound in the engine's encoding: 0 -> rank 0, l in [1, S] -> sample_rank[l - 1],
+ * S + 1 -> n_item (the rank bounds ComputeRankBound can return are exactly these). */
+static int32_t orc_rank_level(int32_t r, const int32_t *sample_rank, int32_t n_sample, int64_t n_item) {
+    if (r == 0) return 0;
+    if (r == n_item) return n_sample + 1;
+    int32_t lo = 0, hi = n_sample - 1;
+    while (lo < hi) {  /* first index with sample_rank[index] >= r */
+        const int32_t m = (lo + hi) / 2;
+        if (sample_rank[m] < r) lo = m + 1; else hi = m;
+    }
+    return lo + 1;
+}
+
+/* The binary32 values as ordered integers: k(x) < k(y) <=> x < y (no NaN). */
+static int64_t orc_fkey(float x) {
+    int32_t i;
+    memcpy(&i, &x, 4);
+    return i >= 0 ? (int64_t) i : -(int64_t) (i & 0x7fffffff);
+}
+static float orc_fval(int64_t k) {
+    const int32_t i = k >= 0 ? (int32_t) k : (int32_t) ((-k) | 0x80000000);
+    float x;
+    memcpy(&x, &i, 4);
+    return x;
+}
+
+/* Score boundaries of one user's rank bound, side 0 the lower bound (a function of qlb), side 1 the
+ * upper bound (of qub): out[g] = the smallest binary32 score whose level (orc_rank_level of
+ * ComputeRankBound, NormalLinearRegressionLP.hpp:326-380) is <= g * stride, g = 0 .. n_out - 1;
+ * +inf where no finite score reaches it, -inf where every finite score does.  Bisection on the
+ * ordered binary32 values; the level never rises with the score (tests/test_level_monotone.py), so
+ * a score's level lies in (g_1 stride, g_0 stride] for the boundaries g_0, g_1 around it.  A checker
+ * for level-boundary tables built on the device. */
+void orc_level_boundaries(const float *rec, const int32_t *sample_rank, int32_t n_sample, int64_t n_item,
+                          int32_t stride, int32_t side, int32_t n_out, float *out) {
+    const int64_t klo = orc_fkey(-INFINITY), khi = orc_fkey(INFINITY);
+    for (int32_t g = 0; g < n_out; g++) {
+        const int32_t L = g * stride;
+        /* level(x) <= L is monotone in x: false ... false true ... true; find the first true */
+        int64_t lo = klo, hi = khi;  /* invariant: level(fval(hi)) <= L or hi = khi */
+        int32_t rl, ru;
+        orc_regression_rank_bound(INFINITY, INFINITY, rec, rec + 2, rec[4], rec + 5, sample_rank, n_sample, n_item,
+                                  &rl, &ru);
+        const int32_t top = orc_rank_level(side ? ru : rl, sample_rank, n_sample, n_item);
+        if (top > L) { out[g] = INFINITY; continue; }
+        orc_regression_rank_bound(-INFINITY, -INFINITY, rec, rec + 2, rec[4], rec + 5, sample_rank, n_sample, n_item,
+                                  &rl, &ru);
+        const int32_t bottom = orc_rank_level(side ? ru : rl, sample_rank, n_sample, n_item);
+        if (bottom <= L) { out[g] = -INFINITY; continue; }
+        while (hi - lo > 1) {
+            const int64_t m = lo + (hi - lo) / 2;
+            const float x = orc_fval(m);
+            orc_regression_rank_bound(x, x, rec, rec + 2, rec[4], rec + 5, sample_rank, n_sample, n_item, &rl, &ru);
+            if (orc_rank_level(side ? ru : rl, sample_rank, n_sample, n_item) <= L) hi = m; else lo = m;
+        }
+        out[g] = orc_fval(hi);
+    }
+}
+
 /* The LP optimum itself (min e s.t. |a x_i + b - y_i| <= e) comes from minimax_line.h.  The
  * reference solves it with a randomised Seidel LP whose constraint order comes from
  * std::random_device (NormalLinearRegressionLP.hpp:97-100), so its (a, b) are not reproducible

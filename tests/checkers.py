@@ -136,6 +136,14 @@ class Oracle:
             lb[i], ub[i] = l.value, h.value
         return lb, ub
 
+    def level_boundaries(self, rec, sample_rank, n_item, stride, side, n_out):
+        """orc_level_boundaries: the smallest score whose rank-bound level is <= g * stride."""
+        rec, sr = _f32(rec), _i32(sample_rank)
+        out = np.empty(n_out, np.float32)
+        self.lib.orc_level_boundaries(_p(rec), _p(sr), C.c_int32(sr.shape[0]), C.c_int64(n_item), C.c_int32(stride),
+                                      C.c_int32(side), C.c_int32(n_out), _p(out))
+        return out
+
     def qs_retrieval(self, user, item, check_dim, sample_rank, thr, query, topk):
         user, item, sr, thr, query = _f32(user), _f32(item), _i32(sample_rank), _f32(thr), _f32(query)
         nq = query.shape[0]

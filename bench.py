@@ -13,9 +13,15 @@ value      queries/s with the queries and results resident in device memory (CUD
 e2e        queries/s through the public host API (rkr_retrieval), host->device copy of the queries
            and device->host copy of the results inside every timed step;
 roofline   the dominant kernel's algorithmic throughput from live per-kernel event timing;
+plain_fp32_gpu  the same batches through the engine's exact FP32 SIMT form (no tensor cores:
+           exact register-tiled score tiles and refinement tiles), the baseline the metric names;
+           vs_baseline = value / its value;
 cpu_baseline  the reference's own QSRPNormalLP::Retrieval (oracle/_ref) on a bounded sample of
            the same queries, all host threads.
---impl reference times only that reference path and prints its line.
+--impl reference times only that reference path and prints its line.  Its index is built on the
+host without the engine library: the reference's own normalisation, sample-item draw, sample-rank
+program, regression fit and SVD (oracle/_ref), with score rows from a BLAS product sorted per
+user (numpy), standing in for the reference's ComputeScoreTableBatch rows.
 
 Multi-GPU (torchrun): every rank holds a replica of the index and answers its own batch of
 queries (weak scaling, no collective on the data path).
@@ -127,6 +133,133 @@ def build_index(R, user_raw, item, cfg, device):
     return ix, parts, stages
 
 
+def _score_blocks(user, item, n_thread, block, fn):
+    """Calls fn(u0, rows) for consecutive blocks of users, rows = user[u0:u0+block] @ item.T (BLAS,
+    float32), on n_thread host threads (numpy releases the GIL in the product and the sort)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    def one(u0):
+        fn(u0, user[u0:u0 + block] @ item.T)
+
+    with ThreadPoolExecutor(max(1, n_thread)) as ex:
+        list(ex.map(one, range(0, user.shape[0], block)))
+
+
+def build_index_reference(user_raw, item, cfg, n_thread):
+    """The reference arm's index, built on the host without the engine library.
+
+    The reference's own code (oracle/_ref) normalises the users (readData), draws the sampled items
+    (SampleItem), picks the sample ranks (ComputeSortKthRank, FindOptimalSampleFast), fits the
+    regression models (NormalLinearRegressionLP) and the SVD transform.  The score rows its build apps
+    sort (ComputeScoreTableBatch, QueryRankByComputation) come from a float32 BLAS product sorted per
+    user: the same index up to the last bit of a few scores, built in seconds instead of the
+    reference's CPU build (about 15 minutes on 16 threads at config 2).  Returns the parts
+    ReferenceTimer takes and the stage times."""
+    from checkers import Reference
+    n_user, n_item, dim, n_sample, n_si, stopk = CONFIGS[cfg][:6]
+    ref = Reference(n_thread)
+    stages = {}
+    t = time.perf_counter()
+    with quiet_stdout():
+        user = ref.normalize(user_raw)
+    stages["normalize"] = time.perf_counter() - t
+    t = time.perf_counter()
+    with quiet_stdout():
+        si = ref.sample_item(n_item, n_si)
+    ranks = np.empty((n_user, n_si), np.int32)
+
+    def qrank(u0, rows):
+        # rank of a sampled item = items scoring strictly above it (QueryRankByComputation.hpp)
+        s = rows[:, si]
+        rows.sort(axis=1)
+        for i in range(rows.shape[0]):
+            ranks[u0 + i] = n_item - np.searchsorted(rows[i], s[i], side="right")
+
+    block = max(64, (256 << 20) // (4 * n_item))  # about 256 MB of score rows per thread
+    _score_blocks(user, item, n_thread, block, qrank)
+    accu = np.empty((n_si, n_item + 1), np.int32)
+    for j in range(n_si):
+        accu[j] = np.cumsum(np.bincount(ranks[:, j], minlength=n_item + 1))
+    stages["query_rank_distribution"] = time.perf_counter() - t
+    t = time.perf_counter()
+    with quiet_stdout():
+        rank, _ = ref.find_optimal_sample_rank(n_user, n_item, n_sample, si, accu, stopk)
+    stages["sample_rank"] = time.perf_counter() - t
+    t = time.perf_counter()
+    thr = np.empty((n_user, n_sample), np.float32)
+    desc = (n_item - 1 - rank).astype(np.int64)  # positions in an ascending row
+
+    def thresholds(u0, rows):
+        rows.sort(axis=1)
+        thr[u0:u0 + rows.shape[0]] = rows[:, desc]
+
+    _score_blocks(user, item, n_thread, block, thresholds)
+    stages["thresholds"] = time.perf_counter() - t
+    t = time.perf_counter()
+    with quiet_stdout():
+        reg = ref.fit_regression(thr, n_item, rank)
+    stages["regression_fit"] = time.perf_counter() - t
+    t = time.perf_counter()
+    with quiet_stdout():
+        ti, su, cd = ref.svd_build(user, item, 0.7)
+    stages["svd"] = time.perf_counter() - t
+    return dict(user=user, rank=rank, thr=thr, reg=reg, ti=ti, su=su, cd=cd), stages
+
+
+def run_reference(args):
+    """--impl reference: the reference's own QSRPNormalLP::Retrieval (oracle/_ref) on an index built
+    without the engine (build_index_reference), each step a bounded sample of the step's batch on
+    all host threads.  Touches no GPU."""
+    n_user, n_item, dim, n_sample, n_si, stopk, batch, topk = CONFIGS[args.config]
+    if args.batch:
+        batch = args.batch
+    if args.config == "config5":
+        print(json.dumps({"impl": "reference", "unavailable": "config5 is a serving loop of the engine; the "
+                          "reference arm is timed on config2/config4 batches"}))
+        return
+    if not reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (needs the reference "
+                          "sources at build time)"}))
+        return
+    n_thread = os.cpu_count() or 1
+    log(f"[bench-ref] generating {args.config} data")
+    user_raw, item, qrng = make_data(args.config, args.seed, 0)
+    t0 = time.perf_counter()
+    parts, stages = build_index_reference(user_raw, item, args.config, n_thread)
+    build_sec = time.perf_counter() - t0
+    log(f"[bench-ref] index built on the host in {build_sec:.1f}s: " +
+        ", ".join(f"{k} {v:.2f}s" for k, v in stages.items()))
+    timer = ReferenceTimer(parts, item, n_thread)
+    runs = []
+    for s in range(args.warmup + args.steps):
+        q = item[qrng.choice(n_item, size=batch, replace=False)].copy()
+        n, secs, _ = timer.run(q, topk, args.cpu_seconds / 4)
+        if s >= args.warmup:
+            runs.append((n, secs))
+    timer.close()
+    secs = sum(r[1] for r in runs)
+    nqs = sum(r[0] for r in runs)
+    v = nqs / secs
+    model = cpu_model()
+    sample = (f"the first {runs[-1][0]} of each step's {batch} queries through the reference's "
+              f"QSRPNormalLP::Retrieval (oracle/_ref, the reference's unmodified headers), {n_thread} OpenMP "
+              f"threads on {model}")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "queries/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / len(runs),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded numpy N(0,1/150) users, lognormal-scaled N(0,1/150) items, queries drawn "
+                    "from the items; index built on the host without the engine (reference code + BLAS rows)",
+            "config": {"workload": f"{args.config}: {n_user} users x {n_item} items, d={dim}, {n_sample} sampled "
+                                   f"thresholds/user + NormalLinearRegressionLP + SVD, QSRPNormalLP, "
+                                   f"{batch} queries/step, k={topk}",
+                       "sample_queries_per_step": int(round(nqs / len(runs)))},
+            "build_sec_host": build_sec, "build_stages_sec": {k: round(v_, 3) for k, v_ in stages.items()},
+            "cpu_baseline": {"value": v, "unit": "queries/s", "cores": n_thread, "cpu_model": model,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
 class Clocks:
     """SM clock and throttle reasons while the timed region runs: one `nvidia-smi -lms 200` process
     started before warm-up and stopped after the timed steps; only samples inside the timed
@@ -192,41 +325,49 @@ def kernel_model(name, cfg, nq, stats, method):
     sizes.
 
     dot_flops counts the exact dot products' binary32 multiplies and adds as separate operations (2 per
-    coordinate and pair).  bytes is what the kernel must move through HBM at the least.  tensor_ops
-    counts the tensor-core operations the kernel issues for them: the pair scores and the refinement
-    both run ten int8 digit products per coordinate (K padded to 32 per part)."""
-    n_user, n_item, dim = CONFIGS[cfg][:3]
+    coordinate and pair).  bytes is what the kernel must move through HBM at the least: for the pair
+    scores (the bound rounds' stream over the resident index) one pass over every user's vector at
+    2 bytes a coordinate, its 28-byte regression record (QSRPNormalLP) and its S sampled thresholds,
+    U * (2 d + 28 + 4 S) per batch, whatever the kernel itself stores per pair.  tensor_ops counts the
+    tensor-core operations the kernel issues: ten int8 digit products per coordinate (K padded to 32
+    per part)."""
+    n_user, n_item, dim, n_sample = CONFIGS[cfg][:4]
     pairs = float(n_user) * nq
     r32 = lambda x: (x + 31) // 32 * 32
     if name == "qsrp_scores_tc":
         qsrp = method == "QSRPNormalLP"
         cd = stats["check_dim"] if qsrp else dim
         kp = r32(cd) + (r32(dim - cd) if dim > cd else 0)
-        # per pair: levels (4 B, QSRP) + coarse group (1 B) + score (4 B) written; per user its digits
-        # (4 kp B), scale and norms (16 B), threshold summary (128 B) and regression record (32 B) read
-        out = (9.0 if qsrp else 5.0) * pairs
-        per_user = 4.0 * kp + 16 + 128 + (32 if qsrp else 0)
-        return 2.0 * pairs * dim, out + n_user * per_user + nq * (4.0 * kp + 20), 10 * 2.0 * pairs * kp
-    if name == "qsrp_round2":
-        return 0.0, 4.0 * pairs + 1.0 * pairs, 0.0
-    if name == "level_hist":
-        return 0.0, 4.0 * pairs, 0.0
+        per_user = 2.0 * dim + (28.0 if qsrp else 0.0) + 4.0 * n_sample
+        return 2.0 * pairs * dim, n_user * per_user + nq * 4.0 * dim, 10 * 2.0 * pairs * kp
     if name == "refine_tc":
-        # per (candidate, item) pair in the norm cut-off; the items' digit chunks read once at the least
+        # per (candidate, item) pair in the norm cut-off; the items read once at the least
         n = stats["n_compute_item"]
         cd = stats["check_dim"] if method != "US" else dim
         kp = r32(cd) + (r32(dim - cd) if dim > cd else 0)
-        return 2.0 * n * dim, 4.0 * kp * n_item, 10 * 2.0 * n * kp
+        return 2.0 * n * dim, 2.0 * dim * n_item, 10 * 2.0 * n * kp
     return 0.0, 0.0, 0.0
 
 
-# DRAM bytes (read + write) per (query, user) pair of the dominant kernel, from one ncu capture at a
-# 200-query batch of the same workload (profiles/qsrp_tc_kernels_batch200_full.md); traffic grows
-# with the pairs a launch processes, so a launch's traffic is this figure times its pairs.
+# DRAM bytes (read + write) per (query, user) pair of the pair-scores kernel, measured by one ncu
+# capture at a 200-query batch of the config-2 workload; traffic grows with the pairs a launch
+# processes, so a launch's traffic is this figure times its pairs.
 NCU_BYTES_PER_PAIR = {("qsrp_scores_tc", "QSRPNormalLP"): (456.031e6 + 814.108e6) / (200 * 480189.0)}
 
 # Nominal dense tensor-core peaks of one B200 (T ops/s), for the tensor_ops figures.
 TENSOR_PEAK_NOMINAL = {"qsrp_scores_tc": ("int8", 4500.0), "refine_tc": ("int8", 4500.0)}
+
+
+def cpu_model():
+    """The host CPU's model name (first 'model name' line of /proc/cpuinfo)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
 
 class ReferenceTimer:
@@ -319,12 +460,20 @@ def main():
     ap.add_argument("--batch", type=int, default=0, help="queries per step (default: the workload's)")
     ap.add_argument("--serve-requests", type=int, default=200, help="config5: requests per trace")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="config5: offered requests/s")
+    ap.add_argument("--no-plain", dest="plain", action="store_false",
+                    help="skip timing the plain FP32 GPU form")
     args = ap.parse_args()
 
-    import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank_id = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        # rank 0 alone times the reference's CPU path; other ranks exit without work
+        if rank_id == 0:
+            run_reference(args)
+        return
+
+    import torch
     dist = None
     if world > 1:
         import datetime
@@ -339,11 +488,6 @@ def main():
         batch = 100  # US answers exactly 100 queries per call when S <= 1000 (US.hpp:117-131)
     n_thread = os.cpu_count() or 1
 
-    if args.impl == "reference" and rank_id != 0:
-        if dist:
-            dist.destroy_process_group()
-        return
-
     import rkr_b200 as R
     log(f"[bench] rank {rank_id}/{world}: generating {args.config} data")
     user_raw, item, qrng = make_data(args.config, args.seed, rank_id)
@@ -357,10 +501,7 @@ def main():
         return item[qrng.choice(n_item, size=batch, replace=False)].copy()
 
     if args.config == "config5":
-        if args.impl == "reference" or rank_id != 0:
-            if args.impl == "reference":
-                print(json.dumps({"impl": "reference", "unavailable": "config5 is a serving loop of the engine; "
-                                  "the reference arm is timed on config2/config4 batches"}))
+        if rank_id != 0:
             ix.close()
             if dist:
                 dist.destroy_process_group()
@@ -390,36 +531,6 @@ def main():
                 "build_sec": build_sec, "hbm_index_bytes": ix.size_bytes(), "clocks": clk.summary()}
         print(json.dumps(line))
         ix.close()
-        return
-
-    if args.impl == "reference":
-        if not reference_available():
-            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (needs the reference "
-                              "sources at build time)"}))
-            return
-        timer = ReferenceTimer(parts, item, n_thread)
-        runs = []
-        for s in range(args.warmup + args.steps):
-            n, secs = timer.run(draw_batch(), topk, args.cpu_seconds / 2)
-            if s >= args.warmup:
-                runs.append((n, secs))
-        timer.close()
-        secs = sum(r[1] for r in runs)
-        nqs = sum(r[0] for r in runs)
-        v = nqs / secs
-        sample = (f"{runs[-1][0]} of each step's {batch} queries through the reference's QSRPNormalLP::Retrieval "
-                  f"(oracle/_ref, the reference's unmodified headers), {n_thread} OpenMP threads")
-        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "queries/s", "n_gpus": 1,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / len(runs),
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-                "data": "synthetic (seeded numpy; index built with librkr_b200, bit-identical to the reference's)",
-                "config": {"workload": f"{args.config}: {n_user} users x {n_item} items, d={dim}, {n_sample} "
-                                       f"thresholds + regression, QSRPNormalLP, k={topk}",
-                           "sample_queries_per_step": int(round(nqs / len(runs)))},
-                "cpu_baseline": {"value": v, "unit": "queries/s", "cores": n_thread, "kind": "reference",
-                                 "sample": sample},
-                "e2e": {"value": v, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line))
         return
 
     # ---- device-resident timing -------------------------------------------------------------------
@@ -461,6 +572,54 @@ def main():
     total_ms = max_over_ranks(total_ms, dist, "cuda")
     value = job_rate(world, batch * args.steps, total_ms / 1e3)
 
+    # ---- the plain FP32 GPU form on the same batches ---------------------------------------------------
+    # A second index over the same data with the tensor-core paths off: exact register-tiled FP32
+    # score tiles and refinement tiles (the results are the same; only the arithmetic path differs).
+    plain = None
+    if args.plain:
+        os.environ["RKR_SCORES_TC"] = "0"
+        os.environ["RKR_REFINE_TC"] = "0"
+        try:
+            ixp = R.Index(parts["user"], item, device=local)
+        finally:
+            os.environ.pop("RKR_SCORES_TC")
+            os.environ.pop("RKR_REFINE_TC")
+        ixp.load_sample_search(parts["rank"], parts["thr"])
+        ixp.load_svd(parts["cd"], parts["ti"], parts["su"])
+        ixp.load_regression(parts["rank"], parts["reg"])
+        d_out_p = torch.empty_like(d_out)
+
+        def run_plain(dq):
+            return ixp.retrieval_device(args.method, dq.data_ptr(), batch, topk, d_out_p.data_ptr(), 0,
+                                        stream=stream.cuda_stream)
+
+        for s in range(args.warmup):
+            run_plain(batches[s])
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for s in range(args.steps):
+            run_plain(batches[args.warmup + s])
+        p1.record(stream)
+        torch.cuda.synchronize()
+        plain_ms = max_over_ranks(p0.elapsed_time(p1), dist, "cuda")
+        # the same queries answered by both forms (both started from the same carried state) agree
+        ix.reset_state()
+        ixp.reset_state()
+        run_step(batches[0])
+        run_plain(batches[0])
+        torch.cuda.synchronize()
+        same_plain = bool(torch.equal(d_out, d_out_p))
+        ixp.close()
+        plain = {"value": job_rate(world, batch * args.steps, plain_ms / 1e3), "unit": "queries/s",
+                 "ms_per_step": plain_ms / args.steps,
+                 "form": "exact FP32 SIMT tiles for the pair scores and the refinement (RKR_SCORES_TC=0 "
+                         "RKR_REFINE_TC=0), same pipeline otherwise",
+                 "results_identical": same_plain}
+
     # ---- per-kernel profile of one more step (outside the timed region) ---------------------------------
     ix.profile(True)
     run_step(batches[0])
@@ -482,11 +641,13 @@ def main():
     peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     ncu_bpp = NCU_BYTES_PER_PAIR.get((dom_name, args.method))
+    traffic = (ncu_bpp * CONFIGS[args.config][0] * batch
+               if ncu_bpp is not None and args.config == "config2" else None)
     roofline = {"kernel": dom_name, "bound": "hbm", "achieved": nbytes / avg_s / 1e9, "peak": hbm_peak,
                 "unit": "GB/s", "frac": (nbytes / avg_s / 1e9) / hbm_peak,
-                "peak_source": "MEASURED_PEAKS.json" if peaks else "fallback",
-                "traffic": (ncu_bpp * CONFIGS[args.config][0] * batch
-                            if ncu_bpp is not None and args.config == "config2" else None),
+                "peak_source": "MEASURED_PEAKS.json (of measured)" if peaks else "fallback",
+                "algorithmic_bytes": nbytes, "traffic": traffic,
+                "traffic_over_algorithmic": traffic / nbytes if traffic and nbytes else None,
                 "avg_launch_ms": avg_s * 1e3,
                 "share_of_step": dom_ms / max(sum(v[0] for v in prof.values()), 1e-9),
                 "dot_tflops_fp32_equivalent": ops / avg_s / 1e12}
@@ -540,7 +701,7 @@ def main():
         got = ix.retrieval(args.method, qs[:n], topk)
         flat = lambda x: np.ascontiguousarray(x).view(np.int32).reshape(-1)
         same = got.shape == ref_res.shape and np.array_equal(flat(got), flat(ref_res))
-        cpu = {"value": n / secs, "unit": "queries/s", "cores": n_thread, "kind": "reference",
+        cpu = {"value": n / secs, "unit": "queries/s", "cores": n_thread, "cpu_model": cpu_model(), "kind": "reference",
                "sample": f"{n} of the step's {batch} queries through the reference's QSRPNormalLP::Retrieval "
                          f"(oracle/_ref, the reference's unmodified headers) on the same index, {n_thread} threads",
                "results_identical_to_engine": bool(same)}
@@ -576,7 +737,10 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "scaling": "weak", "vs_baseline": (value / plain["value"]) if plain else None,
+            "vs_baseline_basis": "value / plain_fp32_gpu.value (the plain FP32 GPU form the metric names, "
+                                 "timed on the same batches in the same run; no published number exists)",
+            "dtype": "f32",
             "data": "synthetic: seeded numpy N(0,1/150) users, lognormal-scaled N(0,1/150) items, queries drawn "
                     "from the items",
             "config": {"workload": f"{args.config}: {n_user} users x {n_item} items, d={dim}, {n_sample} sampled "
@@ -590,7 +754,7 @@ def main():
             "single_query_p99_ms": float(np.percentile(single, 99)) if single else None,
             "build_sec": build_sec, "build_stages_sec": {k: round(v, 3) for k, v in stages.items()},
             "hbm_index_bytes": ix.size_bytes(), "e2e": e2e, "gpu_launches": int(launches_per_step * args.steps), "roofline": roofline,
-            "cpu_baseline": cpu, "clocks": clk.summary(), "query_stats_mean": stats_mean,
+            "plain_fp32_gpu": plain, "cpu_baseline": cpu, "clocks": clk.summary(), "query_stats_mean": stats_mean,
         }
         print(json.dumps(line))
     ix.close()

@@ -161,8 +161,9 @@ int rkr_index_query_rank_distribution(rkr_index *index, const int32_t *sample_it
  * library keeps until the process exits; it holds at most 16384 sample ranks and batches of
  * (32 MiB - 64 KiB) / (4 * round_up(n_item, 4)) score rows, and n_item must also fit the
  * shared-memory row selection (about 24,000 items on B200); larger sizes are RKR_ERR_INVALID.
- * The first call on a device looks the array's device address up (cudaGetSymbolAddress), so
- * make that first call before any stream capture.  Calls share the array: calls that overlap on
+ * Every call looks up the array's device address in the current device's context
+ * (cudaGetSymbolAddress), so the address stays right after a device reset.  Calls share the
+ * array: calls that overlap on
  * the GPU (other streams, other host threads) race; the call returns after its work on `stream`
  * (a cudaStream_t, NULL for the legacy default stream) has finished.  There is no counterpart in
  * the reference, which always allocates its score-table buffers. */

@@ -8,7 +8,6 @@
 // only the bins that contain a requested position.  The row is never sorted as a whole unless a
 // full sort is what the caller wants (rkr_score_sort_batch).
 #include <algorithm>
-#include <mutex>
 #include <vector>
 
 #include "rkr_internal.cuh"
@@ -277,6 +276,21 @@ __global__ void prefix_rows_kernel(int32_t *__restrict__ h, int rows, int64_t le
 
 namespace {
 
+// Raises row_select_kernel's dynamic shared-memory limit on the current device to the largest the
+// device allows.  Every caller sets the same value, so callers on other host threads never lower
+// the limit under each other's launches; it is set on every call (cheap) rather than cached, so a
+// device reset, which restores the default, needs no special handling.
+int row_select_allow_max_smem() {
+    int dev = 0, optin = 0;
+    RKR_CUDA(cudaGetDevice(&dev));
+    RKR_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    cudaFuncAttributes fa;
+    RKR_CUDA(cudaFuncGetAttributes(&fa, row_select_kernel));
+    RKR_CUDA(cudaFuncSetAttribute(row_select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  optin - (int) fa.sharedSizeBytes));
+    return RKR_OK;
+}
+
 struct RowPipeline {
     rkr_index *ix;
     int64_t batch = 0;
@@ -298,7 +312,7 @@ int setup_pipeline(rkr_index *ix, RowPipeline &P) {
     P.smem = (size_t) 2 * n * sizeof(float);
     P.use_smem = P.smem + static_smem + 1024 <= (size_t) dev_smem;
     if (!P.use_smem) P.smem = 0;
-    else RKR_CUDA(cudaFuncSetAttribute(row_select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) P.smem));
+    else RKR_TRY(row_select_allow_max_smem());
     int sms = 0;
     RKR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ix->device));
     P.grid = sms * (P.use_smem ? 1 : 2);
@@ -415,27 +429,17 @@ constexpr size_t kStaticRankBytes = size_t(64) << 10;
 constexpr int kStaticMaxSample = (int) (kStaticRankBytes / sizeof(int32_t));
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
-namespace {
-std::mutex g_static_mu;
-void *g_static_addr[256];  // per device, filled on the first call on that device
-}  // namespace
-
-static int static_scratch_address(int dev, unsigned char **out) {
-    std::lock_guard<std::mutex> lock(g_static_mu);
-    if (dev < 0 || dev >= 256) {
-        set_error("rkr_build_thresholds_static: device ordinal %d out of range", dev);
-        return RKR_ERR_INVALID;
+// The array's device address in the current device's context.  It is looked up on every call
+// (cudaGetSymbolAddress is cheap once the module is loaded) instead of being cached, so that the
+// address is right after a device reset, which reloads the module in a new context.
+static int static_scratch_address(unsigned char **out) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess) {
+        set_error("rkr_build_thresholds_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+        return RKR_ERR_CUDA;
     }
-    if (!g_static_addr[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
-        if (e != cudaSuccess) {
-            set_error("rkr_build_thresholds_static: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
-            return RKR_ERR_CUDA;
-        }
-        g_static_addr[dev] = p;
-    }
-    *out = static_cast<unsigned char *>(g_static_addr[dev]);
+    *out = static_cast<unsigned char *>(p);
     return RKR_OK;
 }
 
@@ -470,12 +474,12 @@ extern "C" int rkr_build_thresholds_static(const float *d_user, int64_t n_user, 
                 "rkr_build_thresholds_static: n_item %lld too large for the shared-memory row selection",
                 (long long) n_item);
     unsigned char *scratch = nullptr;
-    RKR_TRY(static_scratch_address(dev, &scratch));
+    RKR_TRY(static_scratch_address(&scratch));
     int32_t *d_rank = reinterpret_cast<int32_t *>(scratch);
     float *rows = reinterpret_cast<float *>(scratch + kStaticRankBytes);
     cudaStream_t st = (cudaStream_t) stream;
     RKR_CUDA(cudaMemcpyAsync(d_rank, sample_rank, sizeof(int32_t) * n_sample, cudaMemcpyHostToDevice, st));
-    RKR_CUDA(cudaFuncSetAttribute(row_select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    RKR_TRY(row_select_allow_max_smem());
     int sms = 0;
     RKR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     for (int64_t u0 = 0; u0 < n_user; u0 += batch) {

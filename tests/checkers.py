@@ -21,6 +21,14 @@ ORACLE_SO = os.path.join(ORACLE_DIR, "librkr_oracle.so")
 REF_SO = os.path.join(ORACLE_DIR, "_ref", "librkr_ref.so")
 REF_FAST_SO = os.path.join(ORACLE_DIR, "_ref", "librkr_ref_fast.so")  # -Ofast, timing only
 
+
+def reference_root() -> str:
+    """The reference checkout (read-only): $RKR_REFERENCE_ROOT, else a `reference` directory beside
+    this repository.  Only the fixture generators and the CPU-side tests read it; nothing that runs
+    on the GPU needs it."""
+    return os.environ.get("RKR_REFERENCE_ROOT") or os.path.normpath(os.path.join(ROOT, "..", "reference"))
+
+
 USER_RANK = np.dtype([("user_id", np.int32), ("rank", np.int32), ("query_ip", np.float32)])
 STATS = np.dtype([("n_prune", np.int32), ("n_result", np.int32), ("n_refine", np.int32),
                   ("n_candidate", np.int32), ("n_compute_item", np.int64), ("ip_cost", np.int64)])

@@ -4,8 +4,11 @@ The index is built on the device (query-rank distribution, OptimalPart ranks, th
 host (regression fit, SVD), with seeded synthetic data of the shape and value distribution the
 throughput benchmark uses.  QSRPNormalLP retrieval through the C ABI must then equal the oracle bit
 for bit -- user ids, ranks, scores and every per-query counter -- on queries drawn from the items and
-from the same distribution, and, where oracle/_ref was built, the reference's own Retrieval.
+from the same distribution, and, where oracle/_ref was built, the reference's own Retrieval.  The
+full-size build is checked against the reference's own build stages on a subset of the users.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -48,7 +51,7 @@ def full():
     ix.close()
 
 
-@pytest.mark.parametrize("topk", [100, 10])
+@pytest.mark.parametrize("topk", [100, 50, 10])
 def test_qsrp_full_size_matches_oracle(full, topk):
     orc = Oracle()
     ix = full["ix"]
@@ -96,3 +99,20 @@ def test_qsrp_full_batch_matches_oracle_on_sample(full):
         assert np.array_equal(sa[f][pick], sb[f]), (f, sa[f][pick], sb[f])
     assert np.array_equal(a["user_id"][pick], b["user_id"])
     assert np.array_equal(a["rank"][pick], b["rank"])
+
+
+@pytest.mark.skipif(not Reference.available(), reason="oracle/_ref not built (needs the reference sources)")
+def test_full_size_build_matches_reference_on_user_subset(full):
+    """The config-2 thresholds (built for all 480,189 users in the device's batched pipeline) of 2,000
+    users spread over the whole range, and the query-rank distribution of those users over all 17,770
+    items, equal the reference's own build stages (CPUScoreTable rows, sort, SampleSearch gather;
+    QueryRankByComputation) bit for bit."""
+    sub = np.linspace(0, N_USER - 1, 2000).astype(np.int64)
+    ref = Reference(os.cpu_count() or 1)
+    users = np.ascontiguousarray(full["un"][sub])
+    t_ref = ref.build_thresholds(users, full["item"], full["rank"])
+    assert same(full["thr"][sub], t_ref)
+    si = R.sample_item(N_ITEM, N_SAMPLE_ITEM)
+    with R.Index(users, full["item"]) as ix2:
+        accu = ix2.query_rank_distribution(si)
+    assert np.array_equal(accu, ref.query_rank_distribution(users, full["item"], si))

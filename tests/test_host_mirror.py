@@ -6,8 +6,10 @@ import tempfile
 
 import pytest
 
+from checkers import reference_root
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF = "/root/reference/src"
+REF = os.path.join(reference_root(), "src")
 
 DRIVER = r'''
 #include "util/VectorIO.hpp"

@@ -11,11 +11,11 @@ import os
 import numpy as np
 import pytest
 
-from checkers import Oracle, Reference, USER_RANK
+from checkers import Oracle, Reference, USER_RANK, reference_root
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 CASES = ["small", "fakenormal"]
-REF_DATASET = "/root/reference/dataset/fake-normal-30d/fake-normal-30d"
+REF_DATASET = os.path.join(reference_root(), "dataset", "fake-normal-30d", "fake-normal-30d")
 
 
 @pytest.fixture(scope="module")
@@ -76,6 +76,37 @@ def test_query_methods_match_golden(orc, case):
     us, st = orc.us_retrieval(g["user_norm"], g["item"], g["uni_rank"], g["thr_uni"], q100, k)
     assert same_results(us, g["us"])
     assert np.array_equal(st["ip_cost"], g["us_stats"]["ip_cost"])
+
+
+def test_oracle_matches_reference_dataset_golden(orc):
+    """The reference's bundled dataset (dataset/fake-normal-30d) with its driver's parameters
+    (run_rkr.py:73-78,104), every build stage and QS / QSRPNormalLP / US at k = 10, 20, 30, each k from a
+    fresh index: the oracle equals the reference's outputs stored in tests/golden/refdataset.npz."""
+    g = load("refdataset")
+    un = orc.normalize(g["user"])
+    assert np.array_equal(bits(un), bits(g["user_norm"]))
+    n_user, n_item = un.shape[0], g["item"].shape[0]
+    _, accu = orc.query_rank_distribution(un, g["item"], g["sample_item"])
+    assert np.array_equal(accu, g["accu"])
+    kth = orc.kth_rank(accu, int(g["sample_topk"]))
+    sid = np.argsort(kth, kind="stable")
+    opt, cost = orc.optimal_sample_rank(n_user, n_item, g["opt_rank"].shape[0], kth[sid], accu[sid])
+    assert np.array_equal(opt, g["opt_rank"]) and cost == int(g["opt_cost"])
+    assert np.array_equal(orc.uniform_sample_rank(n_item, g["uni_rank"].shape[0]), g["uni_rank"])
+    assert np.array_equal(bits(orc.build_thresholds(un, g["item"], g["opt_rank"])), bits(g["thr"]))
+    assert np.array_equal(bits(orc.build_thresholds(un, g["item"], g["uni_rank"])), bits(g["thr_uni"]))
+    cd = int(g["check_dim"])
+    for k in g["topks"]:
+        qs, st = orc.qs_retrieval(un, g["item"], cd, g["opt_rank"], g["thr"], g["query"], int(k))
+        assert same_results(qs, g[f"qs_{k}"])
+        assert np.array_equal(st["ip_cost"], g[f"qs_stats_{k}"]["ip_cost"])
+        qsrp, st = orc.qsrp_retrieval(un, g["svd_user"], g["transfer_item"], g["item"], cd, g["opt_rank"], g["thr"],
+                                      g["opt_rank"], g["reg"], g["query"], int(k))
+        assert same_results(qsrp, g[f"qsrp_{k}"])
+        assert np.array_equal(st["n_result"], g[f"qsrp_stats_{k}"]["n_result"])
+        us, st = orc.us_retrieval(un, g["item"], g["uni_rank"], g["thr_uni"], g["query"], int(k))
+        assert same_results(us, g[f"us_{k}"])
+        assert np.array_equal(st["ip_cost"], g[f"us_stats_{k}"]["ip_cost"])
 
 
 @pytest.mark.parametrize("case", CASES)

@@ -358,6 +358,45 @@ NCU_BYTES_PER_PAIR = {("qsrp_scores_tc", "QSRPNormalLP"): (456.031e6 + 814.108e6
 TENSOR_PEAK_NOMINAL = {"qsrp_scores_tc": ("int8", 4500.0), "refine_tc": ("int8", 4500.0)}
 
 
+def seq_dot32(a, b):
+    """The reference's InnerProduct for every row pair: a sequential binary32 sum, one rounding per
+    product and per addition (a [n][d], b [m][d] float32 -> [n][m])."""
+    acc = np.zeros((a.shape[0], b.shape[0]), np.float32)
+    for j in range(a.shape[1]):
+        acc = acc + np.outer(a[:, j], b[:, j]).astype(np.float32)
+    return acc
+
+
+def score_error_report(ix, parts, item_queries, method, user_stride=24):
+    """The tensor-core pair scores against the reference's binary32 scores and against FP64, on a
+    sample of pairs (every user_stride-th user x the given queries): the largest error, and the
+    largest ratio of the error to the bound the kernel holds (which must stay below 1)."""
+    est = ix.score_estimates(method, item_queries)
+    users = np.arange(0, est.shape[1], user_stride)
+    e = est[:, users, 0].T.astype(np.float64)
+    bound = est[:, users, 1].T.astype(np.float64)
+    q = item_queries.astype(np.float32)
+    if method == "QSRPNormalLP":
+        ti, cd = parts["ti"], parts["cd"]
+        qt = seq_dot32(q, ti)                        # SVD::TransferQuery, one sequential sum per coordinate
+        u = parts["su"][users]
+        ref = (seq_dot32(u[:, :cd], qt[:, :cd]) + seq_dot32(u[:, cd:], qt[:, cd:])).astype(np.float32)
+    else:
+        qt = q
+        u = parts["user"][users]
+        ref = seq_dot32(u, qt)
+    fp64 = u.astype(np.float64) @ qt.astype(np.float64).T
+    ok = np.isfinite(e)
+    err64 = np.abs(e - fp64)[ok]
+    err32 = np.abs(e - ref.astype(np.float64))[ok]
+    return {"pairs": int(ok.sum()), "estimate": "int8 four-digit tensor-core products, int32 accumulation",
+            "max_abs_err_vs_fp64": float(err64.max()) if err64.size else None,
+            "mean_abs_err_vs_fp64": float(err64.mean()) if err64.size else None,
+            "max_abs_err_vs_reference_binary32": float(err32.max()) if err32.size else None,
+            "max_err_over_bound": float((err32 / bound[ok]).max()) if err32.size else None,
+            "reference_binary32_max_abs_err_vs_fp64": float(np.abs(ref.astype(np.float64) - fp64).max())}
+
+
 def cpu_model():
     """The host CPU's model name (first 'model name' line of /proc/cpuinfo)."""
     try:
@@ -404,13 +443,14 @@ def reference_available():
     return Reference.available()
 
 
-def serve(ix, item, dim, seed, method, n_req, rate, log_prefix="[serve]"):
-    """A serving loop over a seeded Poisson arrival trace: each request holds 1-256 queries (uniform),
-    drawn from the items or out-of-set N(0, 1/dim) vectors with equal odds, and k ~ U[10, 200].
-    Requests are answered in arrival order, one end-to-end call each (host buffers in and out, as a
-    client makes them): QSRPNormalLP carries per-user scores from earlier queries into later results,
-    so the order of the calls is part of the answer, and the reference answers one k per call.
-    Returns per-request arrival, start and end times (seconds from the trace's start) and sizes."""
+def serve(R, ix, item, dim, seed, method, n_req, rate, max_batch=1024, n_workers=2, workspace_bytes=0):
+    """A serving run over a seeded Poisson arrival trace against the persistent server (rkr_server_*):
+    each request holds 1-256 query items (uniform), drawn from the items or out-of-set N(0, 1/dim)
+    vectors with equal odds, and one k ~ U[10, 200] for its items.  A submitter thread offers each
+    request at its arrival time (open loop); the server batches whatever is queued (continuous
+    batching, two batches in flight, graph replay) and answers each request as it would alone.
+    Returns per-request arrival, start and end times (seconds from the trace's start), sizes and the
+    server's counters."""
     rng = np.random.default_rng(seed + 5000)
     arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
     sizes = rng.integers(1, 257, n_req)
@@ -419,26 +459,56 @@ def serve(ix, item, dim, seed, method, n_req, rate, log_prefix="[serve]"):
     reqs = []
     for i in range(n_req):
         if from_items[i]:
-            reqs.append(item[rng.choice(item.shape[0], size=int(sizes[i]), replace=False)].copy())
+            q = item[rng.choice(item.shape[0], size=int(sizes[i]), replace=False)].copy()
         else:
-            reqs.append((rng.standard_normal((int(sizes[i]), dim)) / np.sqrt(dim)).astype(np.float32))
+            q = (rng.standard_normal((int(sizes[i]), dim)) / np.sqrt(dim)).astype(np.float32)
+        reqs.append((q, np.full(int(sizes[i]), int(ks[i]), np.int32)))
     start = np.zeros(n_req)
     end = np.zeros(n_req)
-    t0 = time.perf_counter()
-    for i in range(n_req):
-        now = time.perf_counter() - t0
-        if now < arrivals[i]:
-            time.sleep(arrivals[i] - now)
-        start[i] = time.perf_counter() - t0
-        ix.retrieval(method, reqs[i], int(ks[i]))
-        end[i] = time.perf_counter() - t0
-    return arrivals, start, end, sizes
+    tickets = [None] * n_req
+    submitted = threading.Semaphore(0)
+    with R.Server(ix, method=method, max_batch_queries=max_batch, n_workers=n_workers,
+                  workspace_bytes=workspace_bytes) as srv:
+        # warm-up: every batch size the trace can produce runs once eagerly and once captured
+        for nb in (16, 64, 256, 1024):
+            if nb > max_batch:
+                break
+            for _ in range(2):
+                w = [srv.submit(item[:1], np.array([10], np.int32)) for _ in range(1)]
+                big = item[:min(nb, 256)]
+                w.append(srv.submit(big, np.full(big.shape[0], 200, np.int32)))
+                for t in w:
+                    srv.wait(t, timeout=600.0)
+        c0 = srv.counters()
+        t0 = time.perf_counter()
+
+        def submitter():
+            for i in range(n_req):
+                now = time.perf_counter() - t0
+                if now < arrivals[i]:
+                    time.sleep(arrivals[i] - now)
+                tickets[i] = (time.perf_counter() - t0, srv.submit(*reqs[i]))
+                submitted.release()
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        for i in range(n_req):
+            submitted.acquire()
+            t_sub, tk = tickets[i]
+            _, lat = srv.wait(tk, timeout=600.0)
+            start[i] = t_sub + lat["start"]
+            end[i] = t_sub + lat["done"]
+            arrivals[i] = t_sub  # the offered time as actually submitted
+        th.join()
+        c1 = srv.counters()
+    counters = {k: c1[k] - c0[k] for k in c1}
+    return arrivals, start, end, sizes, counters
 
 
 def serve_summary(arrivals, start, end, sizes, rate):
     lat = (end - arrivals) * 1e3
     svc = (end - start) * 1e3
-    span = end[-1] - arrivals[0]
+    span = end.max() - arrivals[0]
     return {"offered_req_per_s": rate, "requests": int(len(sizes)), "queries": int(sizes.sum()),
             "throughput_req_per_s": len(sizes) / span, "throughput_queries_per_s": float(sizes.sum()) / span,
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
@@ -506,17 +576,18 @@ def main():
             if dist:
                 dist.destroy_process_group()
             return
-        # warm-up: the largest request shape grows every workspace once
-        ix.retrieval(args.method, draw_batch()[:256], 200)
-        ix.retrieval(args.method, draw_batch()[:1], 10)
         with Clocks(local) as clk:
             t_a = time.perf_counter()
-            arr, st_, en, sz = serve(ix, item, dim, args.seed, args.method, args.serve_requests, args.serve_rate)
+            arr, st_, en, sz, cnt = serve(R, ix, item, dim, args.seed, args.method, args.serve_requests,
+                                          args.serve_rate)
             offered = serve_summary(arr, st_, en, sz, args.serve_rate)
-            # the same kind of trace at 70% of the capacity the first trace measured (1 / mean service time)
-            cap = 1e3 / offered["service_ms"]["mean"]
-            arr, st_, en, sz = serve(ix, item, dim, args.seed + 1, args.method, args.serve_requests, 0.7 * cap)
+            offered["server"] = cnt
+            # the same kind of trace at 70% of the throughput the first trace sustained
+            cap = offered["throughput_req_per_s"]
+            arr, st_, en, sz, cnt = serve(R, ix, item, dim, args.seed + 1, args.method, args.serve_requests,
+                                          0.7 * cap)
             sustained = serve_summary(arr, st_, en, sz, 0.7 * cap)
+            sustained["server"] = cnt
             clk.mark(t_a, time.perf_counter())
         line = {"metric": "serving: request latency p50/p99 (ms) and throughput under Poisson arrivals",
                 "value": offered["latency_ms"]["p99"], "unit": "ms (p99 request latency at the offered rate)",
@@ -525,8 +596,9 @@ def main():
                         "1-256 queries, half drawn from the items, half out-of-set N(0,1/150); k ~ U[10,200]",
                 "config": {"workload": f"config5: the config4 index ({n_user} users x {n_item} items, d={dim}, "
                                        f"{n_sample} sampled thresholds/user + NormalLinearRegressionLP + SVD), "
-                                       f"{args.method}, Poisson arrivals, one end-to-end call per request in "
-                                       f"arrival order", "seed": args.seed},
+                                       f"{args.method}, Poisson arrivals, persistent server: continuous "
+                                       f"batching of up to 1024 query items, 2 batches in flight, phase-1 graph "
+                                       f"replay, each request answered as alone", "seed": args.seed},
                 "offered": offered, "at_70pct_capacity": sustained, "capacity_req_per_s": cap,
                 "build_sec": build_sec, "hbm_index_bytes": ix.size_bytes(), "clocks": clk.summary()}
         print(json.dumps(line))
@@ -659,6 +731,12 @@ def main():
                 "kernels_ms_per_step": {k: round(v[0], 4) for k, v in sorted(prof.items(), key=lambda kv: -kv[1][0])},
                 "counters_per_step": counters})
 
+    # ---- the tensor-core screen's estimates against the reference's scores and FP64 -------------------------
+    score_err = None
+    if args.method != "US":
+        score_err = score_error_report(ix, parts, batches[0].cpu().numpy()[:32], args.method)
+        ix.reset_state()
+
     # ---- latency ------------------------------------------------------------------------------------------
     single = []
     q1 = batches[0]
@@ -754,7 +832,7 @@ def main():
             "single_query_p99_ms": float(np.percentile(single, 99)) if single else None,
             "build_sec": build_sec, "build_stages_sec": {k: round(v, 3) for k, v in stages.items()},
             "hbm_index_bytes": ix.size_bytes(), "e2e": e2e, "gpu_launches": int(launches_per_step * args.steps), "roofline": roofline,
-            "plain_fp32_gpu": plain, "cpu_baseline": cpu, "clocks": clk.summary(), "query_stats_mean": stats_mean,
+            "plain_fp32_gpu": plain, "score_error": score_err, "cpu_baseline": cpu, "clocks": clk.summary(), "query_stats_mean": stats_mean,
         }
         print(json.dumps(line))
     ix.close()

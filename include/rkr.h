@@ -92,6 +92,15 @@ int rkr_index_load_svd(rkr_index *index, int32_t check_dim, const float *transfe
  * (Index::queryIP_l_, src/impl/QSRPNormalLP.hpp:73,109); a fresh index starts zeroed. */
 int rkr_index_reset_state(rkr_index *index);
 
+/* The regression models' level-boundary tables, built on the device when the models are loaded:
+ * per user and side (0: the lower rank bound as a function of qlb, 1: the upper bound of qub) 16
+ * entries (T_g, band_g), T_g the smallest binary32 score whose ComputeRankBound level
+ * (NormalLinearRegressionLP.hpp:326-398; 0 -> rank 0, j + 1 -> rank[j], S + 1 -> n_item) is <= g *
+ * stride, band_g the half-width around T_g outside which the reference's binary32 arithmetic is
+ * guaranteed to agree with the table.  tables_out: host [n_user][2][16][2] floats; *stride_out the
+ * level stride.  A diagnostic view of what the query kernels use (no counterpart in the reference). */
+int rkr_index_level_tables(rkr_index *index, int32_t *stride_out, float *tables_out);
+
 /* Device bytes held by the index (BaseIndex::IndexSizeByte counterpart, src/include/struct/MethodBase.hpp:23). */
 int rkr_index_size_bytes(const rkr_index *index, uint64_t *bytes);
 
@@ -119,6 +128,60 @@ int rkr_retrieval(rkr_index *index, int32_t method, const float *query, int32_t 
 int rkr_retrieval_device(rkr_index *index, int32_t method, const float *d_query, int32_t n_query, int32_t topk,
                          rkr_user_rank *d_out, rkr_query_stats *d_stats, int32_t *n_answered, void *stream);
 
+/* BaseIndex::Retrieval with a top-k per query, the serving boundary's form (the reference answers
+ * one topk per Retrieval call, src/app/ReverseRankIndex.cpp:191-192, src/impl/QSRPNormalLP.hpp:116-118;
+ * a batch here may mix them): query i of the answered ones gets k_per_q[i] entries, written after
+ * those of queries 0 .. i-1 (out holds sum(k_per_q[0 .. n_answered)) entries).  The results equal
+ * those of one rkr_retrieval call per query in order with topk = k_per_q[i] (the carried
+ * QSRPNormalLP scores advance the same way).  Every k must be in [1, min(n_user, 4096)]. */
+int rkr_query(rkr_index *index, int32_t method, const float *query, int32_t n_query, const int32_t *k_per_q,
+              rkr_user_rank *out, rkr_query_stats *stats, int32_t *n_answered);
+
+/* Same, with the queries and outputs in device memory (k_per_q stays a host array); runs on `stream`
+ * (or the index's own when NULL) and returns once the result is complete on that stream. */
+int rkr_query_device(rkr_index *index, int32_t method, const float *d_query, int32_t n_query,
+                     const int32_t *k_per_q, rkr_user_rank *d_out, rkr_query_stats *d_stats, int32_t *n_answered,
+                     void *stream);
+
+/* ---- serving ------------------------------------------------------------------------------------- */
+
+/* A persistent serving loop over a resident index (no counterpart in the reference, whose query app
+ * answers one query file per run, src/app/ReverseRankIndex.cpp:83-220).  Requests -- each a set of
+ * query items with a top-k per item -- queue in arrival order; n_workers workers, each on its own
+ * CUDA stream and work arrays over the shared resident index, take requests from the head of the
+ * queue while they fit a batch (at most max_batch_queries items, and at most as many as the
+ * workspace_bytes memory budget holds at about 2 bytes per (query item, user) pair; 0: no memory
+ * limit beyond the slots), pad the batch to the next of the sizes 16, 64, 256, 1024, 4096 and replay
+ * the CUDA graph captured for that size.  Each request gets the result a fresh index would give it
+ * alone (QSRPNormalLP's carried per-user scores, QSRPNormalLP.hpp:73,109,213-218, are scoped to the
+ * request), whatever it is batched with.  Methods: QS and QSRPNormalLP.  The index must stay loaded
+ * and unchanged while a server uses it; the server only reads it. */
+typedef struct {
+    int32_t method;             /* RKR_METHOD_QS or RKR_METHOD_QSRP_NORMAL_LP */
+    int32_t max_batch_queries;  /* query items per batch, 1 .. 4096 */
+    int32_t n_workers;          /* batches in flight, 1 .. 8 */
+    int32_t reserved;
+    int64_t workspace_bytes;    /* per-worker memory budget for a batch's work arrays (0: none) */
+} rkr_server_config;
+typedef struct rkr_server rkr_server;
+
+int rkr_server_create(rkr_index *index, const rkr_server_config *config, rkr_server **out);
+/* Queues a request (copies the query items [n_query][dim] and k_per_q); *ticket names it.  n_query
+ * must fit one batch. */
+int rkr_server_submit(rkr_server *server, const float *query, int32_t n_query, const int32_t *k_per_q,
+                      uint64_t *ticket);
+/* Waits (timeout_s < 0: without limit) for a request and copies its results: out holds sum(k_per_q)
+ * entries laid out as rkr_query's, stats n_query entries (either may be NULL); latency_s, if not
+ * NULL, receives {submit to done, submit to start} in seconds.  A ticket is waited for once. */
+int rkr_server_wait(rkr_server *server, uint64_t ticket, double timeout_s, rkr_user_rank *out,
+                    rkr_query_stats *stats, double *latency_s);
+/* Batches run, requests and query items answered, padding items added, and the workers' summed busy
+ * time since the server started. */
+int rkr_server_counters(rkr_server *server, int64_t *batches, int64_t *requests, int64_t *queries,
+                        int64_t *padded, double *busy_s);
+/* Answers every queued request, then stops the workers and frees their resources. */
+int rkr_server_destroy(rkr_server *server);
+
 /* ---- measurement ---------------------------------------------------------------------------------- */
 
 /* Per-kernel device time: with profiling on, every kernel the index launches is bracketed by CUDA
@@ -137,6 +200,14 @@ int rkr_retrieval_device(rkr_index *index, int32_t method, const float *d_query,
 int rkr_profile_enable(rkr_index *index, int32_t on);
 int rkr_profile_read(rkr_index *index, int32_t max_kernels, char *names, double *total_ms, int64_t *launches,
                      int32_t *n_kernels);
+
+/* Diagnostics of the tensor-core pair scores: for n_query (<= 4096) host queries, out (host,
+ * [n_query][n_user][2] floats) receives each (query, user) pair's estimate of its full score (SVD
+ * space for QSRPNormalLP, as the reference scores round 2) and the bound the kernel holds on its
+ * distance to the reference's binary32 score; NaN where the estimate path did not run (shapes the
+ * exact tiles take).  Runs one pass of the query pipeline on the index's stream (its results are
+ * discarded; the carried QSRPNormalLP scores are restored).  No counterpart in the reference. */
+int rkr_score_estimates(rkr_index *index, int32_t method, const float *query, int32_t n_query, float *out);
 
 /* ---- index build --------------------------------------------------------------------------------- */
 

@@ -220,8 +220,8 @@ int rkr_index_destroy(rkr_index *ix) {
     cudaSetDevice(ix->device);
     if (ix->stream) cudaStreamSynchronize(ix->stream);
     for (DevBuf *b : {&ix->user, &ix->item, &ix->item_sorted, &ix->item_norm, &ix->item_rnorm, &ix->user_rnorm,
-                      &ix->sample_rank, &ix->thr, &ix->thr_summ, &ix->reg_rank, &ix->reg, &ix->transfer_item, &ix->svd_user,
-                      &ix->svd_user_km, &ix->user_km, &ix->item_km, &ix->item_sorted_km, &ix->ws_km, &ix->ri_item_split,
+                      &ix->sample_rank, &ix->thr, &ix->thr_summ, &ix->reg_rank, &ix->reg, &ix->lvt, &ix->transfer_item,
+                      &ix->svd_user, &ix->svd_user_km, &ix->user_km, &ix->item_km, &ix->item_sorted_km, &ix->ws_km, &ix->ri_item_split,
                       &ix->ri_imeta_split, &ix->ri_item_full, &ix->ri_imeta_full, &ix->ws_tc,
                       &ix->svd_unorm, &ix->qip_state, &ix->ws_query, &ix->ws_qtr, &ix->ws_qnorm, &ix->ws_bucket,
                       &ix->ws_bucket2, &ix->ws_levels, &ix->ws_cls, &ix->ws_counts, &ix->ws_hist, &ix->ws_res,
@@ -230,6 +230,8 @@ int rkr_index_destroy(rkr_index *ix) {
                       &ix->sc_user_full, &ix->sc_umeta_full, &ix->sc_cdf_tab})
         b->release();
     ix->prof.release();
+    for (auto &g : ix->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
     if (ix->stream) cudaStreamDestroy(ix->stream);
     delete ix;
     return RKR_OK;
@@ -296,8 +298,9 @@ int rkr_index_load_regression(rkr_index *ix, const int32_t *sample_rank, int32_t
     RKR_TRY(ix->reg.ensure(sizeof(float) * rec8.size()));
     RKR_CUDA(cudaMemcpyAsync(ix->reg_rank.p, sample_rank, sizeof(int32_t) * n_sample, cudaMemcpyHostToDevice, ix->stream));
     RKR_CUDA(cudaMemcpyAsync(ix->reg.p, rec8.data(), sizeof(float) * rec8.size(), cudaMemcpyHostToDevice, ix->stream));
-    RKR_CUDA(cudaStreamSynchronize(ix->stream));
     ix->n_sample_reg = n_sample;
+    RKR_TRY(level_tables_build(ix));
+    RKR_CUDA(cudaStreamSynchronize(ix->stream));
     return RKR_OK;
 }
 
@@ -331,8 +334,8 @@ int rkr_index_size_bytes(const rkr_index *ix, uint64_t *bytes) {
     RKR_REQUIRE(ix && bytes, "null argument");
     uint64_t s = 0;
     for (const DevBuf *b : {&ix->user, &ix->item, &ix->item_sorted, &ix->item_norm, &ix->item_rnorm, &ix->user_rnorm,
-                            &ix->sample_rank, &ix->thr, &ix->thr_summ, &ix->reg_rank, &ix->reg, &ix->transfer_item, &ix->svd_user,
-                            &ix->svd_user_km, &ix->user_km, &ix->item_km, &ix->item_sorted_km, &ix->svd_unorm,
+                            &ix->sample_rank, &ix->thr, &ix->thr_summ, &ix->reg_rank, &ix->reg, &ix->lvt, &ix->transfer_item,
+                            &ix->svd_user, &ix->svd_user_km, &ix->user_km, &ix->item_km, &ix->item_sorted_km, &ix->svd_unorm,
                             &ix->qip_state, &ix->sc_user_split, &ix->sc_umeta_split, &ix->sc_user_full,
                             &ix->sc_umeta_full, &ix->ri_item_split, &ix->ri_imeta_split, &ix->ri_item_full,
                             &ix->ri_imeta_full})
@@ -379,7 +382,9 @@ int rkr_retrieval_device(rkr_index *ix, int32_t method, const float *d_query, in
     RKR_REQUIRE(d_query && d_out, "null query/output pointer");
     RKR_TRY(ensure_device(ix));
     cudaStream_t st = stream ? (cudaStream_t) stream : ix->stream;
-    return query_batch(ix, method, d_query, nq, topk, d_out, d_stats, st);
+    BatchSpec bs;
+    bs.topk = topk;
+    return query_batch(ix, method, d_query, nq, bs, d_out, d_stats, st);
 }
 
 int rkr_retrieval(rkr_index *ix, int32_t method, const float *query, int32_t n_query, int32_t topk, rkr_user_rank *out,
@@ -397,11 +402,109 @@ int rkr_retrieval(rkr_index *ix, int32_t method, const float *query, int32_t n_q
     RKR_TRY(ix->ws_out.ensure(ob));
     RKR_TRY(ix->ws_stats.ensure(sb));
     RKR_CUDA(cudaMemcpyAsync(ix->ws_query.p, query, qb, cudaMemcpyHostToDevice, ix->stream));
-    RKR_TRY(query_batch(ix, method, ix->ws_query.as<float>(), nq, topk, ix->ws_out.as<rkr_user_rank>(),
+    BatchSpec bs;
+    bs.topk = topk;
+    RKR_TRY(query_batch(ix, method, ix->ws_query.as<float>(), nq, bs, ix->ws_out.as<rkr_user_rank>(),
                         stats ? ix->ws_stats.as<rkr_query_stats>() : nullptr, ix->stream));
     RKR_CUDA(cudaMemcpyAsync(out, ix->ws_out.p, ob, cudaMemcpyDeviceToHost, ix->stream));
     if (stats) RKR_CUDA(cudaMemcpyAsync(stats, ix->ws_stats.p, sb, cudaMemcpyDeviceToHost, ix->stream));
     RKR_CUDA(cudaStreamSynchronize(ix->stream));
+    return RKR_OK;
+}
+
+// Per-query top-k: every k in [1, min(n_user, 4096)]; returns the total output entries of the
+// answered queries in *n_out.
+static int check_k_per_q(rkr_index *ix, const int32_t *k_per_q, int32_t n, int64_t *n_out) {
+    RKR_REQUIRE(k_per_q || n == 0, "null k_per_q");
+    int64_t s = 0;
+    for (int32_t q = 0; q < n; q++) {
+        const int32_t k = k_per_q[q];
+        RKR_REQUIRE(k >= 1 && k <= ix->n_user, "k_per_q[%d] = %d outside [1, n_user=%lld]", q, k, (long long) ix->n_user);
+        RKR_REQUIRE(k <= 4096, "k_per_q[%d] = %d above the supported maximum of 4096", q, k);
+        s += k;
+    }
+    *n_out = s;
+    return RKR_OK;
+}
+
+int rkr_query_device(rkr_index *ix, int32_t method, const float *d_query, int32_t n_query, const int32_t *k_per_q,
+                     rkr_user_rank *d_out, rkr_query_stats *d_stats, int32_t *n_answered, void *stream) {
+    int32_t nq = 0;
+    RKR_TRY(check_query_args(ix, method, n_query, 1, &nq));
+    if (n_answered) *n_answered = nq;
+    if (nq == 0) return RKR_OK;
+    int64_t n_out = 0;
+    RKR_TRY(check_k_per_q(ix, k_per_q, nq, &n_out));
+    RKR_REQUIRE(d_query && d_out, "null query/output pointer");
+    RKR_TRY(ensure_device(ix));
+    cudaStream_t st = stream ? (cudaStream_t) stream : ix->stream;
+    BatchSpec bs;
+    bs.k = k_per_q;
+    return query_batch(ix, method, d_query, nq, bs, d_out, d_stats, st);
+}
+
+int rkr_query(rkr_index *ix, int32_t method, const float *query, int32_t n_query, const int32_t *k_per_q,
+              rkr_user_rank *out, rkr_query_stats *stats, int32_t *n_answered) {
+    int32_t nq = 0;
+    RKR_TRY(check_query_args(ix, method, n_query, 1, &nq));
+    if (n_answered) *n_answered = nq;
+    if (nq == 0) return RKR_OK;
+    int64_t n_out = 0;
+    RKR_TRY(check_k_per_q(ix, k_per_q, nq, &n_out));
+    RKR_REQUIRE(query && out, "null query/output pointer");
+    RKR_TRY(ensure_device(ix));
+    const size_t qb = sizeof(float) * (size_t) nq * ix->dim;
+    const size_t ob = sizeof(rkr_user_rank) * (size_t) n_out;
+    const size_t sb = sizeof(rkr_query_stats) * (size_t) nq;
+    RKR_TRY(ix->ws_query.ensure(qb));
+    RKR_TRY(ix->ws_out.ensure(ob));
+    RKR_TRY(ix->ws_stats.ensure(sb));
+    RKR_CUDA(cudaMemcpyAsync(ix->ws_query.p, query, qb, cudaMemcpyHostToDevice, ix->stream));
+    BatchSpec bs;
+    bs.k = k_per_q;
+    RKR_TRY(query_batch(ix, method, ix->ws_query.as<float>(), nq, bs, ix->ws_out.as<rkr_user_rank>(),
+                        stats ? ix->ws_stats.as<rkr_query_stats>() : nullptr, ix->stream));
+    RKR_CUDA(cudaMemcpyAsync(out, ix->ws_out.p, ob, cudaMemcpyDeviceToHost, ix->stream));
+    if (stats) RKR_CUDA(cudaMemcpyAsync(stats, ix->ws_stats.p, sb, cudaMemcpyDeviceToHost, ix->stream));
+    RKR_CUDA(cudaStreamSynchronize(ix->stream));
+    return RKR_OK;
+}
+
+int rkr_score_estimates(rkr_index *ix, int32_t method, const float *query, int32_t n_query, float *out) {
+    int32_t nq = 0;
+    RKR_TRY(check_query_args(ix, method, n_query, 1, &nq));
+    RKR_REQUIRE(method != RKR_METHOD_US, "rkr_score_estimates: QS or QSRPNormalLP");
+    RKR_REQUIRE(nq >= 1 && nq <= kMaxChunkQueries && query && out, "rkr_score_estimates: 1 .. %d queries",
+                kMaxChunkQueries);
+    RKR_TRY(ensure_device(ix));
+    const size_t qb = sizeof(float) * (size_t) nq * ix->dim;
+    const size_t db = sizeof(float2) * (size_t) nq * (size_t) ix->n_user;
+    DevBuf dump;
+    RKR_TRY(dump.ensure(db));
+    RKR_TRY(ix->ws_query.ensure(qb));
+    RKR_TRY(ix->ws_out.ensure(sizeof(rkr_user_rank) * (size_t) nq));
+    RKR_CUDA(cudaMemcpyAsync(ix->ws_query.p, query, qb, cudaMemcpyHostToDevice, ix->stream));
+    RKR_CUDA(cudaMemsetAsync(dump.p, 0xff, db, ix->stream));  // NaN where the tensor cores did not run
+    // one pass of the pipeline with the scores kernel writing its estimates; the state it carries is
+    // put back afterwards
+    std::vector<float> state((size_t) ix->n_user);
+    RKR_CUDA(cudaMemcpyAsync(state.data(), ix->qip_state.p, sizeof(float) * state.size(), cudaMemcpyDeviceToHost,
+                             ix->stream));
+    ix->score_dump = dump.as<float2>();
+    const bool graphs = ix->graphs_on;
+    ix->graphs_on = false;
+    BatchSpec bs;
+    bs.topk = 1;
+    const int rc = query_batch(ix, method, ix->ws_query.as<float>(), nq, bs, ix->ws_out.as<rkr_user_rank>(), nullptr,
+                               ix->stream);
+    ix->score_dump = nullptr;
+    ix->graphs_on = graphs;
+    RKR_TRY(rc);
+    RKR_CUDA(cudaMemcpyAsync(ix->qip_state.p, state.data(), sizeof(float) * state.size(), cudaMemcpyHostToDevice,
+                             ix->stream));
+    RKR_CUDA(cudaMemcpyAsync(out, dump.p, db, cudaMemcpyDeviceToHost, ix->stream));
+    RKR_CUDA(cudaStreamSynchronize(ix->stream));
+    dump.release();
     return RKR_OK;
 }
 

@@ -447,9 +447,14 @@ template <class Epi>
 inline cudaError_t launch_big_split(const KMajor &A, const KMajor &B, int k_split, int k_end, const Epi &epi,
                                     cudaStream_t st) {
     const size_t smem = sizeof(BigOperands) + sizeof(BigResult) + Epi::kExtra;
-    cudaError_t e =
-        cudaFuncSetAttribute(exact_big_split_kernel<Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    // set outside graph capture (an eager run of the same launch sets it first)
+    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(st, &capturing);
     if (e != cudaSuccess) return e;
+    if (capturing == cudaStreamCaptureStatusNone) {
+        e = cudaFuncSetAttribute(exact_big_split_kernel<Epi>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+        if (e != cudaSuccess) return e;
+    }
     dim3 grid((unsigned) ((B.n + kBig - 1) / kBig), (unsigned) ((A.n + kBig - 1) / kBig));
     exact_big_split_kernel<Epi><<<grid, kBigThreads, smem, st>>>(A, B, k_split, k_end, epi);
     return cudaGetLastError();
@@ -704,6 +709,14 @@ __global__ void __launch_bounds__(kHistThreads) bucket_hist_kernel(const T *__re
 // with_aux asks for the entry's fields too, which only the emitting pass needs) and writes the
 // entries.
 
+// The top-k of each query of a batch: k[q] when per-query values are given, else kmax for every
+// query; kmax is also the row stride of the batch's per-query result arrays.
+struct KSpec {
+    const int32_t *k;  // [nq] on the device, or nullptr
+    int kmax;
+    __host__ __device__ int of(int q) const { return k ? k[q] : kmax; }
+};
+
 constexpr int kCompactThreads = 256;
 constexpr int kCompactPer = 16;
 constexpr int64_t kCompactChunk = (int64_t) kCompactThreads * kCompactPer;
@@ -748,7 +761,7 @@ __global__ void __launch_bounds__(kCompactThreads) compact_count_kernel(P p, int
 
 // Offsets per (query, chunk); n_res_emit = min(results, topk); flags a candidate-count mismatch.  With
 // qmap the kernels of this form run on the listed queries only (slot qi holds query qmap[qi]).
-static __global__ void compact_scan_kernel(const int2 *__restrict__ cnt, int nchunks, int nq, int topk, int2 *__restrict__ off,
+static __global__ void compact_scan_kernel(const int2 *__restrict__ cnt, int nchunks, int nq, KSpec ks, int2 *__restrict__ off,
                                     QueryCounts *__restrict__ counts, int *__restrict__ err,
                                     const int32_t *__restrict__ qmap) {
     const int qi = blockIdx.x * blockDim.x + threadIdx.x;
@@ -761,6 +774,7 @@ static __global__ void compact_scan_kernel(const int2 *__restrict__ cnt, int nch
         r += v.x;
         c += v.y;
     }
+    const int topk = ks.of(q);
     counts[q].n_res_emit = r < topk ? r : topk;
     if (c != counts[q].n_cand) atomicAdd(err, 1);
 }
@@ -768,10 +782,11 @@ static __global__ void compact_scan_kernel(const int2 *__restrict__ cnt, int nch
 template <class P>
 __global__ void __launch_bounds__(kCompactThreads) compact_write_kernel(P p, int64_t n_user, int nchunks,
                                                                       const int2 *__restrict__ cnt,
-                                                                      const int2 *__restrict__ off, int topk,
+                                                                      const int2 *__restrict__ off, KSpec ks,
                                                                       const int32_t *__restrict__ qmap) {
     __shared__ int warp_tot[9];
     const int qi = blockIdx.y, q = qmap ? qmap[qi] : qi;
+    const int topk = ks.of(q);
     const int2 cc = cnt[(int64_t) qi * nchunks + blockIdx.x];
     const int2 oo = off[(int64_t) qi * nchunks + blockIdx.x];
     if ((cc.x == 0 || oo.x >= topk) && cc.y == 0) return;
@@ -850,14 +865,14 @@ __global__ void __launch_bounds__(kCompactThreads) compact_need_kernel(P p, int6
 }
 
 template <class P>
-__global__ void __launch_bounds__(kCompactThreads) compact_emit_kernel(P p, int topk, const int32_t *__restrict__ need_n,
+__global__ void __launch_bounds__(kCompactThreads) compact_emit_kernel(P p, KSpec ks, const int32_t *__restrict__ need_n,
                                                                      const int32_t *__restrict__ need_u,
                                                                      QueryCounts *__restrict__ counts, int *__restrict__ err,
                                                                      int32_t *__restrict__ ovf_q) {
     __shared__ int32_t s[kNeedCap];
     __shared__ int warp_tot[9];
     const int q = blockIdx.x, tid = threadIdx.x;
-    const int n = need_n[q];
+    const int n = need_n[q], topk = ks.of(q);
     if (n > kNeedCap) {  // listed for the two-pass form
         if (tid == 0) ovf_q[atomicAdd(err + 1, 1)] = q;
         return;
@@ -994,6 +1009,7 @@ struct rkr_index {
     int n_sample_reg = 0;
     rkr::DevBuf reg_rank;      // [n_sample_reg]
     rkr::DevBuf reg;           // [n_user][8]: a, b, mu, sigma, err, smax, smin, 0
+    rkr::DevBuf lvt;           // [n_user][2][kLvEntries] float2: level-boundary tables (rkr_levels.cu)
     // SVD
     bool has_svd = false;
     rkr::DevBuf transfer_item; // [dim][dim]
@@ -1007,6 +1023,16 @@ struct rkr_index {
     rkr::DevBuf ws_res, ws_cand, ws_cand_off, ws_refine, ws_rank, ws_out, ws_stats, ws_misc, ws_fix, ws_km, ws_tc, ws_sc;
     std::vector<uint8_t> h_scratch;
     rkr::Profiler prof;
+    // CUDA graphs of a batch's phase 1 (rkr_qsrp.cu), one per (method, batch size, workspace
+    // addresses), captured on the second batch of a shape and replayed after; off unless set
+    bool graphs_on = false;
+    struct PhaseGraph {
+        int method, nq;
+        const void *ws[8];
+        cudaGraphExec_t exec;  // nullptr: the shape ran once eagerly (its buffers are sized)
+    };
+    std::vector<PhaseGraph> graphs;
+    float2 *score_dump = nullptr;  // diagnostics (rkr_score_estimates): where the pair scores' estimates go
 };
 
 namespace rkr {
@@ -1025,7 +1051,7 @@ template <typename F> inline void timed(rkr_index *ix, cudaStream_t st, const ch
 // Ordered compaction driver shared by QS and QSRP: the sparse form (streaming pass, per-query sorted
 // lists), and the two-pass form (count, scan, write) for the queries that flag more than kNeedCap users.
 template <class P>
-inline int run_compaction(rkr_index *ix, P p, int nq, int topk, QueryCounts *counts, cudaStream_t st) {
+inline int run_compaction(rkr_index *ix, P p, int nq, KSpec ks, QueryCounts *counts, cudaStream_t st) {
     const int64_t U = ix->n_user;
     const int nchunks = (int) ((U + kCompactChunk - 1) / kCompactChunk);
     const size_t sparse = sizeof(int32_t) * ((size_t) nq * kNeedCap + 2 * (size_t) nq) + 256;
@@ -1047,7 +1073,7 @@ inline int run_compaction(rkr_index *ix, P p, int nq, int topk, QueryCounts *cou
         timed(ix, st, "compact_need", [&] { compact_need_kernel<P><<<g, kCompactThreads, 0, st>>>(p, U, need_n, need_u); });
         RKR_CUDA(cudaGetLastError());
         timed(ix, st, "compact_emit", [&] {
-            compact_emit_kernel<P><<<(unsigned) nq, kCompactThreads, 0, st>>>(p, topk, need_n, need_u, counts, err, ovf_q);
+            compact_emit_kernel<P><<<(unsigned) nq, kCompactThreads, 0, st>>>(p, ks, need_n, need_u, counts, err, ovf_q);
         });
         RKR_CUDA(cudaGetLastError());
         RKR_CUDA(cudaMemcpyAsync(h_err, err, sizeof(h_err), cudaMemcpyDeviceToHost, st));
@@ -1060,11 +1086,11 @@ inline int run_compaction(rkr_index *ix, P p, int nq, int topk, QueryCounts *cou
         timed(ix, st, "compact_count", [&] { compact_count_kernel<P><<<g2, kCompactThreads, 0, st>>>(p, U, nchunks, cnt, qmap); });
         RKR_CUDA(cudaGetLastError());
         timed(ix, st, "compact_scan", [&] {
-            compact_scan_kernel<<<(n_two + 127) / 128, 128, 0, st>>>(cnt, nchunks, n_two, topk, off, counts, err, qmap);
+            compact_scan_kernel<<<(n_two + 127) / 128, 128, 0, st>>>(cnt, nchunks, n_two, ks, off, counts, err, qmap);
         });
         RKR_CUDA(cudaGetLastError());
         timed(ix, st, "compact_write", [&] {
-            compact_write_kernel<P><<<g2, kCompactThreads, 0, st>>>(p, U, nchunks, cnt, off, topk, qmap);
+            compact_write_kernel<P><<<g2, kCompactThreads, 0, st>>>(p, U, nchunks, cnt, off, ks, qmap);
         });
         RKR_CUDA(cudaGetLastError());
         RKR_CUDA(cudaMemcpyAsync(h_err, err, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1105,10 +1131,25 @@ int ensure_device(const rkr_index *ix);
 // Counting step of the refinement on the tensor cores; sets *done = false (and does nothing) where
 // the shape does not fit it, leaving the exact tiles to run.
 int refine_tc(rkr_index *ix, const RefineArgs &ra, cudaStream_t st, bool *done);
+// Builds (once per split) the item tiles refine_tc reads.
+int refine_tc_tiles(rkr_index *ix, bool ipbound, cudaStream_t st);
 int thr_summary_build(rkr_index *ix);
+int level_tables_build(rkr_index *ix);
 int refine_prepare_norms(rkr_index *ix);
-int query_batch(rkr_index *ix, int method, const float *d_query, int n_query, int topk, rkr_user_rank *d_out,
-                rkr_query_stats *d_stats, cudaStream_t st);
+// What a batch of queries asks for: top-k `topk` for every query (k null; outputs [n_query][topk]),
+// or k[q] per query (host array; query q's outputs start at the sum of the earlier k's).  req_first
+// (host, or null) scopes QSRPNormalLP's carried scores to requests: query q belongs to the request
+// that starts at query req_first[q] of the batch, only that request's earlier queries carry scores
+// to it, and a request starts from zero scores, as on a fresh index (the index's carried state is
+// neither read nor advanced).
+constexpr int kMaxChunkQueries = 4096;  // queries per device pass (a larger batch runs in chunks)
+struct BatchSpec {
+    int topk = 0;
+    const int32_t *k = nullptr;
+    const int32_t *req_first = nullptr;
+};
+int query_batch(rkr_index *ix, int method, const float *d_query, int n_query, const BatchSpec &bs,
+                rkr_user_rank *d_out, rkr_query_stats *d_stats, cudaStream_t st);
 int build_sample_search(rkr_index *ix, const int32_t *sample_rank, int n_sample);
 int score_sort_rows(rkr_index *ix, int64_t start, int64_t n_rows, float *h_rows);
 int query_rank_distribution(rkr_index *ix, const int32_t *sample_item, int n_sample_item, int32_t *h_accu);

@@ -7,12 +7,16 @@
 //   2. full SVD-space score for the survivors (ComputeRemainDim, :76-95) -> sampled-threshold
 //      bounds (SampleSearch::RankBound) -> prune again.
 // Here a batch of queries runs as passes over all (query, user) pairs:
-//   * one kernel scores every pair and decides its round-1 levels and the coarse group of its
-//     sampled-threshold bucket (a per-user summary of every 16th threshold): on the tensor cores
-//     (rkr_scores_tc.cu: int8 digit products, a rigorous bound against the reference's sums, exact
-//     resolution of the pairs the bound leaves undecided), or, where that path does not fit, as
-//     exact SIMT tiles (Round1Epi below: exact scores, a fast binary32 screen of the regression
-//     arithmetic, undecided pairs fixed by the reference's own arithmetic);
+//   * one kernel scores every pair and stores two bytes: the coarse levels ceil(level / G) of its
+//     two round-1 bounds (the per-user level-boundary tables, rkr_levels.cu) and the coarse group of
+//     its sampled-threshold bucket (a per-user summary of every 16th threshold), and counts the
+//     coarse levels per query; on the tensor cores (rkr_scores_tc.cu: int8 digit products, a
+//     rigorous bound against the reference's sums, exact resolution of the pairs the bound leaves
+//     undecided), or, where that path does not fit, as exact SIMT tiles (Round1Epi below);
+//   * the round-1 selection (PruneCandidateByBound) runs on the coarse histograms; only the pairs in
+//     a query's critical coarse levels get their exact levels (fine passes: the reference's own
+//     arithmetic, recomputed), first to find the k-th bounds, then to classify the pairs whose
+//     coarse level straddles a class threshold;
 //   * round 2 is a streaming pass that marks the pairs that did not survive round 1 and counts the
 //     survivors by group;
 //   * the exact bucket is resolved only where the k-th bound and the class counts need it: for the
@@ -31,8 +35,8 @@
 namespace rkr {
 
 // in rkr_query.cu
-int refine_and_assemble_pairs(rkr_index *ix, int method, const float *d_query, int nq, int topk,
-                              const QueryCounts *d_counts, const int32_t *d_res_user, const int32_t *d_res_rank,
+int refine_and_assemble_pairs(rkr_index *ix, int method, const float *d_query, int nq, KSpec ks,
+                              const int64_t *d_out_off, const QueryCounts *d_counts, const int32_t *d_res_user, const int32_t *d_res_rank,
                               const float *d_res_qip, int64_t n_cand, int32_t *d_cand_user, int32_t *d_cand_query,
                               int32_t *d_cand_lb, int32_t *d_cand_ub, const float *d_cand_qip,
                               const int64_t *d_cand_off, rkr_user_rank *d_out, rkr_query_stats *d_stats,
@@ -43,6 +47,12 @@ int refine_and_assemble_pairs(rkr_index *ix, int method, const float *d_query, i
 // Round-2 codes per pair: 0..nb a coarse threshold group (nb: bucket S); otherwise the round-1 state.
 constexpr uint8_t kCodeResult1 = 0xfe, kCodePruned1 = 0xff;
 constexpr uint8_t kClsMixed = 0xff;  // a group whose buckets fall in more than one class
+// Coarse-level bytes per pair: lower-bound coarse level (1 .. 15) | upper-bound coarse level << 4.  A
+// lower nibble of 0 never occurs for a level, so it marks a pair whose round-1 class the fine pass
+// settled from its exact levels (class << 4), or, before that, a pair the exact tiles' screen left
+// undecided beyond the fix list's capacity (kLvcUndecided).
+constexpr uint8_t kLvcUndecided = 0x00;
+constexpr uint8_t kLvcResolved = 0x00;  // low nibble of a settled pair; the class is in the high nibble
 
 struct QsrpParams {
     int32_t mode1, all1, L1, U1;           // round 1: equal-bounds mode, "all survivors accepted", k-th bounds
@@ -50,10 +60,22 @@ struct QsrpParams {
     int32_t mode2, L2, U2, n_elig2;        // round 2
     int32_t exact1, lv_res, lv_pr, lv_m1;  // exact1: count round-1 classes pair by pair; level thresholds
     int32_t crit, cum_before, mask1, mask2;  // critical coarse group, users below it, groups to resolve
-    int32_t gneed_lo, gneed_hi, pad0, pad1;  // groups 0..31 / 32 whose pairs the compaction must classify
+    int32_t gneed_lo, gneed_hi, lv_m2, pad1;  // groups 0..31 / 32 the compaction must classify; L2's level
+    int32_t cbl, cbu, cum_l, cum_u;        // round 1: critical coarse levels (-1: none needed), counts below
+    int32_t amb_l, amb_u, res_fine, ple_fine;  // coarse levels straddling a class threshold; their counts
 };
 
-// Round-1 class in level space: rank(level) is non-decreasing in the level, so lb <= U1 is
+// Every level in coarse level c (levels ((c - 1) G, c G], or 0 for c = 0) is <= t / is > t.
+__device__ __forceinline__ bool coarse_all_le(int c, int t, int G) { return c == 0 ? t >= 0 : c * G <= t; }
+__device__ __forceinline__ bool coarse_all_gt(int c, int t, int G) { return c == 0 ? t < 0 : (c - 1) * G >= t; }
+// The coarse level of t whose levels straddle t (some <= t, some > t), or -1 when none does.
+__device__ __forceinline__ int coarse_straddle(int t, int G) {
+    if (t < 1) return -1;
+    const int c = (t + G - 1) / G;
+    return c * G == t ? -1 : c;
+}
+
+// Round-1 class from exact levels: rank(level) is non-decreasing in the level, so lb <= U1 is
 // lvl_lb <= lv_res, L1 <= ub is lvl_ub >= lv_pr and the equal-bounds test is a test against lv_m1.
 __device__ __forceinline__ int class1_lv(const QsrpParams &p, int l, int h) {
     if (p.mode1) return (h <= p.lv_m1 && l <= p.lv_m1) ? kClsResult : kClsIdle;
@@ -62,10 +84,16 @@ __device__ __forceinline__ int class1_lv(const QsrpParams &p, int l, int h) {
     return p.all1 ? kClsResult : kClsRefine;
 }
 
-__device__ __forceinline__ int class1_of(const QsrpParams &p, int lb, int ub) {
-    if (p.mode1) return (ub <= p.L1 && lb <= p.L1) ? kClsResult : kClsIdle;
-    if (lb <= p.U1) return kClsResult;
-    if (p.L1 <= ub) return kClsPrune;
+// The same from a coarse-level byte that no threshold straddles (or that the fine pass settled).
+__device__ __forceinline__ int class1_coarse(const QsrpParams &p, unsigned v, int G) {
+    if ((v & 15) == kLvcResolved) {
+        const int k = (int) (v >> 4);
+        return (k == kClsRefine && p.all1) ? kClsResult : k;
+    }
+    const int cl = (int) (v & 15), cu = (int) (v >> 4);
+    if (p.mode1) return (coarse_all_le(cu, p.lv_m1, G) && coarse_all_le(cl, p.lv_m1, G)) ? kClsResult : kClsIdle;
+    if (coarse_all_le(cl, p.lv_res, G)) return kClsResult;
+    if (coarse_all_gt(cu, p.lv_pr - 1, G)) return kClsPrune;
     return p.all1 ? kClsResult : kClsRefine;
 }
 
@@ -86,53 +114,32 @@ __global__ void transfer_query_kernel(const float *__restrict__ query, const flo
     }
 }
 
-// Exact SVD-space partial score of (query, user) over the first check_dim coordinates
-// (PartDimPartNorm.hpp:62).
-struct ScoreSrc {
-    const float *svd_user, *qtr;
+// The reference's round-1 arithmetic for one pair: the SVD-space partial score over the first
+// check_dim coordinates (PartDimPartNorm.hpp:62), its bounds -+ the product of the remaining norms,
+// and their regression levels (lb | ub << 16).
+struct Round1Src {
+    const float *svd_user, *qtr, *unorm, *qnorm;
+    RegModel m;
     int dim, c;
-    __device__ float left(int64_t u, int64_t q) const { return exact_dot(svd_user + u * dim, qtr + q * dim, c); }
+    __device__ uint32_t levels(int64_t u, int64_t q) const {
+        const float left = exact_dot(svd_user + u * dim, qtr + q * dim, c);
+        const float right = __fmul_rn(__ldg(unorm + u), __ldg(qnorm + q));
+        return regression_levels_exact(m.rec, m.S, m.err_cap, u, __fsub_rn(left, right), __fadd_rn(left, right));
+    }
 };
 
-// The batch's full scores as the tile kernel stored them ([query][user]).
+// The reference's score of a (query, user) pair, recomputed: a sum over [0, c) and one over
+// [c, dim), added once (c == dim: one sum); the user rows are SVD-space for QSRP.
 struct QipView {
-    float *qip;
-    int64_t n_user;
-    // the reference's score of a pair: a sum over [0, c) and one over [c, dim), added once (c == dim:
-    // one sum); the user rows are SVD-space for QSRP
     const float *urow, *qrow;
     int dim, c;
-    PairScreen scr;  // scr.umeta null: the stored scores are the reference's
-    // stored values are read through L2: passes write recomputed scores back
-    __device__ float stored(int64_t u, int64_t q) const { return __ldcg(qip + q * n_user + u); }
-    __device__ bool is_exact(int64_t u, int64_t q) const {
-        if (!scr.umeta) return true;
-        const int64_t words = (n_user + 31) >> 5;
-        return (__ldcg(scr.xbits + q * words + (u >> 5)) >> (u & 31)) & 1u;
-    }
-    // The reference's score; a recomputed one is stored back and marked, so that later passes
-    // over the same pair read it.
+    int *n_exact;  // recomputed scores (a counter), or nullptr
     __device__ float exact(int64_t u, int64_t q) const {
-        const int64_t o = q * n_user + u;
-        if (is_exact(u, q)) return __ldcg(qip + o);
         const float *ur = urow + u * dim, *qr = qrow + q * dim;
         const float left = exact_dot(ur, qr, c);
         const float v = c < dim ? __fadd_rn(left, exact_dot(ur + c, qr + c, dim - c)) : left;
-        qip[o] = v;
-        __threadfence();
-        atomicOr(scr.xbits + q * ((n_user + 31) >> 5) + (u >> 5), 1u << (u & 31));
-        if (scr.n_exact) atomicAdd(scr.n_exact, 1);
+        if (n_exact) atomicAdd(n_exact, 1);
         return v;
-    }
-    // distance bound between a stored score s and the reference's
-    __device__ float delta(int64_t u, int64_t q, float s) const {
-        const float4 um = __ldg(scr.umeta + u), qm = __ldg(scr.qmeta + q);
-        const float ee = um.x * qm.x;
-        // per part: the weighted-norm term, the digits' term and the combination's leading term
-        // 3.002 u |part| <= 2.2 u Wa Wb (|part| <= Wa Wb / sqrt 2: every weight is at least 2)
-        const float nl = um.y * qm.y, nr = um.z * qm.z;
-        const float d = fmaf(scr.cl + 1.32e-7f, nl, ee * scr.kl) + fmaf(scr.cr + 1.32e-7f, nr, ee * scr.kr);
-        return fmaf(fabsf(s), 2.4e-7f, d * 1.0001f);
     }
 };
 
@@ -154,64 +161,41 @@ __device__ __forceinline__ int fine_bucket(const float *__restrict__ row, int S,
     return base + c;
 }
 
-// Thresholds of group g (< nb) >= hi and >= lo, in one pass.
-__device__ __forceinline__ void fine_bucket2(const float *__restrict__ row, int S, int gs, int g, float hi, float lo,
-                                             int &b_hi, int &b_lo) {
-    const int base = g * gs, end = min(base + gs, S);
-    int ch = 0, cl = 0;
-    if ((gs & 3) == 0 && end - base == gs && (S & 3) == 0) {
-        const float4 *p = reinterpret_cast<const float4 *>(row + base);
-        for (int t = 0; t < gs / 4; t++) {
-            const float4 x = __ldg(p + t);
-            ch += (x.x >= hi) + (x.y >= hi) + (x.z >= hi) + (x.w >= hi);
-            cl += (x.x >= lo) + (x.y >= lo) + (x.z >= lo) + (x.w >= lo);
-        }
-    } else {
-        for (int i = base; i < end; i++) {
-            const float x = __ldg(row + i);
-            ch += x >= hi;
-            cl += x >= lo;
-        }
-    }
-    b_hi = base + ch;
-    b_lo = base + cl;
-}
-
-// The bucket (inside its coarse group g) of a pair's reference score: from the stored score when it
-// is exact or no threshold lies within its bound, else from the recomputed score.
+// The bucket (inside its coarse group g) of a pair's reference score.
 __device__ __forceinline__ int pair_bucket(const QipView &sc, const float *__restrict__ thr, int S, int gs, int g,
                                            int64_t u, int64_t q) {
-    const float *row = thr + u * S;
-    if (sc.is_exact(u, q)) return fine_bucket(row, S, gs, g, sc.stored(u, q));  // the bit first, then the value
-    const float s = sc.stored(u, q);
-    const float d = sc.delta(u, q, s);
-    int b_hi, b_lo;
-    fine_bucket2(row, S, gs, g, s + d, s - d, b_hi, b_lo);
-    if (b_hi == b_lo) return b_hi;
-    return fine_bucket(row, S, gs, g, sc.exact(u, q));
+    return fine_bucket(thr + u * S, S, gs, g, sc.exact(u, q));
 }
 
 // Pairs the screen left undecided, resolved by qsrp_fix1_kernel: (query, user, partial score).
-// Past the list's capacity the pair's levels are written as kLvUndecided and count keeps growing,
-// which sends qsrp_fix1_scan_kernel over the whole batch.
+// Past the list's capacity the pair's coarse-level byte is written as kLvcUndecided and count keeps
+// growing, which sends qsrp_fix1_scan_kernel over the whole batch.
 struct FixList {
     int4 *e;
     int *count;
     int cap;
 };
-constexpr uint32_t kLvUndecided = 0xffffffffu;
+
+// One pair's exact levels into its coarse-level byte; the rank-order anomaly check.
+__device__ __forceinline__ uint8_t lvc_of_levels(uint32_t v, int G, const RegModel &m, int *anomaly_q) {
+    const int l = (int) (v & 0xffffu), h = (int) (v >> 16);
+    if (h > l && level_rank(h, m.rank, m.S, m.n_item) > level_rank(l, m.rank, m.S, m.n_item)) atomicAdd(anomaly_q, 1);
+    return (uint8_t) (lvt_coarse(l, G) | (lvt_coarse(h, G) << 4));
+}
 
 // Tiles of 128 users x 128 queries: the partial score over the first check_dim coordinates, the
-// bounds partial -+ norms and their regression levels (lb | ub << 16); then the full score and the
-// coarse group of its sampled-threshold bucket (the round-2 code of the pair if it reaches round 2).
+// bounds partial -+ norms and the coarse values of their regression levels; then the full score and
+// the coarse group of its sampled-threshold bucket (the round-2 code of the pair if it reaches
+// round 2).
 struct Round1Epi {
     static constexpr size_t kExtra = sizeof(float) * kBig;
     static constexpr int kSummStride = ThrSummary::kMaxGroups + 1;
     const float *unorm, *qnorm, *thr_summ;
     RegModel m;
-    uint32_t *lv;
+    int G;
+    uint8_t *lvc;  // nullptr: no round 1 (QS, US)
     uint8_t *code;
-    float *qip;
+    int *anomaly;
     int nb;
     int64_t n_user, n_query;
     FixList fix;
@@ -221,7 +205,7 @@ struct Round1Epi {
         return true;
     }
     __device__ void finish_lo(char *x, const BigResult &res, int64_t a0, int64_t b0) const {
-        if (!lv) return;  // no round 1 (QS, US)
+        if (!lvc) return;  // no round 1 (QS, US)
         const float *qn = reinterpret_cast<const float *>(x);
         const int ra = threadIdx.x & (kBig - 1), half = threadIdx.x >> 7, lane = threadIdx.x & 31;
         const int64_t u = a0 + ra;
@@ -229,14 +213,14 @@ struct Round1Epi {
         if (u >= n_user) return;
         const RegUser r = reg_user(m, u);
         const float un = __ldg(unorm + u);
-        uint32_t *out = lv + (b0 + half) * n_user + u;
+        uint8_t *out = lvc + (b0 + half) * n_user + u;
         const int64_t step = 2 * n_user;
         const int64_t left_rows = (n_query - b0 - half + 1) / 2;
         const int nrow = left_rows < kBig / 2 ? (int) left_rows : kBig / 2;
         // two queries per iteration: their screens are independent chains
         for (int i = 0; i < nrow; i += 2, out += 2 * step) {
             float left[2];
-            uint32_t packed[2];
+            uint8_t packed[2];
             bool ok[2];
 #pragma unroll
             for (int g = 0; g < 2; g++) {
@@ -245,7 +229,9 @@ struct Round1Epi {
                 const float right = __fmul_rn(un, qn[rb]);
                 int l, h;
                 ok[g] = regression_levels_fast(r, m.S, __fsub_rn(left[g], right), __fadd_rn(left[g], right), l, h);
-                packed[g] = (uint32_t) l | ((uint32_t) h << 16);
+                packed[g] = ok[g] ? lvc_of_levels((uint32_t) l | ((uint32_t) h << 16), G, m,
+                                                  anomaly + b0 + half + 2 * min(i + g, nrow - 1))
+                                  : kLvcUndecided;
             }
             ok[1] = ok[1] || i + 1 >= nrow;
 #pragma unroll
@@ -260,7 +246,6 @@ struct Round1Epi {
                         const int idx = base + __popc(need & ((1u << lane) - 1));
                         if (idx < fix.cap)
                             fix.e[idx] = make_int4((int) (b0 + half + 2 * (i + g)), (int) u, __float_as_int(left[g]), 0);
-                        else packed[g] = kLvUndecided;
                     }
                 }
             }
@@ -285,103 +270,76 @@ struct Round1Epi {
         const int nrow = left_rows < kBig / 2 ? (int) left_rows : kBig / 2;
         // Groups are the summary entries >= s (the summary descends; unused entries are -inf):
         // a fixed five-step search plus one compare, four queries at a time.
-        constexpr int G = 4;
-        for (int i0 = 0; i0 < nrow; i0 += G) {
-            float sv[G];
-            int lo[G];
+        constexpr int G4 = 4;
+        for (int i0 = 0; i0 < nrow; i0 += G4) {
+            float sv[G4];
+            int lo[G4];
 #pragma unroll
-            for (int g = 0; g < G; g++) {
+            for (int g = 0; g < G4; g++) {
                 sv[g] = res.v[half + 2 * min(i0 + g, nrow - 1)][ra];
                 lo[g] = 0;
             }
 #pragma unroll
             for (int st = 16; st >= 1; st >>= 1)
 #pragma unroll
-                for (int g = 0; g < G; g++) lo[g] += sm[lo[g] + st - 1] >= sv[g] ? st : 0;
+                for (int g = 0; g < G4; g++) lo[g] += sm[lo[g] + st - 1] >= sv[g] ? st : 0;
 #pragma unroll
-            for (int g = 0; g < G; g++) {
+            for (int g = 0; g < G4; g++) {
                 lo[g] = min(lo[g] + (sm[lo[g]] >= sv[g]), nb);  // a score of -inf passes the padding too
-                if (i0 + g < nrow) {
-                    code[base + (i0 + g) * step] = (uint8_t) lo[g];
-                    qip[base + (i0 + g) * step] = sv[g];
-                }
+                if (i0 + g < nrow) code[base + (i0 + g) * step] = (uint8_t) lo[g];
             }
         }
     }
 };
 
 // The reference's arithmetic for the pairs the screen left undecided (the listed ones).
-__global__ void qsrp_fix1_kernel(FixList fix, RegModel m, const float *__restrict__ unorm,
-                                 const float *__restrict__ qnorm, int64_t n_user, uint32_t *__restrict__ lv) {
+__global__ void qsrp_fix1_kernel(FixList fix, RegModel m, int G, const float *__restrict__ unorm,
+                                 const float *__restrict__ qnorm, int64_t n_user, uint8_t *__restrict__ lvc,
+                                 int *__restrict__ anomaly) {
     const int n = min(*fix.count, fix.cap);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int4 e = fix.e[i];
         const float left = __int_as_float(e.z);
         const float right = __fmul_rn(__ldg(unorm + e.y), __ldg(qnorm + e.x));
-        lv[(int64_t) e.x * n_user + e.y] =
+        const uint32_t v =
             regression_levels_exact(m.rec, m.S, m.err_cap, e.y, __fsub_rn(left, right), __fadd_rn(left, right));
+        lvc[(int64_t) e.x * n_user + e.y] = lvc_of_levels(v, G, m, anomaly + e.x);
     }
 }
 
-// Undecided pairs beyond the list's capacity: a scan of the batch's levels for kLvUndecided, with the
-// partial score recomputed.  Returns at once when the list held them all.
-__global__ void qsrp_fix1_scan_kernel(const int *__restrict__ count, int cap, RegModel m, ScoreSrc sc,
-                                      const float *__restrict__ unorm, const float *__restrict__ qnorm, int64_t n_user,
-                                      int nq, uint32_t *__restrict__ lv) {
+// Undecided pairs beyond the list's capacity: a scan of the batch's coarse-level bytes for
+// kLvcUndecided, with the partial score recomputed.  Returns at once when the list held them all.
+__global__ void qsrp_fix1_scan_kernel(const int *__restrict__ count, int cap, Round1Src src, int G, int64_t n_user,
+                                      int nq, uint8_t *__restrict__ lvc, int *__restrict__ anomaly) {
     if (*count <= cap) return;
     const int64_t n = n_user * nq;
     for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
-        if (lv[i] != kLvUndecided) continue;
+        if (lvc[i] != kLvcUndecided) continue;
         const int64_t q = i / n_user, u = i % n_user;
-        const float left = sc.left(u, q);
-        const float right = __fmul_rn(__ldg(unorm + u), __ldg(qnorm + q));
-        lv[i] = regression_levels_exact(m.rec, m.S, m.err_cap, u, __fsub_rn(left, right), __fadd_rn(left, right));
+        lvc[i] = lvc_of_levels(src.levels(u, q), G, src.m, anomaly + q);
     }
 }
 
-// Histograms of the round-1 lower- and upper-bound levels per query, one CTA per (user chunk,
-// query), counted in per-warp shared-memory copies; also counts pairs whose upper bound exceeds
-// their lower bound (never expected, but it would void the shortcut qsrp_select1 takes for the
-// class counts).
-__global__ void __launch_bounds__(kHistThreads) level_hist_kernel(const uint32_t *__restrict__ lv, int64_t n_user,
-                                                                 const int32_t *__restrict__ rank, int S, int n_item,
-                                                                 int64_t chunk, int *__restrict__ hist,
-                                                                 int *__restrict__ anomaly) {
-    extern __shared__ int h[];
-    __shared__ int anom;
-    const int nl = S + 2, nb = 2 * nl;
-    const int copies = hist_copies(nb);
+// Coarse-level histograms of the exact tiles' batch (the tensor-core kernel counts in its epilogue),
+// one CTA per (user chunk, query); the lower side's last coarse level and the upper side's level 0
+// are left implicit, as there.
+__global__ void __launch_bounds__(kHistThreads) lvc_hist_kernel(const uint8_t *__restrict__ lvc, int64_t n_user,
+                                                               int64_t chunk, int *__restrict__ lhist) {
+    __shared__ int h[2 * kLvEntries];
     const int q = blockIdx.y;
-    for (int b = threadIdx.x; b < copies * nb; b += blockDim.x) h[b] = 0;
-    if (threadIdx.x == 0) anom = 0;
+    for (int b = threadIdx.x; b < 2 * kLvEntries; b += blockDim.x) h[b] = 0;
     __syncthreads();
-    int *mine = h + ((threadIdx.x >> 5) % copies) * nb;
-    const uint32_t *row = lv + (int64_t) q * n_user;
+    const uint8_t *row = lvc + (int64_t) q * n_user;
     const int64_t u0 = (int64_t) blockIdx.x * chunk, u1 = min(u0 + chunk, n_user);
-    int my_anom = 0;
-    constexpr int G = 8;  // loads in flight per thread
-    for (int64_t ub = u0 + threadIdx.x; ub < u1; ub += G * kHistThreads) {
-        uint32_t v[G];
-#pragma unroll
-        for (int g = 0; g < G; g++) v[g] = ub + g * kHistThreads < u1 ? __ldg(row + ub + g * kHistThreads) : 0xffffffffu;
-#pragma unroll
-        for (int g = 0; g < G; g++) {
-            if (v[g] == 0xffffffffu) continue;
-            const int l = v[g] & 0xffff, hh = v[g] >> 16;
-            atomicAdd(mine + l, 1);
-            atomicAdd(mine + nl + hh, 1);
-            my_anom += hh > l && level_rank(hh, rank, S, n_item) > level_rank(l, rank, S, n_item);
-        }
+    for (int64_t u = u0 + threadIdx.x; u < u1; u += blockDim.x) {
+        const unsigned v = row[u];
+        const int cl = (int) (v & 15), cu = (int) (v >> 4);
+        if (cl != kLvEntries - 1) atomicAdd(h + cl, 1);
+        if (cu != 0) atomicAdd(h + kLvEntries + cu, 1);
     }
-    if (my_anom) atomicAdd(&anom, my_anom);
     __syncthreads();
-    int *g = hist + (int64_t) q * nb;
-    for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-        int sum = 0;
-        for (int c = 0; c < copies; c++) sum += h[c * nb + b];
-        if (sum) atomicAdd(g + b, sum);
-    }
-    if (threadIdx.x == 0 && anom) atomicAdd(anomaly + q, anom);
+    for (int b = threadIdx.x; b < 2 * kLvEntries; b += blockDim.x)
+        if (h[b]) atomicAdd(lhist + (int64_t) q * 2 * kLvEntries + b, h[b]);
 }
 
 // ---- one warp per query -------------------------------------------------------------------------
@@ -407,25 +365,151 @@ __device__ __forceinline__ int warp_first_reaching(const int *__restrict__ h, in
     return n - 1;
 }
 
-// Round-1 k-th smallest bounds per query (PruneCandidateByBound.hpp:36-77 with nothing excluded)
-// and the class counts, one warp per query.  While every pair has ub <= lb, a result (lb <= U*)
-// and a prune (ub >= L*) cannot coincide unless L* == U*, so the counts follow from the two
-// histograms; otherwise qsrp_count1 counts pair by pair.  rank(level) is non-decreasing, so the
-// levels with rank <= X form a prefix and the thresholds are counts.
-__global__ void qsrp_select1_kernel(const int *__restrict__ hist_all, const int *__restrict__ anomaly, int64_t n_user,
-                                    const int32_t *__restrict__ rank, int S, int n_item, int topk, int nq,
-                                    QsrpParams *__restrict__ par) {
+// Full coarse counts of one side (the implicit bin restored: every pair is counted once).
+__device__ __forceinline__ void coarse_counts(const int *__restrict__ h, int implicit, int64_t n_user, int *out) {
+    int64_t s = 0;
+    for (int b = 0; b < kLvEntries; b++) {
+        out[b] = b == implicit ? 0 : h[b];
+        s += out[b];
+    }
+    out[implicit] = (int) (n_user - s);
+}
+
+// Round-1 selection, coarse step (PruneCandidateByBound.hpp:36-77 with nothing excluded): the coarse
+// levels holding each side's k-th smallest level, and the users below them.  A critical coarse
+// level 0 (the upper side's level 0) is a single level and needs no fine step.
+__global__ void qsrp_select1c_kernel(const int *__restrict__ lhist, int64_t n_user, KSpec ks, int nq,
+                                     QsrpParams *__restrict__ par) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    const int topk = ks.of(q);
+    int hl[kLvEntries], hu[kLvEntries];
+    coarse_counts(lhist + (int64_t) q * 2 * kLvEntries, kLvEntries - 1, n_user, hl);
+    coarse_counts(lhist + (int64_t) q * 2 * kLvEntries + kLvEntries, 0, n_user, hu);
+    QsrpParams p = {};
+    int64_t cum = 0;
+    p.cbl = kLvEntries - 1;
+    for (int b = 0; b < kLvEntries; b++) {
+        if (cum + hl[b] >= topk) { p.cbl = b; break; }
+        cum += hl[b];
+    }
+    p.cum_l = (int) cum;
+    cum = 0;
+    p.cbu = kLvEntries - 1;
+    for (int b = 0; b < kLvEntries; b++) {
+        if (cum + hu[b] >= topk) { p.cbu = b; break; }
+        cum += hu[b];
+    }
+    p.cum_u = (int) cum;
+    if (p.cbu == 0) p.cbu = -1;  // level 0 exactly
+    p.amb_l = -1;
+    p.amb_u = -1;
+    par[q] = p;
+}
+
+// Exact levels of the pairs in the coarse levels a query flags, one CTA per (user tile, query
+// group), one warp per query row of the tile.  mode 0: the critical coarse levels of the selection,
+// counted by exact level (fine histograms [query][2][G]).  mode 1: the pairs whose coarse level
+// straddles a class threshold (every pair of a query whose class counts must be taken pair by pair),
+// settled to their exact round-1 class in place (lvc = class << 4) and counted.
+__global__ void __launch_bounds__(256) qsrp_fine1_kernel(uint8_t *__restrict__ lvc, Round1Src src, int64_t n_user,
+                                                        int nq, int G, int mode, QsrpParams *__restrict__ par,
+                                                        int *__restrict__ fhist, int *__restrict__ mismatch) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t u0 = (int64_t) blockIdx.x * 128;
+    for (int q = blockIdx.y * 8 + warp; q < nq; q += gridDim.y * 8) {
+        const QsrpParams &p = par[q];
+        int wl, wu;
+        bool all = false;
+        if (mode == 0) {
+            wl = p.cbl;
+            wu = p.cbu;
+        } else {
+            wl = p.amb_l;
+            wu = p.amb_u;
+            all = p.exact1 != 0;
+        }
+        if (wl < 0 && wu < 0 && !all) continue;
+        uint8_t *row = lvc + (int64_t) q * n_user;
+        int n_res = 0, n_ple = 0, c_res = 0, c_pr = 0, c_ref = 0;
+        for (int k = 0; k < 4; k++) {
+            const int64_t u = u0 + 32 * k + lane;
+            const bool in = u < n_user;
+            const unsigned v = in ? row[u] : 0u;
+            const int cl = (int) (v & 15), cu = (int) (v >> 4);
+            const bool hit = in && (all || cl == wl || cu == wu);
+            if (!hit) continue;
+            const uint32_t lv = src.levels(u, q);
+            const int l = (int) (lv & 0xffffu), h = (int) (lv >> 16);
+            if (mode == 0) {
+                // the exact levels lie in the coarse levels the screen gave them; a disagreement is
+                // reported (the call fails) instead of counted
+                int *fh = fhist + (int64_t) q * 2 * G;
+                const int il = l - (wl - 1) * G - 1, iu = h - (wu - 1) * G - 1;
+                if (cl == wl) {
+                    if (il >= 0 && il < G) atomicAdd(fh + il, 1);
+                    else atomicAdd(mismatch, 1);
+                }
+                if (cu == wu) {
+                    if (iu >= 0 && iu < G) atomicAdd(fh + G + iu, 1);
+                    else atomicAdd(mismatch, 1);
+                }
+            } else {
+                const int cls = class1_lv(p, l, h);
+                if (all) {
+                    c_res += cls == kClsResult;
+                    c_pr += cls == kClsPrune;
+                    c_ref += cls == kClsRefine || cls == kClsIdle;
+                } else {
+                    n_res += cl == wl && l <= p.lv_res;
+                    n_ple += cu == wu && h <= p.lv_pr - 1;
+                }
+                row[u] = (uint8_t) ((cls << 4) | kLvcResolved);
+            }
+        }
+        if (mode == 1) {
+            n_res = (int) warp_sum64(n_res);
+            n_ple = (int) warp_sum64(n_ple);
+            c_res = (int) warp_sum64(c_res);
+            c_pr = (int) warp_sum64(c_pr);
+            c_ref = (int) warp_sum64(c_ref);
+            if (lane == 0) {
+                if (n_res) atomicAdd(&par[q].res_fine, n_res);
+                if (n_ple) atomicAdd(&par[q].ple_fine, n_ple);
+                if (c_res) atomicAdd(&par[q].n_res1, c_res);
+                if (c_pr) atomicAdd(&par[q].n_pr1, c_pr);
+                if (c_ref) atomicAdd(&par[q].n_ref1, c_ref);
+            }
+        }
+    }
+}
+
+// Round-1 selection, exact step, one warp per query: each side's k-th smallest level from the fine
+// histogram of its critical coarse level, the bounds (L1, U1), the level thresholds of the classes,
+// the coarse levels that straddle them (settled pair by pair by the fine pass), and the counts of the
+// whole coarse levels on each side of them.  While every pair has ub <= lb, a result (lb <= U*) and a
+// prune (ub >= L*) cannot coincide unless L* == U*, so the class counts follow from the two sides'
+// counts; a query with a pair that breaks the order (anomaly) counts its classes pair by pair.
+// rank(level) is non-decreasing, so the levels with rank <= X form a prefix and the thresholds are
+// counts.
+__global__ void qsrp_select1f_kernel(const int *__restrict__ lhist, const int *__restrict__ fhist,
+                                     const int *__restrict__ anomaly, int64_t n_user, const int32_t *__restrict__ rank,
+                                     int S, int n_item, int G, KSpec ks, int nq, QsrpParams *__restrict__ par) {
     const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (q >= nq) return;
-    const int nl = S + 2;
-    const int *h = hist_all + (int64_t) q * 2 * nl;
-    const int kl = warp_first_reaching(h, nl, topk), kh = warp_first_reaching(h + nl, nl, topk);
-    QsrpParams p = {};
+    const int topk = ks.of(q);
+    QsrpParams p = par[q];
+    int kl, kh;
+    {
+        const int *fh = fhist + (int64_t) q * 2 * G;
+        kl = (p.cbl - 1) * G + 1 + warp_first_reaching(fh, G, topk - p.cum_l);
+        kh = p.cbu < 0 ? 0 : (p.cbu - 1) * G + 1 + warp_first_reaching(fh + G, G, topk - p.cum_u);
+    }
     p.L1 = level_rank(kl, rank, S, n_item);
     p.U1 = level_rank(kh, rank, S, n_item);
     p.mode1 = p.L1 == p.U1;
     int64_t c_res = 0, c_m1 = 0, c_lt = 0;
-    for (int l = lane; l < nl; l += 32) {
+    for (int l = lane; l < S + 2; l += 32) {
         const int rl = level_rank(l, rank, S, n_item);
         c_res += rl <= p.U1;
         c_m1 += rl <= p.L1;
@@ -434,68 +518,55 @@ __global__ void qsrp_select1_kernel(const int *__restrict__ hist_all, const int 
     p.lv_res = (int) warp_sum64(c_res) - 1;
     p.lv_m1 = (int) warp_sum64(c_m1) - 1;
     p.lv_pr = (int) warp_sum64(c_lt);
-    if (!p.mode1) {
-        if (anomaly[q]) {
-            p.exact1 = 1;
-        } else {
-            int64_t nres = 0, npr = 0;
-            for (int b = lane; b < nl; b += 32) {
-                if (b <= p.lv_res) nres += h[b];
-                if (b >= p.lv_pr) npr += h[nl + b];
-            }
-            nres = warp_sum64(nres);
-            npr = warp_sum64(npr);
-            p.n_res1 = (int) nres;
-            p.n_pr1 = (int) npr;
-            p.n_ref1 = (int) (n_user - nres - npr);
+    p.res_fine = 0;
+    p.ple_fine = 0;
+    p.n_res1 = 0;
+    p.n_pr1 = 0;
+    p.n_ref1 = 0;
+    if (p.mode1) {
+        p.amb_l = coarse_straddle(p.lv_m1, G);
+        p.amb_u = coarse_straddle(p.lv_m1, G);
+    } else if (anomaly[q]) {
+        p.exact1 = 1;
+    } else {
+        p.amb_l = coarse_straddle(p.lv_res, G);
+        p.amb_u = coarse_straddle(p.lv_pr - 1, G);
+        // the whole coarse levels: lower side <= lv_res, upper side <= lv_pr - 1
+        int hl[kLvEntries], hu[kLvEntries];
+        coarse_counts(lhist + (int64_t) q * 2 * kLvEntries, kLvEntries - 1, n_user, hl);
+        coarse_counts(lhist + (int64_t) q * 2 * kLvEntries + kLvEntries, 0, n_user, hu);
+        int64_t nres = 0, nle = 0;
+        for (int b = 0; b < kLvEntries; b++) {
+            if (coarse_all_le(b, p.lv_res, G)) nres += hl[b];
+            if (coarse_all_le(b, p.lv_pr - 1, G)) nle += hu[b];
         }
+        p.n_res1 = (int) nres;
+        p.n_pr1 = (int) nle;  // until qsrp_final1: users whose upper level is <= lv_pr - 1 (whole levels)
     }
     if (lane == 0) par[q] = p;
 }
 
-// Round-1 class counts pair by pair (the reduction at PruneCandidateByBound.hpp:115-136), for
-// queries where the histogram shortcut does not apply.
-__global__ void qsrp_count1_kernel(const uint32_t *__restrict__ lv, int64_t n_user, QsrpParams *__restrict__ par) {
-    const int q = blockIdx.y;
-    const QsrpParams p = par[q];
-    if (p.mode1 || !p.exact1) return;
-    __shared__ int cnt[3];
-    if (threadIdx.x < 3) cnt[threadIdx.x] = 0;
-    __syncthreads();
-    int c[3] = {0, 0, 0};
-    const uint32_t *row = lv + (int64_t) q * n_user;
-    for (int64_t u = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; u < n_user; u += (int64_t) gridDim.x * blockDim.x) {
-        const uint32_t v = row[u];
-        const int k = class1_lv(p, v & 0xffff, v >> 16);
-        c[k == kClsResult ? 0 : (k == kClsPrune ? 1 : 2)]++;
-    }
-    for (int i = 0; i < 3; i++) {
-        int v = c[i];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-        if ((threadIdx.x & 31) == 0 && v) atomicAdd(&cnt[i], v);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        atomicAdd(&par[q].n_res1, cnt[0]);
-        atomicAdd(&par[q].n_pr1, cnt[1]);
-        atomicAdd(&par[q].n_ref1, cnt[2]);
-    }
-}
-
 // Round-1 closing rules (PruneCandidateByBound.hpp:93-94, 139-150).
-__global__ void qsrp_final1_kernel(QsrpParams *__restrict__ par, int nq, int topk) {
+__global__ void qsrp_final1_kernel(QsrpParams *__restrict__ par, int nq, KSpec ks, int64_t n_user) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nq) return;
+    const int topk = ks.of(q);
     QsrpParams p = par[q];
     if (p.mode1) {
         p.n_res1 = topk;
         p.n_pr1 = 0;
         p.n_ref1 = 0;
-    } else if (p.n_res1 + p.n_ref1 == topk) {
-        p.all1 = 1;
-        p.n_res1 = topk;
-        p.n_ref1 = 0;
+    } else {
+        if (!p.exact1) {
+            p.n_res1 += p.res_fine;
+            p.n_pr1 = (int) (n_user - p.n_pr1 - p.ple_fine);
+            p.n_ref1 = (int) (n_user - p.n_res1 - p.n_pr1);
+        }
+        if (p.n_res1 + p.n_ref1 == topk) {
+            p.all1 = 1;
+            p.n_res1 = topk;
+            p.n_ref1 = 0;
+        }
     }
     p.skip2 = p.n_res1 >= topk;
     par[q] = p;
@@ -511,6 +582,8 @@ __global__ void qs_params_kernel(QsrpParams *__restrict__ par, int nq, int64_t n
     p.lv_pr = 1 << 30;
     p.lv_m1 = -1;
     p.n_ref1 = (int) n_user;
+    p.amb_l = -1;
+    p.amb_u = -1;
     par[q] = p;
 }
 
@@ -518,9 +591,9 @@ __global__ void qs_params_kernel(QsrpParams *__restrict__ par, int nq, int64_t n
 
 // Round 2 per (user chunk, query): pairs that did not reach round 2 get their round-1 state code in
 // place of the group code; the others are counted by group (per-warp shared-memory copies).
-__global__ void __launch_bounds__(kHistThreads) qsrp_round2_kernel(const uint32_t *__restrict__ lv,
+__global__ void __launch_bounds__(kHistThreads) qsrp_round2_kernel(const uint8_t *__restrict__ lvc,
                                                                   uint8_t *__restrict__ code, int64_t n_user,
-                                                                  const QsrpParams *__restrict__ par, int nb,
+                                                                  const QsrpParams *__restrict__ par, int nb, int G,
                                                                   int64_t chunk, int *__restrict__ hist_c) {
     extern __shared__ int h[];
     const int nbin = nb + 1, copies = hist_copies(nbin);
@@ -530,28 +603,27 @@ __global__ void __launch_bounds__(kHistThreads) qsrp_round2_kernel(const uint32_
         const QsrpParams &g = par[q];
         p.mode1 = g.mode1; p.all1 = g.all1; p.lv_res = g.lv_res; p.lv_pr = g.lv_pr; p.lv_m1 = g.lv_m1;
     }
-    const bool all_survive = lv == nullptr;  // QS and US: no round 1
+    const bool all_survive = lvc == nullptr;  // QS and US: no round 1
     for (int b = threadIdx.x; b < copies * nbin; b += blockDim.x) h[b] = 0;
     __syncthreads();
     int *mine = h + ((threadIdx.x >> 5) % copies) * nbin;
-    const uint32_t *lrow = lv ? lv + (int64_t) q * n_user : nullptr;
+    const uint8_t *lrow = lvc ? lvc + (int64_t) q * n_user : nullptr;
     uint8_t *crow = code + (int64_t) q * n_user;
     const int64_t u0 = (int64_t) blockIdx.x * chunk, u1 = min(u0 + chunk, n_user);
-    constexpr int G = 4;  // pairs in flight per thread; the group code is loaded with the levels
-    for (int64_t ub = u0 + threadIdx.x; ub < u1; ub += G * kHistThreads) {
-        uint32_t v[G];
-        unsigned cc[G];
+    constexpr int GP = 8;  // pairs in flight per thread
+    for (int64_t ub = u0 + threadIdx.x; ub < u1; ub += GP * kHistThreads) {
+        unsigned v[GP], cc[GP];
 #pragma unroll
-        for (int g = 0; g < G; g++) {
+        for (int g = 0; g < GP; g++) {
             const bool in = ub + g * kHistThreads < u1;
-            v[g] = in && !all_survive ? __ldg(lrow + ub + g * kHistThreads) : 0u;
+            v[g] = in && !all_survive ? lrow[ub + g * kHistThreads] : 0u;
             cc[g] = in ? crow[ub + g * kHistThreads] : 0u;
         }
 #pragma unroll
-        for (int g = 0; g < G; g++) {
+        for (int g = 0; g < GP; g++) {
             const int64_t u = ub + g * kHistThreads;
             if (u >= u1) break;
-            const int k = all_survive ? kClsRefine : class1_lv(p, v[g] & 0xffff, v[g] >> 16);
+            const int k = all_survive ? kClsRefine : class1_coarse(p, v[g], G);
             if (k == kClsRefine || k == kClsIdle) atomicAdd(mine + cc[g], 1);
             else crow[u] = k == kClsResult ? kCodeResult1 : kCodePruned1;
         }
@@ -568,10 +640,11 @@ __global__ void __launch_bounds__(kHistThreads) qsrp_round2_kernel(const uint32_
 // Round-2 selection, coarse step (second PruneCandidateByBound call, QSRPNormalLP.hpp:187-190):
 // the coarse group holding the kp-th smallest bucket among the users that reached round 2
 // (kp = topk - round-1 results), or, with fewer such users than kp, the highest occupied group.
-__global__ void qsrp_select2c_kernel(const int *__restrict__ hist_c, int nb, int topk, int nq,
+__global__ void qsrp_select2c_kernel(const int *__restrict__ hist_c, int nb, KSpec ks, int nq,
                                      QsrpParams *__restrict__ par, QueryCounts *__restrict__ counts) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nq) return;
+    const int topk = ks.of(q);
     QsrpParams p = par[q];
     p.crit = -1; p.cum_before = -1; p.mask1 = 0; p.mask2 = 0; p.gneed_lo = 0; p.gneed_hi = 0;
     if (p.skip2) {
@@ -739,11 +812,12 @@ __device__ __forceinline__ uint8_t class2_of(int b, int S, const int32_t *rank, 
 // exact histogram, the bounds (L2, U2), each bucket's and each group's class, and the mixed groups
 // still without an exact histogram (mask2).
 __global__ void qsrp_select2f_kernel(const int *__restrict__ hist_f, int nb, int gs, int S,
-                                     const int32_t *__restrict__ rank, int n_item, int topk, int nq,
+                                     const int32_t *__restrict__ rank, int n_item, KSpec ks, int nq,
                                      QsrpParams *__restrict__ par, uint8_t *__restrict__ cls2,
                                      uint8_t *__restrict__ clsg, int *__restrict__ any2) {
     const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (q >= nq) return;
+    const int topk = ks.of(q);
     QsrpParams p = par[q];
     if (p.skip2) return;
     const int *hf = hist_f + (int64_t) q * (S + 1);
@@ -794,12 +868,20 @@ __global__ void qsrp_select2f_kernel(const int *__restrict__ hist_f, int nb, int
 // whole from the coarse histogram, mixed groups bucket by bucket; then the "all survivors are
 // results" rule and the groups the compaction must classify.
 __global__ void qsrp_final2_kernel(const int *__restrict__ hist_c, const int *__restrict__ hist_f, int nb, int gs, int S,
-                                   int topk, int nq, QsrpParams *__restrict__ par, uint8_t *__restrict__ cls2,
-                                   uint8_t *__restrict__ clsg, QueryCounts *__restrict__ counts) {
+                                   KSpec ks, int nq, const int32_t *__restrict__ reg_rank, int S_reg, int n_item,
+                                   QsrpParams *__restrict__ par, uint8_t *__restrict__ cls2, uint8_t *__restrict__ clsg,
+                                   QueryCounts *__restrict__ counts) {
     const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (q >= nq) return;
+    const int topk = ks.of(q);
     QsrpParams p = par[q];
     if (p.skip2) return;
+    if (reg_rank) {
+        // the largest regression level whose rank is <= L2 (the equal-bounds rule in level space)
+        int64_t c_le = 0;
+        for (int l = lane; l < S_reg + 2; l += 32) c_le += level_rank(l, reg_rank, S_reg, n_item) <= p.L2;
+        p.lv_m2 = (int) warp_sum64(c_le) - 1;
+    }
     QueryCounts c = {};
     c.lstar = p.L2;
     c.ustar = p.U2;
@@ -860,7 +942,9 @@ __global__ void qsrp_final2_kernel(const int *__restrict__ hist_c, const int *__
 // class or the entry's fields are asked for.
 struct QsrpCompactPolicy {
     struct Aux { int rank, fresh, lb, ub; };
-    const uint32_t *lv;
+    const uint8_t *lvc;  // coarse round-1 levels (QSRP), or nullptr
+    Round1Src src;       // the reference's round-1 levels, recomputed
+    int G;
     const uint8_t *code;
     const float *thr;
     QipView sc;
@@ -871,7 +955,7 @@ struct QsrpCompactPolicy {
     const uint8_t *cls2, *clsg;
     const QueryCounts *counts;
     const int64_t *cand_off;
-    int topk;
+    int kstride;  // row stride of the result arrays (the batch's largest k)
     int32_t *res_user, *res_rank;
     uint8_t *res_fresh;
     int32_t *cand_user, *cand_query, *cand_lb, *cand_ub;
@@ -914,17 +998,27 @@ struct QsrpCompactPolicy {
         aux.fresh = 0;
         const QsrpParams &p = par[q];
         if (c == kCodeResult1 || (!p.skip2 && p.mode2)) {
-            const uint32_t v = lv[at];
-            const int lb1 = level_rank(v & 0xffff, reg_rank, S_reg, n_item);
-            const int ub1 = level_rank(v >> 16, reg_rank, S_reg, n_item);
+            if (c != kCodeResult1) {
+                // the equal-bounds rule scans every user: decided from the coarse levels where no
+                // level threshold straddles them
+                const unsigned v = lvc[at];
+                if ((v & 15) != kLvcResolved) {
+                    const int cl = (int) (v & 15), cu = (int) (v >> 4);
+                    if (coarse_all_gt(cu, p.lv_m2, G) || coarse_all_gt(cl, p.lv_m2, G)) return 0;
+                    if (!with_aux && coarse_all_le(cu, p.lv_m2, G) && coarse_all_le(cl, p.lv_m2, G)) return 1;
+                }
+            }
+            const uint32_t v = src.levels(u, q);
+            const int lb1 = level_rank((int) (v & 0xffffu), reg_rank, S_reg, n_item);
+            const int ub1 = level_rank((int) (v >> 16), reg_rank, S_reg, n_item);
             aux.rank = lb1; aux.lb = lb1; aux.ub = ub1;
             if (c == kCodeResult1) return 1;
-            return (ub1 <= p.L2 && lb1 <= p.L2) ? 1 : 0;  // the equal-bounds rule scans every user
+            return (ub1 <= p.L2 && lb1 <= p.L2) ? 1 : 0;
         }
         return 0;
     }
     __device__ void emit_result(int q, int pos, int64_t u, const Aux &aux) const {
-        const int64_t i = (int64_t) q * topk + pos;
+        const int64_t i = (int64_t) q * kstride + pos;
         res_user[i] = (int32_t) u;
         res_rank[i] = aux.rank;
         res_fresh[i] = (uint8_t) aux.fresh;
@@ -940,20 +1034,24 @@ struct QsrpCompactPolicy {
 };
 
 // Scores of the emitted result users: this query's score when the user reached round 2, else the
-// score from its latest earlier round-2 query in the batch, else the carried state.
+// score from its latest earlier round-2 query in the batch, else the carried state.  With req_first
+// (the first query of each query's request) only the request's own earlier queries count and a
+// request starts from a fresh state (zero scores), as a fresh index would.
 __global__ void __launch_bounds__(128, 8) qsrp_result_fill_kernel(const QueryCounts *__restrict__ counts, const int32_t *__restrict__ res_user,
                                         const uint8_t *__restrict__ res_fresh, const uint8_t *__restrict__ code,
-                                        QipView sc, int64_t n_user, const float *__restrict__ state, int topk,
+                                        QipView sc, int64_t n_user, const float *__restrict__ state,
+                                        const int32_t *__restrict__ req_first, int kstride,
                                         float *__restrict__ res_qip) {
     const int q = blockIdx.x;
     const int n = counts[q].n_res_emit;
+    const int first = req_first ? req_first[q] : 0;
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        const int64_t i = (int64_t) q * topk + k;
+        const int64_t i = (int64_t) q * kstride + k;
         const int u = res_user[i];
         int src = res_fresh[i] ? q : -1;
-        for (int qq = q - 1; src < 0 && qq >= 0; qq--)
+        for (int qq = q - 1; src < 0 && qq >= first; qq--)
             if (code[(int64_t) qq * n_user + u] < kCodeResult1) src = qq;
-        res_qip[i] = src >= 0 ? sc.exact(u, src) : state[u];
+        res_qip[i] = src >= 0 ? sc.exact(u, src) : (req_first ? 0.0f : state[u]);
     }
 }
 
@@ -989,44 +1087,111 @@ template <typename T> T *carve(uint8_t *&p, size_t n) {
 inline size_t carve_size(size_t n, size_t elem) { return ((n * elem + 255) & ~size_t(255)) + 256; }
 }  // namespace
 
+// Runs a batch's phase 1: eagerly, or, with ix->graphs_on, from a CUDA graph of the same launches.  A
+// shape (method, batch size, workspace addresses) runs eagerly the first time -- that sizes every
+// buffer it touches -- and is captured the second time and replayed from then on.  A capture that
+// fails (an operation not allowed while capturing) turns graphs off for the index and runs eagerly.
+template <class F> static int run_phase1(rkr_index *ix, int method, int nq, cudaStream_t st, F &&phase1) {
+    if (!ix->graphs_on || ix->prof.on) return phase1(false);
+    const void *ws[8] = {ix->ws_qtr.p, ix->ws_levels.p, ix->ws_cls.p, ix->ws_counts.p,
+                         ix->ws_hist.p, ix->ws_fix.p, ix->ws_sc.p, ix->ws_km.p};
+    rkr_index::PhaseGraph *hit = nullptr;
+    for (auto &g : ix->graphs)
+        if (g.method == method && g.nq == nq && std::equal(ws, ws + 8, g.ws)) hit = &g;
+    if (hit && hit->exec) {
+        RKR_CUDA(cudaGraphLaunch(hit->exec, st));
+        return RKR_OK;
+    }
+    if (!hit) {
+        RKR_TRY(phase1(false));
+        rkr_index::PhaseGraph g;
+        g.method = method;
+        g.nq = nq;
+        // the buffers as they are after the eager run
+        const void *now[8] = {ix->ws_qtr.p, ix->ws_levels.p, ix->ws_cls.p, ix->ws_counts.p,
+                              ix->ws_hist.p, ix->ws_fix.p, ix->ws_sc.p, ix->ws_km.p};
+        std::copy(now, now + 8, g.ws);
+        g.exec = nullptr;
+        ix->graphs.push_back(g);
+        return RKR_OK;
+    }
+    cudaGraph_t graph = nullptr;
+    RKR_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    const int rc = phase1(false);
+    const cudaError_t e = cudaStreamEndCapture(st, &graph);
+    cudaGraphExec_t exec = nullptr;
+    if (rc == RKR_OK && e == cudaSuccess && graph && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+        cudaGraphDestroy(graph);
+        hit->exec = exec;
+        RKR_CUDA(cudaGraphLaunch(exec, st));
+        return RKR_OK;
+    }
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    ix->graphs_on = false;
+    return phase1(false);
+}
+
 // One chunk of queries.  QSRPNormalLP runs both rounds; QS and US (no regression round, scores
 // in the original space) run the scores tile without levels and start at round 2.
-int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, int topk, rkr_user_rank *d_out,
+int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const BatchSpec &bs, rkr_user_rank *d_out,
                rkr_query_stats *d_stats, cudaStream_t st) {
     const bool qsrp = method == RKR_METHOD_QSRP_NORMAL_LP;
+    int kmax = bs.topk;
+    if (bs.k) kmax = *std::max_element(bs.k, bs.k + nq);
     const int64_t U = ix->n_user;
     const int dim = ix->dim, c = ix->check_dim, S = ix->n_sample, Sr = ix->n_sample_reg;
     const int n_item = (int) ix->n_item;
-    const int nl = Sr + 2;
     const int gs = thr_group(S), nb = (S + gs - 1) / gs;
+    const int G = qsrp ? lvt_stride(Sr) : 1;
+    const size_t n_lhist = (size_t) nq * 2 * kLvEntries, n_fhist = (size_t) nq * 2 * G;
     RKR_TRY(ix->ws_qtr.ensure(carve_size((size_t) nq * dim, 4) + carve_size(nq, 4) + carve_size(nq, sizeof(QsrpParams)) +
-                              carve_size(nq, 4) + carve_size(1, 4) * 2 + carve_size(2, 4)));
+                              carve_size(nq, 4) + carve_size(1, 4) * 3 + carve_size(2, 4) + carve_size(n_lhist, 4) +
+                              carve_size(n_fhist, 4) + carve_size(nq, 4) * 2 + carve_size(nq, 8)));
     uint8_t *p0 = ix->ws_qtr.as<uint8_t>();
     float *qtr = carve<float>(p0, (size_t) nq * dim);
+    // per-query k, output offsets and request starts, when given
+    KSpec ks;
+    ks.kmax = kmax;
+    ks.k = nullptr;
+    int32_t *d_k = carve<int32_t>(p0, nq);
+    int64_t *d_out_off = carve<int64_t>(p0, nq);
+    int32_t *d_req_first = carve<int32_t>(p0, nq);
+    if (bs.k) {
+        std::vector<int64_t> oo(nq);
+        int64_t acc = 0;
+        for (int q = 0; q < nq; q++) { oo[q] = acc; acc += bs.k[q]; }
+        RKR_CUDA(cudaMemcpyAsync(d_k, bs.k, sizeof(int32_t) * nq, cudaMemcpyHostToDevice, st));
+        RKR_CUDA(cudaMemcpyAsync(d_out_off, oo.data(), sizeof(int64_t) * nq, cudaMemcpyHostToDevice, st));
+        ks.k = d_k;
+    }
+    if (bs.req_first)
+        RKR_CUDA(cudaMemcpyAsync(d_req_first, bs.req_first, sizeof(int32_t) * nq, cudaMemcpyHostToDevice, st));
     float *qnorm = carve<float>(p0, nq);
     QsrpParams *par = carve<QsrpParams>(p0, nq);
+    uint8_t *pz = p0;  // from here on zeroed per chunk
     int *anomaly = carve<int>(p0, nq);
     int *fix_count = carve<int>(p0, 1);
     int *any2 = carve<int>(p0, 1);
     int *hit_count = carve<int>(p0, 2);
-    RKR_TRY(ix->ws_levels.ensure((size_t) nq * U * 8));
-    RKR_TRY(ix->ws_bucket2.ensure((size_t) nq * U));
+    int *mismatch = carve<int>(p0, 1);
+    int *lhist = carve<int>(p0, n_lhist);
+    int *fhist = carve<int>(p0, n_fhist);
+    RKR_TRY(ix->ws_levels.ensure((size_t) nq * U * (qsrp ? 2 : 1)));
+    uint8_t *code = ix->ws_levels.as<uint8_t>();
+    uint8_t *lvc = qsrp ? code + (size_t) nq * U : nullptr;
     RKR_TRY(ix->ws_cls.ensure(carve_size((size_t) nq * (S + 1), 1) + carve_size((size_t) nq * (nb + 1), 1)));
     RKR_TRY(ix->ws_counts.ensure(sizeof(QueryCounts) * (size_t) nq));
-    const size_t n_hist_l = (size_t) nq * 2 * nl, n_hist_c = (size_t) nq * (nb + 1), n_hist_f = (size_t) nq * (S + 1);
-    RKR_TRY(ix->ws_hist.ensure(carve_size(n_hist_l, 4) + carve_size(n_hist_c, 4) + carve_size(n_hist_f, 4)));
+    const size_t n_hist_c = (size_t) nq * (nb + 1), n_hist_f = (size_t) nq * (S + 1);
+    RKR_TRY(ix->ws_hist.ensure(carve_size(n_hist_c, 4) + carve_size(n_hist_f, 4)));
     const int fix_cap = (int) std::min<int64_t>(int64_t(1) << 26, std::max<int64_t>(int64_t(1) << 20, U * nq / 64));
     const int hit_cap = 1 << 22;
-    RKR_TRY(ix->ws_fix.ensure(carve_size(fix_cap, sizeof(int4)) + carve_size(hit_cap, 8)));
-    uint32_t *lv = ix->ws_levels.as<uint32_t>();
-    float *qip = reinterpret_cast<float *>(lv + (size_t) nq * U);
-    uint8_t *code = ix->ws_bucket2.as<uint8_t>();
+    RKR_TRY(ix->ws_fix.ensure(carve_size(fix_cap, sizeof(int4)) + carve_size(hit_cap, 8) + carve_size(1, 4)));
     uint8_t *pc = ix->ws_cls.as<uint8_t>();
     uint8_t *cls2 = carve<uint8_t>(pc, (size_t) nq * (S + 1));
     uint8_t *clsg = carve<uint8_t>(pc, (size_t) nq * (nb + 1));
     QueryCounts *counts = ix->ws_counts.as<QueryCounts>();
     uint8_t *ph = ix->ws_hist.as<uint8_t>();
-    int *hist_l = carve<int>(ph, n_hist_l);
     int *hist_c = carve<int>(ph, n_hist_c);
     int *hist_f = carve<int>(ph, n_hist_f);
     uint8_t *pm = ix->ws_fix.as<uint8_t>();
@@ -1037,163 +1202,206 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, int topk
     HitList hl;
     hl.e = carve<uint64_t>(pm, hit_cap);
     hl.cap = hit_cap;
-    RKR_CUDA(cudaMemsetAsync(anomaly, 0, sizeof(int) * nq, st));
-    RKR_CUDA(cudaMemsetAsync(fix_count, 0, sizeof(int), st));
-    RKR_CUDA(cudaMemsetAsync(any2, 0, sizeof(int), st));
-    RKR_CUDA(cudaMemsetAsync(hit_count, 0, 2 * sizeof(int), st));
-    RKR_CUDA(cudaMemsetAsync(ix->ws_hist.p, 0, (size_t) (ph - ix->ws_hist.as<uint8_t>()), st));
-
-    if (qsrp) {
-        timed(ix, st, "transfer_query", [&] {
-            transfer_query_kernel<<<nq, 128, 0, st>>>(d_query, ix->transfer_item.as<float>(), dim, c, qtr, qnorm);
-        });
-        RKR_CUDA(cudaGetLastError());
-    } else {
-        RKR_CUDA(cudaMemsetAsync(qnorm, 0, sizeof(float) * nq, st));
-    }
-    ScoreSrc sc;
-    sc.svd_user = ix->svd_user.as<float>();
-    sc.qtr = qtr;
-    sc.dim = dim;
-    sc.c = c;
+    int *n_rescored = carve<int>(pm, 1);
     RegModel m;
     m.rec = ix->reg.as<float>();
     m.rank = ix->reg_rank.as<int32_t>();
     m.S = Sr;
     m.err_cap = (double) Sr - 1e-3;
     m.n_item = n_item;
+    Round1Src r1;
+    r1.svd_user = ix->svd_user.as<float>();
+    r1.qtr = qtr;
+    r1.unorm = ix->svd_unorm.as<float>();
+    r1.qnorm = qnorm;
+    r1.m = m;
+    r1.dim = dim;
+    r1.c = c;
     QipView qv;
-    qv.qip = qip;
-    qv.n_user = U;
     qv.urow = (qsrp ? ix->svd_user : ix->user).as<float>();
     qv.qrow = qsrp ? qtr : d_query;
     qv.dim = dim;
     qv.c = qsrp ? c : dim;
-    Round1Epi e1;
-    e1.unorm = ix->svd_unorm.as<float>();
-    e1.qnorm = qnorm;
-    e1.thr_summ = ix->thr_summ.as<float>();
-    e1.m = m;
-    e1.lv = qsrp ? lv : nullptr;
-    e1.code = code;
-    e1.qip = qip;
-    e1.nb = nb;
-    e1.n_user = U;
-    e1.n_query = nq;
-    e1.fix = fix;
-    // pair scores, levels and coarse groups: on the tensor cores with exact resolution of undecided
-    // pairs where the shape allows, else on the exact tiles
-    bool tc_done = false;
-    {
-        ScoresTcCall call;
-        call.qsrp = qsrp;
-        call.qrows = qv.qrow;
-        call.qnorm = qnorm;
-        call.unorm = e1.unorm;
-        call.nq = nq;
-        call.m = m;
-        call.nb = nb;
-        call.lv = e1.lv;
-        call.code = code;
-        call.qip = qip;
-        RKR_TRY(scores_tc(ix, call, st, &qv.scr, &tc_done));
-    }
-    if (!tc_done) {
-        qv.scr = PairScreen();
-        RKR_TRY(ix->ws_km.ensure(sizeof(float) * (size_t) dim * (size_t) kmajor_ld(nq)));
-        RKR_TRY(to_kmajor(qsrp ? qtr : d_query, nullptr, nq, dim, ix->ws_km.as<float>(), st));
-        cudaError_t ce = cudaSuccess;
-        const KMajor ka = {(qsrp ? ix->svd_user_km : ix->user_km).as<float>(), U, kmajor_ld(U), kmajor_ld(U)};
-        const KMajor kb = {ix->ws_km.as<float>(), nq, kmajor_ld(nq), kmajor_ld(nq)};
-        // QS / US: one sequential sum over all coordinates (QS.hpp:137-143), seen by finish_hi
-        timed(ix, st, "qsrp_scores", [&] { ce = launch_big_split(ka, kb, qsrp ? c : dim, dim, e1, st); });
-        RKR_CUDA(ce);
-    }
-    const int64_t chunk = 16384;
-    dim3 hg((unsigned) ((U + chunk - 1) / chunk), (unsigned) nq);
-    if (qsrp) {
-    if (!tc_done) {
-        timed(ix, st, "qsrp_fix1", [&] { qsrp_fix1_kernel<<<148 * 4, 256, 0, st>>>(fix, m, e1.unorm, qnorm, U, lv); });
-        RKR_CUDA(cudaGetLastError());
-        timed(ix, st, "qsrp_fix1_scan", [&] {
-            qsrp_fix1_scan_kernel<<<148 * 8, 256, 0, st>>>(fix_count, fix_cap, m, sc, e1.unorm, qnorm, U, nq, lv);
-        });
-        RKR_CUDA(cudaGetLastError());
-    }
-    timed(ix, st, "level_hist", [&] {
-        level_hist_kernel<<<hg, kHistThreads, hist_copies(2 * nl) * 2 * nl * sizeof(int), st>>>(lv, U, m.rank, Sr, n_item,
-                                                                                               chunk, hist_l, anomaly);
-    });
-    RKR_CUDA(cudaGetLastError());
-    timed(ix, st, "qsrp_select1", [&] {
-        qsrp_select1_kernel<<<(nq + 3) / 4, 128, 0, st>>>(hist_l, anomaly, U, m.rank, Sr, n_item, topk, nq, par);
-    });
-    RKR_CUDA(cudaGetLastError());
-    {
-        dim3 g((unsigned) std::min<int64_t>((U + 1023) / 1024, 64), (unsigned) nq);
-        timed(ix, st, "qsrp_count1", [&] { qsrp_count1_kernel<<<g, 256, 0, st>>>(lv, U, par); });
-        RKR_CUDA(cudaGetLastError());
-    }
-    timed(ix, st, "qsrp_final1", [&] { qsrp_final1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, topk); });
-    RKR_CUDA(cudaGetLastError());
-    } else {
-        qs_params_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, U);
-        RKR_CUDA(cudaGetLastError());
-    }
-    timed(ix, st, "qsrp_round2", [&] {
-        qsrp_round2_kernel<<<hg, kHistThreads, hist_copies(nb + 1) * (nb + 1) * sizeof(int), st>>>(
-            qsrp ? lv : nullptr, code, U, par, nb, chunk, hist_c);
-    });
-    RKR_CUDA(cudaGetLastError());
-    timed(ix, st, "qsrp_select2c", [&] {
-        qsrp_select2c_kernel<<<(nq + 127) / 128, 128, 0, st>>>(hist_c, nb, topk, nq, par, counts);
-    });
-    RKR_CUDA(cudaGetLastError());
+    qv.n_exact = ix->prof.on ? n_rescored : nullptr;
     const float *thr = ix->thr.as<float>();
     const int32_t *srank = ix->sample_rank.as<int32_t>();
-    const unsigned fg = 148 * 16;
+    const unsigned fg2 = 148 * 16;
     const double inv_user = 1.0 / (double) U;
-    hl.count = hit_count;
-    timed(ix, st, "qsrp_fine2", [&] {
-        qsrp_fine2_kernel<<<fg, 256, 0, st>>>(code, qv, U, nq, inv_user, thr, S, gs, par, 0, any2, hl, hist_f);
-    });
-    RKR_CUDA(cudaGetLastError());
-    timed(ix, st, "qsrp_fine2_list", [&] { qsrp_fine2_list_kernel<<<148 * 8, 256, 0, st>>>(hl, qv, U, thr, S, gs, hist_f); });
-    RKR_CUDA(cudaGetLastError());
-    timed(ix, st, "qsrp_select2f", [&] {
-        qsrp_select2f_kernel<<<(nq + 3) / 4, 128, 0, st>>>(hist_f, nb, gs, S, srank, n_item, topk, nq, par, cls2, clsg, any2);
-    });
-    RKR_CUDA(cudaGetLastError());
-    hl.count = hit_count + 1;
-    timed(ix, st, "qsrp_fine2", [&] {
-        qsrp_fine2_kernel<<<fg, 256, 0, st>>>(code, qv, U, nq, inv_user, thr, S, gs, par, 1, any2, hl, hist_f);
-    });
-    RKR_CUDA(cudaGetLastError());
-    timed(ix, st, "qsrp_fine2_list", [&] { qsrp_fine2_list_kernel<<<148 * 8, 256, 0, st>>>(hl, qv, U, thr, S, gs, hist_f); });
-    RKR_CUDA(cudaGetLastError());
-    timed(ix, st, "qsrp_final2", [&] {
-        qsrp_final2_kernel<<<(nq + 3) / 4, 128, 0, st>>>(hist_c, hist_f, nb, gs, S, topk, nq, par, cls2, clsg, counts);
-    });
-    RKR_CUDA(cudaGetLastError());
+    // Phase 1: both bound rounds up to the round-2 class counts.  Its launches have fixed shapes for
+    // a given batch size and no host synchronisation, so a caller that serves batches of a few sizes
+    // captures it once per size as a CUDA graph and replays it (ix->graphs_on).
+    int *sc_status[2] = {nullptr, nullptr};
+    auto phase1 = [&](bool force_exact) -> int {
+        RKR_CUDA(cudaMemsetAsync(pz, 0, (size_t) (p0 - pz), st));
+        RKR_CUDA(cudaMemsetAsync(n_rescored, 0, sizeof(int), st));
+        RKR_CUDA(cudaMemsetAsync(ix->ws_hist.p, 0, (size_t) (ph - ix->ws_hist.as<uint8_t>()), st));
 
+        if (qsrp) {
+            timed(ix, st, "transfer_query", [&] {
+                transfer_query_kernel<<<nq, 128, 0, st>>>(d_query, ix->transfer_item.as<float>(), dim, c, qtr, qnorm);
+            });
+            RKR_CUDA(cudaGetLastError());
+        } else {
+            RKR_CUDA(cudaMemsetAsync(qnorm, 0, sizeof(float) * nq, st));
+        }
+        // pair codes, coarse levels and their histograms: on the tensor cores with exact resolution of
+        // undecided pairs where the shape allows, else on the exact tiles
+        bool tc_done = false;
+        if (!force_exact) {
+            ScoresTcCall call;
+            call.qsrp = qsrp;
+            call.qrows = qv.qrow;
+            call.qnorm = qnorm;
+            call.unorm = r1.unorm;
+            call.nq = nq;
+            call.m = m;
+            call.nb = nb;
+            call.lvc = lvc;
+            call.code = code;
+            call.lhist = qsrp ? lhist : nullptr;
+            call.anomaly = qsrp ? anomaly : nullptr;
+            call.status = sc_status;
+            RKR_TRY(scores_tc(ix, call, st, &tc_done));
+        }
+        if (!tc_done) {
+            // the exact tiles start from clean counts (a tensor-core run that gave up may have left some)
+            RKR_CUDA(cudaMemsetAsync(lhist, 0, sizeof(int) * n_lhist, st));
+            RKR_CUDA(cudaMemsetAsync(anomaly, 0, sizeof(int) * nq, st));
+            Round1Epi e1;
+            e1.unorm = r1.unorm;
+            e1.qnorm = qnorm;
+            e1.thr_summ = ix->thr_summ.as<float>();
+            e1.m = m;
+            e1.G = G;
+            e1.lvc = lvc;
+            e1.code = code;
+            e1.anomaly = anomaly;
+            e1.nb = nb;
+            e1.n_user = U;
+            e1.n_query = nq;
+            e1.fix = fix;
+            RKR_TRY(ix->ws_km.ensure(sizeof(float) * (size_t) dim * (size_t) kmajor_ld(nq)));
+            RKR_TRY(to_kmajor(qsrp ? qtr : d_query, nullptr, nq, dim, ix->ws_km.as<float>(), st));
+            cudaError_t ce = cudaSuccess;
+            const KMajor ka = {(qsrp ? ix->svd_user_km : ix->user_km).as<float>(), U, kmajor_ld(U), kmajor_ld(U)};
+            const KMajor kb = {ix->ws_km.as<float>(), nq, kmajor_ld(nq), kmajor_ld(nq)};
+            // QS / US: one sequential sum over all coordinates (QS.hpp:137-143), seen by finish_hi
+            timed(ix, st, "qsrp_scores", [&] { ce = launch_big_split(ka, kb, qsrp ? c : dim, dim, e1, st); });
+            RKR_CUDA(ce);
+            if (qsrp) {
+                timed(ix, st, "qsrp_fix1", [&] {
+                    qsrp_fix1_kernel<<<148 * 4, 256, 0, st>>>(fix, m, G, r1.unorm, qnorm, U, lvc, anomaly);
+                });
+                RKR_CUDA(cudaGetLastError());
+                timed(ix, st, "qsrp_fix1_scan", [&] {
+                    qsrp_fix1_scan_kernel<<<148 * 8, 256, 0, st>>>(fix_count, fix_cap, r1, G, U, nq, lvc, anomaly);
+                });
+                RKR_CUDA(cudaGetLastError());
+                const int64_t ch = 65536;
+                const dim3 g((unsigned) ((U + ch - 1) / ch), (unsigned) nq);
+                timed(ix, st, "lvc_hist", [&] { lvc_hist_kernel<<<g, kHistThreads, 0, st>>>(lvc, U, ch, lhist); });
+                RKR_CUDA(cudaGetLastError());
+            }
+        }
+        const int64_t chunk = 16384;
+        dim3 hg((unsigned) ((U + chunk - 1) / chunk), (unsigned) nq);
+        if (qsrp) {
+            timed(ix, st, "qsrp_select1c", [&] {
+                qsrp_select1c_kernel<<<(nq + 127) / 128, 128, 0, st>>>(lhist, U, ks, nq, par);
+            });
+            RKR_CUDA(cudaGetLastError());
+            const dim3 fg((unsigned) ((U + 127) / 128), (unsigned) std::min((nq + 7) / 8, 16));
+            timed(ix, st, "qsrp_fine1", [&] {
+                qsrp_fine1_kernel<<<fg, 256, 0, st>>>(lvc, r1, U, nq, G, 0, par, fhist, mismatch);
+            });
+            RKR_CUDA(cudaGetLastError());
+            timed(ix, st, "qsrp_select1f", [&] {
+                qsrp_select1f_kernel<<<(nq + 3) / 4, 128, 0, st>>>(lhist, fhist, anomaly, U, m.rank, Sr, n_item, G, ks,
+                                                                   nq, par);
+            });
+            RKR_CUDA(cudaGetLastError());
+            timed(ix, st, "qsrp_fine1", [&] {
+                qsrp_fine1_kernel<<<fg, 256, 0, st>>>(lvc, r1, U, nq, G, 1, par, fhist, mismatch);
+            });
+            RKR_CUDA(cudaGetLastError());
+            timed(ix, st, "qsrp_final1", [&] { qsrp_final1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, ks, U); });
+            RKR_CUDA(cudaGetLastError());
+        } else {
+            qs_params_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, U);
+            RKR_CUDA(cudaGetLastError());
+        }
+        timed(ix, st, "qsrp_round2", [&] {
+            qsrp_round2_kernel<<<hg, kHistThreads, hist_copies(nb + 1) * (nb + 1) * sizeof(int), st>>>(
+                lvc, code, U, par, nb, G, chunk, hist_c);
+        });
+        RKR_CUDA(cudaGetLastError());
+        timed(ix, st, "qsrp_select2c", [&] {
+            qsrp_select2c_kernel<<<(nq + 127) / 128, 128, 0, st>>>(hist_c, nb, ks, nq, par, counts);
+        });
+        RKR_CUDA(cudaGetLastError());
+        hl.count = hit_count;
+        timed(ix, st, "qsrp_fine2", [&] {
+            qsrp_fine2_kernel<<<fg2, 256, 0, st>>>(code, qv, U, nq, inv_user, thr, S, gs, par, 0, any2, hl, hist_f);
+        });
+        RKR_CUDA(cudaGetLastError());
+        timed(ix, st, "qsrp_fine2_list", [&] { qsrp_fine2_list_kernel<<<148 * 8, 256, 0, st>>>(hl, qv, U, thr, S, gs, hist_f); });
+        RKR_CUDA(cudaGetLastError());
+        timed(ix, st, "qsrp_select2f", [&] {
+            qsrp_select2f_kernel<<<(nq + 3) / 4, 128, 0, st>>>(hist_f, nb, gs, S, srank, n_item, ks, nq, par, cls2, clsg, any2);
+        });
+        RKR_CUDA(cudaGetLastError());
+        hl.count = hit_count + 1;
+        timed(ix, st, "qsrp_fine2", [&] {
+            qsrp_fine2_kernel<<<fg2, 256, 0, st>>>(code, qv, U, nq, inv_user, thr, S, gs, par, 1, any2, hl, hist_f);
+        });
+        RKR_CUDA(cudaGetLastError());
+        timed(ix, st, "qsrp_fine2_list", [&] { qsrp_fine2_list_kernel<<<148 * 8, 256, 0, st>>>(hl, qv, U, thr, S, gs, hist_f); });
+        RKR_CUDA(cudaGetLastError());
+        timed(ix, st, "qsrp_final2", [&] {
+            qsrp_final2_kernel<<<(nq + 3) / 4, 128, 0, st>>>(hist_c, hist_f, nb, gs, S, ks, nq, qsrp ? m.rank : nullptr, Sr,
+                                                             n_item, par, cls2, clsg, counts);
+        });
+        RKR_CUDA(cudaGetLastError());
+        return RKR_OK;
+    };
+    RKR_TRY(run_phase1(ix, method, nq, st, phase1));
     std::vector<QueryCounts> hc(nq);
-    int h_fix = 0;
+    int h_fix = 0, h_mismatch = 0, h_sc[2] = {0, 0};
     RKR_CUDA(cudaMemcpyAsync(hc.data(), counts, sizeof(QueryCounts) * nq, cudaMemcpyDeviceToHost, st));
     RKR_CUDA(cudaMemcpyAsync(&h_fix, fix_count, sizeof(int), cudaMemcpyDeviceToHost, st));
+    RKR_CUDA(cudaMemcpyAsync(&h_mismatch, mismatch, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (sc_status[0]) {
+        RKR_CUDA(cudaMemcpyAsync(&h_sc[0], sc_status[0], sizeof(int), cudaMemcpyDeviceToHost, st));
+        RKR_CUDA(cudaMemcpyAsync(&h_sc[1], sc_status[1], sizeof(int), cudaMemcpyDeviceToHost, st));
+    }
     RKR_CUDA(cudaStreamSynchronize(st));
+    if (ix->prof.on) ix->prof.add_count("screen_undecided_pairs", h_sc[1]);
+    if (h_sc[0]) {
+        // the tensor-core run gave up (a bounded wait or a full list): the exact tiles redo phase 1
+        RKR_TRY(phase1(true));
+        h_mismatch = 0;
+        RKR_CUDA(cudaMemcpyAsync(hc.data(), counts, sizeof(QueryCounts) * nq, cudaMemcpyDeviceToHost, st));
+        RKR_CUDA(cudaMemcpyAsync(&h_fix, fix_count, sizeof(int), cudaMemcpyDeviceToHost, st));
+        RKR_CUDA(cudaMemcpyAsync(&h_mismatch, mismatch, sizeof(int), cudaMemcpyDeviceToHost, st));
+        RKR_CUDA(cudaStreamSynchronize(st));
+    }
+    if (h_mismatch) {
+        set_error("internal: %d pairs whose exact round-1 level lies outside their coarse level", h_mismatch);
+        return RKR_ERR_STATE;
+    }
     if (ix->prof.on) ix->prof.add_count("screen_undecided_pairs", h_fix);
     std::vector<int64_t> off(nq + 1, 0);
     for (int q = 0; q < nq; q++) off[q + 1] = off[q] + hc[q].n_cand;
     const int64_t n_cand = off[nq];
-    size_t need = carve_size(nq + 1, 8) + carve_size((size_t) nq * topk, 4) * 3 + carve_size((size_t) nq * topk, 1) +
+    size_t need = carve_size(nq + 1, 8) + carve_size((size_t) nq * kmax, 4) * 3 + carve_size((size_t) nq * kmax, 1) +
                   carve_size(n_cand, 4) * 5;
     RKR_TRY(ix->ws_cand.ensure(need));
     uint8_t *p = ix->ws_cand.as<uint8_t>();
     int64_t *d_off = carve<int64_t>(p, nq + 1);
-    int32_t *res_user = carve<int32_t>(p, (size_t) nq * topk);
-    int32_t *res_rank = carve<int32_t>(p, (size_t) nq * topk);
-    float *res_qip = carve<float>(p, (size_t) nq * topk);
-    uint8_t *res_fresh = carve<uint8_t>(p, (size_t) nq * topk);
+    int32_t *res_user = carve<int32_t>(p, (size_t) nq * kmax);
+    int32_t *res_rank = carve<int32_t>(p, (size_t) nq * kmax);
+    float *res_qip = carve<float>(p, (size_t) nq * kmax);
+    uint8_t *res_fresh = carve<uint8_t>(p, (size_t) nq * kmax);
     int32_t *cand_user = carve<int32_t>(p, n_cand);
     int32_t *cand_query = carve<int32_t>(p, n_cand);
     int32_t *cand_lb = carve<int32_t>(p, n_cand);
@@ -1201,7 +1409,9 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, int topk
     float *cand_qip = carve<float>(p, n_cand);
     RKR_CUDA(cudaMemcpyAsync(d_off, off.data(), sizeof(int64_t) * (nq + 1), cudaMemcpyHostToDevice, st));
     QsrpCompactPolicy pol;
-    pol.lv = lv;
+    pol.lvc = lvc;
+    pol.src = r1;
+    pol.G = G;
     pol.code = code;
     pol.thr = thr;
     pol.sc = qv;
@@ -1218,7 +1428,7 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, int topk
     pol.clsg = clsg;
     pol.counts = counts;
     pol.cand_off = d_off;
-    pol.topk = topk;
+    pol.kstride = kmax;
     pol.res_user = res_user;
     pol.res_rank = res_rank;
     pol.res_fresh = res_fresh;
@@ -1226,10 +1436,10 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, int topk
     pol.cand_query = cand_query;
     pol.cand_lb = cand_lb;
     pol.cand_ub = cand_ub;
-    RKR_TRY(run_compaction(ix, pol, nq, topk, counts, st));
+    RKR_TRY(run_compaction(ix, pol, nq, ks, counts, st));
     timed(ix, st, "qsrp_result_fill", [&] {
         qsrp_result_fill_kernel<<<nq, 128, 0, st>>>(counts, res_user, res_fresh, code, qv, U, ix->qip_state.as<float>(),
-                                                    topk, res_qip);
+                                                    bs.req_first ? d_req_first : nullptr, kmax, res_qip);
     });
     RKR_CUDA(cudaGetLastError());
     if (n_cand > 0) {
@@ -1239,16 +1449,18 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, int topk
         });
         RKR_CUDA(cudaGetLastError());
     }
-    RKR_TRY(refine_and_assemble_pairs(ix, method, d_query, nq, topk, counts, res_user, res_rank, res_qip, n_cand,
-                                      cand_user, cand_query, cand_lb, cand_ub, cand_qip, d_off, d_out, d_stats, st));
-    if (qsrp) timed(ix, st, "qsrp_state", [&] {
+    RKR_TRY(refine_and_assemble_pairs(ix, method, d_query, nq, ks, bs.k ? d_out_off : nullptr, counts, res_user,
+                                      res_rank, res_qip, n_cand, cand_user, cand_query, cand_lb, cand_ub, cand_qip, d_off,
+                                      d_out, d_stats, st));
+    // the carried state advances only when requests are not scoped (a scoped request starts fresh)
+    if (qsrp && !bs.req_first) timed(ix, st, "qsrp_state", [&] {
         qsrp_state_kernel<<<(unsigned) ((U + 255) / 256), 256, 0, st>>>(code, qv, U, nq, ix->qip_state.as<float>());
     });
     RKR_CUDA(cudaGetLastError());
     RKR_CUDA(cudaStreamSynchronize(st));
-    if (ix->prof.on && qv.scr.n_exact) {
+    if (ix->prof.on) {
         int h = 0;
-        RKR_CUDA(cudaMemcpy(&h, qv.scr.n_exact, sizeof(int), cudaMemcpyDeviceToHost));
+        RKR_CUDA(cudaMemcpy(&h, n_rescored, sizeof(int), cudaMemcpyDeviceToHost));
         ix->prof.add_count("rescored_pairs", h);
     }
     return RKR_OK;

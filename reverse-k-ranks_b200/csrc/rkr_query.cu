@@ -164,9 +164,10 @@ struct AssembleArgs {
     const int32_t *cand_nproc;
     const int32_t *cand_undecided;
     const int32_t *cand_lb, *cand_ub;
-    int topk;
+    KSpec ks;                    // per-query k; ks.kmax is the result arrays' row stride
+    const int64_t *out_off;      // [n_query] start of each query's output, or nullptr: q * k
     int ipbound, dim, check_dim;
-    rkr_user_rank *out;          // [n_query][topk]
+    rkr_user_rank *out;          // k entries per query
     rkr_query_stats *stats;      // [n_query] or nullptr
     uint64_t *scratch;           // keys for candidates beyond kSortCap (indexed by candidate)
 };
@@ -185,11 +186,11 @@ __global__ void assemble_kernel(AssembleArgs a) {
     __shared__ uint64_t thresh;
     const int q = blockIdx.x;
     const QueryCounts c = a.counts[q];
-    const int topk = a.topk;
-    rkr_user_rank *out = a.out + (int64_t) q * topk;
+    const int topk = a.ks.of(q);
+    rkr_user_rank *out = a.out + (a.out_off ? a.out_off[q] : (int64_t) q * topk);
     const int nres = c.n_res_emit;
     for (int k = threadIdx.x; k < nres; k += blockDim.x) {
-        const int64_t i = (int64_t) q * topk + k;
+        const int64_t i = (int64_t) q * a.ks.kmax + k;
         out[k].user_id = a.res_user[i];
         out[k].rank = a.res_rank[i];
         out[k].query_ip = a.res_qip[i];
@@ -339,8 +340,8 @@ inline size_t carve_size(size_t n, size_t elem) { return ((n * elem + 255) & ~si
 }  // namespace
 
 // Runs candidate refinement and assembly for one chunk whose candidates are listed in the pool.
-static int refine_and_assemble(rkr_index *ix, int method, const float *d_query, int nq, int topk,
-                               const QueryCounts *d_counts, const std::vector<QueryCounts> &h_counts,
+static int refine_and_assemble(rkr_index *ix, int method, const float *d_query, int nq, KSpec ks,
+                               const int64_t *d_out_off, const QueryCounts *d_counts, const std::vector<QueryCounts> &h_counts,
                                const int32_t *d_res_user, const int32_t *d_res_rank, const float *d_res_qip,
                                int64_t n_cand, int32_t *d_cand_user, int32_t *d_cand_query, int32_t *d_cand_lb,
                                int32_t *d_cand_ub, const float *d_cand_qip_given, const int64_t *d_cand_off,
@@ -422,7 +423,8 @@ static int refine_and_assemble(rkr_index *ix, int method, const float *d_query, 
     aa.check_dim = ix->check_dim;
     aa.cand_lb = d_cand_lb;
     aa.cand_ub = d_cand_ub;
-    aa.topk = topk;
+    aa.ks = ks;
+    aa.out_off = d_out_off;
     aa.out = d_out;
     aa.stats = d_stats;
     aa.scratch = nullptr;
@@ -433,35 +435,47 @@ static int refine_and_assemble(rkr_index *ix, int method, const float *d_query, 
 }
 
 // One chunk of queries, every method (rkr_qsrp.cu).
-int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, int topk, rkr_user_rank *d_out,
+int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const BatchSpec &bs, rkr_user_rank *d_out,
                rkr_query_stats *d_stats, cudaStream_t st);
 
-int refine_and_assemble_pairs(rkr_index *ix, int method, const float *d_query, int nq, int topk,
-                              const QueryCounts *d_counts, const int32_t *d_res_user, const int32_t *d_res_rank,
+int refine_and_assemble_pairs(rkr_index *ix, int method, const float *d_query, int nq, KSpec ks,
+                              const int64_t *d_out_off, const QueryCounts *d_counts, const int32_t *d_res_user, const int32_t *d_res_rank,
                               const float *d_res_qip, int64_t n_cand, int32_t *d_cand_user, int32_t *d_cand_query,
                               int32_t *d_cand_lb, int32_t *d_cand_ub, const float *d_cand_qip,
                               const int64_t *d_cand_off, rkr_user_rank *d_out, rkr_query_stats *d_stats,
                               cudaStream_t st) {
     std::vector<QueryCounts> unused;
-    return refine_and_assemble(ix, method, d_query, nq, topk, d_counts, unused, d_res_user, d_res_rank, d_res_qip, n_cand,
+    return refine_and_assemble(ix, method, d_query, nq, ks, d_out_off, d_counts, unused, d_res_user, d_res_rank,
+                               d_res_qip, n_cand,
                                d_cand_user, d_cand_query, d_cand_lb, d_cand_ub, d_cand_qip, d_cand_off, d_out, d_stats,
                                st);
 }
 
-int query_batch(rkr_index *ix, int method, const float *d_query, int n_query, int topk, rkr_user_rank *d_out,
-                rkr_query_stats *d_stats, cudaStream_t st) {
-    // Chunk so the per-pair arrays (levels, scores, codes: 9 bytes a pair) stay within a bounded
-    // slice of device memory.
-    const int64_t budget = int64_t(16) << 30;
-    const int64_t per_q = ix->n_user * 9 + 4096;
+int query_batch(rkr_index *ix, int method, const float *d_query, int n_query, const BatchSpec &bs,
+                rkr_user_rank *d_out, rkr_query_stats *d_stats, cudaStream_t st) {
+    // Chunk so the per-pair arrays (coarse levels and group codes: 2 bytes a pair) stay within a
+    // bounded slice of device memory.
+    const int64_t budget = int64_t(8) << 30;
+    const int64_t per_q = ix->n_user * 2 + 4096;
     int chunk = (int) std::max<int64_t>(1, std::min<int64_t>(n_query, budget / per_q));
-    chunk = std::min(chunk, 4096);
+    chunk = std::min(chunk, kMaxChunkQueries);
+    int64_t out_at = 0;
     for (int q0 = 0; q0 < n_query; q0 += chunk) {
         const int nq = std::min(chunk, n_query - q0);
+        BatchSpec part = bs;
+        std::vector<int32_t> first;
+        if (bs.k) part.k = bs.k + q0;
+        if (bs.req_first) {
+            // a request that started in an earlier chunk continues from this chunk's first query
+            first.resize(nq);
+            for (int q = 0; q < nq; q++) first[q] = std::max(bs.req_first[q0 + q] - q0, 0);
+            part.req_first = first.data();
+        }
         const float *dq = d_query + (int64_t) q0 * ix->dim;
-        rkr_user_rank *dout = d_out + (int64_t) q0 * topk;
         rkr_query_stats *dst = d_stats ? d_stats + q0 : nullptr;
-        RKR_TRY(pair_chunk(ix, method, dq, nq, topk, dout, dst, st));
+        RKR_TRY(pair_chunk(ix, method, dq, nq, part, d_out + out_at, dst, st));
+        if (bs.k) for (int q = 0; q < nq; q++) out_at += bs.k[q0 + q];
+        else out_at += (int64_t) nq * bs.topk;
     }
     return RKR_OK;
 }

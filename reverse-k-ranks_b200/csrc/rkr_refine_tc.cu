@@ -513,6 +513,32 @@ int64_t pick_shares(int64_t tiles, int64_t chunks) {
 
 }  // namespace
 
+// The items' digit chunks and group data for the refinement split (QS / QSRP: at check_dim, in the
+// norm order; US: unsplit), built once per split and kept with the index.
+int refine_tc_tiles(rkr_index *ix, bool ipbound, cudaStream_t st) {
+    const int dim = ix->dim;
+    const int c = ipbound ? ix->check_dim : dim;
+    const int n1 = c, n2 = dim - c;
+    if (n1 <= 0 || n1 > kScMaxPart || n2 > kScMaxPart) return RKR_OK;
+    const int cp = round32(n1), kp = cp + round32(n2);
+    if (kp > kRfMaxKp) return RKR_OK;
+    const int64_t n_item = ix->n_item, item_pad = (n_item + kScN - 1) / kScN * kScN;
+    DevBuf &isl = ipbound ? ix->ri_item_split : ix->ri_item_full;
+    DevBuf &imeta = ipbound ? ix->ri_imeta_split : ix->ri_imeta_full;
+    int &key = ipbound ? ix->ri_key_split : ix->ri_key_full;
+    if (key != c) {
+        key = -2;
+        RKR_TRY(isl.ensure((size_t) item_pad * kScSlices * kp));
+        RKR_TRY(imeta.ensure(sizeof(float4) * 4 * (size_t) (item_pad / kRfGroup)));
+        rf_slice_kernel<<<(unsigned) (item_pad / kRfGroup), 256, 0, st>>>(
+            ix->item_sorted.as<float>(), nullptr, n_item, dim, c, cp, kp, kScN, 1,
+            ipbound ? ix->item_rnorm.as<float>() : nullptr, isl.as<int8_t>(), nullptr, imeta.as<float4>());
+        RKR_CUDA(cudaGetLastError());
+        key = c;
+    }
+    return RKR_OK;
+}
+
 int refine_tc(rkr_index *ix, const RefineArgs &ra, cudaStream_t st, bool *done) {
     *done = false;
     const int dim = ix->dim;
@@ -524,20 +550,9 @@ int refine_tc(rkr_index *ix, const RefineArgs &ra, cudaStream_t st, bool *done) 
     const int64_t n_item = ix->n_item, item_pad = (n_item + kScN - 1) / kScN * kScN;
     const int64_t cand_pad = (ra.n_cand + kScM - 1) / kScM * kScM;
     if (cand_pad / kScM > 65535) return RKR_OK;  // the exact tiles take batches this large
-    // the items' digit chunks and group data for this split, in the norm order (built once, kept)
+    RKR_TRY(refine_tc_tiles(ix, ra.ipbound != 0, st));
     DevBuf &isl = ra.ipbound ? ix->ri_item_split : ix->ri_item_full;
     DevBuf &imeta = ra.ipbound ? ix->ri_imeta_split : ix->ri_imeta_full;
-    int &key = ra.ipbound ? ix->ri_key_split : ix->ri_key_full;
-    if (key != c) {
-        key = -2;
-        RKR_TRY(isl.ensure((size_t) item_pad * kScSlices * kp));
-        RKR_TRY(imeta.ensure(sizeof(float4) * 4 * (size_t) (item_pad / kRfGroup)));
-        rf_slice_kernel<<<(unsigned) (item_pad / kRfGroup), 256, 0, st>>>(
-            ix->item_sorted.as<float>(), nullptr, n_item, dim, c, cp, kp, kScN, 1,
-            ra.ipbound ? ix->item_rnorm.as<float>() : nullptr, isl.as<int8_t>(), nullptr, imeta.as<float4>());
-        RKR_CUDA(cudaGetLastError());
-        key = c;
-    }
     // undecided tests (a small fraction of the candidates' items); past the list they are resolved in line
     const int list_cap = (int) std::min<int64_t>(int64_t(1) << 26,
                                                  std::max<int64_t>(int64_t(1) << 20, cand_pad * n_item / 1024));

@@ -69,6 +69,24 @@ __device__ __forceinline__ int64_t regression_index_exact(float nx, float a, flo
     return upper ? f2i64_x86(floorf(__fsub_rn(pred, err))) : f2i64_x86(ceilf(__fadd_rn(pred, err)));
 }
 
+// One side of ComputeRankBound (:326-380) with the reference's arithmetic at score q: the level of
+// rank_lb (upper = false; 1 .. S + 1) or of rank_ub (upper = true; 0 .. S + 1).  capped: the fit
+// error reached the cap, so the model is not used.
+__device__ __forceinline__ int regression_level_side(float a, float b, float mu, float sigma, float err, float smax,
+                                                     float smin, bool capped, int S, float q, bool upper) {
+    if (!upper) {
+        if (q > smax) return 1;
+        if (q < smin || capped) return S + 1;
+        const int64_t pr = regression_index_exact(__fdiv_rn(__fsub_rn(q, mu), sigma), a, b, err, false);
+        return pr >= S ? S + 1 : (pr < 0 ? 1 : (int) pr + 1);
+    }
+    if (q > smax) return 0;
+    if (q < smin) return S;
+    if (capped) return 0;
+    const int64_t pr = regression_index_exact(__fdiv_rn(__fsub_rn(q, mu), sigma), a, b, err, true);
+    return pr >= S ? S + 1 : (pr < 0 ? 0 : (int) pr + 1);
+}
+
 // ComputeRankBound (:326-380) with the reference's arithmetic, returning levels: 0 -> rank 0,
 // j + 1 -> rank[j], S + 1 -> n_item.
 // Returns lvl_lb | lvl_ub << 16.  Scalar arguments only: a call with a reference to a kernel
@@ -142,33 +160,65 @@ __device__ __forceinline__ bool regression_levels_fast(const RegUser &r, int S, 
     return (!in_l || ok_l) && (!in_u || ok_u) && r.margin < INFINITY;
 }
 
+// ---- per-user level-boundary tables ------------------------------------------------------------------
+//
+// For each user and side, the reference's level is a non-increasing step function of the score.
+// The table holds, at every G-th level value g G (g = 0 .. kLvEntries - 1, G = lvt_stride(S), so
+// that (kLvEntries - 1) G >= S + 1), the smallest binary32 score T_g whose level is <= g G, and a
+// guard band: outside [T_g - band_g, T_g + band_g] the level's relation to g G is the exact-math
+// one (the reference's binary32 evaluation can only differ from it where the model's value lies
+// within its rounding error of the crossing integer).  A score q then has coarse level
+// c = #{g : q < T_g} = ceil(level / G), decided for every score within dq of q when
+// (c == kLvEntries - 1 or q - dq >= T_c + band_c) and (c == 0 or q + dq < T_(c-1) - band_(c-1)).
+// Entries are (T_g, band_g); a user whose record is unusable for the tables (a non-finite value,
+// sigma <= 0, a slope a >= 0) has NaN entries, so none of its pairs is ever decided from them.
+constexpr int kLvEntries = 16;
+
+__host__ __device__ __forceinline__ int lvt_stride(int S) { return (S + 1 + kLvEntries - 2) / (kLvEntries - 1); }
+// coarse level of an exact level (the table's ceil(level / G))
+__device__ __forceinline__ int lvt_coarse(int lvl, int G) { return (lvl + G - 1) / G; }
+
+// Coarse level of score q on one side from the table row (entry j of this user at t[j * stride]),
+// and whether every score within dq of q has it.
+__device__ __forceinline__ bool lvt_screen(const float2 *t, int stride, float q, float dq, int &c) {
+    int k = 0;
+#pragma unroll
+    for (int st = 8; st >= 1; st >>= 1) k += q < t[(k + st - 1) * stride].x ? st : 0;
+    c = k;
+    bool ok = true;
+    if (k < kLvEntries - 1) {
+        const float2 e = t[k * stride];
+        ok = __fsub_rd(q, dq) >= __fadd_ru(e.x, e.y);
+    }
+    if (k > 0) {
+        const float2 e = t[(k - 1) * stride];
+        ok = ok && __fadd_ru(q, dq) < __fsub_rd(e.x, e.y);
+    }
+    return ok;
+}
+
 __device__ __forceinline__ int level_rank(int lvl, const int32_t *rank, int S, int n_item) {
     return lvl == 0 ? 0 : (lvl > S ? n_item : rank[lvl - 1]);
 }
 
-// How the stored pair scores relate to the reference's: exact when umeta is null, else within
-// delta(u, q) of it (the tensor-core scores, rkr_scores_tc.cu).
-struct PairScreen {
-    const float4 *umeta = nullptr, *qmeta = nullptr;  // per row {2^e, |first part|, |second part|, e}
-    float cl = 0.0f, kl = 0.0f, cr = 0.0f, kr = 0.0f;  // bound coefficients of the two parts
-    uint32_t *xbits = nullptr;  // [query][(n_user + 31) / 32]: the stored score is already the reference's
-    int *n_exact = nullptr;     // recomputed scores (a counter)
-};
-
-// One batch of pair scores for the bound rounds (rkr_scores_tc.cu): levels (QSRP), coarse group
-// codes and scores of every (query, user) pair.
+// One batch of pair scores for the bound rounds (rkr_scores_tc.cu): coarse levels (QSRP) and coarse
+// group codes of every (query, user) pair, and the coarse-level histograms.
 struct ScoresTcCall {
     bool qsrp;
     const float *qrows, *qnorm, *unorm;  // queries (SVD space for QSRP), remaining-coordinate norms
     int nq;
     RegModel m;
     int nb;
-    uint32_t *lv;
-    uint8_t *code;
-    float *qip;
+    uint8_t *lvc;    // [nq][n_user] (QSRP)
+    uint8_t *code;   // [nq][n_user]
+    int *lhist;      // [nq][2][kLvEntries] (QSRP), zeroed by the caller
+    int *anomaly;    // [nq] (QSRP), zeroed by the caller
+    int **status = nullptr;  // if set: receives device pointers to the run's status (0: complete) and
+                             // undecided-pair count, and the call does not wait for the device
 };
 // Runs the tensor-core scores where the shape allows; *done = false leaves the batch to the exact
-// tiles.
-int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, PairScreen *screen, bool *done);
+// tiles (the histograms may then hold partial counts: the caller clears them).  With call.status
+// set, *done only says the kernels were launched; the caller checks the status on the device.
+int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, bool *done);
 
 }  // namespace rkr

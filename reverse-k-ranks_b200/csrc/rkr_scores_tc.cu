@@ -44,59 +44,10 @@ namespace {
 
 constexpr int kScEpiWarps = 16;
 constexpr int kScThreads = 32 * (kScEpiWarps + 1);
-constexpr int kScListCap = 4096;                   // undecided pairs per CTA resolved in the kernel
+constexpr int kScListCap = 2048;                   // undecided pairs per CTA resolved in the kernel
 constexpr int kScMaxQ = 1024;                      // queries per launch (their data sits in shared memory)
 constexpr int kScMaxKp = 224;                      // padded coordinates (both parts): shared memory
 constexpr int kScSummStride = kScM;  // summary transposed: entry j of row r at j * kScM + r (lanes hit distinct banks)
-
-// ---- screened regression levels ------------------------------------------------------------------------
-
-// The regression CDF from a table: the reference's formula (Abramowitz & Stegun 7.1.26, as
-// NormalLinearRegressionLP::CDFPhi evaluates it, NormalLinearRegressionLP.hpp:123-143) tabulated in
-// double at z_i = -8 + i / 128 and interpolated by the quadratic through z_i, z_i+1, z_i+2 (Newton
-// form: value, first difference, half the second difference, each rounded to binary32).  Against the
-// reference's own evaluation at the same argument the result is within kCdfTabErr: interpolation
-// f (f-1) (f-2) / 6 h^3 max|f^(3)| < 2e-8, the table's and the evaluation's roundings < 3e-7, the
-// reference's roundings < 4e-7, and the argument's few ulps.
-constexpr int kCdfTabCells = 2048;
-constexpr float kCdfTabErr = 1.0e-6f;
-
-// One side of the screen for a bound score q known to within dq of the reference's.  Within a cell
-// the formula's slope stays within a factor 1.1 of the cell's mean slope D * 128 on the cell widened
-// by dq / sigma <= 2^-10 (|z| <= 8; beyond, the slope is below 1e-14), so the CDF moves by at most
-// (D * 141 + 1e-6) dq / sigma, the 1e-6 covering the formula's deviation from the normal density.
-// A user whose fit error reaches the cap takes the reference's capped levels in range
-// (ComputeRankBound's error test).  Returns false when undecided.
-__device__ __forceinline__ bool level_side(const RegUser &r, float margin0, float cu, int S, float q, float dq,
-                                           bool upper, const float2 *__restrict__ tab, const float *__restrict__ tab2,
-                                           int &lvl) {
-    const float z = __fsub_rn(q, r.mu) * r.inv_sigma;
-    const float t = fminf(fmaxf(fmaf(z, 128.0f, 1024.0f), 0.0f), 2047.0f);
-    const float tu = (t - 0.5f) + 12582912.0f;          // nearest integer of t - 0.5, in the significand
-    const int i = __float_as_int(tu) - 0x4B400000;      // in [0, 2047]: floor(t), or floor(t) - 1 near integral t
-    const float f = t - (tu - 12582912.0f);             // in [0, 1] up to 2^-14
-    const float2 e = tab[i];
-    const float cdf = fmaf(f, fmaf(f - 1.0f, tab2[i], e.y), e.x);
-    const float base = fmaf(cdf, r.a, r.b);
-    const float v = upper ? base - r.err : base + r.err;
-    const float margin = fmaf(cu * dq, fmaf(e.y, 141.0f, 1e-6f), margin0);
-    const bool capped = !(margin0 < INFINITY);
-    const bool above = q - dq > r.smax, below = q + dq < r.smin;
-    const bool inside = q + dq <= r.smax && q - dq >= r.smin;
-    // one rounding instruction: floor; ceil and the distance to the nearest integer follow from it
-    const float fl = floorf(v);
-    const float frac = v - fl;  // exact for |v| < 2^24; larger values stay undecided
-    const float cv = upper ? fl : (frac > 0.0f ? fl + 1.0f : fl);
-    // level of cv (integral): >= S -> S + 1, < 0 -> low, else cv + 1 (cv < 2^22: read off the significand)
-    const int low = upper ? 0 : 1;
-    const int in_range = __float_as_int(cv + 12582912.0f) - 0x4B400000 + 1;
-    const int lv_model = cv >= (float) S ? S + 1 : (cv < 0.0f ? low : in_range);
-    const int in_lvl = capped ? (upper ? 0 : S + 1) : lv_model;
-    if (upper) lvl = above ? 0 : (below ? S : in_lvl);
-    else lvl = above ? 1 : (below ? S + 1 : in_lvl);
-    const bool decided_in = capped || (fminf(frac, 1.0f - frac) > margin && fabsf(v) < 1.6e7f);
-    return (above || below || (inside && decided_in)) && dq * r.inv_sigma <= 9.765625e-4f;
-}
 
 // ---- the tile kernel -----------------------------------------------------------------------------------
 
@@ -107,12 +58,14 @@ struct ScArgs {
     const float *urow, *qrow;      // exact rows: [n_user][dim], [nq][dim]
     const float *thr_summ;
     RegModel m;
-    uint32_t *lv;                  // nullptr: no regression round (QS, US)
-    const float2 *cdf_tab;         // [kCdfTabCells] (value, first difference)
-    const float *cdf_tab2;         // [kCdfTabCells] half the second difference
-    uint8_t *code;
-    float *qip;
-    uint32_t *xbits;               // [query][(n_user + 31) / 32]: pairs whose stored score is the reference's
+    const float2 *lvt;             // [n_user][2][kLvEntries] level tables; nullptr: no regression round (QS, US)
+    int G;                         // the tables' level stride
+    uint8_t *lvc;                  // [query][n_user]: coarse lower-bound level | coarse upper-bound level << 4
+    uint8_t *code;                 // [query][n_user]: coarse threshold group of the full score
+    int *lhist;                    // [query][2][kLvEntries] coarse-level counts; the lower side's last bin and
+                                   // the upper side's bin 0 are left implicit (n_user minus the others)
+    int *anomaly;                  // [query]: pairs whose upper-bound rank exceeds their lower-bound rank
+    float2 *dump;                  // [query][n_user] (estimate of the full score, its bound), or nullptr
     int2 *ovf;                     // undecided pairs, (query, user): each tile's list in one piece
     int *ovf_count, *status, *undecided;
     int ovf_cap;
@@ -158,16 +111,26 @@ __device__ __forceinline__ float exact_dot_any(const float *a, const float *__re
     return acc;
 }
 
-// The user's and the query's rows and the user's threshold summary in global memory.
+// One undecided pair by the reference's arithmetic (batch query q): its coarse levels (counted in
+// the histograms, checked for the rank-order anomaly) and its group code.  The user's row in shared
+// or global memory, its threshold summary in global memory.
 __device__ __forceinline__ void exact_pair(const ScArgs &a, int64_t u, int q, const float *summ, const float *ur) {
     const float *qr = a.qrow + (int64_t) q * a.dim;
     const float left = exact_dot_any(ur, qr, a.c);
     float full = left;
     const int64_t o = (int64_t) q * a.n_user + u;
-    if (a.lv) {
+    if (a.lvt) {
         const float right = __fmul_rn(a.unorm[u], a.qnorm[q]);
-        a.lv[o] = regression_levels_exact(a.m.rec, a.m.S, a.m.err_cap, u, __fsub_rn(left, right),
-                                          __fadd_rn(left, right));
+        const uint32_t v = regression_levels_exact(a.m.rec, a.m.S, a.m.err_cap, u, __fsub_rn(left, right),
+                                                   __fadd_rn(left, right));
+        const int l = (int) (v & 0xffffu), h = (int) (v >> 16);
+        const int cl = lvt_coarse(l, a.G), cu = lvt_coarse(h, a.G);
+        a.lvc[o] = (uint8_t) (cl | (cu << 4));
+        int *hq = a.lhist + (int64_t) q * 2 * kLvEntries;
+        if (cl != kLvEntries - 1) atomicAdd(hq + cl, 1);
+        if (cu != 0) atomicAdd(hq + kLvEntries + cu, 1);
+        if (h > l && level_rank(h, a.m.rank, a.m.S, a.m.n_item) > level_rank(l, a.m.rank, a.m.S, a.m.n_item))
+            atomicAdd(a.anomaly + q, 1);
     }
     if (a.c < a.dim) full = __fadd_rn(left, exact_dot_any(ur + a.c, qr + a.c, a.dim - a.c));
     int g = 0;  // the summary entries >= full (descending, -inf padded)
@@ -175,9 +138,11 @@ __device__ __forceinline__ void exact_pair(const ScArgs &a, int64_t u, int q, co
     for (int st = 16; st >= 1; st >>= 1) g += __ldg(summ + g + st - 1) >= full ? st : 0;
     g += __ldg(summ + g) >= full;
     a.code[o] = (uint8_t) min(g, a.nb);
-    a.qip[o] = full;
-    atomicOr(a.xbits + (int64_t) q * ((a.n_user + 31) >> 5) + (u >> 5), 1u << (u & 31));
 }
+
+// Adds to a shared-memory histogram of byte counters packed four to a word (no counter exceeds
+// kScM = 128, so no byte overflows into the next).
+__device__ __forceinline__ void hist_add(uint32_t *h, int bin, uint32_t n) { atomicAdd(h + (bin >> 2), n << (8 * (bin & 3))); }
 
 __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
     extern __shared__ __align__(1024) uint8_t sm_raw[];
@@ -188,17 +153,19 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
     const int64_t u0 = (int64_t) blockIdx.x * kScM;
     const int kp = a.kp, nq = a.nq;
     const int nchunks = (nq + kScN - 1) / kScN;
+    const bool lev = a.lvt != nullptr;
     // shared memory: the user tile (A), two query chunk buffers (B, slices as consecutive row groups),
-    // the threshold summary, the undecided list, the CDF table and the batch's query data
+    // the threshold summary, the undecided list, the batch's query data, the coarse-level histograms
+    // of two chunks and (QSRP) the tile's level tables
     const uint32_t a_bytes = (uint32_t) (kScSlices * kScM * kp), b_bytes = (uint32_t) (kScSlices * kScN * kp);
     uint8_t *sA = sm_raw;
     uint8_t *sB = sA + a_bytes;
     float *summ = reinterpret_cast<float *>(sB + 2 * b_bytes);
     uint32_t *list = reinterpret_cast<uint32_t *>(summ + ThrSummary::kMaxGroups * kScSummStride);
-    float2 *tab = reinterpret_cast<float2 *>(list + kScListCap);
-    float *tab2 = reinterpret_cast<float *>(tab + kCdfTabCells);
-    float4 *sq = reinterpret_cast<float4 *>(tab2 + kCdfTabCells);  // the batch's query data
+    float4 *sq = reinterpret_cast<float4 *>(list + kScListCap);  // the batch's query data
     float *sqn = reinterpret_cast<float *>(sq + kScMaxQ);
+    uint32_t *shist = reinterpret_cast<uint32_t *>(sqn + kScMaxQ);           // [2][kScN][2][kLvEntries / 4]
+    float2 *stab = reinterpret_cast<float2 *>(shist + 2 * kScN * 2 * (kLvEntries / 4));  // [2 kLvEntries][kScM]
     volatile int *abort = &abort_flag;
 
     if (tid == 0) {
@@ -222,14 +189,16 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
         summ[j * kScSummStride + rr] =
             u0 + rr < a.n_user ? __ldg(a.thr_summ + (u0 + rr) * ThrSummary::kMaxGroups + j) : -INFINITY;
     }
-    if (a.lv)
-        for (int i = tid; i < kCdfTabCells; i += kScThreads) {
-            tab[i] = __ldg(a.cdf_tab + i);
-            tab2[i] = __ldg(a.cdf_tab2 + i);
+    if (lev)
+        for (int idx = tid; idx < kScM * 2 * kLvEntries; idx += kScThreads) {
+            const int rr = idx / (2 * kLvEntries), j = idx % (2 * kLvEntries);
+            stab[j * kScM + rr] = u0 + rr < a.n_user ? __ldg(a.lvt + (u0 + rr) * 2 * kLvEntries + j)
+                                                     : make_float2(NAN, NAN);
         }
+    for (int i = tid; i < 2 * kScN * 2 * (kLvEntries / 4); i += kScThreads) shist[i] = 0u;
     for (int i = tid; i < nq; i += kScThreads) {
         sq[i] = __ldg(a.qmeta + i);
-        sqn[i] = a.lv ? __ldg(a.qnorm + i) : 0.0f;
+        sqn[i] = lev ? __ldg(a.qnorm + i) : 0.0f;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -312,19 +281,21 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
         const int64_t u = u0 + row;
         const bool uval = u < a.n_user;
         const float *srow = summ + row;  // entry j at srow[j * kScSummStride]
-        RegUser r = {};
-        float un = 0.0f, cu = 0.0f, margin0 = 0.0f;
+        const float2 *tl = stab + row, *tu = stab + kLvEntries * kScM + row;  // entry j at t[j * kScM]
+        float un = 0.0f;
         float4 um = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        // the common cases of the two sides in registers: the lower side's last coarse level (scores
+        // surely below T_(E-2) - band) and the upper side's level 0 (scores surely at or above T_0 + band)
+        float lo_last = -INFINITY, hi_first = INFINITY;
         if (uval) {
             um = __ldg(a.umeta + u);
-            if (a.lv) {
-                r = reg_user(a.m, u);
+            if (lev) {
                 un = __ldg(a.unorm + u);
-                cu = fabsf(r.a) * r.inv_sigma * 1.0001f;
-                // the screen's margin for a known score, with the table's error in place of the fast CDF's
-                margin0 = r.margin < INFINITY
-                              ? fabsf(r.a) * kCdfTabErr + (fabsf(r.a) + fabsf(r.b) + fabsf(r.err)) * 4.8e-7f + 1e-6f
-                              : INFINITY;
+                const float2 el = tl[(kLvEntries - 2) * kScM], eu = tu[0];
+                lo_last = __fsub_rd(el.x, el.y);
+                hi_first = __fadd_ru(eu.x, eu.y);
+                if (!(lo_last == lo_last)) lo_last = -INFINITY;   // NaN entries: never the fast path
+                if (!(hi_first == hi_first)) hi_first = INFINITY;
             }
         }
         // the first two steps of the group search from registers
@@ -332,135 +303,170 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
         const int ue = __float_as_int(um.w);
         const float cl_u = a.cl * um.y, cr_u = a.cr * um.z;
         const uint32_t lane_base = taddr + ((uint32_t) (32 * quad) << 16) + (uint32_t) (8 * cg);
-        const int S = a.m.S;
         int n_und = 0;
+        bool dead = false;
         for (int j = 0; j < nchunks; j++) {
             const int b = j & 1;
             const uint32_t ph = (uint32_t) (j >> 1) & 1u;
-            if (!mbar_wait(&bar_mma[b], ph, abort)) {
+            if (!dead && !__all_sync(0xffffffffu, mbar_wait(&bar_mma[b], ph, abort))) {
                 *abort = 1;
                 atomicExch(a.status, 1);
-                break;
+                dead = true;
             }
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            float sl[8], sr[8];
-            {
-                uint32_t v0[8], v1[8], v2[8], v3[8];
-                const uint32_t base = lane_base + (uint32_t) b * buf_cols;
-                tmem_ld8(base, v0);
-                tmem_ld8(base + kScN, v1);
-                tmem_ld8(base + 2 * kScN, v2);
-                tmem_ld8(base + 3 * kScN, v3);
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-                for (int i = 0; i < 8; i++) sl[i] = combine4(v0[i], v1[i], v2[i], v3[i]);
-                if (a.two_parts) {
-                    tmem_ld8(base + 4 * kScN, v0);
-                    tmem_ld8(base + 5 * kScN, v1);
-                    tmem_ld8(base + 6 * kScN, v2);
-                    tmem_ld8(base + 7 * kScN, v3);
+            uint32_t *hb = shist + b * (kScN * 2 * (kLvEntries / 4));
+            if (!dead) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                float sl[8], sr[8];
+                {
+                    uint32_t v0[8], v1[8], v2[8], v3[8];
+                    const uint32_t base = lane_base + (uint32_t) b * buf_cols;
+                    tmem_ld8(base, v0);
+                    tmem_ld8(base + kScN, v1);
+                    tmem_ld8(base + 2 * kScN, v2);
+                    tmem_ld8(base + 3 * kScN, v3);
                     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-                    for (int i = 0; i < 8; i++) sr[i] = combine4(v0[i], v1[i], v2[i], v3[i]);
-                } else {
+                    for (int i = 0; i < 8; i++) sl[i] = combine4(v0[i], v1[i], v2[i], v3[i]);
+                    if (a.two_parts) {
+                        tmem_ld8(base + 4 * kScN, v0);
+                        tmem_ld8(base + 5 * kScN, v1);
+                        tmem_ld8(base + 6 * kScN, v2);
+                        tmem_ld8(base + 7 * kScN, v3);
+                        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-                    for (int i = 0; i < 8; i++) sr[i] = 0.0f;
+                        for (int i = 0; i < 8; i++) sr[i] = combine4(v0[i], v1[i], v2[i], v3[i]);
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < 8; i++) sr[i] = 0.0f;
+                    }
                 }
-            }
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&bar_free[b]);
-            uint32_t und_bits = 0;
-            // four pairs at a time, in side-effect-free phases so that their chains interleave
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bar_free[b]);
+                uint32_t und_bits = 0;
+                // four pairs at a time, in side-effect-free phases so that their chains interleave
 #pragma unroll
-            for (int i0 = 0; i0 < 8; i0 += 4) {
-                constexpr int G = 4;
-                float vl[G], full[G], dl[G], df[G];
-                uint32_t packed[G];
-                bool ok[G];
-#pragma unroll
-                for (int g = 0; g < G; g++) {
-                    const int i = i0 + g;
-                    const float4 qm = sq[min(j * kScN + 8 * cg + i, nq - 1)];
-                    const float scale = __int_as_float((ue + __float_as_int(qm.w) - 35 + 127) << 23);
-                    vl[g] = sl[i] * scale;
-                    const float ee = um.x * qm.x;
-                    dl[g] = fmaf(cl_u, qm.y, fmaf(fabsf(vl[g]), 1.8e-7f, ee * a.kl));
-                    const float vr = sr[i] * scale;
-                    const float dr = fmaf(cr_u, qm.z, fmaf(fabsf(vr), 1.8e-7f, ee * a.kr));
-                    full[g] = a.two_parts ? __fadd_rn(vl[g], vr) : vl[g];
-                    df[g] = fmaf(fabsf(full[g]), 2.4e-7f, (dl[g] + dr) * 1.0001f);
-                    ok[g] = true;
-                    packed[g] = 0;
-                }
-                if (a.lv) {
+                for (int i0 = 0; i0 < 8; i0 += 4) {
+                    constexpr int G = 4;
+                    float vl[G], full[G], dl[G], df[G];
+                    int packed[G];
+                    bool ok[G];
 #pragma unroll
                     for (int g = 0; g < G; g++) {
-                        const float right = __fmul_rn(un, sqn[min(j * kScN + 8 * cg + i0 + g, nq - 1)]);
-                        const float qlb = __fsub_rn(vl[g], right), qub = __fadd_rn(vl[g], right);
-                        const float dq = dl[g] * 1.0001f;
-                        int l, h;
-                        const bool okl = level_side(r, margin0, cu, S, qlb, fmaf(fabsf(qlb), 2.4e-7f, dq), false, tab, tab2, l);
-                        const bool oku = level_side(r, margin0, cu, S, qub, fmaf(fabsf(qub), 2.4e-7f, dq), true, tab, tab2, h);
-                        ok[g] = okl && oku;
-                        packed[g] = (uint32_t) l | ((uint32_t) h << 16);
+                        const int i = i0 + g;
+                        const float4 qm = sq[min(j * kScN + 8 * cg + i, nq - 1)];
+                        const float scale = __int_as_float((ue + __float_as_int(qm.w) - 35 + 127) << 23);
+                        vl[g] = sl[i] * scale;
+                        const float ee = um.x * qm.x;
+                        dl[g] = fmaf(cl_u, qm.y, fmaf(fabsf(vl[g]), 1.8e-7f, ee * a.kl));
+                        const float vr = sr[i] * scale;
+                        const float dr = fmaf(cr_u, qm.z, fmaf(fabsf(vr), 1.8e-7f, ee * a.kr));
+                        full[g] = a.two_parts ? __fadd_rn(vl[g], vr) : vl[g];
+                        df[g] = fmaf(fabsf(full[g]), 2.4e-7f, (dl[g] + dr) * 1.0001f);
+                        ok[g] = true;
+                        packed[g] = 0;
+                    }
+                    if (lev) {
+                        // coarse levels of the bounds partial -+ right (PartDimPartNorm::IPBound) from the
+                        // tables; within dq of the reference's bound scores: the partial score's bound and
+                        // the two roundings of each side
+#pragma unroll
+                        for (int g = 0; g < G; g++) {
+                            const float right = __fmul_rn(un, sqn[min(j * kScN + 8 * cg + i0 + g, nq - 1)]);
+                            const float qlb = __fsub_rn(vl[g], right), qub = __fadd_rn(vl[g], right);
+                            const float dq = dl[g] * 1.0001f;
+                            const float dql = fmaf(fabsf(qlb), 2.4e-7f, dq), dqu = fmaf(fabsf(qub), 2.4e-7f, dq);
+                            int c_l = kLvEntries - 1, c_u = 0;
+                            bool okl = __fadd_ru(qlb, dql) < lo_last, oku = __fsub_rd(qub, dqu) >= hi_first;
+                            if (!okl) okl = lvt_screen(tl, kScM, qlb, dql, c_l);
+                            if (!oku) oku = lvt_screen(tu, kScM, qub, dqu, c_u);
+                            ok[g] = okl && oku;
+                            packed[g] = c_l | (c_u << 4);
+                        }
+                    }
+                    // coarse group: the summary entries >= full (a five-step search and one compare)
+                    int lo[G];
+#pragma unroll
+                    for (int g = 0; g < G; g++) {
+                        lo[g] = s15 >= full[g] ? 16 : 0;
+                        lo[g] += (lo[g] ? s23 : s7) >= full[g] ? 8 : 0;
+                    }
+#pragma unroll
+                    for (int st = 4; st >= 1; st >>= 1)
+#pragma unroll
+                        for (int g = 0; g < G; g++) lo[g] += srow[(lo[g] + st - 1) * kScSummStride] >= full[g] ? st : 0;
+#pragma unroll
+                    for (int g = 0; g < G; g++) {
+                        lo[g] += srow[lo[g] * kScSummStride] >= full[g];
+                        const bool gok = (lo[g] == 0 || srow[(lo[g] - 1) * kScSummStride] >= full[g] + df[g]) &&
+                                         (lo[g] >= ThrSummary::kMaxGroups || srow[lo[g] * kScSummStride] < full[g] - df[g]) &&
+                                         df[g] < 1e30f && full[g] == full[g];
+                        ok[g] = ok[g] && gok;
+                    }
+                    // every pair is stored (the exact pass rewrites the undecided ones); decided pairs are
+                    // counted by coarse level, except the two implicit bins
+#pragma unroll
+                    for (int g = 0; g < G; g++) {
+                        const int qi = 8 * cg + i0 + g, q = j * kScN + qi;
+                        if (!uval || q >= nq) continue;
+                        const int64_t o = (int64_t) q * a.n_user + u;
+                        if (lev) {
+                            a.lvc[o] = (uint8_t) packed[g];
+                            if (ok[g]) {
+                                const int c_l = packed[g] & 15, c_u = packed[g] >> 4;
+                                uint32_t *hq = hb + qi * 2 * (kLvEntries / 4);
+                                if (c_l != kLvEntries - 1) hist_add(hq, c_l, 1u);
+                                if (c_u != 0) hist_add(hq + kLvEntries / 4, c_u, 1u);
+                            }
+                        }
+                        a.code[o] = (uint8_t) min(lo[g], a.nb);
+                        if (a.dump) a.dump[o] = make_float2(full[g], df[g]);
+                        und_bits |= (uint32_t) !ok[g] << (i0 + g);
                     }
                 }
-                // coarse group: the summary entries >= full (a five-step search and one compare)
-                int lo[G];
+                // the chunk's undecided pairs into the list: one shared-memory atomic per warp
+                const int cnt = __popc(und_bits);
+                int incl = cnt;
 #pragma unroll
-                for (int g = 0; g < G; g++) {
-                    lo[g] = s15 >= full[g] ? 16 : 0;
-                    lo[g] += (lo[g] ? s23 : s7) >= full[g] ? 8 : 0;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
                 }
-#pragma unroll
-                for (int st = 4; st >= 1; st >>= 1)
-#pragma unroll
-                    for (int g = 0; g < G; g++) lo[g] += srow[(lo[g] + st - 1) * kScSummStride] >= full[g] ? st : 0;
-#pragma unroll
-                for (int g = 0; g < G; g++) {
-                    lo[g] += srow[lo[g] * kScSummStride] >= full[g];
-                    const bool gok = (lo[g] == 0 || srow[(lo[g] - 1) * kScSummStride] >= full[g] + df[g]) &&
-                                     (lo[g] >= ThrSummary::kMaxGroups || srow[lo[g] * kScSummStride] < full[g] - df[g]) &&
-                                     df[g] < 1e30f && full[g] == full[g];
-                    ok[g] = ok[g] && gok;
-                }
-                // every pair is stored; the exact pass rewrites the undecided ones
-#pragma unroll
-                for (int g = 0; g < G; g++) {
-                    const int q = j * kScN + 8 * cg + i0 + g;
-                    if (!uval || q >= nq) continue;
-                    const int64_t o = (int64_t) q * a.n_user + u;
-                    if (a.lv) a.lv[o] = ok[g] ? packed[g] : 0u;  // a placeholder in range until rewritten
-                    a.code[o] = (uint8_t) min(lo[g], a.nb);
-                    a.qip[o] = full[g];
-                    und_bits |= (uint32_t) !ok[g] << (i0 + g);
-                }
-            }
-            // the chunk's undecided pairs into the list: one shared-memory atomic per warp
-            const int cnt = __popc(und_bits);
-            int incl = cnt;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += y;
-            }
-            const int tot = __shfl_sync(0xffffffffu, incl, 31);
-            if (tot) {
-                int base = 0;
-                if (lane == 31) base = atomicAdd(&list_n, tot);
-                base = __shfl_sync(0xffffffffu, base, 31);
-                int slot = base + incl - cnt;
-                n_und += cnt;
-                for (uint32_t m = und_bits; m; m &= m - 1, slot++) {
-                    const int q = j * kScN + 8 * cg + __ffs(m) - 1;
-                    if (slot < kScListCap) {
-                        list[slot] = (uint32_t) q | ((uint32_t) row << 16);
-                    } else {
-                        const int go = atomicAdd(a.spill_count, 1);
-                        if (go < a.spill_cap) a.spill[go] = make_int2(a.q_base + q, (int) u);
-                        else atomicExch(a.status, 2);
+                const int tot = __shfl_sync(0xffffffffu, incl, 31);
+                if (tot) {
+                    int base = 0;
+                    if (lane == 31) base = atomicAdd(&list_n, tot);
+                    base = __shfl_sync(0xffffffffu, base, 31);
+                    int slot = base + incl - cnt;
+                    n_und += cnt;
+                    for (uint32_t m = und_bits; m; m &= m - 1, slot++) {
+                        const int q = j * kScN + 8 * cg + __ffs(m) - 1;
+                        if (slot < kScListCap) {
+                            list[slot] = (uint32_t) q | ((uint32_t) row << 16);
+                        } else {
+                            const int go = atomicAdd(a.spill_count, 1);
+                            if (go < a.spill_cap) a.spill[go] = make_int2(a.q_base + q, (int) u);
+                            else atomicExch(a.status, 2);
+                        }
                     }
+                }
+            }
+            // every epilogue warp has counted this chunk: its histogram goes to the batch's (nonzero
+            // counters only) and is cleared for the chunk after next; every warp passes the same
+            // barriers, whether or not it gave up waiting
+            asm volatile("bar.sync 1, %0;" ::"n"(32 * kScEpiWarps) : "memory");
+            if (lev && tid < kScN * 2 * (kLvEntries / 4)) {
+                const uint32_t w = hb[tid];
+                if (w) {
+                    const int qi = tid / (2 * (kLvEntries / 4)), side = (tid / (kLvEntries / 4)) & 1;
+                    const int q = j * kScN + qi;
+                    int *gq = a.lhist + ((int64_t) q * 2 + side) * kLvEntries + 4 * (tid & (kLvEntries / 4 - 1));
+#pragma unroll
+                    for (int k = 0; k < 4; k++) {
+                        const uint32_t n = (w >> (8 * k)) & 0xffu;
+                        if (n && q < nq) atomicAdd(gq + k, (int) n);
+                    }
+                    hb[tid] = 0u;
                 }
             }
         }
@@ -546,30 +552,11 @@ __global__ void __launch_bounds__(256, 2) scores_tc_spill_kernel(ScArgs a) {
     }
 }
 
-// The regression CDF table (see level_side): per cell the value at the node, the first difference,
-// and half the second difference.
-void cdf_table_host(float2 *out, float *out2) {
-    auto phi = [](double z) {
-        const double a1 = 0.254829592, a2 = -0.284496736, a3 = 1.421413741;
-        const double a4 = -1.453152027, a5 = 1.061405429, p = 0.3275911;
-        const double sign = z < 0 ? -1.0 : 1.0;
-        const double x = std::fabs(z) / std::sqrt(2.0);
-        const double t = 1.0 / (1.0 + p * x);
-        const double y = 1.0 - (((((a5 * t + a4) * t) + a3) * t + a2) * t + a1) * t * std::exp(-x * x);
-        return 0.5 * (1.0 + sign * y);
-    };
-    for (int i = 0; i < kCdfTabCells; i++) {
-        const double z0 = -8.0 + i / 128.0;
-        const double v0 = phi(z0), v1 = phi(z0 + 1.0 / 128.0), v2 = phi(z0 + 2.0 / 128.0);
-        out[i] = make_float2((float) v0, (float) (v1 - v0));
-        out2[i] = (float) (0.5 * (v2 - 2.0 * v1 + v0));
-    }
-}
-
 }  // namespace
 
-int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, PairScreen *screen, bool *done) {
+int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, bool *done) {
     *done = false;
+    if (call.status) call.status[0] = nullptr;
     if (!ix->scores_tc_on) return RKR_OK;
     const int dim = ix->dim, nq = call.nq;
     const int c = call.qsrp ? ix->check_dim : dim;
@@ -577,9 +564,15 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, PairScre
     if (n1 <= 0 || n1 > kScMaxPart || n2 > kScMaxPart || nq <= 0) return RKR_OK;
     const int cp = round32(n1), kp = cp + round32(n2);
     if (kp > kScMaxKp) return RKR_OK;
+    if (call.qsrp && !ix->lvt.p) return RKR_OK;
     const int64_t U = ix->n_user;
     const int64_t n_tiles = (U + kScM - 1) / kScM;
     if (n_tiles > 0x7fffffff) return RKR_OK;
+    const size_t smem = (size_t) kScSlices * kp * (kScM + 2 * kScN) + sizeof(float) * ThrSummary::kMaxGroups * kScM +
+                        sizeof(uint32_t) * kScListCap + (sizeof(float4) + sizeof(float)) * kScMaxQ +
+                        sizeof(uint32_t) * 2 * kScN * 2 * (kLvEntries / 4) +
+                        (call.qsrp ? sizeof(float2) * 2 * kLvEntries * kScM : 0);
+    if (smem + 1024 > 227 * 1024) return RKR_OK;
     // user digits for this split (built once per split and kept)
     DevBuf &ub = call.qsrp ? ix->sc_user_split : ix->sc_user_full;
     DevBuf &um = call.qsrp ? ix->sc_umeta_split : ix->sc_umeta_full;
@@ -600,13 +593,10 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, PairScre
     const int64_t nq_pad = (int64_t) nchunks * kScN;
     const int ovf_cap = (int) std::min<int64_t>(int64_t(1) << 24, std::max<int64_t>(int64_t(1) << 16, U * nq / 32));
     const size_t b_total = (size_t) nq_pad * kScSlices * kp;
-    const int64_t words = (U + 31) / 32;
-    const size_t xbytes = sizeof(uint32_t) * (size_t) words * nq;
     const int n_launch = (nq + kScMaxQ - 1) / kScMaxQ;
     const int spill_cap = 1 << 20;
     const size_t need = b_total + 256 + sizeof(float4) * (size_t) nq_pad + 256 + sizeof(int2) * (size_t) ovf_cap + 256 +
-                        sizeof(int2) * ((size_t) n_launch * n_tiles + spill_cap) + 512 +
-                        xbytes + 256 + 64;
+                        sizeof(int2) * ((size_t) n_launch * n_tiles + spill_cap) + 512 + 64;
     RKR_TRY(ix->ws_sc.ensure(need));
     uint8_t *p = ix->ws_sc.as<uint8_t>();
     auto take = [&](size_t bytes) {
@@ -619,10 +609,14 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, PairScre
     int2 *ovf = reinterpret_cast<int2 *>(take(sizeof(int2) * (size_t) ovf_cap));
     int2 *tile_rng = reinterpret_cast<int2 *>(take(sizeof(int2) * (size_t) n_launch * n_tiles));
     int2 *spill = reinterpret_cast<int2 *>(take(sizeof(int2) * (size_t) spill_cap));
-    uint32_t *xbits = reinterpret_cast<uint32_t *>(take(xbytes));
-    int *counters = reinterpret_cast<int *>(take(64));  // ovf_count, status, undecided, recomputed scores, spill
+    int *counters = reinterpret_cast<int *>(take(64));  // ovf_count, status, undecided, (unused), spill
     RKR_CUDA(cudaMemsetAsync(counters, 0, 5 * sizeof(int), st));
-    RKR_CUDA(cudaMemsetAsync(xbits, 0, xbytes, st));
+    if (call.status) {
+        // the caller reads the status and the undecided count later (the launches stay free of host
+        // synchronisation, so that they can be captured in a graph)
+        call.status[0] = counters + 1;
+        call.status[1] = counters + 2;
+    }
     {
         const unsigned g = (unsigned) ((nq_pad * 32 + 255) / 256);
         timed(ix, st, "scores_tc_prep", [&] {
@@ -641,10 +635,13 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, PairScre
     a.qrow = call.qrows;
     a.thr_summ = ix->thr_summ.as<float>();
     a.m = call.m;
-    a.lv = call.lv;
+    a.lvt = call.qsrp ? ix->lvt.as<float2>() : nullptr;
+    a.G = call.qsrp ? lvt_stride(call.m.S) : 1;
+    a.lvc = call.lvc;
     a.code = call.code;
-    a.qip = call.qip;
-    a.xbits = xbits;
+    a.lhist = call.lhist;
+    a.anomaly = call.anomaly;
+    a.dump = ix->score_dump;
     a.ovf = ovf;
     a.ovf_count = counters;
     a.status = counters + 1;
@@ -664,22 +661,11 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, PairScre
     a.nb = call.nb;
     part_coef(n1, a.cl, a.kl);
     part_coef(n2, a.cr, a.kr);
-    if (call.qsrp && !ix->sc_cdf_tab.p) {
-        std::vector<float2> h(kCdfTabCells);
-        std::vector<float> h2(kCdfTabCells);
-        cdf_table_host(h.data(), h2.data());
-        RKR_TRY(ix->sc_cdf_tab.ensure((sizeof(float2) + sizeof(float)) * kCdfTabCells));
-        RKR_CUDA(cudaMemcpy(ix->sc_cdf_tab.p, h.data(), sizeof(float2) * kCdfTabCells, cudaMemcpyHostToDevice));
-        RKR_CUDA(cudaMemcpy(ix->sc_cdf_tab.as<uint8_t>() + sizeof(float2) * kCdfTabCells, h2.data(),
-                            sizeof(float) * kCdfTabCells, cudaMemcpyHostToDevice));
-    }
-    a.cdf_tab = ix->sc_cdf_tab.as<float2>();
-    a.cdf_tab2 = reinterpret_cast<const float *>(ix->sc_cdf_tab.as<uint8_t>() + sizeof(float2) * kCdfTabCells);
-    const size_t smem = (size_t) kScSlices * kp * (kScM + 2 * kScN) + sizeof(float) * ThrSummary::kMaxGroups * kScM +
-                        sizeof(uint32_t) * kScListCap + (sizeof(float2) + sizeof(float)) * kCdfTabCells +
-                        (sizeof(float4) + sizeof(float)) * kScMaxQ;
-    if (smem + 1024 > 227 * 1024) return RKR_OK;
-    RKR_CUDA(cudaFuncSetAttribute(scores_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    // function attributes are set outside graph capture (the eager first run of a shape sets them)
+    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+    RKR_CUDA(cudaStreamIsCapturing(st, &capturing));
+    if (capturing == cudaStreamCaptureStatusNone)
+        RKR_CUDA(cudaFuncSetAttribute(scores_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     // launches of at most kScMaxQ queries (whole chunks): their data sits in shared memory
     for (int q0 = 0; q0 < nq; q0 += kScMaxQ) {
         ScArgs s = a;
@@ -689,38 +675,37 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, PairScre
         s.qmeta = qmeta + q0;
         s.qnorm = a.qnorm ? a.qnorm + q0 : nullptr;
         s.qrow = a.qrow + (size_t) q0 * dim;
-        s.lv = a.lv ? a.lv + (size_t) q0 * U : nullptr;
+        s.lvc = a.lvc ? a.lvc + (size_t) q0 * U : nullptr;
         s.code = a.code + (size_t) q0 * U;
-        s.qip = a.qip + (size_t) q0 * U;
-        s.xbits = a.xbits + (size_t) q0 * words;
+        s.lhist = a.lhist ? a.lhist + (size_t) q0 * 2 * kLvEntries : nullptr;
+        s.anomaly = a.anomaly ? a.anomaly + q0 : nullptr;
+        s.dump = a.dump ? a.dump + (size_t) q0 * U : nullptr;
         s.tile_rng = tile_rng + (size_t) (q0 / kScMaxQ) * n_tiles;
         timed(ix, st, "qsrp_scores_tc", [&] { scores_tc_kernel<<<(unsigned) n_tiles, kScThreads, smem, st>>>(s); });
         RKR_CUDA(cudaGetLastError());
     }
     a.tile_rng = tile_rng;
     const size_t rows_smem = sizeof(float) * kScM * (size_t) dim;
-    RKR_CUDA(cudaFuncSetAttribute(scores_tc_exact_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int) rows_smem));
+    if (capturing == cudaStreamCaptureStatusNone)
+        RKR_CUDA(cudaFuncSetAttribute(scores_tc_exact_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int) rows_smem));
     timed(ix, st, "qsrp_scores_tc_exact", [&] {
         scores_tc_exact_tile_kernel<<<dim3((unsigned) n_tiles, (unsigned) n_launch), 256, rows_smem, st>>>(a, (int) n_tiles);
     });
     RKR_CUDA(cudaGetLastError());
     timed(ix, st, "qsrp_scores_tc_spill", [&] { scores_tc_spill_kernel<<<148 * 4, 256, 0, st>>>(a); });
     RKR_CUDA(cudaGetLastError());
+    *done = true;
+    if (call.status) return RKR_OK;
     int h[3] = {0, 0, 0};
     RKR_CUDA(cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, st));
     RKR_CUDA(cudaStreamSynchronize(st));
     if (ix->prof.on) ix->prof.add_count("screen_undecided_pairs", h[2]);
-    if (h[1]) return RKR_OK;  // a wait gave up or the overflow list filled: the exact tiles redo the chunk
-    screen->umeta = a.umeta;
-    screen->qmeta = qmeta;
-    screen->cl = a.cl;
-    screen->kl = a.kl;
-    screen->cr = a.cr;
-    screen->kr = a.kr;
-    screen->xbits = xbits;
-    screen->n_exact = counters + 3;
-    *done = true;
+    if (h[1]) {
+        // a wait gave up or the overflow list filled: the exact tiles redo the batch from clean counts
+        set_error("scores_tc: status %d", h[1]);
+        *done = false;
+    }
     return RKR_OK;
 }
 

@@ -38,6 +38,8 @@ EXPORTS = [
     "rkr_score_sort_batch", "rkr_index_query_rank_distribution", "rkr_normalize", "rkr_sample_item",
     "rkr_sort_kth_rank", "rkr_find_optimal_sample_rank", "rkr_uniform_sample_rank", "rkr_fit_regression",
     "rkr_svd_build", "rkr_profile_enable", "rkr_profile_read", "rkr_build_thresholds_static",
+    "rkr_index_level_tables", "rkr_query", "rkr_query_device", "rkr_server_create", "rkr_server_submit",
+    "rkr_server_wait", "rkr_server_counters", "rkr_server_destroy", "rkr_score_estimates",
 ]
 
 
@@ -217,6 +219,22 @@ class Index:
     def reset_state(self):
         _check(_lib.rkr_index_reset_state(self._h))
 
+    def score_estimates(self, method, query):
+        """The tensor-core pair scores' estimates and bounds (rkr_score_estimates): [n_query][n_user][2]."""
+        m = METHODS[method] if isinstance(method, str) else int(method)
+        q = _f32(query)
+        out = np.empty((q.shape[0], self.n_user, 2), np.float32)
+        _check(_lib.rkr_score_estimates(self._h, C.c_int32(m), _p(q), C.c_int32(q.shape[0]), _p(out)))
+        return out
+
+    def level_tables(self):
+        """The regression models' level-boundary tables (rkr_index_level_tables): (stride G, array
+        [n_user][2][16][2] of (boundary score, guard band))."""
+        g = C.c_int32()
+        out = np.empty((self.n_user, 2, 16, 2), np.float32)
+        _check(_lib.rkr_index_level_tables(self._h, C.byref(g), _p(out)))
+        return g.value, out
+
     def size_bytes(self):
         v = C.c_uint64()
         _check(_lib.rkr_index_size_bytes(self._h, C.byref(v)))
@@ -235,6 +253,34 @@ class Index:
                                   C.byref(na)))
         n = na.value
         return (out[:n], st[:n]) if stats else out[:n]
+
+    def query(self, method, query, k_per_q, stats=False):
+        """Retrieval with a top-k per query (rkr_query): a list of [k_i] USER_RANK arrays, one per
+        answered query (and the QUERY_STATS per query)."""
+        m = METHODS[method] if isinstance(method, str) else int(method)
+        q = _f32(query)
+        ks = _i32(k_per_q)
+        if ks.shape[0] != q.shape[0]:
+            raise ValueError("one k per query")
+        out = np.zeros(int(ks.sum()), USER_RANK)
+        st = np.zeros(max(q.shape[0], 1), QUERY_STATS) if stats else None
+        na = C.c_int32()
+        _check(_lib.rkr_query(self._h, C.c_int32(m), _p(q), C.c_int32(q.shape[0]), _p(ks), _p(out), _p(st),
+                              C.byref(na)))
+        n = na.value
+        off = np.concatenate([[0], np.cumsum(ks[:n])])
+        rows = [out[off[i]:off[i + 1]] for i in range(n)]
+        return (rows, st[:n]) if stats else rows
+
+    def query_device(self, method, d_query, n_query, k_per_q, d_out, d_stats=None, stream=None):
+        """Same with device pointers (ints) for queries and outputs; k_per_q a host array."""
+        m = METHODS[method] if isinstance(method, str) else int(method)
+        ks = _i32(k_per_q)
+        na = C.c_int32()
+        _check(_lib.rkr_query_device(self._h, C.c_int32(m), C.c_void_p(d_query), C.c_int32(n_query), _p(ks),
+                                     C.c_void_p(d_out), C.c_void_p(d_stats or 0), C.byref(na),
+                                     C.c_void_p(stream or 0)))
+        return na.value
 
     def retrieval_device(self, method, d_query, n_query, topk, d_out, d_stats=None, stream=None):
         """Same with device pointers (ints): queries [n_query][dim] f32, out [n][topk] USER_RANK."""
@@ -272,3 +318,71 @@ class Index:
         out = np.empty((si.shape[0], self.n_item + 1), np.int32)
         _check(_lib.rkr_index_query_rank_distribution(self._h, _p(si), C.c_int32(si.shape[0]), _p(out)))
         return out
+
+
+# ---- serving ----------------------------------------------------------------------------------------------
+
+class _ServerConfig(C.Structure):
+    _fields_ = [("method", C.c_int32), ("max_batch_queries", C.c_int32), ("n_workers", C.c_int32),
+                ("reserved", C.c_int32), ("workspace_bytes", C.c_int64)]
+
+
+class Server:
+    """A persistent serving loop over a resident Index (rkr_server_*): submit() queues a request of
+    query items with a top-k per item and returns a ticket; wait(ticket) returns its rows as
+    Index.query would for the request alone on a fresh index."""
+
+    def __init__(self, index, method="QSRPNormalLP", max_batch_queries=1024, n_workers=2, workspace_bytes=0):
+        self.index = index
+        cfg = _ServerConfig(METHODS[method] if isinstance(method, str) else int(method), int(max_batch_queries),
+                            int(n_workers), 0, int(workspace_bytes))
+        h = C.c_void_p()
+        _check(_lib.rkr_server_create(index.handle, C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._k = {}
+
+    def submit(self, query, k_per_q):
+        q = _f32(query)
+        ks = _i32(k_per_q)
+        if q.ndim != 2 or ks.shape[0] != q.shape[0]:
+            raise ValueError("query [n][dim] and one k per query item")
+        t = C.c_uint64()
+        _check(_lib.rkr_server_submit(self._h, _p(q), C.c_int32(q.shape[0]), _p(ks), C.byref(t)))
+        self._k[t.value] = ks
+        return t.value
+
+    def wait(self, ticket, timeout=-1.0, stats=False):
+        """(rows, latency {done, start} in seconds[, stats]): rows a list of [k_i] USER_RANK arrays."""
+        ks = self._k.pop(ticket)
+        out = np.zeros(int(ks.sum()), USER_RANK)
+        st = np.zeros(ks.shape[0], QUERY_STATS)
+        lat = np.zeros(2, np.float64)
+        _check(_lib.rkr_server_wait(self._h, C.c_uint64(ticket), C.c_double(timeout), _p(out), _p(st), _p(lat)))
+        off = np.concatenate([[0], np.cumsum(ks)])
+        rows = [out[off[i]:off[i + 1]] for i in range(ks.shape[0])]
+        lat = {"done": float(lat[0]), "start": float(lat[1])}
+        return (rows, lat, st) if stats else (rows, lat)
+
+    def counters(self):
+        v = [C.c_int64() for _ in range(4)]
+        busy = C.c_double()
+        _check(_lib.rkr_server_counters(self._h, *[C.byref(x) for x in v], C.byref(busy)))
+        return {"batches": v[0].value, "requests": v[1].value, "queries": v[2].value, "padded": v[3].value,
+                "busy_s": busy.value}
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            _lib.rkr_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

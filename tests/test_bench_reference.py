@@ -74,3 +74,19 @@ def test_reference_arm_stage_outputs_match_the_reference_build(monkeypatch):
     mine = np.stack([np.cumsum(np.bincount(ranks[:, j], minlength=2501)) for j in range(150)])
     assert np.abs(mine - accu).max() <= 2
     assert set(stages) >= {"query_rank_distribution", "thresholds", "regression_fit", "svd"}
+
+
+def test_bench_sequential_binary32_sum_is_the_reference_inner_product():
+    """The bench's score-error report compares the tensor-core estimates with the reference's
+    InnerProduct restated in numpy (seq_dot32); it equals the oracle's, bit for bit."""
+    sys.path.insert(0, ROOT)
+    import bench
+    from checkers import Oracle
+    orc = Oracle()
+    rng = np.random.default_rng(8)
+    a = rng.standard_normal((7, 150)).astype(np.float32)
+    b = (rng.standard_normal((5, 150)) * 3).astype(np.float32)
+    got = bench.seq_dot32(a, b)
+    for i in range(7):
+        for j in range(5):
+            assert np.float32(orc.inner_product(a[i], b[j])).view(np.int32) == got[i, j].view(np.int32)

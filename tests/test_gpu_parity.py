@@ -188,3 +188,49 @@ def test_edge_cases(orc):
         ref, _ = orc.qs_retrieval(g["user_norm"], g["item"], int(g["check_dim"]), g["opt_rank"], g["thr"],
                                   g["query"][:1], 1)
         assert same(one, ref)
+
+
+@pytest.mark.parametrize("compact", ["sparse", "two_pass"])
+def test_mixed_k_batch_equals_one_call_per_query(orc, compact, monkeypatch):
+    """rkr_query with a top-k per query: every query's entries equal the oracle's for that query
+    alone with its k, called in order on the same index, so that QSRPNormalLP's carried scores
+    advance exactly as across the reference's consecutive Retrieval calls."""
+    monkeypatch.setenv("RKR_COMPACT_SPARSE", "1" if compact == "sparse" else "0")
+    user, item, query = random_case(97, 1500, 2200, 48, 80)
+    un = orc.normalize(user)
+    rank = np.unique(np.concatenate([np.arange(0, 30), np.linspace(30, 2100, 50).astype(int)])).astype(np.int32)
+    thr = orc.build_thresholds(un, item, rank)
+    reg = orc.fit_regression(thr)
+    ti, su, cd = rkr_b200.svd_build(un, 0.7)
+    ks = np.random.default_rng(3).integers(1, 120, query.shape[0]).astype(np.int32)
+    ks[:3] = (1, 1500, 4)
+    with rkr_b200.Index(un, item) as ix:
+        ix.load_sample_search(rank, thr)
+        ix.load_svd(cd, ti, su)
+        ix.load_regression(rank, reg)
+        for method in ("QS", "QSRPNormalLP"):
+            ix.reset_state()
+            rows, st = ix.query(method, query, ks, stats=True)
+            assert len(rows) == query.shape[0]
+            state = np.zeros(un.shape[0], np.float32)
+            for i, k in enumerate(ks):
+                if method == "QS":
+                    want, ws = orc.qs_retrieval(un, item, cd, rank, thr, query[i:i + 1], int(k))
+                else:
+                    want, ws = orc.qsrp_retrieval(un, su, ti, item, cd, rank, thr, rank, reg, query[i:i + 1], int(k),
+                                                  qip_state=state)
+                assert same(rows[i], want[0]), (method, i, int(k))
+                for f in ("n_prune", "n_result", "n_refine", "ip_cost"):
+                    assert st[f][i] == ws[f][0], (method, i, f)
+        # US answers the first 100 queries per call
+        q100 = np.concatenate([query, query])[:100]
+        k100 = np.concatenate([ks, ks])[:100]
+        with rkr_b200.Index(un, item) as ix2:
+            ix2.load_sample_search(rank, thr)
+            rows = ix2.query("US", q100, k100)
+            assert len(rows) == 100
+            for k in (int(k100[0]), int(k100[7])):
+                want, _ = orc.us_retrieval(un, item, rank, thr, q100, k)
+                for i in range(100):
+                    if int(k100[i]) == k:
+                        assert same(rows[i], want[i])

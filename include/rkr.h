@@ -95,14 +95,18 @@ int rkr_index_reset_state(rkr_index *index);
 /* The regression models' level-boundary tables, built on the device when the models are loaded:
  * per user and side (0: the lower rank bound as a function of qlb, 1: the upper bound of qub) 16
  * entries (T_g, band_g), T_g the smallest binary32 score whose ComputeRankBound level
- * (NormalLinearRegressionLP.hpp:326-398; 0 -> rank 0, j + 1 -> rank[j], S + 1 -> n_item) is <= g *
- * stride, band_g the half-width around T_g outside which the reference's binary32 arithmetic is
- * guaranteed to agree with the table.  tables_out: host [n_user][2][16][2] floats; *stride_out the
- * level stride.  A diagnostic view of what the query kernels use (no counterpart in the reference). */
-int rkr_index_level_tables(rkr_index *index, int32_t *stride_out, float *tables_out);
+ * (NormalLinearRegressionLP.hpp:326-398; 0 -> rank 0, j + 1 -> rank[j], S + 1 -> n_item) is <= L_g,
+ * band_g the half-width around T_g outside which the reference's binary32 arithmetic is guaranteed
+ * to agree with the table.  levels_out: host [16], the levels L_g (0, then 14 steps to S, then
+ * S + 1); tables_out: host [n_user][2][16][2] floats.  A diagnostic view of what the query kernels
+ * use (no counterpart in the reference). */
+int rkr_index_level_tables(rkr_index *index, int32_t *levels_out, float *tables_out);
 
 /* Device bytes held by the index (BaseIndex::IndexSizeByte counterpart, src/include/struct/MethodBase.hpp:23). */
 int rkr_index_size_bytes(const rkr_index *index, uint64_t *bytes);
+
+/* The index's user and item counts and dimension (any may be NULL). */
+int rkr_index_shape(const rkr_index *index, int64_t *n_user, int64_t *n_item, int32_t *dim);
 
 /* Builds the thresholds for `sample_rank` on the device from the resident users and items and
  * keeps them as the index's SampleSearch table (what bsibc computes,
@@ -266,6 +270,64 @@ int rkr_fit_regression(const float *thresholds, int64_t n_user, int32_t n_sample
  * the transformed users and check_dim for the given sigma ratio. */
 int rkr_svd_build(const float *user, int64_t n_user, int32_t dim, float sigma, float *transfer_item_out,
                   float *svd_user_out, int32_t *check_dim_out);
+
+/* ---- index files --------------------------------------------------------------------------------- */
+
+/* The reference's on-disk index layouts, read and written byte for byte (native-endian size_t, int
+ * and float, no padding).  A missing, short or inconsistent file is RKR_ERR_IO; nothing here touches
+ * the GPU.  Each *_info call reads only the header, so that the caller can size the buffers of the
+ * matching read; output buffers may be NULL to skip a part. */
+
+/* SampleSearch::SaveIndex / LoadIndex (src/include/alg/RankBoundRefinement/SampleSearch.hpp:158-244):
+ * size_t n_sample, n_item, n_user; int rank[n_sample]; float thresholds[n_user][n_sample] (the
+ * memory_index form; the qrs_to_sample_index form that fsr writes ends after the ranks:
+ * *has_scores = 0, and writing with thresholds = NULL produces it). */
+int rkr_file_sample_search_info(const char *path, int32_t *n_sample, int64_t *n_item, int64_t *n_user,
+                                int32_t *has_scores);
+int rkr_file_read_sample_search(const char *path, int32_t *rank_out, float *thresholds_out);
+int rkr_file_write_sample_search(const char *path, const int32_t *rank, int32_t n_sample, int64_t n_item,
+                                 int64_t n_user, const float *thresholds);
+
+/* NormalLinearRegressionLP::SaveIndex / LoadIndex (src/include/alg/RegressionPruning/
+ * NormalLinearRegressionLP.hpp:419-487): size_t n_item, n_user; int n_sample; int rank[n_sample];
+ * float (a, b)[n_user], (mu, sigma)[n_user], err[n_user], (smax, smin)[n_user].  Records here are
+ * [n_user][7] = a, b, mu, sigma, err, smax, smin, as rkr_index_load_regression takes them. */
+int rkr_file_regression_info(const char *path, int32_t *n_sample, int64_t *n_item, int64_t *n_user);
+int rkr_file_read_regression(const char *path, int32_t *rank_out, float *records_out);
+int rkr_file_write_regression(const char *path, const int32_t *rank, int32_t n_sample, int64_t n_item,
+                              int64_t n_user, const float *records);
+
+/* SVD::SaveIndex / LoadIndex (src/include/alg/SVD.hpp:126-188): size_t n_user, n_item, dim; float
+ * sigma; int check_dim; float transfer_item[dim][dim], svd_user[n_user][dim], svd_item[n_item][dim]
+ * (svd_item = NULL on write: zeros, a part the query path never reads). */
+int rkr_file_svd_info(const char *path, int64_t *n_user, int64_t *n_item, int32_t *dim, float *sigma,
+                      int32_t *check_dim);
+int rkr_file_read_svd(const char *path, float *transfer_item, float *svd_user, float *svd_item);
+int rkr_file_write_svd(const char *path, int64_t n_user, int64_t n_item, int32_t dim, float sigma, int32_t check_dim,
+                       const float *transfer_item, const float *svd_user, const float *svd_item);
+
+/* The query-distribution directory (WriteDistributionBelowTopk, src/app/build-index/FileIO.hpp:57-137;
+ * read back as ReadQueryDistribution does, OptimalSampleRank.hpp:157-200): dir/sample_itemID_l.txt
+ * (the sampled item ids in sorted-sample order, one per line), dir/sort_kth_rank_l.index
+ * (int[n_sample_item]) and dir/accu_n_user_rank_l.index (the accu rows, [n_sample_item][n_item + 1]
+ * ints, in sorted-sample order).  The write takes what rkr_sample_item,
+ * rkr_index_query_rank_distribution and rkr_sort_kth_rank return (accu in sample order) and creates
+ * dir if needed; the read returns the file order. */
+int rkr_file_write_query_distribution(const char *dir, const int32_t *sample_item, const int32_t *sort_kth_rank,
+                                      const int32_t *sort_sample_id, const int32_t *accu, int32_t n_sample_item,
+                                      int64_t n_item);
+int rkr_file_read_query_distribution(const char *dir, int32_t n_sample_item, int64_t n_item, int32_t *sample_item_out,
+                                     int32_t *sort_kth_rank_out, int32_t *accu_out);
+
+/* Loads the file set the reference's factories read (QS::BuildIndex, src/impl/QS.hpp:259-288;
+ * QSRPNormalLP::BuildIndex, src/impl/QSRPNormalLP.hpp:289-323; US::BuildIndex, src/impl/US.hpp)
+ * from index_dir into the index: the SampleSearch index (memory_index/QS-<dataset>-n_sample_..
+ * -n_sample_query_..-sample_topk_...index, or memory_index/US-<dataset>-n_sample_...index for US),
+ * for QS the check_dim of svd_index/<dataset>.index, for QSRPNormalLP that SVD index and the
+ * regression index (memory_index/NormalLinearRegressionLP-QS-<dataset>-...index).  The files are
+ * memory-mapped and copied to the device from the maps; their user counts must match the index's. */
+int rkr_index_load_files(rkr_index *index, int32_t method, const char *index_dir, const char *dataset_name,
+                         int32_t n_sample, int32_t n_sample_query, int32_t sample_topk);
 
 #ifdef __cplusplus
 }

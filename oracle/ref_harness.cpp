@@ -307,6 +307,29 @@ int ref_regression_rank_bound(const char *work_dir, int64_t n_user, int64_t n_it
     return 0;
 }
 
+// bsibc / fsr: a SampleSearch index file written by SampleSearch::SaveIndex (SampleSearch.hpp:158-197)
+// under work_dir/memory_index, named as the reference names it.
+int ref_write_sample_search(const char *work_dir, const char *ds, const char *name, const int32_t *rank, int32_t S,
+                            const float *thr, int64_t n_user, int64_t n_item, int32_t nsq, int32_t stopk,
+                            int32_t is_query_distribution) {
+    ensure_index_dirs(work_dir);
+    write_sample_index(work_dir, ds, name, rank, S, thr, n_user, n_item, nsq, stopk, is_query_distribution != 0);
+    return 0;
+}
+
+// qdibc: the query-distribution directory written by WriteDistributionBelowTopk
+// (src/app/build-index/FileIO.hpp:57-137) under work_dir/query_distribution.
+int ref_write_query_distribution(const char *work_dir, const char *ds, const int32_t *sample_item,
+                                 const int32_t *sort_kth, const int32_t *sort_sid, const int32_t *accu, int64_t n_item,
+                                 int32_t n_sample_item, int32_t sample_topk) {
+    ensure_index_dirs(work_dir);
+    const size_t n = (size_t) n_sample_item;
+    std::vector<int> si(sample_item, sample_item + n), sk(sort_kth, sort_kth + n), sid(sort_sid, sort_sid + n);
+    std::vector<int> acc(accu, accu + n * (size_t) (n_item + 1));
+    WriteDistributionBelowTopk(si, sk, sid, acc, n_item, n_sample_item, sample_topk, ds, work_dir);
+    return 0;
+}
+
 // bsvdi: SVD(user, item, SIGMA) (SVD.hpp:62-124; the decomposition itself is the stand-in's).
 int ref_svd_build(const float *user, int64_t n_user, const float *item, int64_t n_item, int32_t d, float sigma,
                   float *transfer_item_out, float *svd_user_out, int32_t *check_dim_out) {

@@ -401,16 +401,16 @@ static float orc_fval(int64_t k) {
 
 /* Score boundaries of one user's rank bound, side 0 the lower bound (a function of qlb), side 1 the
  * upper bound (of qub): out[g] = the smallest binary32 score whose level (orc_rank_level of
- * ComputeRankBound, NormalLinearRegressionLP.hpp:326-380) is <= g * stride, g = 0 .. n_out - 1;
+ * ComputeRankBound, NormalLinearRegressionLP.hpp:326-380) is <= levels[g], g = 0 .. n_out - 1;
  * +inf where no finite score reaches it, -inf where every finite score does.  Bisection on the
  * ordered binary32 values; the level never rises with the score (tests/test_level_monotone.py), so
- * a score's level lies in (g_1 stride, g_0 stride] for the boundaries g_0, g_1 around it.  A checker
- * for level-boundary tables built on the device. */
-void orc_level_boundaries(const float *rec, const int32_t *sample_rank, int32_t n_sample, int64_t n_item,
-                          int32_t stride, int32_t side, int32_t n_out, float *out) {
+ * a score's level lies in (levels[g_1], levels[g_0]] for the boundaries g_0, g_1 around it.  A
+ * checker for level-boundary tables built on the device; the levels ascend. */
+void orc_level_boundaries_at(const float *rec, const int32_t *sample_rank, int32_t n_sample, int64_t n_item,
+                             const int32_t *levels, int32_t side, int32_t n_out, float *out) {
     const int64_t klo = orc_fkey(-INFINITY), khi = orc_fkey(INFINITY);
     for (int32_t g = 0; g < n_out; g++) {
-        const int32_t L = g * stride;
+        const int32_t L = levels[g];
         /* level(x) <= L is monotone in x: false ... false true ... true; find the first true */
         int64_t lo = klo, hi = khi;  /* invariant: level(fval(hi)) <= L or hi = khi */
         int32_t rl, ru;
@@ -430,6 +430,14 @@ void orc_level_boundaries(const float *rec, const int32_t *sample_rank, int32_t 
         }
         out[g] = orc_fval(hi);
     }
+}
+
+/* The same at the levels g * stride, g = 0 .. n_out - 1. */
+void orc_level_boundaries(const float *rec, const int32_t *sample_rank, int32_t n_sample, int64_t n_item,
+                          int32_t stride, int32_t side, int32_t n_out, float *out) {
+    int32_t levels[4096];
+    for (int32_t g = 0; g < n_out && g < 4096; g++) levels[g] = g * stride;
+    orc_level_boundaries_at(rec, sample_rank, n_sample, n_item, levels, side, n_out < 4096 ? n_out : 4096, out);
 }
 
 /* The LP optimum itself (min e s.t. |a x_i + b - y_i| <= e) comes from minimax_line.h.  The

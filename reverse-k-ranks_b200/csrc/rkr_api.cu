@@ -330,6 +330,14 @@ int rkr_index_reset_state(rkr_index *ix) {
     return RKR_OK;
 }
 
+int rkr_index_shape(const rkr_index *ix, int64_t *n_user, int64_t *n_item, int32_t *dim) {
+    RKR_REQUIRE(ix, "null index");
+    if (n_user) *n_user = ix->n_user;
+    if (n_item) *n_item = ix->n_item;
+    if (dim) *dim = ix->dim;
+    return RKR_OK;
+}
+
 int rkr_index_size_bytes(const rkr_index *ix, uint64_t *bytes) {
     RKR_REQUIRE(ix && bytes, "null argument");
     uint64_t s = 0;

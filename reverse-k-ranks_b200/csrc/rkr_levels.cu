@@ -4,8 +4,9 @@
 // bound scores into levels of NormalLinearRegressionLP::ComputeRankBound
 // (NormalLinearRegressionLP.hpp:326-398): lower side ceil(pred + err), upper side floor(pred - err),
 // pred = a CDFPhi((q - mu) / sigma) + b, with the extreme-score shortcuts at smax / smin.  For one
-// user and side that level is a non-increasing step function of the score, so the coarse level
-// ceil(level / G) of a score is the number of table boundaries above it.  The tables are built here
+// user and side that level is a non-increasing step function of the score, so the coarse level of a
+// score (which of the table's level intervals holds its level) is the number of table boundaries
+// above it.  The tables are built here
 // once per regression index, with the reference's own arithmetic (bisection over binary32 scores),
 // and each boundary carries a guard band that covers every score where the reference's binary32
 // evaluation could disagree with the exact-math model: where |v(q) - n| <= m, v the model's value
@@ -53,7 +54,7 @@ __device__ __forceinline__ double model_margin(float a, float b, float err) {
     return aa * 1.5e-6 + s * 6e-7 + 1e-6;
 }
 
-__global__ void level_table_kernel(const float *__restrict__ rec, int64_t n_user, int S, double err_cap, int G,
+__global__ void level_table_kernel(const float *__restrict__ rec, int64_t n_user, int S, double err_cap,
                                    float2 *__restrict__ tab) {
     const int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_user * 2 * kLvEntries) return;
@@ -67,7 +68,7 @@ __global__ void level_table_kernel(const float *__restrict__ rec, int64_t n_user
     const bool usable = isfinite(a) && isfinite(b) && isfinite(mu) && isfinite(sigma) && isfinite(err) &&
                         isfinite(smax) && isfinite(smin) && sigma > 0.0f && a < 0.0f && smin <= smax;
     float2 out;
-    const int lim = g * G;  // the entry's level value
+    const int lim = lvt_level(g, S);  // the entry's level value
     if (!usable) {
         out = make_float2(NAN, NAN);
     } else if (g == kLvEntries - 1 || lim >= S + 1) {
@@ -138,22 +139,22 @@ int level_tables_build(rkr_index *ix) {
     RKR_TRY(ix->lvt.ensure(sizeof(float2) * (size_t) n));
     const int S = ix->n_sample_reg;
     level_table_kernel<<<(unsigned) ((n + 127) / 128), 128, 0, ix->stream>>>(
-        ix->reg.as<float>(), ix->n_user, S, (double) S - 1e-3, lvt_stride(S), ix->lvt.as<float2>());
+        ix->reg.as<float>(), ix->n_user, S, (double) S - 1e-3, ix->lvt.as<float2>());
     RKR_CUDA(cudaGetLastError());
     return RKR_OK;
 }
 
 }  // namespace rkr
 
-extern "C" int rkr_index_level_tables(rkr_index *ix, int32_t *stride_out, float *tables_out) {
+extern "C" int rkr_index_level_tables(rkr_index *ix, int32_t *levels_out, float *tables_out) {
     using namespace rkr;
-    RKR_REQUIRE(ix && stride_out && tables_out, "null argument");
+    RKR_REQUIRE(ix && levels_out && tables_out, "null argument");
     if (ix->n_sample_reg <= 0 || !ix->lvt.p) {
         set_error("the index has no regression models");
         return RKR_ERR_STATE;
     }
     RKR_TRY(ensure_device(ix));
-    *stride_out = lvt_stride(ix->n_sample_reg);
+    for (int g = 0; g < kLvEntries; g++) levels_out[g] = lvt_level(g, ix->n_sample_reg);
     RKR_CUDA(cudaMemcpyAsync(tables_out, ix->lvt.p, sizeof(float2) * (size_t) ix->n_user * 2 * kLvEntries,
                              cudaMemcpyDeviceToHost, ix->stream));
     RKR_CUDA(cudaStreamSynchronize(ix->stream));

@@ -7,7 +7,7 @@
 //   2. full SVD-space score for the survivors (ComputeRemainDim, :76-95) -> sampled-threshold
 //      bounds (SampleSearch::RankBound) -> prune again.
 // Here a batch of queries runs as passes over all (query, user) pairs:
-//   * one kernel scores every pair and stores two bytes: the coarse levels ceil(level / G) of its
+//   * one kernel scores every pair and stores two bytes: the coarse levels (lvt_coarse) of its
 //     two round-1 bounds (the per-user level-boundary tables, rkr_levels.cu) and the coarse group of
 //     its sampled-threshold bucket (a per-user summary of every 16th threshold), and counts the
 //     coarse levels per query; on the tensor cores (rkr_scores_tc.cu: int8 digit products, a
@@ -63,17 +63,23 @@ struct QsrpParams {
     int32_t gneed_lo, gneed_hi, lv_m2, pad1;  // groups 0..31 / 32 the compaction must classify; L2's level
     int32_t cbl, cbu, cum_l, cum_u;        // round 1: critical coarse levels (-1: none needed), counts below
     int32_t amb_l, amb_u, res_fine, ple_fine;  // coarse levels straddling a class threshold; their counts
+    int32_t c_res, c_pr, c_m1, w_all;      // coarse-level thresholds of the classes (class1_coarse);
+    int32_t w_l, w_u, pad3, pad4;          // the coarse levels the next fine scan looks for (-1: none), or all
 };
 
-// Every level in coarse level c (levels ((c - 1) G, c G], or 0 for c = 0) is <= t / is > t.
-__device__ __forceinline__ bool coarse_all_le(int c, int t, int G) { return c == 0 ? t >= 0 : c * G <= t; }
-__device__ __forceinline__ bool coarse_all_gt(int c, int t, int G) { return c == 0 ? t < 0 : (c - 1) * G >= t; }
-// The coarse level of t whose levels straddle t (some <= t, some > t), or -1 when none does.
-__device__ __forceinline__ int coarse_straddle(int t, int G) {
-    if (t < 1) return -1;
-    const int c = (t + G - 1) / G;
-    return c * G == t ? -1 : c;
+// The lowest level of coarse level c (its levels are lvt_lo(c) .. lvt_level(c)).
+__device__ __forceinline__ int lvt_lo(int c, int S) { return c == 0 ? 0 : lvt_level(c - 1, S) + 1; }
+// Every level in coarse level c is <= t / is > t.
+__device__ __forceinline__ bool coarse_all_le(int c, int t, int S) { return lvt_level(c, S) <= t; }
+__device__ __forceinline__ bool coarse_all_gt(int c, int t, int S) { return lvt_lo(c, S) > t; }
+// The coarse level whose levels straddle t (some <= t, some > t), or -1 when none does.
+__device__ __forceinline__ int coarse_straddle(int t, int S) {
+    if (t < 0 || t > S) return -1;
+    const int c = lvt_coarse(t, S);
+    return lvt_level(c, S) == t ? -1 : c;
 }
+// A coarse level of more than one level (a selection inside it needs the exact levels), else -1.
+__device__ __forceinline__ int coarse_multi(int c, int S) { return lvt_level(c, S) > lvt_lo(c, S) ? c : -1; }
 
 // Round-1 class from exact levels: rank(level) is non-decreasing in the level, so lb <= U1 is
 // lvl_lb <= lv_res, L1 <= ub is lvl_ub >= lv_pr and the equal-bounds test is a test against lv_m1.
@@ -84,17 +90,30 @@ __device__ __forceinline__ int class1_lv(const QsrpParams &p, int l, int h) {
     return p.all1 ? kClsResult : kClsRefine;
 }
 
-// The same from a coarse-level byte that no threshold straddles (or that the fine pass settled).
-__device__ __forceinline__ int class1_coarse(const QsrpParams &p, unsigned v, int G) {
+// The same from a coarse-level byte that no threshold straddles (or that the fine pass settled):
+// c_res / c_m1 are the last coarse levels wholly <= lv_res / lv_m1, c_pr the first wholly >= lv_pr.
+__device__ __forceinline__ int class1_coarse(const QsrpParams &p, unsigned v) {
     if ((v & 15) == kLvcResolved) {
         const int k = (int) (v >> 4);
         return (k == kClsRefine && p.all1) ? kClsResult : k;
     }
     const int cl = (int) (v & 15), cu = (int) (v >> 4);
-    if (p.mode1) return (coarse_all_le(cu, p.lv_m1, G) && coarse_all_le(cl, p.lv_m1, G)) ? kClsResult : kClsIdle;
-    if (coarse_all_le(cl, p.lv_res, G)) return kClsResult;
-    if (coarse_all_gt(cu, p.lv_pr - 1, G)) return kClsPrune;
+    if (p.mode1) return (cu <= p.c_m1 && cl <= p.c_m1) ? kClsResult : kClsIdle;
+    if (cl <= p.c_res) return kClsResult;
+    if (cu >= p.c_pr) return kClsPrune;
     return p.all1 ? kClsResult : kClsRefine;
+}
+
+// The last coarse level wholly <= t (-1 if none) and the first wholly > t (kLvEntries if none).
+__device__ __forceinline__ int coarse_last_le(int t, int S) {
+    int c = -1;
+    while (c + 1 < kLvEntries && lvt_level(c + 1, S) <= t) c++;
+    return c;
+}
+__device__ __forceinline__ int coarse_first_gt(int t, int S) {
+    int c = 0;
+    while (c < kLvEntries && lvt_lo(c, S) <= t) c++;
+    return c;
 }
 
 // ---- round 1 + full scores -------------------------------------------------------------------------
@@ -177,10 +196,10 @@ struct FixList {
 };
 
 // One pair's exact levels into its coarse-level byte; the rank-order anomaly check.
-__device__ __forceinline__ uint8_t lvc_of_levels(uint32_t v, int G, const RegModel &m, int *anomaly_q) {
+__device__ __forceinline__ uint8_t lvc_of_levels(uint32_t v, const RegModel &m, int *anomaly_q) {
     const int l = (int) (v & 0xffffu), h = (int) (v >> 16);
     if (h > l && level_rank(h, m.rank, m.S, m.n_item) > level_rank(l, m.rank, m.S, m.n_item)) atomicAdd(anomaly_q, 1);
-    return (uint8_t) (lvt_coarse(l, G) | (lvt_coarse(h, G) << 4));
+    return (uint8_t) (lvt_coarse(l, m.S) | (lvt_coarse(h, m.S) << 4));
 }
 
 // Tiles of 128 users x 128 queries: the partial score over the first check_dim coordinates, the
@@ -192,7 +211,6 @@ struct Round1Epi {
     static constexpr int kSummStride = ThrSummary::kMaxGroups + 1;
     const float *unorm, *qnorm, *thr_summ;
     RegModel m;
-    int G;
     uint8_t *lvc;  // nullptr: no round 1 (QS, US)
     uint8_t *code;
     int *anomaly;
@@ -229,7 +247,7 @@ struct Round1Epi {
                 const float right = __fmul_rn(un, qn[rb]);
                 int l, h;
                 ok[g] = regression_levels_fast(r, m.S, __fsub_rn(left[g], right), __fadd_rn(left[g], right), l, h);
-                packed[g] = ok[g] ? lvc_of_levels((uint32_t) l | ((uint32_t) h << 16), G, m,
+                packed[g] = ok[g] ? lvc_of_levels((uint32_t) l | ((uint32_t) h << 16), m,
                                                   anomaly + b0 + half + 2 * min(i + g, nrow - 1))
                                   : kLvcUndecided;
             }
@@ -293,7 +311,7 @@ struct Round1Epi {
 };
 
 // The reference's arithmetic for the pairs the screen left undecided (the listed ones).
-__global__ void qsrp_fix1_kernel(FixList fix, RegModel m, int G, const float *__restrict__ unorm,
+__global__ void qsrp_fix1_kernel(FixList fix, RegModel m, const float *__restrict__ unorm,
                                  const float *__restrict__ qnorm, int64_t n_user, uint8_t *__restrict__ lvc,
                                  int *__restrict__ anomaly) {
     const int n = min(*fix.count, fix.cap);
@@ -303,20 +321,20 @@ __global__ void qsrp_fix1_kernel(FixList fix, RegModel m, int G, const float *__
         const float right = __fmul_rn(__ldg(unorm + e.y), __ldg(qnorm + e.x));
         const uint32_t v =
             regression_levels_exact(m.rec, m.S, m.err_cap, e.y, __fsub_rn(left, right), __fadd_rn(left, right));
-        lvc[(int64_t) e.x * n_user + e.y] = lvc_of_levels(v, G, m, anomaly + e.x);
+        lvc[(int64_t) e.x * n_user + e.y] = lvc_of_levels(v, m, anomaly + e.x);
     }
 }
 
 // Undecided pairs beyond the list's capacity: a scan of the batch's coarse-level bytes for
 // kLvcUndecided, with the partial score recomputed.  Returns at once when the list held them all.
-__global__ void qsrp_fix1_scan_kernel(const int *__restrict__ count, int cap, Round1Src src, int G, int64_t n_user,
+__global__ void qsrp_fix1_scan_kernel(const int *__restrict__ count, int cap, Round1Src src, int64_t n_user,
                                       int nq, uint8_t *__restrict__ lvc, int *__restrict__ anomaly) {
     if (*count <= cap) return;
     const int64_t n = n_user * nq;
     for (int64_t i = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t) gridDim.x * blockDim.x) {
         if (lvc[i] != kLvcUndecided) continue;
         const int64_t q = i / n_user, u = i % n_user;
-        lvc[i] = lvc_of_levels(src.levels(u, q), G, src.m, anomaly + q);
+        lvc[i] = lvc_of_levels(src.levels(u, q), src.m, anomaly + q);
     }
 }
 
@@ -377,8 +395,8 @@ __device__ __forceinline__ void coarse_counts(const int *__restrict__ h, int imp
 
 // Round-1 selection, coarse step (PruneCandidateByBound.hpp:36-77 with nothing excluded): the coarse
 // levels holding each side's k-th smallest level, and the users below them.  A critical coarse
-// level 0 (the upper side's level 0) is a single level and needs no fine step.
-__global__ void qsrp_select1c_kernel(const int *__restrict__ lhist, int64_t n_user, KSpec ks, int nq,
+// level of a single level (0 or S + 1, where most pairs sit) needs no fine step.
+__global__ void qsrp_select1c_kernel(const int *__restrict__ lhist, int64_t n_user, KSpec ks, int nq, int S,
                                      QsrpParams *__restrict__ par) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nq) return;
@@ -401,86 +419,150 @@ __global__ void qsrp_select1c_kernel(const int *__restrict__ lhist, int64_t n_us
         cum += hu[b];
     }
     p.cum_u = (int) cum;
-    if (p.cbu == 0) p.cbu = -1;  // level 0 exactly
+    p.w_l = coarse_multi(p.cbl, S);
+    p.w_u = coarse_multi(p.cbu, S);
     p.amb_l = -1;
     p.amb_u = -1;
     par[q] = p;
 }
 
-// Exact levels of the pairs in the coarse levels a query flags, one CTA per (user tile, query
-// group), one warp per query row of the tile.  mode 0: the critical coarse levels of the selection,
-// counted by exact level (fine histograms [query][2][G]).  mode 1: the pairs whose coarse level
+// Exact levels of the pairs in the coarse levels a query flags (QsrpParams::w_l / w_u / w_all).
+// mode 0: the critical coarse levels of the selection that span more than one level, counted by
+// exact level (fine histograms [query][2][W], W = lvt_width).  mode 1: the pairs whose coarse level
 // straddles a class threshold (every pair of a query whose class counts must be taken pair by pair),
-// settled to their exact round-1 class in place (lvc = class << 4) and counted.
-__global__ void __launch_bounds__(256) qsrp_fine1_kernel(uint8_t *__restrict__ lvc, Round1Src src, int64_t n_user,
-                                                        int nq, int G, int mode, QsrpParams *__restrict__ par,
-                                                        int *__restrict__ fhist, int *__restrict__ mismatch) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t u0 = (int64_t) blockIdx.x * 128;
-    for (int q = blockIdx.y * 8 + warp; q < nq; q += gridDim.y * 8) {
-        const QsrpParams &p = par[q];
-        int wl, wu;
-        bool all = false;
-        if (mode == 0) {
-            wl = p.cbl;
-            wu = p.cbu;
+// settled to their exact round-1 class in place (lvc = class << 4) and counted.  A disagreement
+// between an exact level and its coarse level is reported (the call fails) instead of counted.
+__device__ __forceinline__ void fine1_hit(int mode, QsrpParams *__restrict__ par, const Round1Src &src, int64_t u,
+                                          int q, unsigned v, uint8_t *__restrict__ lvc_at, int S, int W,
+                                          int *__restrict__ fhist, int *__restrict__ mismatch) {
+    const QsrpParams &p = par[q];
+    const int cl = (int) (v & 15), cu = (int) (v >> 4);
+    const uint32_t lv = src.levels(u, q);
+    const int l = (int) (lv & 0xffffu), h = (int) (lv >> 16);
+    if (mode == 0) {
+        int *fh = fhist + (int64_t) q * 2 * W;
+        if (cl == p.w_l) {
+            const int i = l - lvt_lo(cl, S);
+            if (i >= 0 && l <= lvt_level(cl, S)) atomicAdd(fh + i, 1);
+            else atomicAdd(mismatch, 1);
+        }
+        if (cu == p.w_u) {
+            const int i = h - lvt_lo(cu, S);
+            if (i >= 0 && h <= lvt_level(cu, S)) atomicAdd(fh + W + i, 1);
+            else atomicAdd(mismatch, 1);
+        }
+        return;
+    }
+    const int cls = class1_lv(p, l, h);
+    if (p.w_all) {
+        atomicAdd(cls == kClsResult ? &par[q].n_res1 : (cls == kClsPrune ? &par[q].n_pr1 : &par[q].n_ref1), 1);
+    } else {
+        if (cl == p.w_l && l <= p.lv_res) atomicAdd(&par[q].res_fine, 1);
+        if (cu == p.w_u && h <= p.lv_pr - 1) atomicAdd(&par[q].ple_fine, 1);
+    }
+    *lvc_at = (uint8_t) ((cls << 4) | kLvcResolved);
+}
+
+// Hits of a fine scan: (query << 40 | user << 8 | coarse-level byte); past the capacity the scan
+// settles them itself.
+struct Fine1List {
+    uint64_t *e;
+    int *count;
+    int cap;
+};
+
+// The scan: the batch's coarse-level bytes as one flat [query][user] array, 16 per lane and 512 per
+// warp and step (a segment meets at most one query boundary when n_user >= 512).
+__global__ void __launch_bounds__(256) qsrp_fine1_scan_kernel(uint8_t *__restrict__ lvc, Round1Src src, int64_t n_user,
+                                                             int nq, double inv_user, int S, int W, int mode,
+                                                             QsrpParams *__restrict__ par, Fine1List fl,
+                                                             int *__restrict__ fhist, int *__restrict__ mismatch,
+                                                             int *__restrict__ n_hits) {
+    const int64_t total = n_user * nq;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t stride = (int64_t) gridDim.x * blockDim.x * 16;
+    for (int64_t seg = warp * 512; seg < total; seg += stride) {
+        const int64_t base = seg + (int64_t) lane * 16;
+        uint32_t w[4];
+        if (base + 16 <= total) {
+            const uint4 x = *reinterpret_cast<const uint4 *>(lvc + base);
+            w[0] = x.x; w[1] = x.y; w[2] = x.z; w[3] = x.w;
         } else {
-            wl = p.amb_l;
-            wu = p.amb_u;
-            all = p.exact1 != 0;
-        }
-        if (wl < 0 && wu < 0 && !all) continue;
-        uint8_t *row = lvc + (int64_t) q * n_user;
-        int n_res = 0, n_ple = 0, c_res = 0, c_pr = 0, c_ref = 0;
-        for (int k = 0; k < 4; k++) {
-            const int64_t u = u0 + 32 * k + lane;
-            const bool in = u < n_user;
-            const unsigned v = in ? row[u] : 0u;
-            const int cl = (int) (v & 15), cu = (int) (v >> 4);
-            const bool hit = in && (all || cl == wl || cu == wu);
-            if (!hit) continue;
-            const uint32_t lv = src.levels(u, q);
-            const int l = (int) (lv & 0xffffu), h = (int) (lv >> 16);
-            if (mode == 0) {
-                // the exact levels lie in the coarse levels the screen gave them; a disagreement is
-                // reported (the call fails) instead of counted
-                int *fh = fhist + (int64_t) q * 2 * G;
-                const int il = l - (wl - 1) * G - 1, iu = h - (wu - 1) * G - 1;
-                if (cl == wl) {
-                    if (il >= 0 && il < G) atomicAdd(fh + il, 1);
-                    else atomicAdd(mismatch, 1);
-                }
-                if (cu == wu) {
-                    if (iu >= 0 && iu < G) atomicAdd(fh + G + iu, 1);
-                    else atomicAdd(mismatch, 1);
-                }
-            } else {
-                const int cls = class1_lv(p, l, h);
-                if (all) {
-                    c_res += cls == kClsResult;
-                    c_pr += cls == kClsPrune;
-                    c_ref += cls == kClsRefine || cls == kClsIdle;
-                } else {
-                    n_res += cl == wl && l <= p.lv_res;
-                    n_ple += cu == wu && h <= p.lv_pr - 1;
-                }
-                row[u] = (uint8_t) ((cls << 4) | kLvcResolved);
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                w[i] = 0;
+                for (int j = 0; j < 4; j++)
+                    if (base + 4 * i + j < total) w[i] |= (uint32_t) lvc[base + 4 * i + j] << (8 * j);
             }
         }
-        if (mode == 1) {
-            n_res = (int) warp_sum64(n_res);
-            n_ple = (int) warp_sum64(n_ple);
-            c_res = (int) warp_sum64(c_res);
-            c_pr = (int) warp_sum64(c_pr);
-            c_ref = (int) warp_sum64(c_ref);
-            if (lane == 0) {
-                if (n_res) atomicAdd(&par[q].res_fine, n_res);
-                if (n_ple) atomicAdd(&par[q].ple_fine, n_ple);
-                if (c_res) atomicAdd(&par[q].n_res1, c_res);
-                if (c_pr) atomicAdd(&par[q].n_pr1, c_pr);
-                if (c_ref) atomicAdd(&par[q].n_ref1, c_ref);
+        // the segment's first query (once per warp) and the lane's queries
+        int64_t qs = 0;
+        if (lane == 0) {
+            qs = (int64_t) ((double) seg * inv_user);
+            if (qs * n_user > seg) qs--;
+            else if ((qs + 1) * n_user <= seg) qs++;
+        }
+        qs = __shfl_sync(0xffffffffu, qs, 0);
+        uint32_t hits = 0;
+        if (base < total) {
+            int64_t q = qs;
+            while ((q + 1) * n_user <= base) q++;
+            int64_t edge = (q + 1) * n_user;
+            int wl = par[q].w_l, wu = par[q].w_u, wa = par[q].w_all;
+#pragma unroll
+            for (int e = 0; e < 16; e++) {
+                const int64_t pos = base + e;
+                if (pos >= total) break;
+                if (pos >= edge) {  // the next query (and the one after, for short rows)
+                    while ((q + 1) * n_user <= pos) q++;
+                    edge = (q + 1) * n_user;
+                    wl = par[q].w_l; wu = par[q].w_u; wa = par[q].w_all;
+                }
+                const unsigned v = (w[e >> 2] >> (8 * (e & 3))) & 0xffu;
+                hits |= (uint32_t) (wa || (int) (v & 15) == wl || (int) (v >> 4) == wu) << e;
             }
         }
+        if (n_hits) {
+            const int c = __popc(hits);
+            const int tot = __reduce_add_sync(0xffffffffu, c);
+            if (lane == 0 && tot) atomicAdd(n_hits + mode, tot);
+        }
+        // one hit per lane and round: warp-aggregated appends
+        while (__any_sync(0xffffffffu, hits != 0)) {
+            const bool have = hits != 0;
+            const int e = have ? __ffs(hits) - 1 : 0;
+            const unsigned want = __ballot_sync(0xffffffffu, have);
+            const int leader = __ffs(want) - 1;
+            int at = 0;
+            if (lane == leader) at = atomicAdd(fl.count, __popc(want));
+            at = __shfl_sync(0xffffffffu, at, leader) + __popc(want & ((1u << lane) - 1));
+            if (have) {
+                const int64_t pos = base + e;
+                const int64_t q = (int64_t) ((double) pos * inv_user);
+                int64_t qq = q;
+                if (qq * n_user > pos) qq--;
+                else if ((qq + 1) * n_user <= pos) qq++;
+                const int64_t u = pos - qq * n_user;
+                const unsigned v = (w[e >> 2] >> (8 * (e & 3))) & 0xffu;
+                if (at < fl.cap) fl.e[at] = ((uint64_t) qq << 40) | ((uint64_t) u << 8) | v;
+                else fine1_hit(mode, par, src, u, (int) qq, v, lvc + pos, S, W, fhist, mismatch);
+                hits &= hits - 1;
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) qsrp_fine1_list_kernel(uint8_t *__restrict__ lvc, Round1Src src, int64_t n_user,
+                                                             int S, int W, int mode, QsrpParams *__restrict__ par,
+                                                             Fine1List fl, int *__restrict__ fhist,
+                                                             int *__restrict__ mismatch) {
+    const int n = min(*fl.count, fl.cap);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint64_t x = fl.e[i];
+        const int q = (int) (x >> 40);
+        const int64_t u = (int64_t) ((x >> 8) & 0xffffffffu);
+        fine1_hit(mode, par, src, u, q, (unsigned) (x & 0xffu), lvc + (int64_t) q * n_user + u, S, W, fhist, mismatch);
     }
 }
 
@@ -494,16 +576,17 @@ __global__ void __launch_bounds__(256) qsrp_fine1_kernel(uint8_t *__restrict__ l
 // counts.
 __global__ void qsrp_select1f_kernel(const int *__restrict__ lhist, const int *__restrict__ fhist,
                                      const int *__restrict__ anomaly, int64_t n_user, const int32_t *__restrict__ rank,
-                                     int S, int n_item, int G, KSpec ks, int nq, QsrpParams *__restrict__ par) {
+                                     int S, int n_item, int W, KSpec ks, int nq, QsrpParams *__restrict__ par) {
     const int q = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (q >= nq) return;
     const int topk = ks.of(q);
     QsrpParams p = par[q];
     int kl, kh;
     {
-        const int *fh = fhist + (int64_t) q * 2 * G;
-        kl = (p.cbl - 1) * G + 1 + warp_first_reaching(fh, G, topk - p.cum_l);
-        kh = p.cbu < 0 ? 0 : (p.cbu - 1) * G + 1 + warp_first_reaching(fh + G, G, topk - p.cum_u);
+        const int *fh = fhist + (int64_t) q * 2 * W;
+        const int wl = lvt_level(p.cbl, S) - lvt_lo(p.cbl, S) + 1, wu = lvt_level(p.cbu, S) - lvt_lo(p.cbu, S) + 1;
+        kl = lvt_lo(p.cbl, S) + (wl > 1 ? warp_first_reaching(fh, wl, topk - p.cum_l) : 0);
+        kh = lvt_lo(p.cbu, S) + (wu > 1 ? warp_first_reaching(fh + W, wu, topk - p.cum_u) : 0);
     }
     p.L1 = level_rank(kl, rank, S, n_item);
     p.U1 = level_rank(kh, rank, S, n_item);
@@ -518,31 +601,37 @@ __global__ void qsrp_select1f_kernel(const int *__restrict__ lhist, const int *_
     p.lv_res = (int) warp_sum64(c_res) - 1;
     p.lv_m1 = (int) warp_sum64(c_m1) - 1;
     p.lv_pr = (int) warp_sum64(c_lt);
+    p.c_res = coarse_last_le(p.lv_res, S);
+    p.c_m1 = coarse_last_le(p.lv_m1, S);
+    p.c_pr = coarse_first_gt(p.lv_pr - 1, S);
     p.res_fine = 0;
     p.ple_fine = 0;
     p.n_res1 = 0;
     p.n_pr1 = 0;
     p.n_ref1 = 0;
     if (p.mode1) {
-        p.amb_l = coarse_straddle(p.lv_m1, G);
-        p.amb_u = coarse_straddle(p.lv_m1, G);
+        p.amb_l = coarse_straddle(p.lv_m1, S);
+        p.amb_u = coarse_straddle(p.lv_m1, S);
     } else if (anomaly[q]) {
         p.exact1 = 1;
+        p.w_all = 1;
     } else {
-        p.amb_l = coarse_straddle(p.lv_res, G);
-        p.amb_u = coarse_straddle(p.lv_pr - 1, G);
+        p.amb_l = coarse_straddle(p.lv_res, S);
+        p.amb_u = coarse_straddle(p.lv_pr - 1, S);
         // the whole coarse levels: lower side <= lv_res, upper side <= lv_pr - 1
         int hl[kLvEntries], hu[kLvEntries];
         coarse_counts(lhist + (int64_t) q * 2 * kLvEntries, kLvEntries - 1, n_user, hl);
         coarse_counts(lhist + (int64_t) q * 2 * kLvEntries + kLvEntries, 0, n_user, hu);
         int64_t nres = 0, nle = 0;
         for (int b = 0; b < kLvEntries; b++) {
-            if (coarse_all_le(b, p.lv_res, G)) nres += hl[b];
-            if (coarse_all_le(b, p.lv_pr - 1, G)) nle += hu[b];
+            if (coarse_all_le(b, p.lv_res, S)) nres += hl[b];
+            if (coarse_all_le(b, p.lv_pr - 1, S)) nle += hu[b];
         }
         p.n_res1 = (int) nres;
         p.n_pr1 = (int) nle;  // until qsrp_final1: users whose upper level is <= lv_pr - 1 (whole levels)
     }
+    p.w_l = p.amb_l;
+    p.w_u = p.amb_u;
     if (lane == 0) par[q] = p;
 }
 
@@ -593,7 +682,7 @@ __global__ void qs_params_kernel(QsrpParams *__restrict__ par, int nq, int64_t n
 // place of the group code; the others are counted by group (per-warp shared-memory copies).
 __global__ void __launch_bounds__(kHistThreads) qsrp_round2_kernel(const uint8_t *__restrict__ lvc,
                                                                   uint8_t *__restrict__ code, int64_t n_user,
-                                                                  const QsrpParams *__restrict__ par, int nb, int G,
+                                                                  const QsrpParams *__restrict__ par, int nb,
                                                                   int64_t chunk, int *__restrict__ hist_c) {
     extern __shared__ int h[];
     const int nbin = nb + 1, copies = hist_copies(nbin);
@@ -601,7 +690,7 @@ __global__ void __launch_bounds__(kHistThreads) qsrp_round2_kernel(const uint8_t
     QsrpParams p;
     {
         const QsrpParams &g = par[q];
-        p.mode1 = g.mode1; p.all1 = g.all1; p.lv_res = g.lv_res; p.lv_pr = g.lv_pr; p.lv_m1 = g.lv_m1;
+        p.mode1 = g.mode1; p.all1 = g.all1; p.c_res = g.c_res; p.c_pr = g.c_pr; p.c_m1 = g.c_m1;
     }
     const bool all_survive = lvc == nullptr;  // QS and US: no round 1
     for (int b = threadIdx.x; b < copies * nbin; b += blockDim.x) h[b] = 0;
@@ -610,22 +699,19 @@ __global__ void __launch_bounds__(kHistThreads) qsrp_round2_kernel(const uint8_t
     const uint8_t *lrow = lvc ? lvc + (int64_t) q * n_user : nullptr;
     uint8_t *crow = code + (int64_t) q * n_user;
     const int64_t u0 = (int64_t) blockIdx.x * chunk, u1 = min(u0 + chunk, n_user);
-    constexpr int GP = 8;  // pairs in flight per thread
-    for (int64_t ub = u0 + threadIdx.x; ub < u1; ub += GP * kHistThreads) {
-        unsigned v[GP], cc[GP];
+    // 16 consecutive users per thread and step, their bytes from five aligned words per row
+    for (int64_t ub = u0 + (int64_t) threadIdx.x * 16; ub < u1; ub += (int64_t) kHistThreads * 16) {
+        const int n = (int) min((int64_t) 16, u1 - ub);
+        uint32_t lw[4] = {0u, 0u, 0u, 0u}, cw[4];
+        if (!all_survive) load16_bytes(lrow + ub, lw);
+        load16_bytes(crow + ub, cw);
 #pragma unroll
-        for (int g = 0; g < GP; g++) {
-            const bool in = ub + g * kHistThreads < u1;
-            v[g] = in && !all_survive ? lrow[ub + g * kHistThreads] : 0u;
-            cc[g] = in ? crow[ub + g * kHistThreads] : 0u;
-        }
-#pragma unroll
-        for (int g = 0; g < GP; g++) {
-            const int64_t u = ub + g * kHistThreads;
-            if (u >= u1) break;
-            const int k = all_survive ? kClsRefine : class1_coarse(p, v[g], G);
-            if (k == kClsRefine || k == kClsIdle) atomicAdd(mine + cc[g], 1);
-            else crow[u] = k == kClsResult ? kCodeResult1 : kCodePruned1;
+        for (int e = 0; e < 16; e++) {
+            if (e >= n) break;
+            const unsigned v = (lw[e >> 2] >> (8 * (e & 3))) & 0xffu, c = (cw[e >> 2] >> (8 * (e & 3))) & 0xffu;
+            const int k = all_survive ? kClsRefine : class1_coarse(p, v);
+            if (k == kClsRefine || k == kClsIdle) atomicAdd(mine + c, 1);
+            else crow[ub + e] = k == kClsResult ? kCodeResult1 : kCodePruned1;
         }
     }
     __syncthreads();
@@ -944,7 +1030,6 @@ struct QsrpCompactPolicy {
     struct Aux { int rank, fresh, lb, ub; };
     const uint8_t *lvc;  // coarse round-1 levels (QSRP), or nullptr
     Round1Src src;       // the reference's round-1 levels, recomputed
-    int G;
     const uint8_t *code;
     const float *thr;
     QipView sc;
@@ -1004,8 +1089,8 @@ struct QsrpCompactPolicy {
                 const unsigned v = lvc[at];
                 if ((v & 15) != kLvcResolved) {
                     const int cl = (int) (v & 15), cu = (int) (v >> 4);
-                    if (coarse_all_gt(cu, p.lv_m2, G) || coarse_all_gt(cl, p.lv_m2, G)) return 0;
-                    if (!with_aux && coarse_all_le(cu, p.lv_m2, G) && coarse_all_le(cl, p.lv_m2, G)) return 1;
+                    if (coarse_all_gt(cu, p.lv_m2, S_reg) || coarse_all_gt(cl, p.lv_m2, S_reg)) return 0;
+                    if (!with_aux && coarse_all_le(cu, p.lv_m2, S_reg) && coarse_all_le(cl, p.lv_m2, S_reg)) return 1;
                 }
             }
             const uint32_t v = src.levels(u, q);
@@ -1143,10 +1228,10 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
     const int dim = ix->dim, c = ix->check_dim, S = ix->n_sample, Sr = ix->n_sample_reg;
     const int n_item = (int) ix->n_item;
     const int gs = thr_group(S), nb = (S + gs - 1) / gs;
-    const int G = qsrp ? lvt_stride(Sr) : 1;
-    const size_t n_lhist = (size_t) nq * 2 * kLvEntries, n_fhist = (size_t) nq * 2 * G;
+    const int W = qsrp ? lvt_width(Sr) : 1;
+    const size_t n_lhist = (size_t) nq * 2 * kLvEntries, n_fhist = (size_t) nq * 2 * W;
     RKR_TRY(ix->ws_qtr.ensure(carve_size((size_t) nq * dim, 4) + carve_size(nq, 4) + carve_size(nq, sizeof(QsrpParams)) +
-                              carve_size(nq, 4) + carve_size(1, 4) * 3 + carve_size(2, 4) + carve_size(n_lhist, 4) +
+                              carve_size(nq, 4) + carve_size(1, 4) * 3 + carve_size(2, 4) * 3 + carve_size(n_lhist, 4) +
                               carve_size(n_fhist, 4) + carve_size(nq, 4) * 2 + carve_size(nq, 8)));
     uint8_t *p0 = ix->ws_qtr.as<uint8_t>();
     float *qtr = carve<float>(p0, (size_t) nq * dim);
@@ -1175,11 +1260,15 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
     int *any2 = carve<int>(p0, 1);
     int *hit_count = carve<int>(p0, 2);
     int *mismatch = carve<int>(p0, 1);
+    int *n_hits = carve<int>(p0, 2);
+    int *f1_count = carve<int>(p0, 2);
     int *lhist = carve<int>(p0, n_lhist);
     int *fhist = carve<int>(p0, n_fhist);
-    RKR_TRY(ix->ws_levels.ensure((size_t) nq * U * (qsrp ? 2 : 1)));
+    // code [nq][U], then (QSRP) the coarse levels from the next 256-byte boundary (16-byte vector scans)
+    const size_t code_bytes = ((size_t) nq * U + 255) & ~size_t(255);
+    RKR_TRY(ix->ws_levels.ensure(code_bytes + (qsrp ? (size_t) nq * U + 256 : 0)));
     uint8_t *code = ix->ws_levels.as<uint8_t>();
-    uint8_t *lvc = qsrp ? code + (size_t) nq * U : nullptr;
+    uint8_t *lvc = qsrp ? code + code_bytes : nullptr;
     RKR_TRY(ix->ws_cls.ensure(carve_size((size_t) nq * (S + 1), 1) + carve_size((size_t) nq * (nb + 1), 1)));
     RKR_TRY(ix->ws_counts.ensure(sizeof(QueryCounts) * (size_t) nq));
     const size_t n_hist_c = (size_t) nq * (nb + 1), n_hist_f = (size_t) nq * (S + 1);
@@ -1230,7 +1319,7 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
     // Phase 1: both bound rounds up to the round-2 class counts.  Its launches have fixed shapes for
     // a given batch size and no host synchronisation, so a caller that serves batches of a few sizes
     // captures it once per size as a CUDA graph and replays it (ix->graphs_on).
-    int *sc_status[2] = {nullptr, nullptr};
+    int *sc_status[4] = {nullptr, nullptr, nullptr, nullptr};
     auto phase1 = [&](bool force_exact) -> int {
         RKR_CUDA(cudaMemsetAsync(pz, 0, (size_t) (p0 - pz), st));
         RKR_CUDA(cudaMemsetAsync(n_rescored, 0, sizeof(int), st));
@@ -1272,7 +1361,6 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
             e1.qnorm = qnorm;
             e1.thr_summ = ix->thr_summ.as<float>();
             e1.m = m;
-            e1.G = G;
             e1.lvc = lvc;
             e1.code = code;
             e1.anomaly = anomaly;
@@ -1290,11 +1378,11 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
             RKR_CUDA(ce);
             if (qsrp) {
                 timed(ix, st, "qsrp_fix1", [&] {
-                    qsrp_fix1_kernel<<<148 * 4, 256, 0, st>>>(fix, m, G, r1.unorm, qnorm, U, lvc, anomaly);
+                    qsrp_fix1_kernel<<<148 * 4, 256, 0, st>>>(fix, m, r1.unorm, qnorm, U, lvc, anomaly);
                 });
                 RKR_CUDA(cudaGetLastError());
                 timed(ix, st, "qsrp_fix1_scan", [&] {
-                    qsrp_fix1_scan_kernel<<<148 * 8, 256, 0, st>>>(fix_count, fix_cap, r1, G, U, nq, lvc, anomaly);
+                    qsrp_fix1_scan_kernel<<<148 * 8, 256, 0, st>>>(fix_count, fix_cap, r1, U, nq, lvc, anomaly);
                 });
                 RKR_CUDA(cudaGetLastError());
                 const int64_t ch = 65536;
@@ -1307,21 +1395,36 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
         dim3 hg((unsigned) ((U + chunk - 1) / chunk), (unsigned) nq);
         if (qsrp) {
             timed(ix, st, "qsrp_select1c", [&] {
-                qsrp_select1c_kernel<<<(nq + 127) / 128, 128, 0, st>>>(lhist, U, ks, nq, par);
+                qsrp_select1c_kernel<<<(nq + 127) / 128, 128, 0, st>>>(lhist, U, ks, nq, Sr, par);
             });
             RKR_CUDA(cudaGetLastError());
-            const dim3 fg((unsigned) ((U + 127) / 128), (unsigned) std::min((nq + 7) / 8, 16));
+            const double inv_u = 1.0 / (double) U;
+            Fine1List f1;
+            f1.e = hl.e;  // the fine scans of round 2 reuse this list later
+            f1.cap = hl.cap;
+            f1.count = f1_count;
             timed(ix, st, "qsrp_fine1", [&] {
-                qsrp_fine1_kernel<<<fg, 256, 0, st>>>(lvc, r1, U, nq, G, 0, par, fhist, mismatch);
+                qsrp_fine1_scan_kernel<<<148 * 16, 256, 0, st>>>(lvc, r1, U, nq, inv_u, Sr, W, 0, par, f1, fhist, mismatch,
+                                                                 ix->prof.on ? n_hits : nullptr);
+            });
+            RKR_CUDA(cudaGetLastError());
+            timed(ix, st, "qsrp_fine1_list", [&] {
+                qsrp_fine1_list_kernel<<<148 * 4, 256, 0, st>>>(lvc, r1, U, Sr, W, 0, par, f1, fhist, mismatch);
             });
             RKR_CUDA(cudaGetLastError());
             timed(ix, st, "qsrp_select1f", [&] {
-                qsrp_select1f_kernel<<<(nq + 3) / 4, 128, 0, st>>>(lhist, fhist, anomaly, U, m.rank, Sr, n_item, G, ks,
+                qsrp_select1f_kernel<<<(nq + 3) / 4, 128, 0, st>>>(lhist, fhist, anomaly, U, m.rank, Sr, n_item, W, ks,
                                                                    nq, par);
             });
             RKR_CUDA(cudaGetLastError());
+            f1.count = f1_count + 1;
             timed(ix, st, "qsrp_fine1", [&] {
-                qsrp_fine1_kernel<<<fg, 256, 0, st>>>(lvc, r1, U, nq, G, 1, par, fhist, mismatch);
+                qsrp_fine1_scan_kernel<<<148 * 16, 256, 0, st>>>(lvc, r1, U, nq, inv_u, Sr, W, 1, par, f1, fhist, mismatch,
+                                                                 ix->prof.on ? n_hits : nullptr);
+            });
+            RKR_CUDA(cudaGetLastError());
+            timed(ix, st, "qsrp_fine1_list", [&] {
+                qsrp_fine1_list_kernel<<<148 * 4, 256, 0, st>>>(lvc, r1, U, Sr, W, 1, par, f1, fhist, mismatch);
             });
             RKR_CUDA(cudaGetLastError());
             timed(ix, st, "qsrp_final1", [&] { qsrp_final1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, ks, U); });
@@ -1332,7 +1435,7 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
         }
         timed(ix, st, "qsrp_round2", [&] {
             qsrp_round2_kernel<<<hg, kHistThreads, hist_copies(nb + 1) * (nb + 1) * sizeof(int), st>>>(
-                lvc, code, U, par, nb, G, chunk, hist_c);
+                lvc, code, U, par, nb, chunk, hist_c);
         });
         RKR_CUDA(cudaGetLastError());
         timed(ix, st, "qsrp_select2c", [&] {
@@ -1366,16 +1469,21 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
     };
     RKR_TRY(run_phase1(ix, method, nq, st, phase1));
     std::vector<QueryCounts> hc(nq);
-    int h_fix = 0, h_mismatch = 0, h_sc[2] = {0, 0};
+    int h_fix = 0, h_mismatch = 0, h_sc[4] = {0, 0, 0, 0};
     RKR_CUDA(cudaMemcpyAsync(hc.data(), counts, sizeof(QueryCounts) * nq, cudaMemcpyDeviceToHost, st));
     RKR_CUDA(cudaMemcpyAsync(&h_fix, fix_count, sizeof(int), cudaMemcpyDeviceToHost, st));
     RKR_CUDA(cudaMemcpyAsync(&h_mismatch, mismatch, sizeof(int), cudaMemcpyDeviceToHost, st));
     if (sc_status[0]) {
         RKR_CUDA(cudaMemcpyAsync(&h_sc[0], sc_status[0], sizeof(int), cudaMemcpyDeviceToHost, st));
-        RKR_CUDA(cudaMemcpyAsync(&h_sc[1], sc_status[1], sizeof(int), cudaMemcpyDeviceToHost, st));
+        for (int i = 1; i < 4; i++)
+            RKR_CUDA(cudaMemcpyAsync(&h_sc[i], sc_status[i], sizeof(int), cudaMemcpyDeviceToHost, st));
     }
     RKR_CUDA(cudaStreamSynchronize(st));
-    if (ix->prof.on) ix->prof.add_count("screen_undecided_pairs", h_sc[1]);
+    if (ix->prof.on) {
+        ix->prof.add_count("screen_undecided_pairs", h_sc[1]);
+        ix->prof.add_count("lvt_search_lower_pairs", h_sc[2]);
+        ix->prof.add_count("lvt_search_upper_pairs", h_sc[3]);
+    }
     if (h_sc[0]) {
         // the tensor-core run gave up (a bounded wait or a full list): the exact tiles redo phase 1
         RKR_TRY(phase1(true));
@@ -1411,7 +1519,6 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
     QsrpCompactPolicy pol;
     pol.lvc = lvc;
     pol.src = r1;
-    pol.G = G;
     pol.code = code;
     pol.thr = thr;
     pol.sc = qv;
@@ -1459,9 +1566,14 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
     RKR_CUDA(cudaGetLastError());
     RKR_CUDA(cudaStreamSynchronize(st));
     if (ix->prof.on) {
-        int h = 0;
+        int h = 0, hh[2] = {0, 0};
         RKR_CUDA(cudaMemcpy(&h, n_rescored, sizeof(int), cudaMemcpyDeviceToHost));
         ix->prof.add_count("rescored_pairs", h);
+        if (qsrp) {
+            RKR_CUDA(cudaMemcpy(hh, n_hits, sizeof(hh), cudaMemcpyDeviceToHost));
+            ix->prof.add_count("fine1_select_pairs", hh[0]);
+            ix->prof.add_count("fine1_class_pairs", hh[1]);
+        }
     }
     return RKR_OK;
 }

@@ -163,20 +163,31 @@ __device__ __forceinline__ bool regression_levels_fast(const RegUser &r, int S, 
 // ---- per-user level-boundary tables ------------------------------------------------------------------
 //
 // For each user and side, the reference's level is a non-increasing step function of the score.
-// The table holds, at every G-th level value g G (g = 0 .. kLvEntries - 1, G = lvt_stride(S), so
-// that (kLvEntries - 1) G >= S + 1), the smallest binary32 score T_g whose level is <= g G, and a
-// guard band: outside [T_g - band_g, T_g + band_g] the level's relation to g G is the exact-math
-// one (the reference's binary32 evaluation can only differ from it where the model's value lies
-// within its rounding error of the crossing integer).  A score q then has coarse level
-// c = #{g : q < T_g} = ceil(level / G), decided for every score within dq of q when
-// (c == kLvEntries - 1 or q - dq >= T_c + band_c) and (c == 0 or q + dq < T_(c-1) - band_(c-1)).
-// Entries are (T_g, band_g); a user whose record is unusable for the tables (a non-finite value,
-// sigma <= 0, a slope a >= 0) has NaN entries, so none of its pairs is ever decided from them.
+// The table holds, at each of kLvEntries level values L_g (lvt_level: L_0 = 0, then 14 steps of
+// about S / 14 up to L_14 = S, and L_15 = S + 1), the smallest binary32 score T_g whose level is
+// <= L_g, and a guard band: outside [T_g - band_g, T_g + band_g] the level's relation to L_g is the
+// exact-math one (the reference's binary32 evaluation can only differ from it where the model's
+// value lies within its rounding error of the crossing integer).  A score's coarse level is the
+// number of boundaries above it, c = #{g : q < T_g}: the smallest g with level <= L_g.  Coarse
+// level 0 is exactly level 0 and coarse level 15 exactly level S + 1 (the extremes most pairs sit
+// at); the others span (L_(c-1), L_c].  The coarse level of q is decided for every score within dq
+// of q when (c == kLvEntries - 1 or q - dq >= T_c + band_c) and (c == 0 or q + dq < T_(c-1) -
+// band_(c-1)).  Entries are (T_g, band_g); a user whose record is unusable for the tables (a
+// non-finite value, sigma <= 0, a slope a >= 0) has NaN entries, so none of its pairs is ever
+// decided from them.
 constexpr int kLvEntries = 16;
 
-__host__ __device__ __forceinline__ int lvt_stride(int S) { return (S + 1 + kLvEntries - 2) / (kLvEntries - 1); }
-// coarse level of an exact level (the table's ceil(level / G))
-__device__ __forceinline__ int lvt_coarse(int lvl, int G) { return (lvl + G - 1) / G; }
+__host__ __device__ __forceinline__ int lvt_level(int g, int S) {  // S < 2^26: 32-bit products
+    return g >= kLvEntries - 1 ? S + 1 : (g * S + (kLvEntries - 3)) / (kLvEntries - 2);
+}
+// coarse level of an exact level: the smallest g with level <= L_g
+__host__ __device__ __forceinline__ int lvt_coarse(int l, int S) {
+    if (l <= 0) return 0;
+    if (l > S) return kLvEntries - 1;
+    return (kLvEntries - 2) * (l - 1) / S + 1;
+}
+// most levels in one coarse level (the fine histograms' width)
+__host__ __device__ __forceinline__ int lvt_width(int S) { return (S + kLvEntries - 3) / (kLvEntries - 2) + 1; }
 
 // Coarse level of score q on one side from the table row (entry j of this user at t[j * stride]),
 // and whether every score within dq of q has it.
@@ -213,8 +224,9 @@ struct ScoresTcCall {
     uint8_t *code;   // [nq][n_user]
     int *lhist;      // [nq][2][kLvEntries] (QSRP), zeroed by the caller
     int *anomaly;    // [nq] (QSRP), zeroed by the caller
-    int **status = nullptr;  // if set: receives device pointers to the run's status (0: complete) and
-                             // undecided-pair count, and the call does not wait for the device
+    int **status = nullptr;  // if set ([4]): receives device pointers to the run's status (0: complete),
+                             // undecided-pair count and the two table-search counts (lower, upper side:
+                             // warp passes x 32), and the call does not wait for the device
 };
 // Runs the tensor-core scores where the shape allows; *done = false leaves the batch to the exact
 // tiles (the histograms may then hold partial counts: the caller clears them).  With call.status

@@ -44,7 +44,7 @@ namespace {
 
 constexpr int kScEpiWarps = 16;
 constexpr int kScThreads = 32 * (kScEpiWarps + 1);
-constexpr int kScListCap = 2048;                   // undecided pairs per CTA resolved in the kernel
+constexpr int kScListCap = 1024;                   // undecided pairs per CTA resolved in the kernel
 constexpr int kScMaxQ = 1024;                      // queries per launch (their data sits in shared memory)
 constexpr int kScMaxKp = 224;                      // padded coordinates (both parts): shared memory
 constexpr int kScSummStride = kScM;  // summary transposed: entry j of row r at j * kScM + r (lanes hit distinct banks)
@@ -59,7 +59,6 @@ struct ScArgs {
     const float *thr_summ;
     RegModel m;
     const float2 *lvt;             // [n_user][2][kLvEntries] level tables; nullptr: no regression round (QS, US)
-    int G;                         // the tables' level stride
     uint8_t *lvc;                  // [query][n_user]: coarse lower-bound level | coarse upper-bound level << 4
     uint8_t *code;                 // [query][n_user]: coarse threshold group of the full score
     int *lhist;                    // [query][2][kLvEntries] coarse-level counts; the lower side's last bin and
@@ -68,6 +67,7 @@ struct ScArgs {
     float2 *dump;                  // [query][n_user] (estimate of the full score, its bound), or nullptr
     int2 *ovf;                     // undecided pairs, (query, user): each tile's list in one piece
     int *ovf_count, *status, *undecided;
+    int *searches;                 // [2]: warp passes that ran the lower / upper side's table search
     int ovf_cap;
     int2 *tile_rng;                // per tile of the launch: (first entry, entries) in ovf
     int2 *spill;                   // undecided pairs past a tile's shared-memory list
@@ -124,7 +124,7 @@ __device__ __forceinline__ void exact_pair(const ScArgs &a, int64_t u, int q, co
         const uint32_t v = regression_levels_exact(a.m.rec, a.m.S, a.m.err_cap, u, __fsub_rn(left, right),
                                                    __fadd_rn(left, right));
         const int l = (int) (v & 0xffffu), h = (int) (v >> 16);
-        const int cl = lvt_coarse(l, a.G), cu = lvt_coarse(h, a.G);
+        const int cl = lvt_coarse(l, a.m.S), cu = lvt_coarse(h, a.m.S);
         a.lvc[o] = (uint8_t) (cl | (cu << 4));
         int *hq = a.lhist + (int64_t) q * 2 * kLvEntries;
         if (cl != kLvEntries - 1) atomicAdd(hq + cl, 1);
@@ -140,9 +140,22 @@ __device__ __forceinline__ void exact_pair(const ScArgs &a, int64_t u, int q, co
     a.code[o] = (uint8_t) min(g, a.nb);
 }
 
-// Adds to a shared-memory histogram of byte counters packed four to a word (no counter exceeds
-// kScM = 128, so no byte overflows into the next).
-__device__ __forceinline__ void hist_add(uint32_t *h, int bin, uint32_t n) { atomicAdd(h + (bin >> 2), n << (8 * (bin & 3))); }
+// Counts one query column of a warp's pairs by coarse level into the chunk's shared-memory histogram
+// h ([2 sides][kLvEntries]).  Pairs at both implicit levels (the lower side's last, the upper side's
+// 0: most pairs) are not counted; the others are grouped by their two levels, and one lane of each
+// group adds the group's size -- one atomic per distinct pair of levels instead of one per pair (the
+// lanes of a warp mostly share their levels).
+__device__ __forceinline__ void warp_level_hist(uint32_t *h, bool count, int cl, int cu) {
+    const bool part = count && !(cl == kLvEntries - 1 && cu == 0);
+    const unsigned pm = __ballot_sync(0xffffffffu, part);
+    if (!part) return;
+    const unsigned m = __match_any_sync(pm, cl | (cu << 4));
+    if ((threadIdx.x & 31) == __ffs(m) - 1) {
+        const uint32_t n = (uint32_t) __popc(m);
+        if (cl != kLvEntries - 1) atomicAdd(h + cl, n);
+        if (cu != 0) atomicAdd(h + kLvEntries + cu, n);
+    }
+}
 
 __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
     extern __shared__ __align__(1024) uint8_t sm_raw[];
@@ -164,8 +177,8 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
     uint32_t *list = reinterpret_cast<uint32_t *>(summ + ThrSummary::kMaxGroups * kScSummStride);
     float4 *sq = reinterpret_cast<float4 *>(list + kScListCap);  // the batch's query data
     float *sqn = reinterpret_cast<float *>(sq + kScMaxQ);
-    uint32_t *shist = reinterpret_cast<uint32_t *>(sqn + kScMaxQ);           // [2][kScN][2][kLvEntries / 4]
-    float2 *stab = reinterpret_cast<float2 *>(shist + 2 * kScN * 2 * (kLvEntries / 4));  // [2 kLvEntries][kScM]
+    uint32_t *shist = reinterpret_cast<uint32_t *>(sqn + kScMaxQ);           // [2][kScN][2][kLvEntries]
+    float2 *stab = reinterpret_cast<float2 *>(shist + 2 * kScN * 2 * kLvEntries);  // [2 kLvEntries][kScM]
     volatile int *abort = &abort_flag;
 
     if (tid == 0) {
@@ -195,7 +208,7 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
             stab[j * kScM + rr] = u0 + rr < a.n_user ? __ldg(a.lvt + (u0 + rr) * 2 * kLvEntries + j)
                                                      : make_float2(NAN, NAN);
         }
-    for (int i = tid; i < 2 * kScN * 2 * (kLvEntries / 4); i += kScThreads) shist[i] = 0u;
+    for (int i = tid; i < 2 * kScN * 2 * kLvEntries; i += kScThreads) shist[i] = 0u;
     for (int i = tid; i < nq; i += kScThreads) {
         sq[i] = __ldg(a.qmeta + i);
         sqn[i] = lev ? __ldg(a.qnorm + i) : 0.0f;
@@ -286,16 +299,26 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
         float4 um = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         // the common cases of the two sides in registers: the lower side's last coarse level (scores
         // surely below T_(E-2) - band) and the upper side's level 0 (scores surely at or above T_0 + band)
-        float lo_last = -INFINITY, hi_first = INFINITY;
+        // and the upper side's first four boundaries (coarse levels 0 .. 3 hold most of its pairs) as
+        // (T - band, T + band), so that those pairs need no table search
+        float lo_last = -INFINITY;
+        float ulo[4], uhi[4];
+#pragma unroll
+        for (int g = 0; g < 4; g++) { ulo[g] = -INFINITY; uhi[g] = INFINITY; }
         if (uval) {
             um = __ldg(a.umeta + u);
             if (lev) {
                 un = __ldg(a.unorm + u);
-                const float2 el = tl[(kLvEntries - 2) * kScM], eu = tu[0];
+                const float2 el = tl[(kLvEntries - 2) * kScM];
                 lo_last = __fsub_rd(el.x, el.y);
-                hi_first = __fadd_ru(eu.x, eu.y);
                 if (!(lo_last == lo_last)) lo_last = -INFINITY;   // NaN entries: never the fast path
-                if (!(hi_first == hi_first)) hi_first = INFINITY;
+#pragma unroll
+                for (int g = 0; g < 4; g++) {
+                    const float2 e = tu[g * kScM];
+                    ulo[g] = __fsub_rd(e.x, e.y);
+                    uhi[g] = __fadd_ru(e.x, e.y);
+                    if (!(ulo[g] == ulo[g]) || !(uhi[g] == uhi[g])) { ulo[g] = -INFINITY; uhi[g] = INFINITY; }
+                }
             }
         }
         // the first two steps of the group search from registers
@@ -303,7 +326,7 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
         const int ue = __float_as_int(um.w);
         const float cl_u = a.cl * um.y, cr_u = a.cr * um.z;
         const uint32_t lane_base = taddr + ((uint32_t) (32 * quad) << 16) + (uint32_t) (8 * cg);
-        int n_und = 0;
+        int n_und = 0, n_slo = 0, n_sup = 0;
         bool dead = false;
         for (int j = 0; j < nchunks; j++) {
             const int b = j & 1;
@@ -313,7 +336,7 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                 atomicExch(a.status, 1);
                 dead = true;
             }
-            uint32_t *hb = shist + b * (kScN * 2 * (kLvEntries / 4));
+            uint32_t *hb = shist + b * (kScN * 2 * kLvEntries);
             if (!dead) {
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 float sl[8], sr[8];
@@ -377,9 +400,37 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                             const float dq = dl[g] * 1.0001f;
                             const float dql = fmaf(fabsf(qlb), 2.4e-7f, dq), dqu = fmaf(fabsf(qub), 2.4e-7f, dq);
                             int c_l = kLvEntries - 1, c_u = 0;
-                            bool okl = __fadd_ru(qlb, dql) < lo_last, oku = __fsub_rd(qub, dqu) >= hi_first;
-                            if (!okl) okl = lvt_screen(tl, kScM, qlb, dql, c_l);
-                            if (!oku) oku = lvt_screen(tu, kScM, qub, dqu, c_u);
+                            bool okl = __fadd_ru(qlb, dql) < lo_last;
+                            // upper side from the cached boundaries: coarse level = boundaries surely
+                            // above the score, decided when none of the four is within reach and the
+                            // level is below 4
+                            bool oku;
+                            {
+                                const float qm = __fsub_rd(qub, dqu), qp = __fadd_ru(qub, dqu);
+                                int below = 0;
+                                bool amb = false;
+#pragma unroll
+                                for (int k = 0; k < 4; k++) {
+                                    const bool b = qp < ulo[k], ab = qm >= uhi[k];
+                                    below += b;
+                                    amb = amb || !(b || ab);
+                                }
+                                c_u = below;
+                                oku = !amb && below < 4;
+                            }
+                            // the searches run for the whole warp when any lane needs them (no divergence)
+                            if (__any_sync(0xffffffffu, !okl)) {
+                                n_slo++;
+                                int c;
+                                const bool o = lvt_screen(tl, kScM, qlb, dql, c);
+                                if (!okl) { okl = o; c_l = c; }
+                            }
+                            if (__any_sync(0xffffffffu, !oku)) {
+                                n_sup++;
+                                int c;
+                                const bool o = lvt_screen(tu, kScM, qub, dqu, c);
+                                if (!oku) { oku = o; c_u = c; }
+                            }
                             ok[g] = okl && oku;
                             packed[g] = c_l | (c_u << 4);
                         }
@@ -403,22 +454,22 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                                          df[g] < 1e30f && full[g] == full[g];
                         ok[g] = ok[g] && gok;
                     }
-                    // every pair is stored (the exact pass rewrites the undecided ones); decided pairs are
-                    // counted by coarse level, except the two implicit bins
+                    // decided pairs are counted by coarse level (the undecided ones by the exact pass)
+                    if (lev) {
+#pragma unroll
+                        for (int g = 0; g < G; g++) {
+                            const int qi = 8 * cg + i0 + g;
+                            warp_level_hist(hb + qi * 2 * kLvEntries, uval && j * kScN + qi < nq && ok[g],
+                                            packed[g] & 15, packed[g] >> 4);
+                        }
+                    }
+                    // every pair is stored (the exact pass rewrites the undecided ones)
 #pragma unroll
                     for (int g = 0; g < G; g++) {
                         const int qi = 8 * cg + i0 + g, q = j * kScN + qi;
                         if (!uval || q >= nq) continue;
                         const int64_t o = (int64_t) q * a.n_user + u;
-                        if (lev) {
-                            a.lvc[o] = (uint8_t) packed[g];
-                            if (ok[g]) {
-                                const int c_l = packed[g] & 15, c_u = packed[g] >> 4;
-                                uint32_t *hq = hb + qi * 2 * (kLvEntries / 4);
-                                if (c_l != kLvEntries - 1) hist_add(hq, c_l, 1u);
-                                if (c_u != 0) hist_add(hq + kLvEntries / 4, c_u, 1u);
-                            }
-                        }
+                        if (lev) a.lvc[o] = (uint8_t) packed[g];
                         a.code[o] = (uint8_t) min(lo[g], a.nb);
                         if (a.dump) a.dump[o] = make_float2(full[g], df[g]);
                         und_bits |= (uint32_t) !ok[g] << (i0 + g);
@@ -451,26 +502,28 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                     }
                 }
             }
-            // every epilogue warp has counted this chunk: its histogram goes to the batch's (nonzero
-            // counters only) and is cleared for the chunk after next; every warp passes the same
-            // barriers, whether or not it gave up waiting
-            asm volatile("bar.sync 1, %0;" ::"n"(32 * kScEpiWarps) : "memory");
-            if (lev && tid < kScN * 2 * (kLvEntries / 4)) {
-                const uint32_t w = hb[tid];
-                if (w) {
-                    const int qi = tid / (2 * (kLvEntries / 4)), side = (tid / (kLvEntries / 4)) & 1;
+            // the four warps of this column group (one per lane quadrant: the same 8 queries) have
+            // counted this chunk: the group's histograms go to the batch's (nonzero counters only) and
+            // are cleared for the chunk after next; every warp passes the same barriers, whether or not
+            // it gave up waiting
+            asm volatile("bar.sync %0, 128;" ::"r"(1 + cg) : "memory");
+            if (lev)
+                for (int i = 8 * cg * 2 * kLvEntries + 32 * quad + lane; i < (8 * cg + 8) * 2 * kLvEntries; i += 128) {
+                    const uint32_t n = hb[i];
+                    if (!n) continue;
+                    hb[i] = 0u;
+                    const int qi = i / (2 * kLvEntries), side = (i / kLvEntries) & 1, bin = i % kLvEntries;
                     const int q = j * kScN + qi;
-                    int *gq = a.lhist + ((int64_t) q * 2 + side) * kLvEntries + 4 * (tid & (kLvEntries / 4 - 1));
-#pragma unroll
-                    for (int k = 0; k < 4; k++) {
-                        const uint32_t n = (w >> (8 * k)) & 0xffu;
-                        if (n && q < nq) atomicAdd(gq + k, (int) n);
-                    }
-                    hb[tid] = 0u;
+                    // the lower side's last coarse level and the upper side's first stay implicit
+                    if (q < nq && bin != (side ? 0 : kLvEntries - 1))
+                        atomicAdd(a.lhist + ((int64_t) q * 2 + side) * kLvEntries + bin, (int) n);
                 }
-            }
         }
         if (n_und) atomicAdd(a.undecided, n_und);
+        if (lane == 0 && (n_slo | n_sup)) {
+            atomicAdd(a.searches, 32 * n_slo);
+            atomicAdd(a.searches + 1, 32 * n_sup);
+        }
     }
     // all MMAs have completed once every epilogue warp has passed its last wait (or given up)
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -570,7 +623,7 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, bool *do
     if (n_tiles > 0x7fffffff) return RKR_OK;
     const size_t smem = (size_t) kScSlices * kp * (kScM + 2 * kScN) + sizeof(float) * ThrSummary::kMaxGroups * kScM +
                         sizeof(uint32_t) * kScListCap + (sizeof(float4) + sizeof(float)) * kScMaxQ +
-                        sizeof(uint32_t) * 2 * kScN * 2 * (kLvEntries / 4) +
+                        sizeof(uint32_t) * 2 * kScN * 2 * kLvEntries +
                         (call.qsrp ? sizeof(float2) * 2 * kLvEntries * kScM : 0);
     if (smem + 1024 > 227 * 1024) return RKR_OK;
     // user digits for this split (built once per split and kept)
@@ -609,13 +662,16 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, bool *do
     int2 *ovf = reinterpret_cast<int2 *>(take(sizeof(int2) * (size_t) ovf_cap));
     int2 *tile_rng = reinterpret_cast<int2 *>(take(sizeof(int2) * (size_t) n_launch * n_tiles));
     int2 *spill = reinterpret_cast<int2 *>(take(sizeof(int2) * (size_t) spill_cap));
-    int *counters = reinterpret_cast<int *>(take(64));  // ovf_count, status, undecided, (unused), spill
-    RKR_CUDA(cudaMemsetAsync(counters, 0, 5 * sizeof(int), st));
+    // ovf_count, status, undecided, (unused), spill, lower and upper table searches
+    int *counters = reinterpret_cast<int *>(take(64));
+    RKR_CUDA(cudaMemsetAsync(counters, 0, 7 * sizeof(int), st));
     if (call.status) {
-        // the caller reads the status and the undecided count later (the launches stay free of host
+        // the caller reads the status and the counts later (the launches stay free of host
         // synchronisation, so that they can be captured in a graph)
         call.status[0] = counters + 1;
         call.status[1] = counters + 2;
+        call.status[2] = counters + 5;
+        call.status[3] = counters + 6;
     }
     {
         const unsigned g = (unsigned) ((nq_pad * 32 + 255) / 256);
@@ -636,7 +692,6 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, bool *do
     a.thr_summ = ix->thr_summ.as<float>();
     a.m = call.m;
     a.lvt = call.qsrp ? ix->lvt.as<float2>() : nullptr;
-    a.G = call.qsrp ? lvt_stride(call.m.S) : 1;
     a.lvc = call.lvc;
     a.code = call.code;
     a.lhist = call.lhist;
@@ -646,6 +701,7 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, bool *do
     a.ovf_count = counters;
     a.status = counters + 1;
     a.undecided = counters + 2;
+    a.searches = counters + 5;
     a.ovf_cap = ovf_cap;
     a.spill = spill;
     a.spill_count = counters + 4;
@@ -697,10 +753,14 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, bool *do
     RKR_CUDA(cudaGetLastError());
     *done = true;
     if (call.status) return RKR_OK;
-    int h[3] = {0, 0, 0};
+    int h[7] = {0, 0, 0, 0, 0, 0, 0};
     RKR_CUDA(cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, st));
     RKR_CUDA(cudaStreamSynchronize(st));
-    if (ix->prof.on) ix->prof.add_count("screen_undecided_pairs", h[2]);
+    if (ix->prof.on) {
+        ix->prof.add_count("screen_undecided_pairs", h[2]);
+        ix->prof.add_count("lvt_search_lower_pairs", h[5]);
+        ix->prof.add_count("lvt_search_upper_pairs", h[6]);
+    }
     if (h[1]) {
         // a wait gave up or the overflow list filled: the exact tiles redo the batch from clean counts
         set_error("scores_tc: status %d", h[1]);

@@ -2,8 +2,8 @@
 // answers QS / QSRPNormalLP / US retrieval on a B200 through librkr_b200's C ABI (include/rkr.h).
 //
 // Header-only C++ meant to be compiled inside the reference's build (it uses the reference's
-// VectorMatrix, UserRankElement, SingleQueryPerformance, SampleSearch and SVD types and reads the
-// reference's own index files), linked with -lrkr_b200.  It mirrors the reference's factories
+// VectorMatrix, UserRankElement and SingleQueryPerformance types; the library reads the reference's
+// own index files), linked with -lrkr_b200.  It mirrors the reference's factories
 // (QS::BuildIndex, src/impl/QS.hpp:259-288; QSRPNormalLP::BuildIndex, src/impl/QSRPNormalLP.hpp:289-323;
 // US::BuildIndex, src/impl/US.hpp:226-242) and Index::Retrieval; errors throw std::runtime_error
 // where the reference would log and exit.
@@ -12,7 +12,6 @@
 
 #include <chrono>
 #include <cstdio>
-#include <fstream>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -24,37 +23,6 @@ namespace ReverseMIPS::B200 {
 
 inline void check(int status, const char *what) {
     if (status != RKR_OK) throw std::runtime_error(std::string(what) + ": " + rkr_last_error());
-}
-
-// NormalLinearRegressionLP index file (layout of NormalLinearRegressionLP::SaveIndex,
-// NormalLinearRegressionLP.hpp:419-446) -> sample ranks and [n_user][7] records.
-inline void read_regression_index(const char *index_dir, const char *dataset_name, int n_sample, int n_sample_query,
-                                  int sample_topk, std::vector<int32_t> &rank, std::vector<float> &records) {
-    char path[512];
-    std::snprintf(path, sizeof path,
-                  "%s/memory_index/NormalLinearRegressionLP-QS-%s-n_sample_%d-n_sample_query_%d-sample_topk_%d.index",
-                  index_dir, dataset_name, n_sample, n_sample_query, sample_topk);
-    std::ifstream in(path, std::ios::binary);
-    if (!in) throw std::runtime_error(std::string("cannot open ") + path);
-    size_t n_item = 0, n_user = 0;
-    int s = 0;
-    in.read((char *) &n_item, sizeof n_item);
-    in.read((char *) &n_user, sizeof n_user);
-    in.read((char *) &s, sizeof s);
-    rank.resize(s);
-    in.read((char *) rank.data(), sizeof(int) * (size_t) s);
-    std::vector<float> ab(2 * n_user), ms(2 * n_user), er(n_user), ex(2 * n_user);
-    in.read((char *) ab.data(), sizeof(float) * ab.size());
-    in.read((char *) ms.data(), sizeof(float) * ms.size());
-    in.read((char *) er.data(), sizeof(float) * er.size());
-    in.read((char *) ex.data(), sizeof(float) * ex.size());
-    if (!in) throw std::runtime_error(std::string("short read in ") + path);
-    records.resize(7 * n_user);
-    for (size_t u = 0; u < n_user; u++) {
-        float *r = &records[7 * u];
-        r[0] = ab[2 * u]; r[1] = ab[2 * u + 1]; r[2] = ms[2 * u]; r[3] = ms[2 * u + 1];
-        r[4] = er[u]; r[5] = ex[2 * u]; r[6] = ex[2 * u + 1];
-    }
 }
 
 class Index : public BaseIndex {
@@ -127,26 +95,12 @@ inline std::unique_ptr<Index> BuildIndex(const std::string &method, const Vector
                            user.vec_dim_, &h),
           "rkr_index_create");
     std::unique_ptr<Index> idx = std::make_unique<Index>(h, m, user.n_vector_);
-    // SampleSearch index written by bsibc (SampleSearch::SaveIndex, SampleSearch.hpp:158-197).
-    SampleSearch ss(index_dir, dataset_name, SampleSearchIndexName(method).c_str(), n_sample, true, m != RKR_METHOD_US,
-                    n_sample_query, sample_topk);
-    std::vector<float> thr((size_t) user.n_vector_ * n_sample);
-    for (int u = 0; u < user.n_vector_; u++)
-        std::copy(ss.SampleData(u), ss.SampleData(u) + n_sample, thr.begin() + (size_t) u * n_sample);
-    check(rkr_index_load_sample_search(h, ss.known_rank_idx_l_.get(), n_sample, thr.data()), "load_sample_search");
-    if (m != RKR_METHOD_US) {
-        SVD svd(index_dir, dataset_name);  // SVD::LoadIndex (SVD.hpp:258-292)
-        if (m == RKR_METHOD_QSRP_NORMAL_LP) {
-            check(rkr_index_load_svd(h, svd.check_dim_, svd.transfer_item_.getRawData(), svd.transfer_user_.getRawData()),
-                  "load_svd");
-            std::vector<int32_t> rank;
-            std::vector<float> rec;
-            read_regression_index(index_dir, dataset_name, n_sample, n_sample_query, sample_topk, rank, rec);
-            check(rkr_index_load_regression(h, rank.data(), (int32_t) rank.size(), rec.data()), "load_regression");
-        } else {
-            check(rkr_index_set_check_dim(h, svd.check_dim_), "set_check_dim");
-        }
-    }
+    // the files the reference's factory reads: the SampleSearch index (SampleSearch::LoadIndex,
+    // SampleSearch.hpp:199-244), the SVD index (SVD::LoadIndex, SVD.hpp:154-188) and the regression
+    // index (NormalLinearRegressionLP::LoadIndex, NormalLinearRegressionLP.hpp:448-487), read by the
+    // library from memory maps
+    check(rkr_index_load_files(h, m, index_dir, dataset_name, n_sample, n_sample_query, sample_topk),
+          "rkr_index_load_files");
     return idx;
 }
 

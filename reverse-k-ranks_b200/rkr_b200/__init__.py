@@ -39,7 +39,11 @@ EXPORTS = [
     "rkr_sort_kth_rank", "rkr_find_optimal_sample_rank", "rkr_uniform_sample_rank", "rkr_fit_regression",
     "rkr_svd_build", "rkr_profile_enable", "rkr_profile_read", "rkr_build_thresholds_static",
     "rkr_index_level_tables", "rkr_query", "rkr_query_device", "rkr_server_create", "rkr_server_submit",
-    "rkr_server_wait", "rkr_server_counters", "rkr_server_destroy", "rkr_score_estimates",
+    "rkr_server_wait", "rkr_server_counters", "rkr_server_destroy", "rkr_score_estimates", "rkr_index_shape",
+    "rkr_file_sample_search_info", "rkr_file_read_sample_search", "rkr_file_write_sample_search",
+    "rkr_file_regression_info", "rkr_file_read_regression", "rkr_file_write_regression", "rkr_file_svd_info",
+    "rkr_file_read_svd", "rkr_file_write_svd", "rkr_file_write_query_distribution",
+    "rkr_file_read_query_distribution", "rkr_index_load_files",
 ]
 
 
@@ -155,6 +159,82 @@ def build_thresholds_static(d_user, n_user, d_item, n_item, dim, sample_rank, d_
                                             C.c_void_p(d_thresholds), C.c_void_p(stream or 0)))
 
 
+# ---- index files (the reference's on-disk layouts) ------------------------------------------------------
+
+def _b(path):
+    return os.fsencode(path)
+
+
+def read_sample_search(path):
+    """SampleSearch::LoadIndex file -> (ranks, thresholds [n_user][n_sample] or None, n_item)."""
+    s, ni, nu, has = C.c_int32(), C.c_int64(), C.c_int64(), C.c_int32()
+    _check(_lib.rkr_file_sample_search_info(_b(path), C.byref(s), C.byref(ni), C.byref(nu), C.byref(has)))
+    rank = np.empty(s.value, np.int32)
+    thr = np.empty((nu.value, s.value), np.float32) if has.value else None
+    _check(_lib.rkr_file_read_sample_search(_b(path), _p(rank), _p(thr)))
+    return rank, thr, ni.value
+
+
+def write_sample_search(path, sample_rank, n_item, thresholds=None, n_user=None):
+    """SampleSearch::SaveIndex layout; thresholds None writes the ranks-only (qrs_to_sample_index) form."""
+    sr = _i32(sample_rank)
+    thr = None if thresholds is None else _f32(thresholds)
+    nu = thr.shape[0] if thr is not None else int(n_user or 0)
+    _check(_lib.rkr_file_write_sample_search(_b(path), _p(sr), C.c_int32(sr.shape[0]), C.c_int64(n_item),
+                                             C.c_int64(nu), _p(thr)))
+
+
+def read_regression(path):
+    """NormalLinearRegressionLP::LoadIndex file -> (ranks, records [n_user][7], n_item)."""
+    s, ni, nu = C.c_int32(), C.c_int64(), C.c_int64()
+    _check(_lib.rkr_file_regression_info(_b(path), C.byref(s), C.byref(ni), C.byref(nu)))
+    rank = np.empty(s.value, np.int32)
+    rec = np.empty((nu.value, 7), np.float32)
+    _check(_lib.rkr_file_read_regression(_b(path), _p(rank), _p(rec)))
+    return rank, rec, ni.value
+
+
+def write_regression(path, sample_rank, records, n_item):
+    sr, rec = _i32(sample_rank), _f32(records)
+    _check(_lib.rkr_file_write_regression(_b(path), _p(sr), C.c_int32(sr.shape[0]), C.c_int64(n_item),
+                                          C.c_int64(rec.shape[0]), _p(rec)))
+
+
+def read_svd(path, with_items=False):
+    """SVD::LoadIndex file -> dict(transfer_item, svd_user, svd_item or None, check_dim, sigma, n_item)."""
+    nu, ni, d, sg, cd = C.c_int64(), C.c_int64(), C.c_int32(), C.c_float(), C.c_int32()
+    _check(_lib.rkr_file_svd_info(_b(path), C.byref(nu), C.byref(ni), C.byref(d), C.byref(sg), C.byref(cd)))
+    ti = np.empty((d.value, d.value), np.float32)
+    su = np.empty((nu.value, d.value), np.float32)
+    si = np.empty((ni.value, d.value), np.float32) if with_items else None
+    _check(_lib.rkr_file_read_svd(_b(path), _p(ti), _p(su), _p(si)))
+    return dict(transfer_item=ti, svd_user=su, svd_item=si, check_dim=cd.value, sigma=sg.value, n_item=ni.value)
+
+
+def write_svd(path, transfer_item, svd_user, check_dim, n_item, sigma=0.7, svd_item=None):
+    ti, su = _f32(transfer_item), _f32(svd_user)
+    si = None if svd_item is None else _f32(svd_item)
+    _check(_lib.rkr_file_write_svd(_b(path), C.c_int64(su.shape[0]), C.c_int64(n_item), C.c_int32(su.shape[1]),
+                                   C.c_float(sigma), C.c_int32(check_dim), _p(ti), _p(su), _p(si)))
+
+
+def write_query_distribution(dirname, sample_item, sort_kth_rank, sort_sample_id, accu):
+    """WriteDistributionBelowTopk's directory from the build steps' outputs (accu in sample order)."""
+    si, sk, sid, acc = _i32(sample_item), _i32(sort_kth_rank), _i32(sort_sample_id), _i32(accu)
+    _check(_lib.rkr_file_write_query_distribution(_b(dirname), _p(si), _p(sk), _p(sid), _p(acc),
+                                                  C.c_int32(si.shape[0]), C.c_int64(acc.shape[1] - 1)))
+
+
+def read_query_distribution(dirname, n_sample_item, n_item):
+    """-> (sampled item ids, sorted k-th ranks, accu rows), all in the files' (sorted-sample) order."""
+    si = np.empty(n_sample_item, np.int32)
+    sk = np.empty(n_sample_item, np.int32)
+    acc = np.empty((n_sample_item, n_item + 1), np.int32)
+    _check(_lib.rkr_file_read_query_distribution(_b(dirname), C.c_int32(n_sample_item), C.c_int64(n_item), _p(si),
+                                                 _p(sk), _p(acc)))
+    return si, sk, acc
+
+
 # ---- the device index ---------------------------------------------------------------------------------------
 
 class Index:
@@ -219,6 +299,13 @@ class Index:
     def reset_state(self):
         _check(_lib.rkr_index_reset_state(self._h))
 
+    def load_files(self, method, index_dir, dataset_name, n_sample, n_sample_query=0, sample_topk=0):
+        """The file set the reference's factories read (rkr_index_load_files)."""
+        m = METHODS[method] if isinstance(method, str) else int(method)
+        _check(_lib.rkr_index_load_files(self._h, C.c_int32(m), _b(index_dir), _b(dataset_name), C.c_int32(n_sample),
+                                         C.c_int32(n_sample_query), C.c_int32(sample_topk)))
+        self.n_sample = n_sample
+
     def score_estimates(self, method, query):
         """The tensor-core pair scores' estimates and bounds (rkr_score_estimates): [n_query][n_user][2]."""
         m = METHODS[method] if isinstance(method, str) else int(method)
@@ -228,12 +315,12 @@ class Index:
         return out
 
     def level_tables(self):
-        """The regression models' level-boundary tables (rkr_index_level_tables): (stride G, array
+        """The regression models' level-boundary tables (rkr_index_level_tables): (levels L_g [16], array
         [n_user][2][16][2] of (boundary score, guard band))."""
-        g = C.c_int32()
+        lv = np.zeros(16, np.int32)
         out = np.empty((self.n_user, 2, 16, 2), np.float32)
-        _check(_lib.rkr_index_level_tables(self._h, C.byref(g), _p(out)))
-        return g.value, out
+        _check(_lib.rkr_index_level_tables(self._h, _p(lv), _p(out)))
+        return lv, out
 
     def size_bytes(self):
         v = C.c_uint64()

@@ -144,6 +144,14 @@ class Oracle:
             lb[i], ub[i] = l.value, h.value
         return lb, ub
 
+    def level_boundaries_at(self, rec, sample_rank, n_item, levels, side):
+        """orc_level_boundaries_at: the smallest score whose rank-bound level is <= levels[g]."""
+        rec, sr, lv = _f32(rec), _i32(sample_rank), _i32(levels)
+        out = np.empty(lv.shape[0], np.float32)
+        self.lib.orc_level_boundaries_at(_p(rec), _p(sr), C.c_int32(sr.shape[0]), C.c_int64(n_item), _p(lv),
+                                         C.c_int32(side), C.c_int32(lv.shape[0]), _p(out))
+        return out
+
     def level_boundaries(self, rec, sample_rank, n_item, stride, side, n_out):
         """orc_level_boundaries: the smallest score whose rank-bound level is <= g * stride."""
         rec, sr = _f32(rec), _i32(sample_rank)

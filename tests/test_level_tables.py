@@ -2,8 +2,9 @@
 
 The device builds, per user and side, the smallest binary32 score T_g whose level (the reference's
 ComputeRankBound, NormalLinearRegressionLP.hpp:326-380, lower bound of qlb / upper bound of qub) is
-<= g G, and a guard band around it (reverse-k-ranks_b200/csrc/rkr_levels.cu); a score's coarse level
-ceil(level / G) is then decided from the table wherever the score stays outside the bands.  Here:
+<= L_g (L_0 = 0, 14 steps to S, L_15 = S + 1), and a guard band around it
+(reverse-k-ranks_b200/csrc/rkr_levels.cu); a score's coarse level (the smallest g with level <= L_g)
+is then decided from the table wherever the score stays outside the bands.  Here:
 
 * the band's premise: the reference's binary32 model value a CDFPhi((q - mu) / sigma) + b +- err
   differs from the same formula evaluated without roundings by less than a third of the margin the
@@ -24,8 +25,14 @@ from checkers import Oracle
 E = 16  # table entries per side
 
 
-def stride(S):
-    return (S + 1 + E - 2) // (E - 1)
+def table_levels(S):
+    """L_g: 0, then ceil(g S / 14) up to S, then S + 1 (lvt_level)."""
+    return np.array([(g * S + E - 3) // (E - 2) for g in range(E - 1)] + [S + 1], np.int32)
+
+
+def coarse(lv, S):
+    """The smallest g with lv <= L_g (lvt_coarse)."""
+    return int(np.searchsorted(table_levels(S), lv, side="left"))
 
 
 A1, A2, A3, A4, A5, P = (float(np.float32(v)) for v in (0.254829592, -0.284496736, 1.421413741, -1.453152027,
@@ -59,19 +66,19 @@ def level(orc, rec, rank, n_item, q, side):
 def build_tables(orc, rec, rank, n_item):
     """The device's tables for one user, restated: [(T_g, band_g)] per side."""
     S = len(rank)
-    G = stride(S)
+    L = table_levels(S)
     capped = float(rec[4]) >= S - 1e-3
     out = []
     for side in (0, 1):
-        T = orc.level_boundaries(rec, rank, n_item, G, side, E)
+        T = orc.level_boundaries_at(rec, rank, n_item, L, side)
         T[E - 1] = -np.inf
         bands = np.zeros(E, np.float32)
         for g in range(E - 1):
-            if g * G >= S + 1:
+            if L[g] >= S + 1:
                 T[g] = -np.inf
             if not np.isfinite(T[g]) or capped:
                 continue
-            n = g * G if side else g * G - 1
+            n = int(L[g]) if side else int(L[g]) - 1
             m = model_margin(rec)
             smin, smax = float(rec[6]), float(rec[5])
             f = lambda q: model_value(rec, side == 1, q)
@@ -169,7 +176,6 @@ def test_table_screen_decides_the_oracle_coarse_level(S, n_item):
     orc = Oracle()
     rng = np.random.default_rng(S)
     rank, recs = users(orc, rng, S, n_item)
-    G = stride(S)
     for rec in recs:
         tabs = build_tables(orc, rec, rank, n_item)
         for side in (0, 1):
@@ -188,7 +194,7 @@ def test_table_screen_decides_the_oracle_coarse_level(S, n_item):
                     continue
                 decided += 1
                 lv = level(orc, rec, rank, n_item, float(q), side)
-                assert c == (lv + G - 1) // G, (side, float(q), c, lv)
+                assert c == coarse(lv, S), (side, float(q), c, lv)
             assert decided > len(probes) // 3
 
 
@@ -236,8 +242,8 @@ def test_device_tables_match_the_restatement():
     item = rng.standard_normal((n_item, d)).astype(np.float32)
     with rkr_b200.Index(user, item) as ix:
         ix.load_regression(rank, recs)
-        G, tab = ix.level_tables()
-    assert G == stride(S)
+        levels, tab = ix.level_tables()
+    assert np.array_equal(levels, table_levels(S))
     for u, rec in enumerate(recs):
         want = build_tables(orc, rec, rank, n_item)
         for side in (0, 1):

@@ -479,7 +479,19 @@ inline cudaError_t launch_big(const float *A, const int32_t *a_idx, int64_t n_a,
 }
 
 // Sequential binary32 dot product of one pair (thread-serial), same arithmetic as exact_tile.
+__device__ __forceinline__ void prefetch_l1(const void *p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
 __device__ __forceinline__ float exact_dot(const float *__restrict__ a, const float *__restrict__ b, int n) {
+    // every 128-byte line of both rows requested up front, so that the ordered sum below waits for
+    // one memory latency instead of one per line
+    for (int o = 0; o < n; o += 32) {
+        prefetch_l1(a + o);
+        prefetch_l1(b + o);
+    }
+    if (n > 0) {
+        prefetch_l1(a + n - 1);
+        prefetch_l1(b + n - 1);
+    }
     float acc = 0.0f;
     int j = 0;
     if (((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b)) & 7) == 0) {
@@ -900,18 +912,15 @@ __global__ void __launch_bounds__(kCompactThreads) compact_emit_kernel(P p, KSpe
     for (int t0 = 0; t0 < n; t0 += kCompactThreads) {
         const int i = t0 + tid;
         const int64_t u = i < n ? s[i] : 0;
+        // classified once, with the data its emission needs (a user classified here is emitted
+        // unless it is a result past the query's k)
         typename P::Aux aux;
-        const int k = i < n ? p.classify(q, u, aux, false) : 0;
+        const int k = i < n ? p.classify(q, u, aux, true) : 0;
         int tot;
         const int pre = block_excl_scan((k == 1) | ((k == 2) << 16), warp_tot, &tot);
         const int rpos = pr + (pre & 0xffff), cpos = pc + (pre >> 16);
-        if (k == 1 && rpos < topk) {
-            p.classify(q, u, aux, true);
-            p.emit_result(q, rpos, u, aux);
-        } else if (k == 2) {
-            p.classify(q, u, aux, true);
-            p.emit_cand(q, cpos, u, aux);
-        }
+        if (k == 1 && rpos < topk) p.emit_result(q, rpos, u, aux);
+        else if (k == 2) p.emit_cand(q, cpos, u, aux);
         pr += tot & 0xffff;
         pc += tot >> 16;
     }

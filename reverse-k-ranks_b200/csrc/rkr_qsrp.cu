@@ -510,17 +510,36 @@ __global__ void __launch_bounds__(256) qsrp_fine1_scan_kernel(uint8_t *__restric
             while ((q + 1) * n_user <= base) q++;
             int64_t edge = (q + 1) * n_user;
             int wl = par[q].w_l, wu = par[q].w_u, wa = par[q].w_all;
+            if (base + 16 <= edge && base + 16 <= total) {
+                // the lane's 16 pairs in one query row: four bytes at a time, the nibbles compared in
+                // parallel (a byte of t = nibbles ^ wanted is below 0x20, so t + 0x7f keeps its carry
+                // inside the byte: bit 7 is set exactly where the nibble differs)
+                if (wa) {
+                    hits = 0xffffu;
+                } else {
+                    const uint32_t ml = (uint32_t) (wl >= 0 ? wl : 16) * 0x01010101u;
+                    const uint32_t mu = (uint32_t) (wu >= 0 ? wu : 16) * 0x01010101u;
 #pragma unroll
-            for (int e = 0; e < 16; e++) {
-                const int64_t pos = base + e;
-                if (pos >= total) break;
-                if (pos >= edge) {  // the next query (and the one after, for short rows)
-                    while ((q + 1) * n_user <= pos) q++;
-                    edge = (q + 1) * n_user;
-                    wl = par[q].w_l; wu = par[q].w_u; wa = par[q].w_all;
+                    for (int i = 0; i < 4; i++) {
+                        const uint32_t tl = (w[i] & 0x0f0f0f0fu) ^ ml, tu = ((w[i] >> 4) & 0x0f0f0f0fu) ^ mu;
+                        const uint32_t diff = ((tl + 0x7f7f7f7fu) & (tu + 0x7f7f7f7fu)) & 0x80808080u;
+                        const uint32_t eq = diff ^ 0x80808080u;  // bit 7 of each byte: a nibble matches
+                        hits |= ((eq * 0x00204081u) >> 28) << (4 * i);
+                    }
                 }
-                const unsigned v = (w[e >> 2] >> (8 * (e & 3))) & 0xffu;
-                hits |= (uint32_t) (wa || (int) (v & 15) == wl || (int) (v >> 4) == wu) << e;
+            } else {
+#pragma unroll
+                for (int e = 0; e < 16; e++) {
+                    const int64_t pos = base + e;
+                    if (pos >= total) break;
+                    if (pos >= edge) {  // the next query (and the one after, for short rows)
+                        while ((q + 1) * n_user <= pos) q++;
+                        edge = (q + 1) * n_user;
+                        wl = par[q].w_l; wu = par[q].w_u; wa = par[q].w_all;
+                    }
+                    const unsigned v = (w[e >> 2] >> (8 * (e & 3))) & 0xffu;
+                    hits |= (uint32_t) (wa || (int) (v & 15) == wl || (int) (v >> 4) == wu) << e;
+                }
             }
         }
         if (n_hits) {
@@ -684,8 +703,10 @@ __global__ void __launch_bounds__(kHistThreads) qsrp_round2_kernel(const uint8_t
                                                                   uint8_t *__restrict__ code, int64_t n_user,
                                                                   const QsrpParams *__restrict__ par, int nb,
                                                                   int64_t chunk, int *__restrict__ hist_c) {
+    // per-thread counts, bin-major ([bin][thread]): a thread's counters sit in its own bank, so the
+    // increments of a warp never conflict and need no atomics
     extern __shared__ int h[];
-    const int nbin = nb + 1, copies = hist_copies(nbin);
+    const int nbin = nb + 1, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int q = blockIdx.y;
     QsrpParams p;
     {
@@ -693,33 +714,58 @@ __global__ void __launch_bounds__(kHistThreads) qsrp_round2_kernel(const uint8_t
         p.mode1 = g.mode1; p.all1 = g.all1; p.c_res = g.c_res; p.c_pr = g.c_pr; p.c_m1 = g.c_m1;
     }
     const bool all_survive = lvc == nullptr;  // QS and US: no round 1
-    for (int b = threadIdx.x; b < copies * nbin; b += blockDim.x) h[b] = 0;
-    __syncthreads();
-    int *mine = h + ((threadIdx.x >> 5) % copies) * nbin;
+    // The common classes of round 1 four bytes at a time (nibbles n < 16, so n + k with k <= 0x80
+    // keeps its carry inside the byte): cl > c_res is bit 7 of cl + 0x7f - c_res, cu >= c_pr bit 7 of
+    // cu + 0x80 - c_pr, and a zero low nibble marks a pair the fine pass resolved.  Bytes flagged by
+    // any of the three take class1_coarse; the others are round-2 survivors.
+    const bool swar = !all_survive && !p.mode1 && !p.all1;
+    const uint32_t kres = (uint32_t) (0x7f - p.c_res) * 0x01010101u;
+    const uint32_t kpr = (uint32_t) (0x80 - p.c_pr) * 0x01010101u;
+    for (int b = 0; b < nbin; b++) h[b * kHistThreads + tid] = 0;
     const uint8_t *lrow = lvc ? lvc + (int64_t) q * n_user : nullptr;
     uint8_t *crow = code + (int64_t) q * n_user;
     const int64_t u0 = (int64_t) blockIdx.x * chunk, u1 = min(u0 + chunk, n_user);
     // 16 consecutive users per thread and step, their bytes from five aligned words per row
-    for (int64_t ub = u0 + (int64_t) threadIdx.x * 16; ub < u1; ub += (int64_t) kHistThreads * 16) {
+    for (int64_t ub = u0 + (int64_t) tid * 16; ub < u1; ub += (int64_t) kHistThreads * 16) {
         const int n = (int) min((int64_t) 16, u1 - ub);
         uint32_t lw[4] = {0u, 0u, 0u, 0u}, cw[4];
         if (!all_survive) load16_bytes(lrow + ub, lw);
         load16_bytes(crow + ub, cw);
+        uint32_t flag = 0;  // bytes whose class takes class1_coarse
+        if (swar) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const uint32_t lo = lw[i] & 0x0f0f0f0fu, hi = (lw[i] >> 4) & 0x0f0f0f0fu;
+                const uint32_t le_res = ((lo + kres) & 0x80808080u) ^ 0x80808080u;
+                const uint32_t ge_pr = (hi + kpr) & 0x80808080u;
+                const uint32_t zero = ((lo + 0x7f7f7f7fu) & 0x80808080u) ^ 0x80808080u;
+                flag |= (((le_res | ge_pr | zero) * 0x00204081u) >> 28) << (4 * i);
+            }
+        } else if (!all_survive) {
+            flag = 0xffffu;
+        }
+        flag &= n >= 16 ? 0xffffu : (1u << n) - 1u;
 #pragma unroll
         for (int e = 0; e < 16; e++) {
             if (e >= n) break;
-            const unsigned v = (lw[e >> 2] >> (8 * (e & 3))) & 0xffu, c = (cw[e >> 2] >> (8 * (e & 3))) & 0xffu;
-            const int k = all_survive ? kClsRefine : class1_coarse(p, v);
-            if (k == kClsRefine || k == kClsIdle) atomicAdd(mine + c, 1);
-            else crow[ub + e] = k == kClsResult ? kCodeResult1 : kCodePruned1;
+            const unsigned c = (cw[e >> 2] >> (8 * (e & 3))) & 0xffu;
+            bool surv = true;
+            if ((flag >> e) & 1u) {
+                const unsigned v = (lw[e >> 2] >> (8 * (e & 3))) & 0xffu;
+                const int k = class1_coarse(p, v);
+                surv = k == kClsRefine || k == kClsIdle;
+                if (!surv) crow[ub + e] = k == kClsResult ? kCodeResult1 : kCodePruned1;
+            }
+            if (surv) h[min(c, (unsigned) nb) * kHistThreads + tid]++;  // codes are 0 .. nb here
         }
     }
     __syncthreads();
     int *gh = hist_c + (int64_t) q * nbin;
-    for (int b = threadIdx.x; b < nbin; b += blockDim.x) {
+    for (int b = warp; b < nbin; b += kHistThreads / 32) {
         int sum = 0;
-        for (int c = 0; c < copies; c++) sum += h[c * nbin + b];
-        if (sum) atomicAdd(gh + b, sum);
+        for (int t = lane; t < kHistThreads; t += 32) sum += h[b * kHistThreads + t];
+        sum = __reduce_add_sync(0xffffffffu, sum);
+        if (lane == 0 && sum) atomicAdd(gh + b, sum);
     }
 }
 
@@ -1054,11 +1100,29 @@ struct QsrpCompactPolicy {
         uint32_t w[4];
         load16_bytes(code + (int64_t) q * n_user + u, w);
         uint32_t m = 0;
+        if ((gneed & (gneed + 1)) == 0) {
+            // the needed groups are 0 .. gmax (the classes rise with the group): four codes at a time.
+            // A byte's (c | 0x80) - (gmax + 1) stays inside the byte, bit 7 set exactly when c > gmax;
+            // kCodeResult1 is found as a zero byte of c ^ 0xfe; with state_any every code above nb
+            // (the two round-1 codes, bit 7 set) is needed too
+            const int gmax1 = __popcll(gneed);  // gmax + 1
+            const uint32_t g1 = (uint32_t) gmax1 * 0x01010101u;
 #pragma unroll
-        for (int e = 0; e < kCompactPer; e++) {
-            const unsigned c = (w[e >> 2] >> (8 * (e & 3))) & 0xff;
-            const bool nd = c <= (unsigned) nb ? (bool) (gneed >> c & 1) : (c == kCodeResult1 || state_any);
-            m |= (uint32_t) nd << e;
+            for (int i = 0; i < 4; i++) {
+                const uint32_t x = w[i];
+                const uint32_t le = (((x | 0x80808080u) - g1) & 0x80808080u) ^ 0x80808080u;
+                const uint32_t t = x ^ 0xfefefefeu;
+                const uint32_t fe = ~(((t & 0x7f7f7f7fu) + 0x7f7f7f7fu) | t) & 0x80808080u;
+                const uint32_t nd = le | fe | (state_any ? (x & 0x80808080u) : 0u);
+                m |= ((nd * 0x00204081u) >> 28) << (4 * i);
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < kCompactPer; e++) {
+                const unsigned c = (w[e >> 2] >> (8 * (e & 3))) & 0xff;
+                const bool nd = c <= (unsigned) nb ? (bool) (gneed >> c & 1) : (c == kCodeResult1 || state_any);
+                m |= (uint32_t) nd << e;
+            }
         }
         return n >= 32 ? m : m & ((1u << n) - 1);
     }
@@ -1391,7 +1455,7 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
                 RKR_CUDA(cudaGetLastError());
             }
         }
-        const int64_t chunk = 16384;
+        const int64_t chunk = 65536;  // users per round-2 block (its per-thread counters are set up once)
         dim3 hg((unsigned) ((U + chunk - 1) / chunk), (unsigned) nq);
         if (qsrp) {
             timed(ix, st, "qsrp_select1c", [&] {
@@ -1434,8 +1498,8 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
             RKR_CUDA(cudaGetLastError());
         }
         timed(ix, st, "qsrp_round2", [&] {
-            qsrp_round2_kernel<<<hg, kHistThreads, hist_copies(nb + 1) * (nb + 1) * sizeof(int), st>>>(
-                lvc, code, U, par, nb, chunk, hist_c);
+            qsrp_round2_kernel<<<hg, kHistThreads, (nb + 1) * kHistThreads * sizeof(int), st>>>(lvc, code, U, par, nb,
+                                                                                              chunk, hist_c);
         });
         RKR_CUDA(cudaGetLastError());
         timed(ix, st, "qsrp_select2c", [&] {

@@ -83,6 +83,8 @@ struct ScArgs {
 // exact_dot with the first operand in shared or global memory (generic loads; __ldg would not
 // accept a shared-memory address).
 __device__ __forceinline__ float exact_dot_any(const float *a, const float *__restrict__ b, int n) {
+    for (int o = 0; o < n; o += 32) prefetch_l1(b + o);  // the second row's lines, requested up front
+    if (n > 0) prefetch_l1(b + n - 1);
     float acc = 0.0f;
     int j = 0;
     if (((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b)) & 7) == 0) {
@@ -141,20 +143,37 @@ __device__ __forceinline__ void exact_pair(const ScArgs &a, int64_t u, int q, co
 }
 
 // Counts one query column of a warp's pairs by coarse level into the chunk's shared-memory histogram
-// h ([2 sides][kLvEntries]).  Pairs at both implicit levels (the lower side's last, the upper side's
-// 0: most pairs) are not counted; the others are grouped by their two levels, and one lane of each
-// group adds the group's size -- one atomic per distinct pair of levels instead of one per pair (the
-// lanes of a warp mostly share their levels).
+// h ([2 sides][kLvEntries]).  The lanes' levels are balloted bit by bit; lane l then counts the lanes
+// whose lower level (l < 16) or upper level (l >= 16) is l % 16 -- the AND of the four bit masks or
+// their complements -- and adds that count: every bin of both sides in one pass, one shared-memory
+// atomic per occupied bin.  The lower side's last level and the upper side's level 0 stay implicit.
 __device__ __forceinline__ void warp_level_hist(uint32_t *h, bool count, int cl, int cu) {
-    const bool part = count && !(cl == kLvEntries - 1 && cu == 0);
-    const unsigned pm = __ballot_sync(0xffffffffu, part);
-    if (!part) return;
-    const unsigned m = __match_any_sync(pm, cl | (cu << 4));
-    if ((threadIdx.x & 31) == __ffs(m) - 1) {
-        const uint32_t n = (uint32_t) __popc(m);
-        if (cl != kLvEntries - 1) atomicAdd(h + cl, n);
-        if (cu != 0) atomicAdd(h + kLvEntries + cu, n);
+    const unsigned v = __ballot_sync(0xffffffffu, count);
+    if (v == 0u) return;
+    const int lane = threadIdx.x & 31, bin = lane & 15;
+    unsigned m = v;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const unsigned bl = __ballot_sync(0xffffffffu, (cl >> k) & 1), bu = __ballot_sync(0xffffffffu, (cu >> k) & 1);
+        const unsigned b = lane < 16 ? bl : bu;
+        m &= ((bin >> k) & 1) ? b : ~b;
     }
+    const int n = __popc(m);
+    const bool implicit = lane < 16 ? bin == kLvEntries - 1 : bin == 0;
+    if (n && !implicit) atomicAdd(h + lane, (uint32_t) n);
+}
+
+// The bound scores of the regression round, qlb = partial - right and qub = partial + right
+// (PartDimPartNorm::IPBound), and their distances to the reference's binary32 values: the partial
+// score's bound and each side's two roundings.
+__device__ __forceinline__ void level_bounds(float vl, float dl, float un, float qn, float &qlb, float &qub,
+                                             float &dql, float &dqu) {
+    const float right = __fmul_rn(un, qn);
+    qlb = __fsub_rn(vl, right);
+    qub = __fadd_rn(vl, right);
+    const float dq = dl * 1.0001f;
+    dql = fmaf(fabsf(qlb), 2.4e-7f, dq);
+    dqu = fmaf(fabsf(qub), 2.4e-7f, dq);
 }
 
 __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
@@ -209,9 +228,9 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                                                      : make_float2(NAN, NAN);
         }
     for (int i = tid; i < 2 * kScN * 2 * kLvEntries; i += kScThreads) shist[i] = 0u;
-    for (int i = tid; i < nq; i += kScThreads) {
-        sq[i] = __ldg(a.qmeta + i);
-        sqn[i] = lev ? __ldg(a.qnorm + i) : 0.0f;
+    for (int i = tid; i < nchunks * kScN; i += kScThreads) {  // the last chunk padded with the last query
+        sq[i] = __ldg(a.qmeta + min(i, nq - 1));
+        sqn[i] = lev ? __ldg(a.qnorm + min(i, nq - 1)) : 0.0f;
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -297,21 +316,27 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
         const float2 *tl = stab + row, *tu = stab + kLvEntries * kScM + row;  // entry j at t[j * kScM]
         float un = 0.0f;
         float4 um = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        // the common cases of the two sides in registers: the lower side's last coarse level (scores
-        // surely below T_(E-2) - band) and the upper side's level 0 (scores surely at or above T_0 + band)
-        // and the upper side's first four boundaries (coarse levels 0 .. 3 hold most of its pairs) as
-        // (T - band, T + band), so that those pairs need no table search
-        float lo_last = -INFINITY;
-        float ulo[4], uhi[4];
+        // the common cases of the two sides in registers, as (T - band, T + band) rounded outward: the
+        // lower side's last three boundaries T_12 .. T_14 (coarse levels 13 .. 15 hold all but about
+        // 0.1% of its pairs at config 2) and the upper side's first four T_0 .. T_3 (coarse levels 0 .. 3
+        // hold about 94% of its pairs), so that those pairs need no table search
+        float llo[3], lhi[3], ulo[4], uhi[4];
+#pragma unroll
+        for (int g = 0; g < 3; g++) { llo[g] = -INFINITY; lhi[g] = INFINITY; }
 #pragma unroll
         for (int g = 0; g < 4; g++) { ulo[g] = -INFINITY; uhi[g] = INFINITY; }
         if (uval) {
             um = __ldg(a.umeta + u);
             if (lev) {
                 un = __ldg(a.unorm + u);
-                const float2 el = tl[(kLvEntries - 2) * kScM];
-                lo_last = __fsub_rd(el.x, el.y);
-                if (!(lo_last == lo_last)) lo_last = -INFINITY;   // NaN entries: never the fast path
+                // NaN entries (an unusable model): never decided from registers
+#pragma unroll
+                for (int g = 0; g < 3; g++) {
+                    const float2 e = tl[(kLvEntries - 4 + g) * kScM];
+                    llo[g] = __fsub_rd(e.x, e.y);
+                    lhi[g] = __fadd_ru(e.x, e.y);
+                    if (!(llo[g] == llo[g]) || !(lhi[g] == lhi[g])) { llo[g] = -INFINITY; lhi[g] = INFINITY; }
+                }
 #pragma unroll
                 for (int g = 0; g < 4; g++) {
                     const float2 e = tu[g * kScM];
@@ -377,7 +402,7 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
 #pragma unroll
                     for (int g = 0; g < G; g++) {
                         const int i = i0 + g;
-                        const float4 qm = sq[min(j * kScN + 8 * cg + i, nq - 1)];
+                        const float4 qm = sq[j * kScN + 8 * cg + i];
                         const float scale = __int_as_float((ue + __float_as_int(qm.w) - 35 + 127) << 23);
                         vl[g] = sl[i] * scale;
                         const float ee = um.x * qm.x;
@@ -392,19 +417,26 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                     if (lev) {
                         // coarse levels of the bounds partial -+ right (PartDimPartNorm::IPBound) from the
                         // tables; within dq of the reference's bound scores: the partial score's bound and
-                        // the two roundings of each side
+                        // the two roundings of each side.  The register-cached boundaries decide most pairs
+                        // without branches; the table searches run afterwards, for the whole warp, where
+                        // any lane's pair needs one
+                        unsigned needl = 0, needu = 0;
 #pragma unroll
                         for (int g = 0; g < G; g++) {
-                            const float right = __fmul_rn(un, sqn[min(j * kScN + 8 * cg + i0 + g, nq - 1)]);
-                            const float qlb = __fsub_rn(vl[g], right), qub = __fadd_rn(vl[g], right);
-                            const float dq = dl[g] * 1.0001f;
-                            const float dql = fmaf(fabsf(qlb), 2.4e-7f, dq), dqu = fmaf(fabsf(qub), 2.4e-7f, dq);
-                            int c_l = kLvEntries - 1, c_u = 0;
-                            bool okl = __fadd_ru(qlb, dql) < lo_last;
-                            // upper side from the cached boundaries: coarse level = boundaries surely
-                            // above the score, decided when none of the four is within reach and the
-                            // level is below 4
-                            bool oku;
+                            float qlb, qub, dql, dqu;
+                            level_bounds(vl[g], dl[g], un, sqn[j * kScN + 8 * cg + i0 + g], qlb, qub, dql, dqu);
+                            // lower side: coarse level 15 below T_14, 14 between T_14 and T_13, 13 between
+                            // T_13 and T_12, each surely (outside the bands)
+                            int c_l, c_u;
+                            bool okl, oku;
+                            {
+                                const float qml = __fsub_rd(qlb, dql), qpl = __fadd_ru(qlb, dql);
+                                const bool b14 = qpl < llo[2], b13 = qpl < llo[1], b12 = qpl < llo[0];
+                                okl = b14 || (qml >= lhi[2] && b13) || (qml >= lhi[1] && b12);
+                                c_l = b14 ? 15 : (b13 ? 14 : 13);
+                            }
+                            // upper side: coarse level = boundaries surely above the score, decided when
+                            // none of the four is within reach and the level is below 4
                             {
                                 const float qm = __fsub_rd(qub, dqu), qp = __fadd_ru(qub, dqu);
                                 int below = 0;
@@ -418,39 +450,60 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                                 c_u = below;
                                 oku = !amb && below < 4;
                             }
-                            // the searches run for the whole warp when any lane needs them (no divergence)
-                            if (__any_sync(0xffffffffu, !okl)) {
-                                n_slo++;
-                                int c;
-                                const bool o = lvt_screen(tl, kScM, qlb, dql, c);
-                                if (!okl) { okl = o; c_l = c; }
-                            }
-                            if (__any_sync(0xffffffffu, !oku)) {
-                                n_sup++;
-                                int c;
-                                const bool o = lvt_screen(tu, kScM, qub, dqu, c);
-                                if (!oku) { oku = o; c_u = c; }
-                            }
-                            ok[g] = okl && oku;
+                            needl |= (unsigned) !okl << g;
+                            needu |= (unsigned) !oku << g;
                             packed[g] = c_l | (c_u << 4);
                         }
+                        if (__any_sync(0xffffffffu, (needl | needu) != 0u)) {
+#pragma unroll
+                            for (int g = 0; g < G; g++) {
+                                const bool wl = (needl >> g) & 1u, wu = (needu >> g) & 1u;
+                                const bool sl_any = __any_sync(0xffffffffu, wl), su_any = __any_sync(0xffffffffu, wu);
+                                if (!(sl_any || su_any)) continue;
+                                float qlb, qub, dql, dqu;
+                                level_bounds(vl[g], dl[g], un, sqn[j * kScN + 8 * cg + i0 + g], qlb, qub, dql, dqu);
+                                if (sl_any) {
+                                    n_slo++;
+                                    int c;
+                                    const bool o = lvt_screen(tl, kScM, qlb, dql, c);
+                                    if (wl) {
+                                        packed[g] = (packed[g] & 0xf0) | c;
+                                        if (o) needl &= ~(1u << g);
+                                    }
+                                }
+                                if (su_any) {
+                                    n_sup++;
+                                    int c;
+                                    const bool o = lvt_screen(tu, kScM, qub, dqu, c);
+                                    if (wu) {
+                                        packed[g] = (packed[g] & 0x0f) | (c << 4);
+                                        if (o) needu &= ~(1u << g);
+                                    }
+                                }
+                            }
+                        }
+#pragma unroll
+                        for (int g = 0; g < G; g++) ok[g] = !(((needl | needu) >> g) & 1u);
                     }
-                    // coarse group: the summary entries >= full (a five-step search and one compare)
+                    // coarse group: the summary entries >= full.  The search runs on key = full + df:
+                    // with lo entries >= key, the pair is decided when the next entry lies below
+                    // full - df, and then exactly lo entries are >= full (the entries descend)
                     int lo[G];
+                    float key[G];
 #pragma unroll
                     for (int g = 0; g < G; g++) {
-                        lo[g] = s15 >= full[g] ? 16 : 0;
-                        lo[g] += (lo[g] ? s23 : s7) >= full[g] ? 8 : 0;
+                        key[g] = full[g] + df[g];
+                        lo[g] = s15 >= key[g] ? 16 : 0;
+                        lo[g] += (lo[g] ? s23 : s7) >= key[g] ? 8 : 0;
                     }
 #pragma unroll
                     for (int st = 4; st >= 1; st >>= 1)
 #pragma unroll
-                        for (int g = 0; g < G; g++) lo[g] += srow[(lo[g] + st - 1) * kScSummStride] >= full[g] ? st : 0;
+                        for (int g = 0; g < G; g++) lo[g] += srow[(lo[g] + st - 1) * kScSummStride] >= key[g] ? st : 0;
 #pragma unroll
                     for (int g = 0; g < G; g++) {
-                        lo[g] += srow[lo[g] * kScSummStride] >= full[g];
-                        const bool gok = (lo[g] == 0 || srow[(lo[g] - 1) * kScSummStride] >= full[g] + df[g]) &&
-                                         (lo[g] >= ThrSummary::kMaxGroups || srow[lo[g] * kScSummStride] < full[g] - df[g]) &&
+                        lo[g] += srow[lo[g] * kScSummStride] >= key[g];
+                        const bool gok = (lo[g] >= ThrSummary::kMaxGroups || srow[lo[g] * kScSummStride] < full[g] - df[g]) &&
                                          df[g] < 1e30f && full[g] == full[g];
                         ok[g] = ok[g] && gok;
                     }

@@ -85,7 +85,7 @@ def test_index_load_files_answers_as_the_explicit_loads(tmp_path):
     as an index loaded array by array; a file of another user count is refused."""
     orc = Oracle()
     rng = np.random.default_rng(32)
-    n_user, n_item, d, nq, topk = 500, 1200, 20, 40, 10
+    n_user, n_item, d, nq, topk = 500, 1200, 20, 100, 10  # US answers 100 queries per call
     user = orc.normalize((rng.standard_normal((n_user, d)) * 2).astype(np.float32))
     item = (rng.standard_normal((n_item, d)) * 2).astype(np.float32)
     query = item[rng.choice(n_item, nq, replace=False)].copy()

@@ -698,7 +698,7 @@ def main():
     torch.cuda.synchronize()
     prof = ix.profile_read()
     ix.profile(False)
-    is_counter = lambda k: k.endswith("_pairs") or k.endswith("_queries")
+    is_counter = lambda k: k.endswith("_pairs") or k.endswith("_queries") or k.endswith("_rows")
     counters = {k: int(v[1]) for k, v in prof.items() if is_counter(k)}
     prof = {k: v for k, v in prof.items() if not is_counter(k)}
     st = np.frombuffer(d_stats.cpu().numpy().tobytes(), dtype=R.QUERY_STATS)

@@ -192,14 +192,15 @@ int rkr_server_destroy(rkr_server *server);
  * events on the stream it runs on.  rkr_profile_read returns, per kernel name, the summed time and
  * the launch count since the previous complete read (a read with max_kernels >= *n_kernels clears
  * them; a smaller one only reports the count); names is [max_kernels][64] chars.  Entries whose
- * name ends in "_pairs" or "_queries" are counters rather than kernels (time 0, `launches` holds
+ * name ends in "_pairs", "_queries" or "_rows" are counters rather than kernels (time 0, `launches` holds
  * the count): two_pass_compaction_queries counts the queries whose flagged users outgrew the sparse
  * compaction's list and took the two-pass form;
  * screen_undecided_pairs counts the (query, user) pairs whose regression levels or threshold group
  * the screens (tensor-core scores with an error bound, the fast binary32 CDF) left to the
  * reference's own arithmetic; rescored_pairs the pairs whose score a later pass recomputed (a fine
  * threshold bucket within the bound, a reported or carried score); refine_exact_pairs the
- * refinement's (candidate, item) tests the tensor-core bound left undecided.
+ * refinement's (candidate, item) tests the tensor-core bound left undecided; row_select_deferred_rows
+ * the build's score rows that the streaming selection of long rows left to the scatter form.
  * (The reference's counterpart is its TimeRecord per stage, src/include/util/TimeMemory.hpp:7-24.) */
 int rkr_profile_enable(rkr_index *index, int32_t on);
 int rkr_profile_read(rkr_index *index, int32_t max_kernels, char *names, double *total_ms, int64_t *launches,

@@ -120,6 +120,9 @@ struct SelectArgs {
     float *sorted_out;
     // global scratch when the row does not fit in shared memory ([gridDim.x][2][n_item])
     float *gscratch;
+    // rows to process (indices into rows), or nullptr for all n_rows
+    const int32_t *row_list;
+    int n_list;
 };
 
 __device__ __forceinline__ int value_bin(float x, float mn, float scale) {
@@ -144,7 +147,9 @@ __global__ void __launch_bounds__(kSelThreads) row_select_kernel(SelectArgs a, i
         buf = vals + n;
     }
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for (int row = blockIdx.x; row < a.n_rows; row += gridDim.x) {
+    const int n_iter = a.row_list ? a.n_list : a.n_rows;
+    for (int ri = blockIdx.x; ri < n_iter; ri += gridDim.x) {
+        const int row = a.row_list ? a.row_list[ri] : ri;
         const float *src = a.rows + (int64_t) row * a.ld;
         float mn = __int_as_float(0x7f800000), mx = -mn;
         for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -264,6 +269,204 @@ __global__ void __launch_bounds__(kSelThreads) row_select_kernel(SelectArgs a, i
     }
 }
 
+// ---- rows longer than shared memory ------------------------------------------------------------------
+//
+// A row of config-4 size (624,961 items) does not fit in shared memory.  Instead of copying it to a
+// global scratch row and scattering it there in bin order (a scattered 4-byte store per item), the
+// CTA streams the row from where the score pass wrote it: its range, a histogram of kGBins value
+// bins, and then -- for the bins holding a requested position or a sampled item's score only -- a
+// copy of those values into shared memory, where the order statistics are taken.  Requested bins
+// that do not fit the staging buffer together are staged in several rounds (one more stream each).
+// A row whose scores are all equal needs no bins; a row with a requested bin larger than the whole
+// buffer (an extreme concentration of scores) is listed, untouched, for the scatter form
+// (row_select_kernel on global scratch).
+constexpr int kGBins = 16384;
+constexpr int kGStage = 23552;  // staged values (92 KB)
+constexpr size_t kGSmem = sizeof(int) * (2 * kGBins + 1) + sizeof(uint32_t) * (kGBins / 32) + sizeof(float) * kGStage;
+
+__device__ __forceinline__ int value_bin_g(float x, float mn, float scale) {
+    const int b = (int) __fmul_rn(__fsub_rn(x, mn), scale);
+    return min(max(b, 0), kGBins - 1);
+}
+
+// Calls f on every value of a row (16-byte aligned, as the score rows are): four float4 loads in
+// flight per thread, so that one CTA per SM keeps enough of the row in flight.
+template <class F>
+__device__ __forceinline__ void stream_row(const float *__restrict__ src, int n, F f) {
+    const float4 *s4 = reinterpret_cast<const float4 *>(src);
+    const int n4 = n >> 2;
+#pragma unroll 4
+    for (int i = threadIdx.x; i < n4; i += blockDim.x) {
+        const float4 v = __ldg(s4 + i);
+        f(v.x);
+        f(v.y);
+        f(v.z);
+        f(v.w);
+    }
+    for (int i = (n4 << 2) + threadIdx.x; i < n; i += blockDim.x) f(__ldg(src + i));
+}
+
+// The bin holding ascending position p: the last bin whose start is <= p.
+__device__ __forceinline__ int bin_of_pos(const int *start, int p) {
+    int lo = 0, len = kGBins;
+    while (len > 0) {
+        const int h = len >> 1, m = lo + h;
+        if (start[m + 1] <= p) { lo = m + 1; len -= h + 1; } else len = h;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(kSelThreads) row_select_global_kernel(SelectArgs a, int32_t *__restrict__ defer,
+                                                                        int *__restrict__ n_defer) {
+    extern __shared__ int gdyn[];
+    int *hist = gdyn;                                                   // counts, then staging cursors
+    int *start = hist + kGBins;                                         // [kGBins + 1] bin starts
+    uint32_t *want = reinterpret_cast<uint32_t *>(start + kGBins + 1);  // requested bins, one bit each
+    float *stage = reinterpret_cast<float *>(want + kGBins / 32);       // [kGStage]
+    __shared__ float red_mn[32], red_mx[32];
+    __shared__ int warp_tot[32];
+    __shared__ int round_lo, round_hi, too_big;
+    const int n = a.n_item;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    constexpr int per = kGBins / kSelThreads;
+    auto requested = [&](int b) { return (want[b >> 5] >> (b & 31)) & 1u; };
+    for (int row = blockIdx.x; row < a.n_rows; row += gridDim.x) {
+        const float *src = a.rows + (int64_t) row * a.ld;
+        // stream 1: the row's range
+        float mn = __int_as_float(0x7f800000), mx = -mn;
+        stream_row(src, n, [&](float x) {
+            mn = fminf(mn, x);
+            mx = fmaxf(mx, x);
+        });
+        for (int o = 16; o > 0; o >>= 1) {
+            mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+            mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        }
+        if (lane == 0) { red_mn[w] = mn; red_mx[w] = mx; }
+        for (int b = threadIdx.x; b < kGBins; b += blockDim.x) hist[b] = 0;
+        for (int b = threadIdx.x; b < kGBins / 32; b += blockDim.x) want[b] = 0u;
+        if (threadIdx.x == 0) too_big = 0;
+        __syncthreads();
+        mn = red_mn[0];
+        mx = red_mx[0];
+        for (int i = 1; i < nw; i++) { mn = fminf(mn, red_mn[i]); mx = fmaxf(mx, red_mx[i]); }
+        const float range = __fsub_rn(mx, mn);
+        if (!(range > 0.0f)) {
+            // every score equal: every threshold is that score, and no item scores above any other
+            if (a.thr_out)
+                for (int j = threadIdx.x; j < a.S; j += blockDim.x) a.thr_out[(int64_t) row * a.S + j] = mn;
+            if (a.rank_hist)
+                for (int s2 = threadIdx.x; s2 < a.n_si; s2 += blockDim.x) atomicAdd(&a.rank_hist[(int64_t) s2 * (n + 1)], 1);
+            __syncthreads();
+            continue;
+        }
+        const float scale = __fdiv_rn((float) kGBins, range);
+        // stream 2: the histogram
+        stream_row(src, n, [&](float x) { atomicAdd(&hist[value_bin_g(x, mn, scale)], 1); });
+        __syncthreads();
+        {  // exclusive scan of the counts into start
+            int loc[per];
+            int s = 0;
+#pragma unroll
+            for (int t = 0; t < per; t++) { loc[t] = s; s += hist[threadIdx.x * per + t]; }
+            int incl = s;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            if (lane == 31) warp_tot[w] = incl;
+            __syncthreads();
+            if (w == 0) {
+                const int v = lane < nw ? warp_tot[lane] : 0;
+                int iv = v;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int x = __shfl_up_sync(0xffffffffu, iv, o);
+                    if (lane >= o) iv += x;
+                }
+                if (lane < nw) warp_tot[lane] = iv - v;
+            }
+            __syncthreads();
+            const int base = warp_tot[w] + incl - s;
+#pragma unroll
+            for (int t = 0; t < per; t++) start[threadIdx.x * per + t] = base + loc[t];
+            if (threadIdx.x == 0) start[kGBins] = n;
+        }
+        __syncthreads();
+        // the requested bins: each threshold's position (descending rank r is ascending n - 1 - r)
+        // and each sampled item's score
+        if (a.thr_out)
+            for (int j = threadIdx.x; j < a.S; j += blockDim.x) {
+                const int b = bin_of_pos(start, n - 1 - a.sample_rank[j]);
+                atomicOr(&want[b >> 5], 1u << (b & 31));
+                if (start[b + 1] - start[b] > kGStage) too_big = 1;
+            }
+        if (a.rank_hist)
+            for (int s2 = threadIdx.x; s2 < a.n_si; s2 += blockDim.x) {
+                const int b = value_bin_g(__ldg(src + a.sample_item[s2]), mn, scale);
+                atomicOr(&want[b >> 5], 1u << (b & 31));
+                if (start[b + 1] - start[b] > kGStage) too_big = 1;
+            }
+        __syncthreads();
+        if (too_big) {  // left whole to the scatter form
+            if (threadIdx.x == 0) defer[atomicAdd(n_defer, 1)] = row;
+            __syncthreads();
+            continue;
+        }
+        // rounds over the requested bins in bin order, each staging what fits
+        if (threadIdx.x == 0) round_hi = 0;
+        __syncthreads();
+        while (true) {
+            if (threadIdx.x == 0) {
+                int b = round_hi;
+                while (b < kGBins && !requested(b)) b++;
+                round_lo = b;
+                int off = 0, e = b;
+                for (; e < kGBins; e++) {
+                    if (!requested(e)) continue;
+                    const int sz = start[e + 1] - start[e];
+                    if (off + sz > kGStage) break;
+                    hist[e] = off;  // the bin's staging cursor
+                    off += sz;
+                }
+                round_hi = e;
+            }
+            __syncthreads();
+            const int lo_b = round_lo, hi_b = round_hi;
+            if (lo_b >= kGBins) break;
+            // stream 3: this round's values into the staging buffer
+            stream_row(src, n, [&](float x) {
+                const int b = value_bin_g(x, mn, scale);
+                if (b >= lo_b && b < hi_b && requested(b)) stage[atomicAdd(&hist[b], 1)] = x;
+            });
+            __syncthreads();
+            // thresholds whose position lies in this round's bins (a bin's values end at its cursor)
+            if (a.thr_out)
+                for (int j = w; j < a.S; j += nw) {
+                    const int p = n - 1 - a.sample_rank[j];
+                    const int b = bin_of_pos(start, p);
+                    if (b < lo_b || b >= hi_b) continue;
+                    const int sz = start[b + 1] - start[b];
+                    const float v = warp_select(stage + hist[b] - sz, sz, p - start[b]);
+                    if (lane == 0) a.thr_out[(int64_t) row * a.S + j] = v;
+                }
+            // query ranks: items scoring strictly above each sampled item's score
+            if (a.rank_hist)
+                for (int s2 = threadIdx.x; s2 < a.n_si; s2 += blockDim.x) {
+                    const float sv = __ldg(src + a.sample_item[s2]);
+                    const int b = value_bin_g(sv, mn, scale);
+                    if (b < lo_b || b >= hi_b) continue;
+                    const int sz = start[b + 1] - start[b];
+                    const float *seg = stage + hist[b] - sz;
+                    int cnt = n - start[b + 1];
+                    for (int t = 0; t < sz; t++) cnt += seg[t] > sv;
+                    atomicAdd(&a.rank_hist[(int64_t) s2 * (n + 1) + cnt], 1);
+                }
+            __syncthreads();
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void prefix_rows_kernel(int32_t *__restrict__ h, int rows, int64_t len) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= rows) return;
@@ -288,6 +491,9 @@ int row_select_allow_max_smem() {
     RKR_CUDA(cudaFuncGetAttributes(&fa, row_select_kernel));
     RKR_CUDA(cudaFuncSetAttribute(row_select_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   optin - (int) fa.sharedSizeBytes));
+    RKR_CUDA(cudaFuncGetAttributes(&fa, row_select_global_kernel));
+    RKR_CUDA(cudaFuncSetAttribute(row_select_global_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  optin - (int) fa.sharedSizeBytes));
     return RKR_OK;
 }
 
@@ -298,6 +504,7 @@ struct RowPipeline {
     int grid = 0;
     size_t smem = 0;
     int use_smem = 1;
+    int sms = 0;
 };
 
 int setup_pipeline(rkr_index *ix, RowPipeline &P) {
@@ -312,12 +519,13 @@ int setup_pipeline(rkr_index *ix, RowPipeline &P) {
     P.smem = (size_t) 2 * n * sizeof(float);
     P.use_smem = P.smem + static_smem + 1024 <= (size_t) dev_smem;
     if (!P.use_smem) P.smem = 0;
-    else RKR_TRY(row_select_allow_max_smem());
-    int sms = 0;
-    RKR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ix->device));
-    P.grid = sms * (P.use_smem ? 1 : 2);
+    RKR_TRY(row_select_allow_max_smem());
+    RKR_CUDA(cudaDeviceGetAttribute(&P.sms, cudaDevAttrMultiProcessorCount, ix->device));
+    P.grid = P.sms;
     RKR_TRY(ix->ws_bucket.ensure((size_t) P.batch * P.ld * sizeof(float)));
-    if (!P.use_smem) RKR_TRY(ix->ws_misc.ensure((size_t) P.grid * 2 * n * sizeof(float)));
+    // long rows: the deferred-row list of the streaming selection (the scatter form's global
+    // scratch is allocated only if a row is deferred to it)
+    if (!P.use_smem) RKR_TRY(ix->ws_defer.ensure(sizeof(int32_t) * (size_t) (P.batch + 1)));
     return RKR_OK;
 }
 
@@ -340,9 +548,42 @@ int run_rows(RowPipeline &P, int64_t u0, int64_t nu, SelectArgs sa) {
     sa.ld = P.ld;
     sa.n_rows = (int) nu;
     sa.n_item = (int) ix->n_item;
-    sa.gscratch = P.use_smem ? nullptr : ix->ws_misc.as<float>();
-    timed(ix, st, "row_select", [&] { row_select_kernel<<<(unsigned) std::min<int64_t>(P.grid, nu), kSelThreads, P.smem, st>>>(sa, P.use_smem); });
+    if (P.use_smem || sa.sorted_out) {
+        // rows in shared memory; or a full sort (rkr_score_sort_batch), which scatters long rows
+        // on global scratch
+        const int grid = P.use_smem ? P.grid : 2 * P.sms;
+        if (!P.use_smem) {
+            RKR_TRY(ix->ws_misc.ensure((size_t) grid * 2 * ix->n_item * sizeof(float)));
+            sa.gscratch = ix->ws_misc.as<float>();
+        }
+        timed(ix, st, "row_select", [&] {
+            row_select_kernel<<<(unsigned) std::min<int64_t>(grid, nu), kSelThreads, P.smem, st>>>(sa, P.use_smem);
+        });
+        RKR_CUDA(cudaGetLastError());
+        return RKR_OK;
+    }
+    // long rows: the streaming selection; rows it defers (a requested bin larger than its staging
+    // buffer) take the scatter form afterwards
+    int32_t *defer = ix->ws_defer.as<int32_t>();
+    RKR_CUDA(cudaMemsetAsync(defer + P.batch, 0, sizeof(int32_t), st));
+    timed(ix, st, "row_select_stream", [&] {
+        row_select_global_kernel<<<(unsigned) std::min<int64_t>(2 * P.sms, nu), kSelThreads, kGSmem, st>>>(
+            sa, defer, defer + P.batch);
+    });
     RKR_CUDA(cudaGetLastError());
+    int n_defer = 0;
+    RKR_CUDA(cudaMemcpyAsync(&n_defer, defer + P.batch, sizeof(int), cudaMemcpyDeviceToHost, st));
+    RKR_CUDA(cudaStreamSynchronize(st));
+    if (n_defer > 0) {
+        const int grid = std::min(n_defer, P.sms);
+        RKR_TRY(ix->ws_misc.ensure((size_t) grid * 2 * ix->n_item * sizeof(float)));
+        sa.gscratch = ix->ws_misc.as<float>();
+        sa.row_list = defer;
+        sa.n_list = n_defer;
+        timed(ix, st, "row_select", [&] { row_select_kernel<<<(unsigned) grid, kSelThreads, 0, st>>>(sa, 0); });
+        RKR_CUDA(cudaGetLastError());
+        if (ix->prof.on) ix->prof.add_count("row_select_deferred_rows", n_defer);
+    }
     return RKR_OK;
 }
 

@@ -839,41 +839,75 @@ __global__ void __launch_bounds__(kCompactThreads) compact_write_kernel(P p, int
 // ---- sparse form of the same compaction -------------------------------------------------------------
 //
 // The users a query must classify are few (a few hundred of the 480 K at config 2), so the sparse
-// form streams the codes once: compact_need_kernel appends each query's flagged users to its list
-// (one atomic per warp, in no particular order), and compact_emit_kernel, one block per query, sorts
+// form streams the codes once: compact_need_flat_kernel appends each query's flagged users to its
+// list (in no particular order), and compact_emit_kernel, one block per query, sorts
 // the list by user id and runs the ordered classification and emission of compact_write_kernel on
 // it.  A query whose list outgrows kNeedCap is listed and takes the two-pass form above.
 
 constexpr int kNeedCap = 4096;     // flagged users per query on the sparse path
-constexpr int kNeedGroups = 4;     // groups of kCompactPer users per thread in the streaming pass
-constexpr int64_t kNeedSpan = (int64_t) kCompactThreads * kNeedGroups * kCompactPer;
 
+// The flagged users' lists from one flat pass over the batch's codes ([query][user] as one array): 512 bytes
+// per warp and step in aligned 16-byte loads, the next step's load in flight while a step is
+// examined; a lane whose 16 codes lie in one query takes the policy's word-wise need_bits, one that
+// straddles a query boundary goes byte by byte.  Hits are few: one atomic per lane with hits.
 template <class P>
-__global__ void __launch_bounds__(kCompactThreads) compact_need_kernel(P p, int64_t n_user, int32_t *__restrict__ need_n,
-                                                                     int32_t *__restrict__ need_u) {
-    const int q = blockIdx.y;
-    const int64_t base = (int64_t) blockIdx.x * kNeedSpan + (int64_t) threadIdx.x * (kNeedGroups * kCompactPer);
-    uint32_t m[kNeedGroups];
-#pragma unroll
-    for (int g = 0; g < kNeedGroups; g++) {
-        const int64_t u = base + g * kCompactPer;
-        m[g] = u < n_user ? p.need_mask(q, u, (int) (n_user - u < kCompactPer ? n_user - u : kCompactPer)) : 0u;
-    }
-    int cnt = 0;
-#pragma unroll
-    for (int g = 0; g < kNeedGroups; g++) cnt += __popc(m[g]);
+__global__ void __launch_bounds__(256) compact_need_flat_kernel(P p, int64_t n_user, int nq, double inv_user,
+                                                               int32_t *__restrict__ need_n,
+                                                               int32_t *__restrict__ need_u) {
+    const uint8_t *code = p.code;
+    const int64_t total = n_user * nq;
     const int lane = threadIdx.x & 31;
-    const int incl = warp_incl_scan(cnt);
-    const int tot = __shfl_sync(0xffffffffu, incl, 31);
-    if (tot == 0) return;
-    int at = 0;
-    if (lane == 31) at = atomicAdd(need_n + q, tot);
-    at = __shfl_sync(0xffffffffu, at, 31) + incl - cnt;
-    int32_t *list = need_u + (int64_t) q * kNeedCap;
+    const int64_t warp = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int64_t stride = (int64_t) gridDim.x * blockDim.x * 16;
+    auto load = [&](int64_t seg, uint32_t w[4]) {
+        const int64_t base = seg + (int64_t) lane * 16;
+        if (base + 16 <= total) {
+            const uint4 x = __ldg(reinterpret_cast<const uint4 *>(code + base));
+            w[0] = x.x; w[1] = x.y; w[2] = x.z; w[3] = x.w;
+        } else {
 #pragma unroll
-    for (int g = 0; g < kNeedGroups; g++)
-        for (uint32_t x = m[g]; x; x &= x - 1, at++)
-            if (at < kNeedCap) list[at] = (int32_t) (base + g * kCompactPer + __ffs(x) - 1);
+            for (int i = 0; i < 4; i++) {
+                w[i] = 0;
+                for (int j = 0; j < 4; j++)
+                    if (base + 4 * i + j < total) w[i] |= (uint32_t) code[base + 4 * i + j] << (8 * j);
+            }
+        }
+    };
+    uint32_t wn[4] = {0u, 0u, 0u, 0u};
+    if (warp * 512 < total) load(warp * 512, wn);
+    for (int64_t seg = warp * 512; seg < total; seg += stride) {
+        uint32_t w[4] = {wn[0], wn[1], wn[2], wn[3]};
+        if (seg + stride < total) load(seg + stride, wn);
+        const int64_t base = seg + (int64_t) lane * 16;
+        int64_t qs = 0;
+        if (lane == 0) {
+            qs = (int64_t) ((double) seg * inv_user);
+            if (qs * n_user > seg) qs--;
+            else if ((qs + 1) * n_user <= seg) qs++;
+        }
+        qs = __shfl_sync(0xffffffffu, qs, 0);
+        if (base >= total) continue;
+        int64_t q = qs;
+        while ((q + 1) * n_user <= base) q++;
+        if (base + 16 <= (q + 1) * n_user && base + 16 <= total) {
+            uint32_t m = p.need_bits((int) q, w);
+            if (!m) continue;
+            int at = atomicAdd(need_n + q, __popc(m));
+            int32_t *list = need_u + q * kNeedCap;
+            const int64_t u0 = base - q * n_user;
+            for (; m; m &= m - 1, at++)
+                if (at < kNeedCap) list[at] = (int32_t) (u0 + __ffs(m) - 1);
+        } else {
+            for (int e = 0; e < 16; e++) {
+                const int64_t pos = base + e;
+                if (pos >= total) break;
+                while ((q + 1) * n_user <= pos) q++;
+                if (!p.need_byte((int) q, (w[e >> 2] >> (8 * (e & 3))) & 0xffu)) continue;
+                const int at = atomicAdd(need_n + q, 1);
+                if (at < kNeedCap) need_u[q * kNeedCap + at] = (int32_t) (pos - q * n_user);
+            }
+        }
+    }
 }
 
 template <class P>
@@ -1030,6 +1064,7 @@ struct rkr_index {
     // per-call workspace
     rkr::DevBuf ws_query, ws_qtr, ws_qnorm, ws_bucket, ws_bucket2, ws_levels, ws_cls, ws_counts, ws_hist;
     rkr::DevBuf ws_res, ws_cand, ws_cand_off, ws_refine, ws_rank, ws_out, ws_stats, ws_misc, ws_fix, ws_km, ws_tc, ws_sc;
+    rkr::DevBuf ws_defer;  // rows the streaming row selection left to the scatter form
     std::vector<uint8_t> h_scratch;
     rkr::Profiler prof;
     // CUDA graphs of a batch's phase 1 (rkr_qsrp.cu), one per (method, batch size, workspace
@@ -1078,8 +1113,9 @@ inline int run_compaction(rkr_index *ix, P p, int nq, KSpec ks, QueryCounts *cou
     const int32_t *qmap = nullptr;   // which ones (nullptr: all)
     if (ix->compact_sparse_on) {
         RKR_CUDA(cudaMemsetAsync(need_n, 0, sizeof(int32_t) * nq, st));
-        const dim3 g((unsigned) ((U + kNeedSpan - 1) / kNeedSpan), (unsigned) nq);
-        timed(ix, st, "compact_need", [&] { compact_need_kernel<P><<<g, kCompactThreads, 0, st>>>(p, U, need_n, need_u); });
+        timed(ix, st, "compact_need", [&] {
+            compact_need_flat_kernel<P><<<148 * 8, 256, 0, st>>>(p, U, nq, 1.0 / (double) U, need_n, need_u);
+        });
         RKR_CUDA(cudaGetLastError());
         timed(ix, st, "compact_emit", [&] {
             compact_emit_kernel<P><<<(unsigned) nq, kCompactThreads, 0, st>>>(p, ks, need_n, need_u, counts, err, ovf_q);

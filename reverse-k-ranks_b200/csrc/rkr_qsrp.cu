@@ -482,9 +482,9 @@ __global__ void __launch_bounds__(256) qsrp_fine1_scan_kernel(uint8_t *__restric
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int64_t stride = (int64_t) gridDim.x * blockDim.x * 16;
-    for (int64_t seg = warp * 512; seg < total; seg += stride) {
+    // the lane's 16 bytes of a segment (zero past the end)
+    auto load = [&](int64_t seg, uint32_t w[4]) {
         const int64_t base = seg + (int64_t) lane * 16;
-        uint32_t w[4];
         if (base + 16 <= total) {
             const uint4 x = *reinterpret_cast<const uint4 *>(lvc + base);
             w[0] = x.x; w[1] = x.y; w[2] = x.z; w[3] = x.w;
@@ -496,6 +496,14 @@ __global__ void __launch_bounds__(256) qsrp_fine1_scan_kernel(uint8_t *__restric
                     if (base + 4 * i + j < total) w[i] |= (uint32_t) lvc[base + 4 * i + j] << (8 * j);
             }
         }
+    };
+    uint32_t wn[4] = {0u, 0u, 0u, 0u};
+    if (warp * 512 < total) load(warp * 512, wn);
+    for (int64_t seg = warp * 512; seg < total; seg += stride) {
+        const int64_t base = seg + (int64_t) lane * 16;
+        // this segment's bytes, and the next segment's load in flight while they are examined
+        uint32_t w[4] = {wn[0], wn[1], wn[2], wn[3]};
+        if (seg + stride < total) load(seg + stride, wn);
         // the segment's first query (once per warp) and the lane's queries
         int64_t qs = 0;
         if (lane == 0) {
@@ -1093,12 +1101,11 @@ struct QsrpCompactPolicy {
     __device__ bool query_active(int q) const { return true; }
     // Users whose code can make them a result or a candidate: a group the compaction must
     // classify, a round-1 result, or any non-survivor under the equal-bounds rule.
-    __device__ uint32_t need_mask(int q, int64_t u, int n) const {
+    // The needed users among 16 codes of query q (bit e for w's byte e).
+    __device__ uint32_t need_bits(int q, const uint32_t w[4]) const {
         const QsrpParams &p = par[q];
         const uint64_t gneed = (uint64_t) (uint32_t) p.gneed_lo | ((uint64_t) (uint32_t) p.gneed_hi << 32);
         const bool state_any = !p.skip2 && p.mode2;
-        uint32_t w[4];
-        load16_bytes(code + (int64_t) q * n_user + u, w);
         uint32_t m = 0;
         if ((gneed & (gneed + 1)) == 0) {
             // the needed groups are 0 .. gmax (the classes rise with the group): four codes at a time.
@@ -1118,12 +1125,19 @@ struct QsrpCompactPolicy {
             }
         } else {
 #pragma unroll
-            for (int e = 0; e < kCompactPer; e++) {
-                const unsigned c = (w[e >> 2] >> (8 * (e & 3))) & 0xff;
-                const bool nd = c <= (unsigned) nb ? (bool) (gneed >> c & 1) : (c == kCodeResult1 || state_any);
-                m |= (uint32_t) nd << e;
-            }
+            for (int e = 0; e < kCompactPer; e++) m |= (uint32_t) need_byte(q, (w[e >> 2] >> (8 * (e & 3))) & 0xff) << e;
         }
+        return m;
+    }
+    __device__ bool need_byte(int q, unsigned c) const {
+        const QsrpParams &p = par[q];
+        const uint64_t gneed = (uint64_t) (uint32_t) p.gneed_lo | ((uint64_t) (uint32_t) p.gneed_hi << 32);
+        return c <= (unsigned) nb ? (bool) (gneed >> c & 1) : (c == kCodeResult1 || (!p.skip2 && p.mode2));
+    }
+    __device__ uint32_t need_mask(int q, int64_t u, int n) const {
+        uint32_t w[4];
+        load16_bytes(code + (int64_t) q * n_user + u, w);
+        const uint32_t m = need_bits(q, w);
         return n >= 32 ? m : m & ((1u << n) - 1);
     }
     __device__ int classify(int q, int64_t u, Aux &aux, bool with_aux) const {

@@ -377,16 +377,14 @@ __global__ void __launch_bounds__(kRfThreads, 1) refine_tc_kernel(TcArgs a) {
                 tmem_ld8(base + 2 * kScN, v2);
                 tmem_ld8(base + 3 * kScN, v3);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-                for (int j = 0; j < 8; j++) l[j] = combine4(v0[j], v1[j], v2[j], v3[j]);
+                combine4_x8(v0, v1, v2, v3, l);
                 if (has_rest) {
                     tmem_ld8(base + 4 * kScN, v0);
                     tmem_ld8(base + 5 * kScN, v1);
                     tmem_ld8(base + 6 * kScN, v2);
                     tmem_ld8(base + 7 * kScN, v3);
                     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-                    for (int j = 0; j < 8; j++) r[j] = combine4(v0[j], v1[j], v2[j], v3[j]);
+                    combine4_x8(v0, v1, v2, v3, r);
                 } else {
 #pragma unroll
                     for (int j = 0; j < 8; j++) r[j] = 0.0f;

@@ -143,24 +143,21 @@ __device__ __forceinline__ void exact_pair(const ScArgs &a, int64_t u, int q, co
 }
 
 // Counts one query column of a warp's pairs by coarse level into the chunk's shared-memory histogram
-// h ([2 sides][kLvEntries]).  The lanes' levels are balloted bit by bit; lane l then counts the lanes
-// whose lower level (l < 16) or upper level (l >= 16) is l % 16 -- the AND of the four bit masks or
-// their complements -- and adds that count: every bin of both sides in one pass, one shared-memory
-// atomic per occupied bin.  The lower side's last level and the upper side's level 0 stay implicit.
+// h ([2 sides][kLvEntries]).  Pairs at both implicit levels (the lower side's last, the upper side's
+// 0) are not counted; the others are grouped by their two levels, and one lane of each group adds the
+// group's size -- one atomic per distinct pair of levels instead of one per pair (the lanes of a warp
+// mostly share their levels).  (A bit-sliced form -- the levels balloted bit by bit and every bin
+// counted by its own lane -- costs about three times the instructions per pair.)
 __device__ __forceinline__ void warp_level_hist(uint32_t *h, bool count, int cl, int cu) {
-    const unsigned v = __ballot_sync(0xffffffffu, count);
-    if (v == 0u) return;
-    const int lane = threadIdx.x & 31, bin = lane & 15;
-    unsigned m = v;
-#pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const unsigned bl = __ballot_sync(0xffffffffu, (cl >> k) & 1), bu = __ballot_sync(0xffffffffu, (cu >> k) & 1);
-        const unsigned b = lane < 16 ? bl : bu;
-        m &= ((bin >> k) & 1) ? b : ~b;
+    const bool part = count && !(cl == kLvEntries - 1 && cu == 0);
+    const unsigned pm = __ballot_sync(0xffffffffu, part);
+    if (!part) return;
+    const unsigned m = __match_any_sync(pm, cl | (cu << 4));
+    if ((threadIdx.x & 31) == __ffs(m) - 1) {
+        const uint32_t n = (uint32_t) __popc(m);
+        if (cl != kLvEntries - 1) atomicAdd(h + cl, n);
+        if (cu != 0) atomicAdd(h + kLvEntries + cu, n);
     }
-    const int n = __popc(m);
-    const bool implicit = lane < 16 ? bin == kLvEntries - 1 : bin == 0;
-    if (n && !implicit) atomicAdd(h + lane, (uint32_t) n);
 }
 
 // The bound scores of the regression round, qlb = partial - right and qub = partial + right
@@ -169,11 +166,13 @@ __device__ __forceinline__ void warp_level_hist(uint32_t *h, bool count, int cl,
 __device__ __forceinline__ void level_bounds(float vl, float dl, float un, float qn, float &qlb, float &qub,
                                              float &dql, float &dqu) {
     const float right = __fmul_rn(un, qn);
-    qlb = __fsub_rn(vl, right);
-    qub = __fadd_rn(vl, right);
+    const float2 q = __fadd2_rn(make_float2(vl, vl), make_float2(-right, right));
     const float dq = dl * 1.0001f;
-    dql = fmaf(fabsf(qlb), 2.4e-7f, dq);
-    dqu = fmaf(fabsf(qub), 2.4e-7f, dq);
+    const float2 e = __ffma2_rn(make_float2(fabsf(q.x), fabsf(q.y)), make_float2(2.4e-7f, 2.4e-7f), make_float2(dq, dq));
+    qlb = q.x;
+    qub = q.y;
+    dql = e.x;
+    dqu = e.y;
 }
 
 __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
@@ -373,16 +372,14 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                     tmem_ld8(base + 2 * kScN, v2);
                     tmem_ld8(base + 3 * kScN, v3);
                     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-                    for (int i = 0; i < 8; i++) sl[i] = combine4(v0[i], v1[i], v2[i], v3[i]);
+                    combine4_x8(v0, v1, v2, v3, sl);
                     if (a.two_parts) {
                         tmem_ld8(base + 4 * kScN, v0);
                         tmem_ld8(base + 5 * kScN, v1);
                         tmem_ld8(base + 6 * kScN, v2);
                         tmem_ld8(base + 7 * kScN, v3);
                         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-                        for (int i = 0; i < 8; i++) sr[i] = combine4(v0[i], v1[i], v2[i], v3[i]);
+                        combine4_x8(v0, v1, v2, v3, sr);
                     } else {
 #pragma unroll
                         for (int i = 0; i < 8; i++) sr[i] = 0.0f;
@@ -404,11 +401,17 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                         const int i = i0 + g;
                         const float4 qm = sq[j * kScN + 8 * cg + i];
                         const float scale = __int_as_float((ue + __float_as_int(qm.w) - 35 + 127) << 23);
-                        vl[g] = sl[i] * scale;
+                        // the two parts side by side in paired FP32 instructions (per component the
+                        // roundings of the scalar forms)
                         const float ee = um.x * qm.x;
-                        dl[g] = fmaf(cl_u, qm.y, fmaf(fabsf(vl[g]), 1.8e-7f, ee * a.kl));
-                        const float vr = sr[i] * scale;
-                        const float dr = fmaf(cr_u, qm.z, fmaf(fabsf(vr), 1.8e-7f, ee * a.kr));
+                        const float2 v = __fmul2_rn(make_float2(sl[i], sr[i]), make_float2(scale, scale));
+                        const float2 t = __fmul2_rn(make_float2(ee, ee), make_float2(a.kl, a.kr));
+                        const float2 d = __ffma2_rn(make_float2(cl_u, cr_u), make_float2(qm.y, qm.z),
+                                                    __ffma2_rn(make_float2(fabsf(v.x), fabsf(v.y)),
+                                                               make_float2(1.8e-7f, 1.8e-7f), t));
+                        vl[g] = v.x;
+                        dl[g] = d.x;
+                        const float vr = v.y, dr = d.y;
                         full[g] = a.two_parts ? __fadd_rn(vl[g], vr) : vl[g];
                         df[g] = fmaf(fabsf(full[g]), 2.4e-7f, (dl[g] + dr) * 1.0001f);
                         ok[g] = true;

@@ -205,6 +205,25 @@ __device__ __forceinline__ float i2f_small(uint32_t x) {
 __device__ __forceinline__ float combine4(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3) {
     return fmaf(fmaf(fmaf(i2f_small(a0), 128.0f, i2f_small(a1)), 128.0f, i2f_small(a2)), 128.0f, i2f_small(a3));
 }
+// The same for the eight columns of a tcgen05.ld, two columns per paired FP32 instruction
+// (__fadd2_rn / __ffma2_rn round each component as __fadd_rn / __fmaf_rn do: the results are
+// combine4's, bit for bit).
+__device__ __forceinline__ void combine4_x8(const uint32_t a0[8], const uint32_t a1[8], const uint32_t a2[8],
+                                            const uint32_t a3[8], float out[8]) {
+    const float2 off = make_float2(-12582912.0f, -12582912.0f), k128 = make_float2(128.0f, 128.0f);
+    auto f2 = [&](const uint32_t *a, int i) {
+        return __fadd2_rn(make_float2(__int_as_float((int) a[i] + 0x4B400000), __int_as_float((int) a[i + 1] + 0x4B400000)),
+                          off);
+    };
+#pragma unroll
+    for (int i = 0; i < 8; i += 2) {
+        float2 r = __ffma2_rn(f2(a0, i), k128, f2(a1, i));
+        r = __ffma2_rn(r, k128, f2(a2, i));
+        r = __ffma2_rn(r, k128, f2(a3, i));
+        out[i] = r.x;
+        out[i + 1] = r.y;
+    }
+}
 
 // Bound coefficients of a part of n coordinates: (on the product of the rows' weighted norms, on
 // 2^(ea + eb)).  The reference's sequential binary32 sum of p_t = a_t b_t (t = 1..n, one rounding

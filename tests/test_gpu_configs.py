@@ -119,3 +119,23 @@ def test_config1_whole_pipeline_matches_oracle():
         a = ix.retrieval("US", query, k)
         b, _ = orc.us_retrieval(un, item, uni, thr_u, query, k)
         assert same(a, b)
+
+
+@pytest.mark.parametrize("n_item", [40000, 90001])
+def test_build_rows_larger_than_shared_memory_match_oracle(n_item):
+    """Rows too long for the shared-memory selection (config 4 has 624,961 items) take the
+    global-memory path of the row selection: thresholds (a dense head of ranks, then a spread) and
+    the query-rank distribution against the oracle, with lognormal item norms as at config 4."""
+    n_user, d = 192, 24
+    rng = np.random.default_rng(n_item)
+    orc = Oracle()
+    user = orc.normalize(rng.standard_normal((n_user, d)).astype(np.float32))
+    item = (rng.standard_normal((n_item, d)) * np.exp(rng.normal(0, 0.3, (n_item, 1)))).astype(np.float32)
+    rank = np.unique(np.concatenate([np.arange(0, 64), np.linspace(64, n_item - 2, 200).astype(int)])).astype(np.int32)
+    si = R.sample_item(n_item, 40)
+    with R.Index(user, item) as ix:
+        thr = ix.build_sample_search(rank)
+        assert same(thr, orc.build_thresholds(user, item, rank))
+        accu = ix.query_rank_distribution(si)
+        _, accu_o = orc.query_rank_distribution(user, item, si)
+        assert np.array_equal(accu, accu_o)

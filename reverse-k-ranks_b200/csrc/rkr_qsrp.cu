@@ -341,23 +341,39 @@ __global__ void qsrp_fix1_scan_kernel(const int *__restrict__ count, int cap, Ro
 // Coarse-level histograms of the exact tiles' batch (the tensor-core kernel counts in its epilogue),
 // one CTA per (user chunk, query); the lower side's last coarse level and the upper side's level 0
 // are left implicit, as there.
+// Coarse-level histograms of a batch from its coarse-level bytes: per query, the pairs at each lower
+// coarse level and each upper coarse level (the lower side's level 15 and the upper side's 0, which
+// hold most pairs, stay implicit).  Per-thread counters in shared memory, bin-major ([bin][thread]:
+// a thread's counters sit in its own bank), so the increments need no atomics and never conflict;
+// 16 users per thread and step from aligned words.
 __global__ void __launch_bounds__(kHistThreads) lvc_hist_kernel(const uint8_t *__restrict__ lvc, int64_t n_user,
                                                                int64_t chunk, int *__restrict__ lhist) {
-    __shared__ int h[2 * kLvEntries];
-    const int q = blockIdx.y;
-    for (int b = threadIdx.x; b < 2 * kLvEntries; b += blockDim.x) h[b] = 0;
-    __syncthreads();
+    __shared__ int h[2 * kLvEntries * kHistThreads];
+    const int q = blockIdx.y, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int b = 0; b < 2 * kLvEntries; b++) h[b * kHistThreads + tid] = 0;
     const uint8_t *row = lvc + (int64_t) q * n_user;
     const int64_t u0 = (int64_t) blockIdx.x * chunk, u1 = min(u0 + chunk, n_user);
-    for (int64_t u = u0 + threadIdx.x; u < u1; u += blockDim.x) {
-        const unsigned v = row[u];
-        const int cl = (int) (v & 15), cu = (int) (v >> 4);
-        if (cl != kLvEntries - 1) atomicAdd(h + cl, 1);
-        if (cu != 0) atomicAdd(h + kLvEntries + cu, 1);
+    for (int64_t ub = u0 + (int64_t) tid * 16; ub < u1; ub += (int64_t) kHistThreads * 16) {
+        const int n = (int) min((int64_t) 16, u1 - ub);
+        uint32_t w[4];
+        load16_bytes(row + ub, w);
+#pragma unroll
+        for (int e = 0; e < 16; e++) {
+            if (e >= n) break;
+            const unsigned v = (w[e >> 2] >> (8 * (e & 3))) & 0xffu;
+            const int cl = (int) (v & 15), cu = (int) (v >> 4);
+            if (cl != kLvEntries - 1) h[cl * kHistThreads + tid]++;
+            if (cu != 0) h[(kLvEntries + cu) * kHistThreads + tid]++;
+        }
     }
     __syncthreads();
-    for (int b = threadIdx.x; b < 2 * kLvEntries; b += blockDim.x)
-        if (h[b]) atomicAdd(lhist + (int64_t) q * 2 * kLvEntries + b, h[b]);
+    int *gh = lhist + (int64_t) q * 2 * kLvEntries;
+    for (int b = warp; b < 2 * kLvEntries; b += kHistThreads / 32) {
+        int sum = 0;
+        for (int t = lane; t < kHistThreads; t += 32) sum += h[b * kHistThreads + t];
+        sum = __reduce_add_sync(0xffffffffu, sum);
+        if (lane == 0 && sum) atomicAdd(gh + b, sum);
+    }
 }
 
 // ---- one warp per query -------------------------------------------------------------------------
@@ -1352,7 +1368,7 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
     const size_t n_hist_c = (size_t) nq * (nb + 1), n_hist_f = (size_t) nq * (S + 1);
     RKR_TRY(ix->ws_hist.ensure(carve_size(n_hist_c, 4) + carve_size(n_hist_f, 4)));
     const int fix_cap = (int) std::min<int64_t>(int64_t(1) << 26, std::max<int64_t>(int64_t(1) << 20, U * nq / 64));
-    const int hit_cap = 1 << 22;
+    const int hit_cap = 1 << 24;  // fine-pass hits listed per batch (config 4: about 6.6 M per 1,000 queries)
     RKR_TRY(ix->ws_fix.ensure(carve_size(fix_cap, sizeof(int4)) + carve_size(hit_cap, 8) + carve_size(1, 4)));
     uint8_t *pc = ix->ws_cls.as<uint8_t>();
     uint8_t *cls2 = carve<uint8_t>(pc, (size_t) nq * (S + 1));
@@ -1425,14 +1441,12 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
             call.nb = nb;
             call.lvc = lvc;
             call.code = code;
-            call.lhist = qsrp ? lhist : nullptr;
             call.anomaly = qsrp ? anomaly : nullptr;
             call.status = sc_status;
             RKR_TRY(scores_tc(ix, call, st, &tc_done));
         }
         if (!tc_done) {
             // the exact tiles start from clean counts (a tensor-core run that gave up may have left some)
-            RKR_CUDA(cudaMemsetAsync(lhist, 0, sizeof(int) * n_lhist, st));
             RKR_CUDA(cudaMemsetAsync(anomaly, 0, sizeof(int) * nq, st));
             Round1Epi e1;
             e1.unorm = r1.unorm;
@@ -1463,11 +1477,14 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
                     qsrp_fix1_scan_kernel<<<148 * 8, 256, 0, st>>>(fix_count, fix_cap, r1, U, nq, lvc, anomaly);
                 });
                 RKR_CUDA(cudaGetLastError());
-                const int64_t ch = 65536;
-                const dim3 g((unsigned) ((U + ch - 1) / ch), (unsigned) nq);
-                timed(ix, st, "lvc_hist", [&] { lvc_hist_kernel<<<g, kHistThreads, 0, st>>>(lvc, U, ch, lhist); });
-                RKR_CUDA(cudaGetLastError());
             }
+        }
+        if (qsrp) {
+            // the coarse-level histograms, from every pair's final byte
+            const int64_t ch = 65536;
+            const dim3 g((unsigned) ((U + ch - 1) / ch), (unsigned) nq);
+            timed(ix, st, "lvc_hist", [&] { lvc_hist_kernel<<<g, kHistThreads, 0, st>>>(lvc, U, ch, lhist); });
+            RKR_CUDA(cudaGetLastError());
         }
         const int64_t chunk = 65536;  // users per round-2 block (its per-thread counters are set up once)
         dim3 hg((unsigned) ((U + chunk - 1) / chunk), (unsigned) nq);

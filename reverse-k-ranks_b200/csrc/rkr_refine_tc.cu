@@ -413,10 +413,7 @@ __global__ void __launch_bounds__(kRfThreads, 1) refine_tc_kernel(TcArgs a) {
                 const float t_ct = __fadd_ru(highq, Ms) * inv, t_fu = __fadd_rd(highq, -Ms) * inv;
                 const float t_hi = __fadd_ru(qv, Mt) * inv, t_mi = __fadd_rd(qv, -Mt) * inv;
                 const float un_s = un * inv;
-#pragma unroll
-                for (int j = 0; j < 8; j++) {
-                    const float rt = __shfl_sync(0xffffffffu, gv, j) * un_s;  // the reference's right, scaled
-                    const float s = l[j] + rt, d = l[j] - rt, t = l[j] + r[j];
+                auto pair_test = [&](int j, float s, float d, float t) {
                     const bool act = j < nvalid && !(s < t_sk);          // not surely skipped
                     const bool ns = s >= t_ns;                             // surely not skipped
                     const bool c1 = ns && d > t_ct;                        // surely counted on its bound
@@ -426,6 +423,19 @@ __global__ void __launch_bounds__(kRfThreads, 1) refine_tc_kernel(TcArgs a) {
                     und += act && f1;
                     const unsigned lf = act && !c1 && !f1, lc = act && f1 && !hi && !mi;
                     lmask |= (lf | (lc << 1)) << (2 * j);
+                };
+#pragma unroll
+                for (int j = 0; j < 8; j += 2) {
+                    // two columns per paired FP32 instruction (per component the scalar roundings):
+                    // s = left + right, d = left - right, t = left + rest
+                    const float2 rt2 = __fmul2_rn(make_float2(__shfl_sync(0xffffffffu, gv, j),
+                                                              __shfl_sync(0xffffffffu, gv, j + 1)),
+                                                  make_float2(un_s, un_s));  // the reference's right, scaled
+                    const float2 l2 = make_float2(l[j], l[j + 1]);
+                    const float2 s2 = __fadd2_rn(l2, rt2), d2 = __fadd2_rn(l2, make_float2(-rt2.x, -rt2.y));
+                    const float2 t2 = __fadd2_rn(l2, make_float2(r[j], r[j + 1]));
+                    pair_test(j, s2.x, d2.x, t2.x);
+                    pair_test(j + 1, s2.y, d2.y, t2.y);
                 }
             } else {
                 const float M = fmaf(kSigma, nl, DL) * kSafe;

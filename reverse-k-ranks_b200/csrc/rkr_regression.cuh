@@ -213,7 +213,7 @@ __device__ __forceinline__ int level_rank(int lvl, const int32_t *rank, int S, i
 }
 
 // One batch of pair scores for the bound rounds (rkr_scores_tc.cu): coarse levels (QSRP) and coarse
-// group codes of every (query, user) pair, and the coarse-level histograms.
+// group codes of every (query, user) pair (their histograms are a separate pass over the bytes).
 struct ScoresTcCall {
     bool qsrp;
     const float *qrows, *qnorm, *unorm;  // queries (SVD space for QSRP), remaining-coordinate norms
@@ -222,14 +222,13 @@ struct ScoresTcCall {
     int nb;
     uint8_t *lvc;    // [nq][n_user] (QSRP)
     uint8_t *code;   // [nq][n_user]
-    int *lhist;      // [nq][2][kLvEntries] (QSRP), zeroed by the caller
     int *anomaly;    // [nq] (QSRP), zeroed by the caller
     int **status = nullptr;  // if set ([4]): receives device pointers to the run's status (0: complete),
                              // undecided-pair count and the two table-search counts (lower, upper side:
                              // warp passes x 32), and the call does not wait for the device
 };
 // Runs the tensor-core scores where the shape allows; *done = false leaves the batch to the exact
-// tiles (the histograms may then hold partial counts: the caller clears them).  With call.status
+// tiles (the anomaly counts may then be partial: the caller clears them).  With call.status
 // set, *done only says the kernels were launched; the caller checks the status on the device.
 int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, bool *done);
 

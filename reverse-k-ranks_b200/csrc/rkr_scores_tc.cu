@@ -61,8 +61,6 @@ struct ScArgs {
     const float2 *lvt;             // [n_user][2][kLvEntries] level tables; nullptr: no regression round (QS, US)
     uint8_t *lvc;                  // [query][n_user]: coarse lower-bound level | coarse upper-bound level << 4
     uint8_t *code;                 // [query][n_user]: coarse threshold group of the full score
-    int *lhist;                    // [query][2][kLvEntries] coarse-level counts; the lower side's last bin and
-                                   // the upper side's bin 0 are left implicit (n_user minus the others)
     int *anomaly;                  // [query]: pairs whose upper-bound rank exceeds their lower-bound rank
     float2 *dump;                  // [query][n_user] (estimate of the full score, its bound), or nullptr
     int2 *ovf;                     // undecided pairs, (query, user): each tile's list in one piece
@@ -128,9 +126,6 @@ __device__ __forceinline__ void exact_pair(const ScArgs &a, int64_t u, int q, co
         const int l = (int) (v & 0xffffu), h = (int) (v >> 16);
         const int cl = lvt_coarse(l, a.m.S), cu = lvt_coarse(h, a.m.S);
         a.lvc[o] = (uint8_t) (cl | (cu << 4));
-        int *hq = a.lhist + (int64_t) q * 2 * kLvEntries;
-        if (cl != kLvEntries - 1) atomicAdd(hq + cl, 1);
-        if (cu != 0) atomicAdd(hq + kLvEntries + cu, 1);
         if (h > l && level_rank(h, a.m.rank, a.m.S, a.m.n_item) > level_rank(l, a.m.rank, a.m.S, a.m.n_item))
             atomicAdd(a.anomaly + q, 1);
     }
@@ -140,24 +135,6 @@ __device__ __forceinline__ void exact_pair(const ScArgs &a, int64_t u, int q, co
     for (int st = 16; st >= 1; st >>= 1) g += __ldg(summ + g + st - 1) >= full ? st : 0;
     g += __ldg(summ + g) >= full;
     a.code[o] = (uint8_t) min(g, a.nb);
-}
-
-// Counts one query column of a warp's pairs by coarse level into the chunk's shared-memory histogram
-// h ([2 sides][kLvEntries]).  Pairs at both implicit levels (the lower side's last, the upper side's
-// 0) are not counted; the others are grouped by their two levels, and one lane of each group adds the
-// group's size -- one atomic per distinct pair of levels instead of one per pair (the lanes of a warp
-// mostly share their levels).  (A bit-sliced form -- the levels balloted bit by bit and every bin
-// counted by its own lane -- costs about three times the instructions per pair.)
-__device__ __forceinline__ void warp_level_hist(uint32_t *h, bool count, int cl, int cu) {
-    const bool part = count && !(cl == kLvEntries - 1 && cu == 0);
-    const unsigned pm = __ballot_sync(0xffffffffu, part);
-    if (!part) return;
-    const unsigned m = __match_any_sync(pm, cl | (cu << 4));
-    if ((threadIdx.x & 31) == __ffs(m) - 1) {
-        const uint32_t n = (uint32_t) __popc(m);
-        if (cl != kLvEntries - 1) atomicAdd(h + cl, n);
-        if (cu != 0) atomicAdd(h + kLvEntries + cu, n);
-    }
 }
 
 // The bound scores of the regression round, qlb = partial - right and qub = partial + right
@@ -195,8 +172,7 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
     uint32_t *list = reinterpret_cast<uint32_t *>(summ + ThrSummary::kMaxGroups * kScSummStride);
     float4 *sq = reinterpret_cast<float4 *>(list + kScListCap);  // the batch's query data
     float *sqn = reinterpret_cast<float *>(sq + kScMaxQ);
-    uint32_t *shist = reinterpret_cast<uint32_t *>(sqn + kScMaxQ);           // [2][kScN][2][kLvEntries]
-    float2 *stab = reinterpret_cast<float2 *>(shist + 2 * kScN * 2 * kLvEntries);  // [2 kLvEntries][kScM]
+    float2 *stab = reinterpret_cast<float2 *>(sqn + kScMaxQ);  // [2 kLvEntries][kScM]
     volatile int *abort = &abort_flag;
 
     if (tid == 0) {
@@ -226,7 +202,6 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
             stab[j * kScM + rr] = u0 + rr < a.n_user ? __ldg(a.lvt + (u0 + rr) * 2 * kLvEntries + j)
                                                      : make_float2(NAN, NAN);
         }
-    for (int i = tid; i < 2 * kScN * 2 * kLvEntries; i += kScThreads) shist[i] = 0u;
     for (int i = tid; i < nchunks * kScN; i += kScThreads) {  // the last chunk padded with the last query
         sq[i] = __ldg(a.qmeta + min(i, nq - 1));
         sqn[i] = lev ? __ldg(a.qnorm + min(i, nq - 1)) : 0.0f;
@@ -315,15 +290,14 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
         const float2 *tl = stab + row, *tu = stab + kLvEntries * kScM + row;  // entry j at t[j * kScM]
         float un = 0.0f;
         float4 um = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        // the common cases of the two sides in registers, as (T - band, T + band) rounded outward: the
-        // lower side's last three boundaries T_12 .. T_14 (coarse levels 13 .. 15 hold all but about
-        // 0.1% of its pairs at config 2) and the upper side's first four T_0 .. T_3 (coarse levels 0 .. 3
-        // hold about 94% of its pairs), so that those pairs need no table search
-        float llo[3], lhi[3], ulo[4], uhi[4];
+        // the lower side's common cases in registers, as (T - band, T + band) rounded outward: its last
+        // three boundaries T_12 .. T_14 (coarse levels 13 .. 15 hold all but about 0.1% of its pairs at
+        // configs 2 and 4), so that those pairs need no table search.  The upper side's coarse levels
+        // spread over more boundaries (at config 4 nearly every warp holds a pair beyond T_3), so every
+        // pair takes its table search, without branches
+        float llo[3], lhi[3];
 #pragma unroll
         for (int g = 0; g < 3; g++) { llo[g] = -INFINITY; lhi[g] = INFINITY; }
-#pragma unroll
-        for (int g = 0; g < 4; g++) { ulo[g] = -INFINITY; uhi[g] = INFINITY; }
         if (uval) {
             um = __ldg(a.umeta + u);
             if (lev) {
@@ -335,13 +309,6 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                     llo[g] = __fsub_rd(e.x, e.y);
                     lhi[g] = __fadd_ru(e.x, e.y);
                     if (!(llo[g] == llo[g]) || !(lhi[g] == lhi[g])) { llo[g] = -INFINITY; lhi[g] = INFINITY; }
-                }
-#pragma unroll
-                for (int g = 0; g < 4; g++) {
-                    const float2 e = tu[g * kScM];
-                    ulo[g] = __fsub_rd(e.x, e.y);
-                    uhi[g] = __fadd_ru(e.x, e.y);
-                    if (!(ulo[g] == ulo[g]) || !(uhi[g] == uhi[g])) { ulo[g] = -INFINITY; uhi[g] = INFINITY; }
                 }
             }
         }
@@ -360,7 +327,6 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                 atomicExch(a.status, 1);
                 dead = true;
             }
-            uint32_t *hb = shist + b * (kScN * 2 * kLvEntries);
             if (!dead) {
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 float sl[8], sr[8];
@@ -420,9 +386,9 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                     if (lev) {
                         // coarse levels of the bounds partial -+ right (PartDimPartNorm::IPBound) from the
                         // tables; within dq of the reference's bound scores: the partial score's bound and
-                        // the two roundings of each side.  The register-cached boundaries decide most pairs
-                        // without branches; the table searches run afterwards, for the whole warp, where
-                        // any lane's pair needs one
+                        // the two roundings of each side.  The lower side's cached boundaries decide most
+                        // pairs without branches, and its table search runs afterwards, for the whole
+                        // warp, where any lane's pair needs one; the upper side searches every pair
                         unsigned needl = 0, needu = 0;
 #pragma unroll
                         for (int g = 0; g < G; g++) {
@@ -431,57 +397,32 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                             // lower side: coarse level 15 below T_14, 14 between T_14 and T_13, 13 between
                             // T_13 and T_12, each surely (outside the bands)
                             int c_l, c_u;
-                            bool okl, oku;
+                            bool okl;
                             {
                                 const float qml = __fsub_rd(qlb, dql), qpl = __fadd_ru(qlb, dql);
                                 const bool b14 = qpl < llo[2], b13 = qpl < llo[1], b12 = qpl < llo[0];
                                 okl = b14 || (qml >= lhi[2] && b13) || (qml >= lhi[1] && b12);
                                 c_l = b14 ? 15 : (b13 ? 14 : 13);
                             }
-                            // upper side: coarse level = boundaries surely above the score, decided when
-                            // none of the four is within reach and the level is below 4
-                            {
-                                const float qm = __fsub_rd(qub, dqu), qp = __fadd_ru(qub, dqu);
-                                int below = 0;
-                                bool amb = false;
-#pragma unroll
-                                for (int k = 0; k < 4; k++) {
-                                    const bool b = qp < ulo[k], ab = qm >= uhi[k];
-                                    below += b;
-                                    amb = amb || !(b || ab);
-                                }
-                                c_u = below;
-                                oku = !amb && below < 4;
-                            }
+                            const bool oku = lvt_screen(tu, kScM, qub, dqu, c_u);
                             needl |= (unsigned) !okl << g;
                             needu |= (unsigned) !oku << g;
                             packed[g] = c_l | (c_u << 4);
                         }
-                        if (__any_sync(0xffffffffu, (needl | needu) != 0u)) {
+                        n_sup += G;
+                        if (__any_sync(0xffffffffu, needl != 0u)) {
 #pragma unroll
                             for (int g = 0; g < G; g++) {
-                                const bool wl = (needl >> g) & 1u, wu = (needu >> g) & 1u;
-                                const bool sl_any = __any_sync(0xffffffffu, wl), su_any = __any_sync(0xffffffffu, wu);
-                                if (!(sl_any || su_any)) continue;
+                                const bool wl = (needl >> g) & 1u;
+                                if (!__any_sync(0xffffffffu, wl)) continue;
+                                n_slo++;
                                 float qlb, qub, dql, dqu;
                                 level_bounds(vl[g], dl[g], un, sqn[j * kScN + 8 * cg + i0 + g], qlb, qub, dql, dqu);
-                                if (sl_any) {
-                                    n_slo++;
-                                    int c;
-                                    const bool o = lvt_screen(tl, kScM, qlb, dql, c);
-                                    if (wl) {
-                                        packed[g] = (packed[g] & 0xf0) | c;
-                                        if (o) needl &= ~(1u << g);
-                                    }
-                                }
-                                if (su_any) {
-                                    n_sup++;
-                                    int c;
-                                    const bool o = lvt_screen(tu, kScM, qub, dqu, c);
-                                    if (wu) {
-                                        packed[g] = (packed[g] & 0x0f) | (c << 4);
-                                        if (o) needu &= ~(1u << g);
-                                    }
+                                int c;
+                                const bool o = lvt_screen(tl, kScM, qlb, dql, c);
+                                if (wl) {
+                                    packed[g] = (packed[g] & 0xf0) | c;
+                                    if (o) needl &= ~(1u << g);
                                 }
                             }
                         }
@@ -509,15 +450,6 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                         const bool gok = (lo[g] >= ThrSummary::kMaxGroups || srow[lo[g] * kScSummStride] < full[g] - df[g]) &&
                                          df[g] < 1e30f && full[g] == full[g];
                         ok[g] = ok[g] && gok;
-                    }
-                    // decided pairs are counted by coarse level (the undecided ones by the exact pass)
-                    if (lev) {
-#pragma unroll
-                        for (int g = 0; g < G; g++) {
-                            const int qi = 8 * cg + i0 + g;
-                            warp_level_hist(hb + qi * 2 * kLvEntries, uval && j * kScN + qi < nq && ok[g],
-                                            packed[g] & 15, packed[g] >> 4);
-                        }
                     }
                     // every pair is stored (the exact pass rewrites the undecided ones)
 #pragma unroll
@@ -558,22 +490,6 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                     }
                 }
             }
-            // the four warps of this column group (one per lane quadrant: the same 8 queries) have
-            // counted this chunk: the group's histograms go to the batch's (nonzero counters only) and
-            // are cleared for the chunk after next; every warp passes the same barriers, whether or not
-            // it gave up waiting
-            asm volatile("bar.sync %0, 128;" ::"r"(1 + cg) : "memory");
-            if (lev)
-                for (int i = 8 * cg * 2 * kLvEntries + 32 * quad + lane; i < (8 * cg + 8) * 2 * kLvEntries; i += 128) {
-                    const uint32_t n = hb[i];
-                    if (!n) continue;
-                    hb[i] = 0u;
-                    const int qi = i / (2 * kLvEntries), side = (i / kLvEntries) & 1, bin = i % kLvEntries;
-                    const int q = j * kScN + qi;
-                    // the lower side's last coarse level and the upper side's first stay implicit
-                    if (q < nq && bin != (side ? 0 : kLvEntries - 1))
-                        atomicAdd(a.lhist + ((int64_t) q * 2 + side) * kLvEntries + bin, (int) n);
-                }
         }
         if (n_und) atomicAdd(a.undecided, n_und);
         if (lane == 0 && (n_slo | n_sup)) {
@@ -679,7 +595,6 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, bool *do
     if (n_tiles > 0x7fffffff) return RKR_OK;
     const size_t smem = (size_t) kScSlices * kp * (kScM + 2 * kScN) + sizeof(float) * ThrSummary::kMaxGroups * kScM +
                         sizeof(uint32_t) * kScListCap + (sizeof(float4) + sizeof(float)) * kScMaxQ +
-                        sizeof(uint32_t) * 2 * kScN * 2 * kLvEntries +
                         (call.qsrp ? sizeof(float2) * 2 * kLvEntries * kScM : 0);
     if (smem + 1024 > 227 * 1024) return RKR_OK;
     // user digits for this split (built once per split and kept)
@@ -750,7 +665,6 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, bool *do
     a.lvt = call.qsrp ? ix->lvt.as<float2>() : nullptr;
     a.lvc = call.lvc;
     a.code = call.code;
-    a.lhist = call.lhist;
     a.anomaly = call.anomaly;
     a.dump = ix->score_dump;
     a.ovf = ovf;
@@ -789,7 +703,6 @@ int scores_tc(rkr_index *ix, const ScoresTcCall &call, cudaStream_t st, bool *do
         s.qrow = a.qrow + (size_t) q0 * dim;
         s.lvc = a.lvc ? a.lvc + (size_t) q0 * U : nullptr;
         s.code = a.code + (size_t) q0 * U;
-        s.lhist = a.lhist ? a.lhist + (size_t) q0 * 2 * kLvEntries : nullptr;
         s.anomaly = a.anomaly ? a.anomaly + q0 : nullptr;
         s.dump = a.dump ? a.dump + (size_t) q0 * U : nullptr;
         s.tile_rng = tile_rng + (size_t) (q0 / kScMaxQ) * n_tiles;

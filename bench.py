@@ -349,10 +349,12 @@ def kernel_model(name, cfg, nq, stats, method):
     return 0.0, 0.0, 0.0
 
 
-# DRAM bytes (read + write) per (query, user) pair of the pair-scores kernel, measured by one ncu
-# capture at a 200-query batch of the config-2 workload; traffic grows with the pairs a launch
-# processes, so a launch's traffic is this figure times its pairs.
-NCU_BYTES_PER_PAIR = {("qsrp_scores_tc", "QSRPNormalLP"): (456.031e6 + 814.108e6) / (200 * 480189.0)}
+# DRAM traffic of the pair-scores kernel from one ncu capture at a 200-query batch of the config-2
+# workload (dram__bytes_read.sum, dram__bytes_write.sum): the reads are the resident index (the
+# users' digit tiles, threshold summaries and level tables), streamed once per launch whatever its
+# queries; the writes are the two state bytes per (query, user) pair.  A launch's traffic is the
+# read figure plus the write figure per pair times its pairs.
+NCU_TRAFFIC = {("qsrp_scores_tc", "QSRPNormalLP"): (563.645e6, 171.521e6 / (200 * 480189.0))}
 
 # Nominal dense tensor-core peaks of one B200 (T ops/s), for the tensor_ops figures.
 TENSOR_PEAK_NOMINAL = {"qsrp_scores_tc": ("int8", 4500.0), "refine_tc": ("int8", 4500.0)}
@@ -469,14 +471,17 @@ def serve(R, ix, item, dim, seed, method, n_req, rate, max_batch=1024, n_workers
     submitted = threading.Semaphore(0)
     with R.Server(ix, method=method, max_batch_queries=max_batch, n_workers=n_workers,
                   workspace_bytes=workspace_bytes) as srv:
-        # warm-up: every batch size the trace can produce runs once eagerly and once captured
-        for nb in (16, 64, 256, 1024):
+        # warm-up: every batch size the trace can produce runs once eagerly and once captured (the
+        # server pads a batch to the next power of two; requests hold at most 256 items)
+        for nb in (16, 32, 64, 128, 256, 512, 1024):
             if nb > max_batch:
                 break
             for _ in range(2):
-                w = [srv.submit(item[:1], np.array([10], np.int32)) for _ in range(1)]
-                big = item[:min(nb, 256)]
-                w.append(srv.submit(big, np.full(big.shape[0], 200, np.int32)))
+                w, left = [], nb
+                while left > 0:
+                    n = min(left, 256)
+                    w.append(srv.submit(item[:n], np.full(n, 200 if n > 1 else 10, np.int32)))
+                    left -= n
                 for t in w:
                     srv.wait(t, timeout=600.0)
         c0 = srv.counters()
@@ -712,9 +717,10 @@ def main():
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    ncu_bpp = NCU_BYTES_PER_PAIR.get((dom_name, args.method))
-    traffic = (ncu_bpp * CONFIGS[args.config][0] * batch
-               if ncu_bpp is not None and args.config == "config2" else None)
+    ncu_t = NCU_TRAFFIC.get((dom_name, args.method))
+    launches = max(1, -(-batch // 1024))  # the scores kernel takes up to 1,024 queries per launch
+    traffic = (ncu_t[0] + ncu_t[1] * CONFIGS[args.config][0] * batch / launches
+               if ncu_t is not None and args.config == "config2" else None)
     roofline = {"kernel": dom_name, "bound": "hbm", "achieved": nbytes / avg_s / 1e9, "peak": hbm_peak,
                 "unit": "GB/s", "frac": (nbytes / avg_s / 1e9) / hbm_peak,
                 "peak_source": "MEASURED_PEAKS.json (of measured)" if peaks else "fallback",

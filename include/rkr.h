@@ -155,7 +155,7 @@ int rkr_query_device(rkr_index *index, int32_t method, const float *d_query, int
  * CUDA stream and work arrays over the shared resident index, take requests from the head of the
  * queue while they fit a batch (at most max_batch_queries items, and at most as many as the
  * workspace_bytes memory budget holds at about 2 bytes per (query item, user) pair; 0: no memory
- * limit beyond the slots), pad the batch to the next of the sizes 16, 64, 256, 1024, 4096 and replay
+ * limit beyond the slots), pad the batch to the next power of two from 16 to 4096 and replay
  * the CUDA graph captured for that size.  Each request gets the result a fresh index would give it
  * alone (QSRPNormalLP's carried per-user scores, QSRPNormalLP.hpp:73,109,213-218, are scoped to the
  * request), whatever it is batched with.  Methods: QS and QSRPNormalLP.  The index must stay loaded

@@ -1504,7 +1504,7 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
             });
             RKR_CUDA(cudaGetLastError());
             timed(ix, st, "qsrp_fine1_list", [&] {
-                qsrp_fine1_list_kernel<<<148 * 4, 256, 0, st>>>(lvc, r1, U, Sr, W, 0, par, f1, fhist, mismatch);
+                qsrp_fine1_list_kernel<<<148 * 16, 256, 0, st>>>(lvc, r1, U, Sr, W, 0, par, f1, fhist, mismatch);
             });
             RKR_CUDA(cudaGetLastError());
             timed(ix, st, "qsrp_select1f", [&] {
@@ -1519,7 +1519,7 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
             });
             RKR_CUDA(cudaGetLastError());
             timed(ix, st, "qsrp_fine1_list", [&] {
-                qsrp_fine1_list_kernel<<<148 * 4, 256, 0, st>>>(lvc, r1, U, Sr, W, 1, par, f1, fhist, mismatch);
+                qsrp_fine1_list_kernel<<<148 * 16, 256, 0, st>>>(lvc, r1, U, Sr, W, 1, par, f1, fhist, mismatch);
             });
             RKR_CUDA(cudaGetLastError());
             timed(ix, st, "qsrp_final1", [&] { qsrp_final1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, ks, U); });
@@ -1542,7 +1542,7 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
             qsrp_fine2_kernel<<<fg2, 256, 0, st>>>(code, qv, U, nq, inv_user, thr, S, gs, par, 0, any2, hl, hist_f);
         });
         RKR_CUDA(cudaGetLastError());
-        timed(ix, st, "qsrp_fine2_list", [&] { qsrp_fine2_list_kernel<<<148 * 8, 256, 0, st>>>(hl, qv, U, thr, S, gs, hist_f); });
+        timed(ix, st, "qsrp_fine2_list", [&] { qsrp_fine2_list_kernel<<<148 * 16, 256, 0, st>>>(hl, qv, U, thr, S, gs, hist_f); });
         RKR_CUDA(cudaGetLastError());
         timed(ix, st, "qsrp_select2f", [&] {
             qsrp_select2f_kernel<<<(nq + 3) / 4, 128, 0, st>>>(hist_f, nb, gs, S, srank, n_item, ks, nq, par, cls2, clsg, any2);
@@ -1553,7 +1553,7 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
             qsrp_fine2_kernel<<<fg2, 256, 0, st>>>(code, qv, U, nq, inv_user, thr, S, gs, par, 1, any2, hl, hist_f);
         });
         RKR_CUDA(cudaGetLastError());
-        timed(ix, st, "qsrp_fine2_list", [&] { qsrp_fine2_list_kernel<<<148 * 8, 256, 0, st>>>(hl, qv, U, thr, S, gs, hist_f); });
+        timed(ix, st, "qsrp_fine2_list", [&] { qsrp_fine2_list_kernel<<<148 * 16, 256, 0, st>>>(hl, qv, U, thr, S, gs, hist_f); });
         RKR_CUDA(cudaGetLastError());
         timed(ix, st, "qsrp_final2", [&] {
             qsrp_final2_kernel<<<(nq + 3) / 4, 128, 0, st>>>(hist_c, hist_f, nb, gs, S, ks, nq, qsrp ? m.rank : nullptr, Sr,

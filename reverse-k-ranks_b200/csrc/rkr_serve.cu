@@ -30,7 +30,8 @@ namespace rkr {
 namespace {
 
 // Batch sizes a worker pads to (each has its own captured graph).
-constexpr int kBuckets[] = {16, 64, 256, 1024, 4096};
+constexpr int kBuckets[] = {16, 32, 64, 128, 256, 512, 1024, 2048, 4096};
+constexpr int kLastBucket = sizeof(kBuckets) / sizeof(kBuckets[0]) - 1;
 
 struct Request {
     uint64_t ticket = 0;
@@ -122,8 +123,8 @@ void worker_loop(rkr_server *s, int w) {
     rkr_index *sh = s->shadows[w];
     cudaSetDevice(sh->device);
     const int dim = sh->dim;
-    const int cap = s->max_batch <= kBuckets[4] ? s->max_batch : kBuckets[4];
-    int bucket_max = kBuckets[4];
+    const int cap = s->max_batch <= kBuckets[kLastBucket] ? s->max_batch : kBuckets[kLastBucket];
+    int bucket_max = kBuckets[kLastBucket];
     for (int b : kBuckets)
         if (b >= cap) { bucket_max = b; break; }
     // pinned staging and device buffers for the largest batch

@@ -221,14 +221,11 @@ int rkr_index_destroy(rkr_index *ix) {
     if (ix->stream) cudaStreamSynchronize(ix->stream);
     for (DevBuf *b : {&ix->user, &ix->item, &ix->item_sorted, &ix->item_norm, &ix->item_rnorm, &ix->user_rnorm,
                       &ix->sample_rank, &ix->thr, &ix->thr_summ, &ix->reg_rank, &ix->reg, &ix->lvt, &ix->transfer_item,
-                      &ix->svd_user, &ix->svd_user_km, &ix->user_km, &ix->item_km, &ix->item_sorted_km, &ix->ws_km, &ix->ri_item_split,
-                      &ix->ri_imeta_split, &ix->ri_item_full, &ix->ri_imeta_full, &ix->ws_tc,
-                      &ix->svd_unorm, &ix->qip_state, &ix->ws_query, &ix->ws_qtr, &ix->ws_qnorm, &ix->ws_bucket,
-                      &ix->ws_bucket2, &ix->ws_levels, &ix->ws_cls, &ix->ws_counts, &ix->ws_hist, &ix->ws_res,
-                      &ix->ws_cand, &ix->ws_cand_off, &ix->ws_refine, &ix->ws_rank, &ix->ws_out, &ix->ws_stats,
-                      &ix->ws_misc, &ix->ws_fix, &ix->ws_sc, &ix->sc_user_split, &ix->sc_umeta_split,
-                      &ix->sc_user_full, &ix->sc_umeta_full, &ix->sc_cdf_tab})
+                      &ix->svd_user, &ix->svd_user_km, &ix->user_km, &ix->item_km, &ix->item_sorted_km, &ix->ri_item_split,
+                      &ix->ri_imeta_split, &ix->ri_item_full, &ix->ri_imeta_full, &ix->svd_unorm, &ix->qip_state,
+                      &ix->sc_user_split, &ix->sc_umeta_split, &ix->sc_user_full, &ix->sc_umeta_full, &ix->sc_cdf_tab})
         b->release();
+    for (DevBuf *b : ix->workspaces()) b->release();
     ix->prof.release();
     for (auto &g : ix->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);

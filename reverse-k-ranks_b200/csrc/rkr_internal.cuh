@@ -910,12 +910,34 @@ __global__ void __launch_bounds__(256) compact_need_flat_kernel(P p, int64_t n_u
     }
 }
 
+// Every listed user classified at once (one thread per list entry over all queries, so that the
+// reference-arithmetic recomputations of many queries overlap), with the data its emission needs.
+template <class P>
+__global__ void __launch_bounds__(256) compact_classify_kernel(P p, int nq, const int32_t *__restrict__ need_n,
+                                                              const int32_t *__restrict__ need_u,
+                                                              int8_t *__restrict__ cls, typename P::Aux *__restrict__ aux) {
+    const int64_t total = (int64_t) nq * kNeedCap;
+    for (int64_t idx = (int64_t) blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (int64_t) gridDim.x * blockDim.x) {
+        const int q = (int) (idx / kNeedCap), i = (int) (idx % kNeedCap);
+        const int n = need_n[q];
+        if (n > kNeedCap || i >= n) continue;  // unused slot, or a query left to the two-pass form
+        typename P::Aux a;
+        cls[idx] = (int8_t) p.classify(q, need_u[idx], a, true);
+        aux[idx] = a;
+    }
+}
+
+// One block per query: its list sorted by user id (the order the reference lists users in), then
+// the ordered emission from the classes compact_classify_kernel stored.
 template <class P>
 __global__ void __launch_bounds__(kCompactThreads) compact_emit_kernel(P p, KSpec ks, const int32_t *__restrict__ need_n,
                                                                      const int32_t *__restrict__ need_u,
+                                                                     const int8_t *__restrict__ cls,
+                                                                     const typename P::Aux *__restrict__ aux_l,
                                                                      QueryCounts *__restrict__ counts, int *__restrict__ err,
                                                                      int32_t *__restrict__ ovf_q) {
-    __shared__ int32_t s[kNeedCap];
+    __shared__ uint64_t s[kNeedCap];  // user id << 12 | list position
     __shared__ int warp_tot[9];
     const int q = blockIdx.x, tid = threadIdx.x;
     const int n = need_n[q], topk = ks.of(q);
@@ -925,15 +947,17 @@ __global__ void __launch_bounds__(kCompactThreads) compact_emit_kernel(P p, KSpe
     }
     int pn = 1;
     while (pn < n) pn <<= 1;
-    for (int i = tid; i < pn; i += kCompactThreads) s[i] = i < n ? need_u[(int64_t) q * kNeedCap + i] : INT32_MAX;
+    const int64_t row = (int64_t) q * kNeedCap;
+    for (int i = tid; i < pn; i += kCompactThreads)
+        s[i] = i < n ? ((uint64_t) (uint32_t) need_u[row + i] << 12) | (uint64_t) i : ~uint64_t(0);
     __syncthreads();
-    // bitonic sort, ascending user id (the order the reference lists users in)
+    // bitonic sort, ascending user id
     for (int k = 2; k <= pn; k <<= 1)
         for (int j = k >> 1; j > 0; j >>= 1) {
             for (int i = tid; i < pn; i += kCompactThreads) {
                 const int ij = i ^ j;
                 if (ij > i) {
-                    const int32_t a = s[i], b = s[ij];
+                    const uint64_t a = s[i], b = s[ij];
                     if ((a > b) == ((i & k) == 0)) {
                         s[i] = b;
                         s[ij] = a;
@@ -945,16 +969,18 @@ __global__ void __launch_bounds__(kCompactThreads) compact_emit_kernel(P p, KSpe
     int pr = 0, pc = 0;  // results and candidates before this tile
     for (int t0 = 0; t0 < n; t0 += kCompactThreads) {
         const int i = t0 + tid;
-        const int64_t u = i < n ? s[i] : 0;
-        // classified once, with the data its emission needs (a user classified here is emitted
-        // unless it is a result past the query's k)
-        typename P::Aux aux;
-        const int k = i < n ? p.classify(q, u, aux, true) : 0;
+        int k = 0;
+        int64_t u = 0, at = 0;
+        if (i < n) {
+            u = (int64_t) (s[i] >> 12);
+            at = row + (int64_t) (s[i] & 0xfff);
+            k = cls[at];
+        }
         int tot;
         const int pre = block_excl_scan((k == 1) | ((k == 2) << 16), warp_tot, &tot);
         const int rpos = pr + (pre & 0xffff), cpos = pc + (pre >> 16);
-        if (k == 1 && rpos < topk) p.emit_result(q, rpos, u, aux);
-        else if (k == 2) p.emit_cand(q, cpos, u, aux);
+        if (k == 1 && rpos < topk) p.emit_result(q, rpos, u, aux_l[at]);
+        else if (k == 2) p.emit_cand(q, cpos, u, aux_l[at]);
         pr += tot & 0xffff;
         pc += tot >> 16;
     }
@@ -1065,6 +1091,14 @@ struct rkr_index {
     rkr::DevBuf ws_query, ws_qtr, ws_qnorm, ws_bucket, ws_bucket2, ws_levels, ws_cls, ws_counts, ws_hist;
     rkr::DevBuf ws_res, ws_cand, ws_cand_off, ws_refine, ws_rank, ws_out, ws_stats, ws_misc, ws_fix, ws_km, ws_tc, ws_sc;
     rkr::DevBuf ws_defer;  // rows the streaming row selection left to the scatter form
+    rkr::DevBuf ws_emit;   // the sparse compaction's classes and emission data per list entry
+    // Every per-call workspace buffer: a serving worker's shadow of the index owns its own (the
+    // resident data it shares), and destruction releases them.
+    std::vector<rkr::DevBuf *> workspaces() {
+        return {&ws_query, &ws_qtr, &ws_qnorm, &ws_bucket, &ws_bucket2, &ws_levels, &ws_cls, &ws_counts, &ws_hist,
+                &ws_res, &ws_cand, &ws_cand_off, &ws_refine, &ws_rank, &ws_out, &ws_stats, &ws_misc, &ws_fix,
+                &ws_km, &ws_tc, &ws_sc, &ws_defer, &ws_emit};
+    }
     std::vector<uint8_t> h_scratch;
     rkr::Profiler prof;
     // CUDA graphs of a batch's phase 1 (rkr_qsrp.cu), one per (method, batch size, workspace
@@ -1117,8 +1151,17 @@ inline int run_compaction(rkr_index *ix, P p, int nq, KSpec ks, QueryCounts *cou
             compact_need_flat_kernel<P><<<148 * 8, 256, 0, st>>>(p, U, nq, 1.0 / (double) U, need_n, need_u);
         });
         RKR_CUDA(cudaGetLastError());
+        RKR_TRY(ix->ws_emit.ensure((sizeof(int8_t) + sizeof(typename P::Aux)) * (size_t) nq * kNeedCap + 256));
+        int8_t *cls = ix->ws_emit.as<int8_t>();
+        auto *aux = reinterpret_cast<typename P::Aux *>(ix->ws_emit.as<uint8_t>() +
+                                                        (((size_t) nq * kNeedCap + 255) & ~size_t(255)));
+        timed(ix, st, "compact_classify", [&] {
+            compact_classify_kernel<P><<<148 * 16, 256, 0, st>>>(p, nq, need_n, need_u, cls, aux);
+        });
+        RKR_CUDA(cudaGetLastError());
         timed(ix, st, "compact_emit", [&] {
-            compact_emit_kernel<P><<<(unsigned) nq, kCompactThreads, 0, st>>>(p, ks, need_n, need_u, counts, err, ovf_q);
+            compact_emit_kernel<P><<<(unsigned) nq, kCompactThreads, 0, st>>>(p, ks, need_n, need_u, cls, aux, counts,
+                                                                             err, ovf_q);
         });
         RKR_CUDA(cudaGetLastError());
         RKR_CUDA(cudaMemcpyAsync(h_err, err, sizeof(h_err), cudaMemcpyDeviceToHost, st));

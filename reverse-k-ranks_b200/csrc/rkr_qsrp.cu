@@ -357,9 +357,15 @@ __global__ void __launch_bounds__(kHistThreads) lvc_hist_kernel(const uint8_t *_
         const int n = (int) min((int64_t) 16, u1 - ub);
         uint32_t w[4];
         load16_bytes(row + ub, w);
+        if (n < 16)  // past the chunk: bytes at both implicit levels, which count nowhere
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                const int keep = max(0, min(4, n - 4 * i));
+                const uint32_t m = keep == 4 ? 0xffffffffu : (1u << (8 * keep)) - 1u;
+                w[i] = (w[i] & m) | (0x0f0f0f0fu & ~m);
+            }
 #pragma unroll
         for (int e = 0; e < 16; e++) {
-            if (e >= n) break;
             const unsigned v = (w[e >> 2] >> (8 * (e & 3))) & 0xffu;
             const int cl = (int) (v & 15), cu = (int) (v >> 4);
             if (cl != kLvEntries - 1) h[cl * kHistThreads + tid]++;
@@ -487,94 +493,98 @@ struct Fine1List {
     int cap;
 };
 
-// The scan: the batch's coarse-level bytes as one flat [query][user] array, 16 per lane and 512 per
-// warp and step (a segment meets at most one query boundary when n_user >= 512).
+// The scan: the batch's coarse-level bytes as one flat [query][user] array, 64 per lane and 2,048 per
+// warp and step (a lane's bytes nearly always lie in one query row; a lane across a row's end goes
+// byte by byte).
 __global__ void __launch_bounds__(256) qsrp_fine1_scan_kernel(uint8_t *__restrict__ lvc, Round1Src src, int64_t n_user,
                                                              int nq, double inv_user, int S, int W, int mode,
                                                              QsrpParams *__restrict__ par, Fine1List fl,
                                                              int *__restrict__ fhist, int *__restrict__ mismatch,
                                                              int *__restrict__ n_hits) {
+    constexpr int kLaneBytes = 64, kSeg = 32 * kLaneBytes;  // bytes per lane and per warp step
     const int64_t total = n_user * nq;
     const int lane = threadIdx.x & 31;
     const int64_t warp = ((int64_t) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int64_t stride = (int64_t) gridDim.x * blockDim.x * 16;
-    // the lane's 16 bytes of a segment (zero past the end)
-    auto load = [&](int64_t seg, uint32_t w[4]) {
-        const int64_t base = seg + (int64_t) lane * 16;
-        if (base + 16 <= total) {
-            const uint4 x = *reinterpret_cast<const uint4 *>(lvc + base);
-            w[0] = x.x; w[1] = x.y; w[2] = x.z; w[3] = x.w;
-        } else {
+    const int64_t stride = (int64_t) gridDim.x * (blockDim.x / 32) * kSeg;
+    // the lane's 64 bytes of a step (zero past the end), as four aligned 16-byte loads
+    auto load = [&](int64_t seg, uint4 w[4]) {
+        const int64_t base = seg + (int64_t) lane * kLaneBytes;
 #pragma unroll
-            for (int i = 0; i < 4; i++) {
-                w[i] = 0;
-                for (int j = 0; j < 4; j++)
-                    if (base + 4 * i + j < total) w[i] |= (uint32_t) lvc[base + 4 * i + j] << (8 * j);
+        for (int k = 0; k < 4; k++) {
+            const int64_t b = base + 16 * k;
+            if (b + 16 <= total) {
+                w[k] = *reinterpret_cast<const uint4 *>(lvc + b);
+            } else {
+                uint32_t x[4] = {0u, 0u, 0u, 0u};
+                for (int j = 0; j < 16; j++)
+                    if (b + j < total) x[j >> 2] |= (uint32_t) lvc[b + j] << (8 * (j & 3));
+                w[k] = make_uint4(x[0], x[1], x[2], x[3]);
             }
         }
     };
-    uint32_t wn[4] = {0u, 0u, 0u, 0u};
-    if (warp * 512 < total) load(warp * 512, wn);
-    for (int64_t seg = warp * 512; seg < total; seg += stride) {
-        const int64_t base = seg + (int64_t) lane * 16;
-        // this segment's bytes, and the next segment's load in flight while they are examined
-        uint32_t w[4] = {wn[0], wn[1], wn[2], wn[3]};
+    uint4 wn[4] = {};
+    if (warp * kSeg < total) load(warp * kSeg, wn);
+    for (int64_t seg = warp * kSeg; seg < total; seg += stride) {
+        const int64_t base = seg + (int64_t) lane * kLaneBytes;
+        // this step's bytes, and the next step's loads in flight while they are examined
+        uint4 cur[4] = {wn[0], wn[1], wn[2], wn[3]};
         if (seg + stride < total) load(seg + stride, wn);
-        // the segment's first query (once per warp) and the lane's queries
-        int64_t qs = 0;
+        const uint32_t *w = reinterpret_cast<const uint32_t *>(cur);  // 16 words, byte e in word e >> 2
+        // the step's first query and the end of its row, once per warp; a lane's row follows from
+        // them by additions
+        int64_t qs = 0, e0 = 0;
         if (lane == 0) {
             qs = (int64_t) ((double) seg * inv_user);
             if (qs * n_user > seg) qs--;
             else if ((qs + 1) * n_user <= seg) qs++;
+            e0 = (qs + 1) * n_user;
         }
         qs = __shfl_sync(0xffffffffu, qs, 0);
-        uint32_t hits = 0;
+        e0 = __shfl_sync(0xffffffffu, e0, 0);
+        uint64_t hits = 0;
         if (base < total) {
-            int64_t q = qs;
-            while ((q + 1) * n_user <= base) q++;
-            int64_t edge = (q + 1) * n_user;
+            int64_t q = qs, edge = e0;
+            while (edge <= base) { q++; edge += n_user; }
             int wl = par[q].w_l, wu = par[q].w_u, wa = par[q].w_all;
-            if (base + 16 <= edge && base + 16 <= total) {
-                // the lane's 16 pairs in one query row: four bytes at a time, the nibbles compared in
+            if (base + kLaneBytes <= edge && base + kLaneBytes <= total) {
+                // the lane's 64 pairs in one query row: four bytes at a time, the nibbles compared in
                 // parallel (a byte of t = nibbles ^ wanted is below 0x20, so t + 0x7f keeps its carry
                 // inside the byte: bit 7 is set exactly where the nibble differs)
                 if (wa) {
-                    hits = 0xffffu;
+                    hits = ~uint64_t(0);
                 } else {
                     const uint32_t ml = (uint32_t) (wl >= 0 ? wl : 16) * 0x01010101u;
                     const uint32_t mu = (uint32_t) (wu >= 0 ? wu : 16) * 0x01010101u;
 #pragma unroll
-                    for (int i = 0; i < 4; i++) {
+                    for (int i = 0; i < 16; i++) {
                         const uint32_t tl = (w[i] & 0x0f0f0f0fu) ^ ml, tu = ((w[i] >> 4) & 0x0f0f0f0fu) ^ mu;
                         const uint32_t diff = ((tl + 0x7f7f7f7fu) & (tu + 0x7f7f7f7fu)) & 0x80808080u;
                         const uint32_t eq = diff ^ 0x80808080u;  // bit 7 of each byte: a nibble matches
-                        hits |= ((eq * 0x00204081u) >> 28) << (4 * i);
+                        hits |= (uint64_t) ((eq * 0x00204081u) >> 28) << (4 * i);
                     }
                 }
             } else {
-#pragma unroll
-                for (int e = 0; e < 16; e++) {
+                for (int e = 0; e < kLaneBytes; e++) {
                     const int64_t pos = base + e;
                     if (pos >= total) break;
                     if (pos >= edge) {  // the next query (and the one after, for short rows)
-                        while ((q + 1) * n_user <= pos) q++;
-                        edge = (q + 1) * n_user;
+                        while (edge <= pos) { q++; edge += n_user; }
                         wl = par[q].w_l; wu = par[q].w_u; wa = par[q].w_all;
                     }
-                    const unsigned v = (w[e >> 2] >> (8 * (e & 3))) & 0xffu;
-                    hits |= (uint32_t) (wa || (int) (v & 15) == wl || (int) (v >> 4) == wu) << e;
+                    const unsigned v = lvc[pos];  // rare: a lane across a row's end (its words stay in registers)
+                    hits |= (uint64_t) (wa || (int) (v & 15) == wl || (int) (v >> 4) == wu) << e;
                 }
             }
         }
         if (n_hits) {
-            const int c = __popc(hits);
+            const int c = __popcll(hits);
             const int tot = __reduce_add_sync(0xffffffffu, c);
             if (lane == 0 && tot) atomicAdd(n_hits + mode, tot);
         }
         // one hit per lane and round: warp-aggregated appends
         while (__any_sync(0xffffffffu, hits != 0)) {
             const bool have = hits != 0;
-            const int e = have ? __ffs(hits) - 1 : 0;
+            const int e = have ? __ffsll((long long) hits) - 1 : 0;
             const unsigned want = __ballot_sync(0xffffffffu, have);
             const int leader = __ffs(want) - 1;
             int at = 0;
@@ -582,12 +592,10 @@ __global__ void __launch_bounds__(256) qsrp_fine1_scan_kernel(uint8_t *__restric
             at = __shfl_sync(0xffffffffu, at, leader) + __popc(want & ((1u << lane) - 1));
             if (have) {
                 const int64_t pos = base + e;
-                const int64_t q = (int64_t) ((double) pos * inv_user);
-                int64_t qq = q;
-                if (qq * n_user > pos) qq--;
-                else if ((qq + 1) * n_user <= pos) qq++;
-                const int64_t u = pos - qq * n_user;
-                const unsigned v = (w[e >> 2] >> (8 * (e & 3))) & 0xffu;
+                int64_t qq = qs, eq = e0;
+                while (eq <= pos) { qq++; eq += n_user; }
+                const int64_t u = pos - (eq - n_user);
+                const unsigned v = lvc[pos];
                 if (at < fl.cap) fl.e[at] = ((uint64_t) qq << 40) | ((uint64_t) u << 8) | v;
                 else fine1_hit(mode, par, src, u, (int) qq, v, lvc + pos, S, W, fhist, mismatch);
                 hits &= hits - 1;

@@ -54,10 +54,7 @@ double now_s() {
 // arrays, graphs and profiler are its own.
 rkr_index *shadow_create(const rkr_index *ix, int *status) {
     rkr_index *sh = new rkr_index(*ix);
-    for (DevBuf *b : {&sh->ws_query, &sh->ws_qtr, &sh->ws_qnorm, &sh->ws_bucket, &sh->ws_bucket2, &sh->ws_levels,
-                      &sh->ws_cls, &sh->ws_counts, &sh->ws_hist, &sh->ws_res, &sh->ws_cand, &sh->ws_cand_off,
-                      &sh->ws_refine, &sh->ws_rank, &sh->ws_out, &sh->ws_stats, &sh->ws_misc, &sh->ws_fix, &sh->ws_km,
-                      &sh->ws_tc, &sh->ws_sc}) {
+    for (DevBuf *b : sh->workspaces()) {
         b->p = nullptr;
         b->bytes = 0;
     }
@@ -81,11 +78,7 @@ void shadow_destroy(rkr_index *sh) {
     if (!sh) return;
     cudaSetDevice(sh->device);
     if (sh->stream) cudaStreamSynchronize(sh->stream);
-    for (DevBuf *b : {&sh->ws_query, &sh->ws_qtr, &sh->ws_qnorm, &sh->ws_bucket, &sh->ws_bucket2, &sh->ws_levels,
-                      &sh->ws_cls, &sh->ws_counts, &sh->ws_hist, &sh->ws_res, &sh->ws_cand, &sh->ws_cand_off,
-                      &sh->ws_refine, &sh->ws_rank, &sh->ws_out, &sh->ws_stats, &sh->ws_misc, &sh->ws_fix, &sh->ws_km,
-                      &sh->ws_tc, &sh->ws_sc})
-        b->release();
+    for (DevBuf *b : sh->workspaces()) b->release();
     sh->prof.release();
     for (auto &g : sh->graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);

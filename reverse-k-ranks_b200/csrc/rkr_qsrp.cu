@@ -46,6 +46,8 @@ int refine_and_assemble_pairs(rkr_index *ix, int method, const float *d_query, i
 
 // Round-2 codes per pair: 0..nb a coarse threshold group (nb: bucket S); otherwise the round-1 state.
 constexpr uint8_t kCodeResult1 = 0xfe, kCodePruned1 = 0xff;
+// Round 2 counts the codes below this group exactly in its first pass (qsrp_round2_kernel).
+constexpr int kRound2Cap = 12;
 constexpr uint8_t kClsMixed = 0xff;  // a group whose buckets fall in more than one class
 // Coarse-level bytes per pair: lower-bound coarse level (1 .. 15) | upper-bound coarse level << 4.  A
 // lower nibble of 0 never occurs for a level, so it marks a pair whose round-1 class the fine pass
@@ -64,7 +66,8 @@ struct QsrpParams {
     int32_t cbl, cbu, cum_l, cum_u;        // round 1: critical coarse levels (-1: none needed), counts below
     int32_t amb_l, amb_u, res_fine, ple_fine;  // coarse levels straddling a class threshold; their counts
     int32_t c_res, c_pr, c_m1, w_all;      // coarse-level thresholds of the classes (class1_coarse);
-    int32_t w_l, w_u, pad3, pad4;          // the coarse levels the next fine scan looks for (-1: none), or all
+    int32_t w_l, w_u, r2_full, pad4;       // the coarse levels the next fine scan looks for (-1: none), or all;
+                                           // r2_full: round 2 needs the full group histogram
 };
 
 // The lowest level of coarse level c (its levels are lvt_lo(c) .. lvt_level(c)).
@@ -731,15 +734,29 @@ __global__ void qs_params_kernel(QsrpParams *__restrict__ par, int nq, int64_t n
 
 // Round 2 per (user chunk, query): pairs that did not reach round 2 get their round-1 state code in
 // place of the group code; the others are counted by group (per-warp shared-memory copies).
+// The word of w holding byte e (0 .. 15), without indexing the array by a run-time value.
+__device__ __forceinline__ uint32_t word_of(const uint32_t w[4], int e) {
+    return e < 8 ? (e < 4 ? w[0] : w[1]) : (e < 12 ? w[2] : w[3]);
+}
+
+// Pass 0: the round-1 class of every pair (non-survivors' codes rewritten to kCodeResult1 /
+// kCodePruned1), the survivors counted by code for codes below cap only, and the survivors' total at
+// index nb + 1 of the row: qsrp_select2c takes the critical group from those low groups and the
+// lumped count of the rest, where that is exact, and otherwise flags the query for pass 1.  Most
+// codes are at or above cap (at config 2, 89% of pairs), so most bytes cost a few word operations.
+// Pass 1 (flagged queries only): every survivor's code counted (codes 0 .. nb; the non-survivors'
+// rewritten codes lie above nb).  Row stride of hist_c: nb + 2.
 __global__ void __launch_bounds__(kHistThreads) qsrp_round2_kernel(const uint8_t *__restrict__ lvc,
                                                                   uint8_t *__restrict__ code, int64_t n_user,
-                                                                  const QsrpParams *__restrict__ par, int nb,
-                                                                  int64_t chunk, int *__restrict__ hist_c) {
+                                                                  const QsrpParams *__restrict__ par, int nb, int cap,
+                                                                  int pass, int64_t chunk, int *__restrict__ hist_c) {
     // per-thread counts, bin-major ([bin][thread]): a thread's counters sit in its own bank, so the
     // increments of a warp never conflict and need no atomics
     extern __shared__ int h[];
-    const int nbin = nb + 1, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int q = blockIdx.y;
+    if (pass == 1 && !par[q].r2_full) return;
+    const int nbin = pass == 0 ? cap : nb + 1;
     QsrpParams p;
     {
         const QsrpParams &g = par[q];
@@ -749,67 +766,98 @@ __global__ void __launch_bounds__(kHistThreads) qsrp_round2_kernel(const uint8_t
     // The common classes of round 1 four bytes at a time (nibbles n < 16, so n + k with k <= 0x80
     // keeps its carry inside the byte): cl > c_res is bit 7 of cl + 0x7f - c_res, cu >= c_pr bit 7 of
     // cu + 0x80 - c_pr, and a zero low nibble marks a pair the fine pass resolved.  Bytes flagged by
-    // any of the three take class1_coarse; the others are round-2 survivors.
+    // any of the three take class1_coarse; the others are round-2 survivors.  Codes below cap:
+    // bit 7 clear in c + 0x80 - cap (codes are at most nb < 0x60 here).
     const bool swar = !all_survive && !p.mode1 && !p.all1;
     const uint32_t kres = (uint32_t) (0x7f - p.c_res) * 0x01010101u;
     const uint32_t kpr = (uint32_t) (0x80 - p.c_pr) * 0x01010101u;
+    const uint32_t kcap = (uint32_t) (0x80 - cap) * 0x01010101u;
     for (int b = 0; b < nbin; b++) h[b * kHistThreads + tid] = 0;
     const uint8_t *lrow = lvc ? lvc + (int64_t) q * n_user : nullptr;
     uint8_t *crow = code + (int64_t) q * n_user;
     const int64_t u0 = (int64_t) blockIdx.x * chunk, u1 = min(u0 + chunk, n_user);
+    int n_surv = 0;
     // 16 consecutive users per thread and step, their bytes from five aligned words per row
     for (int64_t ub = u0 + (int64_t) tid * 16; ub < u1; ub += (int64_t) kHistThreads * 16) {
         const int n = (int) min((int64_t) 16, u1 - ub);
-        uint32_t lw[4] = {0u, 0u, 0u, 0u}, cw[4];
-        if (!all_survive) load16_bytes(lrow + ub, lw);
+        const uint32_t valid = n >= 16 ? 0xffffu : (1u << n) - 1u;
+        uint32_t cw[4];
         load16_bytes(crow + ub, cw);
-        uint32_t flag = 0;  // bytes whose class takes class1_coarse
-        if (swar) {
+        if (pass == 1) {
 #pragma unroll
-            for (int i = 0; i < 4; i++) {
+            for (int e = 0; e < 16; e++) {
+                const unsigned c = (cw[e >> 2] >> (8 * (e & 3))) & 0xffu;
+                if (((valid >> e) & 1u) && c <= (unsigned) nb) h[c * kHistThreads + tid]++;
+            }
+            continue;
+        }
+        uint32_t lw[4] = {0u, 0u, 0u, 0u};
+        if (!all_survive) load16_bytes(lrow + ub, lw);
+        uint32_t flag = 0, low = 0;  // bytes whose class takes class1_coarse; codes below cap
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const uint32_t lt = ((cw[i] + kcap) & 0x80808080u) ^ 0x80808080u;
+            low |= ((lt * 0x00204081u) >> 28) << (4 * i);
+            if (swar) {
                 const uint32_t lo = lw[i] & 0x0f0f0f0fu, hi = (lw[i] >> 4) & 0x0f0f0f0fu;
                 const uint32_t le_res = ((lo + kres) & 0x80808080u) ^ 0x80808080u;
                 const uint32_t ge_pr = (hi + kpr) & 0x80808080u;
                 const uint32_t zero = ((lo + 0x7f7f7f7fu) & 0x80808080u) ^ 0x80808080u;
                 flag |= (((le_res | ge_pr | zero) * 0x00204081u) >> 28) << (4 * i);
             }
-        } else if (!all_survive) {
-            flag = 0xffffu;
         }
-        flag &= n >= 16 ? 0xffffu : (1u << n) - 1u;
-#pragma unroll
-        for (int e = 0; e < 16; e++) {
-            if (e >= n) break;
-            const unsigned c = (cw[e >> 2] >> (8 * (e & 3))) & 0xffu;
+        if (!all_survive && !swar) flag = 0xffffu;
+        flag &= valid;
+        low &= valid;
+        int n_out = 0;
+        for (uint32_t m = flag | low; m; m &= m - 1) {
+            const int e = __ffs(m) - 1;
+            const unsigned c = (word_of(cw, e) >> (8 * (e & 3))) & 0xffu;
             bool surv = true;
             if ((flag >> e) & 1u) {
-                const unsigned v = (lw[e >> 2] >> (8 * (e & 3))) & 0xffu;
+                const unsigned v = (word_of(lw, e) >> (8 * (e & 3))) & 0xffu;
                 const int k = class1_coarse(p, v);
                 surv = k == kClsRefine || k == kClsIdle;
-                if (!surv) crow[ub + e] = k == kClsResult ? kCodeResult1 : kCodePruned1;
+                if (!surv) {
+                    crow[ub + e] = k == kClsResult ? kCodeResult1 : kCodePruned1;
+                    n_out++;
+                }
             }
-            if (surv) h[min(c, (unsigned) nb) * kHistThreads + tid]++;  // codes are 0 .. nb here
+            if (surv && c < (unsigned) cap) h[c * kHistThreads + tid]++;
         }
+        n_surv += n - n_out;
     }
     __syncthreads();
-    int *gh = hist_c + (int64_t) q * nbin;
+    int *gh = hist_c + (int64_t) q * (nb + 2);
     for (int b = warp; b < nbin; b += kHistThreads / 32) {
         int sum = 0;
         for (int t = lane; t < kHistThreads; t += 32) sum += h[b * kHistThreads + t];
         sum = __reduce_add_sync(0xffffffffu, sum);
         if (lane == 0 && sum) atomicAdd(gh + b, sum);
     }
+    if (pass == 0) {
+        n_surv = __reduce_add_sync(0xffffffffu, n_surv);
+        if (lane == 0 && n_surv) atomicAdd(gh + nb + 1, n_surv);
+    }
 }
 
 // Round-2 selection, coarse step (second PruneCandidateByBound call, QSRPNormalLP.hpp:187-190):
 // the coarse group holding the kp-th smallest bucket among the users that reached round 2
 // (kp = topk - round-1 results), or, with fewer such users than kp, the highest occupied group.
-__global__ void qsrp_select2c_kernel(const int *__restrict__ hist_c, int nb, KSpec ks, int nq,
-                                     QsrpParams *__restrict__ par, QueryCounts *__restrict__ counts) {
+// Pass 0 reads the capped histogram of qsrp_round2_kernel's pass 0: when the kp-th smallest code lies
+// at least two groups below cap, every group from cap on lies beyond the upper bound of the k-th
+// bucket's neighbour (their buckets are pruned, PruneCandidateByBound.hpp:83-150) and their count is
+// the survivors' total minus the low groups', kept in group cap; otherwise the query is flagged for
+// the full histogram (pass 1 of both kernels).
+__global__ void qsrp_select2c_kernel(int *__restrict__ hist_c, int nb, int cap, int pass, const int32_t *__restrict__ rank,
+                                     int gs, KSpec ks, int nq, QsrpParams *__restrict__ par,
+                                     QueryCounts *__restrict__ counts) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= nq) return;
     const int topk = ks.of(q);
     QsrpParams p = par[q];
+    if (pass == 1 && !p.r2_full) return;
+    if (pass == 0) p.r2_full = 0;
     p.crit = -1; p.cum_before = -1; p.mask1 = 0; p.mask2 = 0; p.gneed_lo = 0; p.gneed_hi = 0;
     if (p.skip2) {
         QueryCounts c = {};
@@ -822,8 +870,36 @@ __global__ void qsrp_select2c_kernel(const int *__restrict__ hist_c, int nb, KSp
         par[q] = p;
         return;
     }
-    const int *h = hist_c + (int64_t) q * (nb + 1);
+    int *h = hist_c + (int64_t) q * (nb + 2);
     const int kp = topk - p.n_res1;
+    if (pass == 0 && cap <= nb - 1) {
+        const int64_t total = h[nb + 1];
+        int64_t cum = 0;
+        int crit = -1;
+        if (total >= kp)
+            for (int g = 0; g < cap; g++) {
+                if (cum + h[g] >= kp) { crit = g; break; }
+                cum += h[g];
+            }
+        const int lo_b = max(0, (crit + 1) * gs - 2);  // at or above the k-th bucket's lower neighbour
+        if (crit >= 0 && crit <= cap - 2 && rank[cap * gs] > rank[lo_b]) {
+            int64_t low = 0;
+            for (int g = 0; g < cap; g++) low += h[g];
+            h[cap] = (int) (total - low);
+            p.n_elig2 = (int) total;
+            p.crit = crit;
+            p.cum_before = (int) cum;
+            p.r2_full = 0;
+            if (p.crit < nb) p.mask1 = (int32_t) (1u << p.crit);
+            par[q] = p;
+            return;
+        }
+        // the full histogram: pass 1 recounts every group
+        for (int g = 0; g <= nb + 1; g++) h[g] = 0;
+        p.r2_full = 1;
+        par[q] = p;
+        return;
+    }
     int64_t n_el = 0;
     for (int g = 0; g <= nb; g++) n_el += h[g];
     p.n_elig2 = (int) n_el;
@@ -1059,7 +1135,7 @@ __global__ void qsrp_final2_kernel(const int *__restrict__ hist_c, const int *__
         c.n_prune = p.n_pr1;
         c.n_cand = 0;
     } else {
-        const int *hc = hist_c + (int64_t) q * (nb + 1);
+        const int *hc = hist_c + (int64_t) q * (nb + 2);
         const int *hf = hist_f + (int64_t) q * (S + 1);
         int64_t n[4] = {0, 0, 0, 0};
         for (int g = lane; g <= nb; g += 32) {
@@ -1373,7 +1449,7 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
     uint8_t *lvc = qsrp ? code + code_bytes : nullptr;
     RKR_TRY(ix->ws_cls.ensure(carve_size((size_t) nq * (S + 1), 1) + carve_size((size_t) nq * (nb + 1), 1)));
     RKR_TRY(ix->ws_counts.ensure(sizeof(QueryCounts) * (size_t) nq));
-    const size_t n_hist_c = (size_t) nq * (nb + 1), n_hist_f = (size_t) nq * (S + 1);
+    const size_t n_hist_c = (size_t) nq * (nb + 2), n_hist_f = (size_t) nq * (S + 1);
     RKR_TRY(ix->ws_hist.ensure(carve_size(n_hist_c, 4) + carve_size(n_hist_f, 4)));
     const int fix_cap = (int) std::min<int64_t>(int64_t(1) << 26, std::max<int64_t>(int64_t(1) << 20, U * nq / 64));
     const int hit_cap = 1 << 24;  // fine-pass hits listed per batch (config 4: about 6.6 M per 1,000 queries)
@@ -1536,15 +1612,22 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
             qs_params_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, U);
             RKR_CUDA(cudaGetLastError());
         }
-        timed(ix, st, "qsrp_round2", [&] {
-            qsrp_round2_kernel<<<hg, kHistThreads, (nb + 1) * kHistThreads * sizeof(int), st>>>(lvc, code, U, par, nb,
-                                                                                              chunk, hist_c);
-        });
-        RKR_CUDA(cudaGetLastError());
-        timed(ix, st, "qsrp_select2c", [&] {
-            qsrp_select2c_kernel<<<(nq + 127) / 128, 128, 0, st>>>(hist_c, nb, ks, nq, par, counts);
-        });
-        RKR_CUDA(cudaGetLastError());
+        // round 2's group histogram: the low groups first (pass 0), the full histogram only for the
+        // queries whose selection reaches the lumped groups (pass 1)
+        const int cap = kRound2Cap <= nb - 1 ? kRound2Cap : nb + 1;  // nb + 1: every group exact in pass 0
+        const int32_t *srank_d = ix->sample_rank.as<int32_t>();
+        for (int pass = 0; pass < 2; pass++) {
+            const size_t smem_r2 = (size_t) (pass == 0 ? cap : nb + 1) * kHistThreads * sizeof(int);
+            timed(ix, st, "qsrp_round2", [&] {
+                qsrp_round2_kernel<<<hg, kHistThreads, smem_r2, st>>>(lvc, code, U, par, nb, cap, pass, chunk, hist_c);
+            });
+            RKR_CUDA(cudaGetLastError());
+            timed(ix, st, "qsrp_select2c", [&] {
+                qsrp_select2c_kernel<<<(nq + 127) / 128, 128, 0, st>>>(hist_c, nb, cap, pass, srank_d, gs, ks, nq, par,
+                                                                       counts);
+            });
+            RKR_CUDA(cudaGetLastError());
+        }
         hl.count = hit_count;
         timed(ix, st, "qsrp_fine2", [&] {
             qsrp_fine2_kernel<<<fg2, 256, 0, st>>>(code, qv, U, nq, inv_user, thr, S, gs, par, 0, any2, hl, hist_f);

@@ -130,6 +130,34 @@ void worker_loop(rkr_server *s, int w) {
               cudaMallocHost(&h_stats, sizeof(rkr_query_stats) * (size_t) bucket_max) == cudaSuccess &&
               cudaMalloc(&d_stats, sizeof(rkr_query_stats) * (size_t) bucket_max) == cudaSuccess;
     std::vector<int32_t> k(bucket_max), first(bucket_max);
+    out_cap = (int64_t) bucket_max * 512;
+    ok = ok && cudaMallocHost(&h_out, sizeof(rkr_user_rank) * (size_t) out_cap) == cudaSuccess &&
+         cudaMalloc(&d_out, sizeof(rkr_user_rank) * (size_t) out_cap) == cudaSuccess;
+    if (!ok) out_cap = 0;
+    // warm-up, before the first request: every padded batch size the worker can form, from the largest
+    // down, runs twice (the first run of the largest sizes the worker's work arrays, and a size's
+    // first run is eager, its second captures the size's phase-1 graph), so that no request waits for
+    // an allocation (which synchronises the device) or a capture
+    if (ok) {
+        for (int q = 0; q < bucket_max; q++)
+            for (int j = 0; j < dim; j++) h_query[(size_t) q * dim + j] = (float) ((q + j) % 7) - 3.0f;
+        bool warm = cudaMemcpyAsync(d_query, h_query, sizeof(float) * (size_t) bucket_max * dim,
+                                    cudaMemcpyHostToDevice, sh->stream) == cudaSuccess;
+        for (int bi = kLastBucket; warm && bi >= 0; bi--) {
+            const int b = kBuckets[bi];
+            if (b > bucket_max) continue;
+            for (int q = 0; q < b; q++) {
+                k[q] = 1;
+                first[q] = q;
+            }
+            BatchSpec bs;
+            bs.k = k.data();
+            bs.req_first = first.data();
+            for (int rep = 0; warm && rep < 2; rep++)
+                warm = query_batch(sh, s->method, d_query, b, bs, d_out, d_stats, sh->stream) == RKR_OK;
+        }
+        cudaStreamSynchronize(sh->stream);  // a warm-up failure leaves the batches to size things themselves
+    }
     for (;;) {
         std::vector<std::shared_ptr<Request>> batch;
         int nq = 0;

@@ -330,6 +330,62 @@ int rkr_file_read_query_distribution(const char *dir, int32_t n_sample_item, int
 int rkr_index_load_files(rkr_index *index, int32_t method, const char *index_dir, const char *dataset_name,
                          int32_t n_sample, int32_t n_sample_query, int32_t sample_topk);
 
+/* ---- user shards ---------------------------------------------------------------------------------- */
+/*
+ * An index too large for one GPU is split by users: shard s is an ordinary rkr_index over the
+ * contiguous users [user_offset_s, user_offset_s + n_user_s) of n_user_total (ascending offsets by
+ * shard number), with the same items, sample ranks and SVD transform, and with its users' rows of the
+ * thresholds, regression records and SVD-space users.  The reference's one global step,
+ * PruneCandidateByBound (src/include/alg/RankBoundRefinement/PruneCandidateByBound.hpp:19-179), needs
+ * the k-th smallest rank bound over all users; every selection of the engine reads that k-th value
+ * off a small per-query count array (levels, groups, buckets), so the shards sum those arrays
+ * element-wise and select alike, then classify, refine and assemble their own users.  The host
+ * merges the shards' partial rows (rkr_shard_merge).  There is no counterpart in the reference,
+ * which holds every user in one process.
+ */
+
+/* Element-wise sum over all shards of n int32 counts, in place.  counts is device memory of the
+ * calling shard's GPU (host memory when stream is NULL and the caller is host code), ordered after
+ * the work already queued on stream (a cudaStream_t); the counts must be summed before any later
+ * work on that stream reads them (stream-ordered, or by waiting).  Returns 0, or non-zero to fail
+ * the query.  Every shard makes the same calls in the same order with the same n. */
+typedef int (*rkr_exchange_fn)(void *ctx, int32_t *counts, int64_t n, void *stream);
+
+/* Makes index shard `shard` of n_shards (users [user_offset, user_offset + its n_user) of
+ * n_user_total), summing counts through exchange(ctx, ...).  n_shards == 1 with exchange NULL
+ * makes the index whole again.  A shard answers rkr_shard_query only (rkr_retrieval / rkr_query /
+ * serving are RKR_ERR_STATE on it); rkr_index_query_rank_distribution returns the sum over all
+ * shards (every shard must call it). */
+int rkr_index_set_shard(rkr_index *index, int32_t shard, int32_t n_shards, int64_t user_offset,
+                        int64_t n_user_total, rkr_exchange_fn exchange, void *ctx);
+
+/* This shard's part of rkr_query: every shard calls it with the same queries and k_per_q (host
+ * arrays).  part (host, sum(k_per_q) entries laid out as rkr_query's out) receives, per query,
+ * n_front[q] of this shard's result users in user-id order, then this shard's refined candidates
+ * sorted by (rank, user id), at most k entries in all; unused entries have user_id -1.  User ids
+ * are global (user_offset added).  stats (host, or NULL) receives the global n_prune and n_result
+ * and this shard's share of the other counters (shard 0 also counts the refinement-independent
+ * part of ip_cost). */
+int rkr_shard_query(rkr_index *index, int32_t method, const float *query, int32_t n_query, const int32_t *k_per_q,
+                    rkr_user_rank *part, int32_t *n_front, rkr_query_stats *stats, int32_t *n_answered);
+
+/* Merges the shards' parts (in shard order) into rkr_query's output: the result users of all
+ * shards in user-id order, then the candidates of all shards by (rank, user id), k per query, as
+ * the reference assembles them (src/impl/QSRPNormalLP.hpp:213-226, src/impl/QS.hpp:185-198).
+ * parts[s], n_fronts[s] and stats[s] (stats may be NULL) are shard s's outputs; stats_out may be
+ * NULL.  Host only. */
+int rkr_shard_merge(int32_t n_shards, int32_t n_query, const int32_t *k_per_q, const rkr_user_rank *const *parts,
+                    const int32_t *const *n_fronts, const rkr_query_stats *const *stats, rkr_user_rank *out,
+                    rkr_query_stats *stats_out);
+
+/* An exchange for shards driven by threads of one process (for example several shards on one
+ * GPU, or one per GPU from one process): rkr_host_exchange is an rkr_exchange_fn whose ctx is a
+ * group from rkr_host_exchange_create.  Each call waits for the stream, copies the counts to the
+ * host, waits up to timeout_s for every member's call (or fails), sums and copies back. */
+int rkr_host_exchange_create(int32_t n_members, double timeout_s, void **group);
+int rkr_host_exchange(void *group, int32_t *counts, int64_t n, void *stream);
+int rkr_host_exchange_destroy(void *group);
+
 #ifdef __cplusplus
 }
 #endif

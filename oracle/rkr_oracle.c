@@ -539,16 +539,63 @@ static int32_t kth_smallest_heap(const int32_t *v, const char *skip, int64_t n, 
     return res;
 }
 
-/* PruneCandidateByBound, src/include/alg/RankBoundRefinement/PruneCandidateByBound.hpp:19-153. */
-void orc_prune_candidate_by_bound(const int32_t *rank_lb, const int32_t *rank_ub, int64_t n_user, int32_t topk,
-                                  int32_t *refine_user_size, int32_t *n_result_user, int32_t *n_prune_user,
-                                  char *prune, char *result) {
+/* ---- user shards ---------------------------------------------------------------------------- */
+
+/* A user shard: this call holds users [user_offset, user_offset + n_user) of all shards' users, and
+ * exchange(ctx, counts, n, NULL) sums n int32 host counts over all shards in place (the engine's
+ * rkr_exchange_fn, include/rkr.h).  first: this shard counts the refinement-independent part of
+ * ip_cost.  NULL everywhere below: one whole index. */
+typedef int (*orc_exchange_fn)(void *ctx, int32_t *counts, int64_t n, void *stream);
+typedef struct {
+    orc_exchange_fn exchange;
+    void *ctx;
+    int64_t user_offset, n_user_total;
+    int first;
+    int failed;
+} orc_shard;
+
+static void shard_sum(orc_shard *sh, int32_t *v, int64_t n) {
+    if (sh && sh->exchange(sh->ctx, v, n, NULL) != 0) sh->failed = 1;
+}
+
+/* The k-th smallest of the eligible values of every shard by the heap rule of kth_smallest_heap,
+ * from the per-value counts summed over the shards (rank bounds lie in [0, n_item]). */
+static int32_t kth_smallest_shard(const int32_t *v, const char *skip, int64_t n, int k, int64_t n_item,
+                                  orc_shard *sh) {
+    int32_t *h = (int32_t *) calloc((size_t) n_item + 1, sizeof(int32_t));
+    for (int64_t i = 0; i < n; i++)
+        if (!skip[i]) {
+            if (v[i] < 0 || v[i] > n_item) sh->failed = 1;
+            else h[v[i]]++;
+        }
+    shard_sum(sh, h, n_item + 1);
+    int64_t total = 0;
+    for (int64_t r = 0; r <= n_item; r++) total += h[r];
+    int32_t res = 0;
+    if (total < k) {
+        for (int64_t r = n_item; r >= 0; r--) if (h[r]) { res = (int32_t) r; break; }
+    } else {
+        int64_t cum = 0;
+        for (int64_t r = 0; r <= n_item; r++) { cum += h[r]; if (cum >= k) { res = (int32_t) r; break; } }
+    }
+    free(h);
+    return res;
+}
+
+/* PruneCandidateByBound, src/include/alg/RankBoundRefinement/PruneCandidateByBound.hpp:19-153.
+ * Sharded (sh != NULL): the k-th smallest bounds and the class counts are every shard's (summed
+ * counts), the classes are set on this shard's users. */
+static void prune_sh(const int32_t *rank_lb, const int32_t *rank_ub, int64_t n_user, int32_t topk, int64_t n_item,
+                     int32_t *refine_user_size, int32_t *n_result_user, int32_t *n_prune_user, char *prune,
+                     char *result, orc_shard *sh) {
     if (*n_result_user >= topk) return;
     const int heap_size = topk - *n_result_user;
     char *skip = (char *) malloc((size_t) n_user);
     for (int64_t u = 0; u < n_user; u++) skip[u] = prune[u] || result[u];
-    const int32_t L = kth_smallest_heap(rank_lb, skip, n_user, heap_size);
-    const int32_t U = kth_smallest_heap(rank_ub, skip, n_user, heap_size);
+    const int32_t L = sh ? kth_smallest_shard(rank_lb, skip, n_user, heap_size, n_item, sh)
+                         : kth_smallest_heap(rank_lb, skip, n_user, heap_size);
+    const int32_t U = sh ? kth_smallest_shard(rank_ub, skip, n_user, heap_size, n_item, sh)
+                         : kth_smallest_heap(rank_ub, skip, n_user, heap_size);
     free(skip);
     if (L == U) {
         *n_result_user = topk;
@@ -557,19 +604,32 @@ void orc_prune_candidate_by_bound(const int32_t *rank_lb, const int32_t *rank_ub
             if (rank_ub[u] <= L && rank_lb[u] <= L) result[u] = 1;
         return;
     }
-    int32_t refine = 0, nres = *n_result_user, npr = *n_prune_user;
+    int32_t refine = 0, nres = 0, npr = 0;
     for (int64_t u = 0; u < n_user; u++) {
         if (prune[u] || result[u]) continue;
         if (rank_lb[u] <= U) { result[u] = 1; nres++; }
         else if (L <= rank_ub[u]) { prune[u] = 1; npr++; }
         else refine++;
     }
+    if (sh) {
+        int32_t c[3] = {nres, npr, refine};
+        shard_sum(sh, c, 3);
+        nres = c[0]; npr = c[1]; refine = c[2];
+    }
+    nres += *n_result_user;
+    npr += *n_prune_user;
     *n_result_user = nres; *n_prune_user = npr; *refine_user_size = refine;
     if (nres + refine == topk) {
         for (int64_t u = 0; u < n_user; u++) if (!prune[u] && !result[u]) result[u] = 1;
         *refine_user_size = 0;
         *n_result_user = topk;
     }
+}
+
+void orc_prune_candidate_by_bound(const int32_t *rank_lb, const int32_t *rank_ub, int64_t n_user, int32_t topk,
+                                  int32_t *refine_user_size, int32_t *n_result_user, int32_t *n_prune_user,
+                                  char *prune, char *result) {
+    prune_sh(rank_lb, rank_ub, n_user, topk, 0, refine_user_size, n_result_user, n_prune_user, prune, result, NULL);
 }
 
 /* ---- refinement ----------------------------------------------------------------------------- */
@@ -673,7 +733,7 @@ typedef struct { int32_t n_prune, n_result, n_refine, n_candidate; int64_t n_com
 static void refine_and_assemble(const refine_t *rf, int use_ipbound, const float *item, const float *qip,
                                 const int32_t *lb, const int32_t *ub, const char *prune, const char *result,
                                 int64_t n_user, int32_t topk, int32_t n_result, orc_user_rank *cache,
-                                orc_user_rank *out, orc_query_stats *st) {
+                                orc_user_rank *out, orc_query_stats *st, const orc_shard *sh, int32_t *n_front) {
     const int32_t n_remain = topk - n_result > 0 ? topk - n_result : 0;
     int32_t n_refine = 0, n_cand = 0;
     int64_t n_compute = 0, refine_ip_cost = 0;
@@ -705,18 +765,33 @@ static void refine_and_assemble(const refine_t *rf, int use_ipbound, const float
         if (result[u]) { out[nc].user_id = (int32_t) u; out[nc].rank = lb[u]; out[nc].query_ip = qip[u]; nc++; }
         if (nc == topk) break;
     }
-    for (int c = nc; c < topk; c++) out[c] = cache[c - nc];
+    if (!sh) {
+        for (int c = nc; c < topk; c++) out[c] = cache[c - nc];
+    } else {
+        /* a shard's part: its results, then its candidates in order, then unused entries */
+        const int64_t off = sh->user_offset;
+        *n_front = nc;
+        for (int c = 0; c < nc; c++) out[c].user_id += (int32_t) off;
+        for (int c = nc; c < topk; c++) {
+            if (n_remain != 0 && c - nc < n_cand) {
+                out[c] = cache[c - nc];
+                out[c].user_id += (int32_t) off;
+            } else {
+                out[c].user_id = -1; out[c].rank = -1; out[c].query_ip = -1.0f;
+            }
+        }
+    }
     if (st) { st->n_refine = n_refine; st->n_candidate = n_cand; st->n_compute_item = n_compute; st->ip_cost = refine_ip_cost; }
 }
 
 /* QS::Index::Retrieval, src/impl/QS.hpp:106-230.
  * user: normalised users [n_user][d]; item: data items [n_item][d]; thr: [n_user][S].
  * out: [n_query][topk]; st: [n_query] or NULL.  Returns 0, or -1 on the reference's error exits. */
-int orc_qs_retrieval(const float *user, int64_t n_user, const float *item, int64_t n_item, int32_t d,
-                     int32_t check_dim, const int32_t *sample_rank, int32_t S, const float *thr,
-                     const float *query, int32_t n_query, int32_t topk, orc_user_rank *out,
-                     orc_query_stats *st) {
-    if (topk > n_user) return -1;
+static int qs_impl(const float *user, int64_t n_user, const float *item, int64_t n_item, int32_t d,
+                   int32_t check_dim, const int32_t *sample_rank, int32_t S, const float *thr,
+                   const float *query, int32_t n_query, int32_t topk, orc_user_rank *out,
+                   orc_query_stats *st, orc_shard *sh, int32_t *n_front) {
+    if (!sh && topk > n_user) return -1;
     refine_t rf; refine_init(&rf, user, n_user, item, n_item, d, check_dim);
     float *qip = (float *) calloc((size_t) n_user, sizeof(float));
     int32_t *lb = (int32_t *) calloc((size_t) n_user, sizeof(int32_t));
@@ -731,12 +806,13 @@ int orc_qs_retrieval(const float *user, int64_t n_user, const float *item, int64
         for (int64_t u = 0; u < n_user; u++)
             orc_sample_search_bound(thr + u * S, S, sample_rank, n_item, qip[u], lb + u, ub + u);
         int32_t refine_size = (int32_t) n_user, n_result = 0, n_prune = 0;
-        orc_prune_candidate_by_bound(lb, ub, n_user, topk, &refine_size, &n_result, &n_prune, prune, result);
+        prune_sh(lb, ub, n_user, topk, n_item, &refine_size, &n_result, &n_prune, prune, result, sh);
         orc_query_stats s = {0};
         refine_and_assemble(&rf, 1, item, qip, lb, ub, prune, result, n_user, topk, n_result, cache,
-                            out + (int64_t) q * topk, &s);
+                            out + (int64_t) q * topk, &s, sh, sh ? n_front + q : NULL);
         s.n_prune = n_prune; s.n_result = n_result;
-        s.ip_cost += n_user;  /* QS.hpp:146, 221 */
+        if (!sh) s.ip_cost += n_user;  /* QS.hpp:146, 221 */
+        else if (sh->first) s.ip_cost += sh->n_user_total;
         if (st) st[q] = s;
     }
     free(qip); free(lb); free(ub); free(prune); free(result); free(cache);
@@ -746,11 +822,11 @@ int orc_qs_retrieval(const float *user, int64_t n_user, const float *item, int64
 
 /* US::Index::Retrieval, src/impl/US.hpp:96-213 (the reference answers only the first 100 queries
  * when n_sample <= 1000, US.hpp:113).  Returns the number of queries answered, or -1. */
-int orc_us_retrieval(const float *user, int64_t n_user, const float *item, int64_t n_item, int32_t d,
-                     const int32_t *sample_rank, int32_t S, const float *thr,
-                     const float *query, int32_t n_query, int32_t topk, orc_user_rank *out,
-                     orc_query_stats *st) {
-    if (topk > n_user) return -1;
+static int us_impl(const float *user, int64_t n_user, const float *item, int64_t n_item, int32_t d,
+                   const int32_t *sample_rank, int32_t S, const float *thr,
+                   const float *query, int32_t n_query, int32_t topk, orc_user_rank *out,
+                   orc_query_stats *st, orc_shard *sh, int32_t *n_front) {
+    if (!sh && topk > n_user) return -1;
     const int32_t nq = S <= 1000 ? 100 : n_query;
     if (nq > n_query) return -1;
     refine_t rf; memset(&rf, 0, sizeof(rf));
@@ -767,12 +843,13 @@ int orc_us_retrieval(const float *user, int64_t n_user, const float *item, int64
         for (int64_t u = 0; u < n_user; u++)
             orc_sample_search_bound(thr + u * S, S, sample_rank, n_item, qip[u], lb + u, ub + u);
         int32_t refine_size = (int32_t) n_user, n_result = 0, n_prune = 0;
-        orc_prune_candidate_by_bound(lb, ub, n_user, topk, &refine_size, &n_result, &n_prune, prune, result);
+        prune_sh(lb, ub, n_user, topk, n_item, &refine_size, &n_result, &n_prune, prune, result, sh);
         orc_query_stats s = {0};
         refine_and_assemble(&rf, 0, item, qip, lb, ub, prune, result, n_user, topk, n_result, cache,
-                            out + (int64_t) q * topk, &s);
+                            out + (int64_t) q * topk, &s, sh, sh ? n_front + q : NULL);
         s.n_prune = n_prune; s.n_result = n_result;
-        s.ip_cost += n_user;  /* US.hpp:134, 188 */
+        if (!sh) s.ip_cost += n_user;  /* US.hpp:134, 188 */
+        else if (sh->first) s.ip_cost += sh->n_user_total;
         if (st) st[q] = s;
     }
     free(qip); free(lb); free(ub); free(prune); free(result); free(cache);
@@ -785,13 +862,13 @@ int orc_us_retrieval(const float *user, int64_t n_user, const float *item, int64
  * sample ranks [S_reg].  qip_state: the index's persistent per-user query score vector
  * ([n_user], zero on a fresh index); users accepted by the first (regression) bound are reported
  * with whatever value it holds, as in the reference. */
-int orc_qsrp_retrieval(const float *user, const float *svd_user, const float *transfer_item, int64_t n_user,
-                       const float *item, int64_t n_item, int32_t d, int32_t check_dim,
-                       const int32_t *sample_rank, int32_t S, const float *thr,
-                       const int32_t *reg_rank, int32_t S_reg, const float *reg,
-                       const float *query, int32_t n_query, int32_t topk,
-                       float *qip_state, orc_user_rank *out, orc_query_stats *st) {
-    if (topk > n_user) return -1;
+static int qsrp_impl(const float *user, const float *svd_user, const float *transfer_item, int64_t n_user,
+                     const float *item, int64_t n_item, int32_t d, int32_t check_dim,
+                     const int32_t *sample_rank, int32_t S, const float *thr,
+                     const int32_t *reg_rank, int32_t S_reg, const float *reg,
+                     const float *query, int32_t n_query, int32_t topk,
+                     float *qip_state, orc_user_rank *out, orc_query_stats *st, orc_shard *sh, int32_t *n_front) {
+    if (!sh && topk > n_user) return -1;
     const int c = check_dim, rd = d - check_dim;
     refine_t rf; refine_init(&rf, user, n_user, item, n_item, d, check_dim);
     float *unorm = (float *) malloc(sizeof(float) * (size_t) n_user);      /* PartDimPartNorm::Preprocess :41-50 */
@@ -817,7 +894,7 @@ int orc_qsrp_retrieval(const float *user, const float *svd_user, const float *tr
                                       reg_rank, S_reg, n_item, lb + u, ub + u);
         }
         int32_t refine_size = (int32_t) n_user, n_result = 0, n_prune = 0;
-        orc_prune_candidate_by_bound(lb, ub, n_user, topk, &refine_size, &n_result, &n_prune, prune, result);
+        prune_sh(lb, ub, n_user, topk, n_item, &refine_size, &n_result, &n_prune, prune, result, sh);
         const int32_t ip_cost = refine_size;                                                 /* QSRPNormalLP.hpp:177 */
         for (int64_t u = 0; u < n_user; u++) {                                               /* ComputeRemainDim :76-95 */
             if (prune[u] || result[u]) continue;
@@ -827,17 +904,84 @@ int orc_qsrp_retrieval(const float *user, const float *svd_user, const float *tr
             if (prune[u] || result[u]) continue;
             orc_sample_search_bound(thr + u * S, S, sample_rank, n_item, qip_state[u], lb + u, ub + u);
         }
-        orc_prune_candidate_by_bound(lb, ub, n_user, topk, &refine_size, &n_result, &n_prune, prune, result);
+        prune_sh(lb, ub, n_user, topk, n_item, &refine_size, &n_result, &n_prune, prune, result, sh);
         orc_query_stats s = {0};
         refine_and_assemble(&rf, 1, item, qip_state, lb, ub, prune, result, n_user, topk, n_result, cache,
-                            out + (int64_t) q * topk, &s);
+                            out + (int64_t) q * topk, &s, sh, sh ? n_front + q : NULL);
         s.n_prune = n_prune; s.n_result = n_result;
-        s.ip_cost += ip_cost;
+        if (!sh || sh->first) s.ip_cost += ip_cost;
         if (st) st[q] = s;
     }
     free(unorm); free(left); free(qtr); free(lb); free(ub); free(prune); free(result); free(cache);
     refine_free(&rf);
     return 0;
+}
+
+int orc_qs_retrieval(const float *user, int64_t n_user, const float *item, int64_t n_item, int32_t d,
+                     int32_t check_dim, const int32_t *sample_rank, int32_t S, const float *thr,
+                     const float *query, int32_t n_query, int32_t topk, orc_user_rank *out,
+                     orc_query_stats *st) {
+    return qs_impl(user, n_user, item, n_item, d, check_dim, sample_rank, S, thr, query, n_query, topk, out, st,
+                   NULL, NULL);
+}
+
+int orc_us_retrieval(const float *user, int64_t n_user, const float *item, int64_t n_item, int32_t d,
+                     const int32_t *sample_rank, int32_t S, const float *thr,
+                     const float *query, int32_t n_query, int32_t topk, orc_user_rank *out,
+                     orc_query_stats *st) {
+    return us_impl(user, n_user, item, n_item, d, sample_rank, S, thr, query, n_query, topk, out, st, NULL, NULL);
+}
+
+int orc_qsrp_retrieval(const float *user, const float *svd_user, const float *transfer_item, int64_t n_user,
+                       const float *item, int64_t n_item, int32_t d, int32_t check_dim,
+                       const int32_t *sample_rank, int32_t S, const float *thr,
+                       const int32_t *reg_rank, int32_t S_reg, const float *reg,
+                       const float *query, int32_t n_query, int32_t topk,
+                       float *qip_state, orc_user_rank *out, orc_query_stats *st) {
+    return qsrp_impl(user, svd_user, transfer_item, n_user, item, n_item, d, check_dim, sample_rank, S, thr, reg_rank,
+                     S_reg, reg, query, n_query, topk, qip_state, out, st, NULL, NULL);
+}
+
+/* The same three methods on one user shard holding users [user_offset, user_offset + n_user) of
+ * n_user_total (first: shard 0): every argument is the shard's (its users' rows of user / svd_user / thr /
+ * reg / qip_state), exchange sums counts over the shards (every shard calls with the same queries and
+ * topk).  out[q] is the shard's part of row q as rkr_shard_query returns it (n_front[q] results by
+ * user id, then its candidates by (rank, user id), unused entries user_id -1); stats carry the global
+ * n_prune / n_result and the shard's share of the rest.  Returns the queries answered, or -1 when
+ * the exchange failed or a bound lay outside [0, n_item]. */
+int orc_qs_retrieval_shard(const float *user, int64_t n_user, const float *item, int64_t n_item, int32_t d,
+                           int32_t check_dim, const int32_t *sample_rank, int32_t S, const float *thr,
+                           const float *query, int32_t n_query, int32_t topk, int64_t user_offset,
+                           int64_t n_user_total, int32_t first, orc_exchange_fn exchange, void *ctx,
+                           orc_user_rank *out, int32_t *n_front, orc_query_stats *st) {
+    orc_shard sh = {exchange, ctx, user_offset, n_user_total, first, 0};
+    const int rc = qs_impl(user, n_user, item, n_item, d, check_dim, sample_rank, S, thr, query, n_query, topk, out,
+                           st, &sh, n_front);
+    return sh.failed ? -1 : (rc < 0 ? rc : n_query);
+}
+
+int orc_us_retrieval_shard(const float *user, int64_t n_user, const float *item, int64_t n_item, int32_t d,
+                           const int32_t *sample_rank, int32_t S, const float *thr,
+                           const float *query, int32_t n_query, int32_t topk, int64_t user_offset,
+                           int64_t n_user_total, int32_t first, orc_exchange_fn exchange, void *ctx,
+                           orc_user_rank *out, int32_t *n_front, orc_query_stats *st) {
+    orc_shard sh = {exchange, ctx, user_offset, n_user_total, first, 0};
+    const int rc = us_impl(user, n_user, item, n_item, d, sample_rank, S, thr, query, n_query, topk, out, st, &sh,
+                           n_front);
+    return sh.failed ? -1 : rc;
+}
+
+int orc_qsrp_retrieval_shard(const float *user, const float *svd_user, const float *transfer_item, int64_t n_user,
+                             const float *item, int64_t n_item, int32_t d, int32_t check_dim,
+                             const int32_t *sample_rank, int32_t S, const float *thr,
+                             const int32_t *reg_rank, int32_t S_reg, const float *reg,
+                             const float *query, int32_t n_query, int32_t topk, int64_t user_offset,
+                             int64_t n_user_total, int32_t first, orc_exchange_fn exchange, void *ctx,
+                             float *qip_state, orc_user_rank *out, int32_t *n_front, orc_query_stats *st) {
+    orc_shard sh = {exchange, ctx, user_offset, n_user_total, first, 0};
+    const int rc = qsrp_impl(user, svd_user, transfer_item, n_user, item, n_item, d, check_dim, sample_rank, S, thr,
+                             reg_rank, S_reg, reg, query, n_query, topk, qip_state, out, st, &sh, n_front);
+    return sh.failed ? -1 : (rc < 0 ? rc : n_query);
 }
 
 /* ------------------------------------------------------------------------------------------ */

@@ -349,13 +349,20 @@ int rkr_index_size_bytes(const rkr_index *ix, uint64_t *bytes) {
     return RKR_OK;
 }
 
-static int check_query_args(rkr_index *ix, int32_t method, int32_t n_query, int32_t topk, int32_t *n_answered) {
+static int check_query_args(rkr_index *ix, int32_t method, int32_t n_query, int32_t topk, int32_t *n_answered,
+                            bool shard_call = false) {
     RKR_REQUIRE(ix, "null index");
+    if (ix->sharded() != shard_call) {
+        set_error(ix->sharded() ? "the index is a user shard: query it with rkr_shard_query"
+                                : "rkr_shard_query: the index is not a user shard (rkr_index_set_shard)");
+        return RKR_ERR_STATE;
+    }
     RKR_REQUIRE(method == RKR_METHOD_QS || method == RKR_METHOD_QSRP_NORMAL_LP || method == RKR_METHOD_US,
                 "unknown method %d", method);
     RKR_REQUIRE(n_query >= 0, "negative n_query");
     // QS.hpp:116-119: "top-k is too large"; topk < 1 leaves the reference's heaps empty.
-    RKR_REQUIRE(topk >= 1 && topk <= ix->n_user, "topk %d outside [1, n_user=%lld]", topk, (long long) ix->n_user);
+    RKR_REQUIRE(topk >= 1 && topk <= ix->n_user_all(), "topk %d outside [1, n_user=%lld]", topk,
+                (long long) ix->n_user_all());
     RKR_REQUIRE(topk <= 4096, "topk %d above the supported maximum of 4096", topk);
     if (ix->n_sample <= 0) {
         set_error("method needs the sampled-threshold index (load or build it first)");
@@ -424,7 +431,8 @@ static int check_k_per_q(rkr_index *ix, const int32_t *k_per_q, int32_t n, int64
     int64_t s = 0;
     for (int32_t q = 0; q < n; q++) {
         const int32_t k = k_per_q[q];
-        RKR_REQUIRE(k >= 1 && k <= ix->n_user, "k_per_q[%d] = %d outside [1, n_user=%lld]", q, k, (long long) ix->n_user);
+        RKR_REQUIRE(k >= 1 && k <= ix->n_user_all(), "k_per_q[%d] = %d outside [1, n_user=%lld]", q, k,
+                    (long long) ix->n_user_all());
         RKR_REQUIRE(k <= 4096, "k_per_q[%d] = %d above the supported maximum of 4096", q, k);
         s += k;
     }
@@ -470,6 +478,58 @@ int rkr_query(rkr_index *ix, int32_t method, const float *query, int32_t n_query
     RKR_TRY(query_batch(ix, method, ix->ws_query.as<float>(), nq, bs, ix->ws_out.as<rkr_user_rank>(),
                         stats ? ix->ws_stats.as<rkr_query_stats>() : nullptr, ix->stream));
     RKR_CUDA(cudaMemcpyAsync(out, ix->ws_out.p, ob, cudaMemcpyDeviceToHost, ix->stream));
+    if (stats) RKR_CUDA(cudaMemcpyAsync(stats, ix->ws_stats.p, sb, cudaMemcpyDeviceToHost, ix->stream));
+    RKR_CUDA(cudaStreamSynchronize(ix->stream));
+    return RKR_OK;
+}
+
+int rkr_index_set_shard(rkr_index *ix, int32_t shard, int32_t n_shards, int64_t user_offset, int64_t n_user_total,
+                        rkr_exchange_fn exchange, void *ctx) {
+    RKR_REQUIRE(ix, "null index");
+    RKR_REQUIRE(n_shards >= 1 && shard >= 0 && shard < n_shards, "shard %d of %d", shard, n_shards);
+    if (n_shards == 1 && !exchange) {  // whole again
+        RKR_REQUIRE(user_offset == 0 && (n_user_total == 0 || n_user_total == ix->n_user),
+                    "a whole index starts at user 0 and holds n_user_total users");
+        ix->shard = rkr_index::Shard();
+        return RKR_OK;
+    }
+    RKR_REQUIRE(exchange, "a user shard needs an exchange function");
+    RKR_REQUIRE(user_offset >= 0 && user_offset + ix->n_user <= n_user_total,
+                "users [%lld, %lld) outside [0, n_user_total=%lld)", (long long) user_offset,
+                (long long) (user_offset + ix->n_user), (long long) n_user_total);
+    RKR_REQUIRE(n_user_total <= INT32_MAX, "n_user_total %lld above the 32-bit user ids", (long long) n_user_total);
+    ix->shard.index = shard;
+    ix->shard.count = n_shards;
+    ix->shard.user_offset = user_offset;
+    ix->shard.n_user_total = n_user_total;
+    ix->shard.fn = exchange;
+    ix->shard.ctx = ctx;
+    return RKR_OK;
+}
+
+int rkr_shard_query(rkr_index *ix, int32_t method, const float *query, int32_t n_query, const int32_t *k_per_q,
+                    rkr_user_rank *part, int32_t *n_front, rkr_query_stats *stats, int32_t *n_answered) {
+    int32_t nq = 0;
+    RKR_TRY(check_query_args(ix, method, n_query, 1, &nq, true));
+    if (n_answered) *n_answered = nq;
+    if (nq == 0) return RKR_OK;
+    int64_t n_out = 0;
+    RKR_TRY(check_k_per_q(ix, k_per_q, nq, &n_out));
+    RKR_REQUIRE(query && part && n_front, "null query/part/n_front pointer");
+    RKR_TRY(ensure_device(ix));
+    const size_t qb = sizeof(float) * (size_t) nq * ix->dim;
+    const size_t ob = sizeof(rkr_user_rank) * (size_t) n_out;
+    const size_t sb = sizeof(rkr_query_stats) * (size_t) nq;
+    RKR_TRY(ix->ws_query.ensure(qb));
+    RKR_TRY(ix->ws_out.ensure(ob));
+    RKR_TRY(ix->ws_stats.ensure(sb));
+    RKR_CUDA(cudaMemcpyAsync(ix->ws_query.p, query, qb, cudaMemcpyHostToDevice, ix->stream));
+    BatchSpec bs;
+    bs.k = k_per_q;
+    bs.front = n_front;
+    RKR_TRY(query_batch(ix, method, ix->ws_query.as<float>(), nq, bs, ix->ws_out.as<rkr_user_rank>(),
+                        stats ? ix->ws_stats.as<rkr_query_stats>() : nullptr, ix->stream));
+    RKR_CUDA(cudaMemcpyAsync(part, ix->ws_out.p, ob, cudaMemcpyDeviceToHost, ix->stream));
     if (stats) RKR_CUDA(cudaMemcpyAsync(stats, ix->ws_stats.p, sb, cudaMemcpyDeviceToHost, ix->stream));
     RKR_CUDA(cudaStreamSynchronize(ix->stream));
     return RKR_OK;

@@ -647,6 +647,8 @@ int query_rank_distribution(rkr_index *ix, const int32_t *sample_item, int n_sam
         sa.rank_hist = ix->ws_hist.as<int32_t>();
         RKR_TRY(run_rows(P, u0, nu, sa));
     }
+    // user shards: every shard's counts
+    RKR_TRY(shard_sum(ix, ix->ws_hist.as<int32_t>(), (int64_t) n_sample_item * (n + 1), ix->stream));
     timed(ix, ix->stream, "prefix_rows", [&] { prefix_rows_kernel<<<(n_sample_item + 63) / 64, 64, 0, ix->stream>>>(ix->ws_hist.as<int32_t>(), n_sample_item, n + 1); });
     RKR_CUDA(cudaGetLastError());
     RKR_CUDA(cudaMemcpyAsync(h_accu, ix->ws_hist.p, sizeof(int32_t) * (size_t) n_sample_item * (n + 1),

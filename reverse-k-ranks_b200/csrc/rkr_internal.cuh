@@ -1092,13 +1092,26 @@ struct rkr_index {
     rkr::DevBuf ws_res, ws_cand, ws_cand_off, ws_refine, ws_rank, ws_out, ws_stats, ws_misc, ws_fix, ws_km, ws_tc, ws_sc;
     rkr::DevBuf ws_defer;  // rows the streaming row selection left to the scatter form
     rkr::DevBuf ws_emit;   // the sparse compaction's classes and emission data per list entry
+    rkr::DevBuf ws_shard;  // a user shard's counts on their way to the exchange
+    rkr::DevBuf ws_snap[2];  // ... and its copies of summed counts before a second pass adds to them
     // Every per-call workspace buffer: a serving worker's shadow of the index owns its own (the
     // resident data it shares), and destruction releases them.
     std::vector<rkr::DevBuf *> workspaces() {
         return {&ws_query, &ws_qtr, &ws_qnorm, &ws_bucket, &ws_bucket2, &ws_levels, &ws_cls, &ws_counts, &ws_hist,
                 &ws_res, &ws_cand, &ws_cand_off, &ws_refine, &ws_rank, &ws_out, &ws_stats, &ws_misc, &ws_fix,
-                &ws_km, &ws_tc, &ws_sc, &ws_defer, &ws_emit};
+                &ws_km, &ws_tc, &ws_sc, &ws_defer, &ws_emit, &ws_shard, &ws_snap[0], &ws_snap[1]};
     }
+    // User shard (rkr_index_set_shard): this index holds users [user_offset, user_offset + n_user)
+    // of n_user_total, and the per-query counts each selection reads are summed over the shards
+    // through fn (rkr_shard.cu).
+    struct Shard {
+        int32_t index = 0, count = 1;
+        int64_t user_offset = 0, n_user_total = 0;
+        rkr_exchange_fn fn = nullptr;
+        void *ctx = nullptr;
+    } shard;
+    bool sharded() const { return shard.fn != nullptr; }
+    int64_t n_user_all() const { return shard.fn ? shard.n_user_total : n_user; }
     std::vector<uint8_t> h_scratch;
     rkr::Profiler prof;
     // CUDA graphs of a batch's phase 1 (rkr_qsrp.cu), one per (method, batch size, workspace
@@ -1192,6 +1205,37 @@ inline int run_compaction(rkr_index *ix, P p, int nq, KSpec ks, QueryCounts *cou
     return RKR_OK;
 }
 
+// ---- user shards (rkr_shard.cu) ----
+// counts[0..n) summed over the shards in place (no-op on a whole index).
+int shard_sum(rkr_index *ix, int32_t *counts, int64_t n, cudaStream_t st);
+// A buffer whose counts were already summed and to which a second pass then added this shard's
+// counts: copy it before the second pass (shard_snapshot), then shard_sum_delta sums the added
+// counts only.
+int shard_snapshot(rkr_index *ix, int slot, const int32_t *counts, int64_t n, cudaStream_t st);
+int shard_sum_delta(rkr_index *ix, int slot, int32_t *counts, int64_t n, cudaStream_t st);
+// Sum over the shards of a host value (waits for the stream).
+int shard_sum_host(rkr_index *ix, int32_t v, int32_t *sum, cudaStream_t st);
+// counts[q].n_cand from the shard's (code, class) pairs, and ip_base kept on shard 0 only.
+__global__ void shard_local_counts_kernel(const int2 *__restrict__ cnt, int nchunks, int nq, int keep_base,
+                                          QueryCounts *__restrict__ counts);
+
+// A user shard's candidate count per query: the global selection (counts as summed) decides each
+// user's class, the shard counts its own users of the refinement class; the ordered compaction and
+// refinement then run on the shard's candidates.  The results are counted by the compaction itself.
+template <class P>
+inline int shard_local_counts(rkr_index *ix, P p, int nq, QueryCounts *counts, cudaStream_t st) {
+    const int64_t U = ix->n_user;
+    const int nchunks = (int) ((U + kCompactChunk - 1) / kCompactChunk);
+    RKR_TRY(ix->ws_cand_off.ensure(sizeof(int2) * (size_t) nq * nchunks + 256));
+    int2 *cnt = reinterpret_cast<int2 *>(ix->ws_cand_off.p);
+    const dim3 g((unsigned) nchunks, (unsigned) nq);
+    timed(ix, st, "compact_count", [&] { compact_count_kernel<P><<<g, kCompactThreads, 0, st>>>(p, U, nchunks, cnt, nullptr); });
+    RKR_CUDA(cudaGetLastError());
+    shard_local_counts_kernel<<<(nq + 127) / 128, 128, 0, st>>>(cnt, nchunks, nq, ix->shard.index == 0, counts);
+    RKR_CUDA(cudaGetLastError());
+    return RKR_OK;
+}
+
 // Candidate refinement (refine_prep_kernel, then the per-item counting on tiles).
 struct RefineArgs {
     const float *user;        // rows refined against the items (raw users)
@@ -1235,6 +1279,7 @@ struct BatchSpec {
     int topk = 0;
     const int32_t *k = nullptr;
     const int32_t *req_first = nullptr;
+    int32_t *front = nullptr;  // user shard (host, [n_query]): the result users at the front of each row
 };
 int query_batch(rkr_index *ix, int method, const float *d_query, int n_query, const BatchSpec &bs,
                 rkr_user_rank *d_out, rkr_query_stats *d_stats, cudaStream_t st);

@@ -1337,6 +1337,32 @@ __global__ void __launch_bounds__(256, 4) qsrp_state_kernel(const uint8_t *__res
         }
 }
 
+// A user shard's round-1 class counts from the fine pass (mode 1), summed over the shards: the
+// counters that pass adds to are copied out (their values before it are 0, or the summed whole-level
+// counts of qsrp_select1f for n_res1 / n_pr1 when the query is not counted pair by pair), summed,
+// and written back.
+__global__ void qsrp_shard_counts1_kernel(QsrpParams *__restrict__ par, int nq, int32_t *__restrict__ buf, int unpack) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    QsrpParams &p = par[q];
+    int32_t *b = buf + (int64_t) q * 5;
+    if (!unpack) {
+        b[0] = p.res_fine;
+        b[1] = p.ple_fine;
+        b[2] = p.w_all ? p.n_res1 : 0;
+        b[3] = p.w_all ? p.n_pr1 : 0;
+        b[4] = p.w_all ? p.n_ref1 : 0;
+        return;
+    }
+    p.res_fine = b[0];
+    p.ple_fine = b[1];
+    if (p.w_all) {
+        p.n_res1 = b[2];
+        p.n_pr1 = b[3];
+        p.n_ref1 = b[4];
+    }
+}
+
 // ---- host orchestration ----------------------------------------------------------------------------
 
 namespace {
@@ -1350,12 +1376,23 @@ template <typename T> T *carve(uint8_t *&p, size_t n) {
 inline size_t carve_size(size_t n, size_t elem) { return ((n * elem + 255) & ~size_t(255)) + 256; }
 }  // namespace
 
+static int shard_sum_counts1(rkr_index *ix, QsrpParams *par, int nq, cudaStream_t st) {
+    RKR_TRY(ix->ws_shard.ensure(sizeof(int32_t) * 5 * (size_t) nq));
+    int32_t *buf = ix->ws_shard.as<int32_t>();
+    qsrp_shard_counts1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, buf, 0);
+    RKR_CUDA(cudaGetLastError());
+    RKR_TRY(shard_sum(ix, buf, 5 * (int64_t) nq, st));
+    qsrp_shard_counts1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, buf, 1);
+    RKR_CUDA(cudaGetLastError());
+    return RKR_OK;
+}
+
 // Runs a batch's phase 1: eagerly, or, with ix->graphs_on, from a CUDA graph of the same launches.  A
 // shape (method, batch size, workspace addresses) runs eagerly the first time -- that sizes every
 // buffer it touches -- and is captured the second time and replayed from then on.  A capture that
 // fails (an operation not allowed while capturing) turns graphs off for the index and runs eagerly.
 template <class F> static int run_phase1(rkr_index *ix, int method, int nq, cudaStream_t st, F &&phase1) {
-    if (!ix->graphs_on || ix->prof.on) return phase1(false);
+    if (!ix->graphs_on || ix->prof.on || ix->sharded()) return phase1(false);
     const void *ws[8] = {ix->ws_qtr.p, ix->ws_levels.p, ix->ws_cls.p, ix->ws_counts.p,
                          ix->ws_hist.p, ix->ws_fix.p, ix->ws_sc.p, ix->ws_km.p};
     rkr_index::PhaseGraph *hit = nullptr;
@@ -1403,6 +1440,7 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
     int kmax = bs.topk;
     if (bs.k) kmax = *std::max_element(bs.k, bs.k + nq);
     const int64_t U = ix->n_user;
+    const int64_t Ug = ix->n_user_all();  // a user shard selects over every shard's users
     const int dim = ix->dim, c = ix->check_dim, S = ix->n_sample, Sr = ix->n_sample_reg;
     const int n_item = (int) ix->n_item;
     const int gs = thr_group(S), nb = (S + gs - 1) / gs;
@@ -1569,12 +1607,14 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
             const dim3 g((unsigned) ((U + ch - 1) / ch), (unsigned) nq);
             timed(ix, st, "lvc_hist", [&] { lvc_hist_kernel<<<g, kHistThreads, 0, st>>>(lvc, U, ch, lhist); });
             RKR_CUDA(cudaGetLastError());
+            RKR_TRY(shard_sum(ix, lhist, (int64_t) n_lhist, st));
+            RKR_TRY(shard_sum(ix, anomaly, nq, st));
         }
         const int64_t chunk = 65536;  // users per round-2 block (its per-thread counters are set up once)
         dim3 hg((unsigned) ((U + chunk - 1) / chunk), (unsigned) nq);
         if (qsrp) {
             timed(ix, st, "qsrp_select1c", [&] {
-                qsrp_select1c_kernel<<<(nq + 127) / 128, 128, 0, st>>>(lhist, U, ks, nq, Sr, par);
+                qsrp_select1c_kernel<<<(nq + 127) / 128, 128, 0, st>>>(lhist, Ug, ks, nq, Sr, par);
             });
             RKR_CUDA(cudaGetLastError());
             const double inv_u = 1.0 / (double) U;
@@ -1591,8 +1631,9 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
                 qsrp_fine1_list_kernel<<<148 * 16, 256, 0, st>>>(lvc, r1, U, Sr, W, 0, par, f1, fhist, mismatch);
             });
             RKR_CUDA(cudaGetLastError());
+            RKR_TRY(shard_sum(ix, fhist, (int64_t) n_fhist, st));
             timed(ix, st, "qsrp_select1f", [&] {
-                qsrp_select1f_kernel<<<(nq + 3) / 4, 128, 0, st>>>(lhist, fhist, anomaly, U, m.rank, Sr, n_item, W, ks,
+                qsrp_select1f_kernel<<<(nq + 3) / 4, 128, 0, st>>>(lhist, fhist, anomaly, Ug, m.rank, Sr, n_item, W, ks,
                                                                    nq, par);
             });
             RKR_CUDA(cudaGetLastError());
@@ -1606,10 +1647,11 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
                 qsrp_fine1_list_kernel<<<148 * 16, 256, 0, st>>>(lvc, r1, U, Sr, W, 1, par, f1, fhist, mismatch);
             });
             RKR_CUDA(cudaGetLastError());
-            timed(ix, st, "qsrp_final1", [&] { qsrp_final1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, ks, U); });
+            if (ix->sharded()) RKR_TRY(shard_sum_counts1(ix, par, nq, st));
+            timed(ix, st, "qsrp_final1", [&] { qsrp_final1_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, ks, Ug); });
             RKR_CUDA(cudaGetLastError());
         } else {
-            qs_params_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, U);
+            qs_params_kernel<<<(nq + 127) / 128, 128, 0, st>>>(par, nq, Ug);
             RKR_CUDA(cudaGetLastError());
         }
         // round 2's group histogram: the low groups first (pass 0), the full histogram only for the
@@ -1618,10 +1660,13 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
         const int32_t *srank_d = ix->sample_rank.as<int32_t>();
         for (int pass = 0; pass < 2; pass++) {
             const size_t smem_r2 = (size_t) (pass == 0 ? cap : nb + 1) * kHistThreads * sizeof(int);
+            if (pass == 1) RKR_TRY(shard_snapshot(ix, 0, hist_c, (int64_t) n_hist_c, st));
             timed(ix, st, "qsrp_round2", [&] {
                 qsrp_round2_kernel<<<hg, kHistThreads, smem_r2, st>>>(lvc, code, U, par, nb, cap, pass, chunk, hist_c);
             });
             RKR_CUDA(cudaGetLastError());
+            RKR_TRY(pass == 0 ? shard_sum(ix, hist_c, (int64_t) n_hist_c, st)
+                              : shard_sum_delta(ix, 0, hist_c, (int64_t) n_hist_c, st));
             timed(ix, st, "qsrp_select2c", [&] {
                 qsrp_select2c_kernel<<<(nq + 127) / 128, 128, 0, st>>>(hist_c, nb, cap, pass, srank_d, gs, ks, nq, par,
                                                                        counts);
@@ -1635,17 +1680,20 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
         RKR_CUDA(cudaGetLastError());
         timed(ix, st, "qsrp_fine2_list", [&] { qsrp_fine2_list_kernel<<<148 * 16, 256, 0, st>>>(hl, qv, U, thr, S, gs, hist_f); });
         RKR_CUDA(cudaGetLastError());
+        RKR_TRY(shard_sum(ix, hist_f, (int64_t) n_hist_f, st));
         timed(ix, st, "qsrp_select2f", [&] {
             qsrp_select2f_kernel<<<(nq + 3) / 4, 128, 0, st>>>(hist_f, nb, gs, S, srank, n_item, ks, nq, par, cls2, clsg, any2);
         });
         RKR_CUDA(cudaGetLastError());
         hl.count = hit_count + 1;
+        RKR_TRY(shard_snapshot(ix, 1, hist_f, (int64_t) n_hist_f, st));
         timed(ix, st, "qsrp_fine2", [&] {
             qsrp_fine2_kernel<<<fg2, 256, 0, st>>>(code, qv, U, nq, inv_user, thr, S, gs, par, 1, any2, hl, hist_f);
         });
         RKR_CUDA(cudaGetLastError());
         timed(ix, st, "qsrp_fine2_list", [&] { qsrp_fine2_list_kernel<<<148 * 16, 256, 0, st>>>(hl, qv, U, thr, S, gs, hist_f); });
         RKR_CUDA(cudaGetLastError());
+        RKR_TRY(shard_sum_delta(ix, 1, hist_f, (int64_t) n_hist_f, st));
         timed(ix, st, "qsrp_final2", [&] {
             qsrp_final2_kernel<<<(nq + 3) / 4, 128, 0, st>>>(hist_c, hist_f, nb, gs, S, ks, nq, qsrp ? m.rank : nullptr, Sr,
                                                              n_item, par, cls2, clsg, counts);
@@ -1670,7 +1718,10 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
         ix->prof.add_count("lvt_search_lower_pairs", h_sc[2]);
         ix->prof.add_count("lvt_search_upper_pairs", h_sc[3]);
     }
-    if (h_sc[0]) {
+    int redo = h_sc[0] ? 1 : 0;
+    // user shards redo phase 1 together (its counts are summed over them)
+    if (ix->sharded()) RKR_TRY(shard_sum_host(ix, redo, &redo, st));
+    if (redo) {
         // the tensor-core run gave up (a bounded wait or a full list): the exact tiles redo phase 1
         RKR_TRY(phase1(true));
         h_mismatch = 0;
@@ -1684,6 +1735,31 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
         return RKR_ERR_STATE;
     }
     if (ix->prof.on) ix->prof.add_count("screen_undecided_pairs", h_fix);
+    QsrpCompactPolicy pol = {};
+    pol.lvc = lvc;
+    pol.src = r1;
+    pol.code = code;
+    pol.thr = thr;
+    pol.sc = qv;
+    pol.n_user = U;
+    pol.reg_rank = m.rank;
+    pol.rank = srank;
+    pol.S_reg = Sr;
+    pol.S = S;
+    pol.n_item = n_item;
+    pol.nb = nb;
+    pol.gs = gs;
+    pol.par = par;
+    pol.cls2 = cls2;
+    pol.clsg = clsg;
+    pol.counts = counts;
+    pol.kstride = kmax;
+    if (ix->sharded()) {
+        // the candidates of this shard's users (the counts so far are every shard's)
+        RKR_TRY(shard_local_counts(ix, pol, nq, counts, st));
+        RKR_CUDA(cudaMemcpyAsync(hc.data(), counts, sizeof(QueryCounts) * nq, cudaMemcpyDeviceToHost, st));
+        RKR_CUDA(cudaStreamSynchronize(st));
+    }
     std::vector<int64_t> off(nq + 1, 0);
     for (int q = 0; q < nq; q++) off[q + 1] = off[q] + hc[q].n_cand;
     const int64_t n_cand = off[nq];
@@ -1702,26 +1778,7 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
     int32_t *cand_ub = carve<int32_t>(p, n_cand);
     float *cand_qip = carve<float>(p, n_cand);
     RKR_CUDA(cudaMemcpyAsync(d_off, off.data(), sizeof(int64_t) * (nq + 1), cudaMemcpyHostToDevice, st));
-    QsrpCompactPolicy pol;
-    pol.lvc = lvc;
-    pol.src = r1;
-    pol.code = code;
-    pol.thr = thr;
-    pol.sc = qv;
-    pol.n_user = U;
-    pol.reg_rank = m.rank;
-    pol.rank = srank;
-    pol.S_reg = Sr;
-    pol.S = S;
-    pol.n_item = n_item;
-    pol.nb = nb;
-    pol.gs = gs;
-    pol.par = par;
-    pol.cls2 = cls2;
-    pol.clsg = clsg;
-    pol.counts = counts;
     pol.cand_off = d_off;
-    pol.kstride = kmax;
     pol.res_user = res_user;
     pol.res_rank = res_rank;
     pol.res_fresh = res_fresh;
@@ -1750,7 +1807,10 @@ int pair_chunk(rkr_index *ix, int method, const float *d_query, int nq, const Ba
         qsrp_state_kernel<<<(unsigned) ((U + 255) / 256), 256, 0, st>>>(code, qv, U, nq, ix->qip_state.as<float>());
     });
     RKR_CUDA(cudaGetLastError());
+    if (bs.front) RKR_CUDA(cudaMemcpyAsync(hc.data(), counts, sizeof(QueryCounts) * nq, cudaMemcpyDeviceToHost, st));
     RKR_CUDA(cudaStreamSynchronize(st));
+    if (bs.front)
+        for (int q = 0; q < nq; q++) bs.front[q] = hc[q].n_res_emit;
     if (ix->prof.on) {
         int h = 0, hh[2] = {0, 0};
         RKR_CUDA(cudaMemcpy(&h, n_rescored, sizeof(int), cudaMemcpyDeviceToHost));

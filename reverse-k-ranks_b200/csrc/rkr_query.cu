@@ -169,6 +169,7 @@ struct AssembleArgs {
     int ipbound, dim, check_dim;
     rkr_user_rank *out;          // k entries per query
     rkr_query_stats *stats;      // [n_query] or nullptr
+    int64_t id_offset;           // added to the user ids written (a user shard's first user)
     uint64_t *scratch;           // keys for candidates beyond kSortCap (indexed by candidate)
 };
 
@@ -191,7 +192,7 @@ __global__ void assemble_kernel(AssembleArgs a) {
     const int nres = c.n_res_emit;
     for (int k = threadIdx.x; k < nres; k += blockDim.x) {
         const int64_t i = (int64_t) q * a.ks.kmax + k;
-        out[k].user_id = a.res_user[i];
+        out[k].user_id = (int32_t) (a.res_user[i] + a.id_offset);
         out[k].rank = a.res_rank[i];
         out[k].query_ip = a.res_qip[i];
     }
@@ -297,7 +298,7 @@ __global__ void assemble_kernel(AssembleArgs a) {
                 if (keys[mid] < kk) { lo = mid + 1; len -= h + 1; } else len = h;
             }
             if (lo < m && keys[lo] == kk) {
-                out[nres + lo].user_id = a.cand_user[off + e];
+                out[nres + lo].user_id = (int32_t) (a.cand_user[off + e] + a.id_offset);
                 out[nres + lo].rank = a.cand_rank[off + e];
                 out[nres + lo].query_ip = a.cand_qip[off + e];
             }
@@ -428,6 +429,7 @@ static int refine_and_assemble(rkr_index *ix, int method, const float *d_query, 
     aa.out = d_out;
     aa.stats = d_stats;
     aa.scratch = nullptr;
+    aa.id_offset = ix->shard.user_offset;
     timed(ix, st, "assemble", [&] { assemble_kernel<<<nq, 256, 0, st>>>(aa); });
     RKR_CUDA(cudaGetLastError());
     (void) h_counts;
@@ -456,7 +458,8 @@ int query_batch(rkr_index *ix, int method, const float *d_query, int n_query, co
     // Chunk so the per-pair arrays (coarse levels and group codes: 2 bytes a pair) stay within a
     // bounded slice of device memory.
     const int64_t budget = int64_t(8) << 30;
-    const int64_t per_q = ix->n_user * 2 + 4096;
+    // (user shards chunk alike: their counts are summed chunk by chunk)
+    const int64_t per_q = ix->n_user_all() * 2 + 4096;
     int chunk = (int) std::max<int64_t>(1, std::min<int64_t>(n_query, budget / per_q));
     chunk = std::min(chunk, kMaxChunkQueries);
     int64_t out_at = 0;
@@ -465,6 +468,7 @@ int query_batch(rkr_index *ix, int method, const float *d_query, int n_query, co
         BatchSpec part = bs;
         std::vector<int32_t> first;
         if (bs.k) part.k = bs.k + q0;
+        if (bs.front) part.front = bs.front + q0;
         if (bs.req_first) {
             // a request that started in an earlier chunk continues from this chunk's first query
             first.resize(nq);

@@ -274,6 +274,10 @@ extern "C" {
 int rkr_server_create(rkr_index *ix, const rkr_server_config *cfg, rkr_server **out) {
     RKR_REQUIRE(ix && cfg && out, "null argument");
     *out = nullptr;
+    if (ix->sharded()) {
+        set_error("rkr_server_create: the index is a user shard");
+        return RKR_ERR_STATE;
+    }
     RKR_REQUIRE(cfg->method == RKR_METHOD_QS || cfg->method == RKR_METHOD_QSRP_NORMAL_LP,
                 "rkr_server_create: method %d (QS or QSRPNormalLP; US answers fixed sets of 100 queries)", cfg->method);
     RKR_REQUIRE(cfg->max_batch_queries >= 1 && cfg->max_batch_queries <= kMaxChunkQueries,

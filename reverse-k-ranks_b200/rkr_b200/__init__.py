@@ -43,8 +43,12 @@ EXPORTS = [
     "rkr_file_sample_search_info", "rkr_file_read_sample_search", "rkr_file_write_sample_search",
     "rkr_file_regression_info", "rkr_file_read_regression", "rkr_file_write_regression", "rkr_file_svd_info",
     "rkr_file_read_svd", "rkr_file_write_svd", "rkr_file_write_query_distribution",
-    "rkr_file_read_query_distribution", "rkr_index_load_files",
+    "rkr_file_read_query_distribution", "rkr_index_load_files", "rkr_index_set_shard", "rkr_shard_query",
+    "rkr_shard_merge", "rkr_host_exchange_create", "rkr_host_exchange", "rkr_host_exchange_destroy",
 ]
+
+# rkr_exchange_fn (include/rkr.h): int (*)(void *ctx, int32_t *counts, int64_t n, void *stream)
+EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p)
 
 
 class RkrError(RuntimeError):
@@ -400,11 +404,114 @@ class Index:
         return out
 
     def query_rank_distribution(self, sample_item_ids):
-        """ComputeQueryRankByComputation: accumulated user counts by rank, [n_sample_item][n_item+1]."""
+        """ComputeQueryRankByComputation: accumulated user counts by rank, [n_sample_item][n_item+1]
+        (on a user shard: every shard's users, each shard calling)."""
         si = _i32(sample_item_ids)
         out = np.empty((si.shape[0], self.n_item + 1), np.int32)
         _check(_lib.rkr_index_query_rank_distribution(self._h, _p(si), C.c_int32(si.shape[0]), _p(out)))
         return out
+
+    # ---- user shards ----
+
+    def set_shard(self, shard, n_shards, user_offset, n_user_total, exchange):
+        """rkr_index_set_shard: this index becomes shard `shard` of n_shards, holding users
+        [user_offset, user_offset + n_user) of n_user_total.  exchange: a HostExchange, an
+        (EXCHANGE_FN, ctx) pair, or a Python callable fn(counts_address, n, stream) that sums the n
+        int32 counts over all shards in place (see rkr_b200.shard.TorchExchange); None with
+        n_shards == 1 makes the index whole again."""
+        if exchange is None:
+            fn, ctx, keep = None, None, None
+        elif isinstance(exchange, HostExchange):
+            fn, ctx, keep = exchange.fn, exchange.ctx, exchange
+        elif isinstance(exchange, tuple):
+            fn, ctx = exchange
+            keep = exchange
+        else:
+            fn, ctx = exchange_callback(exchange), None
+            keep = (fn, exchange)
+        _check(_lib.rkr_index_set_shard(self._h, C.c_int32(shard), C.c_int32(n_shards), C.c_int64(user_offset),
+                                        C.c_int64(n_user_total), fn, C.c_void_p(ctx)))
+        self._exchange_keep = keep  # the callback must outlive its use
+
+    def shard_query(self, method, query, k_per_q, stats=False):
+        """rkr_shard_query: this shard's part of rkr_query -- (part, n_front[, stats]) with part the
+        flat sum(k) USER_RANK entries (row q: n_front[q] results, then candidates; user_id -1 unused)."""
+        m = METHODS[method] if isinstance(method, str) else int(method)
+        q = _f32(query)
+        ks = _i32(k_per_q)
+        if ks.shape[0] != q.shape[0]:
+            raise ValueError("one k per query")
+        part = np.zeros(int(ks.sum()), USER_RANK)
+        front = np.zeros(max(q.shape[0], 1), np.int32)
+        st = np.zeros(max(q.shape[0], 1), QUERY_STATS) if stats else None
+        na = C.c_int32()
+        _check(_lib.rkr_shard_query(self._h, C.c_int32(m), _p(q), C.c_int32(q.shape[0]), _p(ks), _p(part), _p(front),
+                                    _p(st), C.byref(na)))
+        n = na.value
+        part = part[:int(ks[:n].sum())]
+        return (part, front[:n], st[:n]) if stats else (part, front[:n])
+
+
+# ---- user shards ------------------------------------------------------------------------------------------
+
+def exchange_callback(fn):
+    """An rkr_exchange_fn calling fn(counts_address, n, stream) (stream 0: host memory); an exception
+    fails the query.  Keep the returned object alive while an index uses it."""
+    def cb(ctx, counts, n, stream):
+        try:
+            fn(counts or 0, int(n), stream or 0)
+            return 0
+        except Exception:  # noqa: BLE001 -- reported to the library as a failed exchange
+            return 1
+    return EXCHANGE_FN(cb)
+
+
+class HostExchange:
+    """rkr_host_exchange: the count exchange of shards driven by threads of one process (for example
+    several shards on one GPU).  Waits up to timeout_s for every member at each exchange."""
+
+    def __init__(self, n_members, timeout_s=60.0):
+        g = C.c_void_p()
+        _check(_lib.rkr_host_exchange_create(C.c_int32(n_members), C.c_double(timeout_s), C.byref(g)))
+        self._g = g
+        self.fn = C.cast(_lib.rkr_host_exchange, EXCHANGE_FN)
+
+    @property
+    def ctx(self):
+        return self._g.value
+
+    def close(self):
+        if getattr(self, "_g", None) is not None and self._g.value:
+            _lib.rkr_host_exchange_destroy(self._g)
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+
+def shard_merge(k_per_q, parts, fronts, stats=None):
+    """rkr_shard_merge: the shards' parts (in shard order) merged into rkr_query's output: a flat
+    sum(k) USER_RANK array (and the merged QUERY_STATS when every shard's stats are given)."""
+    ks = _i32(k_per_q)
+    n_sh, nq = len(parts), ks.shape[0]
+    parts = [np.ascontiguousarray(p, USER_RANK) for p in parts]
+    fronts = [_i32(f) for f in fronts]
+    for p, f in zip(parts, fronts):
+        if p.shape[0] != int(ks.sum()) or f.shape[0] != nq:
+            raise ValueError("every part holds sum(k_per_q) entries and every n_front one per query")
+    pp = (C.c_void_p * n_sh)(*[p.ctypes.data for p in parts])
+    fp = (C.c_void_p * n_sh)(*[f.ctypes.data for f in fronts])
+    sp, st_out = None, None
+    if stats is not None:
+        stats = [np.ascontiguousarray(s, QUERY_STATS) for s in stats]
+        sp = (C.c_void_p * n_sh)(*[s.ctypes.data for s in stats])
+        st_out = np.zeros(max(nq, 1), QUERY_STATS)
+    out = np.zeros(int(ks.sum()), USER_RANK)
+    _check(_lib.rkr_shard_merge(C.c_int32(n_sh), C.c_int32(nq), _p(ks), pp, fp, sp, _p(out), _p(st_out)))
+    return (out, st_out[:nq]) if stats is not None else out
 
 
 # ---- serving ----------------------------------------------------------------------------------------------

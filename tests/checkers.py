@@ -64,7 +64,8 @@ class Oracle:
         L.orc_sqrt_constexpr.restype = C.c_float
         L.orc_sqrt_constexpr.argtypes = [C.c_float]
         L.orc_inner_product.restype = C.c_float
-        for name in ("orc_qs_retrieval", "orc_us_retrieval", "orc_qsrp_retrieval", "orc_optimal_sample_rank"):
+        for name in ("orc_qs_retrieval", "orc_us_retrieval", "orc_qsrp_retrieval", "orc_optimal_sample_rank",
+                     "orc_qs_retrieval_shard", "orc_us_retrieval_shard", "orc_qsrp_retrieval_shard"):
             getattr(L, name).restype = C.c_int
 
     def normalize(self, v):
@@ -199,6 +200,58 @@ class Oracle:
                                          C.c_int32(topk), _p(qip_state), _p(out), _p(st))
         assert rc == 0
         return out, st
+
+    # ---- the same on one user shard (exchange: an (rkr_exchange_fn, ctx) pair summing host counts) ----
+
+    def _shard_out(self, nq, topk):
+        return np.zeros((nq, topk), USER_RANK), np.zeros(nq, np.int32), np.zeros(nq, STATS)
+
+    def qs_retrieval_shard(self, user, item, check_dim, sample_rank, thr, query, topk, user_offset, n_user_total,
+                           exchange):
+        user, item, sr, thr, query = _f32(user), _f32(item), _i32(sample_rank), _f32(thr), _f32(query)
+        nq = query.shape[0]
+        out, front, st = self._shard_out(nq, topk)
+        fn, ctx = exchange
+        rc = self.lib.orc_qs_retrieval_shard(_p(user), C.c_int64(user.shape[0]), _p(item), C.c_int64(item.shape[0]),
+                                             C.c_int32(user.shape[1]), C.c_int32(check_dim), _p(sr),
+                                             C.c_int32(sr.shape[0]), _p(thr), _p(query), C.c_int32(nq),
+                                             C.c_int32(topk), C.c_int64(user_offset), C.c_int64(n_user_total),
+                                             C.c_int32(user_offset == 0), fn, C.c_void_p(ctx), _p(out), _p(front),
+                                             _p(st))
+        assert rc == nq, rc
+        return out, front, st
+
+    def us_retrieval_shard(self, user, item, sample_rank, thr, query, topk, user_offset, n_user_total, exchange):
+        user, item, sr, thr, query = _f32(user), _f32(item), _i32(sample_rank), _f32(thr), _f32(query)
+        nq = query.shape[0]
+        out, front, st = self._shard_out(nq, topk)
+        fn, ctx = exchange
+        n = self.lib.orc_us_retrieval_shard(_p(user), C.c_int64(user.shape[0]), _p(item), C.c_int64(item.shape[0]),
+                                            C.c_int32(user.shape[1]), _p(sr), C.c_int32(sr.shape[0]), _p(thr),
+                                            _p(query), C.c_int32(nq), C.c_int32(topk), C.c_int64(user_offset),
+                                            C.c_int64(n_user_total), C.c_int32(user_offset == 0), fn,
+                                            C.c_void_p(ctx), _p(out), _p(front), _p(st))
+        assert n >= 0, n
+        return out[:n], front[:n], st[:n]
+
+    def qsrp_retrieval_shard(self, user, svd_user, transfer_item, item, check_dim, sample_rank, thr, reg_rank, reg,
+                             query, topk, user_offset, n_user_total, exchange, qip_state=None):
+        user, svd_user, ti, item = _f32(user), _f32(svd_user), _f32(transfer_item), _f32(item)
+        sr, thr, rr, reg, query = _i32(sample_rank), _f32(thr), _i32(reg_rank), _f32(reg), _f32(query)
+        nq, n_user = query.shape[0], user.shape[0]
+        if qip_state is None:
+            qip_state = np.zeros(n_user, np.float32)
+        out, front, st = self._shard_out(nq, topk)
+        fn, ctx = exchange
+        rc = self.lib.orc_qsrp_retrieval_shard(_p(user), _p(svd_user), _p(ti), C.c_int64(n_user), _p(item),
+                                               C.c_int64(item.shape[0]), C.c_int32(user.shape[1]),
+                                               C.c_int32(check_dim), _p(sr), C.c_int32(sr.shape[0]), _p(thr),
+                                               _p(rr), C.c_int32(rr.shape[0]), _p(reg), _p(query), C.c_int32(nq),
+                                               C.c_int32(topk), C.c_int64(user_offset), C.c_int64(n_user_total),
+                                               C.c_int32(user_offset == 0), fn, C.c_void_p(ctx), _p(qip_state),
+                                               _p(out), _p(front), _p(st))
+        assert rc == nq, rc
+        return out, front, st
 
     def exact_rank_f64(self, user, item, query):
         user, item, query = _f32(user), _f32(item), _f32(query)

@@ -533,11 +533,15 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--single-queries", type=int, default=100)
     ap.add_argument("--batch", type=int, default=0, help="queries per step (default: the workload's)")
+    ap.add_argument("--n-user", type=int, default=0,
+                    help="users of the workload (default: the configuration's); smaller for profiler captures")
     ap.add_argument("--serve-requests", type=int, default=200, help="config5: requests per trace")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="config5: offered requests/s")
     ap.add_argument("--no-plain", dest="plain", action="store_false",
                     help="skip timing the plain FP32 GPU form")
     args = ap.parse_args()
+    if args.n_user:
+        CONFIGS[args.config] = (args.n_user,) + CONFIGS[args.config][1:]
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank_id = int(os.environ.get("RANK", "0"))

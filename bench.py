@@ -122,12 +122,10 @@ def build_index(R, user_raw, item, cfg, device):
     thr = ix.build_sample_search(rank)
     stages["thresholds"] = time.perf_counter() - t
     t = time.perf_counter()
-    reg = R.fit_regression(thr)
+    reg = ix.fit_regression()  # on the device, from the resident thresholds; loaded as the index's models
     stages["regression_fit"] = time.perf_counter() - t
     t = time.perf_counter()
-    ti, su, cd = R.svd_build(user, 0.7)
-    ix.load_svd(cd, ti, su)
-    ix.load_regression(rank, reg)
+    ti, su, cd = ix.svd_build(0.7)  # Gram matrix and projection on the device; made the index's
     stages["svd"] = time.perf_counter() - t
     parts = dict(user=user, rank=rank, thr=thr, reg=reg, ti=ti, su=su, cd=cd)
     return ix, parts, stages

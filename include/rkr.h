@@ -267,10 +267,24 @@ int rkr_uniform_sample_rank(int32_t n_item, int32_t n_sample, int32_t *out);
 /* NormalLinearRegressionLP fit (StartPreprocess / BatchLoopPreprocess,
  * NormalLinearRegressionLP.hpp:72-310): records_out [n_user][7] as rkr_index_load_regression takes. */
 int rkr_fit_regression(const float *thresholds, int64_t n_user, int32_t n_sample, float *records_out);
+/* The same fit on the device, from the index's resident sampled thresholds (loaded or built), with
+ * the index's sample ranks as the models' (NormalLinearRegressionLP::BuildIndex fits from the
+ * SampleSearch index of the same ranks): the models become the index's regression index (as
+ * rkr_index_load_regression would load them) and, if records_out (host, [n_user][7]) is not NULL,
+ * are copied out.  The records equal rkr_fit_regression's (the same arithmetic, operation by
+ * operation).  2 <= n_sample <= 4096. */
+int rkr_index_fit_regression(rkr_index *index, float *records_out);
 /* SVD::PerformSVD (src/include/alg/SVD.hpp:62-124): thin SVD of the users, the transfer matrix,
  * the transformed users and check_dim for the given sigma ratio. */
 int rkr_svd_build(const float *user, int64_t n_user, int32_t dim, float sigma, float *transfer_item_out,
                   float *svd_user_out, int32_t *check_dim_out);
+/* The same transform built on the device from the index's resident users (the Gram matrix and the
+ * projection on the device, the d x d eigen-decomposition on the host) and made the index's SVD
+ * index, as rkr_index_load_svd would load it; transfer_item_out (host [dim][dim]), svd_user_out
+ * (host [n_user][dim]) and check_dim_out may be NULL.  A valid transform like rkr_svd_build's (the
+ * Gram matrix's sums run in another order, so the two agree to rounding, not bit for bit). */
+int rkr_index_svd_build(rkr_index *index, float sigma, float *transfer_item_out, float *svd_user_out,
+                        int32_t *check_dim_out);
 
 /* ---- index files --------------------------------------------------------------------------------- */
 

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "rkr.h"
+#include "rkr_svd_host.h"
 
 namespace rkr {
 void set_error(const char *fmt, ...);
@@ -189,6 +190,71 @@ void fit_user(const float *thr, int S, float *rec) {
 }
 
 }  // namespace
+
+namespace rkr {
+
+// The SVD transform from the Gram matrix G = user^T user ([d][d], full; overwritten): cyclic Jacobi
+// rotations to its eigen-decomposition user^T user = E diag(s^2) E^T, the singular values s
+// (descending) with their vectors Es (column k for s[k]), transfer_item[r][c] = s_r * E[c][r], and
+// check_dim, the first dimension whose cumulative singular value reaches sigma_ratio of the total
+// (SVD.hpp:214-226).
+void svd_from_gram(std::vector<double> &G, int d, float sigma_ratio, float *transfer_item, std::vector<double> &Es,
+                   std::vector<float> &s, int *check_dim) {
+    std::vector<double> E((size_t) d * d, 0.0);
+    for (int i = 0; i < d; i++) E[(size_t) i * d + i] = 1.0;
+    for (int sweep = 0; sweep < 60; sweep++) {
+        double off = 0, diag = 0;
+        for (int p = 0; p < d; p++) {
+            diag += G[(size_t) p * d + p] * G[(size_t) p * d + p];
+            for (int q = p + 1; q < d; q++) off += G[(size_t) p * d + q] * G[(size_t) p * d + q];
+        }
+        if (off <= 1e-30 * diag) break;
+        for (int p = 0; p < d; p++)
+            for (int q = p + 1; q < d; q++) {
+                const double apq = G[(size_t) p * d + q];
+                if (std::fabs(apq) < 1e-300) continue;
+                const double th = (G[(size_t) q * d + q] - G[(size_t) p * d + p]) / (2 * apq);
+                const double t = (th >= 0 ? 1.0 : -1.0) / (std::fabs(th) + std::sqrt(th * th + 1));
+                const double c = 1 / std::sqrt(t * t + 1), s = t * c;
+                for (int r = 0; r < d; r++) {
+                    const double x = G[(size_t) r * d + p], y = G[(size_t) r * d + q];
+                    G[(size_t) r * d + p] = c * x - s * y;
+                    G[(size_t) r * d + q] = s * x + c * y;
+                }
+                for (int r = 0; r < d; r++) {
+                    const double x = G[(size_t) p * d + r], y = G[(size_t) q * d + r];
+                    G[(size_t) p * d + r] = c * x - s * y;
+                    G[(size_t) q * d + r] = s * x + c * y;
+                }
+                for (int r = 0; r < d; r++) {
+                    const double x = E[(size_t) r * d + p], y = E[(size_t) r * d + q];
+                    E[(size_t) r * d + p] = c * x - s * y;
+                    E[(size_t) r * d + q] = s * x + c * y;
+                }
+            }
+    }
+    std::vector<int> ord(d);
+    std::iota(ord.begin(), ord.end(), 0);
+    std::sort(ord.begin(), ord.end(), [&](int a, int b) { return G[(size_t) a * d + a] > G[(size_t) b * d + b]; });
+    s.assign(d, 0.0f);
+    Es.assign((size_t) d * d, 0.0);
+    for (int k = 0; k < d; k++) {
+        const int e = ord[k];
+        s[k] = (float) std::sqrt(std::max(G[(size_t) e * d + e], 0.0));
+        for (int i = 0; i < d; i++) Es[(size_t) i * d + k] = E[(size_t) i * d + e];
+    }
+    for (int r = 0; r < d; r++)
+        for (int c = 0; c < d; c++) transfer_item[(size_t) r * d + c] = (float) (s[r] * (float) Es[(size_t) c * d + r]);
+    std::vector<float> cum(d);
+    cum[0] = s[0];
+    for (int c = 1; c < d; c++) cum[c] = cum[c - 1] + s[c];
+    int cdim = 0;
+    for (int c = 0; c < d; c++)
+        if (cum[c] / cum[d - 1] >= sigma_ratio) { cdim = c; break; }
+    *check_dim = cdim;
+}
+
+}  // namespace rkr
 
 extern "C" {
 
@@ -401,51 +467,10 @@ int rkr_svd_build(const float *user, int64_t n_user, int32_t dim, float sigma_ra
     }
     for (int i = 0; i < d; i++)
         for (int j = 0; j < i; j++) G[(size_t) i * d + j] = G[(size_t) j * d + i];
-    std::vector<double> E((size_t) d * d, 0.0);
-    for (int i = 0; i < d; i++) E[(size_t) i * d + i] = 1.0;
-    for (int sweep = 0; sweep < 60; sweep++) {
-        double off = 0, diag = 0;
-        for (int p = 0; p < d; p++) {
-            diag += G[(size_t) p * d + p] * G[(size_t) p * d + p];
-            for (int q = p + 1; q < d; q++) off += G[(size_t) p * d + q] * G[(size_t) p * d + q];
-        }
-        if (off <= 1e-30 * diag) break;
-        for (int p = 0; p < d; p++)
-            for (int q = p + 1; q < d; q++) {
-                const double apq = G[(size_t) p * d + q];
-                if (std::fabs(apq) < 1e-300) continue;
-                const double th = (G[(size_t) q * d + q] - G[(size_t) p * d + p]) / (2 * apq);
-                const double t = (th >= 0 ? 1.0 : -1.0) / (std::fabs(th) + std::sqrt(th * th + 1));
-                const double c = 1 / std::sqrt(t * t + 1), s = t * c;
-                for (int r = 0; r < d; r++) {
-                    const double x = G[(size_t) r * d + p], y = G[(size_t) r * d + q];
-                    G[(size_t) r * d + p] = c * x - s * y;
-                    G[(size_t) r * d + q] = s * x + c * y;
-                }
-                for (int r = 0; r < d; r++) {
-                    const double x = G[(size_t) p * d + r], y = G[(size_t) q * d + r];
-                    G[(size_t) p * d + r] = c * x - s * y;
-                    G[(size_t) q * d + r] = s * x + c * y;
-                }
-                for (int r = 0; r < d; r++) {
-                    const double x = E[(size_t) r * d + p], y = E[(size_t) r * d + q];
-                    E[(size_t) r * d + p] = c * x - s * y;
-                    E[(size_t) r * d + q] = s * x + c * y;
-                }
-            }
-    }
-    std::vector<int> ord(d);
-    std::iota(ord.begin(), ord.end(), 0);
-    std::sort(ord.begin(), ord.end(), [&](int a, int b) { return G[(size_t) a * d + a] > G[(size_t) b * d + b]; });
-    std::vector<float> s(d);
-    std::vector<double> Es((size_t) d * d);
-    for (int k = 0; k < d; k++) {
-        const int e = ord[k];
-        s[k] = (float) std::sqrt(std::max(G[(size_t) e * d + e], 0.0));
-        for (int i = 0; i < d; i++) Es[(size_t) i * d + k] = E[(size_t) i * d + e];
-    }
-    for (int r = 0; r < d; r++)
-        for (int c = 0; c < d; c++) transfer_item[(size_t) r * d + c] = (float) (s[r] * (float) Es[(size_t) c * d + r]);
+    std::vector<double> Es;
+    std::vector<float> s;
+    int check_dim = 0;
+    rkr::svd_from_gram(G, d, sigma_ratio, transfer_item, Es, s, &check_dim);
     // svd_user = user Es diag(1/s), kProjBlock users at a time, each output summed over i in order
     constexpr int kProjBlock = 4;
 #pragma omp parallel
@@ -469,12 +494,6 @@ int rkr_svd_build(const float *user, int64_t n_user, int32_t dim, float sigma_ra
                     svd_user[(u0 + b) * d + k] = s[k] > 0 ? (float) (acc[(size_t) b * d + k] / s[k]) : 0.0f;
         }
     }
-    std::vector<float> cum(d);
-    cum[0] = s[0];
-    for (int c = 1; c < d; c++) cum[c] = cum[c - 1] + s[c];
-    int check_dim = 0;
-    for (int c = 0; c < d; c++)
-        if (cum[c] / cum[d - 1] >= sigma_ratio) { check_dim = c; break; }
     *check_dim_out = check_dim;
     return RKR_OK;
 }

@@ -45,6 +45,7 @@ EXPORTS = [
     "rkr_file_read_svd", "rkr_file_write_svd", "rkr_file_write_query_distribution",
     "rkr_file_read_query_distribution", "rkr_index_load_files", "rkr_index_set_shard", "rkr_shard_query",
     "rkr_shard_merge", "rkr_host_exchange_create", "rkr_host_exchange", "rkr_host_exchange_destroy",
+    "rkr_index_fit_regression", "rkr_index_svd_build",
 ]
 
 # rkr_exchange_fn (include/rkr.h): int (*)(void *ctx, int32_t *counts, int64_t n, void *stream)
@@ -295,6 +296,22 @@ class Index:
     def load_regression(self, sample_rank, records):
         sr, rec = _i32(sample_rank), _f32(records)
         _check(_lib.rkr_index_load_regression(self._h, _p(sr), C.c_int32(sr.shape[0]), _p(rec)))
+
+    def fit_regression(self, records=True):
+        """rkr_index_fit_regression: fit the regression models on the device from the resident
+        thresholds and make them the index's; returns the [n_user][7] records (or None)."""
+        out = np.empty((self.n_user, 7), np.float32) if records else None
+        _check(_lib.rkr_index_fit_regression(self._h, _p(out)))
+        return out
+
+    def svd_build(self, sigma=0.7, copy_out=True):
+        """rkr_index_svd_build: the SVD transform from the resident users on the device, made the
+        index's; returns (transfer_item, svd_user, check_dim) (the arrays None without copy_out)."""
+        ti = np.empty((self.dim, self.dim), np.float32) if copy_out else None
+        su = np.empty((self.n_user, self.dim), np.float32) if copy_out else None
+        cd = C.c_int32()
+        _check(_lib.rkr_index_svd_build(self._h, C.c_float(sigma), _p(ti), _p(su), C.byref(cd)))
+        return ti, su, cd.value
 
     def load_svd(self, check_dim, transfer_item, svd_user):
         ti, su = _f32(transfer_item), _f32(svd_user)

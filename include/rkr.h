@@ -344,6 +344,13 @@ int rkr_file_read_query_distribution(const char *dir, int32_t n_sample_item, int
 int rkr_index_load_files(rkr_index *index, int32_t method, const char *index_dir, const char *dataset_name,
                          int32_t n_sample, int32_t n_sample_query, int32_t sample_topk);
 
+/* bstb's disk score table (src/app/BuildScoreTableBatch.cpp:75-150, written by ReadAll::BuildIndexLoop,
+ * src/include/alg/DiskIndex/ReadAll.hpp): path receives the first n_user_out (<= n_user) users'
+ * score rows against all items, each sorted descending, n_item floats per row, no header (the
+ * reference names it <index_dir>/<dataset>.index and caps the users at its evaluation size).  The
+ * rows are computed on the device, as rkr_score_sort_batch returns them. */
+int rkr_file_write_score_table(rkr_index *index, const char *path, int64_t n_user_out);
+
 /* ---- user shards ---------------------------------------------------------------------------------- */
 /*
  * An index too large for one GPU is split by users: shard s is an ordinary rkr_index over the

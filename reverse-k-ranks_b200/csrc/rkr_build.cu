@@ -152,7 +152,31 @@ __global__ void __launch_bounds__(kSelThreads) row_select_kernel(SelectArgs a, i
         const int row = a.row_list ? a.row_list[ri] : ri;
         const float *src = a.rows + (int64_t) row * a.ld;
         float mn = __int_as_float(0x7f800000), mx = -mn;
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        // the row in 16-byte loads, four per thread in flight before their values are stored (rows
+        // start 16-byte aligned: ld is a multiple of 4)
+        const float4 *src4 = reinterpret_cast<const float4 *>(src);
+        const int n4 = n >> 2;
+        for (int i0 = threadIdx.x; i0 < n4; i0 += 4 * blockDim.x) {
+            float4 x[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int i = i0 + k * blockDim.x;
+                if (i < n4) x[k] = __ldcs(src4 + i);
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int i = i0 + k * blockDim.x;
+                if (i < n4) {
+                    vals[4 * i] = x[k].x;
+                    vals[4 * i + 1] = x[k].y;
+                    vals[4 * i + 2] = x[k].z;
+                    vals[4 * i + 3] = x[k].w;
+                    mn = fminf(fminf(mn, x[k].x), fminf(fminf(x[k].y, x[k].z), x[k].w));
+                    mx = fmaxf(fmaxf(mx, x[k].x), fmaxf(fmaxf(x[k].y, x[k].z), x[k].w));
+                }
+            }
+        }
+        for (int i = 4 * n4 + threadIdx.x; i < n; i += blockDim.x) {
             const float x = src[i];
             vals[i] = x;
             mn = fminf(mn, x);

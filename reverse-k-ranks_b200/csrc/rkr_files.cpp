@@ -13,6 +13,7 @@
 #include <sys/stat.h>
 #include <unistd.h>
 
+#include <algorithm>
 #include <cerrno>
 #include <cstdarg>
 #include <cstdint>
@@ -533,6 +534,30 @@ int rkr_index_load_files(rkr_index *index, int32_t method, const char *index_dir
     std::vector<float> rec((size_t) 7 * (size_t) n_user);
     v.records(rec.data());
     return rkr_index_load_regression(index, v.rank, v.n_sample, rec.data());
+}
+
+// BuildScoreTableBatch (src/app/BuildScoreTableBatch.cpp:75-150) with ReadAll's writer
+// (src/include/alg/DiskIndex/ReadAll.hpp: BuildIndexLoop): the first n_user_out users' score rows,
+// each sorted descending, n_item floats per row in user order, no header.  The rows come from the
+// device (rkr_score_sort_batch) a batch of at most 256 MB at a time.
+int rkr_file_write_score_table(rkr_index *index, const char *path, int64_t n_user_out) {
+    int64_t n_user = 0, n_item = 0;
+    if (!index || !path || rkr_index_shape(index, &n_user, &n_item, nullptr) != RKR_OK || n_user_out < 0 ||
+        n_user_out > n_user || n_item <= 0) {
+        set_error("invalid argument");
+        return RKR_ERR_INVALID;
+    }
+    Writer w;
+    if (int st = w.open(path)) return st;
+    const int64_t batch = std::max<int64_t>(1, (int64_t(256) << 20) / (n_item * (int64_t) sizeof(float)));
+    std::vector<float> rows;
+    for (int64_t u0 = 0; u0 < n_user_out; u0 += batch) {
+        const int64_t nb = std::min(batch, n_user_out - u0);
+        rows.resize((size_t) (nb * n_item));
+        if (int st = rkr_score_sort_batch(index, u0, nb, rows.data())) return st;
+        w.put(rows.data(), rows.size() * sizeof(float));
+    }
+    return w.close();
 }
 
 }  // extern "C"

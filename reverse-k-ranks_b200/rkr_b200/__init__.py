@@ -45,7 +45,7 @@ EXPORTS = [
     "rkr_file_read_svd", "rkr_file_write_svd", "rkr_file_write_query_distribution",
     "rkr_file_read_query_distribution", "rkr_index_load_files", "rkr_index_set_shard", "rkr_shard_query",
     "rkr_shard_merge", "rkr_host_exchange_create", "rkr_host_exchange", "rkr_host_exchange_destroy",
-    "rkr_index_fit_regression", "rkr_index_svd_build",
+    "rkr_index_fit_regression", "rkr_index_svd_build", "rkr_file_write_score_table",
 ]
 
 # rkr_exchange_fn (include/rkr.h): int (*)(void *ctx, int32_t *counts, int64_t n, void *stream)
@@ -413,6 +413,11 @@ class Index:
         cnt = np.zeros(max(k, 1), np.int64)
         _check(_lib.rkr_profile_read(self._h, C.c_int32(k), names, _p(ms), _p(cnt), C.byref(n)))
         return {names.raw[64 * i:64 * i + 64].split(b"\0")[0].decode(): (float(ms[i]), int(cnt[i])) for i in range(k)}
+
+    def write_score_table(self, path, n_user_out=None):
+        """rkr_file_write_score_table: bstb's disk score table (descending rows, no header)."""
+        n = self.n_user if n_user_out is None else int(n_user_out)
+        _check(_lib.rkr_file_write_score_table(self._h, _b(path), C.c_int64(n)))
 
     def score_sort_batch(self, start_user, n_rows):
         """ComputeScoreTableBatch::ComputeSortItemsBatch: descending score rows of users [start, start+n)."""

@@ -101,3 +101,18 @@ def test_device_svd_is_the_host_transform_to_rounding(case):
     want, _ = Oracle().qsrp_retrieval(un, su, ti, g["item"], cd, g["opt_rank"], g["thr"], g["opt_rank"], g["reg"],
                                       g["query"], k)
     assert np.array_equal(bits(out).reshape(-1), bits(want).reshape(-1))
+
+
+def test_score_table_file_matches_the_oracle(tmp_path):
+    """rkr_file_write_score_table: bstb's table (descending score rows, no header) for the first users."""
+    g = load("small")
+    n_out, n_item = 120, g["item"].shape[0]
+    path = tmp_path / "small.index"
+    with R.Index(g["user_norm"], g["item"]) as ix:
+        ix.write_score_table(str(path), n_out)
+        with pytest.raises(R.RkrError):
+            ix.write_score_table(str(tmp_path / "too_many.index"), ix.n_user + 1)
+    rows = np.fromfile(path, np.float32)
+    assert rows.size == n_out * n_item
+    want = Oracle().score_sort_rows(g["user_norm"], g["item"], 0, n_out)
+    assert np.array_equal(bits(rows), bits(want).reshape(-1))

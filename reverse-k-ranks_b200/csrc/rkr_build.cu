@@ -293,6 +293,107 @@ __global__ void __launch_bounds__(kSelThreads) row_select_kernel(SelectArgs a, i
     }
 }
 
+// ---- the query-rank distribution's counting ------------------------------------------------------------
+//
+// ComputeQueryRankByComputation (QueryRankByComputation.hpp:122-242) needs, per user and sampled
+// item, the number of items scoring strictly above the sampled item's score.  Per row: the sampled
+// items' scores sorted descending (w), then one stream of the row in which every score x goes to
+// bucket b(x) = #{k : w_k >= x} (a binary search in shared memory), counted per warp.  A score beats
+// w_p exactly when b(x) <= p, so the rank of the sampled item at sorted position p is the number of
+// scores in buckets 0 .. p.  No copy of the row, no value bins, one pass.
+constexpr int kRankMaxSample = 1024;  // sampled items per row this kernel holds
+inline size_t row_rank_smem(int n_si) {
+    return sizeof(float) * 2 * (size_t) n_si + sizeof(int) * (size_t) n_si +
+           sizeof(int) * (size_t) (kSelThreads / 32) * (size_t) (n_si + 1);
+}
+
+__global__ void __launch_bounds__(kSelThreads) row_rank_kernel(SelectArgs a) {
+    extern __shared__ __align__(16) int rk_smem[];
+    const int ns = a.n_si, n = a.n_item;
+    const int nw = blockDim.x >> 5, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float *sval = reinterpret_cast<float *>(rk_smem);  // [ns] the sampled items' scores
+    float *wsort = sval + ns;                          // [ns] the same, descending
+    int *pos_of = reinterpret_cast<int *>(wsort + ns);  // [ns] sorted position of sampled item s
+    int *cnt = pos_of + ns;                            // [nw][ns + 1] bucket counts per warp
+    const int n_iter = a.row_list ? a.n_list : a.n_rows;
+    for (int ri = blockIdx.x; ri < n_iter; ri += gridDim.x) {
+        const int row = a.row_list ? a.row_list[ri] : ri;
+        const float *src = a.rows + (int64_t) row * a.ld;
+        for (int t = threadIdx.x; t < ns; t += blockDim.x) sval[t] = src[a.sample_item[t]];
+        for (int t = threadIdx.x; t < nw * (ns + 1); t += blockDim.x) cnt[t] = 0;
+        __syncthreads();
+        // sorted position: the scores above it, then the equal ones listed before it
+        for (int t = threadIdx.x; t < ns; t += blockDim.x) {
+            const float v = sval[t];
+            int p = 0;
+            for (int k = 0; k < ns; k++) {
+                const float y = sval[k];
+                p += (y > v) | ((y == v) & (k < t));
+            }
+            wsort[p] = v;
+            pos_of[t] = p;
+        }
+        __syncthreads();
+        int *cw = cnt + w * (ns + 1);
+        auto bucket = [&](float x) {  // first k with wsort[k] < x
+            int lo = 0, len = ns;
+            while (len > 0) {
+                const int half = len >> 1, mid = lo + half;
+                if (wsort[mid] >= x) { lo = mid + 1; len -= half + 1; } else len = half;
+            }
+            return lo;
+        };
+        // the row in 16-byte loads, four in flight per thread (rows start 16-byte aligned)
+        const float4 *src4 = reinterpret_cast<const float4 *>(src);
+        const int n4 = n >> 2;
+        for (int i0 = threadIdx.x; i0 < n4; i0 += 4 * blockDim.x) {
+            float4 x[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int i = i0 + k * blockDim.x;
+                if (i < n4) x[k] = __ldcs(src4 + i);
+            }
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int i = i0 + k * blockDim.x;
+                if (i < n4) {
+                    atomicAdd(&cw[bucket(x[k].x)], 1);
+                    atomicAdd(&cw[bucket(x[k].y)], 1);
+                    atomicAdd(&cw[bucket(x[k].z)], 1);
+                    atomicAdd(&cw[bucket(x[k].w)], 1);
+                }
+            }
+        }
+        for (int i = 4 * n4 + threadIdx.x; i < n; i += blockDim.x) atomicAdd(&cw[bucket(src[i])], 1);
+        __syncthreads();
+        // the warps' counts summed into warp 0's row, then its inclusive prefix (warp 0, 32 at a time)
+        for (int b = threadIdx.x; b <= ns; b += blockDim.x) {
+            int t = 0;
+            for (int k = 0; k < nw; k++) t += cnt[k * (ns + 1) + b];
+            cnt[b] = t;
+        }
+        __syncthreads();
+        if (w == 0) {
+            int base = 0;
+            for (int b0 = 0; b0 <= ns; b0 += 32) {
+                const int b = b0 + lane;
+                int v = b <= ns ? cnt[b] : 0;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, v, o);
+                    if (lane >= o) v += y;
+                }
+                if (b <= ns) cnt[b] = base + v;
+                base += __shfl_sync(0xffffffffu, v, 31);
+            }
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < ns; t += blockDim.x)
+            atomicAdd(&a.rank_hist[(int64_t) t * (n + 1) + cnt[pos_of[t]]], 1);
+        __syncthreads();
+    }
+}
+
 // ---- rows longer than shared memory ------------------------------------------------------------------
 //
 // A row of config-4 size (624,961 items) does not fit in shared memory.  Instead of copying it to a
@@ -572,6 +673,16 @@ int run_rows(RowPipeline &P, int64_t u0, int64_t nu, SelectArgs sa) {
     sa.ld = P.ld;
     sa.n_rows = (int) nu;
     sa.n_item = (int) ix->n_item;
+    if (sa.rank_hist && !sa.thr_out && !sa.sorted_out && sa.n_si <= kRankMaxSample) {
+        // the query-rank distribution alone: one counting stream per row, any row length
+        const size_t smem = row_rank_smem(sa.n_si);
+        RKR_CUDA(cudaFuncSetAttribute(row_rank_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        timed(ix, st, "row_rank", [&] {
+            row_rank_kernel<<<(unsigned) std::min<int64_t>(4 * P.sms, nu), kSelThreads, smem, st>>>(sa);
+        });
+        RKR_CUDA(cudaGetLastError());
+        return RKR_OK;
+    }
     if (P.use_smem || sa.sorted_out) {
         // rows in shared memory; or a full sort (rkr_score_sort_batch), which scatters long rows
         // on global scratch

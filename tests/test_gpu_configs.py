@@ -139,3 +139,21 @@ def test_build_rows_larger_than_shared_memory_match_oracle(n_item):
         accu = ix.query_rank_distribution(si)
         _, accu_o = orc.query_rank_distribution(user, item, si)
         assert np.array_equal(accu, accu_o)
+
+
+@pytest.mark.parametrize("n_item", [3001, 40003])
+def test_query_rank_distribution_with_equal_scores_matches_oracle(n_item):
+    """Items drawn from 50 distinct vectors (every score repeated), rows of both lengths (shared-memory
+    and longer), an item count that is not a multiple of four: the counting of items strictly above
+    each sampled item's score against the oracle."""
+    n_user, d = 300, 16
+    rng = np.random.default_rng(n_item + 7)
+    orc = Oracle()
+    user = orc.normalize(rng.standard_normal((n_user, d)).astype(np.float32))
+    base = rng.standard_normal((50, d)).astype(np.float32)
+    item = base[rng.integers(0, 50, n_item)]
+    si = R.sample_item(n_item, 150)
+    with R.Index(user, item) as ix:
+        accu = ix.query_rank_distribution(si)
+    _, accu_o = orc.query_rank_distribution(user, item, si)
+    assert np.array_equal(accu, accu_o)

@@ -88,6 +88,10 @@ int rkr_index_load_regression(rkr_index *index, const int32_t *sample_rank, int3
  * transformed users [n_user][dim]; also sets check_dim. */
 int rkr_index_load_svd(rkr_index *index, int32_t check_dim, const float *transfer_item, const float *svd_user);
 
+/* The index's SVD index as SVD::SaveIndex would write it (src/include/alg/SVD.hpp:126-188): transfer_item
+ * (host [dim][dim]), the SVD-space users (host [n_user][dim]) and check_dim; any may be NULL. */
+int rkr_index_svd_read(const rkr_index *index, float *transfer_item_out, float *svd_user_out, int32_t *check_dim_out);
+
 /* Zeroes the per-user query-score vector that QSRPNormalLP carries from one query to the next
  * (Index::queryIP_l_, src/impl/QSRPNormalLP.hpp:73,109); a fresh index starts zeroed. */
 int rkr_index_reset_state(rkr_index *index);
@@ -350,6 +354,25 @@ int rkr_index_load_files(rkr_index *index, int32_t method, const char *index_dir
  * reference names it <index_dir>/<dataset>.index and caps the users at its evaluation size).  The
  * rows are computed on the device, as rkr_score_sort_batch returns them. */
 int rkr_file_write_score_table(rkr_index *index, const char *path, int64_t n_user_out);
+
+/* ---- updates ---------------------------------------------------------------------------------------- */
+
+/* QSRPNormalLPUpdate::InsertUser (src/impl/Update/QSRPNormalLPUpdate.hpp:308-347): appends n users
+ * (host [n][dim], L2-normalised) as users n_user .. n_user + n - 1, with their sampled thresholds
+ * (the index's sample ranks) and, when the index has regression models, their models, computed on
+ * the device; an index with an SVD transform gets it rebuilt over every user with sigma, and its
+ * check_dim with it (SVDUpdate::InsertUser, src/include/alg/SVDUpdate.hpp:63-79).  The new users'
+ * carried QSRPNormalLP scores are zero.  The index must have sampled thresholds, and its regression
+ * models (if any) the thresholds' sample ranks.  No other call may use the index meanwhile. */
+int rkr_index_insert_users(rkr_index *index, const float *user, int64_t n, float sigma);
+
+/* QSRPNormalLPUpdate::DeleteUser (:349-365): removes the users ids[0 .. n) (any order, no repeats,
+ * fewer than n_user); the others keep their order (ids close up), thresholds, models and SVD-space
+ * rows, and the transform stays (SVDUpdate.hpp:81-84).  The carried QSRPNormalLP scores are resized
+ * as the reference resizes its vector: the first n_user - n entries stay, whichever users they
+ * belonged to.  No other call may use the index meanwhile.  Item insertion and deletion
+ * (SampleSearchUpdate's rank offsets) are not supported. */
+int rkr_index_delete_users(rkr_index *index, const int64_t *ids, int64_t n);
 
 /* ---- user shards ---------------------------------------------------------------------------------- */
 /*

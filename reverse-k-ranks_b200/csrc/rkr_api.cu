@@ -319,6 +319,22 @@ int rkr_index_load_svd(rkr_index *ix, int32_t check_dim, const float *transfer_i
     return refine_prepare_norms(ix);
 }
 
+int rkr_index_svd_read(const rkr_index *ix, float *transfer_item_out, float *svd_user_out, int32_t *check_dim_out) {
+    RKR_REQUIRE(ix, "null index");
+    if (!ix->has_svd) {
+        set_error("the index has no SVD transform");
+        return RKR_ERR_STATE;
+    }
+    RKR_TRY(ensure_device(ix));
+    const size_t d = (size_t) ix->dim;
+    if (transfer_item_out)
+        RKR_CUDA(cudaMemcpy(transfer_item_out, ix->transfer_item.p, sizeof(float) * d * d, cudaMemcpyDeviceToHost));
+    if (svd_user_out)
+        RKR_CUDA(cudaMemcpy(svd_user_out, ix->svd_user.p, sizeof(float) * d * (size_t) ix->n_user, cudaMemcpyDeviceToHost));
+    if (check_dim_out) *check_dim_out = ix->check_dim;
+    return RKR_OK;
+}
+
 int rkr_index_reset_state(rkr_index *ix) {
     RKR_REQUIRE(ix, "null index");
     RKR_TRY(ensure_device(ix));

@@ -746,6 +746,21 @@ int build_sample_search(rkr_index *ix, const int32_t *sample_rank, int n_sample)
     return RKR_OK;
 }
 
+int build_thresholds_range(rkr_index *ix, int64_t u_begin, int64_t u_end) {
+    RowPipeline P;
+    RKR_TRY(setup_pipeline(ix, P));
+    const int S = ix->n_sample;
+    for (int64_t u0 = u_begin; u0 < u_end; u0 += P.batch) {
+        const int64_t nu = std::min(P.batch, u_end - u0);
+        SelectArgs sa = {};
+        sa.sample_rank = ix->sample_rank.as<int32_t>();
+        sa.S = S;
+        sa.thr_out = ix->thr.as<float>() + u0 * S;
+        RKR_TRY(run_rows(P, u0, nu, sa));
+    }
+    return RKR_OK;
+}
+
 int score_sort_rows(rkr_index *ix, int64_t start, int64_t n_rows, float *h_rows) {
     RKR_TRY(ensure_device(ix));
     RowPipeline P;

@@ -223,7 +223,8 @@ __global__ void __launch_bounds__(32 * kFitMaxWarps) fit_regression_kernel(const
 
 }  // namespace
 
-int fit_regression_device(rkr_index *ix, cudaStream_t st) {
+// Models of users [u_begin, u_end) into ix->reg (already holding n_user records).
+int fit_regression_device(rkr_index *ix, int64_t u_begin, int64_t u_end, cudaStream_t st) {
     const int S = ix->n_sample;
     int optin = 0;
     RKR_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ix->device));
@@ -235,10 +236,12 @@ int fit_regression_device(rkr_index *ix, cudaStream_t st) {
         return RKR_ERR_INVALID;
     }
     RKR_CUDA(cudaFuncSetAttribute(fit_regression_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-    RKR_TRY(ix->reg.ensure(sizeof(float) * 8 * (size_t) ix->n_user));
-    const unsigned grid = (unsigned) ((ix->n_user + warps - 1) / warps);
+    const int64_t nu = u_end - u_begin;
+    if (nu <= 0) return RKR_OK;
+    const unsigned grid = (unsigned) ((nu + warps - 1) / warps);
     timed(ix, st, "fit_regression", [&] {
-        fit_regression_kernel<<<grid, 32 * warps, smem, st>>>(ix->thr.as<float>(), ix->n_user, S, ix->reg.as<float>());
+        fit_regression_kernel<<<grid, 32 * warps, smem, st>>>(ix->thr.as<float>() + u_begin * S, nu, S,
+                                                              ix->reg.as<float>() + u_begin * 8);
     });
     RKR_CUDA(cudaGetLastError());
     return RKR_OK;
@@ -259,7 +262,8 @@ extern "C" int rkr_index_fit_regression(rkr_index *ix, float *records_out) {
                 ix->n_sample, rkr::kFitMaxS);
     RKR_TRY(rkr::ensure_device(ix));
     const int S = ix->n_sample;
-    RKR_TRY(rkr::fit_regression_device(ix, ix->stream));
+    RKR_TRY(ix->reg.ensure(sizeof(float) * 8 * (size_t) ix->n_user));
+    RKR_TRY(rkr::fit_regression_device(ix, 0, ix->n_user, ix->stream));
     RKR_TRY(ix->reg_rank.ensure(sizeof(int32_t) * S));
     RKR_CUDA(cudaMemcpyAsync(ix->reg_rank.p, ix->h_sample_rank.data(), sizeof(int32_t) * S, cudaMemcpyHostToDevice,
                              ix->stream));

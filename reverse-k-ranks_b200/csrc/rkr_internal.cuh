@@ -1266,6 +1266,13 @@ int refine_tc(rkr_index *ix, const RefineArgs &ra, cudaStream_t st, bool *done);
 // Builds (once per split) the item tiles refine_tc reads.
 int refine_tc_tiles(rkr_index *ix, bool ipbound, cudaStream_t st);
 int thr_summary_build(rkr_index *ix);
+// Regression models of users [u_begin, u_end) fitted on the device into ix->reg (rkr_fit.cu).
+int fit_regression_device(rkr_index *ix, int64_t u_begin, int64_t u_end, cudaStream_t st);
+// The SVD transform built on the device over all users and made the index's (rkr_svd.cu).
+int svd_build_device(rkr_index *ix, float sigma_ratio, float *transfer_item_out, float *svd_user_out,
+                     int32_t *check_dim_out);
+// Thresholds of users [u_begin, u_end) for the index's sample ranks into ix->thr (rkr_build.cu).
+int build_thresholds_range(rkr_index *ix, int64_t u_begin, int64_t u_end);
 int level_tables_build(rkr_index *ix);
 int refine_prepare_norms(rkr_index *ix);
 // What a batch of queries asks for: top-k `topk` for every query (k null; outputs [n_query][topk]),

@@ -70,13 +70,10 @@ __global__ void __launch_bounds__(256) project_kernel(const float *__restrict__ 
 }  // namespace
 }  // namespace rkr
 
-using namespace rkr;
+namespace rkr {
 
-extern "C" int rkr_index_svd_build(rkr_index *ix, float sigma_ratio, float *transfer_item_out, float *svd_user_out,
-                                   int32_t *check_dim_out) {
-    RKR_REQUIRE(ix, "null index");
-    RKR_REQUIRE(sigma_ratio > 0.0f && sigma_ratio <= 1.0f, "sigma_ratio %g outside (0, 1]", (double) sigma_ratio);
-    RKR_TRY(ensure_device(ix));
+int svd_build_device(rkr_index *ix, float sigma_ratio, float *transfer_item_out, float *svd_user_out,
+                     int32_t *check_dim_out) {
     const int d = ix->dim;
     const int64_t U = ix->n_user;
     cudaStream_t st = ix->stream;
@@ -132,4 +129,14 @@ extern "C" int rkr_index_svd_build(rkr_index *ix, float sigma_ratio, float *tran
     if (check_dim_out) *check_dim_out = check_dim;
     RKR_CUDA(cudaStreamSynchronize(st));
     return RKR_OK;
+}
+
+}  // namespace rkr
+
+extern "C" int rkr_index_svd_build(rkr_index *ix, float sigma_ratio, float *transfer_item_out, float *svd_user_out,
+                                   int32_t *check_dim_out) {
+    RKR_REQUIRE(ix, "null index");
+    RKR_REQUIRE(sigma_ratio > 0.0f && sigma_ratio <= 1.0f, "sigma_ratio %g outside (0, 1]", (double) sigma_ratio);
+    RKR_TRY(rkr::ensure_device(ix));
+    return rkr::svd_build_device(ix, sigma_ratio, transfer_item_out, svd_user_out, check_dim_out);
 }

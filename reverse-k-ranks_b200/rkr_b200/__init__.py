@@ -45,7 +45,8 @@ EXPORTS = [
     "rkr_file_read_svd", "rkr_file_write_svd", "rkr_file_write_query_distribution",
     "rkr_file_read_query_distribution", "rkr_index_load_files", "rkr_index_set_shard", "rkr_shard_query",
     "rkr_shard_merge", "rkr_host_exchange_create", "rkr_host_exchange", "rkr_host_exchange_destroy",
-    "rkr_index_fit_regression", "rkr_index_svd_build", "rkr_file_write_score_table",
+    "rkr_index_fit_regression", "rkr_index_svd_build", "rkr_file_write_score_table", "rkr_index_insert_users",
+    "rkr_index_delete_users", "rkr_index_svd_read",
 ]
 
 # rkr_exchange_fn (include/rkr.h): int (*)(void *ctx, int32_t *counts, int64_t n, void *stream)
@@ -413,6 +414,28 @@ class Index:
         cnt = np.zeros(max(k, 1), np.int64)
         _check(_lib.rkr_profile_read(self._h, C.c_int32(k), names, _p(ms), _p(cnt), C.byref(n)))
         return {names.raw[64 * i:64 * i + 64].split(b"\0")[0].decode(): (float(ms[i]), int(cnt[i])) for i in range(k)}
+
+    def svd_read(self):
+        """rkr_index_svd_read: (transfer_item, svd_user, check_dim) of the index's SVD transform."""
+        ti = np.empty((self.dim, self.dim), np.float32)
+        su = np.empty((self.n_user, self.dim), np.float32)
+        cd = C.c_int32()
+        _check(_lib.rkr_index_svd_read(self._h, _p(ti), _p(su), C.byref(cd)))
+        return ti, su, cd.value
+
+    def insert_users(self, user, sigma=0.7):
+        """rkr_index_insert_users: append normalised users (thresholds, models, SVD rebuilt on the device)."""
+        u = _f32(user)
+        if u.ndim != 2 or u.shape[1] != self.dim:
+            raise ValueError("users must be [n][dim]")
+        _check(_lib.rkr_index_insert_users(self._h, _p(u), C.c_int64(u.shape[0]), C.c_float(sigma)))
+        self.n_user += u.shape[0]
+
+    def delete_users(self, ids):
+        """rkr_index_delete_users: remove users by id (the rest close up in order)."""
+        d = np.ascontiguousarray(ids, dtype=np.int64)
+        _check(_lib.rkr_index_delete_users(self._h, _p(d), C.c_int64(d.shape[0])))
+        self.n_user -= d.shape[0]
 
     def write_score_table(self, path, n_user_out=None):
         """rkr_file_write_score_table: bstb's disk score table (descending rows, no header)."""

@@ -418,17 +418,55 @@ __device__ __forceinline__ int value_bin_g(float x, float mn, float scale) {
 // flight per thread, so that one CTA per SM keeps enough of the row in flight.
 template <class F>
 __device__ __forceinline__ void stream_row(const float *__restrict__ src, int n, F f) {
+    // 16-byte loads, four in flight per thread before their values are visited
     const float4 *s4 = reinterpret_cast<const float4 *>(src);
     const int n4 = n >> 2;
-#pragma unroll 4
-    for (int i = threadIdx.x; i < n4; i += blockDim.x) {
-        const float4 v = __ldg(s4 + i);
-        f(v.x);
-        f(v.y);
-        f(v.z);
-        f(v.w);
+    for (int i0 = threadIdx.x; i0 < n4; i0 += 4 * blockDim.x) {
+        float4 v[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int i = i0 + k * blockDim.x;
+            if (i < n4) v[k] = __ldg(s4 + i);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            if (i0 + k * blockDim.x < n4) {
+                f(v[k].x);
+                f(v[k].y);
+                f(v[k].z);
+                f(v[k].w);
+            }
+        }
     }
     for (int i = (n4 << 2) + threadIdx.x; i < n; i += blockDim.x) f(__ldg(src + i));
+}
+
+// Exclusive scan of v(b) over the kGBins bins, kGBins / blockDim.x consecutive bins per thread:
+// out(b, offset) for every bin; returns the total in every thread.  Called by the whole block.
+template <class V, class O>
+__device__ __forceinline__ int bins_excl_scan(V v, O out, int *warp_tot) {
+    constexpr int per = kGBins / kSelThreads;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int loc[per];
+    int s = 0;
+#pragma unroll
+    for (int t = 0; t < per; t++) { loc[t] = s; s += v(threadIdx.x * per + t); }
+    int incl = s;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int x = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += x;
+    }
+    __syncthreads();  // warp_tot free
+    if (lane == 31) warp_tot[w] = incl;
+    __syncthreads();
+    int total = 0;
+    for (int i = 0; i < nw; i++) total += warp_tot[i];
+    int before = 0;
+    for (int i = 0; i < w; i++) before += warp_tot[i];
+    const int base = before + incl - s;
+#pragma unroll
+    for (int t = 0; t < per; t++) out(threadIdx.x * per + t, base + loc[t]);
+    return total;
 }
 
 // The bin holding ascending position p: the last bin whose start is <= p.
@@ -537,11 +575,22 @@ __global__ void __launch_bounds__(kSelThreads) row_select_global_kernel(SelectAr
             __syncthreads();
             continue;
         }
-        // rounds over the requested bins in bin order, each staging what fits
+        // The requested bins' staging cursors from a block-wide scan of their sizes: when they fit the
+        // buffer together (nearly always) that is the only round; otherwise rounds over the requested
+        // bins in bin order, each staging what fits, planned bin by bin.
+        const int req_total = bins_excl_scan(
+            [&](int b) { return requested(b) ? start[b + 1] - start[b] : 0; },
+            [&](int b, int off) { if (requested(b)) hist[b] = off; }, warp_tot);
+        const bool one_round = req_total <= kGStage;
         if (threadIdx.x == 0) round_hi = 0;
         __syncthreads();
         while (true) {
-            if (threadIdx.x == 0) {
+            if (one_round) {
+                if (threadIdx.x == 0) {
+                    round_lo = round_hi == 0 ? 0 : kGBins;
+                    round_hi = kGBins;
+                }
+            } else if (threadIdx.x == 0) {
                 int b = round_hi;
                 while (b < kGBins && !requested(b)) b++;
                 round_lo = b;
@@ -592,12 +641,42 @@ __global__ void __launch_bounds__(kSelThreads) row_select_global_kernel(SelectAr
     }
 }
 
-__global__ void prefix_rows_kernel(int32_t *__restrict__ h, int rows, int64_t len) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+// Inclusive prefix sums of each row of h ([rows][len]), one block per row: each thread sums its own
+// contiguous segment, the block scans the segment sums, and each thread rewrites its segment from its
+// starting offset.
+constexpr int kPrefixThreads = 1024;
+__global__ void __launch_bounds__(kPrefixThreads) prefix_rows_kernel(int32_t *__restrict__ h, int rows, int64_t len) {
+    __shared__ int32_t warp_tot[kPrefixThreads / 32];
+    const int r = blockIdx.x;
     if (r >= rows) return;
     int32_t *p = h + (int64_t) r * len;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int64_t per = (len + blockDim.x - 1) / blockDim.x;
+    const int64_t b = (int64_t) threadIdx.x * per, e = min(len, b + per);
     int32_t s = 0;
-    for (int64_t i = 0; i < len; i++) { s += p[i]; p[i] = s; }
+    for (int64_t i = b; i < e; i++) s += p[i];
+    int32_t incl = s;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    if (lane == 31) warp_tot[w] = incl;
+    __syncthreads();
+    if (w == 0) {
+        const int32_t v = lane < nw ? warp_tot[lane] : 0;
+        int32_t iv = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t x = __shfl_up_sync(0xffffffffu, iv, o);
+            if (lane >= o) iv += x;
+        }
+        if (lane < nw) warp_tot[lane] = iv - v;
+    }
+    __syncthreads();
+    int32_t run = warp_tot[w] + incl - s;  // the sum of every segment before this thread's
+    for (int64_t i = b; i < e; i++) {
+        run += p[i];
+        p[i] = run;
+    }
 }
 
 // ---- host side --------------------------------------------------------------------------------------
@@ -799,7 +878,9 @@ int query_rank_distribution(rkr_index *ix, const int32_t *sample_item, int n_sam
     }
     // user shards: every shard's counts
     RKR_TRY(shard_sum(ix, ix->ws_hist.as<int32_t>(), (int64_t) n_sample_item * (n + 1), ix->stream));
-    timed(ix, ix->stream, "prefix_rows", [&] { prefix_rows_kernel<<<(n_sample_item + 63) / 64, 64, 0, ix->stream>>>(ix->ws_hist.as<int32_t>(), n_sample_item, n + 1); });
+    timed(ix, ix->stream, "prefix_rows", [&] {
+        prefix_rows_kernel<<<n_sample_item, kPrefixThreads, 0, ix->stream>>>(ix->ws_hist.as<int32_t>(), n_sample_item, n + 1);
+    });
     RKR_CUDA(cudaGetLastError());
     RKR_CUDA(cudaMemcpyAsync(h_accu, ix->ws_hist.p, sizeof(int32_t) * (size_t) n_sample_item * (n + 1),
                              cudaMemcpyDeviceToHost, ix->stream));

@@ -145,7 +145,8 @@ def test_build_rows_larger_than_shared_memory_match_oracle(n_item):
 def test_query_rank_distribution_with_equal_scores_matches_oracle(n_item):
     """Items drawn from 50 distinct vectors (every score repeated), rows of both lengths (shared-memory
     and longer), an item count that is not a multiple of four: the counting of items strictly above
-    each sampled item's score against the oracle."""
+    each sampled item's score, and the thresholds (requested bins far larger than the staging buffer),
+    against the oracle."""
     n_user, d = 300, 16
     rng = np.random.default_rng(n_item + 7)
     orc = Oracle()
@@ -153,7 +154,10 @@ def test_query_rank_distribution_with_equal_scores_matches_oracle(n_item):
     base = rng.standard_normal((50, d)).astype(np.float32)
     item = base[rng.integers(0, 50, n_item)]
     si = R.sample_item(n_item, 150)
+    rank = np.unique(np.concatenate([np.arange(0, 40), np.linspace(40, n_item - 2, 200).astype(int)])).astype(np.int32)
     with R.Index(user, item) as ix:
         accu = ix.query_rank_distribution(si)
+        thr = ix.build_sample_search(rank)
     _, accu_o = orc.query_rank_distribution(user, item, si)
     assert np.array_equal(accu, accu_o)
+    assert same(thr, orc.build_thresholds(user, item, rank))

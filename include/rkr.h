@@ -198,7 +198,8 @@ int rkr_server_destroy(rkr_server *server);
  * them; a smaller one only reports the count); names is [max_kernels][64] chars.  Entries whose
  * name ends in "_pairs", "_queries" or "_rows" are counters rather than kernels (time 0, `launches` holds
  * the count): two_pass_compaction_queries counts the queries whose flagged users outgrew the sparse
- * compaction's list and took the two-pass form;
+ * compaction's list and took the two-pass form (two_pass_need_to_2x_queries, _to_4x_, _to_16x_ and
+_beyond_ count them by how far their flagged users exceed the list);
  * screen_undecided_pairs counts the (query, user) pairs whose regression levels or threshold group
  * the screens (tensor-core scores with an error bound, the fast binary32 CDF) left to the
  * reference's own arithmetic; rescored_pairs the pairs whose score a later pass recomputed (a fine

@@ -844,7 +844,8 @@ __global__ void __launch_bounds__(kCompactThreads) compact_write_kernel(P p, int
 // the list by user id and runs the ordered classification and emission of compact_write_kernel on
 // it.  A query whose list outgrows kNeedCap is listed and takes the two-pass form above.
 
-constexpr int kNeedCap = 4096;     // flagged users per query on the sparse path
+constexpr int kNeedBits = 12;               // bits of a list position in the sort keys
+constexpr int kNeedCap = 1 << kNeedBits;    // flagged users per query on the sparse path
 
 // The flagged users' lists from one flat pass over the batch's codes ([query][user] as one array): 512 bytes
 // per warp and step in aligned 16-byte loads, the next step's load in flight while a step is
@@ -937,7 +938,8 @@ __global__ void __launch_bounds__(kCompactThreads) compact_emit_kernel(P p, KSpe
                                                                      const typename P::Aux *__restrict__ aux_l,
                                                                      QueryCounts *__restrict__ counts, int *__restrict__ err,
                                                                      int32_t *__restrict__ ovf_q) {
-    __shared__ uint64_t s[kNeedCap];  // user id << 12 | list position
+    extern __shared__ __align__(16) unsigned char emit_smem[];
+    uint64_t *s = reinterpret_cast<uint64_t *>(emit_smem);  // [kNeedCap]: user id << kNeedBits | list position
     __shared__ int warp_tot[9];
     const int q = blockIdx.x, tid = threadIdx.x;
     const int n = need_n[q], topk = ks.of(q);
@@ -949,7 +951,7 @@ __global__ void __launch_bounds__(kCompactThreads) compact_emit_kernel(P p, KSpe
     while (pn < n) pn <<= 1;
     const int64_t row = (int64_t) q * kNeedCap;
     for (int i = tid; i < pn; i += kCompactThreads)
-        s[i] = i < n ? ((uint64_t) (uint32_t) need_u[row + i] << 12) | (uint64_t) i : ~uint64_t(0);
+        s[i] = i < n ? ((uint64_t) (uint32_t) need_u[row + i] << kNeedBits) | (uint64_t) i : ~uint64_t(0);
     __syncthreads();
     // bitonic sort, ascending user id
     for (int k = 2; k <= pn; k <<= 1)
@@ -972,8 +974,8 @@ __global__ void __launch_bounds__(kCompactThreads) compact_emit_kernel(P p, KSpe
         int k = 0;
         int64_t u = 0, at = 0;
         if (i < n) {
-            u = (int64_t) (s[i] >> 12);
-            at = row + (int64_t) (s[i] & 0xfff);
+            u = (int64_t) (s[i] >> kNeedBits);
+            at = row + (int64_t) (s[i] & (kNeedCap - 1));
             k = cls[at];
         }
         int tot;
@@ -1173,7 +1175,7 @@ inline int run_compaction(rkr_index *ix, P p, int nq, KSpec ks, QueryCounts *cou
         });
         RKR_CUDA(cudaGetLastError());
         timed(ix, st, "compact_emit", [&] {
-            compact_emit_kernel<P><<<(unsigned) nq, kCompactThreads, 0, st>>>(p, ks, need_n, need_u, cls, aux, counts,
+            compact_emit_kernel<P><<<(unsigned) nq, kCompactThreads, sizeof(uint64_t) * kNeedCap, st>>>(p, ks, need_n, need_u, cls, aux, counts,
                                                                              err, ovf_q);
         });
         RKR_CUDA(cudaGetLastError());
@@ -1181,6 +1183,23 @@ inline int run_compaction(rkr_index *ix, P p, int nq, KSpec ks, QueryCounts *cou
         RKR_CUDA(cudaStreamSynchronize(st));
         n_two = h_err[1];
         qmap = ovf_q;
+        if (ix->prof.on && n_two) {
+            // how far past the list the two-pass queries' flagged users go
+            std::vector<int32_t> nn((size_t) nq);
+            RKR_CUDA(cudaMemcpy(nn.data(), need_n, sizeof(int32_t) * nq, cudaMemcpyDeviceToHost));
+            int64_t le8 = 0, le16 = 0, le64 = 0, more = 0;
+            for (int32_t v : nn) {
+                if (v <= kNeedCap) continue;
+                if (v <= 2 * kNeedCap) le8++;
+                else if (v <= 4 * kNeedCap) le16++;
+                else if (v <= 16 * kNeedCap) le64++;
+                else more++;
+            }
+            ix->prof.add_count("two_pass_need_to_2x_queries", le8);
+            ix->prof.add_count("two_pass_need_to_4x_queries", le16);
+            ix->prof.add_count("two_pass_need_to_16x_queries", le64);
+            ix->prof.add_count("two_pass_need_beyond_queries", more);
+        }
     }
     if (n_two) {
         const dim3 g2((unsigned) nchunks, (unsigned) n_two);

@@ -519,6 +519,90 @@ def serve_summary(arrivals, start, end, sizes, rate):
                            "mean": float(svc.mean())}}
 
 
+def run_sharded(args, R, user_raw, item, qrng, dist, world, rank_id, local, batch, topk):
+    """User shards (rkr_index_set_shard): rank r builds and holds its user range, the selection counts
+    are summed over the ranks through NCCL on the engine's stream (rkr_b200.shard.TorchExchange), and
+    every query's parts are gathered and merged on every rank.  Every rank draws the same queries.  The
+    timed step is one batch end to end: host queries in, each rank's shard query, the gather of the
+    parts and the merge (the whole answer on every rank)."""
+    import socket
+    import torch
+    import torch.distributed as tdist
+    from rkr_b200.shard import TorchExchange, shard_users
+    own_group = dist is None
+    if own_group:  # one rank: a one-member NCCL group, so that the exchange still runs through NCCL
+        import datetime
+        with socket.socket() as so:
+            so.bind(("127.0.0.1", 0))
+            port = so.getsockname()[1]
+        store = tdist.TCPStore("127.0.0.1", port, 1, True, timeout=datetime.timedelta(seconds=60))
+        tdist.init_process_group("nccl", store=store, rank=0, world_size=1, timeout=datetime.timedelta(seconds=120))
+    n_user, n_item, dim, n_sample, n_si, stopk = CONFIGS[args.config][:6]
+    start, end = shard_users(n_user, world, rank_id)
+    t0 = time.perf_counter()
+    user_all = R.normalize(user_raw)
+    ix = R.Index(user_all[start:end], item, device=local)
+    ex = TorchExchange(None, torch.device("cuda", local))
+    ix.set_shard(rank_id, world, start, n_user, (ex.fn, None))
+    si = R.sample_item(n_item, n_si)
+    accu = ix.query_rank_distribution(si)  # every shard's users (summed through the exchange)
+    kth, sid = R.sort_kth_rank(accu, stopk)
+    rank, _ = R.find_optimal_sample_rank(n_user, n_item, n_sample, kth, accu[sid])
+    ix.build_sample_search(rank, return_thresholds=False)
+    ix.fit_regression(records=False)
+    ti, su, cd = R.svd_build(user_all, 0.7)  # the same transform on every rank (host, all users)
+    ix.load_svd(cd, ti, su[start:end])
+    torch.cuda.synchronize()
+    build_sec = time.perf_counter() - t0
+    ks = np.full(batch, topk, np.int32)
+    batches = [item[qrng.choice(n_item, size=batch, replace=False)].copy() for _ in range(args.warmup + args.steps)]
+
+    def step(q):
+        part, front, st = ix.shard_query(args.method, q, ks, stats=True)
+        if dist is None:
+            return R.shard_merge(ks, [part], [front], [st])
+        got = [None] * world
+        dist.all_gather_object(got, (part, front, st))
+        return R.shard_merge(ks, [g[0] for g in got], [g[1] for g in got], [g[2] for g in got])
+
+    stream = torch.cuda.current_stream()
+    with Clocks(local) as clk:
+        time.sleep(0.5)
+        for s in range(args.warmup):
+            step(batches[s])
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        wall0 = time.perf_counter()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for s in range(args.steps):
+            out, mst = step(batches[args.warmup + s])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clk.mark(wall0, time.perf_counter())
+    total_ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
+    value = batch * args.steps / (total_ms / 1e3)  # the same queries on every rank: the job answers them once
+    if rank_id == 0:
+        line = {"metric": "queries/sec at exact ranks over user shards (k=%d)" % topk, "value": value,
+                "unit": "queries/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded numpy), the workload's shapes",
+                "config": {"workload": f"{args.config}: {n_user} users x {n_item} items, d={dim}, {n_sample} sampled "
+                                       f"thresholds/user, {args.method}, {batch} queries/step, k={topk}; user shards",
+                           "shard_users": [end - start], "parallelism": f"user shards x{world}",
+                           "l2": "inputs larger than L2 (resident index >= 1.6 GB)" if args.config != "config1"
+                           else "small"},
+                "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": batch * dim * 4,
+                        "d2h_bytes_per_step": int(out.nbytes)},
+                "build_sec": build_sec, "clocks": clk.summary()}
+        print(json.dumps(line))
+    ix.close()
+    if own_group:
+        tdist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -531,6 +615,9 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--single-queries", type=int, default=100)
     ap.add_argument("--batch", type=int, default=0, help="queries per step (default: the workload's)")
+    ap.add_argument("--shard-users", action="store_true",
+                    help="user shards instead of replicas: rank r holds users [r U/N, (r+1) U/N), every rank "
+                         "answers the same queries for its users, the parts are merged (strong scaling)")
     ap.add_argument("--n-user", type=int, default=0,
                     help="users of the workload (default: the configuration's); smaller for profiler captures")
     ap.add_argument("--serve-requests", type=int, default=200, help="config5: requests per trace")
@@ -567,7 +654,12 @@ def main():
 
     import rkr_b200 as R
     log(f"[bench] rank {rank_id}/{world}: generating {args.config} data")
-    user_raw, item, qrng = make_data(args.config, args.seed, rank_id)
+    user_raw, item, qrng = make_data(args.config, args.seed, 0 if args.shard_users else rank_id)
+    if args.shard_users:
+        run_sharded(args, R, user_raw, item, qrng, dist, world, rank_id, local, batch, topk)
+        if dist:
+            dist.destroy_process_group()
+        return
     t0 = time.perf_counter()
     ix, parts, stages = build_index(R, user_raw, item, args.config, local)
     torch.cuda.synchronize()

@@ -41,6 +41,7 @@ class TorchExchange:
         self.group = group
         self.device = torch.device(device) if device is not None else None
         self.fn = exchange_callback(self)  # EXCHANGE_FN; kept alive with this object
+        self._views = {}  # (address, n, stream) -> (stream object, tensor view): the engine reuses its buffers
 
     def __call__(self, address, n, stream):
         if n <= 0:
@@ -48,10 +49,16 @@ class TorchExchange:
         if stream:
             # device counts, ordered on the engine's stream: NCCL waits for the work queued there and
             # the stream waits for the sum
-            s = torch.cuda.ExternalStream(stream, device=self.device)
-            with torch.cuda.stream(s):
-                t = torch.as_tensor(_DeviceInts(address, n), device=self.device)
-                dist.all_reduce(t, op=dist.ReduceOp.SUM, group=self.group)
+            key = (address, n, stream)
+            view = self._views.get(key)
+            if view is None:
+                if len(self._views) > 256:
+                    self._views.clear()
+                s = torch.cuda.ExternalStream(stream, device=self.device)
+                view = (s, torch.as_tensor(_DeviceInts(address, n), device=self.device))
+                self._views[key] = view
+            with torch.cuda.stream(view[0]):
+                dist.all_reduce(view[1], op=dist.ReduceOp.SUM, group=self.group)
         else:
             a = np.ctypeslib.as_array((C.c_int32 * n).from_address(address))
             t = torch.from_numpy(a)

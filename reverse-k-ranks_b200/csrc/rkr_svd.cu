@@ -16,10 +16,11 @@ namespace {
 constexpr int kGramUsers = 4096;  // users per block of the Gram pass
 
 // One 32 x 32 tile (rows p0.., columns q0.., p0 <= q0) of the Gram matrix over one chunk of users:
-// 32 users' two column slices staged in shared memory as doubles, four outputs per thread, the
-// chunk's sums added to G.
+// 32 users' two column slices staged in shared memory as doubles, four outputs per thread; the
+// chunk's sums go to its own slice of `part` ([chunk][d][d]), summed in chunk order afterwards, so
+// the matrix is the same on every run.
 __global__ void __launch_bounds__(256) gram_kernel(const float *__restrict__ user, int64_t n_user, int d,
-                                                   const int2 *__restrict__ tiles, double *__restrict__ G) {
+                                                   const int2 *__restrict__ tiles, double *__restrict__ part) {
     __shared__ double sp[32][33], sq[32][33];
     const int2 tl = tiles[blockIdx.x];
     const int p0 = tl.x * 32, q0 = tl.y * 32;
@@ -45,8 +46,19 @@ __global__ void __launch_bounds__(256) gram_kernel(const float *__restrict__ use
 #pragma unroll
     for (int m = 0; m < 4; m++) {
         const int p = p0 + ty + 8 * m, q = q0 + tx;
-        if (p < d && q < d && p <= q) atomicAdd(G + (size_t) p * d + q, acc[m]);
+        if (p < d && q < d && p <= q) part[(size_t) blockIdx.y * d * d + (size_t) p * d + q] = acc[m];
     }
+}
+
+// G[e] = the chunks' partial sums of entry e added in chunk order (upper triangle).
+__global__ void gram_sum_kernel(const double *__restrict__ part, int n_chunks, int d, double *__restrict__ G) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= d * d) return;
+    const int p = e / d, q = e % d;
+    if (p > q) return;
+    double s = 0.0;
+    for (int c = 0; c < n_chunks; c++) s += part[(size_t) c * d * d + e];
+    G[e] = s;
 }
 
 // svd_user[u][k] = user[u] . Es[:, k] / s[k] (0 where s[k] is 0), summed over the coordinates in
@@ -87,12 +99,16 @@ int svd_build_device(rkr_index *ix, float sigma_ratio, float *transfer_item_out,
         ~Scratch() { for (auto &x : b) x.release(); }
     } scratch;
     DevBuf &g = scratch.b[0], &tl = scratch.b[1], &es = scratch.b[2], &sv = scratch.b[3];
-    RKR_TRY(g.ensure(sizeof(double) * (size_t) d * d));
+    const int n_chunks = (int) ((U + kGramUsers - 1) / kGramUsers);
+    RKR_TRY(g.ensure(sizeof(double) * (size_t) d * d * (size_t) (n_chunks + 1)));
+    double *part = g.as<double>() + (size_t) d * d;  // [n_chunks][d][d]; the sums at the front
     RKR_TRY(tl.ensure(sizeof(int2) * tiles.size()));
     RKR_CUDA(cudaMemsetAsync(g.p, 0, sizeof(double) * (size_t) d * d, st));
     RKR_CUDA(cudaMemcpyAsync(tl.p, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice, st));
-    const dim3 gg((unsigned) tiles.size(), (unsigned) ((U + kGramUsers - 1) / kGramUsers));
-    timed(ix, st, "svd_gram", [&] { gram_kernel<<<gg, 256, 0, st>>>(ix->user.as<float>(), U, d, tl.as<int2>(), g.as<double>()); });
+    const dim3 gg((unsigned) tiles.size(), (unsigned) n_chunks);
+    timed(ix, st, "svd_gram", [&] { gram_kernel<<<gg, 256, 0, st>>>(ix->user.as<float>(), U, d, tl.as<int2>(), part); });
+    RKR_CUDA(cudaGetLastError());
+    gram_sum_kernel<<<(unsigned) ((d * d + 255) / 256), 256, 0, st>>>(part, n_chunks, d, g.as<double>());
     RKR_CUDA(cudaGetLastError());
     std::vector<double> G((size_t) d * d);
     RKR_CUDA(cudaMemcpyAsync(G.data(), g.p, sizeof(double) * G.size(), cudaMemcpyDeviceToHost, st));

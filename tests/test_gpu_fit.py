@@ -91,6 +91,9 @@ def test_device_svd_is_the_host_transform_to_rounding(case):
         ix.load_regression(g["opt_rank"], g["reg"])
         k = 10
         out = ix.retrieval("QSRPNormalLP", g["query"], k)
+    with R.Index(un, g["item"]) as ix2:  # the same transform on every run
+        ti2, su2, cd2 = ix2.svd_build(0.7)
+    assert np.array_equal(bits(ti2), bits(ti)) and np.array_equal(bits(su2), bits(su)) and cd2 == cd
     hti, hsu, hcd = R.svd_build(un, 0.7)
     assert cd == hcd
     q = g["query"][:8].astype(np.float64)

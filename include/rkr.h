@@ -289,7 +289,7 @@ int rkr_svd_build(const float *user, int64_t n_user, int32_t dim, float sigma, f
  * (host [n_user][dim]) and check_dim_out may be NULL.  A valid transform like rkr_svd_build's (the
  * Gram matrix's sums run in another order, so the two agree to rounding, not bit for bit); the same
  * users give the same transform on every run (the Gram matrix's partial sums are added in a fixed
- * order). */
+ * order).  A user shard is RKR_ERR_STATE: its transform must be every shard's. */
 int rkr_index_svd_build(rkr_index *index, float sigma, float *transfer_item_out, float *svd_user_out,
                         int32_t *check_dim_out);
 

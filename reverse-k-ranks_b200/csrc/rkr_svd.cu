@@ -153,6 +153,12 @@ extern "C" int rkr_index_svd_build(rkr_index *ix, float sigma_ratio, float *tran
                                    int32_t *check_dim_out) {
     RKR_REQUIRE(ix, "null index");
     RKR_REQUIRE(sigma_ratio > 0.0f && sigma_ratio <= 1.0f, "sigma_ratio %g outside (0, 1]", (double) sigma_ratio);
+    if (ix->sharded()) {
+        // every shard needs the same transform, built over every user
+        ::rkr::set_error("rkr_index_svd_build: the index is a user shard (build the transform over all users, "
+                         "rkr_svd_build, and load each shard's rows)");
+        return RKR_ERR_STATE;
+    }
     RKR_TRY(rkr::ensure_device(ix));
     return rkr::svd_build_device(ix, sigma_ratio, transfer_item_out, svd_user_out, check_dim_out);
 }

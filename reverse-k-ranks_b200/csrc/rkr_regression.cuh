@@ -208,6 +208,43 @@ __device__ __forceinline__ bool lvt_screen(const float2 *t, int stride, float q,
     return ok;
 }
 
+// The same decision from a row of limits (lo_g, hi_g): lo_g at or below T_g - band_g and hi_g at or
+// above T_g + band_g, lo non-increasing and hi non-increasing in g (lvt_limits_row), with qm at or
+// below q - dq and qp at or above q + dq.  c = #{g : qp < lo_g} (a prefix of the entries, lo being
+// monotone), decided when (c == kLvEntries - 1 or qm >= hi_c) and (c == 0 or qp < lo_(c-1)): every
+// score s within dq of q then lies above the band of boundary c and below that of boundary c - 1.
+__device__ __forceinline__ bool lvt_screen_lim(const float2 *t, int stride, float qm, float qp, int &c) {
+    int k = 0;
+#pragma unroll
+    for (int st = 8; st >= 1; st >>= 1) k += qp < t[(k + st - 1) * stride].x ? st : 0;
+    c = k;
+    bool ok = k == kLvEntries - 1 || qm >= t[k * stride].y;
+    if (k > 0) ok = ok && qp < t[(k - 1) * stride].x;
+    return ok;
+}
+
+// One user's table row (entry j at t[j * stride], entries (T_j, band_j)) in place as limits: lo_j =
+// T_j - band_j rounded down, then the running minimum from entry 0; hi_j = T_j + band_j rounded up,
+// then the running maximum from the last entry.  Each limit only moves away from its boundary, so a
+// decision lvt_screen_lim makes from them is one the bands allow.  A row with a NaN stays all NaN.
+__device__ __forceinline__ void lvt_limits_row(float2 *t, int stride) {
+    bool bad = false;
+    float lo = INFINITY;
+    for (int j = 0; j < kLvEntries; j++) {
+        const float2 e = t[j * stride];
+        bad = bad || !(e.x == e.x) || !(e.y == e.y);
+        lo = fminf(lo, __fsub_rd(e.x, e.y));
+        t[j * stride] = make_float2(lo, __fadd_ru(e.x, e.y));
+    }
+    float hi = -INFINITY;
+    for (int j = kLvEntries - 1; j >= 0; j--) {
+        hi = fmaxf(hi, t[j * stride].y);
+        t[j * stride].y = hi;
+    }
+    if (bad)
+        for (int j = 0; j < kLvEntries; j++) t[j * stride] = make_float2(NAN, NAN);
+}
+
 __device__ __forceinline__ int level_rank(int lvl, const int32_t *rank, int S, int n_item) {
     return lvl == 0 ? 0 : (lvl > S ? n_item : rank[lvl - 1]);
 }

@@ -47,6 +47,7 @@ constexpr int kScThreads = 32 * (kScEpiWarps + 1);
 constexpr int kScListCap = 1024;                   // undecided pairs per CTA resolved in the kernel
 constexpr int kScMaxQ = 1024;                      // queries per launch (their data sits in shared memory)
 constexpr int kScMaxKp = 224;                      // padded coordinates (both parts): shared memory
+constexpr int kUpCache = 10;  // upper-side lower limits held in registers (< kLvEntries - 1)
 constexpr int kScSummStride = kScM;  // summary transposed: entry j of row r at j * kScM + r (lanes hit distinct banks)
 
 // ---- the tile kernel -----------------------------------------------------------------------------------
@@ -206,6 +207,12 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
         sq[i] = __ldg(a.qmeta + min(i, nq - 1));
         sqn[i] = lev ? __ldg(a.qnorm + min(i, nq - 1)) : 0.0f;
     }
+    if (lev) {
+        // the level tables as monotone limits (lvt_limits_row): one thread per user and side
+        __syncthreads();
+        for (int idx = tid; idx < 2 * kScM; idx += kScThreads)
+            lvt_limits_row(stab + (idx & 1) * kLvEntries * kScM + (idx >> 1), kScM);
+    }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -290,14 +297,16 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
         const float2 *tl = stab + row, *tu = stab + kLvEntries * kScM + row;  // entry j at t[j * kScM]
         float un = 0.0f;
         float4 um = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        // the lower side's common cases in registers, as (T - band, T + band) rounded outward: its last
-        // three boundaries T_12 .. T_14 (coarse levels 13 .. 15 hold all but about 0.1% of its pairs at
-        // configs 2 and 4), so that those pairs need no table search.  The upper side's coarse levels
-        // spread over more boundaries (at config 4 nearly every warp holds a pair beyond T_3), so every
-        // pair takes its table search, without branches
-        float llo[3], lhi[3];
+        // the common cases in registers, from the tables' limits (lvt_limits_row): the lower side's
+        // last three boundaries T_12 .. T_14 (coarse levels 13 .. 15 hold all but about 0.1% of its
+        // pairs at configs 2 and 4), the upper side's first kUpCache lower limits (its coarse levels
+        // 0 .. kUpCache - 1 hold all but about 0.01% of its pairs at config 2), so that only the rare
+        // pairs beyond them take a table search
+        float llo[3], lhi[3], ulo[kUpCache];
 #pragma unroll
         for (int g = 0; g < 3; g++) { llo[g] = -INFINITY; lhi[g] = INFINITY; }
+#pragma unroll
+        for (int g = 0; g < kUpCache; g++) ulo[g] = NAN;
         if (uval) {
             um = __ldg(a.umeta + u);
             if (lev) {
@@ -306,10 +315,12 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
 #pragma unroll
                 for (int g = 0; g < 3; g++) {
                     const float2 e = tl[(kLvEntries - 4 + g) * kScM];
-                    llo[g] = __fsub_rd(e.x, e.y);
-                    lhi[g] = __fadd_ru(e.x, e.y);
+                    llo[g] = e.x;
+                    lhi[g] = e.y;
                     if (!(llo[g] == llo[g]) || !(lhi[g] == lhi[g])) { llo[g] = -INFINITY; lhi[g] = INFINITY; }
                 }
+#pragma unroll
+                for (int g = 0; g < kUpCache; g++) ulo[g] = tu[g * kScM].x;
             }
         }
         // the first two steps of the group search from registers
@@ -386,10 +397,10 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                     if (lev) {
                         // coarse levels of the bounds partial -+ right (PartDimPartNorm::IPBound) from the
                         // tables; within dq of the reference's bound scores: the partial score's bound and
-                        // the two roundings of each side.  The lower side's cached boundaries decide most
-                        // pairs without branches, and its table search runs afterwards, for the whole
-                        // warp, where any lane's pair needs one; the upper side searches every pair
-                        unsigned needl = 0, needu = 0;
+                        // the two roundings of each side.  The cached limits decide most pairs without
+                        // branches; each side's table search runs afterwards, for the whole warp, where
+                        // any lane's pair needs one
+                        unsigned needl = 0, needu = 0, needx = 0;
 #pragma unroll
                         for (int g = 0; g < G; g++) {
                             float qlb, qub, dql, dqu;
@@ -404,12 +415,38 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                                 okl = b14 || (qml >= lhi[2] && b13) || (qml >= lhi[1] && b12);
                                 c_l = b14 ? 15 : (b13 ? 14 : 13);
                             }
-                            const bool oku = lvt_screen(tu, kScM, qub, dqu, c_u);
+                            // upper side: c_u = #{g : qp < lo_g} over the cached limits (a prefix, lo being
+                            // monotone), decided when qm >= hi_(c_u); a pair at the last cached limit may
+                            // lie beyond it and takes the table search
+                            bool oku;
+                            {
+                                const float qmu = __fsub_rd(qub, dqu), qpu = __fadd_ru(qub, dqu);
+                                c_u = 0;
+#pragma unroll
+                                for (int e = 0; e < kUpCache; e++) c_u += qpu < ulo[e] ? 1 : 0;
+                                oku = qmu >= tu[c_u * kScM].y;
+                                needx |= (unsigned) (!oku && c_u == kUpCache) << g;
+                            }
                             needl |= (unsigned) !okl << g;
                             needu |= (unsigned) !oku << g;
                             packed[g] = c_l | (c_u << 4);
                         }
-                        n_sup += G;
+                        if (__any_sync(0xffffffffu, needx != 0u)) {
+#pragma unroll
+                            for (int g = 0; g < G; g++) {
+                                const bool wx = (needx >> g) & 1u;
+                                if (!__any_sync(0xffffffffu, wx)) continue;
+                                n_sup++;
+                                float qlb, qub, dql, dqu;
+                                level_bounds(vl[g], dl[g], un, sqn[j * kScN + 8 * cg + i0 + g], qlb, qub, dql, dqu);
+                                int c;
+                                const bool o = lvt_screen_lim(tu, kScM, __fsub_rd(qub, dqu), __fadd_ru(qub, dqu), c);
+                                if (wx) {
+                                    packed[g] = (packed[g] & 0x0f) | (c << 4);
+                                    if (o) needu &= ~(1u << g);
+                                }
+                            }
+                        }
                         if (__any_sync(0xffffffffu, needl != 0u)) {
 #pragma unroll
                             for (int g = 0; g < G; g++) {
@@ -419,7 +456,7 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                                 float qlb, qub, dql, dqu;
                                 level_bounds(vl[g], dl[g], un, sqn[j * kScN + 8 * cg + i0 + g], qlb, qub, dql, dqu);
                                 int c;
-                                const bool o = lvt_screen(tl, kScM, qlb, dql, c);
+                                const bool o = lvt_screen_lim(tl, kScM, __fsub_rd(qlb, dql), __fadd_ru(qlb, dql), c);
                                 if (wl) {
                                     packed[g] = (packed[g] & 0xf0) | c;
                                     if (o) needl &= ~(1u << g);

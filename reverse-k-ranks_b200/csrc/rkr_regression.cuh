@@ -245,6 +245,24 @@ __device__ __forceinline__ void lvt_limits_row(float2 *t, int stride) {
         for (int j = 0; j < kLvEntries; j++) t[j * stride] = make_float2(NAN, NAN);
 }
 
+// A row of limits (lvt_limits_row) rewritten in place as verification pairs: entry c = (hi_c,
+// lo_(c-1)), lo_(-1) = +inf.  One entry then decides coarse level c (qm >= hi_c and qp < lo_(c-1)),
+// and lo_j is entry j + 1's second value.
+__device__ __forceinline__ void lvt_verify_row(float2 *t, int stride) {
+    for (int j = kLvEntries - 1; j >= 1; j--) t[j * stride] = make_float2(t[j * stride].y, t[(j - 1) * stride].x);
+    const float h0 = t[0].y;
+    t[0] = make_float2(h0, h0 == h0 ? INFINITY : NAN);
+}
+// lvt_screen_lim on a row of verification pairs.
+__device__ __forceinline__ bool lvt_screen_ver(const float2 *t, int stride, float qm, float qp, int &c) {
+    int k = 0;
+#pragma unroll
+    for (int st = 8; st >= 1; st >>= 1) k += qp < t[(k + st) * stride].y ? st : 0;
+    c = k;
+    const float2 e = t[k * stride];
+    return qm >= e.x && qp < e.y;
+}
+
 __device__ __forceinline__ int level_rank(int lvl, const int32_t *rank, int S, int n_item) {
     return lvl == 0 ? 0 : (lvl > S ? n_item : rank[lvl - 1]);
 }

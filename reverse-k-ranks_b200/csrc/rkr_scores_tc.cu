@@ -47,7 +47,8 @@ constexpr int kScThreads = 32 * (kScEpiWarps + 1);
 constexpr int kScListCap = 1024;                   // undecided pairs per CTA resolved in the kernel
 constexpr int kScMaxQ = 1024;                      // queries per launch (their data sits in shared memory)
 constexpr int kScMaxKp = 224;                      // padded coordinates (both parts): shared memory
-constexpr int kUpCache = 10;  // upper-side lower limits held in registers (< kLvEntries - 1)
+constexpr int kUpCache = 10;  // upper-side lower limits held in registers
+static_assert(kUpCache % 2 == 0 && kUpCache < kLvEntries - 1, "paired terms; the verification index stays a table entry");
 constexpr int kScSummStride = kScM;  // summary transposed: entry j of row r at j * kScM + r (lanes hit distinct banks)
 
 // ---- the tile kernel -----------------------------------------------------------------------------------
@@ -210,8 +211,11 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
     if (lev) {
         // the level tables as monotone limits (lvt_limits_row): one thread per user and side
         __syncthreads();
-        for (int idx = tid; idx < 2 * kScM; idx += kScThreads)
-            lvt_limits_row(stab + (idx & 1) * kLvEntries * kScM + (idx >> 1), kScM);
+        for (int idx = tid; idx < 2 * kScM; idx += kScThreads) {
+            float2 *t = stab + (idx & 1) * kLvEntries * kScM + (idx >> 1);
+            lvt_limits_row(t, kScM);
+            if (idx & 1) lvt_verify_row(t, kScM);  // the upper side: verification pairs
+        }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -299,9 +303,9 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
         float4 um = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         // the common cases in registers, from the tables' limits (lvt_limits_row): the lower side's
         // last three boundaries T_12 .. T_14 (coarse levels 13 .. 15 hold all but about 0.1% of its
-        // pairs at configs 2 and 4), the upper side's first kUpCache lower limits (its coarse levels
-        // 0 .. kUpCache - 1 hold all but about 0.01% of its pairs at config 2), so that only the rare
-        // pairs beyond them take a table search
+        // pairs at configs 2 and 4), the upper side's first kUpCache lower limits, scaled by 2^100
+        // (its coarse levels 0 .. kUpCache - 1 hold all but about 0.01% of its pairs at config 2), so
+        // that only the rare pairs beyond them take a table search
         float llo[3], lhi[3], ulo[kUpCache];
 #pragma unroll
         for (int g = 0; g < 3; g++) { llo[g] = -INFINITY; lhi[g] = INFINITY; }
@@ -320,7 +324,7 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                     if (!(llo[g] == llo[g]) || !(lhi[g] == lhi[g])) { llo[g] = -INFINITY; lhi[g] = INFINITY; }
                 }
 #pragma unroll
-                for (int g = 0; g < kUpCache; g++) ulo[g] = tu[g * kScM].x;
+                for (int g = 0; g < kUpCache; g++) ulo[g] = tu[(g + 1) * kScM].y * 0x1p100f;
             }
         }
         // the first two steps of the group search from registers
@@ -415,16 +419,25 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                                 okl = b14 || (qml >= lhi[2] && b13) || (qml >= lhi[1] && b12);
                                 c_l = b14 ? 15 : (b13 ? 14 : 13);
                             }
-                            // upper side: c_u = #{g : qp < lo_g} over the cached limits (a prefix, lo being
-                            // monotone), decided when qm >= hi_(c_u); a pair at the last cached limit may
-                            // lie beyond it and takes the table search
+                            // upper side: c_u = #{g : qp < lo_g} over the cached limits, counted on the
+                            // FMA pipe (each term saturates (lo_g - qp) 2^100 to [0, 1]: 1 when qp < lo_g,
+                            // 0 otherwise or for NaN, a fraction only for differences below 2^-100, which
+                            // the verification then refuses), and decided by the verification pair of
+                            // c_u: qm >= hi_(c_u) and qp < lo_(c_u - 1).  A pair at the last cached limit
+                            // may lie beyond it and takes the table search
                             bool oku;
                             {
                                 const float qmu = __fsub_rd(qub, dqu), qpu = __fadd_ru(qub, dqu);
-                                c_u = 0;
+                                const float nq = qpu * -0x1p100f;
+                                float2 acc = make_float2(0.0f, 0.0f);
 #pragma unroll
-                                for (int e = 0; e < kUpCache; e++) c_u += qpu < ulo[e] ? 1 : 0;
-                                oku = qmu >= tu[c_u * kScM].y;
+                                for (int e = 0; e + 1 < kUpCache; e += 2)
+                                    acc = __fadd2_rn(acc, make_float2(__saturatef(__fadd_rn(ulo[e], nq)),
+                                                                      __saturatef(__fadd_rn(ulo[e + 1], nq))));
+                                // in [0, kUpCache]: the table index stays in bounds whatever the terms
+                                c_u = __float_as_int(__fadd_rn(__fadd_rn(acc.x, acc.y), 12582912.0f)) - 0x4B400000;
+                                const float2 ve = tu[c_u * kScM];
+                                oku = qmu >= ve.x && qpu < ve.y;
                                 needx |= (unsigned) (!oku && c_u == kUpCache) << g;
                             }
                             needl |= (unsigned) !okl << g;
@@ -440,7 +453,7 @@ __global__ void __launch_bounds__(kScThreads, 1) scores_tc_kernel(ScArgs a) {
                                 float qlb, qub, dql, dqu;
                                 level_bounds(vl[g], dl[g], un, sqn[j * kScN + 8 * cg + i0 + g], qlb, qub, dql, dqu);
                                 int c;
-                                const bool o = lvt_screen_lim(tu, kScM, __fsub_rd(qub, dqu), __fadd_ru(qub, dqu), c);
+                                const bool o = lvt_screen_ver(tu, kScM, __fsub_rd(qub, dqu), __fadd_ru(qub, dqu), c);
                                 if (wx) {
                                     packed[g] = (packed[g] & 0x0f) | (c << 4);
                                     if (o) needu &= ~(1u << g);

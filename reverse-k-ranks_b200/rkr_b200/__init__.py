@@ -349,13 +349,22 @@ class Index:
         _check(_lib.rkr_index_size_bytes(self._h, C.byref(v)))
         return v.value
 
-    def retrieval(self, method, query, topk, stats=False):
-        """BaseIndex::Retrieval: [n_answered][topk] USER_RANK records (and QUERY_STATS per query)."""
+    def retrieval(self, method, query, topk, stats=False, out=None):
+        """BaseIndex::Retrieval: [n_answered][topk] USER_RANK records (and QUERY_STATS per query).
+
+        `out`, if given, is the caller's C-contiguous USER_RANK array of at least n_query x topk
+        records (for instance one buffer in pinned host memory reused across calls); the result is a
+        view of it."""
         m = METHODS[method] if isinstance(method, str) else int(method)
         q = _f32(query)
         nq = q.shape[0]
         n_rows = max(nq, 100)
-        out = np.zeros((n_rows, topk), USER_RANK)
+        if out is None:
+            out = np.zeros((n_rows, topk), USER_RANK)
+        else:
+            if out.dtype != USER_RANK or not out.flags.c_contiguous or out.size < nq * topk:
+                raise ValueError(f"out must be a C-contiguous USER_RANK array of at least {nq} x {topk} records")
+            out = out.reshape(-1)[: nq * topk].reshape(nq, topk)
         st = np.zeros(n_rows, QUERY_STATS) if stats else None
         na = C.c_int32()
         _check(_lib.rkr_retrieval(self._h, C.c_int32(m), _p(q), C.c_int32(nq), C.c_int32(topk), _p(out), _p(st),

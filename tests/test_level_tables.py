@@ -250,3 +250,108 @@ def test_device_tables_match_the_restatement():
             T, band = want[side]
             assert np.array_equal(tab[u, side, :, 0].view(np.int32), T.view(np.int32)), (u, side)
             np.testing.assert_allclose(tab[u, side, :, 1], band, rtol=1e-5, atol=0)
+
+
+# ---- the pair-scores kernel's upper side: monotone limits, a saturated count, a verification pair ----
+
+def rd32(x):
+    """x (a double) rounded down to binary32 (__fsub_rd / __fadd_rd of binary32 operands)."""
+    r = np.float32(x)
+    return f32_down(r) if float(r) > x else r
+
+
+def ru32(x):
+    r = np.float32(x)
+    return f32_up(r) if float(r) < x else r
+
+
+def verify_rows(T, band):
+    """lvt_limits_row then lvt_verify_row (csrc/rkr_regression.cuh): entry c = (hi_c, lo_(c-1))."""
+    lo = np.array([rd32(float(T[j]) - float(band[j])) for j in range(E)], np.float32)
+    hi = np.array([ru32(float(T[j]) + float(band[j])) for j in range(E)], np.float32)
+    if np.isnan(lo).any() or np.isnan(hi).any():
+        return np.full((E, 2), np.nan, np.float32)
+    lo = np.minimum.accumulate(lo)
+    hi = np.maximum.accumulate(hi[::-1])[::-1]
+    ver = np.empty((E, 2), np.float32)
+    ver[:, 0] = hi
+    ver[0, 1] = np.inf
+    ver[1:, 1] = lo[:-1]
+    return ver
+
+
+def screen_directed(T, band, q, dq):
+    """lvt_screen with the device's directed roundings (rd32 / ru32, exact where the result is)."""
+    c = 0
+    for st in (8, 4, 2, 1):
+        if q < T[c + st - 1]:
+            c += st
+    qm, qp = rd32(float(np.float32(q)) - float(np.float32(dq))), ru32(float(np.float32(q)) + float(np.float32(dq)))
+    ok = True
+    if c < E - 1:
+        ok = qm >= ru32(float(T[c]) + float(band[c]))
+    if c > 0:
+        ok = ok and qp < rd32(float(T[c - 1]) - float(band[c - 1]))
+    return c, bool(ok)
+
+
+def sat(x):
+    return np.float32(0) if np.isnan(x) else np.float32(min(max(float(x), 0.0), 1.0))
+
+
+def upper_screen(ver, q, dq, n_cache=10):
+    """The kernel's upper side for bound score q, its distance dq: (decided, coarse level)."""
+    f32 = np.float32
+    qm, qp = rd32(float(f32(q)) - float(f32(dq))), ru32(float(f32(q)) + float(f32(dq)))
+    with np.errstate(over="ignore", invalid="ignore"):
+        cached = [f32(ver[g + 1, 1] * f32(2.0 ** 100)) for g in range(n_cache)]
+        nq = f32(qp * f32(-2.0 ** 100))
+        acc = [f32(0), f32(0)]
+        for e in range(0, n_cache, 2):
+            acc[0] = f32(acc[0] + sat(f32(cached[e] + nq)))
+            acc[1] = f32(acc[1] + sat(f32(cached[e + 1] + nq)))
+    c = int(np.rint(f32(acc[0] + acc[1])))
+    ok = bool(qm >= ver[c, 0] and qp < ver[c, 1])
+    if not ok and c == n_cache:
+        k = 0
+        for st in (8, 4, 2, 1):
+            if qp < ver[k + st, 1]:
+                k += st
+        c, ok = k, bool(qm >= ver[k, 0] and qp < ver[k, 1])
+    return ok, c
+
+
+@pytest.mark.parametrize("S,n_item", [(512, 17770), (64, 5000)])
+def test_upper_side_count_decides_within_the_table_screen(S, n_item):
+    """Every pair the kernel's upper side decides has the oracle's coarse level, and lvt_screen decides
+    it too, with the same level (the monotone limits only move outward); a verification pair accepts
+    no level but the pair's own."""
+    orc = Oracle()
+    rng = np.random.default_rng(100 + S)
+    rank, recs = users(orc, rng, S, n_item)
+    decided = both = 0
+    for rec in recs:
+        T, band = build_tables(orc, rec, rank, n_item)[1]
+        ver = verify_rows(T, band)
+        probes = list(rng.uniform(float(rec[6]) - 0.1, float(rec[5]) + 0.1, 40))
+        for g in range(E - 1):
+            if np.isfinite(T[g]):
+                t = np.float32(T[g])
+                w = max(float(band[g]), 1e-7)
+                probes += [t, f32_down(t), f32_up(t)] + list(t + np.float32(w) * np.linspace(-3, 3, 7))
+        for q in np.array(probes, np.float32):
+            for dq in (0.0, 1e-6, 1e-3):
+                ok, c = upper_screen(ver, q, dq)
+                c0, ok0 = screen_directed(T, band, float(q), dq)
+                if ok0:
+                    both += 1
+                if not ok:
+                    continue
+                decided += 1
+                assert ok0 and c == c0, (float(q), dq, c, c0, ok0)
+                assert c == coarse(level(orc, rec, rank, n_item, float(q), 1), S)
+                qm, qp = rd32(float(q) - dq), ru32(float(q) + dq)
+                for c2 in range(E):
+                    if c2 != c:
+                        assert not (qm >= ver[c2, 0] and qp < ver[c2, 1]), (float(q), c, c2)
+    assert decided > 0.9 * both, (decided, both)

@@ -190,7 +190,10 @@ __host__ __device__ __forceinline__ int lvt_coarse(int l, int S) {
 __host__ __device__ __forceinline__ int lvt_width(int S) { return (S + kLvEntries - 3) / (kLvEntries - 2) + 1; }
 
 // Coarse level of score q on one side from the table row (entry j of this user at t[j * stride]),
-// and whether every score within dq of q has it.
+// and whether every score within dq of q has it.  This is the decision rule itself; the pair-scores
+// kernel applies it through register-cached boundaries (the lower side) and through the limit and
+// verification-pair forms below (lvt_screen_lim, lvt_screen_ver), which decide a subset of its pairs
+// with the same levels (restated on the CPU in tests/test_level_tables.py).
 __device__ __forceinline__ bool lvt_screen(const float2 *t, int stride, float q, float dq, int &c) {
     int k = 0;
 #pragma unroll

@@ -352,7 +352,7 @@ def kernel_model(name, cfg, nq, stats, method):
 # users' digit tiles, threshold summaries and level tables), streamed once per launch whatever its
 # queries; the writes are the two state bytes per (query, user) pair.  A launch's traffic is the
 # read figure plus the write figure per pair times its pairs.
-NCU_TRAFFIC = {("qsrp_scores_tc", "QSRPNormalLP"): (563.645e6, 171.521e6 / (200 * 480189.0))}
+NCU_TRAFFIC = {("qsrp_scores_tc", "QSRPNormalLP"): (563.217e6, 170.901e6 / (200 * 480189.0))}
 
 # Nominal dense tensor-core peaks of one B200 (T ops/s), for the tensor_ops figures.
 TENSOR_PEAK_NOMINAL = {"qsrp_scores_tc": ("int8", 4500.0), "refine_tc": ("int8", 4500.0)}
